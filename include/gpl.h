@@ -1,0 +1,223 @@
+/*
+ * gpl_b200 — the C ABI of the B200 global-placement engine.
+ *
+ * The engine is a drop-in for the `global_placement` command of vyges-gpl. Every entry point
+ * below names the reference interface it replaces (file:line within the vyges-gpl crate).
+ * Plain C types only: the caller owns the arrays it passes; the library copies what it keeps.
+ * All coordinates are database units (DBU).
+ */
+#ifndef GPL_B200_H
+#define GPL_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* How a run ended: `Stop` (src/log.rs:18-21) and the CLI's exit codes (src/main.rs:503-509).
+ * GPL_DEVICE_FAULT has no reference counterpart: a CUDA error, reported with its text in
+ * `reason`; the process is never aborted. */
+#define GPL_PLACED 0
+#define GPL_ERROR 2
+#define GPL_REFUSED 3
+#define GPL_DEVICE_FAULT (-1)
+
+/* Outcome of a placed run (src/run.rs:35-48). */
+#define GPL_OUTCOME_PLACED 0
+#define GPL_OUTCOME_INITIALLY_PLACED 1
+
+/* Instance flags (`DbInst`, src/placer_base.rs:52-75). */
+#define GPL_INST_CORE_AUTO_PLACEABLE 1u
+#define GPL_INST_BLOCK 2u
+#define GPL_INST_FIXED 4u
+#define GPL_INST_PLACED 8u
+#define GPL_INST_HAS_HALO 16u
+
+/* Orientations (`orient_point`, src/initial_place.rs:68-79). */
+#define GPL_R0 0
+#define GPL_R90 1
+#define GPL_R180 2
+#define GPL_R270 3
+#define GPL_MY 4
+#define GPL_MYR90 5
+#define GPL_MX 6
+#define GPL_MXR90 7
+
+/* Port flags (`Port`, src/placer_base.rs:102-107). */
+#define GPL_BTERM_PLACED 1u
+#define GPL_BTERM_FIXED 2u
+
+/*
+ * The design as the placer reads it: `Design` (src/placer_base.rs:185-206) flattened into
+ * arrays. Rectangles are 4 int32 (lx, ly, ux, uy). CSR starts have one more entry than their
+ * owners. Name arrays may be NULL (names are then generated: "i<k>", "n<k>", "p<k>", "g<k>").
+ */
+typedef struct gpl_design {
+  int32_t dbu;
+  int32_t die[4];
+  int32_t core[4];
+  int32_t n_rows;
+  const int32_t *row_box;      /* 4 per row */
+  const uint8_t *row_pad;      /* the row's site class is PAD */
+  const int32_t *row_site;     /* 2 per row: site width, height */
+  int32_t n_insts;
+  const int32_t *inst_box;     /* 4 per instance: getBBox() */
+  const uint32_t *inst_flags;  /* GPL_INST_* */
+  const int32_t *inst_group;   /* index into the groups, -1 for none */
+  const int32_t *inst_halo;    /* 4 per instance, read when GPL_INST_HAS_HALO; may be NULL */
+  const int32_t *inst_signal_pins;
+  const uint8_t *inst_orient;  /* GPL_R0 .. GPL_MXR90 */
+  const int32_t *inst_master;  /* 2 per instance: master width, height */
+  const char *const *inst_name;
+  const char *const *inst_master_name;
+  int32_t n_nets;
+  const uint8_t *net_signal;   /* SIGNAL or CLOCK */
+  const int64_t *net_iterm_start;
+  const int32_t *iterm_inst;
+  const int32_t *iterm_shape;  /* 4 per terminal, master coordinates */
+  const uint8_t *iterm_has_shape;
+  const int32_t *iterm_order;  /* position among its instance's terminals */
+  const int64_t *net_bterm_start;
+  const int32_t *bterm_box;    /* 4 per port */
+  const uint8_t *bterm_flags;  /* GPL_BTERM_* */
+  const char *const *net_name;
+  const char *const *bterm_name;
+  int32_t n_groups;
+  const char *const *group_name;
+  const uint8_t *group_visual_debug;
+  const int32_t *group_region; /* -1 for none */
+  int32_t n_regions;
+  const int32_t *region_bound_start;
+  const int32_t *region_bounds; /* 4 per boundary */
+  const int32_t *region_group_start;
+  const int32_t *region_groups;
+  int32_t n_blockages;
+  const int32_t *blockage_box;
+  const int32_t *blockage_inst;       /* -1 for none */
+  const uint8_t *blockage_inst_fixed;
+  const float *blockage_max_density;
+} gpl_design_t;
+
+/*
+ * The routing services routability-driven placement calls: `trait Router`
+ * (src/route_base.rs:90-126), the RUDY part. Each returns 0 on success. `net_term_boxes` is
+ * called twice per pass: with boxes == NULL to get the count, then to fill `cap` entries.
+ */
+typedef struct gpl_router {
+  void *user;
+  /* Router::write_locations (src/route_base.rs:92): n triples (design instance, x, y). */
+  int (*write_locations)(void *user, int64_t n, const int32_t *locations);
+  /* Router::rudy_inputs (src/route_base.rs:99): die, grid, tile size, up to 32 pitches. */
+  int (*rudy_inputs)(void *user, int32_t die[4], int32_t *x_grids, int32_t *y_grids,
+                     int32_t *tile_size, int32_t *n_pitches, int32_t pitches[32]);
+  /* Router::capacity_reduction (src/route_base.rs:102): x-major (capacity, reduction) bytes. */
+  int (*capacity_reduction)(void *user, uint8_t *cap_red, int64_t n_tiles);
+  /* Router::net_term_boxes (src/route_base.rs:125): design net index and box per net. */
+  int64_t (*net_term_boxes)(void *user, int32_t *net_index, int32_t *boxes, int64_t cap);
+} gpl_router_t;
+
+/*
+ * What one run returns: the JSON report's fields (src/main.rs:249-262, :362-371) and the
+ * written placement (`placed_locations`, src/nesterov.rs:4099-4110). Library-owned memory,
+ * released by gpl_result_free.
+ */
+typedef struct gpl_result {
+  int32_t status;        /* GPL_PLACED / GPL_ERROR / GPL_REFUSED / GPL_DEVICE_FAULT */
+  int32_t outcome;       /* GPL_OUTCOME_* when placed */
+  char code[16];         /* "GPL-0307" on GPL_ERROR */
+  char *reason;          /* refusal or device-fault text */
+  char *lines;           /* the run's lines, each ended by '\n' */
+  char *trace;           /* raw-value probe lines, each ended by '\n' */
+  int64_t insts, nets, pins;
+  int32_t iterations;    /* final Nesterov iteration, -1 when Nesterov did not run */
+  int32_t n_bases;
+  int32_t *bases;        /* 4 per base: group (-1 top level), placed, fixed, dummies */
+  int64_t n_locations;
+  int32_t *locations;    /* 3 per instance: design instance, lower-left x, lower-left y */
+  int64_t final_hpwl;    /* the placer's HPWL over its pins at the end */
+  float final_overflow;  /* average unscaled overflow at the end */
+  int64_t trials;        /* back-tracking trials run */
+  double seconds_initial_place;
+  double seconds_nesterov;
+} gpl_result_t;
+
+typedef struct gpl_ctx gpl_ctx;
+
+/* One context binds one CUDA device and its own stream. Calls on one context are not
+ * reentrant; contexts are independent. Returns NULL when the device cannot be used. */
+gpl_ctx *gpl_create(int device);
+void gpl_destroy(gpl_ctx *ctx);
+
+/* Engine options with no reference counterpart (the reference runs on one thread):
+ *   "poisson" = "mixed" (split-BF16 tcgen05 DCT GEMMs, the default) | "fp32" (SIMT GEMMs)
+ *   "trace"   = "0" | "1" (probe lines, as the reference's `Log.trace`)
+ * Returns 0, or -1 for an unknown name or value. */
+int gpl_set_option(gpl_ctx *ctx, const char *name, const char *value);
+
+/* The `global_placement` proc: `run::global_placement` (src/run.rs:115). `argv` holds the
+ * command's arguments (src/run.rs:16-30 keys and flags); `router` may be NULL (routability
+ * is then refused, as src/run.rs:192). Returns out->status. */
+int gpl_global_placement(gpl_ctx *ctx, const gpl_design_t *design, int argc,
+                         const char *const *argv, const gpl_router_t *router,
+                         gpl_result_t *out);
+void gpl_result_free(gpl_result_t *out);
+
+/* A stand-in for the database's router (src/db_router.rs:260-368): a uniform tile grid over
+ * the die, the given pitches, every tile with `capacity` and no reduction, and each net's
+ * terminal box from its pin shapes at the written locations. No reference counterpart. */
+gpl_router_t *gpl_synthetic_router_create(const gpl_design_t *design, int32_t tile_size,
+                                          int32_t n_pitches, const int32_t *pitches,
+                                          uint8_t capacity);
+void gpl_synthetic_router_destroy(gpl_router_t *router);
+
+/* ---- per-kernel entry points, for per-kernel parity and benchmarks ----
+ * Device pointers on the caller's stream (cudaStream_t passed as void*). Each returns 0, or a
+ * CUDA error code. None has a reference entry point of its own; each names the function whose
+ * result it computes. */
+
+/* The bin-density scatter `update_bins_gcell_density_area` (src/nesterov.rs:2218-2263):
+ * cells' density boxes (centre cx, cy; half sizes hx, hy) over a grid of nx * ny bins whose
+ * edges are bx[0..nx], by[0..ny]; kind 0 std cell, 1 macro, 2 filler. Writes the int64
+ * accumulators inst[nx*ny], filler[nx*ny] (x-major: index x*ny + y), zeroed first. */
+int gpl_kernel_density_scatter(int64_t n_cells, const int32_t *cx, const int32_t *cy,
+                               const int32_t *hx, const int32_t *hy, const float *scale,
+                               const uint8_t *kind, int32_t nx, int32_t ny, const int32_t *bx,
+                               const int32_t *by, double size_x, double size_y,
+                               float target_density, int64_t *inst, int64_t *filler,
+                               void *stream);
+
+/* `Fft::solve` (src/nesterov.rs:412-444) without the potential: density[nx*ny] (x-major) to
+ * field_x, field_y. mode 0 = FP32 SIMT GEMMs, 1 = split-BF16 tcgen05 GEMMs. wx[nx], wy[ny] are
+ * the wavenumbers. `workspace` holds gpl_poisson_workspace_bytes(nx, ny) bytes. */
+size_t gpl_poisson_workspace_bytes(int32_t nx, int32_t ny);
+int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy,
+                       const float *density, float *field_x, float *field_y, int mode,
+                       void *workspace, void *stream);
+
+/* `update_wirelength_force_wa` + `wl_gradient_pin` (src/nesterov.rs:2325-2414): per net (pins
+ * net-major, net_start[n_nets+1]), per pin its position px, py; coefficients cx, cy; writes
+ * each pin's force (gmin - gmax) scaled by its net's weight into grad[2*n_pins]. */
+int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *px,
+                  const int32_t *py, const float *net_weight, float coef_x, float coef_y,
+                  float *grad, void *stream);
+
+/* The initial placement's solver `bicgstab` (src/bicgstab.rs:615-669) on a CSR matrix with
+ * FP64 inner products; x is the start point and the result. Writes iterations and error. */
+int gpl_kernel_bicgstab(int64_t n, const int64_t *row_start, const int32_t *cols,
+                        const float *vals, const float *rhs, float *x, int32_t max_iters,
+                        int32_t *iterations, float *error, void *stream);
+
+/* RUDY `Rudy::calculate` (src/route_base.rs:191-253): net boxes (4 per net) into a tile
+ * demand map (x-major, cnt_x * cnt_y) over tiles of `tile_size` from the die's lower-left,
+ * the last column and row stretched to `die_ux`, `die_uy`. */
+int gpl_kernel_rudy(int64_t n_nets, const int32_t *boxes, int32_t die_lx, int32_t die_ly,
+                    int32_t die_ux, int32_t die_uy, int32_t cnt_x, int32_t cnt_y,
+                    int32_t tile_size, int32_t wire_width, float *demand, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPL_B200_H */

@@ -1,0 +1,71 @@
+"""ctypes binding of the oracle library (oracle/_build/liboracle.so)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+from gpl_b200.design import gpl_result_t, result_to_dict
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build(force=False):
+    """Compile the oracle with its Makefile (g++ -O2 -ffp-contract=off)."""
+    srcs = [os.path.join(HERE, f) for f in ("oracle_place.cpp", "oracle_nesterov.cpp", "oracle.h")]
+    if force or not os.path.exists(SO) or any(os.path.getmtime(s) > os.path.getmtime(SO) for s in srcs):
+        subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+    return SO
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO):
+            build()
+        _lib = C.CDLL(SO)
+        _lib.oracle_global_placement.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_char_p), C.c_void_p, C.c_int, C.POINTER(gpl_result_t)]
+        _lib.oracle_result_free.argtypes = [C.POINTER(gpl_result_t)]
+        _lib.oracle_fast_exp.restype = C.c_float
+        _lib.oracle_fast_exp.argtypes = [C.c_float]
+        _lib.oracle_wavenumber_x.restype = C.c_float
+        _lib.oracle_wavenumber_x.argtypes = [C.c_int, C.c_int]
+        _lib.oracle_wavenumber_y.restype = C.c_float
+        _lib.oracle_wavenumber_y.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float]
+        _lib.oracle_round_down_pow2.restype = C.c_uint32
+        _lib.oracle_union_area.restype = C.c_int64
+        _lib.oracle_distance.restype = C.c_float
+        _lib.oracle_derived_reference_hpwl.restype = C.c_float
+        _lib.oracle_derived_reference_hpwl.argtypes = [C.c_float, C.c_int64]
+        _lib.oracle_fmt.argtypes = [C.c_char_p, C.c_double, C.c_int, C.c_int, C.c_char_p, C.c_int]
+        _lib.oracle_extend_size_by_scale.restype = C.c_int64
+        _lib.oracle_extend_size_by_scale.argtypes = [C.c_void_p, C.c_double]
+        _lib.oracle_eigen_sum.restype = C.c_float
+        _lib.oracle_eigen_sum.argtypes = [C.c_int64, C.c_void_p]
+        _lib.oracle_csr_from_triplets.restype = C.c_int64
+        _lib.oracle_csr_from_triplets.argtypes = [C.c_int64, C.c_int64] + [C.c_void_p] * 6
+        _lib.oracle_bicgstab.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_int, C.c_void_p, C.c_void_p]
+        _lib.oracle_mt19937_nth.restype = C.c_uint32
+        _lib.oracle_mt19937_nth.argtypes = [C.c_uint32, C.c_int64]
+        _lib.oracle_normal_draws.restype = C.c_uint32
+        _lib.oracle_normal_draws.argtypes = [C.c_uint32, C.c_double, C.c_int, C.c_void_p]
+        _lib.oracle_max_iter_takes_snapshot.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_float, C.c_float, C.c_int64]
+        _lib.oracle_poisson.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float] + [C.c_void_p] * 6
+        _lib.oracle_dct1.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        _lib.oracle_transform2.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+    return _lib
+
+
+def global_placement(design, args, router=None, trace=False):
+    """Run the reference's `global_placement` command on the CPU; the JSON-shaped report."""
+    L = lib()
+    cd = design.c_struct()
+    argv = (C.c_char_p * max(len(args), 1))(*[a.encode() for a in args])
+    res = gpl_result_t()
+    L.oracle_global_placement(C.byref(cd), len(args), argv, router, 1 if trace else 0, C.byref(res))
+    try:
+        return result_to_dict(res)
+    finally:
+        L.oracle_result_free(C.byref(res))

@@ -1,0 +1,201 @@
+// The per-kernel C entry points (include/gpl.h) and the synthetic router.
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+#include "../../../include/gpl.h"
+#include "../kernels/bicgstab.h"
+#include "../kernels/engine_kernels.h"
+#include "../kernels/rudy.h"
+
+using namespace gpl;
+
+extern "C" {
+
+int gpl_kernel_density_scatter(int64_t n_cells, const int32_t *cx, const int32_t *cy, const int32_t *hx, const int32_t *hy, const float *scale, const uint8_t *kind, int32_t nx, int32_t ny, int32_t grid_lx, int32_t grid_ly, const int32_t *bx, const int32_t *by, double size_x, double size_y, float target_density, int64_t *inst, int64_t *filler, void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  size_t nb = (size_t)nx * ny;
+  cudaError_t e = cudaMemsetAsync(inst, 0, nb * sizeof(int64_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(filler, 0, nb * sizeof(int64_t), s);
+  if (e != cudaSuccess) return (int)e;
+  if (n_cells <= 0) return 0;
+  RegionArgs r{};
+  r.n_cells = (int32_t)n_cells;
+  r.nx = nx;
+  r.ny = ny;
+  r.lx = grid_lx;
+  r.ly = grid_ly;
+  r.size_x = size_x;
+  r.size_y = size_y;
+  r.target_density = target_density;
+  r.bx = bx;
+  r.by = by;
+  r.acc_inst = inst;
+  r.acc_fill = filler;
+  CellArgs c{};
+  c.dcx = const_cast<int32_t *>(cx);
+  c.dcy = const_cast<int32_t *>(cy);
+  c.hx = hx;
+  c.hy = hy;
+  c.dscale = scale;
+  c.kind = kind;
+  k_place_cells<<<(unsigned)((n_cells + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, s>>>(r, c, PLACE_GIVEN, 0.0f, 0.0f, nullptr);
+  return (int)cudaGetLastError();
+}
+
+int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy, const float *density, float *field_x, float *field_y, int mode, void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaSuccess;
+  PoissonPlan *p = poisson_plan_create(nx, ny, wx, wy, mode, &e);
+  if (!p) return (int)e;
+  int ld = 0;
+  __nv_bfloat16 *split = poisson_split_input(p, &ld);
+  if (split) {
+    // the tensor-core path reads the density as split bf16: convert it
+    e = poisson_split_density(p, density, s);
+  }
+  if (e == cudaSuccess) e = poisson_solve(p, density, field_x, field_y, s);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  poisson_plan_destroy(p);
+  return (int)(e != cudaSuccess ? e : e2);
+}
+
+int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, const float *net_weight, float coef_x, float coef_y, float *grad, void *stream) {
+  if (n_nets <= 0) return 0;
+  WaArgs w{};
+  w.n_nets = (int32_t)n_nets;
+  w.net_start = net_start;
+  w.net_weight = net_weight;
+  w.pin_base = reinterpret_cast<const int2 *>(pin_xy);
+  w.pin_grad = reinterpret_cast<float2 *>(grad);
+  k_wa<<<(unsigned)((n_nets + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, (cudaStream_t)stream>>>(w, coef_x, coef_y);
+  return (int)cudaGetLastError();
+}
+
+int gpl_kernel_bicgstab(int64_t n, const int64_t *row_start, const int32_t *cols, const float *vals, const float *rhs, float *x, int32_t max_iters, int32_t *iterations, float *error, void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  void *scratch = nullptr;
+  cudaError_t e = cudaMalloc(&scratch, bicgstab_scratch_bytes(n));
+  if (e != cudaSuccess) return (int)e;
+  CsrDev A{n, row_start, cols, vals};
+  BicgResult r{};
+  e = bicgstab_solve(A, rhs, x, max_iters, scratch, s, &r);
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  cudaFree(scratch);
+  *iterations = r.iterations;
+  *error = r.error;
+  return (int)(e != cudaSuccess ? e : e2);
+}
+
+int gpl_kernel_rudy(int64_t n_nets, const int32_t *boxes, int32_t die_lx, int32_t die_ly, int32_t die_ux, int32_t die_uy, int32_t cnt_x, int32_t cnt_y, int32_t tile_size, int32_t wire_width, float *demand, void *stream) {
+  RudyGrid g{die_lx, die_ly, die_ux, die_uy, cnt_x, cnt_y, tile_size, wire_width};
+  return (int)rudy_demand(g, n_nets, reinterpret_cast<const int4 *>(boxes), demand, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------- the synthetic router
+struct SynthRouter {
+  gpl_router_t r;
+  int32_t die[4];
+  int32_t tile;
+  std::vector<int32_t> pitches;
+  uint8_t capacity;
+  std::vector<int32_t> inst_xy;   // lower-left per design instance
+  std::vector<int64_t> net_iterm_start, net_bterm_start;
+  std::vector<int32_t> iterm_inst, iterm_shape, bterm_box;
+  std::vector<uint8_t> bterm_placed;
+};
+
+static int sr_write(void *u, int64_t n, const int32_t *loc) {
+  SynthRouter *s = (SynthRouter *)u;
+  for (int64_t k = 0; k < n; k++) {
+    int32_t di = loc[3 * k];
+    if (di < 0 || (size_t)di * 2 + 1 >= s->inst_xy.size()) return 1;
+    s->inst_xy[2 * di] = loc[3 * k + 1];
+    s->inst_xy[2 * di + 1] = loc[3 * k + 2];
+  }
+  return 0;
+}
+static int sr_inputs(void *u, int32_t die[4], int32_t *xg, int32_t *yg, int32_t *ts, int32_t *np, int32_t p[32]) {
+  SynthRouter *s = (SynthRouter *)u;
+  std::memcpy(die, s->die, sizeof s->die);
+  *xg = std::max(1, (s->die[2] - s->die[0]) / s->tile);
+  *yg = std::max(1, (s->die[3] - s->die[1]) / s->tile);
+  *ts = s->tile;
+  *np = (int32_t)std::min<size_t>(32, s->pitches.size());
+  for (int i = 0; i < *np; i++) p[i] = s->pitches[i];
+  return 0;
+}
+static int sr_cap(void *u, uint8_t *cr, int64_t n) {
+  SynthRouter *s = (SynthRouter *)u;
+  for (int64_t i = 0; i < n; i++) {
+    cr[2 * i] = s->capacity;
+    cr[2 * i + 1] = 0;
+  }
+  return 0;
+}
+static int64_t sr_boxes(void *u, int32_t *idx, int32_t *boxes, int64_t cap) {
+  SynthRouter *s = (SynthRouter *)u;
+  int64_t nn = (int64_t)s->net_iterm_start.size() - 1;
+  if (!boxes) return nn;
+  for (int64_t n = 0; n < nn && n < cap; n++) {
+    int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+    for (int64_t t = s->net_iterm_start[n]; t < s->net_iterm_start[n + 1]; t++) {
+      int32_t i = s->iterm_inst[t];
+      const int32_t *sh = &s->iterm_shape[4 * t];
+      int32_t x = s->inst_xy[2 * i], y = s->inst_xy[2 * i + 1];
+      lx = std::min(lx, x + sh[0]);
+      ly = std::min(ly, y + sh[1]);
+      ux = std::max(ux, x + sh[2]);
+      uy = std::max(uy, y + sh[3]);
+    }
+    for (int64_t t = s->net_bterm_start[n]; t < s->net_bterm_start[n + 1]; t++) {
+      if (!s->bterm_placed[t]) continue;
+      const int32_t *b = &s->bterm_box[4 * t];
+      lx = std::min(lx, b[0]);
+      ly = std::min(ly, b[1]);
+      ux = std::max(ux, b[2]);
+      uy = std::max(uy, b[3]);
+    }
+    idx[n] = (int32_t)n;
+    boxes[4 * n] = lx;
+    boxes[4 * n + 1] = ly;
+    boxes[4 * n + 2] = ux;
+    boxes[4 * n + 3] = uy;
+  }
+  return std::min(nn, cap);
+}
+
+gpl_router_t *gpl_synthetic_router_create(const gpl_design_t *d, int32_t tile_size, int32_t n_pitches, const int32_t *pitches, uint8_t capacity) {
+  if (tile_size <= 0) return nullptr;
+  SynthRouter *s = new SynthRouter();
+  std::memcpy(s->die, d->die, sizeof s->die);
+  s->tile = tile_size;
+  s->pitches.assign(pitches, pitches + std::max(0, n_pitches));
+  s->capacity = capacity;
+  s->inst_xy.resize(2 * (size_t)d->n_insts);
+  for (int32_t i = 0; i < d->n_insts; i++) {
+    s->inst_xy[2 * i] = d->inst_box[4 * i];
+    s->inst_xy[2 * i + 1] = d->inst_box[4 * i + 1];
+  }
+  s->net_iterm_start.assign(d->net_iterm_start, d->net_iterm_start + d->n_nets + 1);
+  s->net_bterm_start.assign(d->net_bterm_start, d->net_bterm_start + d->n_nets + 1);
+  int64_t nt = s->net_iterm_start.back(), nb = s->net_bterm_start.back();
+  s->iterm_inst.assign(d->iterm_inst, d->iterm_inst + nt);
+  s->iterm_shape.assign(d->iterm_shape, d->iterm_shape + 4 * nt);
+  s->bterm_box.assign(d->bterm_box, d->bterm_box + 4 * nb);
+  s->bterm_placed.resize(nb);
+  for (int64_t t = 0; t < nb; t++) s->bterm_placed[t] = d->bterm_flags[t] & GPL_BTERM_PLACED;
+  s->r.user = s;
+  s->r.write_locations = sr_write;
+  s->r.rudy_inputs = sr_inputs;
+  s->r.capacity_reduction = sr_cap;
+  s->r.net_term_boxes = sr_boxes;
+  return &s->r;
+}
+
+void gpl_synthetic_router_destroy(gpl_router_t *r) {
+  if (r) delete (SynthRouter *)r->user;
+}
+
+}  // extern "C"

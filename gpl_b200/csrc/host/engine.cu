@@ -1,0 +1,413 @@
+// The device engine: HBM-resident Nesterov state, the trial's launches, the solves.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "../kernels/bicgstab.h"
+#include "../kernels/engine_kernels.h"
+#include "engine.h"
+
+namespace gpl {
+
+struct Engine::Region {
+  RegionArgs args{};
+  int32_t *bx = nullptr, *by = nullptr;
+  float *scaled = nullptr, *density = nullptr, *fx = nullptr, *fy = nullptr;
+  int64_t *np = nullptr, *npu = nullptr, *acc_inst = nullptr, *acc_fill = nullptr;
+  float2 *slot[S_NUM] = {};
+  int64_t cell_off = 0, n_cells = 0;
+  PoissonPlan *plan = nullptr;
+  double *part = nullptr;
+  int nb_bins = 0, nb_cells = 0;
+  __nv_bfloat16 *dens_split = nullptr;
+  int split_ld = 0;
+};
+
+static int blocks_for(int64_t n, int per = kThreadsPerBlock) { return (int)std::max<int64_t>(1, (n + per - 1) / per); }
+
+void Engine::check(cudaError_t e, const char *where) {
+  if (e != cudaSuccess && err_.code == cudaSuccess) {
+    err_.code = e;
+    err_.where = where;
+  }
+}
+
+Engine::Engine(int device) : device_(device) {
+  check(cudaSetDevice(device), "cudaSetDevice");
+  if (!failed()) check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+}
+
+Engine::~Engine() {
+  release();
+  if (ip_scratch_) cudaFree(ip_scratch_);
+  cudaFree(ip_rs_);
+  cudaFree(ip_cols_);
+  cudaFree(ip_vals_);
+  cudaFree(ip_b_);
+  cudaFree(ip_x_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+template <class T>
+static cudaError_t dmalloc(T **p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  return cudaMalloc((void **)p, n * sizeof(T));
+}
+template <class T>
+static cudaError_t upload_vec(T **p, const std::vector<T> &v, cudaStream_t s) {
+  cudaError_t e = dmalloc(p, v.size());
+  if (e != cudaSuccess || v.empty()) return e;
+  return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+// ---------------------------------------------------------------- initial placement
+Solve Engine::solve(const Csr &m, const std::vector<float> &rhs, std::vector<float> &x, int max_iters) {
+  Solve out{0, NAN, false};
+  if (failed()) return out;
+  int64_t n = m.n, nnz = m.starts[n];
+  if ((size_t)n > ip_n_cap_) {
+    cudaFree(ip_rs_);
+    cudaFree(ip_b_);
+    cudaFree(ip_x_);
+    if (ip_scratch_) cudaFree(ip_scratch_);
+    check(dmalloc(&ip_rs_, n + 1), "ip alloc");
+    check(dmalloc(&ip_b_, n), "ip alloc");
+    check(dmalloc(&ip_x_, n), "ip alloc");
+    ip_scratch_bytes_ = bicgstab_scratch_bytes(n);
+    check(cudaMalloc(&ip_scratch_, ip_scratch_bytes_), "ip scratch");
+    ip_n_cap_ = (size_t)n;
+  }
+  if ((size_t)nnz > ip_nnz_cap_) {
+    cudaFree(ip_cols_);
+    cudaFree(ip_vals_);
+    size_t cap = (size_t)(nnz * 1.25) + 16;
+    check(dmalloc(&ip_cols_, cap), "ip alloc");
+    check(dmalloc(&ip_vals_, cap), "ip alloc");
+    ip_nnz_cap_ = cap;
+  }
+  if (failed()) return out;
+  cudaStream_t s = stream_;
+  check(cudaMemcpyAsync(ip_rs_, m.starts.data(), (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s), "ip h2d");
+  if (nnz) {
+    check(cudaMemcpyAsync(ip_cols_, m.cols.data(), nnz * sizeof(int32_t), cudaMemcpyHostToDevice, s), "ip h2d");
+    check(cudaMemcpyAsync(ip_vals_, m.vals.data(), nnz * sizeof(float), cudaMemcpyHostToDevice, s), "ip h2d");
+  }
+  if (n) {
+    check(cudaMemcpyAsync(ip_b_, rhs.data(), n * sizeof(float), cudaMemcpyHostToDevice, s), "ip h2d");
+    check(cudaMemcpyAsync(ip_x_, x.data(), n * sizeof(float), cudaMemcpyHostToDevice, s), "ip h2d");
+  }
+  CsrDev A{n, ip_rs_, ip_cols_, ip_vals_};
+  BicgResult r{};
+  check(bicgstab_solve(A, ip_b_, ip_x_, max_iters, ip_scratch_, s, &r), "bicgstab");
+  if (n) check(cudaMemcpyAsync(x.data(), ip_x_, n * sizeof(float), cudaMemcpyDeviceToHost, s), "ip d2h");
+  check(cudaStreamSynchronize(s), "ip sync");
+  out.iterations = r.iterations;
+  out.error = r.error;
+  out.converged = r.converged;
+  return out;
+}
+
+// ---------------------------------------------------------------- Nesterov state
+void Engine::free_globals() {
+  void *ptrs[] = {dcx_, dcy_, hx_, hy_, dscale_, area_, kind_, locked_, cell_pin_start_, cell_pins_, net_start_, net_order_, pin_cell_, pin_base_, net_weight_, pin_grad_, hpwl_acc_, dev_scal_};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  dcx_ = dcy_ = hx_ = hy_ = nullptr;
+  dscale_ = area_ = nullptr;
+  kind_ = locked_ = nullptr;
+  cell_pin_start_ = nullptr;
+  cell_pins_ = nullptr;
+  net_start_ = nullptr;
+  net_order_ = pin_cell_ = nullptr;
+  pin_base_ = nullptr;
+  net_weight_ = nullptr;
+  pin_grad_ = nullptr;
+  hpwl_acc_ = nullptr;
+  dev_scal_ = nullptr;
+}
+
+void Engine::release() {
+  for (Region *r : regions_) {
+    void *ptrs[] = {r->bx, r->by, r->scaled, r->density, r->fx, r->fy, r->np, r->npu, r->acc_inst, r->acc_fill, r->part};
+    for (void *p : ptrs)
+      if (p) cudaFree(p);
+    for (int k = 0; k < S_NUM; k++)
+      if (r->slot[k]) cudaFree(r->slot[k]);
+    poisson_plan_destroy(r->plan);
+    delete r;
+  }
+  regions_.clear();
+  free_globals();
+}
+
+void Engine::upload(const EngineSetup &s) {
+  release();
+  if (failed()) return;
+  cudaStream_t st = stream_;
+  n_cells_ = (int64_t)s.hx.size();
+  n_pins_ = (int64_t)s.pin_cell.size();
+  n_nets_ = (int32_t)(s.net_start.size() - 1);
+  check(upload_vec(&dcx_, s.dcx, st), "upload cells");
+  check(upload_vec(&dcy_, s.dcy, st), "upload cells");
+  check(upload_vec(&hx_, s.hx, st), "upload cells");
+  check(upload_vec(&hy_, s.hy, st), "upload cells");
+  check(upload_vec(&dscale_, s.dscale, st), "upload cells");
+  check(upload_vec(&area_, s.area, st), "upload cells");
+  check(upload_vec(&kind_, s.kind, st), "upload cells");
+  any_locked_ = std::any_of(s.locked.begin(), s.locked.end(), [](uint8_t v) { return v != 0; });
+  if (any_locked_) check(upload_vec(&locked_, s.locked, st), "upload cells");
+  check(upload_vec(&cell_pin_start_, s.cell_pin_start, st), "upload cells");
+  check(upload_vec(&cell_pins_, s.cell_pins, st), "upload cells");
+  check(upload_vec(&net_start_, s.net_start, st), "upload nets");
+  // nets in degree order: a warp's threads walk nets of one length
+  std::vector<int32_t> order(n_nets_);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return s.net_start[a + 1] - s.net_start[a] < s.net_start[b + 1] - s.net_start[b]; });
+  check(upload_vec(&net_order_, order, st), "upload nets");
+  check(upload_vec(&pin_cell_, s.pin_cell, st), "upload pins");
+  check(dmalloc(&pin_base_, n_pins_), "upload pins");
+  if (n_pins_) check(cudaMemcpyAsync(pin_base_, s.pin_base.data(), n_pins_ * sizeof(int2), cudaMemcpyHostToDevice, st), "upload pins");
+  check(upload_vec(&net_weight_, s.net_weight, st), "upload nets");
+  check(dmalloc(&pin_grad_, n_pins_), "alloc pins");
+  check(dmalloc(&hpwl_acc_, 1), "alloc");
+  check(dmalloc(&dev_scal_, s.regions.size()), "alloc");
+  host_scal_.assign(s.regions.size(), RegionScalars{});
+  for (const RegionSetup &rs : s.regions) {
+    Region *r = new Region();
+    regions_.push_back(r);
+    int64_t nb = (int64_t)rs.nx * rs.ny;
+    r->cell_off = rs.cell_off;
+    r->n_cells = rs.n_cells;
+    check(upload_vec(&r->bx, rs.bx, st), "upload bins");
+    check(upload_vec(&r->by, rs.by, st), "upload bins");
+    check(upload_vec(&r->scaled, rs.scaled, st), "upload bins");
+    check(upload_vec(&r->np, rs.non_place, st), "upload bins");
+    check(upload_vec(&r->npu, rs.non_place_u, st), "upload bins");
+    check(dmalloc(&r->acc_inst, nb), "alloc bins");
+    check(dmalloc(&r->acc_fill, nb), "alloc bins");
+    check(dmalloc(&r->density, nb), "alloc bins");
+    check(dmalloc(&r->fx, nb), "alloc bins");
+    check(dmalloc(&r->fy, nb), "alloc bins");
+    if (!failed()) {
+      check(cudaMemsetAsync(r->acc_inst, 0, nb * sizeof(int64_t), st), "memset");
+      check(cudaMemsetAsync(r->acc_fill, 0, nb * sizeof(int64_t), st), "memset");
+    }
+    for (int k = 0; k < S_NUM; k++) {
+      check(dmalloc(&r->slot[k], rs.n_cells), "alloc slots");
+      if (!failed()) check(cudaMemsetAsync(r->slot[k], 0, std::max<int64_t>(rs.n_cells, 1) * sizeof(float2), st), "memset");
+    }
+    r->nb_bins = (int)std::min<int64_t>(blocks_for(nb), 148 * 4);
+    r->nb_cells = blocks_for(rs.n_cells);
+    check(dmalloc(&r->part, (size_t)std::max(r->nb_bins * 2, r->nb_cells * 4)), "alloc partials");
+    if (!failed()) {
+      cudaError_t pe = cudaSuccess;
+      r->plan = poisson_plan_create(rs.nx, rs.ny, rs.wx.data(), rs.wy.data(), poisson_mode_, &pe);
+      check(pe, poisson_mode_ == 0 ? "poisson plan (fp32)" : "poisson plan (split-bf16 tcgen05)");
+      if (r->plan) r->dens_split = poisson_split_input(r->plan, &r->split_ld);
+    }
+    RegionArgs &a = r->args;
+    a.n_cells = (int32_t)rs.n_cells;
+    a.nx = rs.nx;
+    a.ny = rs.ny;
+    a.lx = rs.lx;
+    a.ly = rs.ly;
+    a.ux = rs.ux;
+    a.uy = rs.uy;
+    a.size_x = rs.size_x;
+    a.size_y = rs.size_y;
+    a.target_density = rs.target_density;
+    a.bx = r->bx;
+    a.by = r->by;
+    a.scaled = r->scaled;
+    a.non_place = r->np;
+    a.non_place_u = r->npu;
+    a.acc_inst = r->acc_inst;
+    a.acc_fill = r->acc_fill;
+    a.density = r->density;
+    a.field_x = r->fx;
+    a.field_y = r->fy;
+  }
+  check(cudaStreamSynchronize(st), "upload sync");
+}
+
+void Engine::update_bins(int b, const RegionSetup &rs) {
+  Region *r = regions_[b];
+  r->args.target_density = rs.target_density;
+  size_t nb = rs.scaled.size();
+  check(cudaMemcpyAsync(r->scaled, rs.scaled.data(), nb * sizeof(float), cudaMemcpyHostToDevice, stream_), "update bins");
+  check(cudaMemcpyAsync(r->np, rs.non_place.data(), nb * sizeof(int64_t), cudaMemcpyHostToDevice, stream_), "update bins");
+  check(cudaMemcpyAsync(r->npu, rs.non_place_u.data(), nb * sizeof(int64_t), cudaMemcpyHostToDevice, stream_), "update bins");
+}
+
+void Engine::rewrite_cells(const EngineSetup &s) {
+  // sizes and density sizes of every cell (routability's inflation and filler changes keep
+  // the cell count of a region's block only when no filler moved; the caller re-uploads then)
+  size_t n = s.hx.size();
+  if ((int64_t)n != n_cells_) {
+    check(cudaErrorInvalidValue, "rewrite_cells: cell count changed");
+    return;
+  }
+  check(cudaMemcpyAsync(hx_, s.hx.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, stream_), "rewrite cells");
+  check(cudaMemcpyAsync(hy_, s.hy.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice, stream_), "rewrite cells");
+  check(cudaMemcpyAsync(dscale_, s.dscale.data(), n * sizeof(float), cudaMemcpyHostToDevice, stream_), "rewrite cells");
+  check(cudaMemcpyAsync(area_, s.area.data(), n * sizeof(float), cudaMemcpyHostToDevice, stream_), "rewrite cells");
+}
+
+static CellArgs cell_args(const int64_t off, int32_t *dcx, int32_t *dcy, int32_t *hx, int32_t *hy, float *dscale, uint8_t *kind, uint8_t *locked, float *area, int64_t *ps, int32_t *pins, float2 *const *slot) {
+  CellArgs c{};
+  c.dcx = dcx + off;
+  c.dcy = dcy + off;
+  c.hx = hx + off;
+  c.hy = hy + off;
+  c.dscale = dscale + off;
+  c.kind = kind + off;
+  c.locked = locked ? locked + off : nullptr;
+  c.area = area + off;
+  c.pin_start = ps + off;
+  c.pins = pins;
+  c.cur_slp = slot[S_CUR_SLP];
+  c.cur_slp_sum = slot[S_CUR_SLP_SUM];
+  c.next_slp = slot[S_NEXT_SLP];
+  c.next_slp_sum = slot[S_NEXT_SLP_SUM];
+  c.prev_slp = slot[S_PREV_SLP];
+  c.prev_slp_sum = slot[S_PREV_SLP_SUM];
+  c.cur = slot[S_CUR];
+  c.next = slot[S_NEXT];
+  return c;
+}
+
+#define CELLS(r) cell_args((r)->cell_off, dcx_, dcy_, hx_, hy_, dscale_, kind_, locked_, area_, cell_pin_start_, cell_pins_, (r)->slot)
+
+void Engine::set_coords(int b, SlotId slot, const std::vector<float> &xy) {
+  Region *r = regions_[b];
+  if (r->n_cells) check(cudaMemcpyAsync(r->slot[slot], xy.data(), r->n_cells * sizeof(float2), cudaMemcpyHostToDevice, stream_), "set_coords");
+}
+
+std::vector<float> Engine::get_coords(int b, SlotId slot) {
+  Region *r = regions_[b];
+  std::vector<float> xy(2 * r->n_cells);
+  if (r->n_cells) check(cudaMemcpyAsync(xy.data(), r->slot[slot], r->n_cells * sizeof(float2), cudaMemcpyDeviceToHost, stream_), "get_coords");
+  check(cudaStreamSynchronize(stream_), "get_coords sync");
+  return xy;
+}
+
+void Engine::place_at(int b, SlotId slot) {
+  if (failed()) return;
+  Region *r = regions_[b];
+  CellArgs c = CELLS(r);
+  if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, c, PLACE_AT, 0.0f, 0.0f, r->slot[slot]);
+  k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld);
+  k_reduce_partials<<<1, kThreadsPerBlock, 0, stream_>>>(r->part, r->nb_bins, 2, &dev_scal_[b].overflow);
+  check(cudaGetLastError(), "place_at");
+}
+
+void Engine::nesterov_step(int b, float step, float coeff) {
+  if (failed()) return;
+  Region *r = regions_[b];
+  CellArgs c = CELLS(r);
+  if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, c, PLACE_NESTEROV, step, coeff, nullptr);
+  k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld);
+  k_reduce_partials<<<1, kThreadsPerBlock, 0, stream_>>>(r->part, r->nb_bins, 2, &dev_scal_[b].overflow);
+  check(cudaGetLastError(), "nesterov_step");
+}
+
+void Engine::field(int b) {
+  if (failed()) return;
+  Region *r = regions_[b];
+  check(poisson_solve(r->plan, r->density, r->fx, r->fy, stream_), "poisson");
+}
+
+void Engine::wa(float cx, float cy) {
+  if (failed() || n_nets_ == 0) return;
+  WaArgs w{};
+  w.n_nets = n_nets_;
+  w.net_start = net_start_;
+  w.net_order = net_order_;
+  w.net_weight = net_weight_;
+  w.pin_cell = pin_cell_;
+  w.pin_base = pin_base_;
+  w.dcx = dcx_;
+  w.dcy = dcy_;
+  w.pin_grad = pin_grad_;
+  k_wa<<<blocks_for(n_nets_), kThreadsPerBlock, 0, stream_>>>(w, cx, cy);
+  check(cudaGetLastError(), "wa");
+}
+
+void Engine::gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, SlotId b2) {
+  if (failed()) return;
+  Region *r = regions_[b];
+  CellArgs c = CELLS(r);
+  const float2 *pa1 = a1 == S_NUM ? nullptr : r->slot[a1];
+  const float2 *pb1 = b1 == S_NUM ? nullptr : r->slot[b1];
+  const float2 *pb2 = b2 == S_NUM ? nullptr : r->slot[b2];
+  if (r->n_cells) {
+    k_gradients<<<r->nb_cells, kThreadsPerBlock, 0, stream_>>>(r->args, c, pin_grad_, penalty, r->slot[out], pa1, pb1, pb2, r->part);
+    k_reduce_partials<<<1, kThreadsPerBlock, 0, stream_>>>(r->part, r->nb_cells, 4, &dev_scal_[b].wl_sum);
+  } else {
+    check(cudaMemsetAsync(&dev_scal_[b].wl_sum, 0, 4 * sizeof(double), stream_), "gradients");
+  }
+  check(cudaGetLastError(), "gradients");
+}
+
+void Engine::prev_slp(int b, float coef) {
+  if (failed()) return;
+  Region *r = regions_[b];
+  if (!r->n_cells) return;
+  k_prev_slp<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, CELLS(r), coef);
+  check(cudaGetLastError(), "prev_slp");
+}
+
+void Engine::hold_locked(int b) {
+  if (failed() || !any_locked_) return;
+  Region *r = regions_[b];
+  if (!r->n_cells) return;
+  k_hold_locked<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, CELLS(r));
+  check(cudaGetLastError(), "hold_locked");
+}
+
+void Engine::swap_slots(int b, SlotId a, SlotId c) { std::swap(regions_[b]->slot[a], regions_[b]->slot[c]); }
+
+void Engine::copy_slot(int b, SlotId dst, SlotId src) {
+  Region *r = regions_[b];
+  if (r->n_cells) check(cudaMemcpyAsync(r->slot[dst], r->slot[src], r->n_cells * sizeof(float2), cudaMemcpyDeviceToDevice, stream_), "copy_slot");
+}
+
+void Engine::fetch() {
+  if (failed() || host_scal_.empty()) return;
+  check(cudaMemcpyAsync(host_scal_.data(), dev_scal_, host_scal_.size() * sizeof(RegionScalars), cudaMemcpyDeviceToHost, stream_), "fetch");
+  check(cudaStreamSynchronize(stream_), "fetch sync");
+}
+
+int64_t Engine::hpwl() {
+  if (failed()) return 0;
+  WaArgs w{};
+  w.n_nets = n_nets_;
+  w.net_start = net_start_;
+  w.pin_cell = pin_cell_;
+  w.pin_base = pin_base_;
+  w.dcx = dcx_;
+  w.dcy = dcy_;
+  check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), stream_), "hpwl");
+  if (n_nets_) k_hpwl<<<blocks_for(n_nets_), kThreadsPerBlock, 0, stream_>>>(w, hpwl_acc_);
+  unsigned long long h = 0;
+  check(cudaMemcpyAsync(&h, hpwl_acc_, sizeof h, cudaMemcpyDeviceToHost, stream_), "hpwl");
+  check(cudaStreamSynchronize(stream_), "hpwl sync");
+  return (int64_t)h;
+}
+
+void Engine::centres(std::vector<int32_t> &dcx, std::vector<int32_t> &dcy) {
+  dcx.resize(n_cells_);
+  dcy.resize(n_cells_);
+  if (n_cells_) {
+    check(cudaMemcpyAsync(dcx.data(), dcx_, n_cells_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "centres");
+    check(cudaMemcpyAsync(dcy.data(), dcy_, n_cells_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "centres");
+  }
+  check(cudaStreamSynchronize(stream_), "centres sync");
+}
+
+void Engine::set_net_weights(const std::vector<float> &w) {
+  if (!w.empty()) check(cudaMemcpyAsync(net_weight_, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, stream_), "net weights");
+}
+
+}  // namespace gpl

@@ -1,0 +1,142 @@
+// The device half of the engine: the Nesterov state resident in HBM and the trial's kernels,
+// and the initial placement's solve. The host control (nesterov.cpp) only sees scalars: the
+// overflow and gradient sums, the step-length distances and the HPWL, read once per trial.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "host.h"
+
+namespace gpl {
+
+struct PoissonPlan;
+
+// What the device needs of one region (a `NesterovBase`'s bin grid).
+struct RegionSetup {
+  int32_t lx = 0, ly = 0, ux = 0, uy = 0, nx = 0, ny = 0;
+  double size_x = 0, size_y = 0;
+  float target_density = 0;
+  std::vector<int32_t> bx, by;                 // bin edges
+  std::vector<float> scaled;                   // x-major: (float)area * target density
+  std::vector<int64_t> non_place, non_place_u; // x-major
+  std::vector<float> wx, wy;                   // wavenumbers
+  int64_t cell_off = 0, n_cells = 0;           // the region's cells in the device order
+};
+
+// Every device cell (regions contiguous, in each region's cell order) and every pin.
+struct EngineSetup {
+  std::vector<int32_t> hx, hy;     // half density size
+  std::vector<float> dscale, area; // density scale; (float)dx * (float)dy of the cell box
+  std::vector<uint8_t> kind;       // CELL_STD / CELL_MACRO / CELL_FILLER
+  std::vector<uint8_t> locked;
+  std::vector<int64_t> cell_pin_start;
+  std::vector<int32_t> cell_pins;
+  std::vector<int32_t> dcx, dcy;   // the density centres as set up
+  std::vector<int64_t> net_start;  // pins net-major
+  std::vector<int32_t> pin_cell;   // device cell, -1 for a pin with no moving cell
+  std::vector<int32_t> pin_base;   // 2 per pin: offset, or the fixed position
+  std::vector<float> net_weight;
+  std::vector<RegionSetup> regions;
+};
+
+enum SlotId { S_CUR_SLP = 0, S_CUR_SLP_SUM, S_NEXT_SLP, S_NEXT_SLP_SUM, S_PREV_SLP, S_PREV_SLP_SUM, S_CUR, S_NEXT, S_SNAP_CUR, S_SNAP_SLP, S_SNAP_SLP_SUM, S_SNAP_PREV_SLP_SUM, S_NUM };
+
+// Per-region scalars the trial reads back (doubles): the overflow sums of the last scatter,
+// the two |gradient| sums and the two step-length distances of the last gradient update.
+struct RegionScalars {
+  double overflow, overflow_u, wl_sum, den_sum, dist1, dist2, pad0, pad1;
+};
+
+struct DeviceError {
+  cudaError_t code;
+  std::string where;
+};
+
+class Engine {
+ public:
+  explicit Engine(int device);
+  ~Engine();
+  int device() const { return device_; }
+  cudaStream_t stream() const { return stream_; }
+  void set_poisson_mode(int m) { poisson_mode_ = m; }
+  int poisson_mode() const { return poisson_mode_; }
+
+  // ---- initial placement: one axis's solve (src/bicgstab.rs:615-669)
+  Solve solve(const Csr &m, const std::vector<float> &rhs, std::vector<float> &x, int max_iters);
+
+  // ---- Nesterov state
+  void upload(const EngineSetup &s);
+  void release();
+  int regions() const { return (int)regions_.size(); }
+  void set_coords(int b, SlotId slot, const std::vector<float> &xy);  // 2 floats per cell
+  std::vector<float> get_coords(int b, SlotId slot);
+  // The density centres at `slot` (PLACE_AT) and the bins; the overflow sums.
+  void place_at(int b, SlotId slot);
+  // nesterovUpdateCoordinates: next, next_slp from cur_slp, cur_slp_sum, cur; then the bins.
+  void nesterov_step(int b, float step, float coeff);
+  void field(int b);
+  void wa(float coef_x, float coef_y);
+  // updateGradients into `out` with the penalty; distances |a1 - b1| and |out - b2| (pass
+  // S_NUM to skip one).
+  void gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, SlotId b2);
+  void prev_slp(int b, float coef);
+  void hold_locked(int b);
+  void swap_slots(int b, SlotId a, SlotId c);
+  void copy_slot(int b, SlotId dst, SlotId src);
+  // Every region's scalars (one synchronisation).
+  void fetch();
+  const RegionScalars &scalars(int b) const { return host_scal_[b]; }
+  int64_t hpwl();  // synchronises
+  void centres(std::vector<int32_t> &dcx, std::vector<int32_t> &dcy);
+  void set_net_weights(const std::vector<float> &w);
+  // New bin targets and fixed areas (a target-density change), same grid.
+  void update_bins(int b, const RegionSetup &r);
+  // Cell data after a routability change: sizes, density sizes, scales, order (a region's
+  // whole cell block is rewritten).
+  void rewrite_cells(const EngineSetup &s);
+  int64_t trials = 0;
+  bool failed() const { return err_.code != cudaSuccess; }
+  const DeviceError &error() const { return err_; }
+  void check(cudaError_t e, const char *where);
+
+  // timing of the device phases (CUDA events on the engine's stream)
+  float ms_poisson = 0;
+
+ private:
+  struct Region;
+  int device_ = 0;
+  int poisson_mode_ = 1;
+  cudaStream_t stream_ = nullptr;
+  DeviceError err_{cudaSuccess, ""};
+  std::vector<Region *> regions_;
+  std::vector<RegionScalars> host_scal_;
+  RegionScalars *dev_scal_ = nullptr;
+  // globals
+  int64_t n_cells_ = 0, n_pins_ = 0;
+  int32_t n_nets_ = 0;
+  int32_t *dcx_ = nullptr, *dcy_ = nullptr, *hx_ = nullptr, *hy_ = nullptr;
+  float *dscale_ = nullptr, *area_ = nullptr;
+  uint8_t *kind_ = nullptr, *locked_ = nullptr;
+  bool any_locked_ = false;
+  int64_t *cell_pin_start_ = nullptr;
+  int32_t *cell_pins_ = nullptr;
+  int64_t *net_start_ = nullptr;
+  int32_t *net_order_ = nullptr, *pin_cell_ = nullptr;
+  int2 *pin_base_ = nullptr;
+  float *net_weight_ = nullptr;
+  float2 *pin_grad_ = nullptr;
+  unsigned long long *hpwl_acc_ = nullptr;
+  // initial placement scratch
+  void *ip_scratch_ = nullptr;
+  size_t ip_scratch_bytes_ = 0;
+  int64_t *ip_rs_ = nullptr;
+  int32_t *ip_cols_ = nullptr;
+  float *ip_vals_ = nullptr, *ip_b_ = nullptr, *ip_x_ = nullptr;
+  size_t ip_nnz_cap_ = 0, ip_n_cap_ = 0;
+  void free_globals();
+};
+
+}  // namespace gpl

@@ -1,0 +1,54 @@
+// Shared device helpers for the placement kernels.
+//
+// Every kernel file that restates the placer's float arithmetic is compiled with
+// --fmad=false, so a*b+c is two rounded operations exactly as the reference evaluates it
+// (no fused multiply-add anywhere on the reference-ordered paths).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gpl {
+
+constexpr int kThreads = 256;
+
+// Rust `as i32` from f32/f64: round toward zero, saturating, NaN to 0 (PTX cvt.rzi clamps).
+__device__ __forceinline__ int32_t f2i_rz(float v) { return __float2int_rz(v); }
+__device__ __forceinline__ int64_t f2l_rz(float v) { return __float2ll_rz(v); }
+__device__ __forceinline__ int32_t d2i_rz(double v) { return __double2int_rz(v); }
+
+// `fastExp` (src/nesterov.rs:308-314): (1 + x/1024)^1024 by ten squarings, in float.
+__device__ __forceinline__ float fast_exp(float x) {
+  float e = __fadd_rn(1.0f, __fdiv_rn(x, 1024.0f));
+#pragma unroll
+  for (int i = 0; i < 10; i++) e = __fmul_rn(e, e);
+  return e;
+}
+
+// Bin span of [lo, hi) on an axis whose bins start at g0 and are `size` wide, clamped to
+// [0, cnt] (`BinGrid::density_idx_x`, src/nesterov.rs:275-284): the quotient in double.
+__device__ __forceinline__ void bin_span(int32_t lo, int32_t hi, int32_t g0, double size, int32_t cnt, int32_t &a, int32_t &b) {
+  a = d2i_rz(__ddiv_rn((double)(lo - g0), size));
+  b = d2i_rz(ceil(__ddiv_rn((double)(hi - g0), size)));
+  a = a < 0 ? 0 : a;
+  b = b > cnt ? cnt : b;
+}
+
+// A block's sum of `v` (double), valid in thread 0. Fixed order for a fixed launch shape.
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double s = 0;
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < NT / 32 ? sh[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  }
+  __syncthreads();
+  return s;
+}
+
+}  // namespace gpl

@@ -1,0 +1,76 @@
+// Kernel argument blocks and launchers shared by the engine's host code and its kernels.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace gpl {
+
+constexpr int kThreadsPerBlock = 256;  // the block size every launch uses
+
+enum CellKind : uint8_t { CELL_STD = 0, CELL_MACRO = 1, CELL_FILLER = 2 };
+enum PlaceMode { PLACE_AT = 0, PLACE_NESTEROV = 1, PLACE_GIVEN = 2 };  // GIVEN: the centres in dcx/dcy
+
+// One region's bin grid (`BinGrid`, src/nesterov.rs:260-295) and its cell count.
+struct RegionArgs {
+  int32_t n_cells;
+  int32_t nx, ny;
+  int32_t lx, ly, ux, uy;        // the grid's box
+  double size_x, size_y;
+  float target_density;
+  const int32_t *bx, *by;        // bin edges, nx+1 and ny+1
+  const float *scaled;           // bin area * target density (float)
+  const int64_t *non_place, *non_place_u;
+  int64_t *acc_inst, *acc_fill;  // scatter accumulators (cleared by the finalize)
+  float *density, *field_x, *field_y;
+};
+
+// One region's cells, SoA, region-local index.
+struct CellArgs {
+  int32_t *dcx, *dcy;            // density centre (the integer box centre)
+  const int32_t *hx, *hy;        // half density size
+  const float *dscale;           // density scale
+  const uint8_t *kind;           // CellKind
+  const uint8_t *locked;         // may be NULL
+  const float *area;             // (float)dx * (float)dy of the cell box, for the preconditioner
+  const int64_t *pin_start;      // the cell's pins (CSR, the cell's own order)
+  const int32_t *pins;
+  float2 *cur_slp, *cur_slp_sum, *next_slp, *next_slp_sum, *prev_slp, *prev_slp_sum, *cur, *next;
+};
+
+// The nets and pins (all regions): pins net-major.
+struct WaArgs {
+  int32_t n_nets;
+  const int64_t *net_start;
+  const int32_t *net_order;      // nets by degree (NULL: natural order)
+  const float *net_weight;       // NULL: 1
+  const int32_t *pin_cell;       // global device cell index, -1 for a pin with no cell
+  const int2 *pin_base;          // offset from the cell's centre, or the fixed position
+  const int32_t *dcx, *dcy;      // global device cell centres
+  float2 *pin_grad;
+};
+
+__global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *coords);
+__global__ void k_bins_finalize(RegionArgs r, double *partials, __nv_bfloat16 *dens_split, int split_ld);
+__global__ void k_wa(WaArgs w, float cx, float cy);
+__global__ void k_gradients(RegionArgs r, CellArgs c, const float2 *pin_grad, float penalty, float2 *out_sum,
+                            const float2 *a1, const float2 *b1, const float2 *b2, double *partials);
+__global__ void k_prev_slp(RegionArgs r, CellArgs c, float coef);
+__global__ void k_hpwl(WaArgs w, unsigned long long *out);
+__global__ void k_hold_locked(RegionArgs r, CellArgs c);
+__global__ void k_reduce_partials(const double *partials, int nblk, int width, double *out);
+
+// The density solver (Fft::solve without the potential): FP32 SIMT GEMMs or split-BF16
+// tcgen05 GEMMs. Workspace layout and basis matrices are the solver's own.
+struct PoissonPlan;
+PoissonPlan *poisson_plan_create(int nx, int ny, const float *wx_host, const float *wy_host, int mode, cudaError_t *err);
+void poisson_plan_destroy(PoissonPlan *p);
+cudaError_t poisson_solve(PoissonPlan *p, const float *density, float *field_x, float *field_y, cudaStream_t s);
+// The split-BF16 density operand the bin finalize can write directly (NULL in FP32 mode).
+__nv_bfloat16 *poisson_split_input(PoissonPlan *p, int *ld);
+// Fill the split-BF16 operand from a float density (when no bin finalize wrote it).
+cudaError_t poisson_split_density(PoissonPlan *p, const float *density, cudaStream_t s);
+size_t poisson_workspace_bytes(int nx, int ny);
+
+}  // namespace gpl

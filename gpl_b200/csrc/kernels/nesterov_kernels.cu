@@ -1,0 +1,331 @@
+// The Nesterov trial's data-parallel stages (src/nesterov.rs:2139-2507, 2718-2772), one
+// region's cells per launch. Cells are SoA in region-contiguous order; bins are x-major
+// (index x*ny + y, the solver's layout, src/nesterov.rs:2283-2293).
+//
+// Compiled with --fmad=false: every float expression below is the reference's, in its order,
+// and the per-cell results (coordinates, density boxes, the int64 bin addends, the density
+// and WA gradients) are bit-identical to the reference's for identical inputs. Only the
+// cross-cell sums (overflow, |gradient| sums, step-length distances) are taken in double and
+// in a different order.
+#include "common.cuh"
+#include "engine_kernels.h"
+
+namespace gpl {
+
+// ---- cells: Nesterov step (nesterovUpdateCoordinates, :2718-2746) or a given point, then the
+// density centre (setDensityCenterLocation, :2139-2153, truncated) and the bin scatter
+// (updateBinsGCellDensityArea, :2218-2250): each (cell, bin) overlap times the density scale
+// (times the bin's target density for a macro), truncated to int64 and added atomically —
+// integer adds, so the accumulators equal the reference's in any order.
+__device__ __forceinline__ float inside_axis(float c, float half, float lo, float hi) {
+  float adj = c;
+  if (__fsub_rn(c, half) < lo) adj = __fadd_rn(lo, half);
+  if (__fadd_rn(c, half) > hi) adj = __fsub_rn(hi, half);
+  return adj;
+}
+
+__global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.n_cells) return;
+  float2 p = make_float2(0.0f, 0.0f);
+  if (mode == PLACE_AT) {
+    p = coords[i];
+  } else if (mode == PLACE_GIVEN) {
+  } else {
+    float2 cs = c.cur_slp[i];
+    if (c.locked && c.locked[i]) {
+      c.next[i] = c.cur[i];
+      c.next_slp[i] = cs;
+      p = cs;
+    } else {
+      float2 g = c.cur_slp_sum[i], cu = c.cur[i];
+      float nx = __fadd_rn(cs.x, __fmul_rn(step, g.x));
+      float ny = __fadd_rn(cs.y, __fmul_rn(step, g.y));
+      float sx = __fadd_rn(nx, __fmul_rn(coeff, __fsub_rn(nx, cu.x)));
+      float sy = __fadd_rn(ny, __fmul_rn(coeff, __fsub_rn(ny, cu.y)));
+      float hx = (float)c.hx[i], hy = (float)c.hy[i];
+      float glx = (float)r.lx, gly = (float)r.ly, gux = (float)r.ux, guy = (float)r.uy;
+      c.next[i] = make_float2(inside_axis(nx, hx, glx, gux), inside_axis(ny, hy, gly, guy));
+      p = make_float2(inside_axis(sx, hx, glx, gux), inside_axis(sy, hy, gly, guy));
+      c.next_slp[i] = p;
+    }
+  }
+  int32_t cx, cy;
+  if (mode == PLACE_GIVEN) {
+    cx = c.dcx[i];
+    cy = c.dcy[i];
+  } else {
+    cx = f2i_rz(p.x);
+    cy = f2i_rz(p.y);
+    c.dcx[i] = cx;
+    c.dcy[i] = cy;
+  }
+  int32_t hx = c.hx[i], hy = c.hy[i];
+  int32_t dlx = cx - hx, dux = cx + hx, dly = cy - hy, duy = cy + hy;
+  int32_t x0, x1, y0, y1;
+  bin_span(dlx, dux, r.lx, r.size_x, r.nx, x0, x1);
+  bin_span(dly, duy, r.ly, r.size_y, r.ny, y0, y1);
+  float scale = c.dscale[i];
+  uint8_t kind = c.kind[i];
+  unsigned long long *acc = (unsigned long long *)(kind == CELL_FILLER ? r.acc_fill : r.acc_inst);
+  for (int32_t y = y0; y < y1; y++) {
+    int32_t bly = r.by[y], buy = r.by[y + 1];
+    int32_t oly = dly > bly ? dly : bly, ouy = duy < buy ? duy : buy;
+    for (int32_t x = x0; x < x1; x++) {
+      int32_t blx = r.bx[x], bux = r.bx[x + 1];
+      int32_t olx = dlx > blx ? dlx : blx, oux = dux < bux ? dux : bux;
+      float a = 0.0f;
+      if (olx < oux && oly < ouy) a = __fmul_rn((float)(oux - olx), (float)(ouy - oly));
+      a = __fmul_rn(a, scale);
+      if (kind == CELL_MACRO) a = __fmul_rn(a, r.target_density);
+      int64_t v = f2l_rz(a);
+      if (v) atomicAdd(&acc[(size_t)x * r.ny + y], (unsigned long long)v);
+    }
+  }
+}
+
+// ---- bins: density and overflow (:2252-2262), accumulators cleared for the next scatter.
+// Optionally the density split into bf16 hi/lo for the tensor-core solver.
+__global__ void k_bins_finalize(RegionArgs r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld) {
+  __shared__ double sh[kThreads / 32];
+  int64_t n = (int64_t)r.nx * r.ny;
+  double o_sum = 0.0, ou_sum = 0.0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    int64_t inst = r.acc_inst[k], fill = r.acc_fill[k];
+    r.acc_inst[k] = 0;
+    r.acc_fill[k] = 0;
+    float fi = __ll2float_rn(inst), fn = __ll2float_rn(r.non_place[k]), fnu = __ll2float_rn(r.non_place_u[k]);
+    float sc = r.scaled[k];
+    float d = __fdiv_rn(__fadd_rn(__fadd_rn(fi, __ll2float_rn(fill)), fn), sc);
+    r.density[k] = d;
+    if (dens_split) {
+      int64_t x = k / r.ny, y = k % r.ny;
+      __nv_bfloat16 hi = __float2bfloat16_rn(d);
+      __nv_bfloat16 lo = __float2bfloat16_rn(d - __bfloat162float(hi));
+      dens_split[x * split_ld + y] = hi;
+      dens_split[x * split_ld + r.ny + y] = lo;
+    }
+    float o = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fn), sc));
+    float ou = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fnu), sc));
+    o_sum += (double)o;
+    ou_sum += (double)ou;
+  }
+  double a = block_sum<kThreads>(o_sum, sh);
+  double b = block_sum<kThreads>(ou_sum, sh);
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = a;
+    partials[2 * blockIdx.x + 1] = b;
+  }
+}
+
+// ---- WA wirelength (updateWireLengthForceWA :2325-2388 + getWireLengthGradientPinWA
+// :2392-2414): one thread per net, nets in degree order so a warp's nets are alike; each
+// net's sums over its pins in the net's order (the reference's float order), then each pin's
+// force in double, times the net's weight. Pin position: its cell's density centre plus the
+// pin's offset, or a fixed point for a pin with no cell.
+__device__ __forceinline__ int2 pin_pos(const WaArgs &w, int64_t p) {
+  int32_t cell = w.pin_cell ? w.pin_cell[p] : -1;
+  int2 b = w.pin_base[p];
+  if (cell >= 0) {
+    b.x += w.dcx[cell];
+    b.y += w.dcy[cell];
+  }
+  return b;
+}
+
+__global__ void k_wa(WaArgs w, float cx, float cy) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= w.n_nets) return;
+  int32_t n = w.net_order ? w.net_order[t] : t;
+  int64_t b = w.net_start[n], e = w.net_start[n + 1];
+  int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+  for (int64_t p = b; p < e; p++) {
+    int2 q = pin_pos(w, p);
+    lx = min(lx, q.x);
+    ly = min(ly, q.y);
+    ux = max(ux, q.x);
+    uy = max(uy, q.y);
+  }
+  const float BAR = -300.0f;
+  float s_minx = 0, s_xminx = 0, s_maxx = 0, s_xmaxx = 0, s_miny = 0, s_yminy = 0, s_maxy = 0, s_ymaxy = 0;
+  for (int64_t p = b; p < e; p++) {
+    int2 q = pin_pos(w, p);
+    float emin_x = __fmul_rn((float)(lx - q.x), cx), emax_x = __fmul_rn((float)(q.x - ux), cx);
+    float emin_y = __fmul_rn((float)(ly - q.y), cy), emax_y = __fmul_rn((float)(q.y - uy), cy);
+    if (emin_x > BAR) {
+      float v = fast_exp(emin_x);
+      s_minx = __fadd_rn(s_minx, v);
+      s_xminx = __fadd_rn(s_xminx, __fmul_rn((float)q.x, v));
+    }
+    if (emax_x > BAR) {
+      float v = fast_exp(emax_x);
+      s_maxx = __fadd_rn(s_maxx, v);
+      s_xmaxx = __fadd_rn(s_xmaxx, __fmul_rn((float)q.x, v));
+    }
+    if (emin_y > BAR) {
+      float v = fast_exp(emin_y);
+      s_miny = __fadd_rn(s_miny, v);
+      s_yminy = __fadd_rn(s_yminy, __fmul_rn((float)q.y, v));
+    }
+    if (emax_y > BAR) {
+      float v = fast_exp(emax_y);
+      s_maxy = __fadd_rn(s_maxy, v);
+      s_ymaxy = __fadd_rn(s_ymaxy, __fmul_rn((float)q.y, v));
+    }
+  }
+  float wt = w.net_weight ? w.net_weight[n] : 1.0f;
+  for (int64_t p = b; p < e; p++) {
+    int2 q = pin_pos(w, p);
+    float qx = (float)q.x, qy = (float)q.y;
+    float emin_x = __fmul_rn((float)(lx - q.x), cx), emax_x = __fmul_rn((float)(q.x - ux), cx);
+    float emin_y = __fmul_rn((float)(ly - q.y), cy), emax_y = __fmul_rn((float)(q.y - uy), cy);
+    float gmin_x = 0, gmax_x = 0, gmin_y = 0, gmax_y = 0;
+    if (emin_x > BAR) {
+      float v = fast_exp(emin_x);
+      double num = __dadd_rn(__dmul_rn((double)s_minx, __dmul_rn((double)v, __dsub_rn(1.0, (double)__fmul_rn(cx, qx)))), (double)__fmul_rn(__fmul_rn(cx, v), s_xminx));
+      gmin_x = __double2float_rn(__ddiv_rn(num, (double)__fmul_rn(s_minx, s_minx)));
+    }
+    if (emax_x > BAR) {
+      float v = fast_exp(emax_x);
+      double num = __dsub_rn(__dmul_rn((double)s_maxx, __dmul_rn((double)v, __dadd_rn(1.0, (double)__fmul_rn(cx, qx)))), (double)__fmul_rn(__fmul_rn(cx, v), s_xmaxx));
+      gmax_x = __double2float_rn(__ddiv_rn(num, (double)__fmul_rn(s_maxx, s_maxx)));
+    }
+    if (emin_y > BAR) {
+      float v = fast_exp(emin_y);
+      double num = __dadd_rn(__dmul_rn((double)s_miny, __dmul_rn((double)v, __dsub_rn(1.0, (double)__fmul_rn(cy, qy)))), (double)__fmul_rn(__fmul_rn(cy, v), s_yminy));
+      gmin_y = __double2float_rn(__ddiv_rn(num, (double)__fmul_rn(s_miny, s_miny)));
+    }
+    if (emax_y > BAR) {
+      float v = fast_exp(emax_y);
+      double num = __dsub_rn(__dmul_rn((double)s_maxy, __dmul_rn((double)v, __dadd_rn(1.0, (double)__fmul_rn(cy, qy)))), (double)__fmul_rn(__fmul_rn(cy, v), s_ymaxy));
+      gmax_y = __double2float_rn(__ddiv_rn(num, (double)__fmul_rn(s_maxy, s_maxy)));
+    }
+    w.pin_grad[p] = make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt));
+  }
+}
+
+// ---- cells: updateGradients (:2455-2507): the WA force over the cell's pins in its order,
+// the density force over its bins (x outer, y inner), the preconditioned sum; block partials
+// of |wl|, |density| and the two step-length distances (getDistance :319-330):
+// |a1 - b1|^2 and |out - b2|^2.
+__global__ void k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials) {
+  __shared__ double sh[kThreads / 32];
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double s_wl = 0, s_den = 0, s_d1 = 0, s_d2 = 0;
+  if (i < r.n_cells) {
+    float wlx = 0.0f, wly = 0.0f;
+    for (int64_t k = c.pin_start[i]; k < c.pin_start[i + 1]; k++) {
+      float2 t = pin_grad[c.pins[k]];
+      wlx = __fadd_rn(wlx, t.x);
+      wly = __fadd_rn(wly, t.y);
+    }
+    int32_t cx = c.dcx[i], cy = c.dcy[i], hx = c.hx[i], hy = c.hy[i];
+    int32_t dlx = cx - hx, dux = cx + hx, dly = cy - hy, duy = cy + hy;
+    int32_t x0, x1, y0, y1;
+    bin_span(dlx, dux, r.lx, r.size_x, r.nx, x0, x1);
+    bin_span(dly, duy, r.ly, r.size_y, r.ny, y0, y1);
+    float scale = c.dscale[i];
+    float fx = 0.0f, fy = 0.0f;
+    for (int32_t x = x0; x < x1; x++) {
+      int32_t blx = r.bx[x], bux = r.bx[x + 1];
+      int32_t olx = dlx > blx ? dlx : blx, oux = dux < bux ? dux : bux;
+      for (int32_t y = y0; y < y1; y++) {
+        int32_t bly = r.by[y], buy = r.by[y + 1];
+        int32_t oly = dly > bly ? dly : bly, ouy = duy < buy ? duy : buy;
+        float a = 0.0f;
+        if (olx < oux && oly < ouy) a = __fmul_rn((float)(oux - olx), (float)(ouy - oly));
+        a = __fmul_rn(a, scale);
+        size_t k = (size_t)x * r.ny + y;
+        fx = __fadd_rn(fx, __fmul_rn(a, r.field_x[k]));
+        fy = __fadd_rn(fy, __fmul_rn(a, r.field_y[k]));
+      }
+    }
+    float sx = __fadd_rn(wlx, __fmul_rn(penalty, fx));
+    float sy = __fadd_rn(wly, __fmul_rn(penalty, fy));
+    float wl_pre = (float)(c.pin_start[i + 1] - c.pin_start[i]);
+    float pre = fmaxf(__fadd_rn(wl_pre, __fmul_rn(penalty, c.area[i])), 1.0f);
+    sx = __fdiv_rn(sx, pre);
+    sy = __fdiv_rn(sy, pre);
+    out_sum[i] = make_float2(sx, sy);
+    s_wl = (double)fabsf(wlx) + (double)fabsf(wly);
+    s_den = (double)fabsf(fx) + (double)fabsf(fy);
+    if (a1) {
+      float2 p = a1[i], q = b1[i];
+      float dx = __fsub_rn(p.x, q.x), dy = __fsub_rn(p.y, q.y);
+      s_d1 = (double)__fmul_rn(dx, dx) + (double)__fmul_rn(dy, dy);
+    }
+    if (b2) {
+      float2 q = b2[i];
+      float dx = __fsub_rn(sx, q.x), dy = __fsub_rn(sy, q.y);
+      s_d2 = (double)__fmul_rn(dx, dx) + (double)__fmul_rn(dy, dy);
+    }
+  }
+  double v0 = block_sum<kThreads>(s_wl, sh);
+  double v1 = block_sum<kThreads>(s_den, sh);
+  double v2 = block_sum<kThreads>(s_d1, sh);
+  double v3 = block_sum<kThreads>(s_d2, sh);
+  if (threadIdx.x == 0) {
+    partials[4 * blockIdx.x + 0] = v0;
+    partials[4 * blockIdx.x + 1] = v1;
+    partials[4 * blockIdx.x + 2] = v2;
+    partials[4 * blockIdx.x + 3] = v3;
+  }
+}
+
+// ---- updateInitialPrevSLPCoordi (:2583-2595): a back-step along the current gradient.
+__global__ void k_prev_slp(RegionArgs r, CellArgs c, float coef) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.n_cells) return;
+  float2 cs = c.cur_slp[i];
+  if (c.locked && c.locked[i]) {
+    c.prev_slp[i] = cs;
+    return;
+  }
+  float2 g = c.cur_slp_sum[i];
+  float px = __fsub_rn(cs.x, __fmul_rn(coef, g.x));
+  float py = __fsub_rn(cs.y, __fmul_rn(coef, g.y));
+  c.prev_slp[i] = make_float2(inside_axis(px, (float)c.hx[i], (float)r.lx, (float)r.ux), inside_axis(py, (float)c.hy[i], (float)r.ly, (float)r.uy));
+}
+
+// ---- getHpwl (:2297-2304): every net's pin box, summed (int64, exact).
+__global__ void k_hpwl(WaArgs w, unsigned long long *__restrict__ out) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  long long h = 0;
+  if (t < w.n_nets) {
+    int64_t b = w.net_start[t], e = w.net_start[t + 1];
+    int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+    for (int64_t p = b; p < e; p++) {
+      int2 q = pin_pos(w, p);
+      lx = min(lx, q.x);
+      ly = min(ly, q.y);
+      ux = max(ux, q.x);
+      uy = max(uy, q.y);
+    }
+    if (ux >= lx) h = ((long long)ux - lx) + ((long long)uy - ly);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+  if ((threadIdx.x & 31) == 0 && h) atomicAdd(out, (unsigned long long)h);
+}
+
+// ---- the locked cells' next state (:2848-2859) and a deterministic reduction of partials.
+__global__ void k_hold_locked(RegionArgs r, CellArgs c) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.n_cells || !c.locked || !c.locked[i] || c.kind[i] == CELL_FILLER) return;
+  c.next_slp[i] = c.cur_slp[i];
+  c.next_slp_sum[i] = c.cur_slp_sum[i];
+  c.next[i] = c.cur[i];
+}
+
+// Sums `nblk` rows of `width` partials in a fixed order into out[0..width).
+__global__ void k_reduce_partials(const double *__restrict__ partials, int nblk, int width, double *__restrict__ out) {
+  __shared__ double sh[kThreads / 32];
+  for (int j = 0; j < width; j++) {
+    double s = 0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partials[(size_t)b * width + j];
+    double t = block_sum<kThreads>(s, sh);
+    if (threadIdx.x == 0) out[j] = t;
+  }
+}
+
+}  // namespace gpl

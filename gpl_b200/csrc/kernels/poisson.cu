@@ -1,0 +1,277 @@
+// The density solver (`Fft::solve`, src/nesterov.rs:412-444) as dense transforms: each 2-D
+// cosine/sine transform of Ooura's package (src/ooura.rs:71-98) is a product with basis
+// matrices on both sides, B_x^T * A * B_y, so the solve is six GEMMs and one spectral step:
+//
+//   T1t[v][x] = sum_y CyTs[v][y] rho[x][y]        forward along y (scale and halving folded in)
+//   Ah[u][v]  = sum_x CxTs[u][x] T1t[v][x]        forward along x
+//   Exh = Ah wx/(wx^2+wy^2), Eyh = Ah wy/(wx^2+wy^2), 0 at (0,0)
+//   T2t[y][u] = sum_v Cy[y][v] Exh[u][v]   ;  Ex[x][y] = sum_u Sx[x][u] T2t[y][u]   (ddsct2d)
+//   T3t[y][u] = sum_v Sy[y][v] Eyh[u][v]   ;  Ey[x][y] = sum_u Cx[x][u] T3t[y][u]   (ddcst2d)
+//
+// Every GEMM is D[m][n] = sum_k A[m][k] B[n][k] with both operands K-contiguous. The forward
+// halving of row and column 0 and the 4/(nx*ny) scale are separable (h_u h_v (2/nx)(2/ny);
+// the (0,0) term they disagree on is zeroed by the solve). Ooura's sine inverse keeps A[n] in
+// a[0]; its basis column 0 is therefore (-1)^x. The potential is not computed: nothing but
+// the reference's probes reads it.
+//
+// Mode 0 (this file): FP32 SIMT GEMMs. Mode 1: split-BF16 tcgen05 GEMMs (poisson_tc.cu).
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "engine_kernels.h"
+#include "poisson_internal.h"
+
+namespace gpl {
+
+// ---------------------------------------------------------------- FP32 SIMT GEMM
+// 128 x 64 output tile per block, K-step 8, 256 threads with 8 x 4 outputs each.
+constexpr int SG_BM = 128, SG_BN = 64, SG_BK = 8;
+
+__global__ void __launch_bounds__(256) k_sgemm_tn(GemmBatch gb) {
+  const GemmProblem P = gb.p[blockIdx.z];
+  const int m0 = blockIdx.y * SG_BM, n0 = blockIdx.x * SG_BN;
+  if (m0 >= P.M || n0 >= P.N) return;
+  __shared__ __align__(16) float As[SG_BK][SG_BM + 4];
+  __shared__ __align__(16) float Bs[SG_BK][SG_BN + 4];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int ar = tid >> 1, ak = (tid & 1) * 4;  // A loader: row, first k
+  const int br = tid >> 2, bk = (tid & 3) * 2;  // B loader
+  float acc[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
+  float ra[4], rb[2];
+  auto load = [&](int k0) {
+    int gm = m0 + ar;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      int gk = k0 + ak + q;
+      ra[q] = (gm < P.M && gk < P.K) ? P.A[(size_t)gm * P.lda + gk] : 0.0f;
+    }
+    int gn = n0 + br;
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      int gk = k0 + bk + q;
+      rb[q] = (gn < P.N && gk < P.K) ? P.B[(size_t)gn * P.ldb + gk] : 0.0f;
+    }
+  };
+  load(0);
+  for (int k0 = 0; k0 < P.K; k0 += SG_BK) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) As[ak + q][ar] = ra[q];
+#pragma unroll
+    for (int q = 0; q < 2; q++) Bs[bk + q][br] = rb[q];
+    __syncthreads();
+    if (k0 + SG_BK < P.K) load(k0 + SG_BK);
+#pragma unroll
+    for (int kk = 0; kk < SG_BK; kk++) {
+      float4 a0 = *reinterpret_cast<const float4 *>(&As[kk][ty * 4]);
+      float4 a1 = *reinterpret_cast<const float4 *>(&As[kk][64 + ty * 4]);
+      float4 b0 = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 4]);
+      float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      float b[4] = {b0.x, b0.y, b0.z, b0.w};
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    int gm = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    if (gm >= P.M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      int gn = n0 + tx * 4 + j;
+      if (gn < P.N) P.D[(size_t)gm * P.ldd + gn] = acc[i][j];
+    }
+  }
+}
+
+cudaError_t sgemm_tn(const GemmBatch &gb, int count, cudaStream_t s) {
+  int M = 0, N = 0;
+  for (int i = 0; i < count; i++) {
+    M = M > gb.p[i].M ? M : gb.p[i].M;
+    N = N > gb.p[i].N ? N : gb.p[i].N;
+  }
+  dim3 grid((N + SG_BN - 1) / SG_BN, (M + SG_BM - 1) / SG_BM, count);
+  k_sgemm_tn<<<grid, 256, 0, s>>>(gb);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- the spectral step
+// (src/nesterov.rs:425-440) on the scaled forward transform: phi = Ah / (wx2 + wy2),
+// Ex = phi wx, Ey = phi wy, in float as the reference; all three zero at (0, 0).
+__global__ void k_spectral(int nx, int ny, const float *__restrict__ ah, const float *__restrict__ wx, const float *__restrict__ wx2, const float *__restrict__ wy, const float *__restrict__ wy2, float *__restrict__ exh, float *__restrict__ eyh) {
+  int64_t n = (int64_t)nx * ny;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    int u = (int)(k / ny), v = (int)(k % ny);
+    float ex = 0.0f, ey = 0.0f;
+    if (u != 0 || v != 0) {
+      float p = __fdiv_rn(ah[k], __fadd_rn(wx2[u], wy2[v]));
+      ex = __fmul_rn(p, wx[u]);
+      ey = __fmul_rn(p, wy[v]);
+    }
+    exh[k] = ex;
+    eyh[k] = ey;
+  }
+}
+
+// ---------------------------------------------------------------- basis matrices (host)
+// Built in double from exact arguments, rounded once.
+void build_basis(int nx, int ny, BasisHost &b) {
+  auto cosv = [](int k, int j, int n) { return std::cos(M_PI * (double)k * ((double)j + 0.5) / (double)n); };
+  auto sinv = [](int k, int j, int n) { return k == 0 ? ((j & 1) ? -1.0 : 1.0) : std::sin(M_PI * (double)k * ((double)j + 0.5) / (double)n); };
+  b.CyTs.assign((size_t)ny * ny, 0);
+  b.Cy.assign((size_t)ny * ny, 0);
+  b.Sy.assign((size_t)ny * ny, 0);
+  for (int v = 0; v < ny; v++)
+    for (int y = 0; y < ny; y++) {
+      double h = (v == 0 ? 0.5 : 1.0) * 2.0 / (double)ny;
+      b.CyTs[(size_t)v * ny + y] = h * cosv(v, y, ny);
+      b.Cy[(size_t)y * ny + v] = cosv(v, y, ny);
+      b.Sy[(size_t)y * ny + v] = sinv(v, y, ny);
+    }
+  b.CxTs.assign((size_t)nx * nx, 0);
+  b.Cx.assign((size_t)nx * nx, 0);
+  b.Sx.assign((size_t)nx * nx, 0);
+  for (int u = 0; u < nx; u++)
+    for (int x = 0; x < nx; x++) {
+      double h = (u == 0 ? 0.5 : 1.0) * 2.0 / (double)nx;
+      b.CxTs[(size_t)u * nx + x] = h * cosv(u, x, nx);
+      b.Cx[(size_t)x * nx + u] = cosv(u, x, nx);
+      b.Sx[(size_t)x * nx + u] = sinv(u, x, nx);
+    }
+}
+
+static cudaError_t upload_f32(const std::vector<double> &h, float **d) {
+  std::vector<float> f(h.size());
+  for (size_t i = 0; i < h.size(); i++) f[i] = (float)h[i];
+  cudaError_t e = cudaMalloc(d, f.size() * sizeof(float));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*d, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
+}
+
+size_t poisson_workspace_bytes(int nx, int ny) {
+  size_t n = (size_t)nx * ny;
+  size_t basis = 3 * (size_t)nx * nx + 3 * (size_t)ny * ny;
+  return (basis + 6 * n) * sizeof(float) + 2 * (size_t)(nx + ny) * sizeof(float);
+}
+
+PoissonPlan *poisson_plan_create(int nx, int ny, const float *wx_host, const float *wy_host, int mode, cudaError_t *err) {
+  PoissonPlan *p = new PoissonPlan();
+  p->nx = nx;
+  p->ny = ny;
+  p->mode = mode;
+  *err = cudaSuccess;
+  std::vector<float> w2((size_t)nx + ny);
+  BasisHost b;
+  build_basis(nx, ny, b);
+  size_t n = (size_t)nx * ny;
+#define TRY(x)              \
+  do {                      \
+    cudaError_t e_ = (x);   \
+    if (e_ != cudaSuccess) { \
+      *err = e_;            \
+      poisson_plan_destroy(p); \
+      return nullptr;       \
+    }                       \
+  } while (0)
+  TRY(cudaMalloc(&p->wx, nx * sizeof(float)));
+  TRY(cudaMalloc(&p->wx2, nx * sizeof(float)));
+  TRY(cudaMalloc(&p->wy, ny * sizeof(float)));
+  TRY(cudaMalloc(&p->wy2, ny * sizeof(float)));
+  std::vector<float> sq(std::max(nx, ny));
+  for (int i = 0; i < nx; i++) sq[i] = wx_host[i] * wx_host[i];
+  TRY(cudaMemcpy(p->wx, wx_host, nx * sizeof(float), cudaMemcpyHostToDevice));
+  TRY(cudaMemcpy(p->wx2, sq.data(), nx * sizeof(float), cudaMemcpyHostToDevice));
+  for (int i = 0; i < ny; i++) sq[i] = wy_host[i] * wy_host[i];
+  TRY(cudaMemcpy(p->wy, wy_host, ny * sizeof(float), cudaMemcpyHostToDevice));
+  TRY(cudaMemcpy(p->wy2, sq.data(), ny * sizeof(float), cudaMemcpyHostToDevice));
+  if (mode == 0) {
+    TRY(upload_f32(b.CyTs, &p->CyTs));
+    TRY(upload_f32(b.CxTs, &p->CxTs));
+    TRY(upload_f32(b.Cy, &p->Cy));
+    TRY(upload_f32(b.Sy, &p->Sy));
+    TRY(upload_f32(b.Sx, &p->Sx));
+    TRY(upload_f32(b.Cx, &p->Cx));
+    TRY(cudaMalloc(&p->t1, n * sizeof(float)));
+    TRY(cudaMalloc(&p->ah, n * sizeof(float)));
+    TRY(cudaMalloc(&p->exh, n * sizeof(float)));
+    TRY(cudaMalloc(&p->eyh, n * sizeof(float)));
+    TRY(cudaMalloc(&p->t2, n * sizeof(float)));
+    TRY(cudaMalloc(&p->t3, n * sizeof(float)));
+  } else {
+    cudaError_t e = tc_plan_init(p, b);
+    if (e != cudaSuccess) {
+      *err = e;
+      poisson_plan_destroy(p);
+      return nullptr;
+    }
+  }
+#undef TRY
+  return p;
+}
+
+void poisson_plan_destroy(PoissonPlan *p) {
+  if (!p) return;
+  float *bufs[] = {p->wx, p->wx2, p->wy, p->wy2, p->CyTs, p->CxTs, p->Cy, p->Sy, p->Sx, p->Cx, p->t1, p->ah, p->exh, p->eyh, p->t2, p->t3};
+  for (float *b : bufs)
+    if (b) cudaFree(b);
+  tc_plan_free(p);
+  delete p;
+}
+
+__nv_bfloat16 *poisson_split_input(PoissonPlan *p, int *ld) {
+  if (p->mode == 0) return nullptr;
+  *ld = 2 * p->ny;
+  return p->tc_dens;
+}
+
+__global__ void k_split_density(int nx, int ny, const float *__restrict__ d, __nv_bfloat16 *__restrict__ out, int ld) {
+  int64_t n = (int64_t)nx * ny;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    int64_t x = k / ny, y = k % ny;
+    float v = d[k];
+    __nv_bfloat16 hi = __float2bfloat16_rn(v);
+    out[x * ld + y] = hi;
+    out[x * ld + ny + y] = __float2bfloat16_rn(v - __bfloat162float(hi));
+  }
+}
+
+cudaError_t poisson_split_density(PoissonPlan *p, const float *density, cudaStream_t s) {
+  if (p->mode == 0) return cudaSuccess;
+  int64_t n = (int64_t)p->nx * p->ny;
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+  k_split_density<<<blocks, 256, 0, s>>>(p->nx, p->ny, density, p->tc_dens, 2 * p->ny);
+  return cudaGetLastError();
+}
+
+cudaError_t poisson_solve(PoissonPlan *p, const float *density, float *field_x, float *field_y, cudaStream_t s) {
+  if (p->mode != 0) return tc_solve(p, field_x, field_y, s);
+  int nx = p->nx, ny = p->ny;
+  GemmBatch g{};
+  g.p[0] = GemmProblem{ny, nx, ny, p->CyTs, ny, density, ny, p->t1, nx};
+  cudaError_t e = sgemm_tn(g, 1, s);
+  if (e != cudaSuccess) return e;
+  g.p[0] = GemmProblem{nx, ny, nx, p->CxTs, nx, p->t1, nx, p->ah, ny};
+  if ((e = sgemm_tn(g, 1, s)) != cudaSuccess) return e;
+  int64_t n = (int64_t)nx * ny;
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+  k_spectral<<<blocks, 256, 0, s>>>(nx, ny, p->ah, p->wx, p->wx2, p->wy, p->wy2, p->exh, p->eyh);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  g.p[0] = GemmProblem{ny, nx, ny, p->Cy, ny, p->exh, ny, p->t2, nx};
+  g.p[1] = GemmProblem{ny, nx, ny, p->Sy, ny, p->eyh, ny, p->t3, nx};
+  if ((e = sgemm_tn(g, 2, s)) != cudaSuccess) return e;
+  g.p[0] = GemmProblem{nx, ny, nx, p->Sx, nx, p->t2, nx, field_x, ny};
+  g.p[1] = GemmProblem{nx, ny, nx, p->Cx, nx, p->t3, nx, field_y, ny};
+  return sgemm_tn(g, 2, s);
+}
+
+}  // namespace gpl

@@ -1,0 +1,50 @@
+// The density solver's internals: GEMM problem descriptors, the plan, the basis matrices.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+namespace gpl {
+
+// D[m][n] = sum_k A[m][k] * B[n][k], row-major, leading dimensions in elements.
+struct GemmProblem {
+  int M, N, K;
+  const float *A;
+  int lda;
+  const float *B;
+  int ldb;
+  float *D;
+  int ldd;
+};
+struct GemmBatch {
+  GemmProblem p[2];
+};
+cudaError_t sgemm_tn(const GemmBatch &gb, int count, cudaStream_t s);
+
+// The six basis matrices in double (see poisson.cu): CyTs[v][y], CxTs[u][x] (forward, scaled
+// and halved), Cy[y][v], Sy[y][v], Sx[x][u], Cx[x][u] (inverses).
+struct BasisHost {
+  std::vector<double> CyTs, CxTs, Cy, Sy, Sx, Cx;
+};
+void build_basis(int nx, int ny, BasisHost &b);
+
+struct TcState;  // the split-BF16 tensor-core path's buffers (poisson_tc.cu)
+
+struct PoissonPlan {
+  int nx = 0, ny = 0, mode = 0;
+  float *wx = nullptr, *wx2 = nullptr, *wy = nullptr, *wy2 = nullptr;
+  // FP32 path
+  float *CyTs = nullptr, *CxTs = nullptr, *Cy = nullptr, *Sy = nullptr, *Sx = nullptr, *Cx = nullptr;
+  float *t1 = nullptr, *ah = nullptr, *exh = nullptr, *eyh = nullptr, *t2 = nullptr, *t3 = nullptr;
+  // tensor-core path
+  __nv_bfloat16 *tc_dens = nullptr;  // density as [nx][2*ny] bf16 (hi | lo)
+  TcState *tc = nullptr;
+};
+
+cudaError_t tc_plan_init(PoissonPlan *p, const BasisHost &b);
+void tc_plan_free(PoissonPlan *p);
+cudaError_t tc_solve(PoissonPlan *p, float *field_x, float *field_y, cudaStream_t s);
+
+}  // namespace gpl

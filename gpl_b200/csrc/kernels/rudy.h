@@ -1,0 +1,15 @@
+// RUDY's tile grid and kernels (src/route_base.rs:130-265).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gpl {
+
+struct RudyGrid {
+  int32_t lx, ly, ux, uy;  // the die
+  int32_t cnt_x, cnt_y, tile, wire_width;
+};
+cudaError_t rudy_demand(const RudyGrid &g, int64_t n_nets, const int4 *boxes, float *demand, cudaStream_t s);
+cudaError_t rudy_congestion(const RudyGrid &g, const float *demand, const float *blockage, float *cong, cudaStream_t s);
+
+}  // namespace gpl

@@ -1,0 +1,110 @@
+"""The engine's Python binding: `global_placement` through the C ABI (include/gpl.h).
+
+`global_placement(design, args)` is the reference's `run::global_placement` (src/run.rs:115):
+the command's arguments as the Tcl proc takes them, the report shaped as the CLI's JSON
+(src/main.rs:249-262). It runs on a CUDA device through libgpl_b200.so and fails loudly when
+the library or the device is missing: there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .design import Design, gpl_design_t, gpl_result_t, result_to_dict
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SO = os.path.join(HERE, "libgpl_b200.so")
+_lib = None
+
+
+class EngineUnavailable(RuntimeError):
+    pass
+
+
+def lib():
+    """The engine library (built by gpl_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(SO):
+            raise EngineUnavailable(f"{SO} is missing: build it with `python -m gpl_b200.build`")
+        L = C.CDLL(SO)
+        L.gpl_create.restype = C.c_void_p
+        L.gpl_create.argtypes = [C.c_int]
+        L.gpl_destroy.argtypes = [C.c_void_p]
+        L.gpl_set_option.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
+        L.gpl_global_placement.argtypes = [C.c_void_p, C.POINTER(gpl_design_t), C.c_int, C.POINTER(C.c_char_p), C.c_void_p, C.POINTER(gpl_result_t)]
+        L.gpl_result_free.argtypes = [C.POINTER(gpl_result_t)]
+        L.gpl_synthetic_router_create.restype = C.c_void_p
+        L.gpl_synthetic_router_create.argtypes = [C.POINTER(gpl_design_t), C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.c_uint8]
+        L.gpl_synthetic_router_destroy.argtypes = [C.c_void_p]
+        L.gpl_kernel_density_scatter.argtypes = [C.c_int64] + [C.c_void_p] * 6 + [C.c_int32] * 4 + [C.c_void_p] * 2 + [C.c_double, C.c_double, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.gpl_kernel_poisson.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        L.gpl_kernel_wa.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p]
+        L.gpl_kernel_bicgstab.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.gpl_kernel_rudy.argtypes = [C.c_int64, C.c_void_p] + [C.c_int32] * 8 + [C.c_void_p, C.c_void_p]
+        _lib = L
+    return _lib
+
+
+class Placer:
+    """One engine context on one CUDA device (`gpl_create`)."""
+
+    def __init__(self, device=0, poisson="mixed", trace=False):
+        L = lib()
+        self._ctx = L.gpl_create(device)
+        if not self._ctx:
+            raise EngineUnavailable(f"CUDA device {device} cannot be used")
+        self.set_option("poisson", poisson)
+        self.set_option("trace", "1" if trace else "0")
+
+    def set_option(self, name, value):
+        if lib().gpl_set_option(self._ctx, name.encode(), str(value).encode()) != 0:
+            raise ValueError(f"unknown option {name}={value}")
+
+    def global_placement(self, design: Design, args, router=None) -> dict:
+        L = lib()
+        cd = design.c_struct()
+        argv = (C.c_char_p * max(len(args), 1))(*[a.encode() for a in args])
+        res = gpl_result_t()
+        L.gpl_global_placement(self._ctx, C.byref(cd), len(args), argv, router, C.byref(res))
+        try:
+            return result_to_dict(res)
+        finally:
+            L.gpl_result_free(C.byref(res))
+
+    def close(self):
+        if self._ctx:
+            lib().gpl_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def global_placement(design: Design, args, router=None, device=0, poisson="mixed") -> dict:
+    """The `global_placement` command on one B200 (src/run.rs:115)."""
+    p = Placer(device, poisson)
+    try:
+        return p.global_placement(design, args, router)
+    finally:
+        p.close()
+
+
+class SyntheticRouter:
+    """The stand-in router (`gpl_synthetic_router_create`): uniform tiles over the die."""
+
+    def __init__(self, design: Design, tile_size, pitches=(380, 380, 380, 380), capacity=20):
+        self._cd = design.c_struct()
+        arr = (C.c_int32 * len(pitches))(*pitches)
+        self.ptr = lib().gpl_synthetic_router_create(C.byref(self._cd), tile_size, len(pitches), arr, capacity)
+
+    def close(self):
+        if self.ptr:
+            lib().gpl_synthetic_router_destroy(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.close()

@@ -177,34 +177,36 @@ void gpl_synthetic_router_destroy(gpl_router_t *router);
  * CUDA error code. None has a reference entry point of its own; each names the function whose
  * result it computes. */
 
-/* The bin-density scatter `update_bins_gcell_density_area` (src/nesterov.rs:2218-2263):
- * cells' density boxes (centre cx, cy; half sizes hx, hy) over a grid of nx * ny bins whose
- * edges are bx[0..nx], by[0..ny]; kind 0 std cell, 1 macro, 2 filler. Writes the int64
- * accumulators inst[nx*ny], filler[nx*ny] (x-major: index x*ny + y), zeroed first. */
+/* The bin-density scatter `update_bins_gcell_density_area` (src/nesterov.rs:2218-2250):
+ * cells' density boxes (integer centre cx, cy; half sizes hx, hy; density scale; kind 0 std
+ * cell, 1 macro, 2 filler) over a grid of nx * ny bins whose lower-left is (grid_lx, grid_ly),
+ * edges bx[0..nx], by[0..ny], bin sizes size_x, size_y. Writes the int64 accumulators
+ * inst[nx*ny] and filler[nx*ny] (x-major: index x*ny + y), zeroed first. */
 int gpl_kernel_density_scatter(int64_t n_cells, const int32_t *cx, const int32_t *cy,
                                const int32_t *hx, const int32_t *hy, const float *scale,
-                               const uint8_t *kind, int32_t nx, int32_t ny, const int32_t *bx,
-                               const int32_t *by, double size_x, double size_y,
-                               float target_density, int64_t *inst, int64_t *filler,
-                               void *stream);
+                               const uint8_t *kind, int32_t nx, int32_t ny, int32_t grid_lx,
+                               int32_t grid_ly, const int32_t *bx, const int32_t *by,
+                               double size_x, double size_y, float target_density,
+                               int64_t *inst, int64_t *filler, void *stream);
 
 /* `Fft::solve` (src/nesterov.rs:412-444) without the potential: density[nx*ny] (x-major) to
- * field_x, field_y. mode 0 = FP32 SIMT GEMMs, 1 = split-BF16 tcgen05 GEMMs. wx[nx], wy[ny] are
- * the wavenumbers. `workspace` holds gpl_poisson_workspace_bytes(nx, ny) bytes. */
-size_t gpl_poisson_workspace_bytes(int32_t nx, int32_t ny);
+ * field_x, field_y (device pointers). mode 0 = FP32 SIMT GEMMs, 1 = split-BF16 tcgen05 GEMMs.
+ * wx[nx], wy[ny] are the wavenumbers (host pointers). Builds its basis matrices and workspace
+ * per call, so it allocates. */
 int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy,
                        const float *density, float *field_x, float *field_y, int mode,
-                       void *workspace, void *stream);
+                       void *stream);
 
 /* `update_wirelength_force_wa` + `wl_gradient_pin` (src/nesterov.rs:2325-2414): per net (pins
- * net-major, net_start[n_nets+1]), per pin its position px, py; coefficients cx, cy; writes
- * each pin's force (gmin - gmax) scaled by its net's weight into grad[2*n_pins]. */
-int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *px,
-                  const int32_t *py, const float *net_weight, float coef_x, float coef_y,
-                  float *grad, void *stream);
+ * net-major, net_start[n_nets+1]), per pin its position pin_xy[2*p], pin_xy[2*p+1];
+ * coefficients coef_x, coef_y; writes each pin's force (gmin - gmax) scaled by its net's weight
+ * (net_weight may be NULL: 1) into grad[2*n_pins]. */
+int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy,
+                  const float *net_weight, float coef_x, float coef_y, float *grad, void *stream);
 
-/* The initial placement's solver `bicgstab` (src/bicgstab.rs:615-669) on a CSR matrix with
- * FP64 inner products; x is the start point and the result. Writes iterations and error. */
+/* The initial placement's solver `bicgstab` (src/bicgstab.rs:615-669) on a CSR matrix (device
+ * pointers) with FP64 inner products; x is the start point and the result. Writes iterations
+ * and error (host pointers). Allocates its scratch vectors per call. */
 int gpl_kernel_bicgstab(int64_t n, const int64_t *row_start, const int32_t *cols,
                         const float *vals, const float *rhs, float *x, int32_t max_iters,
                         int32_t *iterations, float *error, void *stream);

@@ -2659,6 +2659,120 @@ void oracle_poisson(int nx, int ny, float bin_x, float bin_y, const float *densi
   if (wx) std::copy(f.wx.begin(), f.wx.end(), wx);
   if (wy) std::copy(f.wy.begin(), f.wy.end(), wy);
 }
+// ---- per-kernel references for the device kernels (grids x-major as the device's) ----
+static BinGrid make_grid(int nx, int ny, int32_t glx, int32_t gly, const int32_t *bx, const int32_t *by, double sx, double sy, float td) {
+  BinGrid bg;
+  bg.lx = glx;
+  bg.ly = gly;
+  bg.ux = bx[nx];
+  bg.uy = by[ny];
+  bg.cnt_x = nx;
+  bg.cnt_y = ny;
+  bg.size_x = sx;
+  bg.size_y = sy;
+  bg.bins.resize((size_t)nx * ny);
+  for (int y = 0; y < ny; y++)
+    for (int x = 0; x < nx; x++) {
+      Bin &b = bg.bins[(size_t)y * nx + x];
+      b.lx = bx[x];
+      b.ux = bx[x + 1];
+      b.ly = by[y];
+      b.uy = by[y + 1];
+      b.target_density = td;
+    }
+  return bg;
+}
+static GCell cell_at(int32_t cx, int32_t cy, int32_t hx, int32_t hy, float scale, uint8_t kind) {
+  GCell g;
+  g.inst = kind == 2 ? -1 : 0;
+  g.macro_ = kind == 1;
+  g.dlx = cx - hx;
+  g.dux = cx + hx;
+  g.dly = cy - hy;
+  g.duy = cy + hy;
+  g.density_scale = scale;
+  return g;
+}
+// updateBinsGCellDensityArea's scatter (src/nesterov.rs:2218-2250): int64 accumulators.
+void oracle_density_scatter(int64_t n, const int32_t *cx, const int32_t *cy, const int32_t *hx, const int32_t *hy, const float *scale, const uint8_t *kind, int nx, int ny, int32_t glx, int32_t gly, const int32_t *bx, const int32_t *by, double sx, double sy, float td, int64_t *inst, int64_t *filler) {
+  BinGrid bg = make_grid(nx, ny, glx, gly, bx, by, sx, sy, td);
+  for (int64_t i = 0; i < n; i++) {
+    GCell g = cell_at(cx[i], cy[i], hx[i], hy[i], scale[i], kind[i]);
+    auto [x0, x1] = bg.density_idx_x(g);
+    auto [y0, y1] = bg.density_idx_y(g);
+    for (int32_t y = y0; y < y1; y++)
+      for (int32_t x = x0; x < x1; x++) {
+        Bin &bin = bg.bins[(size_t)y * nx + x];
+        float a = overlap_density_area(bin, g) * g.density_scale;
+        if (g.is_macro()) a *= bin.target_density;
+        if (g.is_filler())
+          bin.filler += f2l(overlap_density_area(bin, g) * g.density_scale);
+        else
+          bin.inst_placed_unscaled += f2l(a);
+      }
+  }
+  for (int y = 0; y < ny; y++)
+    for (int x = 0; x < nx; x++) {
+      const Bin &b = bg.bins[(size_t)y * nx + x];
+      inst[(size_t)x * ny + y] = b.inst_placed_unscaled;
+      filler[(size_t)x * ny + y] = b.filler;
+    }
+}
+// getDensityGradient (src/nesterov.rs:2434-2449) per cell over x-major fields.
+void oracle_density_gradient(int64_t n, const int32_t *cx, const int32_t *cy, const int32_t *hx, const int32_t *hy, const float *scale, int nx, int ny, int32_t glx, int32_t gly, const int32_t *bx, const int32_t *by, double sx, double sy, const float *fx, const float *fy, float *out) {
+  BinGrid bg = make_grid(nx, ny, glx, gly, bx, by, sx, sy, 1.0f);
+  for (int y = 0; y < ny; y++)
+    for (int x = 0; x < nx; x++) {
+      bg.bins[(size_t)y * nx + x].field_x = fx[(size_t)x * ny + y];
+      bg.bins[(size_t)y * nx + x].field_y = fy[(size_t)x * ny + y];
+    }
+  for (int64_t i = 0; i < n; i++) {
+    GCell g = cell_at(cx[i], cy[i], hx[i], hy[i], scale[i], 0);
+    auto [x0, x1] = bg.density_idx_x(g);
+    auto [y0, y1] = bg.density_idx_y(g);
+    float f0 = 0, f1 = 0;
+    for (int32_t x = x0; x < x1; x++)
+      for (int32_t y = y0; y < y1; y++) {
+        const Bin &bin = bg.bins[(size_t)y * nx + x];
+        float a = overlap_density_area(bin, g) * g.density_scale;
+        f0 += a * bin.field_x;
+        f1 += a * bin.field_y;
+      }
+    out[2 * i] = f0;
+    out[2 * i + 1] = f1;
+  }
+}
+// updateWireLengthForceWA + getWireLengthGradientPinWA x net weight (src/nesterov.rs:2325-2430)
+// for pins at the given positions, net-major.
+void oracle_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, const float *weight, float cx, float cy, float *grad) {
+  Nesterov np;
+  int64_t np_pins = net_start[n_nets];
+  np.gpins.resize(np_pins);
+  for (int64_t p = 0; p < np_pins; p++) {
+    np.gpins[p].cx = pin_xy[2 * p];
+    np.gpins[p].cy = pin_xy[2 * p + 1];
+  }
+  np.gnets.resize(n_nets);
+  np.pin_net.resize(np_pins);
+  for (int64_t n = 0; n < n_nets; n++)
+    for (int64_t p = net_start[n]; p < net_start[n + 1]; p++) {
+      np.gnets[n].pins.push_back((int)p);
+      np.pin_net[p] = (int)n;
+    }
+  if (weight)
+    for (int64_t n = 0; n < n_nets; n++) np.gnets[n].custom_weight = weight[n];
+  np.wl_coef_x = cx;
+  np.wl_coef_y = cy;
+  np.update_wirelength_force_wa();
+  for (int64_t p = 0; p < np_pins; p++) {
+    int n = np.pin_net[p];
+    FloatPoint t = np.wl_gradient_pin((int)p, n);
+    float w = np.gnets[n].total_weight();
+    grad[2 * p] = t.x * w;
+    grad[2 * p + 1] = t.y * w;
+  }
+}
+
 // The 1-D transforms, for checking against direct sums. kind 0 dct2, 1 idct, 2 idst.
 void oracle_dct1(int n, int kind, const double *in, double *out) {
   Dct1 t(n);

@@ -55,6 +55,22 @@ def lib():
         _lib.oracle_poisson.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float] + [C.c_void_p] * 6
         _lib.oracle_dct1.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         _lib.oracle_transform2.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        _lib.oracle_rudy.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p] + [C.c_void_p] * 5
+        _lib.oracle_top_averages.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        _lib.oracle_density_scatter.argtypes = [C.c_int64] + [C.c_void_p] * 6 + [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_float, C.c_void_p, C.c_void_p]
+        _lib.oracle_density_gradient.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.oracle_wa.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_void_p]
+        _lib.oracle_uniform_int_draws.argtypes = [C.c_uint32, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+        _lib.oracle_min_max_idx.argtypes = [C.c_int32] * 6 + [C.c_void_p]
+        _lib.oracle_snap_outward.argtypes = [C.c_void_p] + [C.c_int32] * 4
+        _lib.oracle_orient_point.argtypes = [C.c_int, C.c_int32, C.c_int32, C.c_void_p]
+        _lib.oracle_union_area.argtypes = [C.c_int, C.c_void_p]
+        _lib.oracle_distance.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
+        _lib.oracle_set_size.argtypes = [C.c_void_p, C.c_int32, C.c_int32]
+        _lib.oracle_diverge_fallback.argtypes = [C.c_int, C.c_int, C.c_int]
+        _lib.oracle_routability_recovery_attempt.argtypes = [C.c_int] * 5
+        _lib.oracle_settle_wait_step.argtypes = [C.c_int] * 4 + [C.c_void_p]
+        _lib.oracle_round_down_pow2.argtypes = [C.c_uint32]
     return _lib
 
 

@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark: Nesterov iterations/s of the global-placement engine on one B200 per rank.
+
+Workload (one "step" = one Nesterov iteration with its back-tracking trials): the 1M-cell
+synthetic design (about 1.05M nets, 4M pins, 32 macros over 15 % of the core) with a
+1024 x 1024 bin grid, `-density 0.70 -bin_grid_count 1024`, after construction, the initial
+placement and the Nesterov set-up (untimed). The mixed form (split-BF16 tcgen05 density
+solve) is the headline; the plain FP32 form is timed beside it on the same placement run.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 (under torchrun): one independent replica per GPU (the path has no exchange step), the
+time is the max over ranks, `value` the iterations of all ranks over it.
+--impl reference: the reference's CPU path (its restatement, single-threaded as the reference
+is) on the same workload, each step one Nesterov iteration.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Nesterov iters/s at 1M cells,1024² bins: mixed vs FP32 GPU at ≤0.1% HPWL"
+CONFIGS = {
+    "cfg3": dict(preset="cfg3", args=["-density", "0.70", "-bin_grid_count", "1024"], name="1M cells / 1.05M nets / 4M pins, 1024x1024 bins"),
+    "cfg2": dict(preset="cfg2", args=["-density", "0.70", "-bin_grid_count", "512"], name="100k cells / 105k nets / 400k pins, 512x512 bins"),
+    "cfg1": dict(preset="cfg1", args=["-density", "0.70", "-bin_grid_count", "64"], name="294 cells / 364 nets / 1122 pins, 64x64 bins"),
+}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() in ("active", "1")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def algorithmic(phase, C, P, N, B, mixed, nx):
+    """Bytes (or FLOPs) one launch of a phase must move (compulsory traffic), per region."""
+    if phase == "scatter":
+        return "hbm", C * 61 + B * 16  # cell state in, next/next_slp/centre out; the two int64 accumulators
+    if phase == "bin_finalize":
+        return "hbm", B * (56 + (4 if mixed else 0))
+    if phase == "wa":
+        return "hbm", N * 16 + P * 28
+    if phase == "gradients":
+        return "hbm", C * 64 + P * 12 + B * 8
+    if phase == "hpwl":
+        return "hbm", N * 8 + P * 20
+    if phase == "density_solve":
+        n3 = float(nx) ** 3
+        return "tensor" if mixed else "fp32", (36.0 if mixed else 12.0) * n3
+    return "hbm", 0
+
+
+def log(msg):
+    print(f"[bench {time.perf_counter() - T0:8.2f}] {msg}", file=sys.stderr, flush=True)
+
+
+T0 = time.perf_counter()
+
+
+def ours(a):
+    import torch
+    import torch.distributed as dist
+    from gpl_b200 import engine, synth
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    cfg = CONFIGS[a.config]
+    design = synth.generate(cfg["preset"])
+    log("design generated")
+    C_cells = design.meta["cells"]
+    placer = engine.Placer(local, a.form)
+    sess = engine.Session(placer, design, cfg["args"])
+    log("session open")
+    sess.iterate(a.warmup)
+    log("warm-up done")
+    if sess.done:
+        raise SystemExit("the loop ended during warm-up: " + json.dumps(sess.close().get("reason")))
+    stream = torch.cuda.ExternalStream(sess.stream, device=local)
+
+    def timed(k, label):
+        sess.set_option("profile", "1")
+        c0 = sess.counters()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            e0.record(stream)
+            t0 = time.perf_counter()
+            done = sess.iterate(k)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            wall = time.perf_counter() - t0
+        if world > 1:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        c1 = sess.counters()
+        prof = sess.profile()
+        sess.set_option("profile", "0")
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return {"ms": float(t.item()), "iters": done, "wall_s": wall, "profile": prof, "clocks": clk.summary(),
+                "launches": c1["launches"] - c0["launches"]}
+
+    cells_total = sess.counters()["cells"]
+    if a.form == "mixed":
+        mixed = timed(a.steps, "mixed")
+        sess.set_option("poisson", "fp32")
+        sess.iterate(min(a.warmup, 3))
+    fp32 = timed(a.steps, "fp32")
+    if a.form == "fp32":
+        mixed = fp32
+    log("timed")
+    res = sess.close()
+    log("session closed")
+    P_pins, N_nets = res["pins"], res["nets"]
+    # the placement run's own figures: fillers in the cell count
+    nx = int(cfg["args"][cfg["args"].index("-bin_grid_count") + 1])
+    B = nx * nx
+    # e2e: the whole command through the public C ABI, host arrays in, locations out
+    e2e = None
+    if not a.no_e2e:
+        t0 = time.perf_counter()
+        r = engine.global_placement(design, cfg["args"], device=local, poisson=a.form)
+        e2e_s = time.perf_counter() - t0
+        log("e2e run done")
+        its = r["nesterov_iterations"] or 0
+        e2e = {"value": its * world / e2e_s if e2e_s > 0 else 0.0, "unit": "iters/s", "seconds": e2e_s,
+               "iterations": its, "status": r["status"],
+               "h2d_bytes_per_step": int(r["h2d_bytes"] / max(its, 1)), "d2h_bytes_per_step": int(r["d2h_bytes"] / max(its, 1)),
+               "final_hpwl": r["final_hpwl"], "final_overflow": r["final_overflow"],
+               "seconds_initial_place": r["seconds_initial_place"], "seconds_nesterov": r["seconds_nesterov"]}
+    if rank != 0:
+        return
+    pk, pk_kind = peaks()
+    value = mixed["iters"] * world / (mixed["ms"] / 1000.0)
+    value_fp32 = fp32["iters"] * world / (fp32["ms"] / 1000.0)
+    # the dominant kernel of the mixed form by device time
+    prof = mixed["profile"]
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    name, (ms_tot, launches) = dom
+    bound, work = algorithmic(name, cells_total, P_pins, N_nets, B, a.form == "mixed", nx)
+    per_launch_s = ms_tot / 1000.0 / max(launches, 1)
+    if bound == "fp32":
+        achieved = work / per_launch_s / 1e12
+        roof = {"bound": "fp32-simt", "achieved": achieved, "peak": 2 * 148 * 128 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12, "unit": "TFLOP/s"}
+    elif bound == "tensor":
+        achieved = work / per_launch_s / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": pk["bf16_tflops_sustained"], "unit": "TFLOP/s"}
+    else:
+        achieved = work / per_launch_s / 1e9
+        roof = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s"}
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    roof["kernel"] = name
+    roof["peak_source"] = pk_kind
+    traffic = None
+    try:
+        summ = json.load(open(os.path.join(ROOT, "profiles", "ncu_traffic.json")))
+        traffic = summ.get(name, {}).get("bytes_per_launch")
+    except Exception:
+        pass
+    roof["traffic"] = traffic
+    phases = {k: {"ms_total": v[0], "launches": v[1], "share": v[0] / max(sum(x[0] for x in prof.values()), 1e-9)} for k, v in prof.items()}
+    cpu = None
+    if world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(a, design)
+    out = {
+        "metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": mixed["ms"] / max(mixed["iters"], 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+bf16x3 (split-BF16 density solve), f64 reductions", "data": "synthetic",
+        "config": {"workload": cfg["name"], "args": cfg["args"], "design": design.meta["config"],
+                   "cells": C_cells, "nets": N_nets, "pins": P_pins, "bins": B, "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2 (126 MB): cells, pins and bins stream from HBM each trial"},
+        "form": a.form,
+        "forms": {"mixed": {"iters_per_s": value, "ms_per_iter": mixed["ms"] / max(mixed["iters"], 1), "iters": mixed["iters"]},
+                  "fp32": {"iters_per_s": value_fp32, "ms_per_iter": fp32["ms"] / max(fp32["iters"], 1), "iters": fp32["iters"]},
+                  "mixed_over_fp32": value / value_fp32 if value_fp32 else None},
+        "phases": phases, "roofline": roof, "gpu_launches": mixed["launches"], "clocks": mixed["clocks"],
+        "e2e": e2e, "cpu_baseline": cpu,
+    }
+    print(json.dumps(out))
+
+
+def cpu_baseline(a, design):
+    """The oracle (the reference's CPU path restated, one thread) on a bounded sample."""
+    import oracle
+    cfg = CONFIGS[a.config]
+    t0 = time.perf_counter()
+    s = oracle.Session(design, cfg["args"] + ["-skip_initial_place"])
+    setup = time.perf_counter() - t0
+    s.iterate(1)
+    k = a.cpu_iters
+    tr0 = s.trials()
+    t0 = time.perf_counter()
+    done = s.iterate(k)
+    dt = time.perf_counter() - t0
+    trials = s.trials() - tr0
+    s.discard()
+    return {"value": done / dt if dt > 0 else 0.0, "unit": "iters/s", "cores": 1, "kind": "port",
+            "sample": f"{done} Nesterov iterations ({trials} trials) of the same design after its set-up ({setup:.1f} s, initial placement skipped), single thread",
+            "seconds_per_iter": dt / max(done, 1)}
+
+
+def reference(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    from gpl_b200 import synth
+    cfg = CONFIGS[a.config]
+    design = synth.generate(cfg["preset"])
+    s = oracle.Session(design, cfg["args"] + ["-skip_initial_place"])
+    s.iterate(a.warmup)
+    tr0 = s.trials()
+    t0 = time.perf_counter()
+    done = s.iterate(a.steps)
+    dt = time.perf_counter() - t0
+    trials = s.trials() - tr0
+    s.discard()
+    v = done / dt if dt > 0 else 0.0
+    out = {"metric": METRIC, "value": v, "unit": "iters/s", "impl": "reference", "n_gpus": world, "steps": a.steps,
+           "warmup": a.warmup, "ms_per_step": 1000.0 * dt / max(done, 1), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 (the reference's float order), f64 where the reference uses double", "data": "synthetic",
+           "config": {"workload": cfg["name"], "args": cfg["args"], "design": design.meta["config"], "parallelism": "1 CPU thread"},
+           "cpu_baseline": {"value": v, "unit": "iters/s", "cores": 1, "kind": "port",
+                            "sample": f"{done} Nesterov iterations ({trials} trials) per the timed steps, initial placement skipped; the reference runs on one thread"},
+           "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="cfg3", choices=list(CONFIGS))
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-iters", type=int, default=8)
+    ap.add_argument("--form", default="mixed", choices=["mixed", "fp32"], help="the density solve timed as the headline")
+    a = ap.parse_args()
+    if a.warmup < 3:
+        a.warmup = 3
+    if a.impl == "reference":
+        reference(a)
+    else:
+        ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -54,10 +54,12 @@ static cudaError_t dmalloc(T **p, size_t n) {
   if (n == 0) n = 1;
   return cudaMalloc((void **)p, n * sizeof(T));
 }
+static int64_t g_h2d = 0;  // bytes the uploads below copied (folded into the engine's counter)
 template <class T>
 static cudaError_t upload_vec(T **p, const std::vector<T> &v, cudaStream_t s) {
   cudaError_t e = dmalloc(p, v.size());
   if (e != cudaSuccess || v.empty()) return e;
+  g_h2d += (int64_t)(v.size() * sizeof(T));
   return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
 }
 
@@ -97,10 +99,13 @@ Solve Engine::solve(const Csr &m, const std::vector<float> &rhs, std::vector<flo
     check(cudaMemcpyAsync(ip_b_, rhs.data(), n * sizeof(float), cudaMemcpyHostToDevice, s), "ip h2d");
     check(cudaMemcpyAsync(ip_x_, x.data(), n * sizeof(float), cudaMemcpyHostToDevice, s), "ip h2d");
   }
+  h2d_bytes += (n + 1) * 8 + nnz * 8 + n * 8;
   CsrDev A{n, ip_rs_, ip_cols_, ip_vals_};
   BicgResult r{};
   check(bicgstab_solve(A, ip_b_, ip_x_, max_iters, ip_scratch_, s, &r), "bicgstab");
   if (n) check(cudaMemcpyAsync(x.data(), ip_x_, n * sizeof(float), cudaMemcpyDeviceToHost, s), "ip d2h");
+  d2h_bytes += n * 4 + (int64_t)(r.iterations + 2) * 64;
+  launches += 4 + (int64_t)r.iterations * 10;
   check(cudaStreamSynchronize(s), "ip sync");
   out.iterations = r.iterations;
   out.error = r.error;
@@ -173,7 +178,13 @@ void Engine::upload(const EngineSetup &s) {
   check(dmalloc(&hpwl_acc_, 1), "alloc");
   check(dmalloc(&dev_scal_, s.regions.size()), "alloc");
   host_scal_.assign(s.regions.size(), RegionScalars{});
+  region_wx_.clear();
+  region_wy_.clear();
+  region_dims_.clear();
   for (const RegionSetup &rs : s.regions) {
+    region_wx_.push_back(rs.wx);
+    region_wy_.push_back(rs.wy);
+    region_dims_.push_back({rs.nx, rs.ny});
     Region *r = new Region();
     regions_.push_back(r);
     int64_t nb = (int64_t)rs.nx * rs.ny;
@@ -229,6 +240,8 @@ void Engine::upload(const EngineSetup &s) {
     a.field_y = r->fy;
   }
   check(cudaStreamSynchronize(st), "upload sync");
+  h2d_bytes += g_h2d + n_pins_ * 8;
+  g_h2d = 0;
 }
 
 void Engine::update_bins(int b, const RegionSetup &rs) {
@@ -282,12 +295,14 @@ static CellArgs cell_args(const int64_t off, int32_t *dcx, int32_t *dcy, int32_t
 void Engine::set_coords(int b, SlotId slot, const std::vector<float> &xy) {
   Region *r = regions_[b];
   if (r->n_cells) check(cudaMemcpyAsync(r->slot[slot], xy.data(), r->n_cells * sizeof(float2), cudaMemcpyHostToDevice, stream_), "set_coords");
+  h2d_bytes += r->n_cells * 8;
 }
 
 std::vector<float> Engine::get_coords(int b, SlotId slot) {
   Region *r = regions_[b];
   std::vector<float> xy(2 * r->n_cells);
   if (r->n_cells) check(cudaMemcpyAsync(xy.data(), r->slot[slot], r->n_cells * sizeof(float2), cudaMemcpyDeviceToHost, stream_), "get_coords");
+  d2h_bytes += r->n_cells * 8;
   check(cudaStreamSynchronize(stream_), "get_coords sync");
   return xy;
 }
@@ -296,9 +311,14 @@ void Engine::place_at(int b, SlotId slot) {
   if (failed()) return;
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
+  ph_begin(PH_PLACE);
+  launches += (r->n_cells ? 1 : 0) + 2;
   if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, c, PLACE_AT, 0.0f, 0.0f, r->slot[slot]);
+  ph_end(PH_PLACE);
+  ph_begin(PH_FINALIZE);
   k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld);
   k_reduce_partials<<<1, kThreadsPerBlock, 0, stream_>>>(r->part, r->nb_bins, 2, &dev_scal_[b].overflow);
+  ph_end(PH_FINALIZE);
   check(cudaGetLastError(), "place_at");
 }
 
@@ -306,16 +326,24 @@ void Engine::nesterov_step(int b, float step, float coeff) {
   if (failed()) return;
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
+  ph_begin(PH_PLACE);
+  launches += (r->n_cells ? 1 : 0) + 2;
   if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, c, PLACE_NESTEROV, step, coeff, nullptr);
+  ph_end(PH_PLACE);
+  ph_begin(PH_FINALIZE);
   k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld);
   k_reduce_partials<<<1, kThreadsPerBlock, 0, stream_>>>(r->part, r->nb_bins, 2, &dev_scal_[b].overflow);
+  ph_end(PH_FINALIZE);
   check(cudaGetLastError(), "nesterov_step");
 }
 
 void Engine::field(int b) {
   if (failed()) return;
   Region *r = regions_[b];
+  ph_begin(PH_POISSON);
   check(poisson_solve(r->plan, r->density, r->fx, r->fy, stream_), "poisson");
+  ph_end(PH_POISSON);
+  launches += poisson_launches(r->plan);
 }
 
 void Engine::wa(float cx, float cy) {
@@ -330,7 +358,10 @@ void Engine::wa(float cx, float cy) {
   w.dcx = dcx_;
   w.dcy = dcy_;
   w.pin_grad = pin_grad_;
+  ph_begin(PH_WA);
+  launches += 1;
   k_wa<<<blocks_for(n_nets_), kThreadsPerBlock, 0, stream_>>>(w, cx, cy);
+  ph_end(PH_WA);
   check(cudaGetLastError(), "wa");
 }
 
@@ -342,8 +373,11 @@ void Engine::gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, S
   const float2 *pb1 = b1 == S_NUM ? nullptr : r->slot[b1];
   const float2 *pb2 = b2 == S_NUM ? nullptr : r->slot[b2];
   if (r->n_cells) {
+    ph_begin(PH_GRAD);
+    launches += 2;
     k_gradients<<<r->nb_cells, kThreadsPerBlock, 0, stream_>>>(r->args, c, pin_grad_, penalty, r->slot[out], pa1, pb1, pb2, r->part);
     k_reduce_partials<<<1, kThreadsPerBlock, 0, stream_>>>(r->part, r->nb_cells, 4, &dev_scal_[b].wl_sum);
+    ph_end(PH_GRAD);
   } else {
     check(cudaMemsetAsync(&dev_scal_[b].wl_sum, 0, 4 * sizeof(double), stream_), "gradients");
   }
@@ -376,7 +410,9 @@ void Engine::copy_slot(int b, SlotId dst, SlotId src) {
 void Engine::fetch() {
   if (failed() || host_scal_.empty()) return;
   check(cudaMemcpyAsync(host_scal_.data(), dev_scal_, host_scal_.size() * sizeof(RegionScalars), cudaMemcpyDeviceToHost, stream_), "fetch");
+  d2h_bytes += (int64_t)(host_scal_.size() * sizeof(RegionScalars));
   check(cudaStreamSynchronize(stream_), "fetch sync");
+  ph_flush();
 }
 
 int64_t Engine::hpwl() {
@@ -389,10 +425,15 @@ int64_t Engine::hpwl() {
   w.dcx = dcx_;
   w.dcy = dcy_;
   check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), stream_), "hpwl");
+  ph_begin(PH_HPWL);
+  launches += n_nets_ ? 1 : 0;
   if (n_nets_) k_hpwl<<<blocks_for(n_nets_), kThreadsPerBlock, 0, stream_>>>(w, hpwl_acc_);
+  ph_end(PH_HPWL);
   unsigned long long h = 0;
   check(cudaMemcpyAsync(&h, hpwl_acc_, sizeof h, cudaMemcpyDeviceToHost, stream_), "hpwl");
+  d2h_bytes += 8;
   check(cudaStreamSynchronize(stream_), "hpwl sync");
+  ph_flush();
   return (int64_t)h;
 }
 
@@ -402,12 +443,86 @@ void Engine::centres(std::vector<int32_t> &dcx, std::vector<int32_t> &dcy) {
   if (n_cells_) {
     check(cudaMemcpyAsync(dcx.data(), dcx_, n_cells_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "centres");
     check(cudaMemcpyAsync(dcy.data(), dcy_, n_cells_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "centres");
+    d2h_bytes += n_cells_ * 8;
   }
   check(cudaStreamSynchronize(stream_), "centres sync");
 }
 
 void Engine::set_net_weights(const std::vector<float> &w) {
   if (!w.empty()) check(cudaMemcpyAsync(net_weight_, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, stream_), "net weights");
+}
+
+void Engine::rebuild_poisson(int mode) {
+  poisson_mode_ = mode;
+  for (size_t b = 0; b < regions_.size(); b++) {
+    Region *r = regions_[b];
+    check(cudaStreamSynchronize(stream_), "rebuild sync");
+    poisson_plan_destroy(r->plan);
+    r->plan = nullptr;
+    r->dens_split = nullptr;
+    r->split_ld = 0;
+    cudaError_t pe = cudaSuccess;
+    r->plan = poisson_plan_create(region_dims_[b].first, region_dims_[b].second, region_wx_[b].data(), region_wy_[b].data(), mode, &pe);
+    check(pe, mode == 0 ? "poisson plan (fp32)" : "poisson plan (split-bf16 tcgen05)");
+    if (r->plan) {
+      r->dens_split = poisson_split_input(r->plan, &r->split_ld);
+      // the current density into the new operand, the field recomputed
+      if (r->dens_split) check(poisson_split_density(r->plan, r->density, stream_), "split density");
+      check(poisson_solve(r->plan, r->density, r->fx, r->fy, stream_), "poisson");
+    }
+  }
+  check(cudaStreamSynchronize(stream_), "rebuild sync");
+}
+
+void Engine::set_profile(bool on) {
+  profile_ = on;
+  for (int k = 0; k < PH_COUNT; k++) {
+    ph_ms_[k] = 0;
+    ph_n_[k] = 0;
+  }
+  ev_pending_.clear();
+  ev_used_ = 0;
+}
+
+void Engine::ph_begin(int ph) {
+  if (!profile_) return;
+  if (ev_used_ + 2 > ev_.size()) {
+    for (int k = 0; k < 64; k++) {
+      cudaEvent_t e;
+      check(cudaEventCreate(&e), "event");
+      ev_.push_back(e);
+    }
+  }
+  check(cudaEventRecord(ev_[ev_used_], stream_), "event record");
+  ev_pending_.push_back({ph, ev_used_});
+  ev_used_ += 2;
+}
+
+void Engine::ph_end(int ph) {
+  if (!profile_ || ev_pending_.empty()) return;
+  check(cudaEventRecord(ev_[ev_pending_.back().second + 1], stream_), "event record");
+}
+
+void Engine::ph_flush() {
+  if (!profile_) return;
+  for (auto &[ph, i] : ev_pending_) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ev_[i], ev_[i + 1]) == cudaSuccess) {
+      ph_ms_[ph] += ms;
+      ph_n_[ph] += 1;
+    }
+  }
+  ev_pending_.clear();
+  ev_used_ = 0;
+}
+
+int Engine::profile_read(double *ms, int64_t *launches, int cap) {
+  int n = std::min<int>(cap, PH_COUNT);
+  for (int k = 0; k < n; k++) {
+    ms[k] = ph_ms_[k];
+    launches[k] = ph_n_[k];
+  }
+  return n;
 }
 
 }  // namespace gpl

@@ -98,6 +98,13 @@ class Engine {
   // whole cell block is rewritten).
   void rewrite_cells(const EngineSetup &s);
   int64_t trials = 0;
+  int64_t launches = 0, h2d_bytes = 0, d2h_bytes = 0;  // counters for the run's report
+  // The density solvers rebuilt in another mode (0 FP32, 1 split-BF16 tensor cores).
+  void rebuild_poisson(int mode);
+  // Per-phase device time (CUDA events on the engine's stream around each launch group).
+  enum Phase { PH_PLACE = 0, PH_FINALIZE, PH_POISSON, PH_WA, PH_GRAD, PH_HPWL, PH_COUNT };
+  void set_profile(bool on);
+  int profile_read(double *ms, int64_t *launches, int cap);
   bool failed() const { return err_.code != cudaSuccess; }
   const DeviceError &error() const { return err_; }
   void check(cudaError_t e, const char *where);
@@ -137,6 +144,18 @@ class Engine {
   float *ip_vals_ = nullptr, *ip_b_ = nullptr, *ip_x_ = nullptr;
   size_t ip_nnz_cap_ = 0, ip_n_cap_ = 0;
   void free_globals();
+  // profiling
+  bool profile_ = false;
+  std::vector<cudaEvent_t> ev_;
+  size_t ev_used_ = 0;
+  std::vector<std::pair<int, size_t>> ev_pending_;
+  double ph_ms_[PH_COUNT] = {};
+  int64_t ph_n_[PH_COUNT] = {};
+  std::vector<std::vector<float>> region_wx_, region_wy_;
+  std::vector<std::pair<int, int>> region_dims_;
+  void ph_begin(int ph);
+  void ph_end(int ph);
+  void ph_flush();
 };
 
 }  // namespace gpl

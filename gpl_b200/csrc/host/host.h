@@ -238,3 +238,9 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v);
 Ip do_bicgstab_place(Log &log, const Design &d, Common &c, const Vars &v, const IpVars &vars, const SolveFn &solve);
 
 }  // namespace gpl
+
+namespace gpl {
+// Progress lines on stderr, with the seconds since the first call, when GPL_LOG is set in the
+// environment (timings of the host phases; the run's report is unaffected).
+void progress(const char *fmt, ...) __attribute__((format(printf, 1, 2)));
+}  // namespace gpl

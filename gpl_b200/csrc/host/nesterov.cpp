@@ -1580,52 +1580,63 @@ static EngineSetup engine_setup(Placer &P) {
   return s;
 }
 
-// `resume_nesterov_place` (src/nesterov.rs:4440-4610) from iteration 0, routability off.
-static int resume_nesterov_place(Log &log, const Design &d, Placer &P) {
-  log.info("GPL", 84, "---- Execute Nesterov Global Placement.");
-  if (P.num_region_diverged > 0) log.error("GPL", P.diverge_code, P.diverge_msg);
-  int64_t original_area = 0;
-  for (auto &nb : P.nbs) {
-    nb.max_phi_coef_changed = false;
-    nb.min_sum_overflow = 1e30f;
-    nb.hpwl_with_min_sum_overflow = 1e30f;
-    nb.is_converged = false;
-    original_area += nesterov_insts_area(nb);
-  }
+// `resume_nesterov_place` (src/nesterov.rs:4440-4610) from iteration 0, routability off, cut
+// into its prologue, one loop iteration at a time, and its epilogue (so a caller can step it).
+struct NesterovLoop {
   LoopSnapshots snaps;
   float cur_a = 1.0f;
   int iter = 0;
-  while (iter < P.max_iter) {
+  int64_t original_area = 0;
+  bool done = false;
+
+  void begin(Log &log, Placer &P) {
+    log.info("GPL", 84, "---- Execute Nesterov Global Placement.");
+    if (P.num_region_diverged > 0) log.error("GPL", P.diverge_code, P.diverge_msg);
+    for (auto &nb : P.nbs) {
+      nb.max_phi_coef_changed = false;
+      nb.min_sum_overflow = 1e30f;
+      nb.hpwl_with_min_sum_overflow = 1e30f;
+      nb.is_converged = false;
+      original_area += nesterov_insts_area(nb);
+    }
+  }
+  // One pass of the loop's body; false once the loop has ended.
+  bool step(Log &log, const Design &d, Placer &P) {
+    if (done || iter >= P.max_iter) return !(done = true);
+    if (iter % 50 == 0) progress("iteration %d: overflow %.4f, %ld trials", iter, (double)P.average_overflow_unscaled, (long)P.trials);
     float prev_a = cur_a;
     cur_a = (float)((1.0 + std::sqrt(4.0 * (double)prev_a * (double)prev_a + 1.0)) * 0.5);
     float coeff = (float)(((double)prev_a - 1.0) / (double)cur_a);
     P.do_back_tracking(coeff);
     for (size_t b = 0; b < P.nbs.size(); b++) P.nesterov_adjust_phi((int)b);
-    if (P.num_region_diverged > 0) break;
+    if (P.num_region_diverged > 0) return !(done = true);
     P.np_update_next_iter(log, d, iter);
     DivergeAction act = P.np_is_diverged(log, snaps, cur_a);
-    if (act == DivergeAction::Stop) break;
+    if (act == DivergeAction::Stop) return !(done = true);
     if (act == DivergeAction::Resume) {
       iter++;
-      continue;
+      return true;
     }
     int converged = 0;
     for (size_t b = 0; b < P.nbs.size(); b++) converged += P.check_convergence(log, d, (int)b, iter) ? 1 : 0;
-    if (converged == (int)P.nbs.size()) break;
+    if (converged == (int)P.nbs.size()) return !(done = true);
     iter++;
+    return true;
   }
-  if (max_iter_takes_min_hpwl_snapshot(iter, P.max_iter, P.o.disable_revert_if_diverge, snaps, P.diverge_snapshot_overflow, P.average_overflow_unscaled, P.hpwl())) {
-    log.warn("GPL", 121, "Reached the maximum number of iterations, reverting to snapshot with min hpwl.");
-    P.revert_to_diverge_snapshot(log, snaps);
+  int end(Log &log, const Design &d, Placer &P) {
+    if (max_iter_takes_min_hpwl_snapshot(iter, P.max_iter, P.o.disable_revert_if_diverge, snaps, P.diverge_snapshot_overflow, P.average_overflow_unscaled, P.hpwl())) {
+      log.warn("GPL", 121, "Reached the maximum number of iterations, reverting to snapshot with min hpwl.");
+      P.revert_to_diverge_snapshot(log, snaps);
+    }
+    if (iter >= P.max_iter) log.warn("GPL", 1010, sfmt("GPL reached the maximum number of iterations for nesterov %d. Placement may have failed to converge.", P.max_iter));
+    int64_t new_area = 0;
+    for (auto &nb : P.nbs) new_area += nesterov_insts_area(nb);
+    float diff = (float)(100.0 * (double)(new_area - original_area) / (double)original_area);
+    log.info("GPL", 1014, sfmt("Final placement area: %.2f (%+.2f%%)", dbu_area(d, (double)new_area), (double)diff));
+    if (P.num_region_diverged > 0) log.error("GPL", P.diverge_code, P.diverge_msg);
+    return iter;
   }
-  if (iter >= P.max_iter) log.warn("GPL", 1010, sfmt("GPL reached the maximum number of iterations for nesterov %d. Placement may have failed to converge.", P.max_iter));
-  int64_t new_area = 0;
-  for (auto &nb : P.nbs) new_area += nesterov_insts_area(nb);
-  float diff = (float)(100.0 * (double)(new_area - original_area) / (double)original_area);
-  log.info("GPL", 1014, sfmt("Final placement area: %.2f (%+.2f%%)", dbu_area(d, (double)new_area), (double)diff));
-  if (P.num_region_diverged > 0) log.error("GPL", P.diverge_code, P.diverge_msg);
-  return iter;
-}
+};
 
 // `placed_locations` (src/nesterov.rs:4099-4110) from the device's density centres.
 static std::vector<std::array<int32_t, 3>> placed_locations(const Common &c, Placer &P) {
@@ -1652,112 +1663,146 @@ struct RunResult {
   float final_overflow = 0;
   int64_t trials = 0;
   double t_ip = 0, t_np = 0;
+  int64_t h2d = 0, d2h = 0, launches = 0;
 };
 
-// `global_placement` (src/run.rs:115-201) and `do_initial_place` (:292-308).
-static void global_placement(RunResult &res, Engine &eng, const Design &d, const std::vector<std::string> &args, const gpl_router_t *router) {
-  Log &log = res.log;
-  std::map<std::string, std::string> keys;
-  std::vector<std::string> flags;
-  parse_key_args(log, args, keys, flags);
-  auto flag = [&](const char *f) { return std::find(flags.begin(), flags.end(), f) != flags.end(); };
-  if (flag("-place_ios")) {
-    if (flag("-skip_io")) log.error("GPL", 169, "-place_ios cannot be used with -skip_io placement.");
-    if (flag("-incremental")) log.error("GPL", 170, "-place_ios cannot be used with -incremental placement.");
-    if (flag("-skip_nesterov_place")) log.error("GPL", 182, "-place_ios cannot be used with -skip_nesterov_place placement.");
-  }
-  auto in = [&](const char *k) -> int32_t {
-    auto it = keys.find(k);
-    if (it == keys.end()) return 0;
-    int32_t x;
-    if (!parse_i32(it->second, x)) refuse(std::string(k) + " " + it->second + ": not an integer");
-    return x;
-  };
-  Vars vars;
-  vars.pad_left = in("-pad_left");
-  vars.pad_right = in("-pad_right");
-  vars.skip_io = flag("-skip_io");
-  vars.place_ios = flag("-place_ios");
-  vars.disable_pin_density_adjust = flag("-disable_pin_density_adjust");
-  IpVars ipv;
-  ipv.force_center = flag("-force_center_initial_place");
-  if (flag("-skip_initial_place")) ipv.max_iter = 0;
-  if (keys.count("-initial_place_max_iter")) ipv.max_iter = std::max(in("-initial_place_max_iter"), 0);
-  if (keys.count("-initial_place_max_fanout")) ipv.max_fanout = std::max(in("-initial_place_max_fanout"), 0);
-  if (flag("-skip_io")) ipv.max_iter = 0;
-  if (flag("-incremental")) refuse("-incremental placement is outside this engine's path");
-  if (flag("-place_ios")) refuse("-place_ios (concurrent IO placement) is outside this engine's path");
-  if (flag("-timing_driven")) refuse("-timing_driven needs the design database's resizer");
-  bool skip_nesterov = flag("-skip_nesterov_place");
-  Opts o;
-  if (!skip_nesterov) o = nesterov_opts(keys, flags, vars);
-  if (o.routability) {
-    if (!router) refuse("-routability_driven / -timing_driven need the design database");
-    refuse("-routability_driven on the device is not built yet");
-  }
-  bool has_core_row = false;
-  for (auto &r : d.rows)
-    if (!r.pad) has_core_row = true;
-  if (!has_core_row) log.error("GPL", 130, "No rows defined in design. Use initialize_floorplan to add rows.");
-  Common c = placer_base_common(log, d, vars);
+// One run of the command: `global_placement` (src/run.rs:115-201) with `do_initial_place`
+// (:292-308) in `open`, the Nesterov loop stepped by `step`, and the report in `close`.
+struct Run {
+  RunResult res;
+  Engine &eng;
+  Design d;
+  Common c;
   std::vector<Base> bases;
-  bases.push_back(placer_base(log, d, c, -1, true));
-  for (auto &reg : d.regions)
-    for (int g : reg.groups) bases.push_back(placer_base(log, d, c, g, true));
-  if (bases[0].place_insts.empty()) {
-    log.warn("GPL", 123, "No placeable instances in the top-level region. Removing it.");
-    bases.erase(bases.begin());
-  }
-  auto t0 = std::chrono::steady_clock::now();
-  SolveFn solve = [&](const Csr &m, const std::vector<float> &rhs, std::vector<float> &x, int max_iters) {
-    Solve s = eng.solve(m, rhs, x, max_iters);
-    if (eng.failed()) throw std::runtime_error("device: " + std::string(cudaGetErrorString(eng.error().code)) + " in " + eng.error().where);
-    return s;
-  };
-  Ip ip = do_bicgstab_place(log, d, c, vars, ipv, solve);
-  auto t1 = std::chrono::steady_clock::now();
-  res.t_ip = std::chrono::duration<double>(t1 - t0).count();
-  res.insts = (int64_t)c.insts.size();
-  res.nets = (int64_t)c.nets.size();
-  res.pins = c.pins;
-  for (auto &b : bases) res.bases.push_back({b.group, (int32_t)b.place_insts.size(), (int32_t)b.fixed_insts.size(), (int32_t)b.dummies.size()});
-  if (skip_nesterov) {
-    res.outcome = GPL_OUTCOME_INITIALLY_PLACED;
-    for (int k : ip.place) {
-      int di = c.insts[k].db;
-      res.locations.push_back({di, ip.db_bbox[di].lx, ip.db_bbox[di].ly});
+  Ip ip;
+  std::unique_ptr<Placer> P;
+  NesterovLoop loop;
+  bool nesterov = false;
+  bool ended = false;
+  std::chrono::steady_clock::time_point t2;
+  explicit Run(Engine &e) : eng(e) {}
+
+  void open(const std::vector<std::string> &args, const gpl_router_t *router) {
+    Log &log = res.log;
+    std::map<std::string, std::string> keys;
+    std::vector<std::string> flags;
+    parse_key_args(log, args, keys, flags);
+    auto flag = [&](const char *f) { return std::find(flags.begin(), flags.end(), f) != flags.end(); };
+    if (flag("-place_ios")) {
+      if (flag("-skip_io")) log.error("GPL", 169, "-place_ios cannot be used with -skip_io placement.");
+      if (flag("-incremental")) log.error("GPL", 170, "-place_ios cannot be used with -incremental placement.");
+      if (flag("-skip_nesterov_place")) log.error("GPL", 182, "-place_ios cannot be used with -skip_nesterov_place placement.");
     }
-    return;
-  }
-  Placer P(eng);
-  P.o = o;
-  init_nesterov_place(log, d, c, ip, bases, P);
-  // the first HPWL (the reference HPWL's base) over the pins as the placer copied them
-  int64_t design_hpwl = 0;
-  for (auto &np : P.net_pins) {
-    int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
-    for (int p : np) {
-      lx = std::min(lx, P.gpins[p].cx);
-      ly = std::min(ly, P.gpins[p].cy);
-      ux = std::max(ux, P.gpins[p].cx);
-      uy = std::max(uy, P.gpins[p].cy);
+    auto in = [&](const char *k) -> int32_t {
+      auto it = keys.find(k);
+      if (it == keys.end()) return 0;
+      int32_t x;
+      if (!parse_i32(it->second, x)) refuse(std::string(k) + " " + it->second + ": not an integer");
+      return x;
+    };
+    Vars vars;
+    vars.pad_left = in("-pad_left");
+    vars.pad_right = in("-pad_right");
+    vars.skip_io = flag("-skip_io");
+    vars.place_ios = flag("-place_ios");
+    vars.disable_pin_density_adjust = flag("-disable_pin_density_adjust");
+    IpVars ipv;
+    ipv.force_center = flag("-force_center_initial_place");
+    if (flag("-skip_initial_place")) ipv.max_iter = 0;
+    if (keys.count("-initial_place_max_iter")) ipv.max_iter = std::max(in("-initial_place_max_iter"), 0);
+    if (keys.count("-initial_place_max_fanout")) ipv.max_fanout = std::max(in("-initial_place_max_fanout"), 0);
+    if (flag("-skip_io")) ipv.max_iter = 0;
+    if (flag("-incremental")) refuse("-incremental placement is outside this engine's path");
+    if (flag("-place_ios")) refuse("-place_ios (concurrent IO placement) is outside this engine's path");
+    if (flag("-timing_driven")) refuse("-timing_driven needs the design database's resizer");
+    bool skip_nesterov = flag("-skip_nesterov_place");
+    Opts o;
+    if (!skip_nesterov) o = nesterov_opts(keys, flags, vars);
+    if (o.routability) {
+      if (!router) refuse("-routability_driven / -timing_driven need the design database");
+      refuse("-routability_driven on the device is not built yet");
     }
-    if (ux >= lx) design_hpwl += ((int64_t)ux - lx) + ((int64_t)uy - ly);
+    bool has_core_row = false;
+    for (auto &r : d.rows)
+      if (!r.pad) has_core_row = true;
+    if (!has_core_row) log.error("GPL", 130, "No rows defined in design. Use initialize_floorplan to add rows.");
+    c = placer_base_common(log, d, vars);
+    bases.push_back(placer_base(log, d, c, -1, true));
+    for (auto &reg : d.regions)
+      for (int g : reg.groups) bases.push_back(placer_base(log, d, c, g, true));
+    if (bases[0].place_insts.empty()) {
+      log.warn("GPL", 123, "No placeable instances in the top-level region. Removing it.");
+      bases.erase(bases.begin());
+    }
+    progress("placer built: %zu instances, %zu nets, %zu bases", c.insts.size(), c.nets.size(), bases.size());
+    auto t0 = std::chrono::steady_clock::now();
+    Engine &E = eng;
+    SolveFn solve = [&E](const Csr &m, const std::vector<float> &rhs, std::vector<float> &x, int max_iters) {
+      Solve s = E.solve(m, rhs, x, max_iters);
+      if (E.failed()) throw std::runtime_error("device: " + std::string(cudaGetErrorString(E.error().code)) + " in " + E.error().where);
+      return s;
+    };
+    ip = do_bicgstab_place(log, d, c, vars, ipv, solve);
+    auto t1 = std::chrono::steady_clock::now();
+    res.t_ip = std::chrono::duration<double>(t1 - t0).count();
+    res.insts = (int64_t)c.insts.size();
+    res.nets = (int64_t)c.nets.size();
+    res.pins = c.pins;
+    for (auto &b : bases) res.bases.push_back({b.group, (int32_t)b.place_insts.size(), (int32_t)b.fixed_insts.size(), (int32_t)b.dummies.size()});
+    if (skip_nesterov) {
+      res.outcome = GPL_OUTCOME_INITIALLY_PLACED;
+      for (int k : ip.place) {
+        int di = c.insts[k].db;
+        res.locations.push_back({di, ip.db_bbox[di].lx, ip.db_bbox[di].ly});
+      }
+      return;
+    }
+    P = std::make_unique<Placer>(eng);
+    P->o = o;
+    init_nesterov_place(log, d, c, ip, bases, *P);
+    // the first HPWL (the reference HPWL's base) over the pins as the placer copied them
+    int64_t design_hpwl = 0;
+    for (auto &np : P->net_pins) {
+      int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+      for (int p : np) {
+        lx = std::min(lx, P->gpins[p].cx);
+        ly = std::min(ly, P->gpins[p].cy);
+        ux = std::max(ux, P->gpins[p].cx);
+        uy = std::max(uy, P->gpins[p].cy);
+      }
+      if (ux >= lx) design_hpwl += ((int64_t)ux - lx) + ((int64_t)uy - ly);
+    }
+    t2 = std::chrono::steady_clock::now();
+    progress("nesterov set up: %zu cells, %zu regions", P->gcells.size(), P->nbs.size());
+    eng.upload(engine_setup(*P));
+    P->device_check();
+    progress("uploaded");
+    P->reference_hpwl = derived_reference_hpwl(o.reference_hpwl, design_hpwl);
+    P->np_init(log);
+    progress("nesterov init done");
+    loop.begin(log, *P);
+    nesterov = true;
   }
-  auto t2 = std::chrono::steady_clock::now();
-  eng.upload(engine_setup(P));
-  P.device_check();
-  P.reference_hpwl = derived_reference_hpwl(o.reference_hpwl, design_hpwl);
-  P.np_init(log);
-  int iter = resume_nesterov_place(log, d, P);
-  res.locations = placed_locations(c, P);
-  auto t3 = std::chrono::steady_clock::now();
-  res.t_np = std::chrono::duration<double>(t3 - t2).count();
-  res.iterations = iter;
-  res.final_hpwl = P.hpwl();
-  res.final_overflow = P.average_overflow_unscaled;
-  res.trials = P.trials;
-}
+  bool step() {
+    if (!nesterov || ended) return false;
+    bool more = loop.step(res.log, d, *P);
+    if (!more) ended = true;
+    return more;
+  }
+  void close() {
+    if (!nesterov) return;
+    while (step()) {
+    }
+    int iter = loop.end(res.log, d, *P);
+    res.locations = placed_locations(c, *P);
+    auto t3 = std::chrono::steady_clock::now();
+    res.t_np = std::chrono::duration<double>(t3 - t2).count();
+    res.iterations = iter;
+    res.final_hpwl = P->hpwl();
+    res.final_overflow = P->average_overflow_unscaled;
+    res.trials = P->trials;
+  }
+};
 
 }  // namespace gpl
 
@@ -1775,6 +1820,64 @@ static char *dupstr(const std::string &s) {
   std::memcpy(p, s.c_str(), s.size() + 1);
   return p;
 }
+
+static void fill_result(RunResult &r, gpl_result_t *out) {
+  std::memset(out, 0, sizeof *out);
+  out->status = r.status;
+  out->outcome = r.outcome;
+  std::snprintf(out->code, sizeof out->code, "%s", r.code.c_str());
+  out->reason = dupstr(r.reason);
+  std::string lines, trace;
+  for (auto &l : r.log.lines) lines += l + "\n";
+  for (auto &l : r.log.trace) trace += l + "\n";
+  out->lines = dupstr(lines);
+  out->trace = dupstr(trace);
+  out->insts = r.insts;
+  out->nets = r.nets;
+  out->pins = r.pins;
+  out->iterations = r.iterations;
+  out->n_bases = (int32_t)r.bases.size();
+  out->bases = (int32_t *)malloc(sizeof(int32_t) * 4 * (r.bases.size() + 1));
+  for (size_t b = 0; b < r.bases.size(); b++)
+    for (int q = 0; q < 4; q++) out->bases[4 * b + q] = r.bases[b][q];
+  out->n_locations = (int64_t)r.locations.size();
+  out->locations = (int32_t *)malloc(sizeof(int32_t) * 3 * (r.locations.size() + 1));
+  for (size_t k = 0; k < r.locations.size(); k++)
+    for (int q = 0; q < 3; q++) out->locations[3 * k + q] = r.locations[k][q];
+  out->final_hpwl = r.final_hpwl;
+  out->final_overflow = r.final_overflow;
+  out->trials = r.trials;
+  out->seconds_initial_place = r.t_ip;
+  out->seconds_nesterov = r.t_np;
+  out->h2d_bytes = r.h2d;
+  out->d2h_bytes = r.d2h;
+  out->launches = r.launches;
+}
+
+// Runs `f` and turns a stop into the result's status: the reference's error, a refusal, or a
+// device fault.
+template <class F>
+static void guarded(RunResult &r, F f) {
+  try {
+    f();
+  } catch (const StopEx &s) {
+    if (s.error) {
+      r.status = GPL_ERROR;
+      r.code = sfmt("%s-%04d", s.tool.c_str(), s.id);
+    } else {
+      r.status = GPL_REFUSED;
+      r.reason = s.why;
+    }
+  } catch (const std::exception &e) {
+    r.status = GPL_DEVICE_FAULT;
+    r.reason = e.what();
+  }
+}
+
+struct gpl_session {
+  gpl_ctx *ctx;
+  std::unique_ptr<Run> run;
+};
 
 extern "C" {
 
@@ -1808,54 +1911,98 @@ int gpl_set_option(gpl_ctx *c, const char *name, const char *value) {
   return -1;
 }
 
+static void reset_counters(Engine &e) {
+  e.launches = 0;
+  e.h2d_bytes = 0;
+  e.d2h_bytes = 0;
+  e.trials = 0;
+}
+
 int gpl_global_placement(gpl_ctx *ctx, const gpl_design_t *cd, int argc, const char *const *argv, const gpl_router_t *router, gpl_result_t *out) {
-  RunResult r;
-  r.log.trace_on = ctx->trace;
   ctx->eng->set_poisson_mode(ctx->poisson_mode);
-  try {
-    Design d = design_from_c(cd);
-    std::vector<std::string> args(argv, argv + argc);
-    global_placement(r, *ctx->eng, d, args, router);
-  } catch (const StopEx &s) {
-    if (s.error) {
-      r.status = GPL_ERROR;
-      r.code = sfmt("%s-%04d", s.tool.c_str(), s.id);
-    } else {
-      r.status = GPL_REFUSED;
-      r.reason = s.why;
-    }
-  } catch (const std::exception &e) {
-    r.status = GPL_DEVICE_FAULT;
-    r.reason = e.what();
-  }
+  reset_counters(*ctx->eng);
+  Run run(*ctx->eng);
+  run.res.log.trace_on = ctx->trace;
+  guarded(run.res, [&] {
+    run.d = design_from_c(cd);
+    run.open(std::vector<std::string>(argv, argv + argc), router);
+    run.close();
+  });
+  run.res.h2d = ctx->eng->h2d_bytes + run.res.locations.size() * 0;
+  run.res.d2h = ctx->eng->d2h_bytes;
+  run.res.launches = ctx->eng->launches;
   ctx->eng->release();
-  std::memset(out, 0, sizeof *out);
-  out->status = r.status;
-  out->outcome = r.outcome;
-  std::snprintf(out->code, sizeof out->code, "%s", r.code.c_str());
-  out->reason = dupstr(r.reason);
-  std::string lines, trace;
-  for (auto &l : r.log.lines) lines += l + "\n";
-  for (auto &l : r.log.trace) trace += l + "\n";
-  out->lines = dupstr(lines);
-  out->trace = dupstr(trace);
-  out->insts = r.insts;
-  out->nets = r.nets;
-  out->pins = r.pins;
-  out->iterations = r.iterations;
-  out->n_bases = (int32_t)r.bases.size();
-  out->bases = (int32_t *)malloc(sizeof(int32_t) * 4 * (r.bases.size() + 1));
-  for (size_t b = 0; b < r.bases.size(); b++)
-    for (int q = 0; q < 4; q++) out->bases[4 * b + q] = r.bases[b][q];
-  out->n_locations = (int64_t)r.locations.size();
-  out->locations = (int32_t *)malloc(sizeof(int32_t) * 3 * (r.locations.size() + 1));
-  for (size_t k = 0; k < r.locations.size(); k++)
-    for (int q = 0; q < 3; q++) out->locations[3 * k + q] = r.locations[k][q];
-  out->final_hpwl = r.final_hpwl;
-  out->final_overflow = r.final_overflow;
-  out->trials = r.trials;
-  out->seconds_initial_place = r.t_ip;
-  out->seconds_nesterov = r.t_np;
+  fill_result(run.res, out);
+  return out->status;
+}
+
+gpl_session *gpl_session_open(gpl_ctx *ctx, const gpl_design_t *cd, int argc, const char *const *argv, const gpl_router_t *router) {
+  ctx->eng->set_poisson_mode(ctx->poisson_mode);
+  reset_counters(*ctx->eng);
+  auto *s = new gpl_session{ctx, std::make_unique<Run>(*ctx->eng)};
+  s->run->res.log.trace_on = ctx->trace;
+  guarded(s->run->res, [&] {
+    s->run->d = design_from_c(cd);
+    s->run->open(std::vector<std::string>(argv, argv + argc), router);
+  });
+  return s;
+}
+
+int gpl_session_iterate(gpl_session *s, int n, int *done) {
+  int k = 0;
+  if (s->run->res.status != GPL_PLACED) {
+    *done = 1;
+    return 0;
+  }
+  guarded(s->run->res, [&] {
+    while (k < n && s->run->step()) k++;
+  });
+  *done = (s->run->ended || !s->run->nesterov || s->run->res.status != GPL_PLACED) ? 1 : 0;
+  return k;
+}
+
+int gpl_session_set_option(gpl_session *s, const char *name, const char *value) {
+  std::string n = name, v = value;
+  if (n == "poisson") {
+    int mode = v == "fp32" ? 0 : v == "mixed" ? 1 : -1;
+    if (mode < 0) return -1;
+    if (!s->run->nesterov) return -1;
+    s->ctx->eng->rebuild_poisson(mode);
+    return s->ctx->eng->failed() ? -1 : 0;
+  }
+  if (n == "profile") {
+    s->ctx->eng->set_profile(v == "1");
+    return 0;
+  }
+  return -1;
+}
+
+int gpl_session_profile(gpl_session *s, double *ms, int64_t *launches, int cap) {
+  return s->ctx->eng->profile_read(ms, launches, cap);
+}
+
+void *gpl_session_stream(gpl_session *s) { return (void *)s->ctx->eng->stream(); }
+
+void gpl_session_counters(gpl_session *s, int64_t out[4]) {
+  out[0] = s->ctx->eng->launches;
+  out[1] = s->ctx->eng->h2d_bytes;
+  out[2] = s->ctx->eng->d2h_bytes;
+  out[3] = s->run->P ? (int64_t)s->run->P->gcell_of_dev.size() : 0;
+}
+
+void gpl_session_discard(gpl_session *s) {
+  s->ctx->eng->release();
+  delete s;
+}
+
+int gpl_session_close(gpl_session *s, gpl_result_t *out) {
+  if (s->run->res.status == GPL_PLACED) guarded(s->run->res, [&] { s->run->close(); });
+  s->run->res.h2d = s->ctx->eng->h2d_bytes;
+  s->run->res.d2h = s->ctx->eng->d2h_bytes;
+  s->run->res.launches = s->ctx->eng->launches;
+  s->ctx->eng->release();
+  fill_result(s->run->res, out);
+  delete s;
   return out->status;
 }
 

@@ -891,14 +891,19 @@ Ip do_bicgstab_place(Log &log, const Design &d, Common &c, const Vars &v, const 
   Ip ip = make_pins(d, c, v);
   place_insts_initial_positions(log, d, c, ip, vars);
   System sx, sy;
+  progress("initial placement: %zu pins, %zu nets", ip.pins.size(), ip.net_pins.size());
   for (int iter = 1; iter <= vars.max_iter; iter++) {
     update_pin_info(ip);
     create_sparse_matrix(c, ip, vars, sx, sy);
+    progress("  round %d: B2B assembled (%zu + %zu triplets)", iter, sx.triplets.size(), sy.triplets.size());
     int64_t n = (int64_t)ip.place.size();
     Csr mx = Csr::from_triplets(n, sx.triplets);
+    progress("  round %d: CSR x built", iter);
     Solve ex = solve(mx, sx.rhs, sx.x, vars.max_solver_iter);
+    progress("  round %d: x solved (%d iterations)", iter, ex.iterations);
     Csr my = Csr::from_triplets(n, sy.triplets);
     Solve ey = solve(my, sy.rhs, sy.x, vars.max_solver_iter);
+    progress("  round %d: y solved (%d iterations)", iter, ey.iterations);
     uint32_t exb, eyb;
     std::memcpy(&exb, &ex.error, 4);
     std::memcpy(&eyb, &ey.error, 4);
@@ -1113,4 +1118,22 @@ static double unit_normal(Mt19937 &eng) {
 // `normal` (src/normal.rs:131-133).
 double normal(Mt19937 &eng, double mean, double sigma) { return unit_normal(eng) * sigma + mean; }
 
+}  // namespace gpl
+
+#include <chrono>
+#include <cstdlib>
+namespace gpl {
+void progress(const char *fmt, ...) {
+  static const bool on = std::getenv("GPL_LOG") != nullptr;
+  static const auto t0 = std::chrono::steady_clock::now();
+  if (!on) return;
+  double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  std::fprintf(stderr, "[gpl %9.3f] %s\n", s, buf);
+  std::fflush(stderr);
+}
 }  // namespace gpl

@@ -72,5 +72,7 @@ __nv_bfloat16 *poisson_split_input(PoissonPlan *p, int *ld);
 // Fill the split-BF16 operand from a float density (when no bin finalize wrote it).
 cudaError_t poisson_split_density(PoissonPlan *p, const float *density, cudaStream_t s);
 size_t poisson_workspace_bytes(int nx, int ny);
+// Kernel launches one poisson_solve makes.
+int poisson_launches(const PoissonPlan *p);
 
 }  // namespace gpl

@@ -253,6 +253,8 @@ cudaError_t poisson_split_density(PoissonPlan *p, const float *density, cudaStre
   return cudaGetLastError();
 }
 
+int poisson_launches(const PoissonPlan *p) { return p->mode == 0 ? 5 : tc_launches(p); }
+
 cudaError_t poisson_solve(PoissonPlan *p, const float *density, float *field_x, float *field_y, cudaStream_t s) {
   if (p->mode != 0) return tc_solve(p, field_x, field_y, s);
   int nx = p->nx, ny = p->ny;

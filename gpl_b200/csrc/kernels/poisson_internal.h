@@ -46,5 +46,6 @@ struct PoissonPlan {
 cudaError_t tc_plan_init(PoissonPlan *p, const BasisHost &b);
 void tc_plan_free(PoissonPlan *p);
 cudaError_t tc_solve(PoissonPlan *p, float *field_x, float *field_y, cudaStream_t s);
+int tc_launches(const PoissonPlan *p);
 
 }  // namespace gpl

@@ -6,5 +6,6 @@ namespace gpl {
 cudaError_t tc_plan_init(PoissonPlan *, const BasisHost &) { return cudaErrorNotSupported; }
 void tc_plan_free(PoissonPlan *) {}
 cudaError_t tc_solve(PoissonPlan *, float *, float *, cudaStream_t) { return cudaErrorNotSupported; }
+int tc_launches(const PoissonPlan *) { return 0; }
 
 }  // namespace gpl

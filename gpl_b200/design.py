@@ -104,11 +104,11 @@ class Design:
             self.iterm_has_shape = np.ones(n_iterms, np.uint8)
         if self.iterm_order is None:
             # position among the instance's terminals, in net order
-            order = np.zeros(n_iterms, np.int32)
-            seen = {}
-            for t, i in enumerate(self.iterm_inst.tolist()):
-                order[t] = seen.get(i, 0)
-                seen[i] = order[t] + 1
+            inst = np.asarray(self.iterm_inst, np.int64)
+            srt = np.argsort(inst, kind="stable")
+            first = np.searchsorted(inst[srt], inst[srt], side="left")
+            order = np.empty(n_iterms, np.int32)
+            order[srt] = (np.arange(n_iterms) - first).astype(np.int32)
             self.iterm_order = order
         if self.inst_signal_pins is None:
             self.inst_signal_pins = np.bincount(self.iterm_inst, minlength=n_insts).astype(np.int32)
@@ -207,7 +207,7 @@ class gpl_result_t(C.Structure):
         ("iterations", C.c_int32), ("n_bases", C.c_int32), ("bases", _P(C.c_int32)),
         ("n_locations", C.c_int64), ("locations", _P(C.c_int32)), ("final_hpwl", C.c_int64),
         ("final_overflow", C.c_float), ("trials", C.c_int64), ("seconds_initial_place", C.c_double),
-        ("seconds_nesterov", C.c_double),
+        ("seconds_nesterov", C.c_double), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64), ("launches", C.c_int64),
     ]
 
 
@@ -234,5 +234,6 @@ def result_to_dict(r: gpl_result_t) -> dict:
         "final_hpwl": r.final_hpwl, "final_overflow": r.final_overflow, "trials": r.trials,
         "seconds_initial_place": r.seconds_initial_place, "seconds_nesterov": r.seconds_nesterov,
         "outcome": "placed" if r.outcome == 0 else "initially_placed",
+        "h2d_bytes": r.h2d_bytes, "d2h_bytes": r.d2h_bytes, "launches": r.launches,
     }
     return out

@@ -108,3 +108,78 @@ class SyntheticRouter:
 
     def __del__(self):
         self.close()
+
+
+def _session_lib():
+    L = lib()
+    if not getattr(L, "_session_ready", False):
+        L.gpl_session_open.restype = C.c_void_p
+        L.gpl_session_open.argtypes = [C.c_void_p, C.POINTER(gpl_design_t), C.c_int, C.POINTER(C.c_char_p), C.c_void_p]
+        L.gpl_session_iterate.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+        L.gpl_session_set_option.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p]
+        L.gpl_session_profile.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64), C.c_int]
+        L.gpl_session_stream.restype = C.c_void_p
+        L.gpl_session_stream.argtypes = [C.c_void_p]
+        L.gpl_session_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        L.gpl_session_close.argtypes = [C.c_void_p, C.POINTER(gpl_result_t)]
+        L._session_ready = True
+    return L
+
+
+PHASES = ("scatter", "bin_finalize", "density_solve", "wa", "gradients", "hpwl")
+
+
+class Session:
+    """The command with its Nesterov loop stepped by the caller (`gpl_session_*`)."""
+
+    def __init__(self, placer: "Placer", design: Design, args, router=None):
+        L = _session_lib()
+        self._cd = design.c_struct()
+        argv = (C.c_char_p * max(len(args), 1))(*[a.encode() for a in args])
+        self._h = L.gpl_session_open(placer._ctx, C.byref(self._cd), len(args), argv, router)
+        self.done = False
+
+    def iterate(self, n) -> int:
+        d = C.c_int()
+        k = _session_lib().gpl_session_iterate(self._h, n, C.byref(d))
+        self.done = bool(d.value)
+        return k
+
+    def set_option(self, name, value):
+        if _session_lib().gpl_session_set_option(self._h, name.encode(), str(value).encode()) != 0:
+            raise RuntimeError(f"session option {name}={value} failed")
+
+    def profile(self):
+        ms = (C.c_double * 8)()
+        n = (C.c_int64 * 8)()
+        k = _session_lib().gpl_session_profile(self._h, ms, n, 8)
+        return {PHASES[i]: (ms[i], n[i]) for i in range(k)}
+
+    def counters(self):
+        out = (C.c_int64 * 4)()
+        _session_lib().gpl_session_counters(self._h, out)
+        return {"launches": out[0], "h2d_bytes": out[1], "d2h_bytes": out[2], "cells": out[3]}
+
+    @property
+    def stream(self):
+        return _session_lib().gpl_session_stream(self._h)
+
+    def close(self) -> dict:
+        res = gpl_result_t()
+        _session_lib().gpl_session_close(self._h, C.byref(res))
+        self._h = None
+        try:
+            return result_to_dict(res)
+        finally:
+            lib().gpl_result_free(C.byref(res))
+
+
+def _discard(self):
+    """Drops the session where it stands (`gpl_session_discard`)."""
+    L = _session_lib()
+    L.gpl_session_discard.argtypes = [C.c_void_p]
+    L.gpl_session_discard(self._h)
+    self._h = None
+
+
+Session.discard = _discard

@@ -141,6 +141,9 @@ typedef struct gpl_result {
   int64_t trials;        /* back-tracking trials run */
   double seconds_initial_place;
   double seconds_nesterov;
+  int64_t h2d_bytes;     /* host-to-device bytes the run copied */
+  int64_t d2h_bytes;     /* device-to-host bytes the run copied */
+  int64_t launches;      /* kernel launches the run made */
 } gpl_result_t;
 
 typedef struct gpl_ctx gpl_ctx;
@@ -163,6 +166,31 @@ int gpl_global_placement(gpl_ctx *ctx, const gpl_design_t *design, int argc,
                          const char *const *argv, const gpl_router_t *router,
                          gpl_result_t *out);
 void gpl_result_free(gpl_result_t *out);
+
+/* The same command with its Nesterov loop stepped by the caller: `open` is `run::global_placement`
+ * up to the loop (construction, `do_initial_place`, `init_nesterov_place`, `init_nesterov_loop`:
+ * src/run.rs:115-159, src/nesterov.rs:4123-4127); `iterate` runs up to n iterations of
+ * `resume_nesterov_place`'s loop (src/nesterov.rs:4478-4575) and sets *done when the loop has
+ * ended; `close` finishes it and writes the result as gpl_global_placement does. A stop in
+ * `open` or `iterate` is reported by `close`. */
+typedef struct gpl_session gpl_session;
+gpl_session *gpl_session_open(gpl_ctx *ctx, const gpl_design_t *design, int argc,
+                              const char *const *argv, const gpl_router_t *router);
+int gpl_session_iterate(gpl_session *s, int n, int *done);
+/* "poisson" = "mixed" | "fp32" (solvers rebuilt, the field recomputed); "profile" = "0" | "1"
+ * (per-phase device time from CUDA events). No reference counterpart. */
+int gpl_session_set_option(gpl_session *s, const char *name, const char *value);
+/* Per-phase device milliseconds and launch counts since "profile" was set: scatter, bin
+ * finalize, density solve, WA, gradients, HPWL. Returns the number of phases written. */
+int gpl_session_profile(gpl_session *s, double *ms, int64_t *launches, int cap);
+/* Kernel launches, host-to-device and device-to-host bytes since the session opened, and the
+ * Nesterov cells (instances and fillers) on the device (4 int64). */
+void gpl_session_counters(gpl_session *s, int64_t out[4]);
+/* The session's CUDA stream (cudaStream_t), for timing with events on it. */
+void *gpl_session_stream(gpl_session *s);
+int gpl_session_close(gpl_session *s, gpl_result_t *out);
+/* Drops a session where it stands: no loop to the end, no result. */
+void gpl_session_discard(gpl_session *s);
 
 /* A stand-in for the database's router (src/db_router.rs:260-368): a uniform tile grid over
  * the die, the given pitches, every tile with `capacity` and no reduction, and each net's

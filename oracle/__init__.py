@@ -3,4 +3,4 @@
 Only the tests, `__graft_entry__.smoke()` and `bench.py`'s CPU-baseline leg load it, as the
 checker; the engine never does.
 """
-from .oracle_py import lib, build, global_placement  # noqa: F401
+from .oracle_py import Session, build, global_placement, lib  # noqa: F401

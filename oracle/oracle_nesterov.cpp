@@ -2047,107 +2047,115 @@ static Nesterov init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip
   return np;
 }
 
-// `resume_nesterov_place` (src/nesterov.rs:4440-4610), from iteration 0.
-static int resume_nesterov_place(Log &log, const Design &d, Nesterov &np, Routability *route) {
-  log.info("GPL", 84, "---- Execute Nesterov Global Placement.");
-  if (np.num_region_diverged > 0) log.error("GPL", np.diverge_code, np.diverge_msg);
+// `resume_nesterov_place` (src/nesterov.rs:4440-4610) from iteration 0: its prologue, one
+// pass of the loop at a time, its epilogue.
+struct OracleLoop {
   int64_t original_area = 0;
-  for (auto &nb : np.nbs) {
-    nb.max_phi_coef_changed = false;
-    nb.min_sum_overflow = 1e30f;
-    nb.hpwl_with_min_sum_overflow = 1e30f;
-    nb.is_converged = false;
-    original_area += nesterov_insts_area(nb);
-  }
   LoopSnapshots snaps;
   int route_iters = 0, route_reverts = 0;
   float cur_a = 1.0f;
   int iter = 0;
-  while (iter < np.max_iter) {
-    float prev_a = cur_a;
-    cur_a = (float)((1.0 + std::sqrt(4.0 * (double)prev_a * (double)prev_a + 1.0)) * 0.5);
-    float coeff = (float)(((double)prev_a - 1.0) / (double)cur_a);
-    np.do_back_tracking(coeff);
-    for (size_t b = 0; b < np.nbs.size(); b++) np.nesterov_adjust_phi((int)b);
-    if (np.num_region_diverged > 0) break;
-    np.np_update_next_iter(log, d, iter);
-    bool routability = np.o.routability;
-    bool routability_gpl_iter = snaps.route_saved && np.average_overflow_unscaled > np.o.routability_end_overflow;
-    if (routability_gpl_iter) {
-      route_iters++;
-      np.max_iter++;
+  bool done = false;
+  void begin(Log &log, Nesterov &np) {
+    log.info("GPL", 84, "---- Execute Nesterov Global Placement.");
+    if (np.num_region_diverged > 0) log.error("GPL", np.diverge_code, np.diverge_msg);
+    for (auto &nb : np.nbs) {
+      nb.max_phi_coef_changed = false;
+      nb.min_sum_overflow = 1e30f;
+      nb.hpwl_with_min_sum_overflow = 1e30f;
+      nb.is_converged = false;
+      original_area += nesterov_insts_area(nb);
     }
-    DivergeAction act = np.np_is_diverged(log, snaps, cur_a, route);
-    if (act == DivergeAction::Stop) break;
-    if (act == DivergeAction::Resume) {
-      iter++;
-      continue;
-    }
-    if (routability && !snaps.route_saved && np.o.routability_snapshot_overflow >= np.average_overflow_unscaled) {
-      snaps.route_coef[0] = np.wl_coef_x;
-      snaps.route_coef[1] = np.wl_coef_y;
-      snaps.route_a = cur_a;
-      snaps.route_saved = true;
-      for (size_t b = 0; b < np.nbs.size(); b++) np.save_snapshot((int)b);
-      log.info("GPL", 38, sfmt("Routability snapshot saved at iter = %d", iter + 1));
-      int64_t h = np.hpwl();
-      log.report(sfmt("%9d | %8.4f | %s | %-8s | %-9s | %5s", iter, (double)np.average_overflow_unscaled, fmt_e((double)h / (double)d.dbu, 6, 13).c_str(), " ", " ", " "));
-    }
-    if (route) {
-      bool active = np.routability_need && np.average_overflow_unscaled <= np.o.routability_end_overflow;
-      bool settled = active && np.is_placement_settled();
-      int extra = 0;
-      auto [start, event] = settle_wait_step(np.routability_settle_wait_start_iter, iter, active, settled, extra);
-      np.routability_settle_wait_start_iter = start;
-      if (event == 1)
-        log.info("GPL", 99, sfmt("Routability end extended at iter = %d: overflow %.4f reached %.4f, but cells are still moving at %.0f%% of peak displacement (waiting for %.0f%%).", iter + 1, (double)np.average_overflow_unscaled, (double)np.o.routability_end_overflow, (double)(np.worst_settle_ratio() * 100.0f), (double)(SETTLE_FRACTION * 100.0f)));
-      else if (event == 2)
-        log.info("GPL", 103, sfmt("Routability end extension finished at iter = %d after %d extra iterations: overflow %.4f, cells moving at %.0f%% of peak displacement.", iter + 1, extra, (double)np.average_overflow_unscaled, (double)(np.worst_settle_ratio() * 100.0f)));
-      if (settled) {
-        np.nbs[0].reprint_header = true;
-        route_reverts++;
-        auto [need, revert_init] = np.routability(log, d, *route, route_reverts);
-        np.routability_need = need;
-        np.min_hpwl = INT64_MAX;
-        np.is_min_hpwl = false;
-        if (need || revert_init) {
-          cur_a = snaps.route_a;
-          np.wl_coef_x = snaps.route_coef[0];
-          np.wl_coef_y = snaps.route_coef[1];
-          np.update_wirelength_force_wa();
-          for (size_t b = 0; b < np.nbs.size(); b++) {
-            np.revert_to_snapshot((int)b);
-            np.reset_min_sum_overflow((int)b);
-          }
-        }
-        if (need && revert_init) log.info("GPL", 87, "Routability end iteration: increase inflation and revert back to snapshot.");
-        if (!need && revert_init) log.info("GPL", 89, "Routability finished. Reverting to minimal observed routing congestion, could not reach target.");
-        if (!need && !revert_init) log.info("GPL", 90, "Routability finished. Target routing congestion achieved succesfully.");
-      }
-    }
-    int converged = 0;
-    for (size_t b = 0; b < np.nbs.size(); b++) converged += np.check_convergence(log, d, (int)b, iter, route, route_iters) ? 1 : 0;
-    if (converged == (int)np.nbs.size()) break;
+  }
+  bool step(Log &log, const Design &d, Nesterov &np, Routability *route) {
+    if (done || iter >= np.max_iter) return !(done = true);
+  float prev_a = cur_a;
+  cur_a = (float)((1.0 + std::sqrt(4.0 * (double)prev_a * (double)prev_a + 1.0)) * 0.5);
+  float coeff = (float)(((double)prev_a - 1.0) / (double)cur_a);
+  np.do_back_tracking(coeff);
+  for (size_t b = 0; b < np.nbs.size(); b++) np.nesterov_adjust_phi((int)b);
+  if (np.num_region_diverged > 0) return !(done = true);
+  np.np_update_next_iter(log, d, iter);
+  bool routability = np.o.routability;
+  bool routability_gpl_iter = snaps.route_saved && np.average_overflow_unscaled > np.o.routability_end_overflow;
+  if (routability_gpl_iter) {
+    route_iters++;
+    np.max_iter++;
+  }
+  DivergeAction act = np.np_is_diverged(log, snaps, cur_a, route);
+  if (act == DivergeAction::Stop) return !(done = true);
+  if (act == DivergeAction::Resume) {
     iter++;
+    return true;
   }
-  if (max_iter_takes_min_hpwl_snapshot(iter, np.max_iter, np.o.disable_revert_if_diverge, snaps, np.diverge_snapshot_overflow, np.average_overflow_unscaled, np.hpwl())) {
-    log.warn("GPL", 121, "Reached the maximum number of iterations, reverting to snapshot with min hpwl.");
-    np.revert_to_diverge_snapshot(log, snaps);
+  if (routability && !snaps.route_saved && np.o.routability_snapshot_overflow >= np.average_overflow_unscaled) {
+    snaps.route_coef[0] = np.wl_coef_x;
+    snaps.route_coef[1] = np.wl_coef_y;
+    snaps.route_a = cur_a;
+    snaps.route_saved = true;
+    for (size_t b = 0; b < np.nbs.size(); b++) np.save_snapshot((int)b);
+    log.info("GPL", 38, sfmt("Routability snapshot saved at iter = %d", iter + 1));
+    int64_t h = np.hpwl();
+    log.report(sfmt("%9d | %8.4f | %s | %-8s | %-9s | %5s", iter, (double)np.average_overflow_unscaled, fmt_e((double)h / (double)d.dbu, 6, 13).c_str(), " ", " ", " "));
   }
-  if (iter >= np.max_iter) log.warn("GPL", 1010, sfmt("GPL reached the maximum number of iterations for nesterov %d. Placement may have failed to converge.", np.max_iter));
-  if (route) log.info("GPL", 1011, sfmt("Original area (um^2): %.2f", dbu_area(d, (double)original_area)));
   if (route) {
-    int64_t inflation = route->rb.total_inflation();
-    float pct = (float)(100.0 * (double)inflation / (double)original_area);
-    log.info("GPL", 1012, sfmt("Total routability artificial inflation: %.2f (%+.2f%%)", dbu_area(d, (double)inflation), (double)pct));
+    bool active = np.routability_need && np.average_overflow_unscaled <= np.o.routability_end_overflow;
+    bool settled = active && np.is_placement_settled();
+    int extra = 0;
+    auto [start, event] = settle_wait_step(np.routability_settle_wait_start_iter, iter, active, settled, extra);
+    np.routability_settle_wait_start_iter = start;
+    if (event == 1)
+      log.info("GPL", 99, sfmt("Routability end extended at iter = %d: overflow %.4f reached %.4f, but cells are still moving at %.0f%% of peak displacement (waiting for %.0f%%).", iter + 1, (double)np.average_overflow_unscaled, (double)np.o.routability_end_overflow, (double)(np.worst_settle_ratio() * 100.0f), (double)(SETTLE_FRACTION * 100.0f)));
+    else if (event == 2)
+      log.info("GPL", 103, sfmt("Routability end extension finished at iter = %d after %d extra iterations: overflow %.4f, cells moving at %.0f%% of peak displacement.", iter + 1, extra, (double)np.average_overflow_unscaled, (double)(np.worst_settle_ratio() * 100.0f)));
+    if (settled) {
+      np.nbs[0].reprint_header = true;
+      route_reverts++;
+      auto [need, revert_init] = np.routability(log, d, *route, route_reverts);
+      np.routability_need = need;
+      np.min_hpwl = INT64_MAX;
+      np.is_min_hpwl = false;
+      if (need || revert_init) {
+        cur_a = snaps.route_a;
+        np.wl_coef_x = snaps.route_coef[0];
+        np.wl_coef_y = snaps.route_coef[1];
+        np.update_wirelength_force_wa();
+        for (size_t b = 0; b < np.nbs.size(); b++) {
+          np.revert_to_snapshot((int)b);
+          np.reset_min_sum_overflow((int)b);
+        }
+      }
+      if (need && revert_init) log.info("GPL", 87, "Routability end iteration: increase inflation and revert back to snapshot.");
+      if (!need && revert_init) log.info("GPL", 89, "Routability finished. Reverting to minimal observed routing congestion, could not reach target.");
+      if (!need && !revert_init) log.info("GPL", 90, "Routability finished. Target routing congestion achieved succesfully.");
+    }
   }
-  int64_t new_area = 0;
-  for (auto &nb : np.nbs) new_area += nesterov_insts_area(nb);
-  float diff = (float)(100.0 * (double)(new_area - original_area) / (double)original_area);
-  log.info("GPL", 1014, sfmt("Final placement area: %.2f (%+.2f%%)", dbu_area(d, (double)new_area), (double)diff));
-  if (np.num_region_diverged > 0) log.error("GPL", np.diverge_code, np.diverge_msg);
-  return iter;
-}
+  int converged = 0;
+  for (size_t b = 0; b < np.nbs.size(); b++) converged += np.check_convergence(log, d, (int)b, iter, route, route_iters) ? 1 : 0;
+  if (converged == (int)np.nbs.size()) return !(done = true);
+  iter++;
+    return true;
+  }
+  int end(Log &log, const Design &d, Nesterov &np, Routability *route) {
+    if (max_iter_takes_min_hpwl_snapshot(iter, np.max_iter, np.o.disable_revert_if_diverge, snaps, np.diverge_snapshot_overflow, np.average_overflow_unscaled, np.hpwl())) {
+      log.warn("GPL", 121, "Reached the maximum number of iterations, reverting to snapshot with min hpwl.");
+      np.revert_to_diverge_snapshot(log, snaps);
+    }
+    if (iter >= np.max_iter) log.warn("GPL", 1010, sfmt("GPL reached the maximum number of iterations for nesterov %d. Placement may have failed to converge.", np.max_iter));
+    if (route) log.info("GPL", 1011, sfmt("Original area (um^2): %.2f", dbu_area(d, (double)original_area)));
+    if (route) {
+      int64_t inflation = route->rb.total_inflation();
+      float pct = (float)(100.0 * (double)inflation / (double)original_area);
+      log.info("GPL", 1012, sfmt("Total routability artificial inflation: %.2f (%+.2f%%)", dbu_area(d, (double)inflation), (double)pct));
+    }
+    int64_t new_area = 0;
+    for (auto &nb : np.nbs) new_area += nesterov_insts_area(nb);
+    float diff = (float)(100.0 * (double)(new_area - original_area) / (double)original_area);
+    log.info("GPL", 1014, sfmt("Final placement area: %.2f (%+.2f%%)", dbu_area(d, (double)new_area), (double)diff));
+    if (np.num_region_diverged > 0) log.error("GPL", np.diverge_code, np.diverge_msg);
+    return iter;
+  }
+};
 
 // ---------------------------------------------------------------- run.rs
 static const char *KEYS[] = {"-bin_grid_count", "-density", "-init_density_penalty", "-init_wirelength_coef", "-min_phi_coef", "-max_phi_coef", "-overflow", "-reference_hpwl", "-initial_place_max_iter", "-initial_place_max_fanout", "-routability_check_overflow", "-routability_snapshot_overflow", "-routability_max_density", "-routability_target_rc_metric", "-routability_inflation_ratio_coef", "-routability_max_inflation_ratio", "-routability_min_congestion_for_inflation", "-routability_max_inflation_total", "-routability_net_weight_max", "-routability_congested_nets_percentage", "-routability_rc_coefficients", "-timing_driven_net_reweight_overflow", "-timing_driven_net_weight_max", "-timing_driven_nets_percentage", "-timing_driven_repair_tns_end_percent", "-keep_resize_below_overflow", "-virtual_cts_max_skew_fraction", "-random_seed", "-perturb_dist", "-pad_left", "-pad_right", nullptr};
@@ -2287,7 +2295,40 @@ static Opts nesterov_opts(const std::map<std::string, std::string> &keys, const 
 }
 
 // `global_placement` (src/run.rs:115-201) and `do_initial_place` (:292-308).
-static void global_placement(RunResult &res, const Design &d, const std::vector<std::string> &args, const gpl_router_t *router) {
+struct OracleRun {
+  RunResult res;
+  Design d;
+  Common c;
+  std::vector<Base> bases;
+  Ip ip;
+  Nesterov np;
+  std::unique_ptr<Routability> route;
+  OracleLoop loop;
+  bool nesterov = false, ended = false;
+  std::chrono::steady_clock::time_point t2;
+  void open(const std::vector<std::string> &args, const gpl_router_t *router);
+  bool step() {
+    if (!nesterov || ended) return false;
+    bool more = loop.step(res.log, d, np, route.get());
+    if (!more) ended = true;
+    return more;
+  }
+  void close() {
+    if (!nesterov) return;
+    while (step()) {
+    }
+    int iter = loop.end(res.log, d, np, route.get());
+    auto t3 = std::chrono::steady_clock::now();
+    res.t_np = std::chrono::duration<double>(t3 - t2).count();
+    res.iterations = iter;
+    res.locations = np.placed_locations(c);
+    res.final_hpwl = np.hpwl();
+    res.final_overflow = np.average_overflow_unscaled;
+    res.trials = np.trials;
+  }
+};
+
+void OracleRun::open(const std::vector<std::string> &args, const gpl_router_t *router) {
   Log &log = res.log;
   std::map<std::string, std::string> keys;
   std::vector<std::string> flags;
@@ -2328,8 +2369,7 @@ static void global_placement(RunResult &res, const Design &d, const std::vector<
   for (auto &r : d.rows)
     if (!r.pad) has_core_row = true;
   if (!has_core_row) log.error("GPL", 130, "No rows defined in design. Use initialize_floorplan to add rows.");
-  Common c = placer_base_common(log, d, vars);
-  std::vector<Base> bases;
+  c = placer_base_common(log, d, vars);
   bases.push_back(placer_base(log, d, c, -1, true));
   for (auto &reg : d.regions)
     for (int g : reg.groups) bases.push_back(placer_base(log, d, c, g, true));
@@ -2338,7 +2378,7 @@ static void global_placement(RunResult &res, const Design &d, const std::vector<
     bases.erase(bases.begin());
   }
   auto t0 = std::chrono::steady_clock::now();
-  Ip ip = do_bicgstab_place(log, d, c, vars, ipv);
+  ip = do_bicgstab_place(log, d, c, vars, ipv);
   auto t1 = std::chrono::steady_clock::now();
   res.t_ip = std::chrono::duration<double>(t1 - t0).count();
   res.insts = (int64_t)c.insts.size();
@@ -2353,8 +2393,7 @@ static void global_placement(RunResult &res, const Design &d, const std::vector<
     }
     return;
   }
-  Nesterov np = init_nesterov_place(log, d, c, ip, bases, o);
-  std::unique_ptr<Routability> route;
+  np = init_nesterov_place(log, d, c, ip, bases, o);
   if (o.routability) {
     if (!router) refuse("-routability_driven / -timing_driven need the design database");
     route = std::make_unique<Routability>();
@@ -2366,18 +2405,12 @@ static void global_placement(RunResult &res, const Design &d, const std::vector<
     route->rb.init(np.nbs.size(), area);
     np.min_rc_cell_size.assign(np.gcells.size(), {0, 0});
   }
-  auto t2 = std::chrono::steady_clock::now();
+  t2 = std::chrono::steady_clock::now();
   int64_t design_hpwl = np.hpwl();
   np.reference_hpwl = derived_reference_hpwl(np.o.reference_hpwl, design_hpwl);
   np.np_init(log);
-  int iter = resume_nesterov_place(log, d, np, route.get());
-  auto t3 = std::chrono::steady_clock::now();
-  res.t_np = std::chrono::duration<double>(t3 - t2).count();
-  res.iterations = iter;
-  res.locations = np.placed_locations(c);
-  res.final_hpwl = np.hpwl();
-  res.final_overflow = np.average_overflow_unscaled;
-  res.trials = np.trials;
+  loop.begin(log, np);
+  nesterov = true;
 }
 
 // ---------------------------------------------------------------- test-facing entry points
@@ -2431,16 +2464,10 @@ static void fill_result(RunResult &r, gpl_result_t *out) {
   out->seconds_nesterov = r.t_np;
 }
 
-extern "C" {
-
-// The reference's `global_placement` command, on the CPU (src/run.rs:115).
-int oracle_global_placement(const gpl_design_t *cd, int argc, const char *const *argv, const gpl_router_t *router, int trace, gpl_result_t *out) {
-  RunResult r;
-  r.log.trace_on = trace != 0;
+template <class F>
+static void oracle_guarded(RunResult &r, F f) {
   try {
-    Design d = design_from_c(cd);
-    std::vector<std::string> args(argv, argv + argc);
-    global_placement(r, d, args, router);
+    f();
   } catch (const StopEx &s) {
     if (s.error) {
       r.status = GPL_ERROR;
@@ -2450,9 +2477,51 @@ int oracle_global_placement(const gpl_design_t *cd, int argc, const char *const 
       r.reason = s.why;
     }
   }
-  fill_result(r, out);
+}
+
+extern "C" {
+
+// The reference's `global_placement` command, on the CPU (src/run.rs:115).
+int oracle_global_placement(const gpl_design_t *cd, int argc, const char *const *argv, const gpl_router_t *router, int trace, gpl_result_t *out) {
+  OracleRun run;
+  run.res.log.trace_on = trace != 0;
+  oracle_guarded(run.res, [&] {
+    run.d = design_from_c(cd);
+    run.open(std::vector<std::string>(argv, argv + argc), router);
+    run.close();
+  });
+  fill_result(run.res, out);
   return out->status;
 }
+
+// The command with its loop stepped by the caller (for timing a bounded sample).
+void *oracle_session_open(const gpl_design_t *cd, int argc, const char *const *argv, const gpl_router_t *router) {
+  OracleRun *run = new OracleRun();
+  oracle_guarded(run->res, [&] {
+    run->d = design_from_c(cd);
+    run->open(std::vector<std::string>(argv, argv + argc), router);
+  });
+  return run;
+}
+int oracle_session_iterate(void *h, int n, int *done) {
+  OracleRun *run = (OracleRun *)h;
+  int k = 0;
+  if (run->res.status == GPL_PLACED) oracle_guarded(run->res, [&] {
+      while (k < n && run->step()) k++;
+    });
+  *done = (run->ended || !run->nesterov || run->res.status != GPL_PLACED) ? 1 : 0;
+  return k;
+}
+int64_t oracle_session_trials(void *h) { return ((OracleRun *)h)->np.trials; }
+int oracle_session_close(void *h, gpl_result_t *out) {
+  OracleRun *run = (OracleRun *)h;
+  if (run->res.status == GPL_PLACED) oracle_guarded(run->res, [&] { run->close(); });
+  fill_result(run->res, out);
+  delete run;
+  return out->status;
+}
+// Drops a session where it stands (no loop to the end, no report).
+void oracle_session_discard(void *h) { delete (OracleRun *)h; }
 
 void oracle_result_free(gpl_result_t *out) {
   free(out->reason);

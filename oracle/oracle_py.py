@@ -85,3 +85,46 @@ def global_placement(design, args, router=None, trace=False):
         return result_to_dict(res)
     finally:
         L.oracle_result_free(C.byref(res))
+
+
+class Session:
+    """The oracle's command with its Nesterov loop stepped by the caller."""
+
+    def __init__(self, design, args, router=None):
+        L = lib()
+        L.oracle_session_open.restype = C.c_void_p
+        L.oracle_session_open.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_char_p), C.c_void_p]
+        L.oracle_session_iterate.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+        L.oracle_session_trials.restype = C.c_int64
+        L.oracle_session_trials.argtypes = [C.c_void_p]
+        L.oracle_session_close.argtypes = [C.c_void_p, C.POINTER(gpl_result_t)]
+        self._cd = design.c_struct()
+        argv = (C.c_char_p * max(len(args), 1))(*[a.encode() for a in args])
+        self._h = L.oracle_session_open(C.byref(self._cd), len(args), argv, router)
+        self.done = False
+
+    def iterate(self, n):
+        d = C.c_int()
+        k = lib().oracle_session_iterate(self._h, n, C.byref(d))
+        self.done = bool(d.value)
+        return k
+
+    def trials(self):
+        return lib().oracle_session_trials(self._h)
+
+    def close(self):
+        res = gpl_result_t()
+        lib().oracle_session_close(self._h, C.byref(res))
+        try:
+            return result_to_dict(res)
+        finally:
+            lib().oracle_result_free(C.byref(res))
+
+
+def _discard(self):
+    lib().oracle_session_discard.argtypes = [C.c_void_p]
+    lib().oracle_session_discard(self._h)
+    self._h = None
+
+
+Session.discard = _discard

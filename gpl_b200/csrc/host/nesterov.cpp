@@ -1062,7 +1062,7 @@ struct Placer {
     size_t n = nb.cells.size();
     std::vector<float> xy(2 * n);
     for (size_t i = 0; i < n; i++) {
-      GCell &g = gcells[nb.cells[i]];
+      GCell &g = gcells[gcell_of_dev[nb.cell_off + i]];  // the device's order of the region's cells
       // updateDensityCoordiLayoutInside (:2173-2185) on the host copy of the density box
       float tlx = fmaxr((float)g.dlx, (float)nb.bg.lx), tly = fmaxr((float)g.dly, (float)nb.bg.ly);
       if (tlx + (float)g.d_dx() > (float)nb.bg.ux) tlx = (float)(nb.bg.ux - g.d_dx());
@@ -1517,11 +1517,33 @@ static EngineSetup engine_setup(Placer &P) {
   EngineSetup s;
   P.dev_of_gcell.assign(P.gcells.size(), -1);
   P.gcell_of_dev.clear();
+  // Device order: each region's cells along a Z-order curve of their density centres over
+  // its bin grid, so a warp's and a block's cells lie close together (their bins and their
+  // pins' cells share cache lines and shared-memory tiles). The order is the device's only:
+  // the region's own cell order (nb.cells) is kept for everything the reference orders by.
+  auto spread = [](uint32_t v) {
+    uint64_t x = v & 0xffff;
+    x = (x | (x << 8)) & 0x00ff00ff;
+    x = (x | (x << 4)) & 0x0f0f0f0f;
+    x = (x | (x << 2)) & 0x33333333;
+    x = (x | (x << 1)) & 0x55555555;
+    return x;
+  };
   for (auto &nb : P.nbs) {
     nb.cell_off = (int64_t)P.gcell_of_dev.size();
+    std::vector<std::pair<uint64_t, int>> keyed;
+    keyed.reserve(nb.cells.size());
     for (int gi : nb.cells) {
-      P.dev_of_gcell[gi] = (int64_t)P.gcell_of_dev.size();
-      P.gcell_of_dev.push_back(gi);
+      const GCell &g = P.gcells[gi];
+      double fx = ((double)g.d_cx() - nb.bg.lx) / std::max(nb.bg.size_x, 1.0);
+      double fy = ((double)g.d_cy() - nb.bg.ly) / std::max(nb.bg.size_y, 1.0);
+      uint32_t qx = (uint32_t)std::min(std::max(fx, 0.0), 65535.0), qy = (uint32_t)std::min(std::max(fy, 0.0), 65535.0);
+      keyed.push_back({spread(qx) | (spread(qy) << 1), gi});
+    }
+    std::stable_sort(keyed.begin(), keyed.end(), [](const std::pair<uint64_t, int> &a, const std::pair<uint64_t, int> &b) { return a.first < b.first; });
+    for (auto &kv : keyed) {
+      P.dev_of_gcell[kv.second] = (int64_t)P.gcell_of_dev.size();
+      P.gcell_of_dev.push_back(kv.second);
     }
   }
   size_t n = P.gcell_of_dev.size();

@@ -24,9 +24,33 @@ __device__ __forceinline__ float inside_axis(float c, float half, float lo, floa
   return adj;
 }
 
-__global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
+// The block's cells lie close together (the device orders each region's cells along a Z
+// curve): the block first sums its addends in a shared-memory tile of the bins its cells
+// cover, then adds each touched bin to HBM once. A block whose cells spread over more than
+// kTileBins bins adds straight to HBM. Integer adds either way: the same accumulators.
+constexpr int kTileBins = 2048;
+
+__device__ __forceinline__ int64_t cell_bin_addend(const RegionArgs &r, int32_t dlx, int32_t dux, int32_t dly, int32_t duy, int32_t x, int32_t y, float scale, uint8_t kind) {
+  int32_t blx = r.bx[x], bux = r.bx[x + 1], bly = r.by[y], buy = r.by[y + 1];
+  int32_t olx = dlx > blx ? dlx : blx, oux = dux < bux ? dux : bux;
+  int32_t oly = dly > bly ? dly : bly, ouy = duy < buy ? duy : buy;
+  float a = 0.0f;
+  if (olx < oux && oly < ouy) a = __fmul_rn((float)(oux - olx), (float)(ouy - oly));
+  a = __fmul_rn(a, scale);
+  if (kind == CELL_MACRO) a = __fmul_rn(a, r.target_density);
+  return f2l_rz(a);
+}
+
+__global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
+  __shared__ unsigned long long s_inst[kTileBins], s_fill[kTileBins];
+  __shared__ int s_box[4];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.n_cells) return;
+  const bool valid = i < r.n_cells;
+  int32_t x0 = INT32_MAX, x1 = INT32_MIN, y0 = INT32_MAX, y1 = INT32_MIN;
+  int32_t dlx = 0, dux = 0, dly = 0, duy = 0;
+  float scale = 0.0f;
+  uint8_t kind = 0;
+  if (valid) {
   float2 p = make_float2(0.0f, 0.0f);
   if (mode == PLACE_AT) {
     p = coords[i];
@@ -61,25 +85,62 @@ __global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, fl
     c.dcy[i] = cy;
   }
   int32_t hx = c.hx[i], hy = c.hy[i];
-  int32_t dlx = cx - hx, dux = cx + hx, dly = cy - hy, duy = cy + hy;
-  int32_t x0, x1, y0, y1;
+  dlx = cx - hx;
+  dux = cx + hx;
+  dly = cy - hy;
+  duy = cy + hy;
   bin_span(dlx, dux, r.lx, r.size_x, r.nx, x0, x1);
   bin_span(dly, duy, r.ly, r.size_y, r.ny, y0, y1);
-  float scale = c.dscale[i];
-  uint8_t kind = c.kind[i];
-  unsigned long long *acc = (unsigned long long *)(kind == CELL_FILLER ? r.acc_fill : r.acc_inst);
-  for (int32_t y = y0; y < y1; y++) {
-    int32_t bly = r.by[y], buy = r.by[y + 1];
-    int32_t oly = dly > bly ? dly : bly, ouy = duy < buy ? duy : buy;
-    for (int32_t x = x0; x < x1; x++) {
-      int32_t blx = r.bx[x], bux = r.bx[x + 1];
-      int32_t olx = dlx > blx ? dlx : blx, oux = dux < bux ? dux : bux;
-      float a = 0.0f;
-      if (olx < oux && oly < ouy) a = __fmul_rn((float)(oux - olx), (float)(ouy - oly));
-      a = __fmul_rn(a, scale);
-      if (kind == CELL_MACRO) a = __fmul_rn(a, r.target_density);
-      int64_t v = f2l_rz(a);
-      if (v) atomicAdd(&acc[(size_t)x * r.ny + y], (unsigned long long)v);
+  scale = c.dscale[i];
+  kind = c.kind[i];
+  }
+  // the block's bin box
+  if (threadIdx.x == 0) {
+    s_box[0] = INT32_MAX;
+    s_box[1] = INT32_MIN;
+    s_box[2] = INT32_MAX;
+    s_box[3] = INT32_MIN;
+  }
+  __syncthreads();
+  bool any = valid && x0 < x1 && y0 < y1;
+  int32_t wx0 = __reduce_min_sync(0xffffffffu, any ? x0 : INT32_MAX), wx1 = __reduce_max_sync(0xffffffffu, any ? x1 : INT32_MIN);
+  int32_t wy0 = __reduce_min_sync(0xffffffffu, any ? y0 : INT32_MAX), wy1 = __reduce_max_sync(0xffffffffu, any ? y1 : INT32_MIN);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&s_box[0], wx0);
+    atomicMax(&s_box[1], wx1);
+    atomicMin(&s_box[2], wy0);
+    atomicMax(&s_box[3], wy1);
+  }
+  __syncthreads();
+  const int32_t tx0 = s_box[0], ty0 = s_box[2];
+  const int32_t tw = s_box[1] - tx0, th = s_box[3] - ty0;
+  const bool tile = tw > 0 && th > 0 && (int64_t)tw * th <= kTileBins;
+  if (tile) {
+    for (int k = threadIdx.x; k < tw * th; k += blockDim.x) {
+      s_inst[k] = 0;
+      s_fill[k] = 0;
+    }
+    __syncthreads();
+  }
+  if (any) {
+    unsigned long long *acc = (unsigned long long *)(kind == CELL_FILLER ? r.acc_fill : r.acc_inst);
+    unsigned long long *sacc = kind == CELL_FILLER ? s_fill : s_inst;
+    for (int32_t y = y0; y < y1; y++)
+      for (int32_t x = x0; x < x1; x++) {
+        int64_t v = cell_bin_addend(r, dlx, dux, dly, duy, x, y, scale, kind);
+        if (!v) continue;
+        if (tile)
+          atomicAdd(&sacc[(x - tx0) * th + (y - ty0)], (unsigned long long)v);
+        else
+          atomicAdd(&acc[(size_t)x * r.ny + y], (unsigned long long)v);
+      }
+  }
+  if (tile) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < tw * th; k += blockDim.x) {
+      size_t g = (size_t)(tx0 + k / th) * r.ny + (ty0 + k % th);
+      if (s_inst[k]) atomicAdd((unsigned long long *)&r.acc_inst[g], s_inst[k]);
+      if (s_fill[k]) atomicAdd((unsigned long long *)&r.acc_fill[g], s_fill[k]);
     }
   }
 }

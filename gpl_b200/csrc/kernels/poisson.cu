@@ -168,6 +168,9 @@ PoissonPlan *poisson_plan_create(int nx, int ny, const float *wx_host, const flo
   PoissonPlan *p = new PoissonPlan();
   p->nx = nx;
   p->ny = ny;
+  // the tensor-core tiles are 128 x 64 with K-blocks of 64: a grid whose sides are not
+  // multiples of 128 (small or odd -bin_grid_count grids) is solved with the FP32 GEMMs
+  if (mode == 1 && (nx % 128 != 0 || ny % 128 != 0)) mode = 0;
   p->mode = mode;
   *err = cudaSuccess;
   std::vector<float> w2((size_t)nx + ny);

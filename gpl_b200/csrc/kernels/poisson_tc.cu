@@ -1,11 +1,405 @@
-// Split-BF16 tensor-core density solver: placeholder until the tcgen05 GEMMs land.
+// The density solver's transforms as split-BF16 GEMMs on the 5th-generation tensor cores.
+//
+// Every operand X (a basis matrix, the density, an intermediate) is stored as two bfloat16
+// halves side by side along K: [X_hi | X_lo] with X_hi = bf16(X) and X_lo = bf16(X - X_hi).
+// One GEMM D = A B^T then runs three K segments, A_hi B_hi + A_hi B_lo + A_lo B_hi (the
+// compensated product; A_lo B_lo is below FP32 accumulation noise), accumulated in FP32 in
+// tensor memory. The epilogue reads the accumulator back (tcgen05.ld) and writes the next
+// GEMM's split operand directly, or the spectral step's two operands, or the FP32 field.
+//
+// Kernel: one 128 x 64 output tile per CTA of 128 threads. Thread 0 issues the TMA loads of
+// the K-blocks (128B-swizzled 128x64 A and 64x64 B bf16 tiles) into a 6-stage ring; thread 32
+// issues tcgen05.mma (M=128, N=64, K=16, kind::f16, bf16 in, f32 accumulate) as the stages
+// land, committing each stage back to the producer; after the last K-block all four warps
+// read their 32 TMEM lanes. Every wait is bounded by the GPU's global timer (1 s): a wait that
+// runs out records an error word, and the CTA drains and returns.
+//
+// The four launches of a solve (see poisson.cu for the algebra):
+//   1  T1t = CyTs rho^T                      split out
+//   2  Ah  = CxTs T1t^T  -> Exh, Eyh         spectral epilogue, two split outs
+//   3  T2t = Cy Exh^T ; T3t = Sy Eyh^T       batched, split outs
+//   4  Ex  = Sx T2t^T ; Ey  = Cx T3t^T       batched, FP32 outs
+// Grid sides must be multiples of 128 (the engine runs the FP32 solver otherwise).
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "engine_kernels.h"
 #include "poisson_internal.h"
 
 namespace gpl {
 
-cudaError_t tc_plan_init(PoissonPlan *, const BasisHost &) { return cudaErrorNotSupported; }
-void tc_plan_free(PoissonPlan *) {}
-cudaError_t tc_solve(PoissonPlan *, float *, float *, cudaStream_t) { return cudaErrorNotSupported; }
-int tc_launches(const PoissonPlan *) { return 0; }
+namespace {
+
+constexpr int BM = 128, BN = 64, BK = 64, STAGES = 6;
+constexpr int A_TILE = BM * BK * 2;            // 16 KB
+constexpr int B_TILE = BN * BK * 2;            // 8 KB
+constexpr int STAGE_BYTES = A_TILE + B_TILE;   // 24 KB, a multiple of 1 KB
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr uint32_t TMEM_COLS = 64;             // BN fp32 accumulator columns
+constexpr uint64_t WAIT_NS = 1000000000ull;    // a wait that lasts a second is an error
+
+enum Epi { EPI_SPLIT = 0, EPI_SPECTRAL = 1, EPI_F32 = 2 };
+
+struct TcOut {
+  void *out0, *out1;  // split: [M][2*ldk] bf16; f32: [M][N] float
+  int ld;             // split: the next GEMM's K (= this N); f32: N
+};
+struct TcArgs {
+  int M, N, K;        // multiples of 128, 64, 64
+  TcOut o[2];         // per batch entry (blockIdx.z)
+  const float *wx, *wx2, *wy, *wy2;
+  int *err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint64_t gtimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait on a phase; false (and the error word set) when it runs out or another role
+// already failed.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *fail, int *err, int code) {
+  uint64_t t0 = gtimer();
+  while (!mbar_try(b, parity)) {
+    if (*fail) return false;
+    if (gtimer() - t0 > WAIT_NS) {
+      *fail = 1;
+      atomicExch(err, code);
+      return false;
+    }
+  }
+  return true;
+}
+__device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, uint64_t *bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+// K-major, 128-byte swizzle, 8-row groups 1 KB apart, Blackwell descriptor version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+// kind::f16 instruction descriptor: D f32, A and B bf16, both K-major, M=128, N=64.
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(IDESC), "r"(accumulate));
+}
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]),
+        "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void split_store(__nv_bfloat16 *row_hi, __nv_bfloat16 *row_lo, const float *v) {
+  // 64 values: hi and lo halves, 16-byte stores
+#pragma unroll
+  for (int c = 0; c < BN; c += 8) {
+    __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      h[q] = __float2bfloat16_rn(v[c + q]);
+      l[q] = __float2bfloat16_rn(v[c + q] - __bfloat162float(h[q]));
+    }
+    *reinterpret_cast<uint4 *>(row_hi + c) = *reinterpret_cast<const uint4 *>(h);
+    *reinterpret_cast<uint4 *>(row_lo + c) = *reinterpret_cast<const uint4 *>(l);
+  }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tB0,
+                                                   const __grid_constant__ CUtensorMap tA1, const __grid_constant__ CUtensorMap tB1, TcArgs args) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t *full = (uint64_t *)(smem + STAGES * STAGE_BYTES);
+  uint64_t *empty = full + STAGES;
+  uint64_t *done = empty + STAGES;
+  uint32_t *tmem_slot = (uint32_t *)(done + 1);
+  volatile int *fail = (volatile int *)(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int z = blockIdx.z;
+  const CUtensorMap *mA = z ? &tA1 : &tA0;
+  const CUtensorMap *mB = z ? &tB1 : &tB0;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int kb_per_seg = args.K / BK, nkb = 3 * kb_per_seg;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {  // the whole warp allocates the accumulator columns
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)), "r"(TMEM_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (threadIdx.x == 0) {
+    // producer: K-block kb of segment seg reads A at column (seg == 2 ? K : 0) + k0 and B at
+    // column (seg == 1 ? K : 0) + k0: hi*hi, hi*lo, lo*hi
+    for (int kb = 0; kb < nkb; kb++) {
+      int s = kb % STAGES, round = kb / STAGES;
+      if (round > 0 && !mbar_wait(&empty[s], (round - 1) & 1, fail, args.err, 1)) break;
+      int seg = kb / kb_per_seg, k0 = (kb % kb_per_seg) * BK;
+      int ax = (seg == 2 ? args.K : 0) + k0, bx = (seg == 1 ? args.K : 0) + k0;
+      uint8_t *sa = smem + s * STAGE_BYTES, *sb = sa + A_TILE;
+      mbar_expect_tx(&full[s], STAGE_BYTES);
+      tma_load(sa, mA, &full[s], ax, m0);
+      tma_load(sb, mB, &full[s], bx, n0);
+    }
+  } else if (threadIdx.x == 32) {
+    // MMA issuer
+    for (int kb = 0; kb < nkb; kb++) {
+      int s = kb % STAGES, round = kb / STAGES;
+      if (!mbar_wait(&full[s], round & 1, fail, args.err, 2)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t a = smem_u32(smem + s * STAGE_BYTES), b = a + A_TILE;
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; kk++) umma(tmem, smem_desc(a + kk * 32), smem_desc(b + kk * 32), (kb > 0 || kk > 0) ? 1u : 0u);
+      umma_commit(&empty[s]);
+    }
+    umma_commit(done);
+  }
+  __syncwarp();
+  // epilogue: every warp reads its 32 lanes (rows) of the 128 x 64 accumulator; lane 0 waits
+  // for the last commit, so the warp stays converged for the aligned TMEM loads
+  int okw = 0;
+  if (lane == 0) okw = mbar_wait(done, 0, fail, args.err, 3) && !*fail;
+  okw = __shfl_sync(0xffffffffu, okw, 0);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (okw) {
+    float v[BN];
+    uint32_t base = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+    for (int c = 0; c < BN; c += 16) tmem_ld16(base + c, v + c);
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    const int m = m0 + warp * 32 + lane;
+    const TcOut &o = args.o[z];
+    if (m < args.M) {
+      if (EPI == EPI_F32) {
+        float *row = (float *)o.out0 + (size_t)m * o.ld + n0;
+#pragma unroll
+        for (int c = 0; c < BN; c += 4) *reinterpret_cast<float4 *>(row + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+      } else if (EPI == EPI_SPLIT) {
+        __nv_bfloat16 *row = (__nv_bfloat16 *)o.out0 + (size_t)m * 2 * o.ld;
+        split_store(row + n0, row + o.ld + n0, v);
+      } else {
+        // the spectral step (src/nesterov.rs:425-440) on the scaled forward transform
+        float ex[BN], ey[BN];
+        float wxu = args.wx[m], wx2u = args.wx2[m];
+#pragma unroll
+        for (int c = 0; c < BN; c++) {
+          int n = n0 + c;
+          float p = (m == 0 && n == 0) ? 0.0f : __fdiv_rn(v[c], __fadd_rn(wx2u, args.wy2[n]));
+          ex[c] = __fmul_rn(p, wxu);
+          ey[c] = __fmul_rn(p, args.wy[n]);
+        }
+        __nv_bfloat16 *rx = (__nv_bfloat16 *)o.out0 + (size_t)m * 2 * o.ld;
+        __nv_bfloat16 *ry = (__nv_bfloat16 *)o.out1 + (size_t)m * 2 * o.ld;
+        split_store(rx + n0, rx + o.ld + n0, ex);
+        split_store(ry + n0, ry + o.ld + n0, ey);
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
+}
+
+// ---------------------------------------------------------------- host side
+typedef CUresult (*EncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  if (!fn) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess) fn = (EncodeTiled)p;
+  }
+  return fn;
+}
+
+// A split operand [rows][2*k] bf16 as a TMA map with a (box_rows x 64) box, 128B swizzle.
+cudaError_t make_map(CUtensorMap *m, const __nv_bfloat16 *base, int rows, int k, int box_rows) {
+  EncodeTiled enc = encode_fn();
+  if (!enc) return cudaErrorNotSupported;
+  if (((uintptr_t)base & 15) != 0 || (k * 2 * 2) % 16 != 0) return cudaErrorInvalidValue;
+  cuuint64_t dims[2] = {(cuuint64_t)(2 * k), (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(2 * k) * 2};
+  cuuint32_t box[2] = {BK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void *)base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+struct TcState {
+  __nv_bfloat16 *CyTs = nullptr, *CxTs = nullptr, *Cy = nullptr, *Sy = nullptr, *Sx = nullptr, *Cx = nullptr;
+  __nv_bfloat16 *t1 = nullptr, *exh = nullptr, *eyh = nullptr, *t2 = nullptr, *t3 = nullptr;
+  int *err = nullptr;
+  CUtensorMap mCyTs, mCxTs, mCy, mSy, mSx, mCx;  // A operands (BM-row boxes)
+  CUtensorMap mDens, mT1, mExh, mEyh, mT2, mT3;  // B operands (BN-row boxes)
+};
+
+static cudaError_t upload_split(const std::vector<double> &h, int rows, int k, __nv_bfloat16 **d) {
+  std::vector<__nv_bfloat16> v((size_t)rows * 2 * k);
+  for (int r = 0; r < rows; r++)
+    for (int c = 0; c < k; c++) {
+      float x = (float)h[(size_t)r * k + c];
+      __nv_bfloat16 hi = __float2bfloat16_rn(x);
+      v[(size_t)r * 2 * k + c] = hi;
+      v[(size_t)r * 2 * k + k + c] = __float2bfloat16_rn(x - __bfloat162float(hi));
+    }
+  cudaError_t e = cudaMalloc(d, v.size() * sizeof(__nv_bfloat16));
+  if (e != cudaSuccess) return e;
+  return cudaMemcpy(*d, v.data(), v.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice);
+}
+
+cudaError_t tc_plan_init(PoissonPlan *p, const BasisHost &b) {
+  int nx = p->nx, ny = p->ny;
+  if (nx % 128 != 0 || ny % 128 != 0) return cudaErrorNotSupported;
+  TcState *t = new TcState();
+  p->tc = t;
+  cudaError_t e;
+#define TRY(x)                            \
+  do {                                    \
+    if ((e = (x)) != cudaSuccess) return e; \
+  } while (0)
+  TRY(upload_split(b.CyTs, ny, ny, &t->CyTs));
+  TRY(upload_split(b.CxTs, nx, nx, &t->CxTs));
+  TRY(upload_split(b.Cy, ny, ny, &t->Cy));
+  TRY(upload_split(b.Sy, ny, ny, &t->Sy));
+  TRY(upload_split(b.Sx, nx, nx, &t->Sx));
+  TRY(upload_split(b.Cx, nx, nx, &t->Cx));
+  size_t n = (size_t)nx * ny * 2;
+  TRY(cudaMalloc(&p->tc_dens, n * sizeof(__nv_bfloat16)));
+  TRY(cudaMalloc(&t->t1, n * sizeof(__nv_bfloat16)));
+  TRY(cudaMalloc(&t->exh, n * sizeof(__nv_bfloat16)));
+  TRY(cudaMalloc(&t->eyh, n * sizeof(__nv_bfloat16)));
+  TRY(cudaMalloc(&t->t2, n * sizeof(__nv_bfloat16)));
+  TRY(cudaMalloc(&t->t3, n * sizeof(__nv_bfloat16)));
+  TRY(cudaMemset(p->tc_dens, 0, n * sizeof(__nv_bfloat16)));
+  TRY(cudaMalloc(&t->err, sizeof(int)));
+  TRY(cudaMemset(t->err, 0, sizeof(int)));
+  // A operands [M][2K]: 128-row boxes
+  TRY(make_map(&t->mCyTs, t->CyTs, ny, ny, BM));
+  TRY(make_map(&t->mCxTs, t->CxTs, nx, nx, BM));
+  TRY(make_map(&t->mCy, t->Cy, ny, ny, BM));
+  TRY(make_map(&t->mSy, t->Sy, ny, ny, BM));
+  TRY(make_map(&t->mSx, t->Sx, nx, nx, BM));
+  TRY(make_map(&t->mCx, t->Cx, nx, nx, BM));
+  // B operands [N][2K]: 64-row boxes
+  TRY(make_map(&t->mDens, p->tc_dens, nx, ny, BN));  // rows x, K = y
+  TRY(make_map(&t->mT1, t->t1, ny, nx, BN));         // rows v, K = x
+  TRY(make_map(&t->mExh, t->exh, nx, ny, BN));       // rows u, K = v
+  TRY(make_map(&t->mEyh, t->eyh, nx, ny, BN));
+  TRY(make_map(&t->mT2, t->t2, ny, nx, BN));         // rows y, K = u
+  TRY(make_map(&t->mT3, t->t3, ny, nx, BN));
+#undef TRY
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_tc_gemm<EPI_SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_tc_gemm<EPI_SPECTRAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_tc_gemm<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    attr = true;
+  }
+  return cudaGetLastError();
+}
+
+void tc_plan_free(PoissonPlan *p) {
+  if (p->tc_dens) cudaFree(p->tc_dens);
+  p->tc_dens = nullptr;
+  TcState *t = p->tc;
+  if (!t) return;
+  void *bufs[] = {t->CyTs, t->CxTs, t->Cy, t->Sy, t->Sx, t->Cx, t->t1, t->exh, t->eyh, t->t2, t->t3, t->err};
+  for (void *b : bufs)
+    if (b) cudaFree(b);
+  delete t;
+  p->tc = nullptr;
+}
+
+int tc_launches(const PoissonPlan *) { return 4; }
+
+cudaError_t tc_solve(PoissonPlan *p, float *field_x, float *field_y, cudaStream_t s) {
+  TcState *t = p->tc;
+  int nx = p->nx, ny = p->ny;
+  TcArgs a{};
+  a.wx = p->wx;
+  a.wx2 = p->wx2;
+  a.wy = p->wy;
+  a.wy2 = p->wy2;
+  a.err = t->err;
+  // 1: T1t[v][x] = sum_y CyTs[v][y] rho[x][y]      M = ny, N = nx, K = ny
+  a.M = ny, a.N = nx, a.K = ny;
+  a.o[0] = TcOut{t->t1, nullptr, nx};
+  k_tc_gemm<EPI_SPLIT><<<dim3(nx / BN, ny / BM, 1), 128, SMEM_BYTES, s>>>(t->mCyTs, t->mDens, t->mCyTs, t->mDens, a);
+  // 2: Ah[u][v] = sum_x CxTs[u][x] T1t[v][x]; spectral  M = nx, N = ny, K = nx
+  a.M = nx, a.N = ny, a.K = nx;
+  a.o[0] = TcOut{t->exh, t->eyh, ny};
+  k_tc_gemm<EPI_SPECTRAL><<<dim3(ny / BN, nx / BM, 1), 128, SMEM_BYTES, s>>>(t->mCxTs, t->mT1, t->mCxTs, t->mT1, a);
+  // 3: T2t[y][u] = sum_v Cy[y][v] Exh[u][v]; T3t = Sy Eyh^T   M = ny, N = nx, K = ny
+  a.M = ny, a.N = nx, a.K = ny;
+  a.o[0] = TcOut{t->t2, nullptr, nx};
+  a.o[1] = TcOut{t->t3, nullptr, nx};
+  k_tc_gemm<EPI_SPLIT><<<dim3(nx / BN, ny / BM, 2), 128, SMEM_BYTES, s>>>(t->mCy, t->mExh, t->mSy, t->mEyh, a);
+  // 4: Ex[x][y] = sum_u Sx[x][u] T2t[y][u]; Ey = Cx T3t^T     M = nx, N = ny, K = nx
+  a.M = nx, a.N = ny, a.K = nx;
+  a.o[0] = TcOut{field_x, nullptr, ny};
+  a.o[1] = TcOut{field_y, nullptr, ny};
+  k_tc_gemm<EPI_F32><<<dim3(ny / BN, nx / BM, 2), 128, SMEM_BYTES, s>>>(t->mSx, t->mT2, t->mCx, t->mT3, a);
+  return cudaGetLastError();
+}
+
+int tc_error(const PoissonPlan *p) {
+  int h = 0;
+  if (p->tc && p->tc->err) cudaMemcpy(&h, p->tc->err, sizeof h, cudaMemcpyDeviceToHost);
+  return h;
+}
 
 }  // namespace gpl

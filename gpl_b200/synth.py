@@ -5,7 +5,10 @@ generator for every size):
 
 * DBU 1000; rows 1.4 um (1400) high; one non-PAD site 0.19 um (190) wide; rows tile the core.
 * Standard cells: one row high, widths uniform in [w_min, w_max] sites; unplaced (their
-  database box at the origin), so initial placement starts them at the core centre.
+  database box at the origin), so initial placement starts them at the core centre. With
+  `placed=True` each cell is instead placed at its latent position (the point the locality
+  window is drawn around), snapped to the site/row grid inside the core: a spread start for
+  runs that skip the initial placement (`-skip_initial_place`).
 * Nets: degree 2 (55 %), 3 (20 %), 4 (10 %), else uniform 5..16 (with `max_degree` above 16,
   one net in a hundred is uniform 17..max_degree instead). Each net's terminals are cells drawn
   within a window of +-15 % of the core around an anchor (a cell, or the net's IO port);
@@ -93,6 +96,7 @@ def _place_macros(rng, n, frac, core_w, core_h):
 def generate(cfg="cfg1", **over) -> Design:
     """A seeded synthetic design: a preset name, optionally with parameters overridden."""
     p = dict(PRESETS[cfg]) if isinstance(cfg, str) else dict(cfg)
+    placed = bool(over.pop("placed", False))
     p.update(over)
     rng = np.random.default_rng(p["seed"])
     m = int(p["cells"])
@@ -209,6 +213,12 @@ def generate(cfg="cfg1", **over) -> Design:
     inst_master[m:, 1] = macros[:, 3] - macros[:, 1] if n_mac else 0
     inst_flags = np.full(n_inst, INST_CORE_AUTO_PLACEABLE, np.uint32)
     inst_flags[m:] |= INST_BLOCK | INST_FIXED | INST_PLACED
+    if placed:
+        llx = np.clip(np.round((lat_x - cw / 2) / SITE_W) * SITE_W, 0, core_w - cw).astype(np.int64)
+        lly = np.clip(np.round((lat_y - ch / 2) / ROW_H) * ROW_H, 0, core_h - ch).astype(np.int64)
+        inst_box[:m, 0], inst_box[:m, 1] = llx, lly
+        inst_box[:m, 2], inst_box[:m, 3] = llx + cw, lly + ch
+        inst_flags[:m] |= INST_PLACED
 
     n_rows = core_h // ROW_H
     row_box = np.zeros((n_rows, 4), np.int32)
@@ -225,6 +235,6 @@ def generate(cfg="cfg1", **over) -> Design:
         net_iterm_start=starts, iterm_inst=cell.astype(np.int32), iterm_shape=iterm_shape,
         net_bterm_start=bstart_n.astype(np.int64), bterm_box=bterm_box,
         bterm_flags=np.full(n_io, BTERM_PLACED | BTERM_FIXED, np.uint8),
-        meta=dict(config=cfg if isinstance(cfg, str) else "custom", params=p,
+        meta=dict(config=cfg if isinstance(cfg, str) else "custom", params=p, placed=placed,
                   cells=m, macros=n_mac, nets=n_nets, pins=int(total + n_io)),
     )

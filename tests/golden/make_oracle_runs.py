@@ -1,0 +1,64 @@
+"""Writes tests/golden/oracle_runs.json: the oracle's whole `global_placement` run on the
+100k-cell and 1M-cell synthetic designs, summarised (the report's construction lines, the
+`[InitialPlace]` rows, the iteration count, final HPWL and overflow, and a checksum of the
+written placement).
+
+These runs take minutes (100k cells) to about an hour (1M cells) on one CPU thread, so the
+GPU tests compare against this summary instead of re-running the oracle. Run from the
+repository root:
+
+    python tests/golden/make_oracle_runs.py [cfg2] [cfg3]
+"""
+import json
+import os
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from gpl_b200 import synth  # noqa: E402
+
+ARGS = {
+    "cfg2": ["-density", "0.70", "-bin_grid_count", "512"],
+    "cfg3": ["-density", "0.70", "-bin_grid_count", "1024"],
+}
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle_runs.json")
+
+
+def summarise(cfg, res, seconds):
+    lines = res["lines"]
+    header = []
+    for l in lines:
+        if l.startswith("[InitialPlace]"):
+            break
+        header.append(l)
+    loc = res["locations"]
+    return {
+        "config": cfg, "args": ARGS[cfg], "status": res["status"],
+        "insts": res["insts"], "nets": res["nets"], "pins": res["pins"],
+        "header": header,
+        "initial_place": [l for l in lines if l.startswith("[InitialPlace]")],
+        "nesterov_iterations": res["nesterov_iterations"],
+        "final_hpwl": res["final_hpwl"], "final_overflow": res["final_overflow"],
+        "locations": int(len(loc)),
+        "location_sums": [int(loc[:, 1].astype("int64").sum()), int(loc[:, 2].astype("int64").sum())] if len(loc) else [0, 0],
+        "seconds": seconds,
+    }
+
+
+def main(cfgs):
+    out = json.load(open(OUT)) if os.path.exists(OUT) else {}
+    for cfg in cfgs:
+        d = synth.generate(cfg)
+        t0 = time.perf_counter()
+        res = oracle.global_placement(d, ARGS[cfg])
+        out[cfg] = summarise(cfg, res, time.perf_counter() - t0)
+        print(cfg, out[cfg]["status"], out[cfg]["nesterov_iterations"], out[cfg]["final_hpwl"], out[cfg]["final_overflow"], flush=True)
+        with open(OUT, "w") as f:
+            json.dump(out, f, indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or ["cfg2"])

@@ -19,7 +19,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 # (source, exact float order?)
 CU = [("kernels/nesterov_kernels.cu", True), ("kernels/bicgstab.cu", True), ("kernels/rudy.cu", True),
       ("kernels/poisson.cu", False), ("kernels/poisson_tc.cu", False), ("host/engine.cu", True),
-      ("host/capi_kernels.cu", True)]
+      ("host/capi_kernels.cu", True), ("host/bicgstab_noalloc.cu", True)]
 CPP = ["host/place.cpp", "host/nesterov.cpp"]
 
 

@@ -239,6 +239,25 @@ int gpl_kernel_bicgstab(int64_t n, const int64_t *row_start, const int32_t *cols
                         const float *vals, const float *rhs, float *x, int32_t max_iters,
                         int32_t *iterations, float *error, void *stream);
 
+/* gpl_kernel_bicgstab without any device allocation. This entry point has no counterpart in the
+ * reference. It is for callers that cannot call cudaMalloc: code held to a device-memory pool
+ * sized in advance, which a library must not bypass; hosts that forbid a plug-in library to
+ * allocate device memory on its own; and code that shares the GPU with latency-critical
+ * streams, where cudaMalloc and cudaFree may wait for the whole device. Its scratch is one fixed device array of this
+ * library (reserved when the library is loaded, on every device that loads it, until the
+ * process exits), so it serves systems of at most GPL_BICGSTAB_NOALLOC_MAX_ROWS rows (about
+ * 3.7 MB of scratch); a larger n returns GPL_NOALLOC_TOO_LARGE and touches nothing. The first
+ * call on a device looks up the array's device address there (cudaGetSymbolAddress, with that
+ * device current): make that first call before any stream capture. Every call on a device
+ * shares the one array, so calls that overlap on the GPU (other streams, other threads) race:
+ * serialise them. Arguments and results as gpl_kernel_bicgstab's. */
+#define GPL_BICGSTAB_NOALLOC_MAX_ROWS 131072
+#define GPL_NOALLOC_TOO_LARGE (-2)
+int gpl_kernel_bicgstab_noalloc(int64_t n, const int64_t *row_start, const int32_t *cols,
+                                const float *vals, const float *rhs, float *x,
+                                int32_t max_iters, int32_t *iterations, float *error,
+                                void *stream);
+
 /* RUDY `Rudy::calculate` (src/route_base.rs:191-253): net boxes (4 per net) into a tile
  * demand map (x-major, cnt_x * cnt_y) over tiles of `tile_size` from the die's lower-left,
  * the last column and row stretched to `die_ux`, `die_uy`. */

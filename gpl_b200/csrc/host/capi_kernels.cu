@@ -28,20 +28,29 @@ int gpl_kernel_density_scatter(int64_t n_cells, const int32_t *cx, const int32_t
   r.ly = grid_ly;
   r.size_x = size_x;
   r.size_y = size_y;
+  r.inv_size_x = 1.0 / size_x;
+  r.inv_size_y = 1.0 / size_y;
   r.target_density = target_density;
   r.bx = bx;
   r.by = by;
   r.acc_inst = inst;
   r.acc_fill = filler;
+  // the engine keeps a cell's centre as one int2: pack the caller's two arrays
+  int2 *dc = nullptr;
+  e = cudaMallocAsync((void **)&dc, (size_t)n_cells * sizeof(int2), s);
+  if (e != cudaSuccess) return (int)e;
+  unsigned blocks = (unsigned)((n_cells + kThreadsPerBlock - 1) / kThreadsPerBlock);
+  k_pack_centres<<<blocks, kThreadsPerBlock, 0, s>>>(n_cells, cx, cy, dc);
   CellArgs c{};
-  c.dcx = const_cast<int32_t *>(cx);
-  c.dcy = const_cast<int32_t *>(cy);
+  c.dc = dc;
   c.hx = hx;
   c.hy = hy;
   c.dscale = scale;
   c.kind = kind;
-  k_place_cells<<<(unsigned)((n_cells + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, s>>>(r, c, PLACE_GIVEN, 0.0f, 0.0f, nullptr);
-  return (int)cudaGetLastError();
+  k_place_cells<<<blocks, kThreadsPerBlock, 0, s>>>(r, c, PLACE_GIVEN, 0.0f, 0.0f, nullptr);
+  e = cudaGetLastError();
+  cudaError_t e2 = cudaFreeAsync(dc, s);
+  return (int)(e != cudaSuccess ? e : e2);
 }
 
 int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy, const float *density, float *field_x, float *field_y, int mode, void *stream) {
@@ -63,14 +72,39 @@ int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy,
 
 int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, const float *net_weight, float coef_x, float coef_y, float *grad, void *stream) {
   if (n_nets <= 0) return 0;
-  WaArgs w{};
-  w.n_nets = (int32_t)n_nets;
-  w.net_start = net_start;
-  w.net_weight = net_weight;
-  w.pin_base = reinterpret_cast<const int2 *>(pin_xy);
-  w.pin_grad = reinterpret_cast<float2 *>(grad);
-  k_wa<<<(unsigned)((n_nets + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, (cudaStream_t)stream>>>(w, coef_x, coef_y);
-  return (int)cudaGetLastError();
+  cudaStream_t s = (cudaStream_t)stream;
+  // the engine's tiles of consecutive nets, built from the pin starts
+  std::vector<int64_t> starts((size_t)n_nets + 1);
+  cudaError_t e = cudaMemcpyAsync(starts.data(), net_start, starts.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return (int)e;
+  std::vector<int2> tiles;
+  std::vector<int32_t> big;
+  wa_tiles(starts.data(), (int32_t)n_nets, tiles, big);
+  int2 *d_tiles = nullptr;
+  int32_t *d_big = nullptr;
+  e = cudaMalloc((void **)&d_tiles, std::max<size_t>(tiles.size(), 1) * sizeof(int2));
+  if (e == cudaSuccess) e = cudaMalloc((void **)&d_big, std::max<size_t>(big.size(), 1) * sizeof(int32_t));
+  if (e == cudaSuccess && !tiles.empty()) e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !big.empty()) e = cudaMemcpyAsync(d_big, big.data(), big.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    WaArgs w{};
+    w.n_nets = (int32_t)big.size();
+    w.net_start = net_start;
+    w.net_order = d_big;
+    w.net_weight = net_weight;
+    w.pin_base = reinterpret_cast<const int2 *>(pin_xy);
+    w.pin_grad = reinterpret_cast<float2 *>(grad);
+    w.n_tiles = (int32_t)tiles.size();
+    w.tiles = d_tiles;
+    if (!tiles.empty()) k_wa_tiles<<<(unsigned)tiles.size(), kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y);
+    if (!big.empty()) k_wa<<<(unsigned)((big.size() + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y);
+    e = cudaGetLastError();
+  }
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  cudaFree(d_tiles);
+  cudaFree(d_big);
+  return (int)(e != cudaSuccess ? e : e2);
 }
 
 int gpl_kernel_bicgstab(int64_t n, const int64_t *row_start, const int32_t *cols, const float *vals, const float *rhs, float *x, int32_t max_iters, int32_t *iterations, float *error, void *stream) {

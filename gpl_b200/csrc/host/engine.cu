@@ -13,7 +13,8 @@ struct Engine::Region {
   RegionArgs args{};
   int32_t *bx = nullptr, *by = nullptr;
   float *scaled = nullptr, *density = nullptr, *fx = nullptr, *fy = nullptr;
-  int64_t *np = nullptr, *npu = nullptr, *acc_inst = nullptr, *acc_fill = nullptr;
+  float *np = nullptr, *npu = nullptr;
+  int64_t *acc_inst = nullptr, *acc_fill = nullptr;
   float2 *slot[S_NUM] = {};
   int64_t cell_off = 0, n_cells = 0;
   PoissonPlan *plan = nullptr;
@@ -21,9 +22,17 @@ struct Engine::Region {
   int nb_bins = 0, nb_cells = 0;
   __nv_bfloat16 *dens_split = nullptr;
   int split_ld = 0;
+  std::vector<float> np_host, npu_host;  // staging of an update_bins copy
 };
 
 static int blocks_for(int64_t n, int per = kThreadsPerBlock) { return (int)std::max<int64_t>(1, (n + per - 1) / per); }
+
+// The fixed areas as float (int64 -> float, round to nearest), as the bin density reads them.
+static std::vector<float> as_float(const std::vector<int64_t> &v) {
+  std::vector<float> out(v.size());
+  for (size_t k = 0; k < v.size(); k++) out[k] = (float)v[k];
+  return out;
+}
 
 void Engine::check(cudaError_t e, const char *where) {
   if (e != cudaSuccess && err_.code == cudaSuccess) {
@@ -115,17 +124,18 @@ Solve Engine::solve(const Csr &m, const std::vector<float> &rhs, std::vector<flo
 
 // ---------------------------------------------------------------- Nesterov state
 void Engine::free_globals() {
-  void *ptrs[] = {dcx_, dcy_, hx_, hy_, dscale_, area_, kind_, locked_, cell_pin_start_, cell_pins_, net_start_, net_order_, pin_cell_, pin_base_, net_weight_, pin_grad_, hpwl_acc_, dev_scal_};
+  void *ptrs[] = {dc_, hx_, hy_, dscale_, area_, kind_, locked_, cell_pin_start_, net_start_, pin_cell_, pin_slot_, big_nets_, pin_base_, tiles_, net_weight_, pin_grad_, hpwl_acc_, dev_scal_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
-  dcx_ = dcy_ = hx_ = hy_ = nullptr;
+  dc_ = nullptr;
+  hx_ = hy_ = nullptr;
   dscale_ = area_ = nullptr;
   kind_ = locked_ = nullptr;
   cell_pin_start_ = nullptr;
-  cell_pins_ = nullptr;
   net_start_ = nullptr;
-  net_order_ = pin_cell_ = nullptr;
-  pin_base_ = nullptr;
+  pin_cell_ = pin_slot_ = big_nets_ = nullptr;
+  pin_base_ = tiles_ = nullptr;
+  n_tiles_ = n_big_ = 0;
   net_weight_ = nullptr;
   pin_grad_ = nullptr;
   hpwl_acc_ = nullptr;
@@ -153,8 +163,11 @@ void Engine::upload(const EngineSetup &s) {
   n_cells_ = (int64_t)s.hx.size();
   n_pins_ = (int64_t)s.pin_cell.size();
   n_nets_ = (int32_t)(s.net_start.size() - 1);
-  check(upload_vec(&dcx_, s.dcx, st), "upload cells");
-  check(upload_vec(&dcy_, s.dcy, st), "upload cells");
+  {
+    std::vector<int2> dc(n_cells_);
+    for (int64_t i = 0; i < n_cells_; i++) dc[i] = make_int2(s.dcx[i], s.dcy[i]);
+    check(upload_vec(&dc_, dc, st), "upload cells");
+  }
   check(upload_vec(&hx_, s.hx, st), "upload cells");
   check(upload_vec(&hy_, s.hy, st), "upload cells");
   check(upload_vec(&dscale_, s.dscale, st), "upload cells");
@@ -163,18 +176,28 @@ void Engine::upload(const EngineSetup &s) {
   any_locked_ = std::any_of(s.locked.begin(), s.locked.end(), [](uint8_t v) { return v != 0; });
   if (any_locked_) check(upload_vec(&locked_, s.locked, st), "upload cells");
   check(upload_vec(&cell_pin_start_, s.cell_pin_start, st), "upload cells");
-  check(upload_vec(&cell_pins_, s.cell_pins, st), "upload cells");
   check(upload_vec(&net_start_, s.net_start, st), "upload nets");
-  // nets in degree order: a warp's threads walk nets of one length
-  std::vector<int32_t> order(n_nets_);
-  std::iota(order.begin(), order.end(), 0);
-  std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return s.net_start[a + 1] - s.net_start[a] < s.net_start[b + 1] - s.net_start[b]; });
-  check(upload_vec(&net_order_, order, st), "upload nets");
+  {
+    // WA's tiles of consecutive nets, and the nets too large for a tile (in degree order,
+    // so a warp's threads walk nets of one length)
+    std::vector<int2> tiles;
+    std::vector<int32_t> big;
+    wa_tiles(s.net_start.data(), n_nets_, tiles, big);
+    std::stable_sort(big.begin(), big.end(), [&](int32_t a, int32_t b) { return s.net_start[a + 1] - s.net_start[a] < s.net_start[b + 1] - s.net_start[b]; });
+    n_tiles_ = (int32_t)tiles.size();
+    n_big_ = (int32_t)big.size();
+    check(upload_vec(&tiles_, tiles, st), "upload nets");
+    check(upload_vec(&big_nets_, big, st), "upload nets");
+    // each pin's force goes to its place in its cell's pin list
+    std::vector<int32_t> slot(n_pins_, -1);
+    for (size_t k = 0; k < s.cell_pins.size(); k++) slot[s.cell_pins[k]] = (int32_t)k;
+    check(upload_vec(&pin_slot_, slot, st), "upload pins");
+  }
   check(upload_vec(&pin_cell_, s.pin_cell, st), "upload pins");
   check(dmalloc(&pin_base_, n_pins_), "upload pins");
   if (n_pins_) check(cudaMemcpyAsync(pin_base_, s.pin_base.data(), n_pins_ * sizeof(int2), cudaMemcpyHostToDevice, st), "upload pins");
   check(upload_vec(&net_weight_, s.net_weight, st), "upload nets");
-  check(dmalloc(&pin_grad_, n_pins_), "alloc pins");
+  check(dmalloc(&pin_grad_, s.cell_pins.size()), "alloc pins");
   check(dmalloc(&hpwl_acc_, 1), "alloc");
   check(dmalloc(&dev_scal_, s.regions.size()), "alloc");
   host_scal_.assign(s.regions.size(), RegionScalars{});
@@ -193,8 +216,8 @@ void Engine::upload(const EngineSetup &s) {
     check(upload_vec(&r->bx, rs.bx, st), "upload bins");
     check(upload_vec(&r->by, rs.by, st), "upload bins");
     check(upload_vec(&r->scaled, rs.scaled, st), "upload bins");
-    check(upload_vec(&r->np, rs.non_place, st), "upload bins");
-    check(upload_vec(&r->npu, rs.non_place_u, st), "upload bins");
+    check(upload_vec(&r->np, as_float(rs.non_place), st), "upload bins");
+    check(upload_vec(&r->npu, as_float(rs.non_place_u), st), "upload bins");
     check(dmalloc(&r->acc_inst, nb), "alloc bins");
     check(dmalloc(&r->acc_fill, nb), "alloc bins");
     check(dmalloc(&r->density, nb), "alloc bins");
@@ -227,6 +250,8 @@ void Engine::upload(const EngineSetup &s) {
     a.uy = rs.uy;
     a.size_x = rs.size_x;
     a.size_y = rs.size_y;
+    a.inv_size_x = 1.0 / rs.size_x;
+    a.inv_size_y = 1.0 / rs.size_y;
     a.target_density = rs.target_density;
     a.bx = r->bx;
     a.by = r->by;
@@ -249,8 +274,12 @@ void Engine::update_bins(int b, const RegionSetup &rs) {
   r->args.target_density = rs.target_density;
   size_t nb = rs.scaled.size();
   check(cudaMemcpyAsync(r->scaled, rs.scaled.data(), nb * sizeof(float), cudaMemcpyHostToDevice, stream_), "update bins");
-  check(cudaMemcpyAsync(r->np, rs.non_place.data(), nb * sizeof(int64_t), cudaMemcpyHostToDevice, stream_), "update bins");
-  check(cudaMemcpyAsync(r->npu, rs.non_place_u.data(), nb * sizeof(int64_t), cudaMemcpyHostToDevice, stream_), "update bins");
+  // staged in the region (the copy is asynchronous), converted as the density reads them
+  r->np_host = as_float(rs.non_place);
+  r->npu_host = as_float(rs.non_place_u);
+  check(cudaMemcpyAsync(r->np, r->np_host.data(), nb * sizeof(float), cudaMemcpyHostToDevice, stream_), "update bins");
+  check(cudaMemcpyAsync(r->npu, r->npu_host.data(), nb * sizeof(float), cudaMemcpyHostToDevice, stream_), "update bins");
+  check(cudaStreamSynchronize(stream_), "update bins");
 }
 
 void Engine::rewrite_cells(const EngineSetup &s) {
@@ -267,10 +296,9 @@ void Engine::rewrite_cells(const EngineSetup &s) {
   check(cudaMemcpyAsync(area_, s.area.data(), n * sizeof(float), cudaMemcpyHostToDevice, stream_), "rewrite cells");
 }
 
-static CellArgs cell_args(const int64_t off, int32_t *dcx, int32_t *dcy, int32_t *hx, int32_t *hy, float *dscale, uint8_t *kind, uint8_t *locked, float *area, int64_t *ps, int32_t *pins, float2 *const *slot) {
+static CellArgs cell_args(const int64_t off, int2 *dc, int32_t *hx, int32_t *hy, float *dscale, uint8_t *kind, uint8_t *locked, float *area, int64_t *ps, float2 *const *slot) {
   CellArgs c{};
-  c.dcx = dcx + off;
-  c.dcy = dcy + off;
+  c.dc = dc + off;
   c.hx = hx + off;
   c.hy = hy + off;
   c.dscale = dscale + off;
@@ -278,7 +306,6 @@ static CellArgs cell_args(const int64_t off, int32_t *dcx, int32_t *dcy, int32_t
   c.locked = locked ? locked + off : nullptr;
   c.area = area + off;
   c.pin_start = ps + off;
-  c.pins = pins;
   c.cur_slp = slot[S_CUR_SLP];
   c.cur_slp_sum = slot[S_CUR_SLP_SUM];
   c.next_slp = slot[S_NEXT_SLP];
@@ -290,7 +317,7 @@ static CellArgs cell_args(const int64_t off, int32_t *dcx, int32_t *dcy, int32_t
   return c;
 }
 
-#define CELLS(r) cell_args((r)->cell_off, dcx_, dcy_, hx_, hy_, dscale_, kind_, locked_, area_, cell_pin_start_, cell_pins_, (r)->slot)
+#define CELLS(r) cell_args((r)->cell_off, dc_, hx_, hy_, dscale_, kind_, locked_, area_, cell_pin_start_, (r)->slot)
 
 void Engine::set_coords(int b, SlotId slot, const std::vector<float> &xy) {
   Region *r = regions_[b];
@@ -346,21 +373,34 @@ void Engine::field(int b) {
   launches += poisson_launches(r->plan);
 }
 
-void Engine::wa(float cx, float cy) {
-  if (failed() || n_nets_ == 0) return;
+WaArgs Engine::wa_args() const {
   WaArgs w{};
-  w.n_nets = n_nets_;
+  w.n_nets = n_big_;
   w.net_start = net_start_;
-  w.net_order = net_order_;
+  w.net_order = big_nets_;
   w.net_weight = net_weight_;
   w.pin_cell = pin_cell_;
   w.pin_base = pin_base_;
-  w.dcx = dcx_;
-  w.dcy = dcy_;
+  w.dc = dc_;
+  w.pin_slot = pin_slot_;
   w.pin_grad = pin_grad_;
+  w.n_tiles = n_tiles_;
+  w.tiles = tiles_;
+  return w;
+}
+
+void Engine::wa(float cx, float cy) {
+  if (failed() || n_nets_ == 0) return;
+  WaArgs w = wa_args();
   ph_begin(PH_WA);
-  launches += 1;
-  k_wa<<<blocks_for(n_nets_), kThreadsPerBlock, 0, stream_>>>(w, cx, cy);
+  if (n_tiles_) {
+    launches += 1;
+    k_wa_tiles<<<n_tiles_, kThreadsPerBlock, 0, stream_>>>(w, cx, cy);
+  }
+  if (n_big_) {
+    launches += 1;
+    k_wa<<<blocks_for(n_big_), kThreadsPerBlock, 0, stream_>>>(w, cx, cy);
+  }
   ph_end(PH_WA);
   check(cudaGetLastError(), "wa");
 }
@@ -417,17 +457,17 @@ void Engine::fetch() {
 
 int64_t Engine::hpwl() {
   if (failed()) return 0;
-  WaArgs w{};
-  w.n_nets = n_nets_;
-  w.net_start = net_start_;
-  w.pin_cell = pin_cell_;
-  w.pin_base = pin_base_;
-  w.dcx = dcx_;
-  w.dcy = dcy_;
+  WaArgs w = wa_args();
   check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), stream_), "hpwl");
   ph_begin(PH_HPWL);
-  launches += n_nets_ ? 1 : 0;
-  if (n_nets_) k_hpwl<<<blocks_for(n_nets_), kThreadsPerBlock, 0, stream_>>>(w, hpwl_acc_);
+  if (n_tiles_) {
+    launches += 1;
+    k_hpwl_tiles<<<n_tiles_, kThreadsPerBlock, 0, stream_>>>(w, hpwl_acc_);
+  }
+  if (n_big_) {
+    launches += 1;
+    k_hpwl<<<blocks_for(n_big_), kThreadsPerBlock, 0, stream_>>>(w, hpwl_acc_);
+  }
   ph_end(PH_HPWL);
   unsigned long long h = 0;
   check(cudaMemcpyAsync(&h, hpwl_acc_, sizeof h, cudaMemcpyDeviceToHost, stream_), "hpwl");
@@ -438,14 +478,18 @@ int64_t Engine::hpwl() {
 }
 
 void Engine::centres(std::vector<int32_t> &dcx, std::vector<int32_t> &dcy) {
-  dcx.resize(n_cells_);
-  dcy.resize(n_cells_);
+  std::vector<int2> dc(n_cells_);
   if (n_cells_) {
-    check(cudaMemcpyAsync(dcx.data(), dcx_, n_cells_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "centres");
-    check(cudaMemcpyAsync(dcy.data(), dcy_, n_cells_ * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "centres");
+    check(cudaMemcpyAsync(dc.data(), dc_, n_cells_ * sizeof(int2), cudaMemcpyDeviceToHost, stream_), "centres");
     d2h_bytes += n_cells_ * 8;
   }
   check(cudaStreamSynchronize(stream_), "centres sync");
+  dcx.resize(n_cells_);
+  dcy.resize(n_cells_);
+  for (int64_t i = 0; i < n_cells_; i++) {
+    dcx[i] = dc[i].x;
+    dcy[i] = dc[i].y;
+  }
 }
 
 void Engine::set_net_weights(const std::vector<float> &w) {

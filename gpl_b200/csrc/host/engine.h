@@ -13,6 +13,7 @@
 namespace gpl {
 
 struct PoissonPlan;
+struct WaArgs;
 
 // What the device needs of one region (a `NesterovBase`'s bin grid).
 struct RegionSetup {
@@ -124,17 +125,18 @@ class Engine {
   // globals
   int64_t n_cells_ = 0, n_pins_ = 0;
   int32_t n_nets_ = 0;
-  int32_t *dcx_ = nullptr, *dcy_ = nullptr, *hx_ = nullptr, *hy_ = nullptr;
+  int2 *dc_ = nullptr;
+  int32_t *hx_ = nullptr, *hy_ = nullptr;
   float *dscale_ = nullptr, *area_ = nullptr;
   uint8_t *kind_ = nullptr, *locked_ = nullptr;
   bool any_locked_ = false;
   int64_t *cell_pin_start_ = nullptr;
-  int32_t *cell_pins_ = nullptr;
   int64_t *net_start_ = nullptr;
-  int32_t *net_order_ = nullptr, *pin_cell_ = nullptr;
-  int2 *pin_base_ = nullptr;
+  int32_t *pin_cell_ = nullptr, *pin_slot_ = nullptr, *big_nets_ = nullptr;
+  int2 *pin_base_ = nullptr, *tiles_ = nullptr;
+  int32_t n_tiles_ = 0, n_big_ = 0;
   float *net_weight_ = nullptr;
-  float2 *pin_grad_ = nullptr;
+  float2 *pin_grad_ = nullptr;  // the WA force of every pin of a cell, cell-major (cell_pins order)
   unsigned long long *hpwl_acc_ = nullptr;
   // initial placement scratch
   void *ip_scratch_ = nullptr;
@@ -144,6 +146,7 @@ class Engine {
   float *ip_vals_ = nullptr, *ip_b_ = nullptr, *ip_x_ = nullptr;
   size_t ip_nnz_cap_ = 0, ip_n_cap_ = 0;
   void free_globals();
+  WaArgs wa_args() const;
   // profiling
   bool profile_ = false;
   std::vector<cudaEvent_t> ev_;

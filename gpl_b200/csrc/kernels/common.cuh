@@ -24,11 +24,26 @@ __device__ __forceinline__ float fast_exp(float x) {
   return e;
 }
 
+// Truncation and ceiling of the correctly rounded double quotient num / size. The product
+// with the rounded reciprocal `inv` is within 1e-15 (relative) of that quotient, so where no
+// integer lies within 1e-9 of the product both have the same truncation and ceiling; near
+// an integer the IEEE division itself decides.
+__device__ __forceinline__ int32_t quot_trunc(int32_t num, double size, double inv) {
+  double a = (double)num, q = __dmul_rn(a, inv);
+  if (fabs(q - rint(q)) > 1e-9 * fmax(fabs(q), 1.0)) return d2i_rz(q);
+  return d2i_rz(__ddiv_rn(a, size));
+}
+__device__ __forceinline__ int32_t quot_ceil(int32_t num, double size, double inv) {
+  double a = (double)num, q = __dmul_rn(a, inv);
+  if (fabs(q - rint(q)) > 1e-9 * fmax(fabs(q), 1.0)) return d2i_rz(ceil(q));
+  return d2i_rz(ceil(__ddiv_rn(a, size)));
+}
+
 // Bin span of [lo, hi) on an axis whose bins start at g0 and are `size` wide, clamped to
 // [0, cnt] (`BinGrid::density_idx_x`, src/nesterov.rs:275-284): the quotient in double.
-__device__ __forceinline__ void bin_span(int32_t lo, int32_t hi, int32_t g0, double size, int32_t cnt, int32_t &a, int32_t &b) {
-  a = d2i_rz(__ddiv_rn((double)(lo - g0), size));
-  b = d2i_rz(ceil(__ddiv_rn((double)(hi - g0), size)));
+__device__ __forceinline__ void bin_span(int32_t lo, int32_t hi, int32_t g0, double size, double inv, int32_t cnt, int32_t &a, int32_t &b) {
+  a = quot_trunc(lo - g0, size, inv);
+  b = quot_ceil(hi - g0, size, inv);
   a = a < 0 ? 0 : a;
   b = b > cnt ? cnt : b;
 }

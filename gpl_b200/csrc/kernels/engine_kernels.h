@@ -4,13 +4,20 @@
 #include <cstdint>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <vector>
 
 namespace gpl {
 
 constexpr int kThreadsPerBlock = 256;  // the block size every launch uses
 
 enum CellKind : uint8_t { CELL_STD = 0, CELL_MACRO = 1, CELL_FILLER = 2 };
-enum PlaceMode { PLACE_AT = 0, PLACE_NESTEROV = 1, PLACE_GIVEN = 2 };  // GIVEN: the centres in dcx/dcy
+enum PlaceMode { PLACE_AT = 0, PLACE_NESTEROV = 1, PLACE_GIVEN = 2 };  // GIVEN: the centres in dc
+
+// WA and HPWL run over tiles of consecutive nets (pins are net-major, so a tile's pins are
+// contiguous): at most kWaTilePins pins and kWaTileNets nets per tile, one block per tile.
+// A net with more pins than a tile holds runs in the thread-per-net kernels instead.
+constexpr int kWaTilePins = 512;
+constexpr int kWaTileNets = 256;
 
 // One region's bin grid (`BinGrid`, src/nesterov.rs:260-295) and its cell count.
 struct RegionArgs {
@@ -18,46 +25,56 @@ struct RegionArgs {
   int32_t nx, ny;
   int32_t lx, ly, ux, uy;        // the grid's box
   double size_x, size_y;
+  double inv_size_x, inv_size_y; // 1 / size, rounded (the bin span's fast path)
   float target_density;
   const int32_t *bx, *by;        // bin edges, nx+1 and ny+1
   const float *scaled;           // bin area * target density (float)
-  const int64_t *non_place, *non_place_u;
+  const float *non_place, *non_place_u;  // the fixed areas (int64) as float, as the density reads them
   int64_t *acc_inst, *acc_fill;  // scatter accumulators (cleared by the finalize)
   float *density, *field_x, *field_y;
 };
 
 // One region's cells, SoA, region-local index.
 struct CellArgs {
-  int32_t *dcx, *dcy;            // density centre (the integer box centre)
+  int2 *dc;                      // density centre (the integer box centre)
   const int32_t *hx, *hy;        // half density size
   const float *dscale;           // density scale
   const uint8_t *kind;           // CellKind
   const uint8_t *locked;         // may be NULL
   const float *area;             // (float)dx * (float)dy of the cell box, for the preconditioner
-  const int64_t *pin_start;      // the cell's pins (CSR, the cell's own order)
-  const int32_t *pins;
+  const int64_t *pin_start;      // the cell's pins (CSR, the cell's own order): its WA forces
   float2 *cur_slp, *cur_slp_sum, *next_slp, *next_slp_sum, *prev_slp, *prev_slp_sum, *cur, *next;
 };
 
 // The nets and pins (all regions): pins net-major.
 struct WaArgs {
-  int32_t n_nets;
+  int32_t n_nets;                // nets the thread-per-net kernels walk (net_order, or 0..n)
   const int64_t *net_start;
-  const int32_t *net_order;      // nets by degree (NULL: natural order)
+  const int32_t *net_order;      // NULL: natural order
   const float *net_weight;       // NULL: 1
-  const int32_t *pin_cell;       // global device cell index, -1 for a pin with no cell
+  const int32_t *pin_cell;       // global device cell index, -1 for a pin with no cell (NULL: none)
   const int2 *pin_base;          // offset from the cell's centre, or the fixed position
-  const int32_t *dcx, *dcy;      // global device cell centres
+  const int2 *dc;                // global device cell centres
+  const int32_t *pin_slot;       // where a pin's force goes (-1: nowhere); NULL: at the pin
   float2 *pin_grad;
+  int32_t n_tiles;               // tiles of consecutive nets: [first, last) per tile
+  const int2 *tiles;
 };
 
 __global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *coords);
 __global__ void k_bins_finalize(RegionArgs r, double *partials, __nv_bfloat16 *dens_split, int split_ld);
 __global__ void k_wa(WaArgs w, float cx, float cy);
+__global__ void k_wa_tiles(WaArgs w, float cx, float cy);
 __global__ void k_gradients(RegionArgs r, CellArgs c, const float2 *pin_grad, float penalty, float2 *out_sum,
                             const float2 *a1, const float2 *b1, const float2 *b2, double *partials);
 __global__ void k_prev_slp(RegionArgs r, CellArgs c, float coef);
 __global__ void k_hpwl(WaArgs w, unsigned long long *out);
+__global__ void k_hpwl_tiles(WaArgs w, unsigned long long *out);
+__global__ void k_pack_centres(int64_t n, const int32_t *x, const int32_t *y, int2 *out);
+
+// Tiles of consecutive nets (at most kWaTilePins pins and kWaTileNets nets each) and the nets
+// too large for a tile, from the nets' pin starts.
+void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int2> &tiles, std::vector<int32_t> &big);
 __global__ void k_hold_locked(RegionArgs r, CellArgs c);
 __global__ void k_reduce_partials(const double *partials, int nblk, int width, double *out);
 

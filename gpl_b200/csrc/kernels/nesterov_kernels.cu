@@ -76,21 +76,21 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
   }
   int32_t cx, cy;
   if (mode == PLACE_GIVEN) {
-    cx = c.dcx[i];
-    cy = c.dcy[i];
+    int2 d = c.dc[i];
+    cx = d.x;
+    cy = d.y;
   } else {
     cx = f2i_rz(p.x);
     cy = f2i_rz(p.y);
-    c.dcx[i] = cx;
-    c.dcy[i] = cy;
+    c.dc[i] = make_int2(cx, cy);
   }
   int32_t hx = c.hx[i], hy = c.hy[i];
   dlx = cx - hx;
   dux = cx + hx;
   dly = cy - hy;
   duy = cy + hy;
-  bin_span(dlx, dux, r.lx, r.size_x, r.nx, x0, x1);
-  bin_span(dly, duy, r.ly, r.size_y, r.ny, y0, y1);
+  bin_span(dlx, dux, r.lx, r.size_x, r.inv_size_x, r.nx, x0, x1);
+  bin_span(dly, duy, r.ly, r.size_y, r.inv_size_y, r.ny, y0, y1);
   scale = c.dscale[i];
   kind = c.kind[i];
   }
@@ -146,30 +146,33 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
 }
 
 // ---- bins: density and overflow (:2252-2262), accumulators cleared for the next scatter.
-// Optionally the density split into bf16 hi/lo for the tensor-core solver.
+// Optionally the density split into bf16 hi/lo for the tensor-core solver. Blocks walk whole
+// x rows (threads along y), so no index is divided.
 __global__ void k_bins_finalize(RegionArgs r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld) {
   __shared__ double sh[kThreads / 32];
-  int64_t n = (int64_t)r.nx * r.ny;
   double o_sum = 0.0, ou_sum = 0.0;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-    int64_t inst = r.acc_inst[k], fill = r.acc_fill[k];
-    r.acc_inst[k] = 0;
-    r.acc_fill[k] = 0;
-    float fi = __ll2float_rn(inst), fn = __ll2float_rn(r.non_place[k]), fnu = __ll2float_rn(r.non_place_u[k]);
-    float sc = r.scaled[k];
-    float d = __fdiv_rn(__fadd_rn(__fadd_rn(fi, __ll2float_rn(fill)), fn), sc);
-    r.density[k] = d;
-    if (dens_split) {
-      int64_t x = k / r.ny, y = k % r.ny;
-      __nv_bfloat16 hi = __float2bfloat16_rn(d);
-      __nv_bfloat16 lo = __float2bfloat16_rn(d - __bfloat162float(hi));
-      dens_split[x * split_ld + y] = hi;
-      dens_split[x * split_ld + r.ny + y] = lo;
+  for (int32_t x = blockIdx.x; x < r.nx; x += gridDim.x) {
+    const size_t row = (size_t)x * r.ny;
+    for (int32_t y = threadIdx.x; y < r.ny; y += blockDim.x) {
+      size_t k = row + y;
+      int64_t inst = r.acc_inst[k], fill = r.acc_fill[k];
+      r.acc_inst[k] = 0;
+      r.acc_fill[k] = 0;
+      float fi = __ll2float_rn(inst), fn = r.non_place[k], fnu = r.non_place_u[k];
+      float sc = r.scaled[k];
+      float d = __fdiv_rn(__fadd_rn(__fadd_rn(fi, __ll2float_rn(fill)), fn), sc);
+      r.density[k] = d;
+      if (dens_split) {
+        __nv_bfloat16 hi = __float2bfloat16_rn(d);
+        __nv_bfloat16 lo = __float2bfloat16_rn(d - __bfloat162float(hi));
+        dens_split[(size_t)x * split_ld + y] = hi;
+        dens_split[(size_t)x * split_ld + r.ny + y] = lo;
+      }
+      float o = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fn), sc));
+      float ou = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fnu), sc));
+      o_sum += (double)o;
+      ou_sum += (double)ou;
     }
-    float o = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fn), sc));
-    float ou = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fnu), sc));
-    o_sum += (double)o;
-    ou_sum += (double)ou;
   }
   double a = block_sum<kThreads>(o_sum, sh);
   double b = block_sum<kThreads>(ou_sum, sh);
@@ -188,10 +191,27 @@ __device__ __forceinline__ int2 pin_pos(const WaArgs &w, int64_t p) {
   int32_t cell = w.pin_cell ? w.pin_cell[p] : -1;
   int2 b = w.pin_base[p];
   if (cell >= 0) {
-    b.x += w.dcx[cell];
-    b.y += w.dcy[cell];
+    int2 d = w.dc[cell];
+    b.x += d.x;
+    b.y += d.y;
   }
   return b;
+}
+
+__device__ __forceinline__ void wa_store(const WaArgs &w, int64_t p, float2 g) {
+  int64_t at = w.pin_slot ? (int64_t)w.pin_slot[p] : p;
+  if (at >= 0) w.pin_grad[at] = g;
+}
+
+// One pin's force from its net's sums (getWireLengthGradientPinWA :2392-2414): each quotient
+// in double, rounded to float; gmin - gmax per axis, times the net weight.
+__device__ __forceinline__ float wa_term_min(float s, float sx, float v, float c, float q) {
+  double num = __dadd_rn(__dmul_rn((double)s, __dmul_rn((double)v, __dsub_rn(1.0, (double)__fmul_rn(c, q)))), (double)__fmul_rn(__fmul_rn(c, v), sx));
+  return __double2float_rn(__ddiv_rn(num, (double)__fmul_rn(s, s)));
+}
+__device__ __forceinline__ float wa_term_max(float s, float sx, float v, float c, float q) {
+  double num = __dsub_rn(__dmul_rn((double)s, __dmul_rn((double)v, __dadd_rn(1.0, (double)__fmul_rn(c, q)))), (double)__fmul_rn(__fmul_rn(c, v), sx));
+  return __double2float_rn(__ddiv_rn(num, (double)__fmul_rn(s, s)));
 }
 
 __global__ void k_wa(WaArgs w, float cx, float cy) {
@@ -261,7 +281,100 @@ __global__ void k_wa(WaArgs w, float cx, float cy) {
       double num = __dsub_rn(__dmul_rn((double)s_maxy, __dmul_rn((double)v, __dadd_rn(1.0, (double)__fmul_rn(cy, qy)))), (double)__fmul_rn(__fmul_rn(cy, v), s_ymaxy));
       gmax_y = __double2float_rn(__ddiv_rn(num, (double)__fmul_rn(s_maxy, s_maxy)));
     }
-    w.pin_grad[p] = make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt));
+    wa_store(w, p, make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt)));
+  }
+}
+
+// The same WA over a tile of consecutive nets, one block per tile, the pin work spread over
+// the block's threads and each net's sums still taken by one thread in pin order:
+//   1. pins' positions into shared memory (coalesced; one gather of the cell centre each);
+//   2. a thread per net: the net's box, and each pin's net;
+//   3. a thread per pin: the four exp terms (zero where the exponent is at or below -300,
+//      which leaves a sum unchanged: the reference skips those terms);
+//   4. a thread per net: the eight sums in pin order (the reference's float order);
+//   5. a thread per pin: its force.
+// The results are the thread-per-net kernel's bit for bit.
+__global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float cy) {
+  __shared__ int2 s_pos[kWaTilePins];
+  __shared__ float4 s_v[kWaTilePins];
+  __shared__ uint16_t s_pnet[kWaTilePins];
+  __shared__ int32_t s_nstart[kWaTileNets + 1];
+  __shared__ int4 s_box[kWaTileNets];
+  __shared__ float s_sum[8][kWaTileNets];
+  const int2 t = w.tiles[blockIdx.x];
+  const int32_t nn = t.y - t.x;
+  const int64_t p0 = w.net_start[t.x];
+  for (int j = threadIdx.x; j <= nn; j += blockDim.x) s_nstart[j] = (int32_t)(w.net_start[t.x + j] - p0);
+  __syncthreads();
+  const int32_t np = s_nstart[nn];
+  for (int j = threadIdx.x; j < np; j += blockDim.x) s_pos[j] = pin_pos(w, p0 + j);
+  __syncthreads();
+  for (int j = threadIdx.x; j < nn; j += blockDim.x) {
+    int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+    for (int32_t k = s_nstart[j]; k < s_nstart[j + 1]; k++) {
+      int2 q = s_pos[k];
+      lx = min(lx, q.x);
+      ly = min(ly, q.y);
+      ux = max(ux, q.x);
+      uy = max(uy, q.y);
+      s_pnet[k] = (uint16_t)j;
+    }
+    s_box[j] = make_int4(lx, ly, ux, uy);
+  }
+  __syncthreads();
+  const float BAR = -300.0f;
+  for (int j = threadIdx.x; j < np; j += blockDim.x) {
+    int2 q = s_pos[j];
+    int4 b = s_box[s_pnet[j]];
+    float emin_x = __fmul_rn((float)(b.x - q.x), cx), emax_x = __fmul_rn((float)(q.x - b.z), cx);
+    float emin_y = __fmul_rn((float)(b.y - q.y), cy), emax_y = __fmul_rn((float)(q.y - b.w), cy);
+    float4 v;
+    v.x = emin_x > BAR ? fast_exp(emin_x) : 0.0f;
+    v.y = emax_x > BAR ? fast_exp(emax_x) : 0.0f;
+    v.z = emin_y > BAR ? fast_exp(emin_y) : 0.0f;
+    v.w = emax_y > BAR ? fast_exp(emax_y) : 0.0f;
+    s_v[j] = v;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < nn; j += blockDim.x) {
+    float s_minx = 0, s_xminx = 0, s_maxx = 0, s_xmaxx = 0, s_miny = 0, s_yminy = 0, s_maxy = 0, s_ymaxy = 0;
+    for (int32_t k = s_nstart[j]; k < s_nstart[j + 1]; k++) {
+      int2 q = s_pos[k];
+      float4 v = s_v[k];
+      float qx = (float)q.x, qy = (float)q.y;
+      s_minx = __fadd_rn(s_minx, v.x);
+      s_xminx = __fadd_rn(s_xminx, __fmul_rn(qx, v.x));
+      s_maxx = __fadd_rn(s_maxx, v.y);
+      s_xmaxx = __fadd_rn(s_xmaxx, __fmul_rn(qx, v.y));
+      s_miny = __fadd_rn(s_miny, v.z);
+      s_yminy = __fadd_rn(s_yminy, __fmul_rn(qy, v.z));
+      s_maxy = __fadd_rn(s_maxy, v.w);
+      s_ymaxy = __fadd_rn(s_ymaxy, __fmul_rn(qy, v.w));
+    }
+    s_sum[0][j] = s_minx;
+    s_sum[1][j] = s_xminx;
+    s_sum[2][j] = s_maxx;
+    s_sum[3][j] = s_xmaxx;
+    s_sum[4][j] = s_miny;
+    s_sum[5][j] = s_yminy;
+    s_sum[6][j] = s_maxy;
+    s_sum[7][j] = s_ymaxy;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < np; j += blockDim.x) {
+    int2 q = s_pos[j];
+    float4 v = s_v[j];
+    int n = s_pnet[j];
+    int4 b = s_box[n];
+    float qx = (float)q.x, qy = (float)q.y;
+    float emin_x = __fmul_rn((float)(b.x - q.x), cx), emax_x = __fmul_rn((float)(q.x - b.z), cx);
+    float emin_y = __fmul_rn((float)(b.y - q.y), cy), emax_y = __fmul_rn((float)(q.y - b.w), cy);
+    float gmin_x = emin_x > BAR ? wa_term_min(s_sum[0][n], s_sum[1][n], v.x, cx, qx) : 0.0f;
+    float gmax_x = emax_x > BAR ? wa_term_max(s_sum[2][n], s_sum[3][n], v.y, cx, qx) : 0.0f;
+    float gmin_y = emin_y > BAR ? wa_term_min(s_sum[4][n], s_sum[5][n], v.z, cy, qy) : 0.0f;
+    float gmax_y = emax_y > BAR ? wa_term_max(s_sum[6][n], s_sum[7][n], v.w, cy, qy) : 0.0f;
+    float wt = w.net_weight ? w.net_weight[t.x + n] : 1.0f;
+    wa_store(w, p0 + j, make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt)));
   }
 }
 
@@ -276,15 +389,16 @@ __global__ void k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__
   if (i < r.n_cells) {
     float wlx = 0.0f, wly = 0.0f;
     for (int64_t k = c.pin_start[i]; k < c.pin_start[i + 1]; k++) {
-      float2 t = pin_grad[c.pins[k]];
+      float2 t = pin_grad[k];
       wlx = __fadd_rn(wlx, t.x);
       wly = __fadd_rn(wly, t.y);
     }
-    int32_t cx = c.dcx[i], cy = c.dcy[i], hx = c.hx[i], hy = c.hy[i];
+    int2 d = c.dc[i];
+    int32_t cx = d.x, cy = d.y, hx = c.hx[i], hy = c.hy[i];
     int32_t dlx = cx - hx, dux = cx + hx, dly = cy - hy, duy = cy + hy;
     int32_t x0, x1, y0, y1;
-    bin_span(dlx, dux, r.lx, r.size_x, r.nx, x0, x1);
-    bin_span(dly, duy, r.ly, r.size_y, r.ny, y0, y1);
+    bin_span(dlx, dux, r.lx, r.size_x, r.inv_size_x, r.nx, x0, x1);
+    bin_span(dly, duy, r.ly, r.size_y, r.inv_size_y, r.ny, y0, y1);
     float scale = c.dscale[i];
     float fx = 0.0f, fy = 0.0f;
     for (int32_t x = x0; x < x1; x++) {
@@ -353,7 +467,8 @@ __global__ void k_hpwl(WaArgs w, unsigned long long *__restrict__ out) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   long long h = 0;
   if (t < w.n_nets) {
-    int64_t b = w.net_start[t], e = w.net_start[t + 1];
+    int32_t n = w.net_order ? w.net_order[t] : t;
+    int64_t b = w.net_start[n], e = w.net_start[n + 1];
     int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
     for (int64_t p = b; p < e; p++) {
       int2 q = pin_pos(w, p);
@@ -367,6 +482,64 @@ __global__ void k_hpwl(WaArgs w, unsigned long long *__restrict__ out) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
   if ((threadIdx.x & 31) == 0 && h) atomicAdd(out, (unsigned long long)h);
+}
+
+// The HPWL over a tile of consecutive nets: pins' positions loaded by the whole block, a
+// thread per net for its box. Integer sums: the order does not matter.
+__global__ void __launch_bounds__(kThreads) k_hpwl_tiles(WaArgs w, unsigned long long *__restrict__ out) {
+  __shared__ int2 s_pos[kWaTilePins];
+  __shared__ int32_t s_nstart[kWaTileNets + 1];
+  const int2 t = w.tiles[blockIdx.x];
+  const int32_t nn = t.y - t.x;
+  const int64_t p0 = w.net_start[t.x];
+  for (int j = threadIdx.x; j <= nn; j += blockDim.x) s_nstart[j] = (int32_t)(w.net_start[t.x + j] - p0);
+  __syncthreads();
+  const int32_t np = s_nstart[nn];
+  for (int j = threadIdx.x; j < np; j += blockDim.x) s_pos[j] = pin_pos(w, p0 + j);
+  __syncthreads();
+  long long h = 0;
+  for (int j = threadIdx.x; j < nn; j += blockDim.x) {
+    int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+    for (int32_t k = s_nstart[j]; k < s_nstart[j + 1]; k++) {
+      int2 q = s_pos[k];
+      lx = min(lx, q.x);
+      ly = min(ly, q.y);
+      ux = max(ux, q.x);
+      uy = max(uy, q.y);
+    }
+    if (ux >= lx) h += ((long long)ux - lx) + ((long long)uy - ly);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+  if ((threadIdx.x & 31) == 0 && h) atomicAdd(out, (unsigned long long)h);
+}
+
+__global__ void k_pack_centres(int64_t n, const int32_t *__restrict__ x, const int32_t *__restrict__ y, int2 *__restrict__ out) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_int2(x[i], y[i]);
+}
+
+void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int2> &tiles, std::vector<int32_t> &big) {
+  tiles.clear();
+  big.clear();
+  int32_t first = 0;
+  auto close = [&](int32_t end) {
+    if (end > first) tiles.push_back(make_int2(first, end));
+  };
+  for (int32_t n = 0; n < n_nets; n++) {
+    int64_t deg = net_start[n + 1] - net_start[n];
+    if (deg > kWaTilePins) {
+      close(n);
+      big.push_back(n);
+      first = n + 1;
+      continue;
+    }
+    if (n - first + 1 > kWaTileNets || net_start[n + 1] - net_start[first] > kWaTilePins) {
+      close(n);
+      first = n;
+    }
+  }
+  close(n_nets);
 }
 
 // ---- the locked cells' next state (:2848-2859) and a deterministic reduction of partials.

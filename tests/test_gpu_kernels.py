@@ -36,11 +36,20 @@ def random_cells(rng, n, bx, by, macro_frac=0.02, filler_frac=0.2):
     return cx, cy, hx, hy, scale, kind
 
 
-@pytest.mark.parametrize("nx,ny", [(64, 64), (96, 40)])
-def test_density_scatter_bit_exact(L, nx, ny):
-    rng = np.random.default_rng(nx * 1000 + ny)
-    bx, by, sx, sy = grid(nx, ny, 123457.0, 76543.0, lx=1000, ly=-500)
-    cx, cy, hx, hy, sc, kind = random_cells(rng, 20000, bx, by)
+@pytest.mark.parametrize("nx,ny,aligned", [(64, 64, False), (96, 40, False), (64, 64, True), (40, 80, True)])
+def test_density_scatter_bit_exact(L, nx, ny, aligned):
+    rng = np.random.default_rng(nx * 1000 + ny + aligned)
+    if aligned:
+        # bins 1000 x 1250 DBU wide and cell edges on multiples of 250: many spans end exactly
+        # on a bin edge, where the bin index is decided by the division itself
+        bx, by, sx, sy = grid(nx, ny, nx * 1000.0, ny * 1250.0, lx=1000, ly=-500)
+        cx, cy, hx, hy, sc, kind = random_cells(rng, 20000, bx, by)
+        cx, cy, hx, hy = ((a // 250) * 250 for a in (cx, cy, hx, hy))
+        hx, hy = np.maximum(hx, 250).astype(np.int32), np.maximum(hy, 250).astype(np.int32)
+        cx, cy = cx.astype(np.int32), cy.astype(np.int32)
+    else:
+        bx, by, sx, sy = grid(nx, ny, 123457.0, 76543.0, lx=1000, ly=-500)
+        cx, cy, hx, hy, sc, kind = random_cells(rng, 20000, bx, by)
     td = np.float32(0.7)
     want_i = np.zeros(nx * ny, np.int64)
     want_f = np.zeros(nx * ny, np.int64)
@@ -61,6 +70,11 @@ def test_density_scatter_bit_exact(L, nx, ny):
 
 def random_nets(rng, n_nets, span=200000):
     deg = np.where(rng.random(n_nets) < 0.9, rng.integers(2, 6, n_nets), rng.integers(6, 65, n_nets))
+    # nets without pins and with one pin, and nets larger than one WA tile (512 pins)
+    deg[rng.integers(0, n_nets, 40)] = 0
+    deg[rng.integers(0, n_nets, 40)] = 1
+    deg[rng.integers(0, n_nets, 5)] = rng.integers(513, 3000, 5)
+    deg[-1] = 700
     start = np.concatenate([[0], np.cumsum(deg)]).astype(np.int64)
     npins = int(start[-1])
     xy = rng.integers(0, span, (npins, 2)).astype(np.int32)

@@ -125,6 +125,14 @@ def ours(a):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
     cfg = CONFIGS[a.config]
+    if a.initial_place_only:
+        # a profiling case: the command through the initial placement only
+        design = synth.generate(cfg["preset"])
+        t0 = time.perf_counter()
+        r = engine.global_placement(design, cfg["args"] + ["-skip_nesterov_place"], device=local)
+        print(json.dumps({"case": "initial placement only", "config": cfg["name"], "status": r["status"],
+                          "seconds": time.perf_counter() - t0, "seconds_initial_place": r["seconds_initial_place"]}))
+        return
     design = synth.generate(cfg["preset"], placed=a.start == "placed")
     log("design generated")
     C_cells = design.meta["cells"]
@@ -308,6 +316,8 @@ def main():
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp32"], help="the density solve timed as the headline")
     ap.add_argument("--start", default="ip", choices=["ip", "placed"],
                     help="time the loop after the initial placement, or from the generator's spread placement with the initial placement skipped (a short case for profiling)")
+    ap.add_argument("--initial-place-only", action="store_true",
+                    help="run the command through the initial placement once and print its time (a profiling case)")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

@@ -236,6 +236,8 @@ double normal(Mt19937 &eng, double mean, double sigma);
 std::pair<int32_t, int32_t> orient_point(int orient, int32_t x, int32_t y);
 Ip make_pins(const Design &d, const Common &c, const Vars &v);
 Ip do_bicgstab_place(Log &log, const Design &d, Common &c, const Vars &v, const IpVars &vars, const SolveFn &solve);
+class IpDevice;
+Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v, const IpVars &vars, IpDevice &dev);
 
 }  // namespace gpl
 

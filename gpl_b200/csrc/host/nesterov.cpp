@@ -15,6 +15,7 @@
 
 #include "../kernels/engine_kernels.h"
 #include "engine.h"
+#include "../kernels/b2b.h"
 #include "host.h"
 
 namespace gpl {
@@ -960,6 +961,13 @@ static Opts nesterov_opts(const std::map<std::string, std::string> &keys, const 
 // ---------------------------------------------------------------- the placer on the device
 // `NesterovPlace` with every per-cell vector on the device (Engine): the same decisions as
 // src/nesterov.rs, taken on the scalars the trial reads back.
+// The routability pass's state and services (the reference's RouteBase with its router).
+struct Routability {
+  RouteBase rb;
+  const gpl_router_t *router = nullptr;
+  const Common *common = nullptr;
+};
+
 struct Placer {
   Opts o;
   Engine &eng;
@@ -1305,6 +1313,8 @@ struct Placer {
     eng.copy_slot(b, S_SNAP_SLP, S_CUR_SLP);
     eng.copy_slot(b, S_SNAP_SLP_SUM, S_CUR_SLP_SUM);
     eng.copy_slot(b, S_SNAP_PREV_SLP_SUM, S_PREV_SLP_SUM);
+    has_snapshot.resize(nbs.size(), 0);
+    has_snapshot[b] = 1;
     nb.snapshot_density_penalty = nb.density_penalty;
     nb.snapshot_step_length = nb.step_length;
   }
@@ -1353,11 +1363,12 @@ struct Placer {
       reset_min_sum_overflow((int)b);
     }
   }
-  // isDiverged (src/nesterov.rs:3009-3052), routability off.
-  DivergeAction np_is_diverged(Log &log, LoopSnapshots &s, float &cur_a) {
+  // isDiverged (src/nesterov.rs:3009-3052).
+  DivergeAction np_is_diverged(Log &log, LoopSnapshots &s, float &cur_a, Routability *route) {
     num_region_diverged = 0;
     for (size_t b = 0; b < nbs.size(); b++) num_region_diverged += check_divergence(log, (int)b) ? 1 : 0;
-    if (num_region_diverged == 0 && is_min_hpwl && !o.disable_revert_if_diverge) {
+    bool routability_off = !o.routability || !routability_need;
+    if (num_region_diverged == 0 && is_min_hpwl && !o.disable_revert_if_diverge && routability_off) {
       s.diverge_coef[0] = wl_coef_x;
       s.diverge_coef[1] = wl_coef_y;
       s.diverge_hpwl = min_hpwl;
@@ -1366,6 +1377,10 @@ struct Placer {
     }
     if (num_region_diverged == 0) return DivergeAction::None;
     log.report(sfmt("Divergence occured in %d regions.", num_region_diverged));
+    if (!o.disable_revert_if_diverge && try_routability_diverge_recovery(log, s, cur_a, route)) {
+      num_region_diverged = 0;
+      return DivergeAction::Resume;
+    }
     switch (diverge_fallback(s, o.disable_revert_if_diverge)) {
       case DivergeFallback::RevertAndResume:
         s.diverge_reverts++;
@@ -1386,7 +1401,298 @@ struct Placer {
         return DivergeAction::Stop;
     }
   }
-  bool check_convergence(Log &log, const Design &d, int b, int iter) {  // src/nesterov.rs:3107-3159
+  // ---- routability (src/nesterov.rs:3771-4093). It runs between device iterations on the
+  // host's copy of the state: pull_state() brings the device's coordinate slots and density
+  // centres into the regions' per-cell vectors (in each region's own cell order), the
+  // reference's host logic resizes cells, removes or restores fillers and moves target
+  // densities, and push_state() rebuilds the device from the result.
+  bool routability_need = true;
+  int routability_settle_wait_start_iter = -1;
+  std::vector<std::pair<int32_t, int32_t>> min_rc_cell_size;
+  std::vector<uint8_t> has_snapshot;  // per region: the snapshot slots hold a saved snapshot
+  std::vector<FloatPoint> *slot_vec(Nb &nb, int k) {
+    std::vector<FloatPoint> *v[12] = {&nb.cur_slp, &nb.cur_slp_sum, &nb.next_slp, &nb.next_slp_sum, &nb.prev_slp, &nb.prev_slp_sum, &nb.cur, &nb.next, &nb.snapshot, &nb.snapshot_slp, &nb.snapshot_slp_sum, &nb.snapshot_prev_slp_sum};
+    return v[k];
+  }
+  static SlotId slot_id(int k) {
+    static const SlotId ids[12] = {S_CUR_SLP, S_CUR_SLP_SUM, S_NEXT_SLP, S_NEXT_SLP_SUM, S_PREV_SLP, S_PREV_SLP_SUM, S_CUR, S_NEXT, S_SNAP_CUR, S_SNAP_SLP, S_SNAP_SLP_SUM, S_SNAP_PREV_SLP_SUM};
+    return ids[k];
+  }
+  void pull_state() {
+    sync_host_centres();
+    has_snapshot.resize(nbs.size(), 0);
+    for (size_t b = 0; b < nbs.size(); b++) {
+      Nb &nb = nbs[b];
+      size_t n = nb.cells.size();
+      for (int k = 0; k < 12; k++) {
+        std::vector<FloatPoint> *v = slot_vec(nb, k);
+        if (k >= 8 && !has_snapshot[b]) {
+          v->clear();
+          continue;
+        }
+        std::vector<float> xy = eng.get_coords((int)b, slot_id(k));
+        device_check();
+        v->assign(n, FloatPoint{});
+        for (size_t i = 0; i < n; i++) {
+          int64_t dv = dev_of_gcell[nb.cells[i]] - nb.cell_off;
+          (*v)[i] = FloatPoint{xy[2 * dv], xy[2 * dv + 1]};
+        }
+      }
+      // the gradient's two parts are not kept on the device; sized for the filler moves
+      for (auto *v : {&nb.cur_slp_wl, &nb.cur_slp_den, &nb.next_slp_wl, &nb.next_slp_den, &nb.prev_slp_wl, &nb.prev_slp_den}) v->resize(n);
+    }
+  }
+  void push_state();  // after engine_setup (below)
+  bool is_std_instance(int gi) const { return gcells[gi].is_instance() && !gcells[gi].macro_; }
+  void set_target_density(int b, float density) {  // src/nesterov.rs:3795-3802
+    nbs[b].target_density = density;
+    for (auto &bin : nbs[b].bg.bins) bin.target_density = density;
+    update_bins_non_place_area(nbs[b]);
+  }
+  void update_areas(int b) {  // src/nesterov.rs:3805-3821
+    int64_t st = 0, mac = 0;
+    for (int gi : nbs[b].cells) {
+      const GCell &g = gcells[gi];
+      if (!g.is_instance()) continue;
+      int64_t a = (int64_t)g.dx() * (int64_t)g.dy();
+      if (g.macro_)
+        mac += a;
+      else
+        st += a;
+    }
+    nbs[b].std_insts_area = st;
+    nbs[b].macro_insts_area = mac;
+  }
+  void update_density_size_nb(int b) {
+    for (int gi : nbs[b].cells) update_density_size_one(gcells[gi], nbs[b]);
+  }
+  // `cutFillerCells` (src/nesterov.rs:3826-3869).
+  void cut_filler_cells(Log &log, const Design &d, int b, int64_t inflation_area) {
+    if (inflation_area < 0) {
+      log.warn("GPL", 313, "Negative area provided to remove fillers: " + rust_f64(dbu_area(d, (double)inflation_area)) + ". Expected positive value, ignoring.");
+      return;
+    }
+    int64_t single = (int64_t)nbs[b].filler_dx * (int64_t)nbs[b].filler_dy;
+    int64_t max_remove = std::min(inflation_area / single, nbs[b].fillers);
+    int64_t available = single * nbs[b].fillers;
+    int64_t removed = 0;
+    int64_t i = (int64_t)nbs[b].cells.size() - 1;
+    while (i >= 0 && removed < max_remove) {
+      int gi = nbs[b].cells[i];
+      if (gcells[gi].is_filler()) {
+        RemovedFiller f = nbs[b].swap_pop((size_t)i);
+        nbs[b].removed_fillers.push_back(f);
+        nbs[b].fillers--;
+        available -= single;
+        removed++;
+      }
+      i--;
+    }
+    nbs[b].total_filler_area = available;
+    Nb &nb = nbs[b];
+    if (single * nb.fillers != nb.total_filler_area) log.warn("GPL", 312, "Unexpected filler area! The value " + rust_f64(dbu_area(d, (double)(single * nb.fillers))) + ", should be equal to totalFillerArea_ " + rust_f64(dbu_area(d, (double)nb.total_filler_area)) + ".");
+    int64_t removed_area = single * removed;
+    int64_t remaining = inflation_area - removed_area;
+    if (remaining > single) {
+      int64_t total = nesterov_insts_area(nb) + removed_area + nb.total_filler_area + remaining;
+      float density = (float)total / (float)nb.white_space_area;
+      set_target_density(b, density);
+      nbs[b].movable_area = f2l((float)nbs[b].white_space_area * nbs[b].target_density);
+    }
+  }
+  // `restoreRemovedFillers` (src/nesterov.rs:3873-3892).
+  void restore_removed_fillers(int b) {
+    Nb &nb = nbs[b];
+    if (nb.removed_fillers.empty()) return;
+    int64_t single = (int64_t)nb.filler_dx * (int64_t)nb.filler_dy;
+    std::vector<RemovedFiller> removed;
+    std::swap(removed, nb.removed_fillers);
+    for (auto &f : removed) {
+      nb.push_back(f);
+      nb.fillers++;
+      nb.total_filler_area += single;
+    }
+  }
+  // `applyNetWeights` (src/nesterov.rs:3926-3939): no net is reweighted (weights of 1), which
+  // the device's net weights already hold after a rebuild.
+  void apply_net_weights(const RouteBase &) {}
+  // `revertToMinCongestion` (src/nesterov.rs:3897-3922).
+  void revert_to_min_congestion(Log &log, RouteBase &rb) {
+    if (rb.revert_count < 1) return;
+    float first = rb.min_rc_target_density.empty() ? 0.0f : rb.min_rc_target_density[0];
+    log.info("GPL", 55, sfmt("Reverting inflation and target density to the pass with the minimum observed routing congestion (%.4f), target density %.4f.", (double)rb.min_rc, (double)first));
+    for (size_t gi = 0; gi < gcells.size(); gi++)
+      if (is_std_instance((int)gi)) set_size(gcells[gi], min_rc_cell_size[gi].first, min_rc_cell_size[gi].second);
+    for (size_t b = 0; b < nbs.size(); b++) {
+      set_target_density((int)b, rb.min_rc_target_density[b]);
+      restore_removed_fillers((int)b);
+      update_density_size_nb((int)b);
+      rb.accumulated[b] = rb.min_rc_inflated[b];
+    }
+    apply_net_weights(rb);
+    rb.reset_resources();
+  }
+  // `scaleInflationToBudget` (src/nesterov.rs:3945-3975).
+  bool scale_inflation_to_budget(RouteBase &rb) {
+    if (rb.original_movable_area <= 0) return false;
+    double budget = (double)rb.original_movable_area * (double)rb.vars.max_inflation_total;
+    double spent = (double)rb.total_inflation();
+    double allowed = std::min(budget / 6.0, budget - spent);
+    double wanted = 0.0;
+    for (auto &nb : nbs)
+      for (int gi : nb.cells) {
+        if (!is_std_instance(gi)) continue;
+        const GCell &g = gcells[gi];
+        float ratio;
+        if (!rb.inflated_ratio_at(g.d_cx(), g.d_cy(), ratio)) continue;
+        if ((double)ratio <= 1.0) continue;
+        wanted += (double)g.dx() * (double)g.dy() * ((double)ratio - 1.0);
+      }
+    if (wanted <= 0.0 || wanted <= allowed) return spent + wanted >= budget;
+    double scale = std::fmax(0.0, allowed / wanted);
+    rb.scale_inflated(scale);
+    return spent + allowed >= budget;
+  }
+  std::vector<std::pair<int32_t, int32_t>> std_centres() const {
+    std::vector<std::pair<int32_t, int32_t>> out;
+    for (auto &nb : nbs)
+      for (int gi : nb.cells) {
+        const GCell &g = gcells[gi];
+        if (g.is_instance() && !g.macro_) out.push_back({g.d_cx(), g.d_cy()});
+      }
+    return out;
+  }
+  // `placed_locations` (src/nesterov.rs:4099-4110) from the host's density centres.
+  std::vector<std::array<int32_t, 3>> host_locations(const Common &c) const {
+    std::vector<std::array<int32_t, 3>> out;
+    for (auto &g : gcells) {
+      if (g.inst < 0) continue;
+      const Instance &i = c.insts[g.inst];
+      out.push_back({i.db, g.d_cx() - i.dx() / 2 + c.site_x * o.pad_left, g.d_cy() - i.dy() / 2});
+    }
+    return out;
+  }
+  // `RouteBase::routability` (src/nesterov.rs:3985-4093) on the pulled state.
+  std::pair<bool, bool> routability(Log &log, const Design &d, Routability &r, int revert_count) {
+    float cur_rc = r.rb.measure(log, r.router, host_locations(*r.common), std_centres());
+    RouteVars v = r.rb.vars;
+    if (cur_rc < v.target_rc) {
+      log.info("GPL", 50, sfmt("Weighted routing congestion is lower than target routing congestion(%.4f), end routability optimization.", (double)v.target_rc));
+      r.rb.reset_resources();
+      return {false, false};
+    }
+    if ((r.rb.min_rc - cur_rc) > r.rb.min_rc * 0.005f) {
+      log.info("GPL", 48, "Congestion improved on previous minimum (" + fmt_g_prec((double)r.rb.min_rc, 4) + "); updating minimum.");
+      r.rb.min_rc = cur_rc;
+      r.rb.min_rc_violated = 0;
+      for (size_t b = 0; b < nbs.size(); b++) {
+        r.rb.min_rc_target_density[b] = nbs[b].target_density;
+        nbs[b].removed_fillers.clear();
+      }
+      for (size_t gi = 0; gi < gcells.size(); gi++)
+        if (is_std_instance((int)gi)) min_rc_cell_size[gi] = {gcells[gi].dx(), gcells[gi].dy()};
+      r.rb.min_rc_inflated = r.rb.accumulated;
+    } else {
+      r.rb.min_rc_violated++;
+      log.info("GPL", 49, sfmt("No improvement on minimum (%.4f); consecutive non-improvement count: %d.", (double)r.rb.min_rc, r.rb.min_rc_violated));
+    }
+    r.rb.set_inflated_ratios();
+    bool budget_spent = scale_inflation_to_budget(r.rb);
+    size_t n = nbs.size();
+    for (size_t b = 0; b < n; b++) {
+      r.rb.inflated_delta[b] = 0;
+      for (size_t k = 0; k < nbs[b].cells.size(); k++) {
+        int gi = nbs[b].cells[k];
+        if (!is_std_instance(gi)) continue;
+        const GCell &g = gcells[gi];
+        float ratio;
+        if (!r.rb.inflated_ratio_at(g.d_cx(), g.d_cy(), ratio)) continue;
+        if ((double)ratio <= 1.0) continue;
+        int64_t prev = (int64_t)g.dx() * (int64_t)g.dy();
+        float root = std::sqrt(ratio);
+        int32_t nx = f2i(std::round((float)g.dx() * root)), ny = f2i(std::round((float)g.dy() * root));
+        set_size(gcells[gi], nx, ny);
+        r.rb.inflated_delta[b] += (int64_t)gcells[gi].dx() * (int64_t)gcells[gi].dy() - prev;
+      }
+      r.rb.accumulated[b] += r.rb.inflated_delta[b];
+      int64_t delta = r.rb.inflated_delta[b];
+      float pct = ((float)delta / (float)nesterov_insts_area(nbs[b])) * 100.0f;
+      float delta_um2 = (float)dbu_area(d, (double)delta);
+      cut_filler_cells(log, d, (int)b, delta);
+      {
+        const Nb &nb = nbs[b];
+        double spent = r.rb.original_movable_area > 0 ? 100.0 * (double)r.rb.total_inflation() / (double)r.rb.original_movable_area : 0.0;
+        std::string group = nb.group >= 0 ? " in group " + nb.group_name : "";
+        log.info("GPL", 86, sfmt("Inflation %+.3f um^2 (%+.2f%% of movable), %.2f%% of the %.2f%% budget spent; target density %.4f%s.", (double)delta_um2, (double)pct, spent, 100.0 * (double)v.max_inflation_total, (double)nb.target_density, group.c_str()));
+      }
+      if (nbs[b].target_density > v.max_density) {
+        const Nb &nb = nbs[b];
+        std::string group = nb.group >= 0 ? " in group " + nb.group_name : "";
+        log.info("GPL", 53, sfmt("Target density %.4f exceeds the maximum allowed %.4f%s.", (double)nb.target_density, (double)v.max_density, group.c_str()));
+        revert_to_min_congestion(log, r.rb);
+        return {false, true};
+      }
+    }
+    if (revert_count >= 50) {
+      log.info("GPL", 91, sfmt("Routability mode reached the maximum allowed reverts %d", revert_count));
+      revert_to_min_congestion(log, r.rb);
+      return {false, true};
+    }
+    if (r.rb.min_rc_violated >= 3) {
+      log.info("GPL", 54, sfmt("No improvement in routing congestion for %d consecutive iterations (limit is %d).", r.rb.min_rc_violated, 3));
+      revert_to_min_congestion(log, r.rb);
+      return {false, true};
+    }
+    for (size_t b = 0; b < n; b++) {
+      update_areas((int)b);
+      update_density_size_nb((int)b);
+    }
+    if (v.net_weight_max > 1.0f && v.congested_nets_percentage > 0.0f) refuse("routability net reweighting (-routability_net_weight_max above 1) is not modelled");
+    apply_net_weights(r.rb);
+    r.rb.reset_resources();
+    if (budget_spent) {
+      log.info("GPL", 97, sfmt("Total routability inflation %.2f%% of the movable area spent the %.2f%% budget, ending routability.", 100.0 * (double)r.rb.total_inflation() / (double)r.rb.original_movable_area, 100.0 * (double)r.rb.vars.max_inflation_total));
+      revert_to_min_congestion(log, r.rb);
+    }
+    return {!budget_spent, true};
+  }
+  // `tryRoutabilityDivergeRecovery` (src/nesterov.rs:3061-3088).
+  bool try_routability_diverge_recovery(Log &log, LoopSnapshots &s, float &cur_a, Routability *route) {
+    int attempt = routability_recovery_attempt(s, routability_need);
+    if (attempt == 0) return false;
+    s.route_attempts = attempt;
+    bool last = s.route_attempts == MAX_ROUTABILITY_DIVERGE_ATTEMPTS;
+    if (routability_need && route) {
+      pull_state();
+      revert_to_min_congestion(log, route->rb);
+      push_state();
+    }
+    if (last) routability_need = false;
+    log.warn("GPL", 112, sfmt("Divergence detected, reverting to the routability snapshot (attempt %d of %d), further inflation %s.", s.route_attempts, MAX_ROUTABILITY_DIVERGE_ATTEMPTS, last ? "disabled" : "still allowed"));
+    wl_coef_x = s.route_coef[0];
+    wl_coef_y = s.route_coef[1];
+    wa();
+    for (size_t b = 0; b < nbs.size(); b++) {
+      revert_to_snapshot((int)b);
+      reset_min_sum_overflow((int)b);
+    }
+    cur_a = 1.0f;
+    routability_settle_wait_start_iter = -1;
+    min_hpwl = INT64_MAX;
+    is_min_hpwl = false;
+    return true;
+  }
+  bool is_placement_settled() const {
+    for (auto &nb : nbs)
+      if (!(nb.peak_coordi_distance > 0.0f && nb.coordi_distance <= SETTLE_FRACTION * nb.peak_coordi_distance)) return false;
+    return true;
+  }
+  float worst_settle_ratio() const {
+    float w = 0.0f;
+    for (auto &nb : nbs) w = fmaxr(w, nb.peak_coordi_distance <= 0.0f ? 1.0f : nb.coordi_distance / nb.peak_coordi_distance);
+    return w;
+  }
+  bool check_convergence(Log &log, const Design &d, int b, int iter, Routability *route, int route_iters) {  // src/nesterov.rs:3107-3159
     if (nbs[b].is_converged) return true;
     if (nbs[b].sum_overflow_unscaled > o.overflow) return false;
     int64_t h = hpwl();
@@ -1395,8 +1701,16 @@ struct Placer {
     log.report("---------------------------------------------------------------");
     if (nb.group >= 0)
       log.info("GPL", 1016, sfmt("Region '%s' placement finished at iteration %d", nb.group_name.c_str(), iter));
-    else
+    else {
       log.info("GPL", 1001, sfmt("Global placement finished at iteration %d", iter));
+      if (o.routability) log.info("GPL", 1017, sfmt("Routability mode iteration count: %d", route_iters));
+    }
+    if (route) {
+      sync_host_centres();
+      route->rb.calculate_rudy_tiles(route->router, host_locations(*route->common), std_centres());
+      route->rb.update_rudy_average();
+      log.info("GPL", 1005, sfmt("Routability final weighted congestion: %.4f", (double)route->rb.final_average_rc));
+    }
     int64_t nia = nesterov_insts_area(nb);
     log.info("GPL", 1002, sfmt("Placed Cell Area            %10.4f", dbu_area(d, (double)nia)));
     log.info("GPL", 1003, sfmt("Available Free Area         %10.4f", dbu_area(d, (double)nb.white_space_area)));
@@ -1407,6 +1721,8 @@ struct Placer {
     log.info("GPL", 1008, sfmt("    - For 80%% usage of free space: %.4f", (double)nia / (w * 0.80)));
     if ((double)nia / (w * 0.50) <= 1.0) log.info("GPL", 1009, sfmt("    - For 50%% usage of free space: %.4f", (double)nia / (w * 0.50)));
     if (nb.uniform_target_density > 0.95f) log.warn("GPL", 1015, sfmt("High uniform density (>%.2f) may cause congestion or legalization issues.", (double)nb.uniform_target_density));
+    for (int gi : nbs[b].cells)
+      if (gcells[gi].is_instance()) gcells[gi].locked = true;
     nbs[b].is_converged = true;
     return true;
   }
@@ -1513,7 +1829,7 @@ static RegionSetup region_setup(const Nb &nb) {
 }
 
 // The device's view of the placer: cells in region order, pins net-major.
-static EngineSetup engine_setup(Placer &P) {
+static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
   EngineSetup s;
   P.dev_of_gcell.assign(P.gcells.size(), -1);
   P.gcell_of_dev.clear();
@@ -1566,8 +1882,9 @@ static EngineSetup engine_setup(Placer &P) {
     s.locked[dv] = g.locked ? 1 : 0;
     s.dcx[dv] = g.d_cx();
     s.dcy[dv] = g.d_cy();
-    // a cell's pins sit where the placer copied them (before the perturbation)
-    if (!g.pins.empty()) {
+    // a cell's pins sit where the placer copied them (before the perturbation); a rebuild
+    // keeps the current centres
+    if (!rebuild && !g.pins.empty()) {
       const GPin &q = P.gpins[g.pins[0]];
       s.dcx[dv] = q.cx - q.off_x;
       s.dcy[dv] = q.cy - q.off_y;
@@ -1602,12 +1919,37 @@ static EngineSetup engine_setup(Placer &P) {
   return s;
 }
 
-// `resume_nesterov_place` (src/nesterov.rs:4440-4610) from iteration 0, routability off, cut
-// into its prologue, one loop iteration at a time, and its epilogue (so a caller can step it).
+// The device rebuilt from the host's state (after a routability change): cells, pins and bins
+// uploaded again, the coordinate slots written back in the new device order.
+void Placer::push_state() {
+  eng.upload(engine_setup(*this, true));
+  device_check();
+  for (size_t b = 0; b < nbs.size(); b++) {
+    Nb &nb = nbs[b];
+    size_t n = nb.cells.size();
+    for (int k = 0; k < 12; k++) {
+      std::vector<FloatPoint> *v = slot_vec(nb, k);
+      if (v->size() != n) continue;  // a snapshot never saved stays zero
+      std::vector<float> xy(2 * n);
+      for (size_t i = 0; i < n; i++) {
+        int64_t dv = dev_of_gcell[nb.cells[i]] - nb.cell_off;
+        xy[2 * dv] = (*v)[i].x;
+        xy[2 * dv + 1] = (*v)[i].y;
+      }
+      eng.set_coords((int)b, slot_id(k), xy);
+    }
+  }
+  device_check();
+  hpwl_dirty = true;
+}
+
+// `resume_nesterov_place` (src/nesterov.rs:4440-4610) from iteration 0, cut into its
+// prologue, one loop iteration at a time, and its epilogue (so a caller can step it).
 struct NesterovLoop {
   LoopSnapshots snaps;
   float cur_a = 1.0f;
   int iter = 0;
+  int route_iters = 0, route_reverts = 0;
   int64_t original_area = 0;
   bool done = false;
 
@@ -1623,7 +1965,7 @@ struct NesterovLoop {
     }
   }
   // One pass of the loop's body; false once the loop has ended.
-  bool step(Log &log, const Design &d, Placer &P) {
+  bool step(Log &log, const Design &d, Placer &P, Routability *route) {
     if (done || iter >= P.max_iter) return !(done = true);
     if (iter % 50 == 0) progress("iteration %d: overflow %.4f, %ld trials", iter, (double)P.average_overflow_unscaled, (long)P.trials);
     float prev_a = cur_a;
@@ -1633,24 +1975,81 @@ struct NesterovLoop {
     for (size_t b = 0; b < P.nbs.size(); b++) P.nesterov_adjust_phi((int)b);
     if (P.num_region_diverged > 0) return !(done = true);
     P.np_update_next_iter(log, d, iter);
-    DivergeAction act = P.np_is_diverged(log, snaps, cur_a);
+    bool routability = P.o.routability;
+    bool routability_gpl_iter = snaps.route_saved && P.average_overflow_unscaled > P.o.routability_end_overflow;
+    if (routability_gpl_iter) {
+      route_iters++;
+      P.max_iter++;
+    }
+    DivergeAction act = P.np_is_diverged(log, snaps, cur_a, route);
     if (act == DivergeAction::Stop) return !(done = true);
     if (act == DivergeAction::Resume) {
       iter++;
       return true;
     }
+    if (routability && !snaps.route_saved && P.o.routability_snapshot_overflow >= P.average_overflow_unscaled) {
+      snaps.route_coef[0] = P.wl_coef_x;
+      snaps.route_coef[1] = P.wl_coef_y;
+      snaps.route_a = cur_a;
+      snaps.route_saved = true;
+      for (size_t b = 0; b < P.nbs.size(); b++) P.save_snapshot((int)b);
+      log.info("GPL", 38, sfmt("Routability snapshot saved at iter = %d", iter + 1));
+      int64_t h = P.hpwl();
+      log.report(sfmt("%9d | %8.4f | %s | %-8s | %-9s | %5s", iter, (double)P.average_overflow_unscaled, fmt_e((double)h / (double)d.dbu, 6, 13).c_str(), " ", " ", " "));
+    }
+    if (route) {
+      bool active = P.routability_need && P.average_overflow_unscaled <= P.o.routability_end_overflow;
+      bool settled = active && P.is_placement_settled();
+      int extra = 0;
+      auto [start, event] = settle_wait_step(P.routability_settle_wait_start_iter, iter, active, settled, extra);
+      P.routability_settle_wait_start_iter = start;
+      if (event == 1)
+        log.info("GPL", 99, sfmt("Routability end extended at iter = %d: overflow %.4f reached %.4f, but cells are still moving at %.0f%% of peak displacement (waiting for %.0f%%).", iter + 1, (double)P.average_overflow_unscaled, (double)P.o.routability_end_overflow, (double)(P.worst_settle_ratio() * 100.0f), (double)(SETTLE_FRACTION * 100.0f)));
+      else if (event == 2)
+        log.info("GPL", 103, sfmt("Routability end extension finished at iter = %d after %d extra iterations: overflow %.4f, cells moving at %.0f%% of peak displacement.", iter + 1, extra, (double)P.average_overflow_unscaled, (double)(P.worst_settle_ratio() * 100.0f)));
+      if (settled) {
+        P.nbs[0].reprint_header = true;
+        route_reverts++;
+        progress("routability pass %d at iteration %d", route_reverts, iter);
+        P.pull_state();
+        auto [need, revert_init] = P.routability(log, d, *route, route_reverts);
+        P.routability_need = need;
+        P.min_hpwl = INT64_MAX;
+        P.is_min_hpwl = false;
+        if (need || revert_init) {
+          P.push_state();
+          cur_a = snaps.route_a;
+          P.wl_coef_x = snaps.route_coef[0];
+          P.wl_coef_y = snaps.route_coef[1];
+          P.wa();
+          for (size_t b = 0; b < P.nbs.size(); b++) {
+            P.revert_to_snapshot((int)b);
+            P.reset_min_sum_overflow((int)b);
+          }
+        }
+        if (need && revert_init) log.info("GPL", 87, "Routability end iteration: increase inflation and revert back to snapshot.");
+        if (!need && revert_init) log.info("GPL", 89, "Routability finished. Reverting to minimal observed routing congestion, could not reach target.");
+        if (!need && !revert_init) log.info("GPL", 90, "Routability finished. Target routing congestion achieved succesfully.");
+      }
+    }
     int converged = 0;
-    for (size_t b = 0; b < P.nbs.size(); b++) converged += P.check_convergence(log, d, (int)b, iter) ? 1 : 0;
+    for (size_t b = 0; b < P.nbs.size(); b++) converged += P.check_convergence(log, d, (int)b, iter, route, route_iters) ? 1 : 0;
     if (converged == (int)P.nbs.size()) return !(done = true);
     iter++;
     return true;
   }
-  int end(Log &log, const Design &d, Placer &P) {
+  int end(Log &log, const Design &d, Placer &P, Routability *route) {
     if (max_iter_takes_min_hpwl_snapshot(iter, P.max_iter, P.o.disable_revert_if_diverge, snaps, P.diverge_snapshot_overflow, P.average_overflow_unscaled, P.hpwl())) {
       log.warn("GPL", 121, "Reached the maximum number of iterations, reverting to snapshot with min hpwl.");
       P.revert_to_diverge_snapshot(log, snaps);
     }
     if (iter >= P.max_iter) log.warn("GPL", 1010, sfmt("GPL reached the maximum number of iterations for nesterov %d. Placement may have failed to converge.", P.max_iter));
+    if (route) log.info("GPL", 1011, sfmt("Original area (um^2): %.2f", dbu_area(d, (double)original_area)));
+    if (route) {
+      int64_t inflation = route->rb.total_inflation();
+      float pct = (float)(100.0 * (double)inflation / (double)original_area);
+      log.info("GPL", 1012, sfmt("Total routability artificial inflation: %.2f (%+.2f%%)", dbu_area(d, (double)inflation), (double)pct));
+    }
     int64_t new_area = 0;
     for (auto &nb : P.nbs) new_area += nesterov_insts_area(nb);
     float diff = (float)(100.0 * (double)(new_area - original_area) / (double)original_area);
@@ -1698,6 +2097,7 @@ struct Run {
   std::vector<Base> bases;
   Ip ip;
   std::unique_ptr<Placer> P;
+  std::unique_ptr<Routability> route;
   NesterovLoop loop;
   bool nesterov = false;
   bool ended = false;
@@ -1740,10 +2140,7 @@ struct Run {
     bool skip_nesterov = flag("-skip_nesterov_place");
     Opts o;
     if (!skip_nesterov) o = nesterov_opts(keys, flags, vars);
-    if (o.routability) {
-      if (!router) refuse("-routability_driven / -timing_driven need the design database");
-      refuse("-routability_driven on the device is not built yet");
-    }
+    if (o.routability && !router) refuse("-routability_driven / -timing_driven need the design database");
     bool has_core_row = false;
     for (auto &r : d.rows)
       if (!r.pad) has_core_row = true;
@@ -1758,13 +2155,13 @@ struct Run {
     }
     progress("placer built: %zu instances, %zu nets, %zu bases", c.insts.size(), c.nets.size(), bases.size());
     auto t0 = std::chrono::steady_clock::now();
-    Engine &E = eng;
-    SolveFn solve = [&E](const Csr &m, const std::vector<float> &rhs, std::vector<float> &x, int max_iters) {
-      Solve s = E.solve(m, rhs, x, max_iters);
-      if (E.failed()) throw std::runtime_error("device: " + std::string(cudaGetErrorString(E.error().code)) + " in " + E.error().where);
-      return s;
-    };
-    ip = do_bicgstab_place(log, d, c, vars, ipv, solve);
+    {
+      IpDevice dev(eng.stream());
+      ip = do_bicgstab_place_device(log, d, c, vars, ipv, dev);
+      eng.launches += dev.launches;
+      eng.h2d_bytes += dev.h2d_bytes;
+      eng.d2h_bytes += dev.d2h_bytes;
+    }
     auto t1 = std::chrono::steady_clock::now();
     res.t_ip = std::chrono::duration<double>(t1 - t0).count();
     res.insts = (int64_t)c.insts.size();
@@ -1782,6 +2179,16 @@ struct Run {
     P = std::make_unique<Placer>(eng);
     P->o = o;
     init_nesterov_place(log, d, c, ip, bases, *P);
+    if (o.routability) {
+      route = std::make_unique<Routability>();
+      route->rb.vars = o.rv;
+      route->router = router;
+      route->common = &c;
+      int64_t area = 0;
+      for (auto &nb : P->nbs) area += nesterov_insts_area(nb);
+      route->rb.init(P->nbs.size(), area);
+      P->min_rc_cell_size.assign(P->gcells.size(), {0, 0});
+    }
     // the first HPWL (the reference HPWL's base) over the pins as the placer copied them
     int64_t design_hpwl = 0;
     for (auto &np : P->net_pins) {
@@ -1807,7 +2214,7 @@ struct Run {
   }
   bool step() {
     if (!nesterov || ended) return false;
-    bool more = loop.step(res.log, d, *P);
+    bool more = loop.step(res.log, d, *P, route.get());
     if (!more) ended = true;
     return more;
   }
@@ -1815,7 +2222,7 @@ struct Run {
     if (!nesterov) return;
     while (step()) {
     }
-    int iter = loop.end(res.log, d, *P);
+    int iter = loop.end(res.log, d, *P, route.get());
     res.locations = placed_locations(c, *P);
     auto t3 = std::chrono::steady_clock::now();
     res.t_np = std::chrono::duration<double>(t3 - t2).count();

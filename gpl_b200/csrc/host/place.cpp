@@ -9,9 +9,11 @@
 #include <cstdio>
 #include <cstring>
 #include <numeric>
+#include <stdexcept>
 #include <tuple>
 
 #include "host.h"
+#include "../kernels/b2b.h"
 
 namespace gpl {
 
@@ -917,6 +919,126 @@ Ip do_bicgstab_place(Log &log, const Design &d, Common &c, const Vars &v, const 
     log.report(sfmt("[InitialPlace]  Iter: %d conjugate gradient residual: %.8f HPWL: %ld", iter, (double)error_max, (long)ip_hpwl(d, c, ip, v)));
     update_coordi(d, c, ip, sx.x, sy.x);
     if ((double)error_max <= 1e-5 && iter >= 5) break;
+  }
+  return ip;
+}
+
+// `doBicgstabPlace` with its matrices assembled, collapsed and solved on the device
+// (kernels/b2b.cu): the same rounds, report lines, probes and stop rules as the host loop
+// above; the host reads back the two solves' scalars and the report's HPWL per round.
+Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v, const IpVars &vars, IpDevice &dev) {
+  log.info("GPL", 5, "---- Execute Conjugate Gradient Initial Placement.");
+  Ip ip = make_pins(d, c, v);
+  place_insts_initial_positions(log, d, c, ip, vars);
+  if (vars.max_iter < 1) return ip;
+  auto device = [](cudaError_t e, const char *where) {
+    if (e != cudaSuccess) throw std::runtime_error(std::string("device: ") + cudaGetErrorString(e) + " in " + where);
+  };
+  // the device's view: placed instances in `ip.place` order, pins net by net
+  IpSetup s;
+  const size_t n = ip.place.size();
+  std::vector<int32_t> ext(c.insts.size(), -1);
+  for (size_t e = 0; e < n; e++) ext[ip.place[e]] = (int32_t)e;
+  s.core = make_int4(d.core.lx, d.core.ly, d.core.ux, d.core.uy);
+  for (size_t e = 0; e < n; e++) {
+    const Instance &i = c.insts[ip.place[e]];
+    s.box.push_back(make_int4(i.lx, i.ly, i.ux, i.uy));
+    s.locked.push_back(i.locked ? 1 : 0);
+    int g = d.insts[i.db].group;
+    bool grouped = g >= 0 && d.groups[g].region >= 0;
+    Rect r = grouped ? region_box_of(d, d.groups[g].region) : Rect{};
+    s.grouped.push_back(grouped ? 1 : 0);
+    s.clamp.push_back(make_int4(r.lx, r.ly, r.ux, r.uy));
+    Rect b = ip.db_bbox[i.db];
+    s.db_box.push_back(make_int4(b.lx, b.ly, b.ux, b.uy));
+    s.db_size.push_back(make_int2(b.dx(), b.dy()));
+  }
+  std::vector<int> inst_map(d.insts.size(), -1);
+  for (size_t k = 0; k < c.insts.size(); k++)
+    if (c.insts[k].db >= 0) inst_map[c.insts[k].db] = (int)k;
+  s.net_start.push_back(0);
+  size_t pk = 0;
+  for (auto &[net, cnt] : c.nets) {
+    const DbNet &dn = d.nets[net];
+    for (auto &t : dn.iterms) {
+      const Pin &p = ip.pins[pk++];
+      int k = inst_map[t.inst];
+      bool placed = p.inst >= 0 && !c.insts[p.inst].fixed;
+      s.pin_e.push_back(placed ? ext[p.inst] : -1);
+      s.pin_inst.push_back(p.inst);
+      s.pin_mio.push_back(p.movable_io ? 1 : 0);
+      s.pin_off.push_back(make_int2(p.off_x, p.off_y));
+      s.pin_xy.push_back(make_int2(p.cx, p.cy));
+      bool dynamic = k >= 0 && !c.insts[k].fixed;
+      Rect b = ip.db_bbox[t.inst];
+      s.pin_hp.push_back(dynamic ? 0 : 1);
+      s.pin_static.push_back(make_int4(b.lx, b.ly, b.ux, b.uy));
+    }
+    if (!v.skip_io)
+      for (auto &pt : dn.bterms) {
+        const Pin &p = ip.pins[pk++];
+        s.pin_e.push_back(-1);
+        s.pin_inst.push_back(p.inst);
+        s.pin_mio.push_back(p.movable_io ? 1 : 0);
+        s.pin_off.push_back(make_int2(p.off_x, p.off_y));
+        s.pin_xy.push_back(make_int2(p.cx, p.cy));
+        s.pin_hp.push_back(pt.has_bbox ? 1 : 2);
+        s.pin_static.push_back(make_int4(pt.bbox.lx, pt.bbox.ly, pt.bbox.ux, pt.bbox.uy));
+      }
+    s.net_start.push_back((int64_t)pk);
+  }
+  if (pk != ip.pins.size()) throw std::runtime_error("initial placement: pin order mismatch");
+  s.max_fanout = vars.max_fanout;
+  s.min_diff = vars.min_diff_length;
+  s.weight_scale = vars.net_weight_scale;
+  device(dev.upload(s), "initial placement upload");
+  progress("initial placement (device): %zu pins, %zu nets", ip.pins.size(), ip.net_pins.size());
+  std::vector<float> xs, ys;
+  for (int iter = 1; iter <= vars.max_iter; iter++) {
+    IpAxisResult r[2];
+    device(dev.assemble(r), "initial placement assembly");
+    progress("  round %d: B2B assembled and collapsed (%lld + %lld triplets)", iter, (long long)r[0].triplets, (long long)r[1].triplets);
+    device(dev.solve(0, vars.max_solver_iter, r[0]), "initial placement solve x");
+    device(dev.solve(1, vars.max_solver_iter, r[1]), "initial placement solve y");
+    const BicgResult &ex = r[0].solve, &ey = r[1].solve;
+    progress("  round %d: solved (%d + %d iterations)", iter, ex.iterations, ey.iterations);
+    if (log.trace_on) {
+      device(dev.solution(0, xs), "initial placement solution");
+      device(dev.solution(1, ys), "initial placement solution");
+    }
+    uint32_t exb, eyb;
+    std::memcpy(&exb, &ex.error, 4);
+    std::memcpy(&eyb, &ey.error, 4);
+    log.probe(sfmt("VYGIPS|%d|x|%d|%08x|%d|%016llx", iter, ex.iterations, exb, ex.converged ? 0 : 2, (unsigned long long)fnv_f32(xs)));
+    log.probe(sfmt("VYGIPS|%d|y|%d|%08x|%d|%016llx", iter, ey.iterations, eyb, ey.converged ? 0 : 2, (unsigned long long)fnv_f32(ys)));
+    if (std::isnan(ex.error) || std::isnan(ey.error)) {
+      log.warn("GPL", 325, sfmt("Conjugate gradient initial placement solver failed at iteration %d. ", iter));
+      break;
+    }
+    float error_max = fmaxr(ex.error, ey.error);
+    int64_t hp = 0;
+    device(dev.hpwl(&hp), "initial placement hpwl");
+    log.report(sfmt("[InitialPlace]  Iter: %d conjugate gradient residual: %.8f HPWL: %ld", iter, (double)error_max, (long)hp));
+    device(dev.update(), "initial placement update");
+    if ((double)error_max <= 1e-5 && iter >= 5) break;
+  }
+  // the placed instances, their database boxes and their pins back on the host
+  std::vector<int4> box, db_box;
+  device(dev.download(box, db_box), "initial placement download");
+  for (size_t e = 0; e < n; e++) {
+    int k = ip.place[e];
+    Instance &i = c.insts[k];
+    if (i.locked) continue;
+    i.lx = box[e].x;
+    i.ly = box[e].y;
+    i.ux = box[e].z;
+    i.uy = box[e].w;
+    ip.db_bbox[i.db] = Rect{db_box[e].x, db_box[e].y, db_box[e].z, db_box[e].w};
+    int32_t cx = i.cx(), cy = i.cy();
+    for (int q : ip.inst_pins[k]) {
+      ip.pins[q].cx = cx + ip.pins[q].off_x;
+      ip.pins[q].cy = cy + ip.pins[q].off_y;
+    }
   }
   return ip;
 }

@@ -1,0 +1,669 @@
+// The initial placement on the device: bound-to-bound assembly (`createSparseMatrix`,
+// src/initial_place.rs:264-355), the triplets' collapse into CSR (`Csr::from_triplets`,
+// src/bicgstab.rs:501-541), BiCGSTAB, `updateCoordi` and the report's HPWL.
+//
+// Bit-exact with the host restatement: every triplet and right-hand-side term is written at
+// the position the host's net loop would append it (per-net counts, an exclusive scan, then
+// the same loop writing), and each row's duplicates are summed in that order (a row's
+// entries sorted by (column, position)), the first occurrence first, as the reference sums
+// them into the first.
+#include <algorithm>
+#include <cstring>
+
+#include "b2b.h"
+#include "common.cuh"
+
+namespace gpl {
+
+namespace {
+
+constexpr int kScanBlock = 1024;
+
+enum PinFlag : uint8_t { F_MIN_X = 1, F_MAX_X = 2, F_MIN_Y = 4, F_MAX_Y = 8 };
+
+struct IpArgs {
+  int32_t n_nets;
+  const int64_t *net_start;
+  const int32_t *pin_e, *pin_inst;
+  const uint8_t *pin_mio;
+  const int2 *pin_xy;
+  uint8_t *pin_flag;
+  const int4 *box;
+  const uint8_t *locked;
+  int32_t max_fanout, min_diff;
+  float weight_scale;
+};
+
+// Where one axis's terms go: triplets (row, col, value) and right-hand-side terms (row,
+// value), each net's run starting at its scanned offset.
+struct AxisOut {
+  int32_t *t_row, *t_col;
+  float *t_val;
+  int32_t *r_row;
+  float *r_val;
+  const int64_t *t_off, *r_off;  // per net
+  int64_t t_base;                // the locked diagonal precedes the nets' triplets
+};
+
+// `updatePinInfo` (src/initial_place.rs:203-252): per net, the first strict extreme per side.
+__global__ void k_pin_info(IpArgs a) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n >= a.n_nets) return;
+  int64_t b = a.net_start[n], e = a.net_start[n + 1];
+  int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+  int64_t pminx = -1, pmaxx = -1, pminy = -1, pmaxy = -1;
+  for (int64_t k = b; k < e; k++) a.pin_flag[k] = 0;
+  for (int64_t k = b; k < e; k++) {
+    if (a.pin_mio[k]) continue;
+    int2 q = a.pin_xy[k];
+    if (lx > q.x) {
+      if (pminx >= 0) a.pin_flag[pminx] &= (uint8_t)~F_MIN_X;
+      lx = q.x;
+      pminx = k;
+      a.pin_flag[k] |= F_MIN_X;
+    }
+    if (ux < q.x) {
+      if (pmaxx >= 0) a.pin_flag[pmaxx] &= (uint8_t)~F_MAX_X;
+      ux = q.x;
+      pmaxx = k;
+      a.pin_flag[k] |= F_MAX_X;
+    }
+    if (ly > q.y) {
+      if (pminy >= 0) a.pin_flag[pminy] &= (uint8_t)~F_MIN_Y;
+      ly = q.y;
+      pminy = k;
+      a.pin_flag[k] |= F_MIN_Y;
+    }
+    if (uy < q.y) {
+      if (pmaxy >= 0) a.pin_flag[pmaxy] &= (uint8_t)~F_MAX_Y;
+      uy = q.y;
+      pmaxy = k;
+      a.pin_flag[k] |= F_MAX_Y;
+    }
+  }
+}
+
+__device__ __forceinline__ int32_t centre(const int4 &b, int axis) { return axis == 0 ? (b.x + b.z) / 2 : (b.y + b.w) / 2; }
+
+// One net's pairs in the host's order (the second pin from the second solve pin on, the first
+// below it; x then y): counted (EMIT false) or written at the net's offsets (EMIT true).
+template <bool EMIT>
+__device__ void net_pairs(const IpArgs &a, int n, int64_t *cnt, int64_t stride, const AxisOut *out) {
+  int64_t b = a.net_start[n], e = a.net_start[n + 1];
+  int64_t deg = e - b;
+  int64_t tpos[2] = {0, 0}, rpos[2] = {0, 0};
+  if (EMIT) {
+#pragma unroll
+    for (int ax = 0; ax < 2; ax++) {
+      tpos[ax] = out[ax].t_base + out[ax].t_off[n];
+      rpos[ax] = out[ax].r_off[n];
+    }
+  }
+  int64_t tc[2] = {0, 0}, rc[2] = {0, 0};
+  if (deg > 1 && deg < a.max_fanout) {
+    float net_weight = __fdiv_rn(a.weight_scale, (float)(deg - 1));
+    for (int64_t k1 = b; k1 < e; k1++) {
+      if (a.pin_mio[k1]) continue;
+      for (int64_t k2 = b; k2 < k1; k2++) {
+        if (a.pin_mio[k2]) continue;
+        if (a.pin_inst[k1] == a.pin_inst[k2]) continue;
+        uint8_t f = a.pin_flag[k1] | a.pin_flag[k2];
+        int2 q1 = a.pin_xy[k1], q2 = a.pin_xy[k2];
+        int32_t ea = a.pin_e[k1], eb = a.pin_e[k2];
+#pragma unroll
+        for (int axis = 0; axis < 2; axis++) {
+          uint8_t mask = axis == 0 ? (F_MIN_X | F_MAX_X) : (F_MIN_Y | F_MAX_Y);
+          if (!(f & mask)) continue;
+          int32_t c1 = axis == 0 ? q1.x : q1.y, c2 = axis == 0 ? q2.x : q2.y;
+          int32_t diff = abs(c1 - c2);
+          float weight = diff > a.min_diff ? __fdiv_rn(net_weight, (float)diff) : __fdiv_rn(net_weight, (float)a.min_diff);
+          int nt = 0, nr = 0;
+          int32_t rows[4], cols[4], rr[2];
+          float vals[4], rv[2];
+          if (ea >= 0 && eb >= 0) {
+            bool la = a.locked[ea], lb = a.locked[eb];
+            if (!la && !lb) {
+              int32_t ca = centre(a.box[ea], axis), cb = centre(a.box[eb], axis);
+              rows[0] = ea, cols[0] = ea, vals[0] = weight;
+              rows[1] = eb, cols[1] = eb, vals[1] = weight;
+              rows[2] = ea, cols[2] = eb, vals[2] = -weight;
+              rows[3] = eb, cols[3] = ea, vals[3] = -weight;
+              nt = 4;
+              rr[0] = ea, rv[0] = __fmul_rn(-weight, (float)((c1 - ca) - (c2 - cb)));
+              rr[1] = eb, rv[1] = __fmul_rn(-weight, (float)((c2 - cb) - (c1 - ca)));
+              nr = 2;
+            } else if (la && !lb) {
+              int32_t cb = centre(a.box[eb], axis);
+              rows[0] = eb, cols[0] = eb, vals[0] = weight, nt = 1;
+              rr[0] = eb, rv[0] = __fmul_rn(weight, (float)(c1 - (c2 - cb))), nr = 1;
+            } else if (!la && lb) {
+              int32_t ca = centre(a.box[ea], axis);
+              rows[0] = ea, cols[0] = ea, vals[0] = weight, nt = 1;
+              rr[0] = ea, rv[0] = __fmul_rn(weight, (float)(c2 - (c1 - ca))), nr = 1;
+            }
+          } else if (ea < 0 && eb >= 0) {
+            int32_t cb = centre(a.box[eb], axis);
+            rows[0] = eb, cols[0] = eb, vals[0] = weight, nt = 1;
+            rr[0] = eb, rv[0] = __fmul_rn(weight, (float)(c1 - (c2 - cb))), nr = 1;
+          } else if (ea >= 0 && eb < 0) {
+            int32_t ca = centre(a.box[ea], axis);
+            rows[0] = ea, cols[0] = ea, vals[0] = weight, nt = 1;
+            rr[0] = ea, rv[0] = __fmul_rn(weight, (float)(c2 - (c1 - ca))), nr = 1;
+          }
+          if (EMIT) {
+            const AxisOut &o = out[axis];
+            for (int q = 0; q < nt; q++) {
+              int64_t at = tpos[axis]++;
+              o.t_row[at] = rows[q];
+              o.t_col[at] = cols[q];
+              o.t_val[at] = vals[q];
+            }
+            for (int q = 0; q < nr; q++) {
+              int64_t at = rpos[axis]++;
+              o.r_row[at] = rr[q];
+              o.r_val[at] = rv[q];
+            }
+          }
+          tc[axis] += nt;
+          rc[axis] += nr;
+        }
+      }
+    }
+  }
+  if (!EMIT) {
+    cnt[n] = tc[0];
+    cnt[stride + n] = tc[1];
+    cnt[2 * stride + n] = rc[0];
+    cnt[3 * stride + n] = rc[1];
+  }
+}
+
+__global__ void k_count(IpArgs a, int64_t *cnt, int64_t stride) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < a.n_nets) net_pairs<false>(a, n, cnt, stride, nullptr);
+}
+
+__global__ void k_emit(IpArgs a, AxisOut x, AxisOut y) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  AxisOut out[2] = {x, y};
+  if (n < a.n_nets) net_pairs<true>(a, n, nullptr, 0, out);
+}
+
+// The locked instances' unit diagonal (first in the triplet list, in instance order), and
+// each axis's start vector: the instances' centres.
+__global__ void k_locked_and_x0(int64_t n, const int4 *box, const uint8_t *locked, const int32_t *rank, AxisOut x, AxisOut y, float *x0, float *y0) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  int4 b = box[e];
+  x0[e] = (float)centre(b, 0);
+  y0[e] = (float)centre(b, 1);
+  if (locked[e]) {
+    int32_t at = rank[e];
+    x.t_row[at] = (int32_t)e, x.t_col[at] = (int32_t)e, x.t_val[at] = 1.0f;
+    y.t_row[at] = (int32_t)e, y.t_col[at] = (int32_t)e, y.t_val[at] = 1.0f;
+  }
+}
+
+// ---- the collapse into CSR: rows bucketed, each row's entries ordered by (column, position)
+__global__ void k_row_count(int64_t nt, const int32_t *row, unsigned long long *cnt) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t < nt) atomicAdd(&cnt[row[t]], 1ull);
+}
+
+// Each triplet's key (column << 32 | position) into its row's bucket; the order within a
+// bucket is settled by the sort that follows.
+__global__ void k_bucket(int64_t nt, const int32_t *row, const int32_t *col, const int64_t *row_off, int32_t *fill, unsigned long long *bucket) {
+  int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= nt) return;
+  int32_t r = row[t];
+  int64_t at = row_off[r] + atomicAdd(&fill[r], 1);
+  uint32_t c = col ? (uint32_t)col[t] : 0u;
+  bucket[at] = ((unsigned long long)c << 32) | (unsigned long long)(uint32_t)t;
+}
+
+// Per row: keys sorted (column, then position; Shell's sort, the keys are distinct), each
+// column's run summed in position order (the first value, then the rest added to it), the
+// distinct columns compacted.
+__global__ void k_row_collapse(int64_t n, const int64_t *row_off, unsigned long long *bucket, const float *val, int32_t *ucol, float *uval, int64_t *ucount) {
+  int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const int64_t b = row_off[r], e = row_off[r + 1], m = e - b;
+  unsigned long long *k = bucket + b;
+  const int gaps[] = {1750, 701, 301, 132, 57, 23, 10, 4, 1};
+  for (int gi = 0; gi < 9; gi++) {
+    const int64_t g = gaps[gi];
+    if (g >= m) continue;
+    for (int64_t i = g; i < m; i++) {
+      unsigned long long v = k[i];
+      int64_t j = i;
+      while (j >= g && v < k[j - g]) {
+        k[j] = k[j - g];
+        j -= g;
+      }
+      k[j] = v;
+    }
+  }
+  int64_t u = 0, i = 0;
+  while (i < m) {
+    unsigned long long key = k[i];
+    uint32_t c = (uint32_t)(key >> 32);
+    float s = val[(uint32_t)key];
+    int64_t j = i + 1;
+    for (; j < m; j++) {
+      unsigned long long k2 = k[j];
+      if ((uint32_t)(k2 >> 32) != c) break;
+      s = __fadd_rn(s, val[(uint32_t)k2]);
+    }
+    ucol[b + u] = (int32_t)c;
+    uval[b + u] = s;
+    u++;
+    i = j;
+  }
+  ucount[r] = u;
+}
+
+__global__ void k_row_fill(int64_t n, const int64_t *row_off, const int64_t *starts, const int32_t *ucol, const float *uval, int32_t *cols, float *vals) {
+  int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  int64_t b = row_off[r], o = starts[r], m = starts[r + 1] - o;
+  for (int64_t j = 0; j < m; j++) {
+    cols[o + j] = ucol[b + j];
+    vals[o + j] = uval[b + j];
+  }
+}
+
+// The right-hand side: the locked rows' centre, else the row's terms summed in order onto 0.
+__global__ void k_rhs(int64_t n, int axis, const int4 *box, const uint8_t *locked, const int64_t *row_off, const int64_t *ucount, const float *uval, float *rhs) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  if (locked[e]) {
+    rhs[e] = (float)centre(box[e], axis);
+    return;
+  }
+  // the host adds every term onto 0.0f; the run's sum from its first term differs from that
+  // only in the sign of a zero, which one more + 0.0f settles
+  rhs[e] = ucount[e] ? __fadd_rn(uval[row_off[e]], 0.0f) : 0.0f;
+}
+
+// ---- exclusive scan of int64 counts (in place; data[n] receives the total)
+__global__ void k_scan_block(int64_t *data, int64_t n, int64_t *totals) {
+  __shared__ int64_t warp_sum[kScanBlock / 32];
+  int64_t i = blockIdx.x * (int64_t)kScanBlock + threadIdx.x;
+  int64_t v = i < n ? data[i] : 0;
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int64_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int64_t s = warp_sum[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int64_t y = __shfl_up_sync(0xffffffffu, s, o);
+      if (lane >= o) s += y;
+    }
+    warp_sum[lane] = s;
+  }
+  __syncthreads();
+  int64_t before = w ? warp_sum[w - 1] : 0;
+  if (i < n) data[i] = before + x - v;
+  if (threadIdx.x == kScanBlock - 1) totals[blockIdx.x] = before + x;
+}
+
+// The block totals' exclusive scan: one block of 1024 threads, a chunk of totals each.
+__global__ void k_scan_totals(int64_t *totals, int64_t nb) {
+  __shared__ int64_t part[kScanBlock];
+  const int64_t per = (nb + kScanBlock - 1) / kScanBlock;
+  const int64_t lo = threadIdx.x * per, hi = min(nb, lo + per);
+  int64_t s = 0;
+  for (int64_t b = lo; b < hi; b++) s += totals[b];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t run = 0;
+    for (int t = 0; t < kScanBlock; t++) {
+      int64_t q = part[t];
+      part[t] = run;
+      run += q;
+    }
+    totals[nb] = run;
+  }
+  __syncthreads();
+  int64_t run = part[threadIdx.x];
+  for (int64_t b = lo; b < hi; b++) {
+    int64_t q = totals[b];
+    totals[b] = run;
+    run += q;
+  }
+}
+
+__global__ void k_scan_add(int64_t *data, int64_t n, const int64_t *totals, int64_t nb) {
+  int64_t i = blockIdx.x * (int64_t)kScanBlock + threadIdx.x;
+  if (i < n) data[i] += totals[blockIdx.x];
+  if (i == 0) data[n] = totals[nb];
+}
+
+// ---- updateCoordi (src/initial_place.rs:391-417) and setCenterLocation (:152-165)
+__global__ void k_update(int64_t n, const float *x, const float *y, int4 core, const int4 *region, const uint8_t *grouped, const uint8_t *locked, int4 *box, int4 *db_box, const int2 *db_size) {
+  int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= n || locked[e]) return;
+  int32_t nx = f2i_rz(x[e]), ny = f2i_rz(y[e]);
+  nx = min(max(nx, core.x), core.z);
+  ny = min(max(ny, core.y), core.w);
+  if (grouped[e]) {
+    int4 r = region[e];
+    nx = min(max(nx, r.x), r.z);
+    ny = min(max(ny, r.y), r.w);
+  }
+  int4 b = box[e];
+  int32_t hx = (b.z - b.x) / 2, hy = (b.w - b.y) / 2;
+  b = make_int4(nx - hx, ny - hy, nx + hx, ny + hy);
+  box[e] = b;
+  int2 d = db_size[e];
+  db_box[e] = make_int4(b.x, b.y, b.x + d.x, b.y + d.y);
+}
+
+__global__ void k_pins(int64_t np, const int32_t *pin_e, const uint8_t *locked, const int4 *box, const int2 *off, int2 *xy) {
+  int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (k >= np) return;
+  int32_t e = pin_e[k];
+  if (e < 0 || locked[e]) return;
+  int4 b = box[e];
+  int2 o = off[k];
+  xy[k] = make_int2(centre(b, 0) + o.x, centre(b, 1) + o.y);
+}
+
+// The report's HPWL over the database boxes (src/initial_place.rs:359-386).
+__global__ void k_db_hpwl(int32_t n_nets, const int64_t *net_start, const int32_t *pin_e, const uint8_t *hp, const int4 *stat, const int4 *db_box, unsigned long long *out) {
+  int n = blockIdx.x * blockDim.x + threadIdx.x;
+  long long h = 0;
+  if (n < n_nets) {
+    int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+    for (int64_t k = net_start[n]; k < net_start[n + 1]; k++) {
+      uint8_t m = hp[k];
+      if (m == 2) continue;
+      int4 b = m == 0 ? db_box[pin_e[k]] : stat[k];
+      lx = min(lx, b.x);
+      ly = min(ly, b.y);
+      ux = max(ux, b.z);
+      uy = max(uy, b.w);
+    }
+    if (ux >= lx) h = ((long long)ux - lx) + ((long long)uy - ly);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+  if ((threadIdx.x & 31) == 0 && h) atomicAdd(out, (unsigned long long)h);
+}
+
+unsigned grid(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + kThreads - 1) / kThreads); }
+
+template <class T>
+cudaError_t alloc(T **p, size_t n) {
+  *p = nullptr;
+  return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+}
+template <class T>
+cudaError_t put(T **p, const std::vector<T> &v, cudaStream_t s, int64_t &bytes) {
+  cudaError_t e = alloc(p, v.size());
+  if (e != cudaSuccess || v.empty()) return e;
+  bytes += (int64_t)(v.size() * sizeof(T));
+  return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+// Grows a set of buffers to hold n entries each.
+template <class... T>
+cudaError_t grow(size_t n, size_t &cap, T **...bufs) {
+  if (n <= cap) return cudaSuccess;
+  size_t c = (size_t)(n * 1.1) + 16;
+  cudaError_t e = cudaSuccess;
+  auto one = [&](auto **p) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    if (e == cudaSuccess) e = alloc(p, c);
+  };
+  (one(bufs), ...);
+  cap = e == cudaSuccess ? c : 0;
+  return e;
+}
+
+}  // namespace
+
+#define CK(x)                         \
+  do {                                \
+    cudaError_t _e = (x);             \
+    if (_e != cudaSuccess) return _e; \
+  } while (0)
+
+IpDevice::~IpDevice() { release(); }
+
+void IpDevice::release() {
+  void *ptrs[] = {box_, clamp_, db_box_, pin_static_, db_size_, pin_off_, pin_xy_, locked_, grouped_, pin_mio_, pin_hp_, pin_flag_, pin_e_, pin_inst_, locked_rank_,
+                  net_start_, cnt_, scan_tmp_, t_row_, t_col_, t_val_, r_row_, r_val_, bucket_, fill_, row_off_, ucount_, ucol_, uval_, scratch_, hpwl_acc_};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (auto &a : ax_) {
+    void *q[] = {a.starts, a.cols, a.vals, a.rhs, a.x};
+    for (void *p : q)
+      if (p) cudaFree(p);
+    a = Axis{};
+  }
+  box_ = clamp_ = db_box_ = pin_static_ = nullptr;
+  db_size_ = pin_off_ = pin_xy_ = nullptr;
+  locked_ = grouped_ = pin_mio_ = pin_hp_ = pin_flag_ = nullptr;
+  pin_e_ = pin_inst_ = locked_rank_ = nullptr;
+  net_start_ = cnt_ = scan_tmp_ = row_off_ = ucount_ = nullptr;
+  t_row_ = t_col_ = r_row_ = fill_ = ucol_ = nullptr;
+  t_val_ = r_val_ = uval_ = nullptr;
+  bucket_ = nullptr;
+  scratch_ = nullptr;
+  hpwl_acc_ = nullptr;
+  t_cap_ = r_cap_ = w_cap_ = scan_tmp_n_ = 0;
+}
+
+cudaError_t IpDevice::upload(const IpSetup &s) {
+  release();
+  cfg_.max_fanout = s.max_fanout;
+  cfg_.min_diff = s.min_diff;
+  cfg_.weight_scale = s.weight_scale;
+  cfg_.core = s.core;
+  n_ = (int64_t)s.box.size();
+  n_pins_ = (int64_t)s.pin_e.size();
+  n_nets_ = (int32_t)(s.net_start.size() - 1);
+  std::vector<int32_t> rank(n_, -1);
+  n_locked_ = 0;
+  for (int64_t e = 0; e < n_; e++)
+    if (s.locked[e]) rank[e] = (int32_t)n_locked_++;
+  int64_t &b = h2d_bytes;
+  CK(put(&box_, s.box, s_, b));
+  CK(put(&locked_, s.locked, s_, b));
+  CK(put(&clamp_, s.clamp, s_, b));
+  CK(put(&grouped_, s.grouped, s_, b));
+  CK(put(&db_box_, s.db_box, s_, b));
+  CK(put(&db_size_, s.db_size, s_, b));
+  CK(put(&locked_rank_, rank, s_, b));
+  CK(put(&pin_e_, s.pin_e, s_, b));
+  CK(put(&pin_inst_, s.pin_inst, s_, b));
+  CK(put(&pin_mio_, s.pin_mio, s_, b));
+  CK(put(&pin_off_, s.pin_off, s_, b));
+  CK(put(&pin_xy_, s.pin_xy, s_, b));
+  CK(put(&pin_hp_, s.pin_hp, s_, b));
+  CK(put(&pin_static_, s.pin_static, s_, b));
+  CK(put(&net_start_, s.net_start, s_, b));
+  CK(alloc(&pin_flag_, n_pins_));
+  CK(alloc(&cnt_, 4 * ((size_t)n_nets_ + 1)));
+  CK(alloc(&row_off_, n_ + 1));
+  CK(alloc(&ucount_, n_ + 1));
+  CK(alloc(&fill_, n_));
+  CK(alloc(&hpwl_acc_, 1));
+  for (auto &a : ax_) {
+    CK(alloc(&a.starts, n_ + 1));
+    CK(alloc(&a.rhs, n_));
+    CK(alloc(&a.x, n_));
+  }
+  scratch_bytes_ = bicgstab_scratch_bytes(n_);
+  CK(cudaMalloc(&scratch_, scratch_bytes_));
+  return cudaStreamSynchronize(s_);
+}
+
+cudaError_t IpDevice::scan(int64_t *data, int64_t n) {
+  int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+  if ((size_t)(nb + 1) > scan_tmp_n_) {
+    if (scan_tmp_) cudaFree(scan_tmp_);
+    scan_tmp_n_ = (size_t)(nb + 1);
+    CK(alloc(&scan_tmp_, scan_tmp_n_));
+  }
+  if (nb == 0) return cudaMemsetAsync(data, 0, sizeof(int64_t), s_);
+  k_scan_block<<<(unsigned)nb, kScanBlock, 0, s_>>>(data, n, scan_tmp_);
+  k_scan_totals<<<1, kScanBlock, 0, s_>>>(scan_tmp_, nb);
+  k_scan_add<<<(unsigned)nb, kScanBlock, 0, s_>>>(data, n, scan_tmp_, nb);
+  launches += 3;
+  return cudaGetLastError();
+}
+
+// Collapses triplets (row, col or one column, val) [0, n_trip) into CSR rows; with no
+// output arrays it stops at the per-row sums (row_off_, ucount_, uval_).
+cudaError_t IpDevice::collapse(int64_t n_trip, const int32_t *row, const int32_t *col, const float *val, int64_t *starts_out, int32_t **cols, float **vals, size_t *cap, int64_t *nnz) {
+  CK(cudaMemsetAsync(row_off_, 0, (n_ + 1) * sizeof(int64_t), s_));
+  CK(cudaMemsetAsync(fill_, 0, std::max<int64_t>(n_, 1) * sizeof(int32_t), s_));
+  if (n_trip) k_row_count<<<grid(n_trip), kThreads, 0, s_>>>(n_trip, row, (unsigned long long *)row_off_);
+  CK(scan(row_off_, n_));
+  if (n_trip) k_bucket<<<grid(n_trip), kThreads, 0, s_>>>(n_trip, row, col, row_off_, fill_, bucket_);
+  if (n_) k_row_collapse<<<grid(n_), kThreads, 0, s_>>>(n_, row_off_, bucket_, val, ucol_, uval_, ucount_);
+  launches += 3;
+  if (!cols) return cudaGetLastError();
+  CK(cudaMemcpyAsync(starts_out, ucount_, n_ * sizeof(int64_t), cudaMemcpyDeviceToDevice, s_));
+  CK(scan(starts_out, n_));
+  CK(cudaMemcpyAsync(nnz, starts_out + n_, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  d2h_bytes += 8;
+  if ((size_t)*nnz > *cap) {
+    if (*cols) cudaFree(*cols);
+    if (*vals) cudaFree(*vals);
+    *cols = nullptr;
+    *vals = nullptr;
+    *cap = (size_t)(*nnz * 1.25) + 16;
+    CK(alloc(cols, *cap));
+    CK(alloc(vals, *cap));
+  }
+  if (n_) k_row_fill<<<grid(n_), kThreads, 0, s_>>>(n_, row_off_, starts_out, ucol_, uval_, *cols, *vals);
+  launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t IpDevice::assemble(IpAxisResult out[2]) {
+  IpArgs a{};
+  a.n_nets = n_nets_;
+  a.net_start = net_start_;
+  a.pin_e = pin_e_;
+  a.pin_inst = pin_inst_;
+  a.pin_mio = pin_mio_;
+  a.pin_xy = pin_xy_;
+  a.pin_flag = pin_flag_;
+  a.box = box_;
+  a.locked = locked_;
+  a.max_fanout = cfg_.max_fanout;
+  a.min_diff = cfg_.min_diff;
+  a.weight_scale = cfg_.weight_scale;
+  const int64_t stride = (int64_t)n_nets_ + 1;
+  if (n_nets_) {
+    k_pin_info<<<grid(n_nets_), kThreads, 0, s_>>>(a);
+    k_count<<<grid(n_nets_), kThreads, 0, s_>>>(a, cnt_, stride);
+    launches += 2;
+  }
+  for (int q = 0; q < 4; q++) CK(scan(cnt_ + q * stride, n_nets_));
+  int64_t tot[4];
+  for (int q = 0; q < 4; q++) CK(cudaMemcpyAsync(&tot[q], cnt_ + q * stride + n_nets_, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  d2h_bytes += 32;
+  // both axes side by side: x's triplets (the locked diagonal first) then y's; the same
+  // for the right-hand-side terms
+  const int64_t nt[2] = {n_locked_ + tot[0], n_locked_ + tot[1]}, nr[2] = {tot[2], tot[3]};
+  CK(grow((size_t)(nt[0] + nt[1]), t_cap_, &t_row_, &t_col_, &t_val_));
+  CK(grow((size_t)(nr[0] + nr[1]), r_cap_, &r_row_, &r_val_));
+  CK(grow((size_t)std::max({nt[0], nt[1], nr[0], nr[1]}), w_cap_, &bucket_, &ucol_, &uval_));
+  AxisOut ox{}, oy{};
+  ox.t_row = t_row_, ox.t_col = t_col_, ox.t_val = t_val_;
+  oy.t_row = t_row_ + nt[0], oy.t_col = t_col_ + nt[0], oy.t_val = t_val_ + nt[0];
+  ox.t_off = cnt_, oy.t_off = cnt_ + stride;
+  ox.t_base = oy.t_base = n_locked_;
+  ox.r_row = r_row_, ox.r_val = r_val_;
+  oy.r_row = r_row_ + nr[0], oy.r_val = r_val_ + nr[0];
+  ox.r_off = cnt_ + 2 * stride, oy.r_off = cnt_ + 3 * stride;
+  if (n_) k_locked_and_x0<<<grid(n_), kThreads, 0, s_>>>(n_, box_, locked_, locked_rank_, ox, oy, ax_[0].x, ax_[1].x);
+  if (n_nets_) k_emit<<<grid(n_nets_), kThreads, 0, s_>>>(a, ox, oy);
+  launches += 2;
+  CK(cudaGetLastError());
+  for (int ax = 0; ax < 2; ax++) {
+    Axis &A = ax_[ax];
+    int64_t o = ax ? nt[0] : 0;
+    CK(collapse(nt[ax], t_row_ + o, t_col_ + o, t_val_ + o, A.starts, &A.cols, &A.vals, &A.cap, &A.nnz));
+    out[ax].triplets = nt[ax];
+    // the right-hand side: this axis's terms as one-column triplets, summed per row in order
+    int64_t r = ax ? nr[0] : 0;
+    CK(collapse(nr[ax], r_row_ + r, nullptr, r_val_ + r, nullptr, nullptr, nullptr, nullptr, nullptr));
+    if (n_) {
+      k_rhs<<<grid(n_), kThreads, 0, s_>>>(n_, ax, box_, locked_, row_off_, ucount_, uval_, A.rhs);
+      launches += 1;
+    }
+    CK(cudaGetLastError());
+  }
+  return cudaStreamSynchronize(s_);
+}
+
+cudaError_t IpDevice::solve(int axis, int max_iters, IpAxisResult &out) {
+  Axis &A = ax_[axis];
+  CsrDev m{n_, A.starts, A.cols, A.vals};
+  BicgResult r{};
+  cudaError_t e = bicgstab_solve(m, A.rhs, A.x, max_iters, scratch_, s_, &r);
+  launches += 4 + (int64_t)r.iterations * 10;
+  d2h_bytes += (int64_t)(r.iterations + 2) * 64;
+  out.solve = r;
+  return e;
+}
+
+cudaError_t IpDevice::hpwl(int64_t *out) {
+  CK(cudaMemsetAsync(hpwl_acc_, 0, sizeof(int64_t), s_));
+  if (n_nets_) {
+    k_db_hpwl<<<grid(n_nets_), kThreads, 0, s_>>>(n_nets_, net_start_, pin_e_, pin_hp_, pin_static_, db_box_, (unsigned long long *)hpwl_acc_);
+    launches += 1;
+  }
+  CK(cudaMemcpyAsync(out, hpwl_acc_, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  d2h_bytes += 8;
+  return cudaStreamSynchronize(s_);
+}
+
+cudaError_t IpDevice::update() {
+  if (n_) {
+    k_update<<<grid(n_), kThreads, 0, s_>>>(n_, ax_[0].x, ax_[1].x, cfg_.core, clamp_, grouped_, locked_, box_, db_box_, db_size_);
+    launches += 1;
+  }
+  if (n_pins_) {
+    k_pins<<<grid(n_pins_), kThreads, 0, s_>>>(n_pins_, pin_e_, locked_, box_, pin_off_, pin_xy_);
+    launches += 1;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t IpDevice::solution(int axis, std::vector<float> &x) {
+  x.resize(n_);
+  if (n_) CK(cudaMemcpyAsync(x.data(), ax_[axis].x, n_ * sizeof(float), cudaMemcpyDeviceToHost, s_));
+  d2h_bytes += n_ * 4;
+  return cudaStreamSynchronize(s_);
+}
+
+cudaError_t IpDevice::download(std::vector<int4> &box, std::vector<int4> &db_box) {
+  box.resize(n_);
+  db_box.resize(n_);
+  if (n_) {
+    CK(cudaMemcpyAsync(box.data(), box_, n_ * sizeof(int4), cudaMemcpyDeviceToHost, s_));
+    CK(cudaMemcpyAsync(db_box.data(), db_box_, n_ * sizeof(int4), cudaMemcpyDeviceToHost, s_));
+  }
+  d2h_bytes += n_ * 32;
+  return cudaStreamSynchronize(s_);
+}
+
+}  // namespace gpl

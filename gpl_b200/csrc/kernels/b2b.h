@@ -1,0 +1,101 @@
+// The initial placement's device half: the bound-to-bound matrix of each axis assembled,
+// collapsed into CSR and solved on the GPU, the coordinates updated there, and the report's
+// HPWL over the instances' database boxes. The host loop (place.cpp) keeps the reference's
+// control flow (`doBicgstabPlace`, src/initial_place.rs:420-446) and reads back scalars only.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "bicgstab.h"
+
+namespace gpl {
+
+// What the device needs, in the initial placement's own orders: instances in `Ip::place`
+// order (e), pins net by net (`Ip::pins`).
+struct IpSetup {
+  // per placed instance e
+  std::vector<int4> box;       // lx, ly, ux, uy after the initial positions
+  std::vector<uint8_t> locked;
+  std::vector<int4> clamp;     // the group's region box, for grouped instances
+  std::vector<uint8_t> grouped;
+  std::vector<int4> db_box;    // the database box the report's HPWL reads (the design's at first)
+  std::vector<int2> db_size;   // the database box's width and height
+  // per pin
+  std::vector<int32_t> pin_e;     // placed instance, -1 for none (port, fixed, outside the set)
+  std::vector<int32_t> pin_inst;  // placer instance (-1 for ports): the "same instance" test
+  std::vector<uint8_t> pin_mio;   // movable IO: left out of the matrix and the extremes
+  std::vector<int2> pin_off, pin_xy;
+  std::vector<uint8_t> pin_hp;    // report HPWL: 0 the instance's db box, 1 the static box, 2 none
+  std::vector<int4> pin_static;   // the static box (fixed instance, outside instance, port bbox)
+  std::vector<int64_t> net_start;
+  int4 core{};                    // `updateCoordi` clamps to the core first
+  int32_t max_fanout = 200, min_diff = 1500;
+  float weight_scale = 800.0f;
+};
+
+struct IpAxisResult {
+  int64_t triplets = 0;  // triplets assembled (the locked diagonal included)
+  BicgResult solve{};
+};
+
+class IpDevice {
+ public:
+  explicit IpDevice(cudaStream_t s) : s_(s) {}
+  ~IpDevice();
+  cudaError_t upload(const IpSetup &s);
+  // `updatePinInfo` then `createSparseMatrix` for both axes, each collapsed to CSR
+  // (`Csr::from_triplets`), with its right-hand side and start vector.
+  cudaError_t assemble(IpAxisResult out[2]);
+  // One axis's BiCGSTAB (src/bicgstab.rs:615-669).
+  cudaError_t solve(int axis, int max_iters, IpAxisResult &out);
+  // The report's HPWL over the database boxes (src/initial_place.rs:359-386).
+  cudaError_t hpwl(int64_t *out);
+  // `updateCoordi` (src/initial_place.rs:391-417) from both solutions.
+  cudaError_t update();
+  // The solution vector of an axis (for the trace's probe lines).
+  cudaError_t solution(int axis, std::vector<float> &x);
+  // The placed instances' boxes and database boxes.
+  cudaError_t download(std::vector<int4> &box, std::vector<int4> &db_box);
+  int64_t launches = 0, h2d_bytes = 0, d2h_bytes = 0;
+
+ private:
+  cudaStream_t s_;
+  int64_t n_ = 0, n_pins_ = 0, n_locked_ = 0;
+  int32_t n_nets_ = 0;
+  IpSetup cfg_;
+  // device state
+  int4 *box_ = nullptr, *clamp_ = nullptr, *db_box_ = nullptr, *pin_static_ = nullptr;
+  int2 *db_size_ = nullptr, *pin_off_ = nullptr, *pin_xy_ = nullptr;
+  uint8_t *locked_ = nullptr, *grouped_ = nullptr, *pin_mio_ = nullptr, *pin_hp_ = nullptr, *pin_flag_ = nullptr;
+  int32_t *pin_e_ = nullptr, *pin_inst_ = nullptr, *locked_rank_ = nullptr;
+  int64_t *net_start_ = nullptr;
+  // counts and offsets, triplets and right-hand-side terms of both axes, the collapse's work
+  int64_t *cnt_ = nullptr;       // [4][n_nets + 1]: triplets x, triplets y, rhs x, rhs y
+  int64_t *scan_tmp_ = nullptr;
+  size_t scan_tmp_n_ = 0;
+  int32_t *t_row_ = nullptr, *t_col_ = nullptr, *r_row_ = nullptr;
+  float *t_val_ = nullptr, *r_val_ = nullptr;
+  size_t t_cap_ = 0, r_cap_ = 0, w_cap_ = 0;
+  unsigned long long *bucket_ = nullptr;  // (column << 32 | position) per triplet, by row
+  int32_t *fill_ = nullptr;
+  int64_t *row_off_ = nullptr, *ucount_ = nullptr;
+  int32_t *ucol_ = nullptr;
+  float *uval_ = nullptr;
+  struct Axis {
+    int64_t *starts = nullptr;
+    int32_t *cols = nullptr;
+    float *vals = nullptr, *rhs = nullptr, *x = nullptr;
+    size_t cap = 0;
+    int64_t nnz = 0;
+  } ax_[2];
+  void *scratch_ = nullptr;
+  size_t scratch_bytes_ = 0;
+  int64_t *hpwl_acc_ = nullptr;
+  void release();
+  cudaError_t collapse(int64_t n_trip, const int32_t *row, const int32_t *col, const float *val, int64_t *starts_out, int32_t **cols, float **vals, size_t *cap, int64_t *nnz);
+  cudaError_t scan(int64_t *data, int64_t n);
+};
+
+}  // namespace gpl

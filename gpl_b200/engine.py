@@ -66,6 +66,8 @@ class Placer:
         cd = design.c_struct()
         argv = (C.c_char_p * max(len(args), 1))(*[a.encode() for a in args])
         res = gpl_result_t()
+        if isinstance(router, SyntheticRouter):
+            router = router.ptr
         L.gpl_global_placement(self._ctx, C.byref(cd), len(args), argv, router, C.byref(res))
         try:
             return result_to_dict(res)

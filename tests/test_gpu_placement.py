@@ -51,3 +51,53 @@ def test_skip_nesterov_initial_placement_is_close(cfg1):
     a, b = got["locations"][:, 1:].astype(float), ref["locations"][:, 1:].astype(float)
     # per-coordinate: within 1e-5 of the core size (the coordinates are truncated integers)
     assert np.max(np.abs(a - b)) <= max(2.0, 1e-5 * 60000)
+
+
+def _ip_rows(lines):
+    rows = []
+    for l in lines:
+        if l.startswith("[InitialPlace]"):
+            parts = l.split()
+            rows.append((int(parts[2]), float(parts[6]), int(parts[8])))
+    return rows
+
+
+def test_initial_place_rounds_match_the_oracle(cfg1):
+    d, _ = cfg1
+    ref = oracle.global_placement(d, ARGS + ["-skip_nesterov_place"])
+    got = engine.global_placement(d, ARGS + ["-skip_nesterov_place"])
+    a, b = _ip_rows(got["lines"]), _ip_rows(ref["lines"])
+    assert len(a) == len(b) and len(a) >= 5
+    # round 1's HPWL reads the design's boxes only: exact; later rounds follow solves whose dot
+    # products are FP64 on the device (the oracle keeps the reference's f32 packet order)
+    assert a[0][2] == b[0][2]
+    for (ia, ra, ha), (ib, rb, hb) in zip(a, b):
+        assert ia == ib
+        assert abs(ha - hb) <= 1e-3 * hb
+
+
+def _lines_with(lines, code):
+    return [l for l in lines if f"GPL-{code}]" in l]
+
+
+def test_routability_driven_matches_the_oracle(cfg1):
+    """-routability_driven with the synthetic router (one wide routing pitch, so the RUDY map
+    overflows and the pass inflates cells, cuts fillers and reverts to its snapshot several
+    times). The trajectories part after the first reordered sum, so the comparison is of the
+    course, not of bits: the snapshot within 10 iterations, the same number of passes (+-1),
+    both ending placed under the overflow target, final HPWL within 5 % and the final
+    placement area (cells as inflated) within 1 %."""
+    d, _ = cfg1
+    args = ARGS + ["-routability_driven"]
+    rt = engine.SyntheticRouter(d, 3000, pitches=(1200,))
+    ref = oracle.global_placement(d, args, router=rt.ptr)
+    got = engine.global_placement(d, args, router=rt)
+    assert ref["status"] == "placed" and got["status"] == "placed", got["reason"]
+    snap = lambda r: int(_lines_with(r["lines"], "0038")[0].split("=")[-1])
+    assert abs(snap(got) - snap(ref)) <= 10
+    assert abs(len(_lines_with(got["lines"], "0040")) - len(_lines_with(ref["lines"], "0040"))) <= 1
+    assert len(_lines_with(got["lines"], "0040")) >= 2
+    assert got["final_overflow"] <= 0.1
+    assert abs(got["final_hpwl"] - ref["final_hpwl"]) <= 0.05 * ref["final_hpwl"]
+    area = lambda r: float(_lines_with(r["lines"], "1014")[0].split(":")[1].split("(")[0])
+    assert abs(area(got) - area(ref)) <= 0.01 * area(ref)

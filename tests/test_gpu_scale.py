@@ -1,0 +1,51 @@
+"""The whole command at scale against the oracle's own full runs (tests/golden/oracle_runs.json,
+written by tests/golden/make_oracle_runs.py: minutes to an hour of CPU per run, so they are
+recorded once instead of re-run here).
+
+Tolerances as the whole-command test on the small design: identical construction lines,
+the `[InitialPlace]` rounds' HPWL within 0.1 % (the first exact), final HPWL within 0.1 % and
+final overflow within 0.005 of the oracle's."""
+import json
+import os
+
+import pytest
+
+from gpl_b200 import engine, synth
+
+pytestmark = pytest.mark.gpu
+
+_PATH = os.path.join(os.path.dirname(__file__), "golden", "oracle_runs.json")
+RUNS = json.load(open(_PATH)) if os.path.exists(_PATH) else {}
+
+
+def header(lines):
+    out = []
+    for l in lines:
+        if l.startswith("[InitialPlace]"):
+            break
+        out.append(l)
+    return out
+
+
+def ip_hpwl(lines):
+    return [int(l.split()[8]) for l in lines if l.startswith("[InitialPlace]")]
+
+
+@pytest.mark.parametrize("cfg,mode", [("cfg2", "fp32"), ("cfg2", "mixed"), ("cfg3", "mixed"), ("cfg3", "fp32")])
+def test_full_run_matches_the_oracle(cfg, mode):
+    if cfg not in RUNS:
+        pytest.skip(f"no recorded oracle run for {cfg}")
+    ref = RUNS[cfg]
+    d = synth.generate(cfg)
+    got = engine.global_placement(d, ref["args"], poisson=mode)
+    assert got["status"] == "placed", got["reason"]
+    assert header(got["lines"]) == ref["header"]
+    assert (got["insts"], got["nets"], got["pins"]) == (ref["insts"], ref["nets"], ref["pins"])
+    a, b = ip_hpwl(got["lines"]), ip_hpwl(ref["initial_place"])
+    assert len(a) == len(b) and a[0] == b[0]
+    for ha, hb in zip(a, b):
+        assert abs(ha - hb) <= 1e-3 * hb
+    assert abs(got["final_hpwl"] - ref["final_hpwl"]) <= 1e-3 * ref["final_hpwl"]
+    assert abs(got["final_overflow"] - ref["final_overflow"]) <= 0.005
+    assert got["final_overflow"] <= 0.1
+    assert len(got["locations"]) == ref["locations"]

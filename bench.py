@@ -24,6 +24,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -132,12 +134,24 @@ def ours(a):
         r = engine.global_placement(design, cfg["args"] + ["-skip_nesterov_place"], device=local)
         print(json.dumps({"case": "initial placement only", "config": cfg["name"], "status": r["status"],
                           "seconds": time.perf_counter() - t0, "seconds_initial_place": r["seconds_initial_place"]}))
+        if a.save_placement:
+            np.save(a.save_placement, r["locations"])
         return
     design = synth.generate(cfg["preset"], placed=a.start == "placed")
+    if a.start_from:
+        # the saved initial placement as the design's placement (lower-left corners), so the
+        # loop starts where the initial placement left it without running it again
+        loc = np.load(a.start_from)
+        box = design.inst_box
+        w, h = box[loc[:, 0], 2] - box[loc[:, 0], 0], box[loc[:, 0], 3] - box[loc[:, 0], 1]
+        box[loc[:, 0], 0], box[loc[:, 0], 1] = loc[:, 1], loc[:, 2]
+        box[loc[:, 0], 2], box[loc[:, 0], 3] = loc[:, 1] + w, loc[:, 2] + h
+        design.inst_flags[loc[:, 0]] |= synth.INST_PLACED
     log("design generated")
     C_cells = design.meta["cells"]
     placer = engine.Placer(local, a.form)
-    sess = engine.Session(placer, design, cfg["args"] + (["-skip_initial_place"] if a.start == "placed" else []))
+    skip_ip = a.start == "placed" or bool(a.start_from)
+    sess = engine.Session(placer, design, cfg["args"] + (["-skip_initial_place"] if skip_ip else []))
     log("session open")
     sess.iterate(a.warmup)
     log("warm-up done")
@@ -241,7 +255,7 @@ def ours(a):
         "vs_baseline": None, "dtype": "f32+bf16x3 (split-BF16 density solve), f64 reductions", "data": "synthetic",
         "config": {"workload": cfg["name"], "args": cfg["args"], "design": design.meta["config"],
                    "cells": C_cells, "nets": N_nets, "pins": P_pins, "bins": B, "parallelism": f"replicas x{world}",
-                   "start": "after the initial placement" if a.start == "ip" else "the generator's spread placement, initial placement skipped",
+                   "start": ("the saved initial placement, not re-run" if a.start_from else "after the initial placement") if a.start == "ip" else "the generator's spread placement, initial placement skipped",
                    "l2": "working set > L2 (126 MB): cells, pins and bins stream from HBM each trial"},
         "form": a.form,
         "forms": {"mixed": {"iters_per_s": value, "ms_per_iter": mixed["ms"] / max(mixed["iters"], 1), "iters": mixed["iters"]},
@@ -318,6 +332,8 @@ def main():
                     help="time the loop after the initial placement, or from the generator's spread placement with the initial placement skipped (a short case for profiling)")
     ap.add_argument("--initial-place-only", action="store_true",
                     help="run the command through the initial placement once and print its time (a profiling case)")
+    ap.add_argument("--save-placement", default="", help="with --initial-place-only: save the locations (.npy)")
+    ap.add_argument("--start-from", default="", help="start the loop from saved initial-placement locations (a profiling case)")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

@@ -30,6 +30,14 @@ int gpl_kernel_density_scatter(int64_t n_cells, const int32_t *cx, const int32_t
   r.size_y = size_y;
   r.inv_size_x = 1.0 / size_x;
   r.inv_size_y = 1.0 / size_y;
+  {
+    std::vector<int32_t> hbx(nx + 1), hby(ny + 1);
+    e = cudaMemcpyAsync(hbx.data(), bx, hbx.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hby.data(), by, hby.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return (int)e;
+    r.narrow = narrow_tile(hbx, hby) ? 1 : 0;
+  }
   r.target_density = target_density;
   r.bx = bx;
   r.by = by;

@@ -27,6 +27,16 @@ struct Engine::Region {
 
 static int blocks_for(int64_t n, int per = kThreadsPerBlock) { return (int)std::max<int64_t>(1, (n + per - 1) / per); }
 
+// Whether the scatter's shared tile can sum in 32 bits: a cell adds at most a bin's area to a
+// bin (its overlap, times a scale of at most 1), once, so a block's sum for one bin stays below
+// kThreadsPerBlock times the largest bin area.
+bool narrow_tile(const std::vector<int32_t> &bx, const std::vector<int32_t> &by) {
+  int64_t w = 0, h = 0;
+  for (size_t k = 0; k + 1 < bx.size(); k++) w = std::max<int64_t>(w, (int64_t)bx[k + 1] - bx[k]);
+  for (size_t k = 0; k + 1 < by.size(); k++) h = std::max<int64_t>(h, (int64_t)by[k + 1] - by[k]);
+  return (double)w * (double)h * kThreadsPerBlock < 4294967295.0;
+}
+
 // The fixed areas as float (int64 -> float, round to nearest), as the bin density reads them.
 static std::vector<float> as_float(const std::vector<int64_t> &v) {
   std::vector<float> out(v.size());
@@ -231,7 +241,7 @@ void Engine::upload(const EngineSetup &s) {
       check(dmalloc(&r->slot[k], rs.n_cells), "alloc slots");
       if (!failed()) check(cudaMemsetAsync(r->slot[k], 0, std::max<int64_t>(rs.n_cells, 1) * sizeof(float2), st), "memset");
     }
-    r->nb_bins = (int)std::min<int64_t>(blocks_for(nb), 148 * 4);
+    r->nb_bins = rs.nx;  // the bin finalize runs one block per x row
     r->nb_cells = blocks_for(rs.n_cells);
     check(dmalloc(&r->part, (size_t)std::max(r->nb_bins * 2, r->nb_cells * 4)), "alloc partials");
     if (!failed()) {
@@ -252,6 +262,7 @@ void Engine::upload(const EngineSetup &s) {
     a.size_y = rs.size_y;
     a.inv_size_x = 1.0 / rs.size_x;
     a.inv_size_y = 1.0 / rs.size_y;
+    a.narrow = narrow_tile(rs.bx, rs.by) ? 1 : 0;
     a.target_density = rs.target_density;
     a.bx = r->bx;
     a.by = r->by;

@@ -16,9 +16,10 @@ __device__ __forceinline__ int32_t f2i_rz(float v) { return __float2int_rz(v); }
 __device__ __forceinline__ int64_t f2l_rz(float v) { return __float2ll_rz(v); }
 __device__ __forceinline__ int32_t d2i_rz(double v) { return __double2int_rz(v); }
 
-// `fastExp` (src/nesterov.rs:308-314): (1 + x/1024)^1024 by ten squarings, in float.
+// `fastExp` (src/nesterov.rs:308-314): (1 + x/1024)^1024 by ten squarings, in float. x/1024
+// is taken as x * 2^-10: both are the one correctly rounded value of the same real number.
 __device__ __forceinline__ float fast_exp(float x) {
-  float e = __fadd_rn(1.0f, __fdiv_rn(x, 1024.0f));
+  float e = __fadd_rn(1.0f, __fmul_rn(x, 0.0009765625f));
 #pragma unroll
   for (int i = 0; i < 10; i++) e = __fmul_rn(e, e);
   return e;

@@ -26,6 +26,7 @@ struct RegionArgs {
   int32_t lx, ly, ux, uy;        // the grid's box
   double size_x, size_y;
   double inv_size_x, inv_size_y; // 1 / size, rounded (the bin span's fast path)
+  int32_t narrow;                // a block's sum into one bin fits 32 bits (the scatter's tile)
   float target_density;
   const int32_t *bx, *by;        // bin edges, nx+1 and ny+1
   const float *scaled;           // bin area * target density (float)
@@ -71,6 +72,9 @@ __global__ void k_prev_slp(RegionArgs r, CellArgs c, float coef);
 __global__ void k_hpwl(WaArgs w, unsigned long long *out);
 __global__ void k_hpwl_tiles(WaArgs w, unsigned long long *out);
 __global__ void k_pack_centres(int64_t n, const int32_t *x, const int32_t *y, int2 *out);
+
+// Whether a grid's bins are small enough for the scatter's 32-bit shared tile.
+bool narrow_tile(const std::vector<int32_t> &bx, const std::vector<int32_t> &by);
 
 // Tiles of consecutive nets (at most kWaTilePins pins and kWaTileNets nets each) and the nets
 // too large for a tile, from the nets' pin starts.

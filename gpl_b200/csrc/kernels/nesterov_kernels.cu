@@ -27,7 +27,11 @@ __device__ __forceinline__ float inside_axis(float c, float half, float lo, floa
 // The block's cells lie close together (the device orders each region's cells along a Z
 // curve): the block first sums its addends in a shared-memory tile of the bins its cells
 // cover, then adds each touched bin to HBM once. A block whose cells spread over more than
-// kTileBins bins adds straight to HBM. Integer adds either way: the same accumulators.
+// kTileBins bins adds straight to HBM. Into the tile, a warp's lanes walk their cells' bins
+// in step, and lanes that hit the same bin in a step pool their addends first (one shared
+// atomic per distinct bin): after the initial placement many cells share a bin. The tile
+// holds 32-bit sums when a block's sum for one bin cannot reach 2^32 (RegionArgs::narrow).
+// Integer adds throughout: the same accumulators in any order.
 constexpr int kTileBins = 2048;
 
 __device__ __forceinline__ int64_t cell_bin_addend(const RegionArgs &r, int32_t dlx, int32_t dux, int32_t dly, int32_t duy, int32_t x, int32_t y, float scale, uint8_t kind) {
@@ -42,7 +46,8 @@ __device__ __forceinline__ int64_t cell_bin_addend(const RegionArgs &r, int32_t 
 }
 
 __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
-  __shared__ unsigned long long s_inst[kTileBins], s_fill[kTileBins];
+  __shared__ unsigned long long s_tile[2 * kTileBins];  // cells then fillers; 32-bit when narrow
+  __shared__ unsigned long long s_red[kThreads];
   __shared__ int s_box[4];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < r.n_cells;
@@ -51,48 +56,48 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
   float scale = 0.0f;
   uint8_t kind = 0;
   if (valid) {
-  float2 p = make_float2(0.0f, 0.0f);
-  if (mode == PLACE_AT) {
-    p = coords[i];
-  } else if (mode == PLACE_GIVEN) {
-  } else {
-    float2 cs = c.cur_slp[i];
-    if (c.locked && c.locked[i]) {
-      c.next[i] = c.cur[i];
-      c.next_slp[i] = cs;
-      p = cs;
+    float2 p = make_float2(0.0f, 0.0f);
+    if (mode == PLACE_AT) {
+      p = coords[i];
+    } else if (mode == PLACE_GIVEN) {
     } else {
-      float2 g = c.cur_slp_sum[i], cu = c.cur[i];
-      float nx = __fadd_rn(cs.x, __fmul_rn(step, g.x));
-      float ny = __fadd_rn(cs.y, __fmul_rn(step, g.y));
-      float sx = __fadd_rn(nx, __fmul_rn(coeff, __fsub_rn(nx, cu.x)));
-      float sy = __fadd_rn(ny, __fmul_rn(coeff, __fsub_rn(ny, cu.y)));
-      float hx = (float)c.hx[i], hy = (float)c.hy[i];
-      float glx = (float)r.lx, gly = (float)r.ly, gux = (float)r.ux, guy = (float)r.uy;
-      c.next[i] = make_float2(inside_axis(nx, hx, glx, gux), inside_axis(ny, hy, gly, guy));
-      p = make_float2(inside_axis(sx, hx, glx, gux), inside_axis(sy, hy, gly, guy));
-      c.next_slp[i] = p;
+      float2 cs = c.cur_slp[i];
+      if (c.locked && c.locked[i]) {
+        c.next[i] = c.cur[i];
+        c.next_slp[i] = cs;
+        p = cs;
+      } else {
+        float2 g = c.cur_slp_sum[i], cu = c.cur[i];
+        float nx = __fadd_rn(cs.x, __fmul_rn(step, g.x));
+        float ny = __fadd_rn(cs.y, __fmul_rn(step, g.y));
+        float sx = __fadd_rn(nx, __fmul_rn(coeff, __fsub_rn(nx, cu.x)));
+        float sy = __fadd_rn(ny, __fmul_rn(coeff, __fsub_rn(ny, cu.y)));
+        float hx = (float)c.hx[i], hy = (float)c.hy[i];
+        float glx = (float)r.lx, gly = (float)r.ly, gux = (float)r.ux, guy = (float)r.uy;
+        c.next[i] = make_float2(inside_axis(nx, hx, glx, gux), inside_axis(ny, hy, gly, guy));
+        p = make_float2(inside_axis(sx, hx, glx, gux), inside_axis(sy, hy, gly, guy));
+        c.next_slp[i] = p;
+      }
     }
-  }
-  int32_t cx, cy;
-  if (mode == PLACE_GIVEN) {
-    int2 d = c.dc[i];
-    cx = d.x;
-    cy = d.y;
-  } else {
-    cx = f2i_rz(p.x);
-    cy = f2i_rz(p.y);
-    c.dc[i] = make_int2(cx, cy);
-  }
-  int32_t hx = c.hx[i], hy = c.hy[i];
-  dlx = cx - hx;
-  dux = cx + hx;
-  dly = cy - hy;
-  duy = cy + hy;
-  bin_span(dlx, dux, r.lx, r.size_x, r.inv_size_x, r.nx, x0, x1);
-  bin_span(dly, duy, r.ly, r.size_y, r.inv_size_y, r.ny, y0, y1);
-  scale = c.dscale[i];
-  kind = c.kind[i];
+    int32_t cx, cy;
+    if (mode == PLACE_GIVEN) {
+      int2 d = c.dc[i];
+      cx = d.x;
+      cy = d.y;
+    } else {
+      cx = f2i_rz(p.x);
+      cy = f2i_rz(p.y);
+      c.dc[i] = make_int2(cx, cy);
+    }
+    int32_t hx = c.hx[i], hy = c.hy[i];
+    dlx = cx - hx;
+    dux = cx + hx;
+    dly = cy - hy;
+    duy = cy + hy;
+    bin_span(dlx, dux, r.lx, r.size_x, r.inv_size_x, r.nx, x0, x1);
+    bin_span(dly, duy, r.ly, r.size_y, r.inv_size_y, r.ny, y0, y1);
+    scale = c.dscale[i];
+    kind = c.kind[i];
   }
   // the block's bin box
   if (threadIdx.x == 0) {
@@ -102,10 +107,11 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
     s_box[3] = INT32_MIN;
   }
   __syncthreads();
-  bool any = valid && x0 < x1 && y0 < y1;
+  const bool any = valid && x0 < x1 && y0 < y1;
   int32_t wx0 = __reduce_min_sync(0xffffffffu, any ? x0 : INT32_MAX), wx1 = __reduce_max_sync(0xffffffffu, any ? x1 : INT32_MIN);
   int32_t wy0 = __reduce_min_sync(0xffffffffu, any ? y0 : INT32_MAX), wy1 = __reduce_max_sync(0xffffffffu, any ? y1 : INT32_MIN);
-  if ((threadIdx.x & 31) == 0) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
     atomicMin(&s_box[0], wx0);
     atomicMax(&s_box[1], wx1);
     atomicMin(&s_box[2], wy0);
@@ -115,52 +121,99 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
   const int32_t tx0 = s_box[0], ty0 = s_box[2];
   const int32_t tw = s_box[1] - tx0, th = s_box[3] - ty0;
   const bool tile = tw > 0 && th > 0 && (int64_t)tw * th <= kTileBins;
-  if (tile) {
-    for (int k = threadIdx.x; k < tw * th; k += blockDim.x) {
-      s_inst[k] = 0;
-      s_fill[k] = 0;
+  const bool narrow = r.narrow != 0;
+  unsigned int *t32 = reinterpret_cast<unsigned int *>(s_tile);
+  if (!tile) {
+    if (any) {
+      unsigned long long *acc = (unsigned long long *)(kind == CELL_FILLER ? r.acc_fill : r.acc_inst);
+      for (int32_t y = y0; y < y1; y++)
+        for (int32_t x = x0; x < x1; x++) {
+          int64_t v = cell_bin_addend(r, dlx, dux, dly, duy, x, y, scale, kind);
+          if (v) atomicAdd(&acc[(size_t)x * r.ny + y], (unsigned long long)v);
+        }
     }
-    __syncthreads();
+    return;
   }
-  if (any) {
-    unsigned long long *acc = (unsigned long long *)(kind == CELL_FILLER ? r.acc_fill : r.acc_inst);
-    unsigned long long *sacc = kind == CELL_FILLER ? s_fill : s_inst;
-    for (int32_t y = y0; y < y1; y++)
-      for (int32_t x = x0; x < x1; x++) {
-        int64_t v = cell_bin_addend(r, dlx, dux, dly, duy, x, y, scale, kind);
-        if (!v) continue;
-        if (tile)
-          atomicAdd(&sacc[(x - tx0) * th + (y - ty0)], (unsigned long long)v);
-        else
-          atomicAdd(&acc[(size_t)x * r.ny + y], (unsigned long long)v);
+  const int nt = tw * th;
+  for (int k = threadIdx.x; k < 2 * kTileBins; k += blockDim.x) s_tile[k] = 0;
+  __syncthreads();
+  // the warp's lanes in step over their bins (x outer, y inner); key = tile slot * 2 + filler
+  const int nb = any ? (x1 - x0) * (y1 - y0) : 0;
+  const int rounds = __reduce_max_sync(0xffffffffu, nb);
+  int32_t x = x0, y = y0;
+  for (int q = 0; q < rounds; q++) {
+    int key = -1;
+    unsigned long long v = 0;
+    if (q < nb) {
+      int64_t a = cell_bin_addend(r, dlx, dux, dly, duy, x, y, scale, kind);
+      if (a) {
+        v = (unsigned long long)a;
+        key = (((x - tx0) * th + (y - ty0)) << 1) | (kind == CELL_FILLER ? 1 : 0);
       }
-  }
-  if (tile) {
-    __syncthreads();
-    for (int k = threadIdx.x; k < tw * th; k += blockDim.x) {
-      size_t g = (size_t)(tx0 + k / th) * r.ny + (ty0 + k % th);
-      if (s_inst[k]) atomicAdd((unsigned long long *)&r.acc_inst[g], s_inst[k]);
-      if (s_fill[k]) atomicAdd((unsigned long long *)&r.acc_fill[g], s_fill[k]);
+      if (++y == y1) {
+        y = y0;
+        x++;
+      }
     }
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    s_red[threadIdx.x] = v;
+    __syncwarp();
+    if (key >= 0 && lane == __ffs(peers) - 1) {
+      unsigned long long sum = 0;
+      for (unsigned m = peers; m; m &= m - 1) sum += s_red[(threadIdx.x & ~31) + __ffs(m) - 1];
+      int slot = (key & 1) * kTileBins + (key >> 1);
+      if (narrow)
+        atomicAdd(&t32[slot], (unsigned int)sum);
+      else
+        atomicAdd(&s_tile[slot], sum);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nt; k += blockDim.x) {
+    size_t g = (size_t)(tx0 + k / th) * r.ny + (ty0 + k % th);
+    unsigned long long vi = narrow ? t32[k] : s_tile[k];
+    unsigned long long vf = narrow ? t32[kTileBins + k] : s_tile[kTileBins + k];
+    if (vi) atomicAdd((unsigned long long *)&r.acc_inst[g], vi);
+    if (vf) atomicAdd((unsigned long long *)&r.acc_fill[g], vf);
   }
 }
 
 // ---- bins: density and overflow (:2252-2262), accumulators cleared for the next scatter.
-// Optionally the density split into bf16 hi/lo for the tensor-core solver. Blocks walk whole
-// x rows (threads along y), so no index is divided.
-__global__ void k_bins_finalize(RegionArgs r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld) {
+// Optionally the density split into bf16 hi/lo for the tensor-core solver. One block per x
+// row (threads along y, kBinsPerThread bins each with their loads issued together), so no
+// index is divided; block partials of the two overflow sums.
+constexpr int kBinsPerThread = 4;
+
+__global__ void __launch_bounds__(kThreads) k_bins_finalize(RegionArgs r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld) {
   __shared__ double sh[kThreads / 32];
   double o_sum = 0.0, ou_sum = 0.0;
-  for (int32_t x = blockIdx.x; x < r.nx; x += gridDim.x) {
-    const size_t row = (size_t)x * r.ny;
-    for (int32_t y = threadIdx.x; y < r.ny; y += blockDim.x) {
+  const int32_t x = blockIdx.x;
+  const size_t row = (size_t)x * r.ny;
+  for (int32_t y0 = threadIdx.x; y0 < r.ny; y0 += blockDim.x * kBinsPerThread) {
+    int64_t inst[kBinsPerThread], fill[kBinsPerThread];
+    float fn[kBinsPerThread], fnu[kBinsPerThread], sc[kBinsPerThread];
+#pragma unroll
+    for (int q = 0; q < kBinsPerThread; q++) {
+      int32_t y = y0 + q * blockDim.x;
+      if (y < r.ny) {
+        size_t k = row + y;
+        inst[q] = r.acc_inst[k];
+        fill[q] = r.acc_fill[k];
+        fn[q] = r.non_place[k];
+        fnu[q] = r.non_place_u[k];
+        sc[q] = r.scaled[k];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kBinsPerThread; q++) {
+      int32_t y = y0 + q * blockDim.x;
+      if (y >= r.ny) continue;
       size_t k = row + y;
-      int64_t inst = r.acc_inst[k], fill = r.acc_fill[k];
       r.acc_inst[k] = 0;
       r.acc_fill[k] = 0;
-      float fi = __ll2float_rn(inst), fn = r.non_place[k], fnu = r.non_place_u[k];
-      float sc = r.scaled[k];
-      float d = __fdiv_rn(__fadd_rn(__fadd_rn(fi, __ll2float_rn(fill)), fn), sc);
+      float fi = __ll2float_rn(inst[q]);
+      float d = __fdiv_rn(__fadd_rn(__fadd_rn(fi, __ll2float_rn(fill[q])), fn[q]), sc[q]);
       r.density[k] = d;
       if (dens_split) {
         __nv_bfloat16 hi = __float2bfloat16_rn(d);
@@ -168,8 +221,8 @@ __global__ void k_bins_finalize(RegionArgs r, double *__restrict__ partials, __n
         dens_split[(size_t)x * split_ld + y] = hi;
         dens_split[(size_t)x * split_ld + r.ny + y] = lo;
       }
-      float o = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fn), sc));
-      float ou = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fnu), sc));
+      float o = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fn[q]), sc[q]));
+      float ou = fmaxf(0.0f, __fsub_rn(__fadd_rn(fi, fnu[q]), sc[q]));
       o_sum += (double)o;
       ou_sum += (double)ou;
     }

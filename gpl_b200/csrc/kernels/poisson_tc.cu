@@ -2,17 +2,18 @@
 //
 // Every operand X (a basis matrix, the density, an intermediate) is stored as two bfloat16
 // halves side by side along K: [X_hi | X_lo] with X_hi = bf16(X) and X_lo = bf16(X - X_hi).
-// One GEMM D = A B^T then runs three K segments, A_hi B_hi + A_hi B_lo + A_lo B_hi (the
-// compensated product; A_lo B_lo is below FP32 accumulation noise), accumulated in FP32 in
-// tensor memory. The epilogue reads the accumulator back (tcgen05.ld) and writes the next
-// GEMM's split operand directly, or the spectral step's two operands, or the FP32 field.
+// One GEMM D = A B^T takes, per K step, the compensated product A_hi B_hi + A_hi B_lo +
+// A_lo B_hi (A_lo B_lo is below FP32 accumulation noise), accumulated in FP32 in tensor
+// memory. The epilogue reads the accumulator back (tcgen05.ld) and writes the next GEMM's
+// split operand directly, or the spectral step's two operands, or the FP32 field.
 //
-// Kernel: one 128 x 64 output tile per CTA of 128 threads. Thread 0 issues the TMA loads of
-// the K-blocks (128B-swizzled 128x64 A and 64x64 B bf16 tiles) into a 6-stage ring; thread 32
-// issues tcgen05.mma (M=128, N=64, K=16, kind::f16, bf16 in, f32 accumulate) as the stages
-// land, committing each stage back to the producer; after the last K-block all four warps
-// read their 32 TMEM lanes. Every wait is bounded by the GPU's global timer (1 s): a wait that
-// runs out records an error word, and the CTA drains and returns.
+// Kernel: one 128 x 128 output tile per CTA of 128 threads. Thread 0 issues the TMA loads of
+// each K-block (128B-swizzled 128x64 bf16 tiles: A_hi, A_lo, B_hi, B_lo) into a 3-stage ring;
+// thread 32 issues tcgen05.mma (M=128, N=128, K=16, kind::f16, bf16 in, f32 accumulate),
+// three per K step, as the stages land, committing each stage back to the producer; after the
+// last K-block all four warps read their 32 TMEM lanes, 32 columns at a time. Every wait is
+// bounded by the GPU's global timer (1 s): a wait that runs out records an error word, and
+// the CTA drains and returns.
 //
 // The four launches of a solve (see poisson.cu for the algebra):
 //   1  T1t = CyTs rho^T                      split out
@@ -35,12 +36,16 @@ namespace gpl {
 
 namespace {
 
-constexpr int BM = 128, BN = 64, BK = 64, STAGES = 6;
-constexpr int A_TILE = BM * BK * 2;            // 16 KB
-constexpr int B_TILE = BN * BK * 2;            // 8 KB
-constexpr int STAGE_BYTES = A_TILE + B_TILE;   // 24 KB, a multiple of 1 KB
+// A stage holds one K-block of both halves of both operands: A_hi, A_lo (BM x BK each) and
+// B_hi, B_lo (BN x BK each); its three products hi*hi, hi*lo, lo*hi all accumulate into the
+// one TMEM tile, so each operand byte crosses from L2 once per output tile.
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3;
+constexpr int A_TILE = BM * BK * 2;                    // 16 KB
+constexpr int B_TILE = BN * BK * 2;                    // 16 KB
+constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;   // 64 KB, a multiple of 1 KB
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr uint32_t TMEM_COLS = 64;             // BN fp32 accumulator columns
+constexpr uint32_t TMEM_COLS = BN;                     // fp32 accumulator columns
+constexpr int EPI_COLS = 32;                           // accumulator columns per epilogue step
 constexpr uint64_t WAIT_NS = 1000000000ull;    // a wait that lasts a second is an error
 
 enum Epi { EPI_SPLIT = 0, EPI_SPECTRAL = 1, EPI_F32 = 2 };
@@ -103,7 +108,7 @@ __device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, uint
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
-// kind::f16 instruction descriptor: D f32, A and B bf16, both K-major, M=128, N=64.
+// kind::f16 instruction descriptor: D f32, A and B bf16, both K-major, M=BM, N=BN.
 constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 
 __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
@@ -128,9 +133,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
 }
 
 __device__ __forceinline__ void split_store(__nv_bfloat16 *row_hi, __nv_bfloat16 *row_lo, const float *v) {
-  // 64 values: hi and lo halves, 16-byte stores
+  // EPI_COLS values: hi and lo halves, 16-byte stores
 #pragma unroll
-  for (int c = 0; c < BN; c += 8) {
+  for (int c = 0; c < EPI_COLS; c += 8) {
     __align__(16) __nv_bfloat16 h[8], l[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) {
@@ -157,7 +162,7 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
   const CUtensorMap *mA = z ? &tA1 : &tA0;
   const CUtensorMap *mB = z ? &tB1 : &tB0;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  const int kb_per_seg = args.K / BK, nkb = 3 * kb_per_seg;
+  const int nkb = args.K / BK;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; s++) {
@@ -178,69 +183,83 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
   const uint32_t tmem = *tmem_slot;
 
   if (threadIdx.x == 0) {
-    // producer: K-block kb of segment seg reads A at column (seg == 2 ? K : 0) + k0 and B at
-    // column (seg == 1 ? K : 0) + k0: hi*hi, hi*lo, lo*hi
+    // producer: K-block kb brings A_hi, A_lo (columns k0 and K + k0 of A) and B_hi, B_lo
     for (int kb = 0; kb < nkb; kb++) {
       int s = kb % STAGES, round = kb / STAGES;
       if (round > 0 && !mbar_wait(&empty[s], (round - 1) & 1, fail, args.err, 1)) break;
-      int seg = kb / kb_per_seg, k0 = (kb % kb_per_seg) * BK;
-      int ax = (seg == 2 ? args.K : 0) + k0, bx = (seg == 1 ? args.K : 0) + k0;
-      uint8_t *sa = smem + s * STAGE_BYTES, *sb = sa + A_TILE;
+      int k0 = kb * BK;
+      uint8_t *st = smem + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
-      tma_load(sa, mA, &full[s], ax, m0);
-      tma_load(sb, mB, &full[s], bx, n0);
+      tma_load(st, mA, &full[s], k0, m0);
+      tma_load(st + A_TILE, mA, &full[s], args.K + k0, m0);
+      tma_load(st + 2 * A_TILE, mB, &full[s], k0, n0);
+      tma_load(st + 2 * A_TILE + B_TILE, mB, &full[s], args.K + k0, n0);
     }
   } else if (threadIdx.x == 32) {
-    // MMA issuer
+    // MMA issuer: per 16-wide K step, hi*hi, hi*lo, lo*hi
     for (int kb = 0; kb < nkb; kb++) {
       int s = kb % STAGES, round = kb / STAGES;
       if (!mbar_wait(&full[s], round & 1, fail, args.err, 2)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      uint32_t a = smem_u32(smem + s * STAGE_BYTES), b = a + A_TILE;
+      uint32_t ahi = smem_u32(smem + s * STAGE_BYTES), alo = ahi + A_TILE, bhi = ahi + 2 * A_TILE, blo = bhi + B_TILE;
 #pragma unroll
-      for (int kk = 0; kk < BK / 16; kk++) umma(tmem, smem_desc(a + kk * 32), smem_desc(b + kk * 32), (kb > 0 || kk > 0) ? 1u : 0u);
+      for (int kk = 0; kk < BK / 16; kk++) {
+        uint32_t o = kk * 32;
+        umma(tmem, smem_desc(ahi + o), smem_desc(bhi + o), (kb > 0 || kk > 0) ? 1u : 0u);
+        umma(tmem, smem_desc(ahi + o), smem_desc(blo + o), 1u);
+        umma(tmem, smem_desc(alo + o), smem_desc(bhi + o), 1u);
+      }
       umma_commit(&empty[s]);
     }
     umma_commit(done);
   }
   __syncwarp();
-  // epilogue: every warp reads its 32 lanes (rows) of the 128 x 64 accumulator; lane 0 waits
-  // for the last commit, so the warp stays converged for the aligned TMEM loads
+  // epilogue: every warp reads its 32 lanes (rows) of the BM x BN accumulator, EPI_COLS
+  // columns at a time; lane 0 waits for the last commit, so the warp stays converged for the
+  // aligned TMEM loads
   int okw = 0;
   if (lane == 0) okw = mbar_wait(done, 0, fail, args.err, 3) && !*fail;
   okw = __shfl_sync(0xffffffffu, okw, 0);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (okw) {
-    float v[BN];
-    uint32_t base = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
-    for (int c = 0; c < BN; c += 16) tmem_ld16(base + c, v + c);
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16);
     const int m = m0 + warp * 32 + lane;
     const TcOut &o = args.o[z];
-    if (m < args.M) {
-      if (EPI == EPI_F32) {
-        float *row = (float *)o.out0 + (size_t)m * o.ld + n0;
+    const bool in = m < args.M;
+    float wxu = 0.0f, wx2u = 0.0f;
+    if (EPI == EPI_SPECTRAL && in) {
+      wxu = args.wx[m];
+      wx2u = args.wx2[m];
+    }
+#pragma unroll 1
+    for (int c0 = 0; c0 < BN; c0 += EPI_COLS) {
+      float v[EPI_COLS];
 #pragma unroll
-        for (int c = 0; c < BN; c += 4) *reinterpret_cast<float4 *>(row + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
+      for (int c = 0; c < EPI_COLS; c += 16) tmem_ld16(base + c0 + c, v + c);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (!in) continue;
+      const int nb = n0 + c0;
+      if (EPI == EPI_F32) {
+        float *row = (float *)o.out0 + (size_t)m * o.ld + nb;
+#pragma unroll
+        for (int c = 0; c < EPI_COLS; c += 4) *reinterpret_cast<float4 *>(row + c) = make_float4(v[c], v[c + 1], v[c + 2], v[c + 3]);
       } else if (EPI == EPI_SPLIT) {
         __nv_bfloat16 *row = (__nv_bfloat16 *)o.out0 + (size_t)m * 2 * o.ld;
-        split_store(row + n0, row + o.ld + n0, v);
+        split_store(row + nb, row + o.ld + nb, v);
       } else {
         // the spectral step (src/nesterov.rs:425-440) on the scaled forward transform
-        float ex[BN], ey[BN];
-        float wxu = args.wx[m], wx2u = args.wx2[m];
+        float ex[EPI_COLS], ey[EPI_COLS];
 #pragma unroll
-        for (int c = 0; c < BN; c++) {
-          int n = n0 + c;
+        for (int c = 0; c < EPI_COLS; c++) {
+          int n = nb + c;
           float p = (m == 0 && n == 0) ? 0.0f : __fdiv_rn(v[c], __fadd_rn(wx2u, args.wy2[n]));
           ex[c] = __fmul_rn(p, wxu);
           ey[c] = __fmul_rn(p, args.wy[n]);
         }
         __nv_bfloat16 *rx = (__nv_bfloat16 *)o.out0 + (size_t)m * 2 * o.ld;
         __nv_bfloat16 *ry = (__nv_bfloat16 *)o.out1 + (size_t)m * 2 * o.ld;
-        split_store(rx + n0, rx + o.ld + n0, ex);
-        split_store(ry + n0, ry + o.ld + n0, ey);
+        split_store(rx + nb, rx + o.ld + nb, ex);
+        split_store(ry + nb, ry + o.ld + nb, ey);
       }
     }
   }

@@ -18,6 +18,10 @@ generator for every size):
   cover the stated fraction of the core; non-overlapping, on the site/row grid.
 * Core: the stated size, or square and sized for the stated utilisation
   (movable area / (core area - macro area)).
+* Region groups (`regions=(kx, ky, k)`): the core is cut into kx x ky tiles on the site/row
+  grid and the first k tiles (row by row) become regions, one group each; a cell joins the
+  group whose tile holds its latent position, the rest stay top-level. No fixed instance
+  then (a fixed instance against a region's boundary is outside the placer's model).
 """
 from __future__ import annotations
 
@@ -40,6 +44,10 @@ PRESETS = {
     # 1M cells, ~1.05M nets, ~4M pins, 32 macros over 15 % of the core.
     "cfg3": dict(cells=1_000_000, nets=1_050_000, w_min=2, w_max=24, util=0.60, n_io=256,
                  macros=32, macro_frac=0.15, max_degree=64, seed=3),
+    # 4 region groups over a 3 x 2 grid of core tiles (2000 cells, no macro): the small
+    # multi-region case the parity tests run on both sides.
+    "cfg4s": dict(cells=2000, nets=2100, w_min=2, w_max=12, util=0.55, n_io=32,
+                  macros=0, macro_frac=0.0, max_degree=16, seed=4, regions=(3, 2, 4)),
     # 2M cells, ~2.1M nets, ~8M pins, as cfg3.
     "cfg5": dict(cells=2_000_000, nets=2_100_000, w_min=2, w_max=24, util=0.60, n_io=256,
                  macros=32, macro_frac=0.15, max_degree=64, seed=5),
@@ -227,6 +235,25 @@ def generate(cfg="cfg1", **over) -> Design:
     row_box[:, 3] = row_box[:, 1] + ROW_H
     row_site = np.tile(np.array([SITE_W, ROW_H], np.int32), (n_rows, 1))
 
+    groups = {}
+    if p.get("regions"):
+        kx, ky, k = p["regions"]
+        if n_mac:
+            raise ValueError("region groups and fixed macros do not mix")
+        xs = [int(round(core_w * i / kx / SITE_W)) * SITE_W for i in range(kx + 1)]
+        ys = [int(round(core_h * j / ky / ROW_H)) * ROW_H for j in range(ky + 1)]
+        boxes = [(xs[t % kx], ys[t // kx], xs[t % kx + 1], ys[t // kx + 1]) for t in range(k)]
+        tx = np.minimum((lat_x * kx / core_w).astype(np.int64), kx - 1)
+        ty = np.minimum((lat_y * ky / core_h).astype(np.int64), ky - 1)
+        tile = ty * kx + tx
+        inst_group = np.full(n_inst, -1, np.int32)
+        inst_group[:m] = np.where(tile < k, tile, -1)
+        groups = dict(
+            inst_group=inst_group, group_names=[f"region{g}" for g in range(k)],
+            group_region=np.arange(k, dtype=np.int32),
+            region_bound_start=np.arange(k + 1, dtype=np.int32), region_bounds=np.array(boxes, np.int32).reshape(k, 4),
+            region_group_start=np.arange(k + 1, dtype=np.int32), region_groups=np.arange(k, dtype=np.int32))
+
     bstart_n = np.concatenate([[0], np.cumsum(has_io.astype(np.int64))])
     return Design(
         dbu=DBU, die=(0, 0, die_w, die_h), core=(0, 0, core_w, core_h),
@@ -237,4 +264,5 @@ def generate(cfg="cfg1", **over) -> Design:
         bterm_flags=np.full(n_io, BTERM_PLACED | BTERM_FIXED, np.uint8),
         meta=dict(config=cfg if isinstance(cfg, str) else "custom", params=p, placed=placed,
                   cells=m, macros=n_mac, nets=n_nets, pins=int(total + n_io)),
+        **groups,
     )

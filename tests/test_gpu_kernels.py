@@ -36,7 +36,8 @@ def random_cells(rng, n, bx, by, macro_frac=0.02, filler_frac=0.2):
     return cx, cy, hx, hy, scale, kind
 
 
-@pytest.mark.parametrize("nx,ny,aligned", [(64, 64, False), (96, 40, False), (64, 64, True), (40, 80, True)])
+# (8, 8): bins so large that the scatter's shared tile sums in 64 bits
+@pytest.mark.parametrize("nx,ny,aligned", [(64, 64, False), (96, 40, False), (64, 64, True), (40, 80, True), (8, 8, False)])
 def test_density_scatter_bit_exact(L, nx, ny, aligned):
     rng = np.random.default_rng(nx * 1000 + ny + aligned)
     if aligned:

@@ -101,3 +101,24 @@ def test_routability_driven_matches_the_oracle(cfg1):
     assert abs(got["final_hpwl"] - ref["final_hpwl"]) <= 0.05 * ref["final_hpwl"]
     area = lambda r: float(_lines_with(r["lines"], "1014")[0].split(":")[1].split("(")[0])
     assert abs(area(got) - area(ref)) <= 0.01 * area(ref)
+
+
+def test_region_groups_match_the_oracle():
+    """Four region groups beside the top level (five Nesterov regions, each with its own bin
+    grid, sharing the WA coefficient and the back-tracking): identical construction lines,
+    every region finishing within 10 iterations of the oracle's, final HPWL within 0.1 % and
+    overflow within 0.005."""
+    d = synth.generate("cfg4s")
+    args = ["-density", "0.70"]
+    ref = oracle.global_placement(d, args)
+    got = engine.global_placement(d, args)
+    assert got["status"] == "placed", got["reason"]
+    assert header(got["lines"]) == header(ref["lines"])
+    assert got["bases"] == ref["bases"]
+    fin = lambda r: {l.split("'")[1] if "'" in l else "top": int(l.split()[-1]) for l in r["lines"] if "GPL-1016]" in l or "GPL-1001]" in l}
+    a, b = fin(got), fin(ref)
+    assert a.keys() == b.keys() and len(a) == 5
+    for k in a:
+        assert abs(a[k] - b[k]) <= 10, (k, a[k], b[k])
+    assert abs(got["final_hpwl"] - ref["final_hpwl"]) <= 1e-3 * ref["final_hpwl"]
+    assert abs(got["final_overflow"] - ref["final_overflow"]) <= 0.005

@@ -249,6 +249,7 @@ def ours(a):
     cpu = None
     if world == 1 and not a.no_cpu_baseline:
         cpu = cpu_baseline(a)
+    precision = precision_report(local, nx)
     out = {
         "metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": mixed["ms"] / max(mixed["iters"], 1), "higher_is_better": True, "scaling": "weak",
@@ -262,9 +263,36 @@ def ours(a):
                   "fp32": {"iters_per_s": value_fp32, "ms_per_iter": fp32["ms"] / max(fp32["iters"], 1), "iters": fp32["iters"]},
                   "mixed_over_fp32": value / value_fp32 if value_fp32 else None},
         "phases": phases, "roofline": roof, "gpu_launches": mixed["launches"], "clocks": mixed["clocks"],
-        "e2e": e2e, "cpu_baseline": cpu,
+        "e2e": e2e, "cpu_baseline": cpu, "precision": precision,
     }
     print(json.dumps(out))
+
+
+def precision_report(local, n):
+    """Each form's field error against the FP64 device solve (the same transforms in double),
+    on a seeded density of the workload's grid: max |error| over max |field|."""
+    import ctypes as C
+    import torch
+    from gpl_b200 import engine
+    L = engine.lib()
+    L.gpl_kernel_poisson_fp64.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(n)
+    dens = torch.from_numpy((rng.random(n * n) * 1.5).astype(np.float32)).cuda(local)
+    wx = (np.pi * np.arange(n) / n).astype(np.float32)
+    wy = wx.copy()
+    st = C.c_void_p(torch.cuda.current_stream(local).cuda_stream)
+    ex, ey = torch.zeros(n * n, dtype=torch.float64, device=f"cuda:{local}"), torch.zeros(n * n, dtype=torch.float64, device=f"cuda:{local}")
+    if L.gpl_kernel_poisson_fp64(n, n, wx.ctypes.data, wy.ctypes.data, C.c_void_p(dens.data_ptr()), C.c_void_p(ex.data_ptr()), C.c_void_p(ey.data_ptr()), st) != 0:
+        return None
+    out = {"yardstick": f"FP64 device solve, {n}x{n} seeded density"}
+    for name, mode in (("mixed", 1), ("fp32", 0)):
+        gx, gy = torch.zeros(n * n, device=f"cuda:{local}"), torch.zeros(n * n, device=f"cuda:{local}")
+        if L.gpl_kernel_poisson(n, n, wx.ctypes.data, wy.ctypes.data, C.c_void_p(dens.data_ptr()), C.c_void_p(gx.data_ptr()), C.c_void_p(gy.data_ptr()), mode, st) != 0:
+            continue
+        torch.cuda.synchronize(local)
+        e = max(float((gx.double() - ex).abs().max() / ex.abs().max()), float((gy.double() - ey).abs().max() / ey.abs().max()))
+        out[f"field_rel_err_{name}"] = e
+    return out
 
 
 def cpu_baseline(a):

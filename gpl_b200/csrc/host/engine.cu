@@ -168,6 +168,7 @@ void Engine::release() {
 
 void Engine::upload(const EngineSetup &s) {
   release();
+  hpwl_ready_ = false;  // the density centres move
   if (failed()) return;
   cudaStream_t st = stream_;
   n_cells_ = (int64_t)s.hx.size();
@@ -347,6 +348,7 @@ std::vector<float> Engine::get_coords(int b, SlotId slot) {
 
 void Engine::place_at(int b, SlotId slot) {
   if (failed()) return;
+  hpwl_ready_ = false;  // the density centres move
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
   ph_begin(PH_PLACE);
@@ -362,6 +364,7 @@ void Engine::place_at(int b, SlotId slot) {
 
 void Engine::nesterov_step(int b, float step, float coeff) {
   if (failed()) return;
+  hpwl_ready_ = false;  // the density centres move
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
   ph_begin(PH_PLACE);
@@ -403,6 +406,10 @@ WaArgs Engine::wa_args() const {
 void Engine::wa(float cx, float cy) {
   if (failed() || n_nets_ == 0) return;
   WaArgs w = wa_args();
+  // the kernels add the HPWL of these same positions: hpwl() reads it without a launch
+  check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), stream_), "wa");
+  w.hpwl_out = hpwl_acc_;
+  hpwl_ready_ = true;
   ph_begin(PH_WA);
   if (n_tiles_) {
     launches += 1;
@@ -469,6 +476,7 @@ void Engine::fetch() {
 int64_t Engine::hpwl() {
   if (failed()) return 0;
   WaArgs w = wa_args();
+  if (!hpwl_ready_) {
   check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), stream_), "hpwl");
   ph_begin(PH_HPWL);
   if (n_tiles_) {
@@ -480,6 +488,8 @@ int64_t Engine::hpwl() {
     k_hpwl<<<blocks_for(n_big_), kThreadsPerBlock, 0, stream_>>>(w, hpwl_acc_);
   }
   ph_end(PH_HPWL);
+  hpwl_ready_ = true;
+  }
   unsigned long long h = 0;
   check(cudaMemcpyAsync(&h, hpwl_acc_, sizeof h, cudaMemcpyDeviceToHost, stream_), "hpwl");
   d2h_bytes += 8;

@@ -138,6 +138,7 @@ class Engine {
   float *net_weight_ = nullptr;
   float2 *pin_grad_ = nullptr;  // the WA force of every pin of a cell, cell-major (cell_pins order)
   unsigned long long *hpwl_acc_ = nullptr;
+  bool hpwl_ready_ = false;  // hpwl_acc_ holds the HPWL of the current centres (from the WA)
   // initial placement scratch
   void *ip_scratch_ = nullptr;
   size_t ip_scratch_bytes_ = 0;

@@ -16,6 +16,7 @@
 #include "../kernels/engine_kernels.h"
 #include "engine.h"
 #include "../kernels/b2b.h"
+#include "../kernels/rudy.h"
 #include "host.h"
 
 namespace gpl {
@@ -287,6 +288,19 @@ struct Rudy {
     blockage.assign((size_t)cnt_x * cnt_y, 0.0f);
   }
   size_t at(int32_t x, int32_t y) const { return (size_t)(x * cnt_y + y); }
+  // The demand map on the device (kernels/rudy.cu: the same deposits, added atomically), the
+  // blockage on the host from the router's (capacity, reduction) bytes.
+  cudaStream_t stream = nullptr;
+  int4 *d_boxes = nullptr;
+  float *d_demand = nullptr;
+  size_t box_cap = 0;
+  Rudy() = default;
+  Rudy(const Rudy &) = delete;
+  Rudy &operator=(const Rudy &) = delete;
+  ~Rudy() {
+    if (d_boxes) cudaFree(d_boxes);
+    if (d_demand) cudaFree(d_demand);
+  }
   void calculate(const std::vector<uint8_t> &cap_red, const std::vector<std::array<int32_t, 4>> &nets) {
     std::fill(demand.begin(), demand.end(), 0.0f);
     std::fill(blockage.begin(), blockage.end(), 0.0f);
@@ -294,29 +308,21 @@ struct Rudy {
       uint8_t cap = cap_red[2 * i], red = cap_red[2 * i + 1];
       blockage[i] = cap == 0 ? 1.0f : fminr((float)red / (float)cap, 1.0f);
     }
-    for (auto &n : nets) visit(n);
-  }
-  // `visitNetTiles` (src/route_base.rs:224-253).
-  void visit(const std::array<int32_t, 4> &b) {
-    int32_t xl = b[0], yl = b[1], xh = b[2], yh = b[3];
-    if (xl > xh || yl > yh) return;
-    int64_t net_area = (int64_t)(xh - xl) * (int64_t)(yh - yl);
-    if (net_area == 0) return;
-    float hpwl = (float)((xh - xl) + (yh - yl));
-    float net_congestion = (hpwl * (float)wire_width) / (float)net_area;
-    int32_t glx = die[0], gly = die[1];
-    int32_t min_x = std::max(0, (xl - glx) / tile_size), max_x = std::min(cnt_x - 1, (xh - glx) / tile_size);
-    int32_t min_y = std::max(0, (yl - gly) / tile_size), max_y = std::min(cnt_y - 1, (yh - gly) / tile_size);
-    for (int32_t x = min_x; x <= max_x; x++)
-      for (int32_t y = min_y; y <= max_y; y++) {
-        size_t i = at(x, y);
-        auto &t = rects[i];
-        if (!(t[2] > xl && t[0] < xh && t[3] > yl && t[1] < yh)) continue;
-        int64_t inter = (int64_t)(std::min(xh, t[2]) - std::max(xl, t[0])) * (int64_t)(std::min(yh, t[3]) - std::max(yl, t[1]));
-        int64_t tile_area = (int64_t)(t[2] - t[0]) * (int64_t)(t[3] - t[1]);
-        float ratio = (float)inter / (float)tile_area;
-        demand[i] += net_congestion * ratio * 100.0f;
-      }
+    auto ok = [](cudaError_t e, const char *where) {
+      if (e != cudaSuccess) throw std::runtime_error(std::string("device: ") + cudaGetErrorString(e) + " in " + where);
+    };
+    if (!d_demand) ok(cudaMalloc((void **)&d_demand, std::max<size_t>(demand.size(), 1) * sizeof(float)), "rudy alloc");
+    if (nets.size() > box_cap) {
+      if (d_boxes) cudaFree(d_boxes);
+      d_boxes = nullptr;
+      box_cap = nets.size();
+      ok(cudaMalloc((void **)&d_boxes, std::max<size_t>(box_cap, 1) * sizeof(int4)), "rudy alloc");
+    }
+    if (!nets.empty()) ok(cudaMemcpyAsync(d_boxes, nets.data(), nets.size() * sizeof(int4), cudaMemcpyHostToDevice, stream), "rudy boxes");
+    RudyGrid g{die[0], die[1], die[2], die[3], cnt_x, cnt_y, tile_size, wire_width};
+    ok(rudy_demand(g, (int64_t)nets.size(), d_boxes, d_demand, stream), "rudy");
+    ok(cudaMemcpyAsync(demand.data(), d_demand, demand.size() * sizeof(float), cudaMemcpyDeviceToHost, stream), "rudy demand");
+    ok(cudaStreamSynchronize(stream), "rudy sync");
   }
   float congestion(int32_t x, int32_t y) const {
     size_t i = at(x, y);

@@ -67,4 +67,29 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return s;
 }
 
+// A block's sums of four doubles at once (one barrier pass), valid in thread 0. Fixed order
+// for a fixed launch shape.
+template <int NT>
+__device__ __forceinline__ double4 block_sum4(double4 v, double4 *sh) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+    v.z += __shfl_down_sync(0xffffffffu, v.z, o);
+    v.w += __shfl_down_sync(0xffffffffu, v.w, o);
+  }
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  double4 s = make_double4(0, 0, 0, 0);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < NT / 32; k++) {
+      s.x += sh[k].x;
+      s.y += sh[k].y;
+      s.z += sh[k].z;
+      s.w += sh[k].w;
+    }
+  return s;
+}
+
 }  // namespace gpl

@@ -60,6 +60,7 @@ struct WaArgs {
   float2 *pin_grad;
   int32_t n_tiles;               // tiles of consecutive nets: [first, last) per tile
   const int2 *tiles;
+  unsigned long long *hpwl_out;  // WA adds the HPWL of the same pin positions here (NULL: not)
 };
 
 __global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *coords);

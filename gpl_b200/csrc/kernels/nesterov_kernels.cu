@@ -280,6 +280,7 @@ __global__ void k_wa(WaArgs w, float cx, float cy) {
     ux = max(ux, q.x);
     uy = max(uy, q.y);
   }
+  if (w.hpwl_out && ux >= lx) atomicAdd(w.hpwl_out, (unsigned long long)(((long long)ux - lx) + ((long long)uy - ly)));
   const float BAR = -300.0f;
   float s_minx = 0, s_xminx = 0, s_maxx = 0, s_xmaxx = 0, s_miny = 0, s_yminy = 0, s_maxy = 0, s_ymaxy = 0;
   for (int64_t p = b; p < e; p++) {
@@ -362,6 +363,7 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
   const int32_t np = s_nstart[nn];
   for (int j = threadIdx.x; j < np; j += blockDim.x) s_pos[j] = pin_pos(w, p0 + j);
   __syncthreads();
+  long long h = 0;  // the same pins' HPWL, for the iteration's report
   for (int j = threadIdx.x; j < nn; j += blockDim.x) {
     int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
     for (int32_t k = s_nstart[j]; k < s_nstart[j + 1]; k++) {
@@ -373,6 +375,12 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
       s_pnet[k] = (uint16_t)j;
     }
     s_box[j] = make_int4(lx, ly, ux, uy);
+    if (ux >= lx) h += ((long long)ux - lx) + ((long long)uy - ly);
+  }
+  if (w.hpwl_out) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+    if ((threadIdx.x & 31) == 0 && h) atomicAdd(w.hpwl_out, (unsigned long long)h);
   }
   __syncthreads();
   const float BAR = -300.0f;
@@ -435,8 +443,8 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
 // the density force over its bins (x outer, y inner), the preconditioned sum; block partials
 // of |wl|, |density| and the two step-length distances (getDistance :319-330):
 // |a1 - b1|^2 and |out - b2|^2.
-__global__ void k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials) {
-  __shared__ double sh[kThreads / 32];
+__global__ void __launch_bounds__(kThreads, 5) k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials) {
+  __shared__ double4 sh[kThreads / 32];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double s_wl = 0, s_den = 0, s_d1 = 0, s_d2 = 0;
   if (i < r.n_cells) {
@@ -488,15 +496,12 @@ __global__ void k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__
       s_d2 = (double)__fmul_rn(dx, dx) + (double)__fmul_rn(dy, dy);
     }
   }
-  double v0 = block_sum<kThreads>(s_wl, sh);
-  double v1 = block_sum<kThreads>(s_den, sh);
-  double v2 = block_sum<kThreads>(s_d1, sh);
-  double v3 = block_sum<kThreads>(s_d2, sh);
+  double4 v = block_sum4<kThreads>(make_double4(s_wl, s_den, s_d1, s_d2), sh);
   if (threadIdx.x == 0) {
-    partials[4 * blockIdx.x + 0] = v0;
-    partials[4 * blockIdx.x + 1] = v1;
-    partials[4 * blockIdx.x + 2] = v2;
-    partials[4 * blockIdx.x + 3] = v3;
+    partials[4 * blockIdx.x + 0] = v.x;
+    partials[4 * blockIdx.x + 1] = v.y;
+    partials[4 * blockIdx.x + 2] = v.z;
+    partials[4 * blockIdx.x + 3] = v.w;
   }
 }
 

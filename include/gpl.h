@@ -265,6 +265,43 @@ int gpl_kernel_rudy(int64_t n_nets, const int32_t *boxes, int32_t die_lx, int32_
                     int32_t die_ux, int32_t die_uy, int32_t cnt_x, int32_t cnt_y,
                     int32_t tile_size, int32_t wire_width, float *demand, void *stream);
 
+/* The density solve of gpl_kernel_poisson in double precision throughout (basis matrices,
+ * products, spectral step): the yardstick the FP32 and split-BF16 forms' errors are reported
+ * against. Fields as double, x-major. No reference counterpart in this precision: it is the
+ * exact transform the reference's float Ooura transforms approximate. */
+int gpl_kernel_poisson_fp64(int32_t nx, int32_t ny, const float *wx, const float *wy,
+                            const float *density, double *field_x, double *field_y,
+                            void *stream);
+
+/* ---- the objectives and their adjoints (double precision, device pointers) ----
+ * The reference takes only the gradients (forces) of its two objectives: the WA wirelength's
+ * in `update_wirelength_force_wa` + `wl_gradient_pin` (src/nesterov.rs:2325-2430) and the
+ * electrostatic energy's in `density_gradient` (:2434-2449) over `Fft::solve` (:412-444).
+ * These entry points give the values and their exact derivatives, for gradient checks by
+ * finite differences and for callers that differentiate through the objective.
+ *
+ * WA: W = sum_n w_n sum_{axis} (sum x e^{c x} / sum e^{c x} - sum x e^{-c x} / sum e^{-c x})
+ * over each net's pins (pin_xy[2*p], pin_xy[2*p+1]), exact exponentials, coefficient c per
+ * axis. The backward writes seed * dW/d(pin x, y) into grad[2*n_pins]. */
+int gpl_fn_wa_forward(int64_t n_nets, const int64_t *net_start, const double *pin_xy,
+                      const float *net_weight, double coef_x, double coef_y, double *value,
+                      void *stream);
+int gpl_fn_wa_backward(int64_t n_nets, const int64_t *net_start, const double *pin_xy,
+                       const float *net_weight, double coef_x, double coef_y, double seed,
+                       double *grad, void *stream);
+/* Electrostatic energy E = 1/2 rho^T G rho over nx * ny uniform bins of bin_w x bin_h from
+ * (grid_lx, grid_ly): rho the cells' overlap areas (centre cell_xy[2*i..], half sizes
+ * half[2*i..]) times their density scales, G the reference's DCT Poisson solve. The backward
+ * writes seed * dE/d(cell x, y) into grad[2*n_cells]. */
+int gpl_fn_density_forward(int64_t n_cells, const double *cell_xy, const double *half,
+                           const double *scale, int32_t nx, int32_t ny, double grid_lx,
+                           double grid_ly, double bin_w, double bin_h, double *energy,
+                           void *stream);
+int gpl_fn_density_backward(int64_t n_cells, const double *cell_xy, const double *half,
+                            const double *scale, int32_t nx, int32_t ny, double grid_lx,
+                            double grid_ly, double bin_w, double bin_h, double seed,
+                            double *grad, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

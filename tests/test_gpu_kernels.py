@@ -196,3 +196,26 @@ def test_rudy_matches_the_oracle(L):
     sync()
     assert rc == 0
     np.testing.assert_allclose(gd.cpu().numpy(), dem, rtol=1e-5, atol=1e-3)
+
+
+@pytest.mark.parametrize("nx,ny", [(128, 256), (512, 512)])
+def test_poisson_errors_against_the_fp64_solve(L, nx, ny):
+    """The FP64 device solve is the yardstick: the oracle (an f64 FFT rounded to f32) sits
+    within 1e-6 of it, the FP32 GEMM form within 1e-4 and the split-BF16 form within 5e-4 of
+    the field's maximum."""
+    L.gpl_kernel_poisson_fp64.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    rng = np.random.default_rng(nx * 7 + ny)
+    dens = (rng.random(nx * ny) * 1.5).astype(np.float32)
+    fx, fy, wx, wy = _poisson_oracle(nx, ny, 900.0, 1400.0, dens)
+    d = dev(dens)
+    ex64, ey64 = dev(np.zeros(nx * ny)), dev(np.zeros(nx * ny))
+    assert L.gpl_kernel_poisson_fp64(nx, ny, wx.ctypes.data, wy.ctypes.data, ptr(d), ptr(ex64), ptr(ey64), stream()) == 0
+    sync()
+    ex64, ey64 = ex64.cpu().numpy(), ey64.cpu().numpy()
+    err = lambda a, b: np.max(np.abs(a - b)) / np.max(np.abs(b))
+    assert err(fx, ex64) <= 1e-6 and err(fy, ey64) <= 1e-6
+    for mode, tol in ((0, 1e-4), (1, 5e-4)):
+        gx, gy = dev(np.zeros(nx * ny, np.float32)), dev(np.zeros(nx * ny, np.float32))
+        assert L.gpl_kernel_poisson(nx, ny, wx.ctypes.data, wy.ctypes.data, ptr(d), ptr(gx), ptr(gy), mode, stream()) == 0
+        sync()
+        assert err(gx.cpu().numpy(), ex64) <= tol and err(gy.cpu().numpy(), ey64) <= tol, mode

@@ -108,6 +108,17 @@ def algorithmic(phase, C, P, N, B, mixed, nx):
     return "hbm", 0
 
 
+def max_over_ranks(x, device=None):
+    """The largest of every rank's x (each rank calls it at the same point); x itself on one rank."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def log(msg):
     print(f"[bench {time.perf_counter() - T0:8.2f}] {msg}", file=sys.stderr, flush=True)
 
@@ -179,10 +190,8 @@ def ours(a):
         c1 = sess.counters()
         prof = sess.profile()
         sess.set_option("profile", "0")
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return {"ms": float(t.item()), "iters": done, "wall_s": wall, "profile": prof, "clocks": clk.summary(),
+        ms = max_over_ranks(ms, f"cuda:{local}")
+        return {"ms": ms, "iters": done, "wall_s": wall, "profile": prof, "clocks": clk.summary(),
                 "launches": c1["launches"] - c0["launches"]}
 
     cells_total = sess.counters()["cells"]
@@ -207,7 +216,7 @@ def ours(a):
             design = synth.generate(cfg["preset"])
         t0 = time.perf_counter()
         r = engine.global_placement(design, cfg["args"], device=local, poisson=a.form)
-        e2e_s = time.perf_counter() - t0
+        e2e_s = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
         log("e2e run done")
         its = r["nesterov_iterations"] or 0
         e2e = {"value": its * world / e2e_s if e2e_s > 0 else 0.0, "unit": "iters/s", "seconds": e2e_s,
@@ -215,6 +224,9 @@ def ours(a):
                "h2d_bytes_per_step": int(r["h2d_bytes"] / max(its, 1)), "d2h_bytes_per_step": int(r["d2h_bytes"] / max(its, 1)),
                "final_hpwl": r["final_hpwl"], "final_overflow": r["final_overflow"],
                "seconds_initial_place": r["seconds_initial_place"], "seconds_nesterov": r["seconds_nesterov"]}
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
     if rank != 0:
         return
     pk, pk_kind = peaks()

@@ -54,6 +54,15 @@ void Engine::check(cudaError_t e, const char *where) {
 Engine::Engine(int device) : device_(device) {
   check(cudaSetDevice(device), "cudaSetDevice");
   if (!failed()) check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!failed()) check(cudaStreamCreateWithFlags(&wa_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!failed()) check(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming), "cudaEventCreate");
+  if (!failed()) check(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming), "cudaEventCreate");
+}
+
+void Engine::join() {
+  if (!wa_pending_) return;
+  check(cudaStreamWaitEvent(stream_, ev_join_, 0), "join");
+  wa_pending_ = false;
 }
 
 Engine::~Engine() {
@@ -64,7 +73,11 @@ Engine::~Engine() {
   cudaFree(ip_vals_);
   cudaFree(ip_b_);
   cudaFree(ip_x_);
+  if (wa_stream_) cudaStreamSynchronize(wa_stream_);
   if (stream_) cudaStreamDestroy(stream_);
+  if (wa_stream_) cudaStreamDestroy(wa_stream_);
+  if (ev_fork_) cudaEventDestroy(ev_fork_);
+  if (ev_join_) cudaEventDestroy(ev_join_);
 }
 
 template <class T>
@@ -84,6 +97,7 @@ static cudaError_t upload_vec(T **p, const std::vector<T> &v, cudaStream_t s) {
 
 // ---------------------------------------------------------------- initial placement
 Solve Engine::solve(const Csr &m, const std::vector<float> &rhs, std::vector<float> &x, int max_iters) {
+  join();
   Solve out{0, NAN, false};
   if (failed()) return out;
   int64_t n = m.n, nnz = m.starts[n];
@@ -153,6 +167,7 @@ void Engine::free_globals() {
 }
 
 void Engine::release() {
+  join();
   for (Region *r : regions_) {
     void *ptrs[] = {r->bx, r->by, r->scaled, r->density, r->fx, r->fy, r->np, r->npu, r->acc_inst, r->acc_fill, r->part};
     for (void *p : ptrs)
@@ -282,6 +297,7 @@ void Engine::upload(const EngineSetup &s) {
 }
 
 void Engine::update_bins(int b, const RegionSetup &rs) {
+  join();
   Region *r = regions_[b];
   r->args.target_density = rs.target_density;
   size_t nb = rs.scaled.size();
@@ -295,6 +311,7 @@ void Engine::update_bins(int b, const RegionSetup &rs) {
 }
 
 void Engine::rewrite_cells(const EngineSetup &s) {
+  join();
   // sizes and density sizes of every cell (routability's inflation and filler changes keep
   // the cell count of a region's block only when no filler moved; the caller re-uploads then)
   size_t n = s.hx.size();
@@ -332,12 +349,14 @@ static CellArgs cell_args(const int64_t off, int2 *dc, int32_t *hx, int32_t *hy,
 #define CELLS(r) cell_args((r)->cell_off, dc_, hx_, hy_, dscale_, kind_, locked_, area_, cell_pin_start_, (r)->slot)
 
 void Engine::set_coords(int b, SlotId slot, const std::vector<float> &xy) {
+  join();
   Region *r = regions_[b];
   if (r->n_cells) check(cudaMemcpyAsync(r->slot[slot], xy.data(), r->n_cells * sizeof(float2), cudaMemcpyHostToDevice, stream_), "set_coords");
   h2d_bytes += r->n_cells * 8;
 }
 
 std::vector<float> Engine::get_coords(int b, SlotId slot) {
+  join();
   Region *r = regions_[b];
   std::vector<float> xy(2 * r->n_cells);
   if (r->n_cells) check(cudaMemcpyAsync(xy.data(), r->slot[slot], r->n_cells * sizeof(float2), cudaMemcpyDeviceToHost, stream_), "get_coords");
@@ -347,6 +366,7 @@ std::vector<float> Engine::get_coords(int b, SlotId slot) {
 }
 
 void Engine::place_at(int b, SlotId slot) {
+  join();
   if (failed()) return;
   hpwl_ready_ = false;  // the density centres move
   Region *r = regions_[b];
@@ -363,6 +383,7 @@ void Engine::place_at(int b, SlotId slot) {
 }
 
 void Engine::nesterov_step(int b, float step, float coeff) {
+  join();
   if (failed()) return;
   hpwl_ready_ = false;  // the density centres move
   Region *r = regions_[b];
@@ -405,25 +426,33 @@ WaArgs Engine::wa_args() const {
 
 void Engine::wa(float cx, float cy) {
   if (failed() || n_nets_ == 0) return;
+  join();
   WaArgs w = wa_args();
+  // forked after the work queued so far (the centres), joined by the forces' readers
+  check(cudaEventRecord(ev_fork_, stream_), "wa fork");
+  check(cudaStreamWaitEvent(wa_stream_, ev_fork_, 0), "wa fork");
+  cudaStream_t st = wa_stream_;
   // the kernels add the HPWL of these same positions: hpwl() reads it without a launch
-  check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), stream_), "wa");
+  check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), st), "wa");
   w.hpwl_out = hpwl_acc_;
   hpwl_ready_ = true;
-  ph_begin(PH_WA);
+  ph_begin(PH_WA, st);
   if (n_tiles_) {
     launches += 1;
-    k_wa_tiles<<<n_tiles_, kThreadsPerBlock, 0, stream_>>>(w, cx, cy);
+    k_wa_tiles<<<n_tiles_, kThreadsPerBlock, 0, st>>>(w, cx, cy);
   }
   if (n_big_) {
     launches += 1;
-    k_wa<<<blocks_for(n_big_), kThreadsPerBlock, 0, stream_>>>(w, cx, cy);
+    k_wa<<<blocks_for(n_big_), kThreadsPerBlock, 0, st>>>(w, cx, cy);
   }
-  ph_end(PH_WA);
+  ph_end(PH_WA, st);
   check(cudaGetLastError(), "wa");
+  check(cudaEventRecord(ev_join_, st), "wa join");
+  wa_pending_ = true;
 }
 
 void Engine::gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, SlotId b2) {
+  join();
   if (failed()) return;
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
@@ -443,6 +472,7 @@ void Engine::gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, S
 }
 
 void Engine::prev_slp(int b, float coef) {
+  join();
   if (failed()) return;
   Region *r = regions_[b];
   if (!r->n_cells) return;
@@ -451,6 +481,7 @@ void Engine::prev_slp(int b, float coef) {
 }
 
 void Engine::hold_locked(int b) {
+  join();
   if (failed() || !any_locked_) return;
   Region *r = regions_[b];
   if (!r->n_cells) return;
@@ -461,11 +492,13 @@ void Engine::hold_locked(int b) {
 void Engine::swap_slots(int b, SlotId a, SlotId c) { std::swap(regions_[b]->slot[a], regions_[b]->slot[c]); }
 
 void Engine::copy_slot(int b, SlotId dst, SlotId src) {
+  join();
   Region *r = regions_[b];
   if (r->n_cells) check(cudaMemcpyAsync(r->slot[dst], r->slot[src], r->n_cells * sizeof(float2), cudaMemcpyDeviceToDevice, stream_), "copy_slot");
 }
 
 void Engine::fetch() {
+  join();
   if (failed() || host_scal_.empty()) return;
   check(cudaMemcpyAsync(host_scal_.data(), dev_scal_, host_scal_.size() * sizeof(RegionScalars), cudaMemcpyDeviceToHost, stream_), "fetch");
   d2h_bytes += (int64_t)(host_scal_.size() * sizeof(RegionScalars));
@@ -474,6 +507,7 @@ void Engine::fetch() {
 }
 
 int64_t Engine::hpwl() {
+  join();
   if (failed()) return 0;
   WaArgs w = wa_args();
   if (!hpwl_ready_) {
@@ -499,6 +533,7 @@ int64_t Engine::hpwl() {
 }
 
 void Engine::centres(std::vector<int32_t> &dcx, std::vector<int32_t> &dcy) {
+  join();
   std::vector<int2> dc(n_cells_);
   if (n_cells_) {
     check(cudaMemcpyAsync(dc.data(), dc_, n_cells_ * sizeof(int2), cudaMemcpyDeviceToHost, stream_), "centres");
@@ -514,10 +549,12 @@ void Engine::centres(std::vector<int32_t> &dcx, std::vector<int32_t> &dcy) {
 }
 
 void Engine::set_net_weights(const std::vector<float> &w) {
+  join();
   if (!w.empty()) check(cudaMemcpyAsync(net_weight_, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, stream_), "net weights");
 }
 
 void Engine::rebuild_poisson(int mode) {
+  join();
   poisson_mode_ = mode;
   for (size_t b = 0; b < regions_.size(); b++) {
     Region *r = regions_[b];
@@ -549,8 +586,9 @@ void Engine::set_profile(bool on) {
   ev_used_ = 0;
 }
 
-void Engine::ph_begin(int ph) {
+void Engine::ph_begin(int ph, cudaStream_t on) {
   if (!profile_) return;
+  if (!on) on = stream_;
   if (ev_used_ + 2 > ev_.size()) {
     for (int k = 0; k < 64; k++) {
       cudaEvent_t e;
@@ -558,14 +596,14 @@ void Engine::ph_begin(int ph) {
       ev_.push_back(e);
     }
   }
-  check(cudaEventRecord(ev_[ev_used_], stream_), "event record");
+  check(cudaEventRecord(ev_[ev_used_], on), "event record");
   ev_pending_.push_back({ph, ev_used_});
   ev_used_ += 2;
 }
 
-void Engine::ph_end(int ph) {
+void Engine::ph_end(int ph, cudaStream_t on) {
   if (!profile_ || ev_pending_.empty()) return;
-  check(cudaEventRecord(ev_[ev_pending_.back().second + 1], stream_), "event record");
+  check(cudaEventRecord(ev_[ev_pending_.back().second + 1], on ? on : stream_), "event record");
 }
 
 void Engine::ph_flush() {

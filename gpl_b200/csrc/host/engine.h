@@ -139,6 +139,12 @@ class Engine {
   float2 *pin_grad_ = nullptr;  // the WA force of every pin of a cell, cell-major (cell_pins order)
   unsigned long long *hpwl_acc_ = nullptr;
   bool hpwl_ready_ = false;  // hpwl_acc_ holds the HPWL of the current centres (from the WA)
+  // The WA runs on its own stream, beside the density solve (it needs the centres, not the
+  // field); everything that reads its forces or moves the centres joins it first.
+  cudaStream_t wa_stream_ = nullptr;
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+  bool wa_pending_ = false;
+  void join();
   // initial placement scratch
   void *ip_scratch_ = nullptr;
   size_t ip_scratch_bytes_ = 0;
@@ -157,8 +163,8 @@ class Engine {
   int64_t ph_n_[PH_COUNT] = {};
   std::vector<std::vector<float>> region_wx_, region_wy_;
   std::vector<std::pair<int, int>> region_dims_;
-  void ph_begin(int ph);
-  void ph_end(int ph);
+  void ph_begin(int ph, cudaStream_t on = nullptr);
+  void ph_end(int ph, cudaStream_t on = nullptr);
   void ph_flush();
 };
 

@@ -1194,13 +1194,12 @@ struct Placer {
     for (int nbt = 0; nbt < 10; nbt++) {
       trials++;
       eng.trials++;
-      for (size_t b = 0; b < nbs.size(); b++) {
-        if (nbs[b].is_converged) continue;
-        eng.nesterov_step((int)b, nbs[b].step_length, coeff);
-        eng.field((int)b);
-      }
+      for (size_t b = 0; b < nbs.size(); b++)
+        if (!nbs[b].is_converged) eng.nesterov_step((int)b, nbs[b].step_length, coeff);
       hpwl_dirty = true;
-      wa();
+      wa();  // beside the density solves: it needs the new centres, not the field
+      for (size_t b = 0; b < nbs.size(); b++)
+        if (!nbs[b].is_converged) eng.field((int)b);
       for (size_t b = 0; b < nbs.size(); b++)
         if (!nbs[b].is_converged) eng.gradients((int)b, S_NEXT_SLP_SUM, nbs[b].density_penalty, S_CUR_SLP, S_NEXT_SLP, S_CUR_SLP_SUM);
       eng.fetch();

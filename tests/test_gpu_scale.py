@@ -49,3 +49,16 @@ def test_full_run_matches_the_oracle(cfg, mode):
     assert abs(got["final_overflow"] - ref["final_overflow"]) <= 0.005
     assert got["final_overflow"] <= 0.1
     assert len(got["locations"]) == ref["locations"]
+
+
+def test_mixed_and_fp32_forms_agree_at_2m_cells():
+    """The largest synthetic design (2M cells, 2048x2048 bins), where no CPU run is recorded:
+    both density solvers place it under the overflow target, and the split-BF16 tensor-core
+    form's final HPWL is within 0.1 % of the FP32 form's."""
+    d = synth.generate("cfg5")
+    args = ["-density", "0.70", "-bin_grid_count", "2048"]
+    a = engine.global_placement(d, args, poisson="mixed")
+    b = engine.global_placement(d, args, poisson="fp32")
+    assert a["status"] == "placed" and b["status"] == "placed", (a["reason"], b["reason"])
+    assert a["final_overflow"] <= 0.1 and b["final_overflow"] <= 0.1
+    assert abs(a["final_hpwl"] - b["final_hpwl"]) <= 1e-3 * b["final_hpwl"]

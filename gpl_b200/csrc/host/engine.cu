@@ -67,12 +67,6 @@ void Engine::join() {
 
 Engine::~Engine() {
   release();
-  if (ip_scratch_) cudaFree(ip_scratch_);
-  cudaFree(ip_rs_);
-  cudaFree(ip_cols_);
-  cudaFree(ip_vals_);
-  cudaFree(ip_b_);
-  cudaFree(ip_x_);
   if (wa_stream_) cudaStreamSynchronize(wa_stream_);
   if (stream_) cudaStreamDestroy(stream_);
   if (wa_stream_) cudaStreamDestroy(wa_stream_);
@@ -93,57 +87,6 @@ static cudaError_t upload_vec(T **p, const std::vector<T> &v, cudaStream_t s) {
   if (e != cudaSuccess || v.empty()) return e;
   g_h2d += (int64_t)(v.size() * sizeof(T));
   return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
-}
-
-// ---------------------------------------------------------------- initial placement
-Solve Engine::solve(const Csr &m, const std::vector<float> &rhs, std::vector<float> &x, int max_iters) {
-  join();
-  Solve out{0, NAN, false};
-  if (failed()) return out;
-  int64_t n = m.n, nnz = m.starts[n];
-  if ((size_t)n > ip_n_cap_) {
-    cudaFree(ip_rs_);
-    cudaFree(ip_b_);
-    cudaFree(ip_x_);
-    if (ip_scratch_) cudaFree(ip_scratch_);
-    check(dmalloc(&ip_rs_, n + 1), "ip alloc");
-    check(dmalloc(&ip_b_, n), "ip alloc");
-    check(dmalloc(&ip_x_, n), "ip alloc");
-    ip_scratch_bytes_ = bicgstab_scratch_bytes(n);
-    check(cudaMalloc(&ip_scratch_, ip_scratch_bytes_), "ip scratch");
-    ip_n_cap_ = (size_t)n;
-  }
-  if ((size_t)nnz > ip_nnz_cap_) {
-    cudaFree(ip_cols_);
-    cudaFree(ip_vals_);
-    size_t cap = (size_t)(nnz * 1.25) + 16;
-    check(dmalloc(&ip_cols_, cap), "ip alloc");
-    check(dmalloc(&ip_vals_, cap), "ip alloc");
-    ip_nnz_cap_ = cap;
-  }
-  if (failed()) return out;
-  cudaStream_t s = stream_;
-  check(cudaMemcpyAsync(ip_rs_, m.starts.data(), (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s), "ip h2d");
-  if (nnz) {
-    check(cudaMemcpyAsync(ip_cols_, m.cols.data(), nnz * sizeof(int32_t), cudaMemcpyHostToDevice, s), "ip h2d");
-    check(cudaMemcpyAsync(ip_vals_, m.vals.data(), nnz * sizeof(float), cudaMemcpyHostToDevice, s), "ip h2d");
-  }
-  if (n) {
-    check(cudaMemcpyAsync(ip_b_, rhs.data(), n * sizeof(float), cudaMemcpyHostToDevice, s), "ip h2d");
-    check(cudaMemcpyAsync(ip_x_, x.data(), n * sizeof(float), cudaMemcpyHostToDevice, s), "ip h2d");
-  }
-  h2d_bytes += (n + 1) * 8 + nnz * 8 + n * 8;
-  CsrDev A{n, ip_rs_, ip_cols_, ip_vals_};
-  BicgResult r{};
-  check(bicgstab_solve(A, ip_b_, ip_x_, max_iters, ip_scratch_, s, &r), "bicgstab");
-  if (n) check(cudaMemcpyAsync(x.data(), ip_x_, n * sizeof(float), cudaMemcpyDeviceToHost, s), "ip d2h");
-  d2h_bytes += n * 4 + (int64_t)(r.iterations + 2) * 64;
-  launches += 4 + (int64_t)r.iterations * 10;
-  check(cudaStreamSynchronize(s), "ip sync");
-  out.iterations = r.iterations;
-  out.error = r.error;
-  out.converged = r.converged;
-  return out;
 }
 
 // ---------------------------------------------------------------- Nesterov state

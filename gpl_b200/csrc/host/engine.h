@@ -65,8 +65,6 @@ class Engine {
   void set_poisson_mode(int m) { poisson_mode_ = m; }
   int poisson_mode() const { return poisson_mode_; }
 
-  // ---- initial placement: one axis's solve (src/bicgstab.rs:615-669)
-  Solve solve(const Csr &m, const std::vector<float> &rhs, std::vector<float> &x, int max_iters);
 
   // ---- Nesterov state
   void upload(const EngineSetup &s);
@@ -145,13 +143,6 @@ class Engine {
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   bool wa_pending_ = false;
   void join();
-  // initial placement scratch
-  void *ip_scratch_ = nullptr;
-  size_t ip_scratch_bytes_ = 0;
-  int64_t *ip_rs_ = nullptr;
-  int32_t *ip_cols_ = nullptr;
-  float *ip_vals_ = nullptr, *ip_b_ = nullptr, *ip_x_ = nullptr;
-  size_t ip_nnz_cap_ = 0, ip_n_cap_ = 0;
   void free_globals();
   WaArgs wa_args() const;
   // profiling

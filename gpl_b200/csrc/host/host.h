@@ -206,21 +206,6 @@ struct Ip {
   std::vector<int> place;
   std::vector<std::vector<int>> inst_pins;
 };
-struct Csr {
-  int64_t n = 0;
-  std::vector<int64_t> starts;
-  std::vector<int32_t> cols;
-  std::vector<float> vals;
-  static Csr from_triplets(int64_t n, const std::vector<std::tuple<int64_t, int64_t, float>> &t);
-  void mul(const float *x, float *y) const;
-};
-struct Solve {
-  int iterations;
-  float error;
-  bool converged;
-};
-// The solve the initial placement calls per axis (the device BiCGSTAB).
-using SolveFn = std::function<Solve(const Csr &m, const std::vector<float> &rhs, std::vector<float> &x, int max_iters)>;
 
 // ---- random numbers (src/normal.rs) ----
 struct Mt19937 {
@@ -235,7 +220,6 @@ double normal(Mt19937 &eng, double mean, double sigma);
 
 std::pair<int32_t, int32_t> orient_point(int orient, int32_t x, int32_t y);
 Ip make_pins(const Design &d, const Common &c, const Vars &v);
-Ip do_bicgstab_place(Log &log, const Design &d, Common &c, const Vars &v, const IpVars &vars, const SolveFn &solve);
 class IpDevice;
 Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v, const IpVars &vars, IpDevice &dev);
 

@@ -694,186 +694,6 @@ static void place_insts_initial_positions(Log &log, const Design &d, Common &c, 
   log.info("GPL", 51, sfmt("Source of initial instance position counters:\n\tOdb location = %ld\tCore center = %ld\tRegion center = %ld", db, core, region));
 }
 
-// `updatePinInfo` (src/initial_place.rs:203-252).
-static void update_pin_info(Ip &ip) {
-  for (auto &p : ip.pins) p.min_x = p.max_x = p.min_y = p.max_y = false;
-  for (auto &net : ip.net_pins) {
-    int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
-    int pminx = -1, pminy = -1, pmaxx = -1, pmaxy = -1;
-    for (int k : net) {
-      if (ip.pins[k].movable_io) continue;
-      int32_t cx = ip.pins[k].cx, cy = ip.pins[k].cy;
-      if (lx > cx) {
-        if (pminx >= 0) ip.pins[pminx].min_x = false;
-        lx = cx;
-        pminx = k;
-        ip.pins[k].min_x = true;
-      }
-      if (ux < cx) {
-        if (pmaxx >= 0) ip.pins[pmaxx].max_x = false;
-        ux = cx;
-        pmaxx = k;
-        ip.pins[k].max_x = true;
-      }
-      if (ly > cy) {
-        if (pminy >= 0) ip.pins[pminy].min_y = false;
-        ly = cy;
-        pminy = k;
-        ip.pins[k].min_y = true;
-      }
-      if (uy < cy) {
-        if (pmaxy >= 0) ip.pins[pmaxy].max_y = false;
-        uy = cy;
-        pmaxy = k;
-        ip.pins[k].max_y = true;
-      }
-    }
-  }
-}
-
-struct System {
-  std::vector<std::tuple<int64_t, int64_t, float>> triplets;
-  std::vector<float> rhs, x;
-};
-
-// `createSparseMatrix` (src/initial_place.rs:264-355).
-static void create_sparse_matrix(const Common &c, const Ip &ip, const IpVars &vars, System &sx, System &sy) {
-  size_t n = ip.place.size();
-  std::vector<int64_t> ext(c.insts.size(), -1);
-  for (size_t e = 0; e < n; e++) ext[ip.place[e]] = (int64_t)e;
-  sx.triplets.clear();
-  sy.triplets.clear();
-  sx.rhs.assign(n, 0.0f);
-  sy.rhs.assign(n, 0.0f);
-  sx.x.assign(n, 0.0f);
-  sy.x.assign(n, 0.0f);
-  for (size_t e = 0; e < n; e++) {
-    int k = ip.place[e];
-    sx.x[e] = (float)c.insts[k].cx();
-    sy.x[e] = (float)c.insts[k].cy();
-    if (c.insts[k].locked) {
-      sx.triplets.emplace_back(e, e, 1.0f);
-      sy.triplets.emplace_back(e, e, 1.0f);
-      sx.rhs[e] = (float)c.insts[k].cx();
-      sy.rhs[e] = (float)c.insts[k].cy();
-    }
-  }
-  auto placed = [&](const Pin &p) -> int { return (p.inst >= 0 && !c.insts[p.inst].fixed) ? p.inst : -1; };
-  std::vector<int> solve;
-  for (auto &net : ip.net_pins) {
-    if (net.size() <= 1 || (int)net.size() >= vars.max_fanout) continue;
-    float net_weight = vars.net_weight_scale / (float)(net.size() - 1);
-    solve.clear();
-    for (int k : net)
-      if (!ip.pins[k].movable_io) solve.push_back(k);
-    for (size_t i1 = 1; i1 < solve.size(); i1++) {
-      const Pin &p1 = ip.pins[solve[i1]];
-      for (size_t i2 = 0; i2 < i1; i2++) {
-        const Pin &p2 = ip.pins[solve[i2]];
-        if (p1.inst == p2.inst) continue;
-        for (int axis = 0; axis < 2; axis++) {
-          bool marked;
-          int32_t c1, c2;
-          System *sys;
-          if (axis == 0) {
-            marked = p1.min_x || p1.max_x || p2.min_x || p2.max_x;
-            c1 = p1.cx;
-            c2 = p2.cx;
-            sys = &sx;
-          } else {
-            marked = p1.min_y || p1.max_y || p2.min_y || p2.max_y;
-            c1 = p1.cy;
-            c2 = p2.cy;
-            sys = &sy;
-          }
-          if (!marked) continue;
-          auto center = [&](int k) { return axis == 0 ? c.insts[k].cx() : c.insts[k].cy(); };
-          int32_t diff = std::abs(c1 - c2);
-          float weight = diff > vars.min_diff_length ? net_weight / (float)diff : net_weight / (float)vars.min_diff_length;
-          int a = placed(p1), bb = placed(p2);
-          if (a >= 0 && bb >= 0) {
-            bool la = c.insts[a].locked, lb = c.insts[bb].locked;
-            if (!la && !lb) {
-              int64_t e1 = ext[a], e2 = ext[bb];
-              sys->triplets.emplace_back(e1, e1, weight);
-              sys->triplets.emplace_back(e2, e2, weight);
-              sys->triplets.emplace_back(e1, e2, -weight);
-              sys->triplets.emplace_back(e2, e1, -weight);
-              sys->rhs[e1] += -weight * (float)((c1 - center(a)) - (c2 - center(bb)));
-              sys->rhs[e2] += -weight * (float)((c2 - center(bb)) - (c1 - center(a)));
-            } else if (la && !lb) {
-              int64_t e2 = ext[bb];
-              sys->triplets.emplace_back(e2, e2, weight);
-              sys->rhs[e2] += weight * (float)(c1 - (c2 - center(bb)));
-            } else if (!la && lb) {
-              int64_t e1 = ext[a];
-              sys->triplets.emplace_back(e1, e1, weight);
-              sys->rhs[e1] += weight * (float)(c2 - (c1 - center(a)));
-            }
-          } else if (a < 0 && bb >= 0) {
-            int64_t e2 = ext[bb];
-            sys->triplets.emplace_back(e2, e2, weight);
-            sys->rhs[e2] += weight * (float)(c1 - (c2 - center(bb)));
-          } else if (a >= 0 && bb < 0) {
-            int64_t e1 = ext[a];
-            sys->triplets.emplace_back(e1, e1, weight);
-            sys->rhs[e1] += weight * (float)(c2 - (c1 - center(a)));
-          }
-        }
-      }
-    }
-  }
-}
-
-// `hpwl` over the database boxes (src/initial_place.rs:359-386).
-static int64_t ip_hpwl(const Design &d, const Common &c, const Ip &ip, const Vars &v) {
-  int64_t total = 0;
-  for (auto &[net, cnt] : c.nets) {
-    const DbNet &n = d.nets[net];
-    int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
-    for (auto &t : n.iterms) {
-      Rect b = ip.db_bbox[t.inst];
-      lx = std::min(lx, b.lx);
-      ly = std::min(ly, b.ly);
-      ux = std::max(ux, b.ux);
-      uy = std::max(uy, b.uy);
-    }
-    if (!v.skip_io)
-      for (auto &p : n.bterms)
-        if (p.has_bbox) {
-          lx = std::min(lx, p.bbox.lx);
-          ly = std::min(ly, p.bbox.ly);
-          ux = std::max(ux, p.bbox.ux);
-          uy = std::max(uy, p.bbox.uy);
-        }
-    if (ux >= lx) total += (int64_t)(ux - lx) + (int64_t)(uy - ly);
-  }
-  return total;
-}
-
-// `updateCoordi` (src/initial_place.rs:391-417).
-static void update_coordi(const Design &d, Common &c, Ip &ip, const std::vector<float> &sx, const std::vector<float> &sy) {
-  std::vector<int> place = ip.place;
-  for (size_t e = 0; e < place.size(); e++) {
-    int k = place[e];
-    if (c.insts[k].locked) continue;
-    int32_t nx = f2i(sx[e]), ny = f2i(sy[e]);
-    nx = std::min(std::max(nx, d.core.lx), d.core.ux);
-    ny = std::min(std::max(ny, d.core.ly), d.core.uy);
-    int di = c.insts[k].db;
-    int g = d.insts[di].group;
-    if (g >= 0 && d.groups[g].region >= 0) {
-      Rect b = region_box_of(d, d.groups[g].region);
-      nx = std::min(std::max(nx, b.lx), b.ux);
-      ny = std::min(std::max(ny, b.ly), b.uy);
-    }
-    set_center_location(c, ip, k, nx, ny);
-    int32_t lx = c.insts[k].lx, ly = c.insts[k].ly;
-    Rect b = ip.db_bbox[di];
-    ip.db_bbox[di] = Rect{lx, ly, lx + b.dx(), ly + b.dy()};
-  }
-}
-
 static uint64_t fnv_f32(const std::vector<float> &v) {
   uint64_t h = 1469598103934665603ull;
   for (float f : v) {
@@ -887,45 +707,9 @@ static uint64_t fnv_f32(const std::vector<float> &v) {
   return h;
 }
 
-// `doBicgstabPlace` (src/initial_place.rs:420-446).
-Ip do_bicgstab_place(Log &log, const Design &d, Common &c, const Vars &v, const IpVars &vars, const SolveFn &solve) {
-  log.info("GPL", 5, "---- Execute Conjugate Gradient Initial Placement.");
-  Ip ip = make_pins(d, c, v);
-  place_insts_initial_positions(log, d, c, ip, vars);
-  System sx, sy;
-  progress("initial placement: %zu pins, %zu nets", ip.pins.size(), ip.net_pins.size());
-  for (int iter = 1; iter <= vars.max_iter; iter++) {
-    update_pin_info(ip);
-    create_sparse_matrix(c, ip, vars, sx, sy);
-    progress("  round %d: B2B assembled (%zu + %zu triplets)", iter, sx.triplets.size(), sy.triplets.size());
-    int64_t n = (int64_t)ip.place.size();
-    Csr mx = Csr::from_triplets(n, sx.triplets);
-    progress("  round %d: CSR x built", iter);
-    Solve ex = solve(mx, sx.rhs, sx.x, vars.max_solver_iter);
-    progress("  round %d: x solved (%d iterations)", iter, ex.iterations);
-    Csr my = Csr::from_triplets(n, sy.triplets);
-    Solve ey = solve(my, sy.rhs, sy.x, vars.max_solver_iter);
-    progress("  round %d: y solved (%d iterations)", iter, ey.iterations);
-    uint32_t exb, eyb;
-    std::memcpy(&exb, &ex.error, 4);
-    std::memcpy(&eyb, &ey.error, 4);
-    log.probe(sfmt("VYGIPS|%d|x|%d|%08x|%d|%016llx", iter, ex.iterations, exb, ex.converged ? 0 : 2, (unsigned long long)fnv_f32(sx.x)));
-    log.probe(sfmt("VYGIPS|%d|y|%d|%08x|%d|%016llx", iter, ey.iterations, eyb, ey.converged ? 0 : 2, (unsigned long long)fnv_f32(sy.x)));
-    if (std::isnan(ex.error) || std::isnan(ey.error)) {
-      log.warn("GPL", 325, sfmt("Conjugate gradient initial placement solver failed at iteration %d. ", iter));
-      break;
-    }
-    float error_max = fmaxr(ex.error, ey.error);
-    log.report(sfmt("[InitialPlace]  Iter: %d conjugate gradient residual: %.8f HPWL: %ld", iter, (double)error_max, (long)ip_hpwl(d, c, ip, v)));
-    update_coordi(d, c, ip, sx.x, sy.x);
-    if ((double)error_max <= 1e-5 && iter >= 5) break;
-  }
-  return ip;
-}
-
-// `doBicgstabPlace` with its matrices assembled, collapsed and solved on the device
-// (kernels/b2b.cu): the same rounds, report lines, probes and stop rules as the host loop
-// above; the host reads back the two solves' scalars and the report's HPWL per round.
+// `doBicgstabPlace` (src/initial_place.rs:420-446) with its matrices assembled, collapsed and
+// solved on the device (kernels/b2b.cu): the reference's rounds, report lines, probes and stop
+// rules; the host reads back the two solves' scalars and the report's HPWL per round.
 Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v, const IpVars &vars, IpDevice &dev) {
   log.info("GPL", 5, "---- Execute Conjugate Gradient Initial Placement.");
   Ip ip = make_pins(d, c, v);
@@ -1041,62 +825,6 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
     }
   }
   return ip;
-}
-
-// ---------------------------------------------------------------- bicgstab.rs
-
-// `Csr::from_triplets` (src/bicgstab.rs:501-541): duplicates summed per column in triplet
-// order into the first occurrence, then rows in column order.
-Csr Csr::from_triplets(int64_t n, const std::vector<std::tuple<int64_t, int64_t, float>> &t) {
-  // bucket the triplets by column, keeping their order
-  std::vector<int64_t> cstart(n + 1, 0);
-  for (auto &[r, cc, v] : t) cstart[cc + 1]++;
-  for (int64_t i = 0; i < n; i++) cstart[i + 1] += cstart[i];
-  std::vector<int64_t> fill(cstart.begin(), cstart.end() - 1);
-  std::vector<std::pair<int64_t, float>> bycol(t.size());
-  for (auto &[r, cc, v] : t) bycol[fill[cc]++] = {r, v};
-  // collapse duplicates per column
-  std::vector<int64_t> slot(n, -1);
-  std::vector<std::vector<std::pair<int64_t, float>>> collapsed(n);
-  for (int64_t cc = 0; cc < n; cc++) {
-    auto &out = collapsed[cc];
-    for (int64_t q = cstart[cc]; q < cstart[cc + 1]; q++) {
-      auto [r, v] = bycol[q];
-      if (slot[r] >= 0)
-        out[slot[r]].second += v;
-      else {
-        slot[r] = (int64_t)out.size();
-        out.push_back({r, v});
-      }
-    }
-    for (auto &e : out) slot[e.first] = -1;
-  }
-  // transposed copy: rows in column order
-  Csr m;
-  m.n = n;
-  std::vector<int64_t> rcount(n + 1, 0);
-  for (int64_t cc = 0; cc < n; cc++)
-    for (auto &e : collapsed[cc]) rcount[e.first + 1]++;
-  for (int64_t i = 0; i < n; i++) rcount[i + 1] += rcount[i];
-  m.starts = rcount;
-  m.cols.resize(rcount[n]);
-  m.vals.resize(rcount[n]);
-  std::vector<int64_t> rf(rcount.begin(), rcount.end() - 1);
-  for (int64_t cc = 0; cc < n; cc++)
-    for (auto &e : collapsed[cc]) {
-      m.cols[rf[e.first]] = (int32_t)cc;
-      m.vals[rf[e.first]++] = e.second;
-    }
-  return m;
-}
-
-// `Csr::mul` (src/bicgstab.rs:544-554).
-void Csr::mul(const float *x, float *y) const {
-  for (int64_t i = 0; i < n; i++) {
-    float tmp = 0.0f;
-    for (int64_t k = starts[i]; k < starts[i + 1]; k++) tmp += vals[k] * x[cols[k]];
-    y[i] = 0.0f + 1.0f * tmp;
-  }
 }
 
 // ---------------------------------------------------------------- normal.rs

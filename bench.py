@@ -9,6 +9,10 @@ solve) is the headline; the plain FP32 form is timed beside it on the same place
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
+The timed iterations run as the engine runs them (the WA on its own stream beside the density
+solve); a separate pass of 10 iterations with the WA after the solve times each phase with CUDA
+events for the phase shares and the roofline of the dominant kernel.
+
 N > 1 (under torchrun): one independent replica per GPU (the path has no exchange step), the
 time is the max over ranks, `value` the iterations of all ranks over it.
 --impl reference: the reference's CPU path (its restatement, single-threaded as the reference
@@ -171,7 +175,6 @@ def ours(a):
     stream = torch.cuda.ExternalStream(sess.stream, device=local)
 
     def timed(k, label):
-        sess.set_option("profile", "1")
         c0 = sess.counters()
         if world > 1:
             dist.barrier()
@@ -188,18 +191,28 @@ def ours(a):
             dist.barrier()
         ms = e0.elapsed_time(e1)
         c1 = sess.counters()
+        ms = max_over_ranks(ms, f"cuda:{local}")
+        return {"ms": ms, "iters": done, "wall_s": wall, "clocks": clk.summary(), "launches": c1["launches"] - c0["launches"]}
+
+    def phase_times(k):
+        # each phase's own device time: events around each phase's launches, with the WA after
+        # the density solve instead of beside it (outside the timed region above)
+        sess.set_option("overlap", "0")
+        sess.set_option("profile", "1")
+        sess.iterate(k)
         prof = sess.profile()
         sess.set_option("profile", "0")
-        ms = max_over_ranks(ms, f"cuda:{local}")
-        return {"ms": ms, "iters": done, "wall_s": wall, "profile": prof, "clocks": clk.summary(),
-                "launches": c1["launches"] - c0["launches"]}
+        sess.set_option("overlap", "1")
+        return prof
 
     cells_total = sess.counters()["cells"]
     if a.form == "mixed":
         mixed = timed(a.steps, "mixed")
+        mixed["profile"] = phase_times(min(a.steps, 10))
         sess.set_option("poisson", "fp32")
         sess.iterate(min(a.warmup, 3))
     fp32 = timed(a.steps, "fp32")
+    fp32["profile"] = phase_times(min(a.steps, 10))
     if a.form == "fp32":
         mixed = fp32
     log("timed")

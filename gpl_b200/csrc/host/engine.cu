@@ -372,9 +372,11 @@ void Engine::wa(float cx, float cy) {
   join();
   WaArgs w = wa_args();
   // forked after the work queued so far (the centres), joined by the forces' readers
-  check(cudaEventRecord(ev_fork_, stream_), "wa fork");
-  check(cudaStreamWaitEvent(wa_stream_, ev_fork_, 0), "wa fork");
-  cudaStream_t st = wa_stream_;
+  cudaStream_t st = overlap_ ? wa_stream_ : stream_;
+  if (overlap_) {
+    check(cudaEventRecord(ev_fork_, stream_), "wa fork");
+    check(cudaStreamWaitEvent(wa_stream_, ev_fork_, 0), "wa fork");
+  }
   // the kernels add the HPWL of these same positions: hpwl() reads it without a launch
   check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), st), "wa");
   w.hpwl_out = hpwl_acc_;
@@ -390,8 +392,10 @@ void Engine::wa(float cx, float cy) {
   }
   ph_end(PH_WA, st);
   check(cudaGetLastError(), "wa");
-  check(cudaEventRecord(ev_join_, st), "wa join");
-  wa_pending_ = true;
+  if (overlap_) {
+    check(cudaEventRecord(ev_join_, st), "wa join");
+    wa_pending_ = true;
+  }
 }
 
 void Engine::gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, SlotId b2) {

@@ -103,6 +103,10 @@ class Engine {
   // Per-phase device time (CUDA events on the engine's stream around each launch group).
   enum Phase { PH_PLACE = 0, PH_FINALIZE, PH_POISSON, PH_WA, PH_GRAD, PH_HPWL, PH_COUNT };
   void set_profile(bool on);
+  void set_overlap(bool on) {
+    join();
+    overlap_ = on;
+  }
   int profile_read(double *ms, int64_t *launches, int cap);
   bool failed() const { return err_.code != cudaSuccess; }
   const DeviceError &error() const { return err_; }
@@ -142,6 +146,7 @@ class Engine {
   cudaStream_t wa_stream_ = nullptr;
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   bool wa_pending_ = false;
+  bool overlap_ = true;
   void join();
   void free_globals();
   WaArgs wa_args() const;

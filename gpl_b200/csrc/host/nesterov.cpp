@@ -2151,6 +2151,7 @@ struct Run {
       if (!r.pad) has_core_row = true;
     if (!has_core_row) log.error("GPL", 130, "No rows defined in design. Use initialize_floorplan to add rows.");
     c = placer_base_common(log, d, vars);
+    progress("placer common built");
     bases.push_back(placer_base(log, d, c, -1, true));
     for (auto &reg : d.regions)
       for (int g : reg.groups) bases.push_back(placer_base(log, d, c, g, true));
@@ -2183,7 +2184,9 @@ struct Run {
     }
     P = std::make_unique<Placer>(eng);
     P->o = o;
+    progress("initial placement done");
     init_nesterov_place(log, d, c, ip, bases, *P);
+    progress("placer regions built");
     if (o.routability) {
       route = std::make_unique<Routability>();
       route->rb.vars = o.rv;
@@ -2358,9 +2361,12 @@ int gpl_global_placement(gpl_ctx *ctx, const gpl_design_t *cd, int argc, const c
   Run run(*ctx->eng);
   run.res.log.trace_on = ctx->trace;
   guarded(run.res, [&] {
+    progress("command start");
     run.d = design_from_c(cd);
+    progress("design read: %zu instances, %zu nets", run.d.insts.size(), run.d.nets.size());
     run.open(std::vector<std::string>(argv, argv + argc), router);
     run.close();
+    progress("command done");
   });
   run.res.h2d = ctx->eng->h2d_bytes + run.res.locations.size() * 0;
   run.res.d2h = ctx->eng->d2h_bytes;

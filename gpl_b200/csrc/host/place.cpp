@@ -713,6 +713,7 @@ static uint64_t fnv_f32(const std::vector<float> &v) {
 Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v, const IpVars &vars, IpDevice &dev) {
   log.info("GPL", 5, "---- Execute Conjugate Gradient Initial Placement.");
   Ip ip = make_pins(d, c, v);
+  progress("pins made");
   place_insts_initial_positions(log, d, c, ip, vars);
   if (vars.max_iter < 1) return ip;
   auto device = [](cudaError_t e, const char *where) {
@@ -772,6 +773,7 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
     s.net_start.push_back((int64_t)pk);
   }
   if (pk != ip.pins.size()) throw std::runtime_error("initial placement: pin order mismatch");
+  progress("initial placement set up on the host");
   s.max_fanout = vars.max_fanout;
   s.min_diff = vars.min_diff_length;
   s.weight_scale = vars.net_weight_scale;

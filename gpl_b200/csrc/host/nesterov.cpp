@@ -1738,6 +1738,8 @@ struct Placer {
 static void init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip, const std::vector<Base> &bases, Placer &P) {
   const Opts &o = P.o;
   std::vector<int> inst_cell(c.insts.size(), -1);
+  P.gcells.reserve(ip.place.size() + ip.place.size() / 4);
+  P.gpins.reserve(ip.pins.size());
   for (int k : ip.place) {
     const Instance &i = c.insts[k];
     inst_cell[k] = (int)P.gcells.size();
@@ -1762,7 +1764,7 @@ static void init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip, co
   }
   for (size_t k = 0; k < ip.inst_pins.size(); k++)
     if (inst_cell[k] >= 0) P.gcells[inst_cell[k]].pins = ip.inst_pins[k];
-  P.net_pins = ip.net_pins;
+  P.net_pins = std::move(ip.net_pins);  // the initial placement is done with them
   for (auto &b : bases)
     for (int k : b.place_insts)
       if (inst_cell[k] < 0) refuse("a placer region holding an instance outside the common placed set is not modelled");

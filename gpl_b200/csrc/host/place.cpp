@@ -191,6 +191,10 @@ Rect Rect::intersect(const Rect &o) const {
 
 static Rect rect4(const int32_t *p) { return Rect{p[0], p[1], p[2], p[3]}; }
 
+// An instance's (or its master's) name, generated as "i<k>" ("m<k>") when the caller gave none.
+std::string inst_label(const Design &d, size_t k) { return d.insts[k].name.empty() ? sfmt("i%zu", k) : d.insts[k].name; }
+std::string master_label(const Design &d, size_t k) { return d.insts[k].master.empty() ? sfmt("m%zu", k) : d.insts[k].master; }
+
 Design design_from_c(const gpl_design_t *c) {
   Design d;
   d.dbu = c->dbu;
@@ -200,8 +204,9 @@ Design design_from_c(const gpl_design_t *c) {
   d.insts.resize(c->n_insts);
   for (int k = 0; k < c->n_insts; k++) {
     DbInst &i = d.insts[k];
-    i.name = c->inst_name ? c->inst_name[k] : sfmt("i%d", k);
-    i.master = c->inst_master_name ? c->inst_master_name[k] : sfmt("m%d", k);
+    // names the caller did not give are generated when a message needs them (inst_label)
+    if (c->inst_name) i.name = c->inst_name[k];
+    if (c->inst_master_name) i.master = c->inst_master_name[k];
     uint32_t f = c->inst_flags[k];
     i.core_auto_placeable = f & GPL_INST_CORE_AUTO_PLACEABLE;
     i.master_is_block = f & GPL_INST_BLOCK;
@@ -219,7 +224,7 @@ Design design_from_c(const gpl_design_t *c) {
   d.nets.resize(c->n_nets);
   for (int n = 0; n < c->n_nets; n++) {
     DbNet &net = d.nets[n];
-    net.name = c->net_name ? c->net_name[n] : sfmt("n%d", n);
+    if (c->net_name) net.name = c->net_name[n];
     net.signal_or_clock = c->net_signal[n] != 0;
     for (int64_t t = c->net_iterm_start[n]; t < c->net_iterm_start[n + 1]; t++) {
       Term tm;
@@ -250,7 +255,7 @@ Design design_from_c(const gpl_design_t *c) {
     bl.bbox = rect4(c->blockage_box + 4 * b);
     bl.inst = c->blockage_inst[b];
     bl.inst_fixed = c->blockage_inst_fixed[b] != 0;
-    if (bl.inst >= 0) bl.inst_name = d.insts[bl.inst].name;
+    if (bl.inst >= 0) bl.inst_name = inst_label(d, bl.inst);
     bl.max_density = c->blockage_max_density[b];
     d.blockages.push_back(bl);
   }
@@ -312,7 +317,7 @@ Common placer_base_common(Log &log, const Design &d, const Vars &v) {
     bool macro_ = di.master_is_block;
     if (!macro_ && di.bbox.dy() > ROW_LIMIT * site_y) {
       macro_ = true;
-      log.warn("GPL", 134, sfmt("Master %s is not marked as a BLOCK in LEF but is more than %d rows tall.  It will be treated as a macro.", di.master.c_str(), ROW_LIMIT));
+      log.warn("GPL", 134, sfmt("Master %s is not marked as a BLOCK in LEF but is more than %d rows tall.  It will be treated as a macro.", master_label(d, k).c_str(), ROW_LIMIT));
     }
     Instance inst;
     inst.db = (int)k;
@@ -326,8 +331,8 @@ Common placer_base_common(Log &log, const Design &d, const Vars &v) {
       inst.lx -= v.pad_left * site_x;
       inst.ux += v.pad_right * site_x;
     }
-    if (di.bbox.dy() > d.core.dy()) log.error("GPL", 119, sfmt("instance %s height is larger than core.", di.name.c_str()));
-    if (di.bbox.dx() > d.core.dx()) log.error("GPL", 120, sfmt("instance %s width is larger than core.", di.name.c_str()));
+    if (di.bbox.dy() > d.core.dy()) log.error("GPL", 119, sfmt("instance %s height is larger than core.", inst_label(d, k).c_str()));
+    if (di.bbox.dx() > d.core.dx()) log.error("GPL", 120, sfmt("instance %s width is larger than core.", inst_label(d, k).c_str()));
     if (inst.fixed) inst.snap_outward(d.core.lx, d.core.ly, site_x, site_y);
     c.insts.push_back(inst);
   }
@@ -598,11 +603,25 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
   for (size_t k = 0; k < c.insts.size(); k++)
     if (c.insts[k].db >= 0) inst_map[c.insts[k].db] = (int)k;
   Ip ip;
+  ip.db_bbox.reserve(d.insts.size());
   for (auto &i : d.insts) ip.db_bbox.push_back(i.bbox);
+  // sized up front: the pins, each net's list, each instance's list
+  size_t total = 0;
+  std::vector<int> per_inst(c.insts.size(), 0);
+  for (auto &[net, cnt] : c.nets) {
+    const DbNet &n = d.nets[net];
+    total += n.iterms.size() + (v.skip_io ? 0 : n.bterms.size());
+    for (auto &t : n.iterms)
+      if (inst_map[t.inst] >= 0) per_inst[inst_map[t.inst]]++;
+  }
+  ip.pins.reserve(total);
+  ip.net_pins.reserve(c.nets.size());
   ip.inst_pins.resize(c.insts.size());
+  for (size_t k = 0; k < c.insts.size(); k++) ip.inst_pins[k].reserve(per_inst[k]);
   for (auto &[net, cnt] : c.nets) {
     const DbNet &n = d.nets[net];
     std::vector<int> list;
+    list.reserve(n.iterms.size() + (v.skip_io ? 0 : n.bterms.size()));
     for (auto &t : n.iterms) {
       auto p4 = iterm_pin(d, t.inst, t);
       int pk = (int)ip.pins.size();
@@ -628,7 +647,7 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
         ip.pins.push_back(p);
       }
     }
-    ip.net_pins.push_back(list);
+    ip.net_pins.push_back(std::move(list));
   }
   std::vector<int> order(ip.pins.size(), 0);
   size_t k = 0;
@@ -637,7 +656,9 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
     for (auto &t : n.iterms) order[k++] = t.order;
     if (!v.skip_io) k += n.bterms.size();
   }
-  for (auto &pins : ip.inst_pins) std::stable_sort(pins.begin(), pins.end(), [&](int a, int b) { return order[a] < order[b]; });
+  for (auto &pins : ip.inst_pins)
+    if (!std::is_sorted(pins.begin(), pins.end(), [&](int a, int b) { return order[a] < order[b]; }))
+      std::stable_sort(pins.begin(), pins.end(), [&](int a, int b) { return order[a] < order[b]; });
   for (size_t q = 0; q < c.insts.size(); q++)
     if (!c.insts[q].fixed) ip.place.push_back((int)q);
   return ip;
@@ -725,6 +746,21 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
   std::vector<int32_t> ext(c.insts.size(), -1);
   for (size_t e = 0; e < n; e++) ext[ip.place[e]] = (int32_t)e;
   s.core = make_int4(d.core.lx, d.core.ly, d.core.ux, d.core.uy);
+  s.box.reserve(n);
+  s.locked.reserve(n);
+  s.grouped.reserve(n);
+  s.clamp.reserve(n);
+  s.db_box.reserve(n);
+  s.db_size.reserve(n);
+  const size_t np = ip.pins.size();
+  s.pin_e.reserve(np);
+  s.pin_inst.reserve(np);
+  s.pin_mio.reserve(np);
+  s.pin_off.reserve(np);
+  s.pin_xy.reserve(np);
+  s.pin_hp.reserve(np);
+  s.pin_static.reserve(np);
+  s.net_start.reserve(c.nets.size() + 1);
   for (size_t e = 0; e < n; e++) {
     const Instance &i = c.insts[ip.place[e]];
     s.box.push_back(make_int4(i.lx, i.ly, i.ux, i.uy));

@@ -67,6 +67,7 @@ void Engine::join() {
 
 Engine::~Engine() {
   release();
+  if (pinned_) cudaFreeHost(pinned_);
   if (wa_stream_) cudaStreamSynchronize(wa_stream_);
   if (stream_) cudaStreamDestroy(stream_);
   if (wa_stream_) cudaStreamDestroy(wa_stream_);
@@ -126,7 +127,7 @@ void Engine::release() {
 
 void Engine::upload(const EngineSetup &s) {
   release();
-  hpwl_ready_ = false;  // the density centres move
+  hpwl_ready_ = hpwl_fetched_ = false;  // the density centres move
   if (failed()) return;
   cudaStream_t st = stream_;
   n_cells_ = (int64_t)s.hx.size();
@@ -145,31 +146,71 @@ void Engine::upload(const EngineSetup &s) {
   any_locked_ = std::any_of(s.locked.begin(), s.locked.end(), [](uint8_t v) { return v != 0; });
   if (any_locked_) check(upload_vec(&locked_, s.locked, st), "upload cells");
   check(upload_vec(&cell_pin_start_, s.cell_pin_start, st), "upload cells");
-  check(upload_vec(&net_start_, s.net_start, st), "upload nets");
   {
-    // WA's tiles of consecutive nets, and the nets too large for a tile (in degree order,
-    // so a warp's threads walk nets of one length)
+    // The nets in degree order (stable), their pins following them: a WA tile then holds
+    // nets of one degree, so its thread-per-net phases do not diverge. No result depends on
+    // the order: each pin's force goes to its place in its cell's pin list (pin_slot), the
+    // HPWL is an integer sum, a net's weight moves with it.
+    std::vector<int64_t> by_deg;
+    int64_t max_deg = 0;
+    for (int32_t n = 0; n < n_nets_; n++) max_deg = std::max(max_deg, s.net_start[n + 1] - s.net_start[n]);
+    net_order_.resize(n_nets_);
+    if (max_deg <= (int64_t)1 << 20) {
+      by_deg.assign(max_deg + 2, 0);
+      for (int32_t n = 0; n < n_nets_; n++) by_deg[s.net_start[n + 1] - s.net_start[n] + 1]++;
+      for (int64_t d = 0; d <= max_deg; d++) by_deg[d + 1] += by_deg[d];
+      for (int32_t n = 0; n < n_nets_; n++) net_order_[by_deg[s.net_start[n + 1] - s.net_start[n]]++] = n;
+    } else {
+      for (int32_t n = 0; n < n_nets_; n++) net_order_[n] = n;
+      std::stable_sort(net_order_.begin(), net_order_.end(), [&](int32_t a, int32_t b) { return s.net_start[a + 1] - s.net_start[a] < s.net_start[b + 1] - s.net_start[b]; });
+    }
+    // each pin's force goes to its place in its cell's pin list
+    std::vector<int32_t> slot(n_pins_, -1);
+    for (size_t k = 0; k < s.cell_pins.size(); k++) slot[s.cell_pins[k]] = (int32_t)k;
+    std::vector<int64_t> ns(n_nets_ + 1, 0);
+    std::vector<int32_t> pc(n_pins_), ps(n_pins_);
+    std::vector<int2> pb(n_pins_);
+    std::vector<float> wt(n_nets_);
+    int64_t at = 0;
+    for (int32_t i = 0; i < n_nets_; i++) {
+      int32_t n = net_order_[i];
+      for (int64_t q = s.net_start[n]; q < s.net_start[n + 1]; q++, at++) {
+        pc[at] = s.pin_cell[q];
+        ps[at] = slot[q];
+        pb[at] = make_int2(s.pin_base[2 * q], s.pin_base[2 * q + 1]);
+      }
+      ns[i + 1] = at;
+      wt[i] = s.net_weight[n];
+    }
+    check(upload_vec(&net_start_, ns, st), "upload nets");
+    // WA's tiles of consecutive nets, and the nets too large for a tile (already in degree
+    // order, so a warp's threads walk nets of one length)
     std::vector<int2> tiles;
     std::vector<int32_t> big;
-    wa_tiles(s.net_start.data(), n_nets_, tiles, big);
-    std::stable_sort(big.begin(), big.end(), [&](int32_t a, int32_t b) { return s.net_start[a + 1] - s.net_start[a] < s.net_start[b + 1] - s.net_start[b]; });
+    wa_tiles(ns.data(), n_nets_, tiles, big);
     n_tiles_ = (int32_t)tiles.size();
     n_big_ = (int32_t)big.size();
     check(upload_vec(&tiles_, tiles, st), "upload nets");
     check(upload_vec(&big_nets_, big, st), "upload nets");
-    // each pin's force goes to its place in its cell's pin list
-    std::vector<int32_t> slot(n_pins_, -1);
-    for (size_t k = 0; k < s.cell_pins.size(); k++) slot[s.cell_pins[k]] = (int32_t)k;
-    check(upload_vec(&pin_slot_, slot, st), "upload pins");
+    check(upload_vec(&pin_slot_, ps, st), "upload pins");
+    check(upload_vec(&pin_cell_, pc, st), "upload pins");
+    check(upload_vec(&pin_base_, pb, st), "upload pins");
+    check(upload_vec(&net_weight_, wt, st), "upload nets");
   }
-  check(upload_vec(&pin_cell_, s.pin_cell, st), "upload pins");
-  check(dmalloc(&pin_base_, n_pins_), "upload pins");
-  if (n_pins_) check(cudaMemcpyAsync(pin_base_, s.pin_base.data(), n_pins_ * sizeof(int2), cudaMemcpyHostToDevice, st), "upload pins");
-  check(upload_vec(&net_weight_, s.net_weight, st), "upload nets");
   check(dmalloc(&pin_grad_, s.cell_pins.size()), "alloc pins");
   check(dmalloc(&hpwl_acc_, 1), "alloc");
   check(dmalloc(&dev_scal_, s.regions.size()), "alloc");
   host_scal_.assign(s.regions.size(), RegionScalars{});
+  {
+    size_t need = s.regions.size() * sizeof(RegionScalars) + sizeof(unsigned long long);
+    if (need > pinned_bytes_) {
+      if (pinned_) cudaFreeHost(pinned_);
+      pinned_ = nullptr;
+      pinned_bytes_ = 0;
+      check(cudaHostAlloc((void **)&pinned_, need, cudaHostAllocDefault), "alloc pinned");
+      if (pinned_) pinned_bytes_ = need;
+    }
+  }
   region_wx_.clear();
   region_wy_.clear();
   region_dims_.clear();
@@ -311,7 +352,7 @@ std::vector<float> Engine::get_coords(int b, SlotId slot) {
 void Engine::place_at(int b, SlotId slot) {
   join();
   if (failed()) return;
-  hpwl_ready_ = false;  // the density centres move
+  hpwl_ready_ = hpwl_fetched_ = false;  // the density centres move
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
   ph_begin(PH_PLACE);
@@ -328,7 +369,7 @@ void Engine::place_at(int b, SlotId slot) {
 void Engine::nesterov_step(int b, float step, float coeff) {
   join();
   if (failed()) return;
-  hpwl_ready_ = false;  // the density centres move
+  hpwl_ready_ = hpwl_fetched_ = false;  // the density centres move
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
   ph_begin(PH_PLACE);
@@ -381,6 +422,7 @@ void Engine::wa(float cx, float cy) {
   check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), st), "wa");
   w.hpwl_out = hpwl_acc_;
   hpwl_ready_ = true;
+  hpwl_fetched_ = false;
   ph_begin(PH_WA, st);
   if (n_tiles_) {
     launches += 1;
@@ -447,15 +489,28 @@ void Engine::copy_slot(int b, SlotId dst, SlotId src) {
 void Engine::fetch() {
   join();
   if (failed() || host_scal_.empty()) return;
-  check(cudaMemcpyAsync(host_scal_.data(), dev_scal_, host_scal_.size() * sizeof(RegionScalars), cudaMemcpyDeviceToHost, stream_), "fetch");
-  d2h_bytes += (int64_t)(host_scal_.size() * sizeof(RegionScalars));
+  const size_t bytes = host_scal_.size() * sizeof(RegionScalars);
+  const bool with_hpwl = hpwl_ready_ && !hpwl_fetched_;
+  check(cudaMemcpyAsync(pinned_, dev_scal_, bytes, cudaMemcpyDeviceToHost, stream_), "fetch");
+  d2h_bytes += (int64_t)bytes;
+  if (with_hpwl) {
+    check(cudaMemcpyAsync(pinned_ + bytes, hpwl_acc_, sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_), "fetch");
+    d2h_bytes += (int64_t)sizeof(unsigned long long);
+  }
   check(cudaStreamSynchronize(stream_), "fetch sync");
+  if (failed()) return;
+  std::memcpy(host_scal_.data(), pinned_, bytes);
+  if (with_hpwl) {
+    std::memcpy(&hpwl_host_, pinned_ + bytes, sizeof hpwl_host_);
+    hpwl_fetched_ = true;
+  }
   ph_flush();
 }
 
 int64_t Engine::hpwl() {
   join();
   if (failed()) return 0;
+  if (hpwl_ready_ && hpwl_fetched_) return (int64_t)hpwl_host_;  // read with the trial's scalars
   WaArgs w = wa_args();
   if (!hpwl_ready_) {
   check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), stream_), "hpwl");
@@ -476,6 +531,10 @@ int64_t Engine::hpwl() {
   d2h_bytes += 8;
   check(cudaStreamSynchronize(stream_), "hpwl sync");
   ph_flush();
+  if (!failed()) {
+    hpwl_host_ = h;
+    hpwl_fetched_ = true;
+  }
   return (int64_t)h;
 }
 
@@ -497,7 +556,15 @@ void Engine::centres(std::vector<int32_t> &dcx, std::vector<int32_t> &dcy) {
 
 void Engine::set_net_weights(const std::vector<float> &w) {
   join();
-  if (!w.empty()) check(cudaMemcpyAsync(net_weight_, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, stream_), "net weights");
+  if (w.empty()) return;
+  if (w.size() != net_order_.size()) {
+    check(cudaErrorInvalidValue, "net weights");
+    return;
+  }
+  // in the device's net order (a copy from pageable memory returns once the data is staged)
+  std::vector<float> dw(w.size());
+  for (size_t i = 0; i < w.size(); i++) dw[i] = w[net_order_[i]];
+  check(cudaMemcpyAsync(net_weight_, dw.data(), dw.size() * sizeof(float), cudaMemcpyHostToDevice, stream_), "net weights");
 }
 
 void Engine::rebuild_poisson(int mode) {

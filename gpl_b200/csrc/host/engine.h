@@ -133,6 +133,9 @@ class Engine {
   uint8_t *kind_ = nullptr, *locked_ = nullptr;
   bool any_locked_ = false;
   int64_t *cell_pin_start_ = nullptr;
+  // The device's nets (and their pins) in degree order, net_order_[i] being the i-th one's
+  // index in the placer's order: WA tiles then hold nets of one degree.
+  std::vector<int32_t> net_order_;
   int64_t *net_start_ = nullptr;
   int32_t *pin_cell_ = nullptr, *pin_slot_ = nullptr, *big_nets_ = nullptr;
   int2 *pin_base_ = nullptr, *tiles_ = nullptr;
@@ -141,6 +144,13 @@ class Engine {
   float2 *pin_grad_ = nullptr;  // the WA force of every pin of a cell, cell-major (cell_pins order)
   unsigned long long *hpwl_acc_ = nullptr;
   bool hpwl_ready_ = false;  // hpwl_acc_ holds the HPWL of the current centres (from the WA)
+  // Page-locked read-back: the trial's region scalars and, beside them, the HPWL the WA
+  // added up (hpwl_fetched_: that value is in hpwl_host_), so one copy and one wait serve
+  // both each trial.
+  uint8_t *pinned_ = nullptr;
+  size_t pinned_bytes_ = 0;
+  bool hpwl_fetched_ = false;
+  unsigned long long hpwl_host_ = 0;
   // The WA runs on its own stream, beside the density solve (it needs the centres, not the
   // field); everything that reads its forces or moves the centres joins it first.
   cudaStream_t wa_stream_ = nullptr;

@@ -199,12 +199,32 @@ struct Pin {
   int32_t off_x = 0, off_y = 0, cx = 0, cy = 0;
   bool min_x = false, max_x = false, min_y = false, max_y = false;
 };
+// Lists of pin indices, one per owner (a net, an instance), stored flat: owner k's pins are
+// items[start[k] .. start[k + 1]). The reference keeps a vector per owner; one array of all
+// of them builds without a heap block per owner.
+struct PinLists {
+  struct Span {
+    const int *b = nullptr, *e = nullptr;
+    const int *begin() const { return b; }
+    const int *end() const { return e; }
+    size_t size() const { return (size_t)(e - b); }
+    bool empty() const { return b == e; }
+    int operator[](size_t i) const { return b[i]; }
+  };
+  std::vector<int64_t> start{0};
+  std::vector<int> items;
+  size_t size() const { return start.size() - 1; }
+  Span operator[](size_t k) const { return {items.data() + start[k], items.data() + start[k + 1]}; }
+  int *begin_of(size_t k) { return items.data() + start[k]; }
+  int *end_of(size_t k) { return items.data() + start[k + 1]; }
+};
+
 struct Ip {
   std::vector<Pin> pins;
-  std::vector<std::vector<int>> net_pins;
+  PinLists net_pins;
   std::vector<Rect> db_bbox;
   std::vector<int> place;
-  std::vector<std::vector<int>> inst_pins;
+  PinLists inst_pins;
 };
 
 // ---- random numbers (src/normal.rs) ----

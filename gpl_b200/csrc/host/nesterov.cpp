@@ -42,7 +42,6 @@ struct GCell {
   bool macro_ = false;
   int32_t lx = 0, ly = 0, ux = 0, uy = 0, dlx = 0, dly = 0, dux = 0, duy = 0;
   float density_scale = 0;
-  std::vector<int> pins;
   bool locked = false;
   static GCell filler(int32_t cx, int32_t cy, int32_t dx, int32_t dy) {
     GCell g;
@@ -979,7 +978,8 @@ struct Placer {
   Engine &eng;
   std::vector<GCell> gcells;  // host copy: sizes and, after the loop, the placed centres
   std::vector<GPin> gpins;
-  std::vector<std::vector<int>> net_pins;
+  PinLists net_pins;
+  PinLists inst_pins;  // each instance's pins (a cell's are those of its instance)
   std::vector<int> pin_net;
   std::vector<Nb> nbs;
   std::vector<int64_t> dev_of_gcell;  // gcell -> device cell (-1: in no region)
@@ -1762,8 +1762,6 @@ static void init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip, co
     q.gcell = p.inst >= 0 ? inst_cell[p.inst] : -1;
     P.gpins.push_back(q);
   }
-  for (size_t k = 0; k < ip.inst_pins.size(); k++)
-    if (inst_cell[k] >= 0) P.gcells[inst_cell[k]].pins = ip.inst_pins[k];
   P.net_pins = std::move(ip.net_pins);  // the initial placement is done with them
   for (auto &b : bases)
     for (int k : b.place_insts)
@@ -1796,6 +1794,7 @@ static void init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip, co
     for (int gi : nb.cells) update_density_size_one(P.gcells[gi], nb);
     P.nbs.push_back(std::move(nb));
   }
+  P.inst_pins = std::move(ip.inst_pins);  // the perturbation above moves pins through them
 }
 
 static RegionSetup region_setup(const Nb &nb) {
@@ -1891,13 +1890,14 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
     s.dcy[dv] = g.d_cy();
     // a cell's pins sit where the placer copied them (before the perturbation); a rebuild
     // keeps the current centres
-    if (!rebuild && !g.pins.empty()) {
-      const GPin &q = P.gpins[g.pins[0]];
+    PinLists::Span pins = g.is_filler() ? PinLists::Span{} : P.inst_pins[g.inst];
+    if (!rebuild && !pins.empty()) {
+      const GPin &q = P.gpins[pins[0]];
       s.dcx[dv] = q.cx - q.off_x;
       s.dcy[dv] = q.cy - q.off_y;
     }
-    s.cell_pin_start[dv + 1] = s.cell_pin_start[dv] + (int64_t)g.pins.size();
-    for (int p : g.pins) s.cell_pins.push_back(p);
+    s.cell_pin_start[dv + 1] = s.cell_pin_start[dv] + (int64_t)pins.size();
+    for (int p : pins) s.cell_pins.push_back(p);
   }
   s.net_start.assign(P.net_pins.size() + 1, 0);
   size_t np = P.gpins.size();
@@ -2169,7 +2169,9 @@ struct Run {
       eng.launches += dev.launches;
       eng.h2d_bytes += dev.h2d_bytes;
       eng.d2h_bytes += dev.d2h_bytes;
+      progress("initial placement applied on the host");
     }
+    progress("initial placement device memory released");
     auto t1 = std::chrono::steady_clock::now();
     res.t_ip = std::chrono::duration<double>(t1 - t0).count();
     res.insts = (int64_t)c.insts.size();
@@ -2201,9 +2203,9 @@ struct Run {
     }
     // the first HPWL (the reference HPWL's base) over the pins as the placer copied them
     int64_t design_hpwl = 0;
-    for (auto &np : P->net_pins) {
+    for (size_t nn = 0; nn < P->net_pins.size(); nn++) {
       int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
-      for (int p : np) {
+      for (int p : P->net_pins[nn]) {
         lx = std::min(lx, P->gpins[p].cx);
         ly = std::min(ly, P->gpins[p].cy);
         ux = std::max(ux, P->gpins[p].cx);

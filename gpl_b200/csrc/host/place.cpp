@@ -607,58 +607,60 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
   for (auto &i : d.insts) ip.db_bbox.push_back(i.bbox);
   // sized up front: the pins, each net's list, each instance's list
   size_t total = 0;
-  std::vector<int> per_inst(c.insts.size(), 0);
+  ip.inst_pins.start.assign(c.insts.size() + 1, 0);
+  ip.net_pins.start.reserve(c.nets.size() + 1);
   for (auto &[net, cnt] : c.nets) {
     const DbNet &n = d.nets[net];
     total += n.iterms.size() + (v.skip_io ? 0 : n.bterms.size());
+    ip.net_pins.start.push_back((int64_t)total);
     for (auto &t : n.iterms)
-      if (inst_map[t.inst] >= 0) per_inst[inst_map[t.inst]]++;
+      if (inst_map[t.inst] >= 0) ip.inst_pins.start[inst_map[t.inst] + 1]++;
   }
-  ip.pins.reserve(total);
-  ip.net_pins.reserve(c.nets.size());
-  ip.inst_pins.resize(c.insts.size());
-  for (size_t k = 0; k < c.insts.size(); k++) ip.inst_pins[k].reserve(per_inst[k]);
+  for (size_t k = 0; k < c.insts.size(); k++) ip.inst_pins.start[k + 1] += ip.inst_pins.start[k];
+  ip.inst_pins.items.resize((size_t)ip.inst_pins.start.back());
+  std::vector<int64_t> fill(ip.inst_pins.start.begin(), ip.inst_pins.start.end() - 1);
+  // pins are made net by net, so net n's list is the run of pin numbers from its start
+  ip.net_pins.items.resize(total);
+  for (size_t q = 0; q < total; q++) ip.net_pins.items[q] = (int)q;
+  ip.pins.resize(total);
+  size_t pk = 0;
   for (auto &[net, cnt] : c.nets) {
     const DbNet &n = d.nets[net];
-    std::vector<int> list;
-    list.reserve(n.iterms.size() + (v.skip_io ? 0 : n.bterms.size()));
     for (auto &t : n.iterms) {
       auto p4 = iterm_pin(d, t.inst, t);
-      int pk = (int)ip.pins.size();
-      list.push_back(pk);
-      if (inst_map[t.inst] >= 0) ip.inst_pins[inst_map[t.inst]].push_back(pk);
-      Pin p;
-      p.inst = inst_map[t.inst];
+      int k = inst_map[t.inst];
+      if (k >= 0) ip.inst_pins.items[fill[k]++] = (int)pk;
+      Pin &p = ip.pins[pk++];
+      p.inst = k;
       p.off_x = p4[0];
       p.off_y = p4[1];
       p.cx = p4[2];
       p.cy = p4[3];
-      ip.pins.push_back(p);
     }
     if (!v.skip_io) {
       for (auto &pt : n.bterms) {
         Rect b = pt.has_bbox ? pt.bbox : Rect{};
-        list.push_back((int)ip.pins.size());
-        Pin p;
+        Pin &p = ip.pins[pk++];
         p.port = true;
         p.movable_io = v.place_ios && !pt.fixed;
         p.cx = (b.lx + b.ux) / 2;
         p.cy = (b.ly + b.uy) / 2;
-        ip.pins.push_back(p);
       }
     }
-    ip.net_pins.push_back(std::move(list));
   }
-  std::vector<int> order(ip.pins.size(), 0);
+  // each instance's pins in its iterms' order (the reference walks an instance's iterms)
+  std::vector<int> order(total, 0);
   size_t k = 0;
   for (auto &[net, cnt] : c.nets) {
     const DbNet &n = d.nets[net];
     for (auto &t : n.iterms) order[k++] = t.order;
     if (!v.skip_io) k += n.bterms.size();
   }
-  for (auto &pins : ip.inst_pins)
-    if (!std::is_sorted(pins.begin(), pins.end(), [&](int a, int b) { return order[a] < order[b]; }))
-      std::stable_sort(pins.begin(), pins.end(), [&](int a, int b) { return order[a] < order[b]; });
+  auto by_order = [&](int a, int b) { return order[a] < order[b]; };
+  for (size_t q = 0; q < c.insts.size(); q++) {
+    int *b = ip.inst_pins.begin_of(q), *e = ip.inst_pins.end_of(q);
+    if (!std::is_sorted(b, e, by_order)) std::stable_sort(b, e, by_order);
+  }
   for (size_t q = 0; q < c.insts.size(); q++)
     if (!c.insts[q].fixed) ip.place.push_back((int)q);
   return ip;
@@ -844,9 +846,11 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
     device(dev.update(), "initial placement update");
     if ((double)error_max <= 1e-5 && iter >= 5) break;
   }
+  progress("initial placement rounds done");
   // the placed instances, their database boxes and their pins back on the host
   std::vector<int4> box, db_box;
   device(dev.download(box, db_box), "initial placement download");
+  progress("initial placement downloaded");
   for (size_t e = 0; e < n; e++) {
     int k = ip.place[e];
     Instance &i = c.insts[k];

@@ -1,8 +1,11 @@
 // The initial placement's solver (`bicgstab`, src/bicgstab.rs:615-669) on the device: CSR
 // SpMV with each row summed in column order (the reference's `Csr::mul` order), float vectors,
 // and the inner products and residual norms in double (deterministic block partials). The
-// scalars (rho, alpha, omega) live on the device; the host reads two numbers per iteration
-// (the residual norm and the next rho) to run the loop's tests, restart included.
+// scalars (rho, alpha, omega) live on the device, and so do the loop's tests: the last kernel
+// of an iteration decides whether the loop goes on, ends (the residual bound, the iteration
+// cap) or must restart (rho too small), and every kernel of the next iteration returns at once
+// unless it goes on. The host enqueues iterations in batches, reads the loop's state once per
+// batch and runs a restart itself when the device asks for one.
 #include "bicgstab.h"
 #include "common.cuh"
 
@@ -11,35 +14,76 @@ namespace gpl {
 namespace {
 
 enum Scal { S_RHO = 0, S_RHO_OLD, S_ALPHA, S_W, S_RR, S_R0R, S_R0SQ, S_BB, S_COUNT };
+// The loop's state, after the three sums k_scalar's case 0 writes from S_R0SQ: the iteration
+// count, the state (0 iterate, 1 waiting for a restart, 2 ended), and the bounds the tests
+// compare with. Small integers, exact in double.
+enum Loop { S_I = 10, S_STATE, S_TOL2, S_EPS2, S_MAXIT, S_END };
+constexpr double kIterate = 0.0, kRestart = 1.0, kEnded = 2.0;
+// Which launches run: every one (kAlways), or only while the loop iterates (kLive).
+enum Gate { kAlways = -1, kLive = 0 };
+__device__ __forceinline__ bool gated_off(const double *S, int gate) {
+  return gate == kLive && S[S_STATE] != kIterate;
+}
+
+// The loop's tests (`while rr > tol2 && i < max_iters`, then the restart test
+// |rho| < eps^2 |r0|^2 at the head of the next iteration), in the reference's order.
+__device__ __forceinline__ double loop_state(const double *S) {
+  if (!(S[S_RR] > S[S_TOL2] && S[S_I] < S[S_MAXIT])) return kEnded;
+  return fabs(S[S_RHO]) < S[S_EPS2] * S[S_R0SQ] ? kRestart : kIterate;
+}
 
 // y = A x, then `0 + 1 * tmp` as the library writes it. A block's rows are contiguous in
 // the CSR arrays: the block first forms every product vals[k] * x[cols[k]] of its rows with
-// coalesced loads into shared memory, then each thread sums its row's products in column
-// order (the reference's order). A block whose rows hold more than kSpmvTile entries sums
-// straight from memory.
+// coalesced loads into shared memory (four entries per thread in flight), then each thread
+// sums its row's products in column order (the reference's order). A block whose rows hold
+// more than kSpmvTile entries sums straight from memory.
 constexpr int kSpmvTile = 6144;
+constexpr int kSpmvUnroll = 4;
 
-__global__ void __launch_bounds__(kThreads) k_spmv(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y) {
+__global__ void __launch_bounds__(kThreads) k_spmv(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
+  if (gated_off(S, gate)) return;
   __shared__ float prod[kSpmvTile];
-  const int64_t r0 = blockIdx.x * (int64_t)blockDim.x;
-  const int64_t r1 = min(n, r0 + (int64_t)blockDim.x);
+  const int64_t r0 = blockIdx.x * (int64_t)kThreads;
+  const int64_t r1 = min(n, r0 + (int64_t)kThreads);
   const int64_t k0 = rs[r0], k1 = rs[r1];
   const bool tiled = k1 - k0 <= kSpmvTile;
-  if (tiled)
-    for (int64_t k = k0 + threadIdx.x; k < k1; k += blockDim.x) prod[k - k0] = __fmul_rn(vals[k], x[cols[k]]);
+  if (tiled) {
+    const int cnt = (int)(k1 - k0);
+    const int32_t *c = cols + k0;
+    const float *v = vals + k0;
+    for (int j = threadIdx.x; j < cnt; j += kSpmvUnroll * kThreads) {
+      int cc[kSpmvUnroll];
+      float vv[kSpmvUnroll], xv[kSpmvUnroll];
+#pragma unroll
+      for (int u = 0; u < kSpmvUnroll; u++) {
+        int q = j + u * kThreads;
+        cc[u] = q < cnt ? c[q] : 0;
+        vv[u] = q < cnt ? v[q] : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kSpmvUnroll; u++) xv[u] = j + u * kThreads < cnt ? x[cc[u]] : 0.0f;
+#pragma unroll
+      for (int u = 0; u < kSpmvUnroll; u++) {
+        int q = j + u * kThreads;
+        if (q < cnt) prod[q] = __fmul_rn(vv[u], xv[u]);
+      }
+    }
+  }
   __syncthreads();
   const int64_t i = r0 + threadIdx.x;
   if (i >= n) return;
   float tmp = 0.0f;
+  const int64_t b = rs[i], e = rs[i + 1];
   if (tiled)
-    for (int64_t k = rs[i]; k < rs[i + 1]; k++) tmp = __fadd_rn(tmp, prod[k - k0]);
+    for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, prod[k - k0]);
   else
-    for (int64_t k = rs[i]; k < rs[i + 1]; k++) tmp = __fadd_rn(tmp, __fmul_rn(vals[k], x[cols[k]]));
+    for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, __fmul_rn(vals[k], x[cols[k]]));
   y[i] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
 }
 
 // Up to three dot products at once; partials[blk * 3 + j].
-__global__ void k_dots(int64_t n, const float *__restrict__ a0, const float *__restrict__ b0, const float *__restrict__ a1, const float *__restrict__ b1, const float *__restrict__ a2, const float *__restrict__ b2, double *__restrict__ part) {
+__global__ void k_dots(int64_t n, const float *__restrict__ a0, const float *__restrict__ b0, const float *__restrict__ a1, const float *__restrict__ b1, const float *__restrict__ a2, const float *__restrict__ b2, double *__restrict__ part, const double *__restrict__ S, int gate) {
+  if (gated_off(S, gate)) return;
   __shared__ double sh[kThreads / 32];
   double s0 = 0, s1 = 0, s2 = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -61,9 +105,11 @@ __global__ void k_dots(int64_t n, const float *__restrict__ a0, const float *__r
 //  which 0: S[dst0..dst0+2] = sums
 //  which 1 (alpha): S_ALPHA = rho / sum0
 //  which 2 (omega): S_W = sum0 > 0 ? sum1 / sum0 : 0
-//  which 3 (end of iteration): S_RR = sum0; S_RHO_OLD = S_RHO; S_RHO = sum1
+//  which 3 (end of iteration): S_RR = sum0; S_RHO_OLD = S_RHO; S_RHO = sum1; one more
+//           iteration; the loop's tests for the next one
 //  which 4 (restart): S_R0SQ = S_RHO = S_RR = sum0
-__global__ void k_scalar(const double *__restrict__ part, int nblk, double *__restrict__ S, int which, int dst0) {
+__global__ void k_scalar(const double *__restrict__ part, int nblk, double *__restrict__ S, int which, int dst0, int gate) {
+  if (gated_off(S, gate)) return;
   __shared__ double sh[kThreads / 32];
   double v[3];
   for (int j = 0; j < 3; j++) {
@@ -84,6 +130,8 @@ __global__ void k_scalar(const double *__restrict__ part, int nblk, double *__re
       S[S_RR] = v[0];
       S[S_RHO_OLD] = S[S_RHO];
       S[S_RHO] = v[1];
+      S[S_I] += 1.0;
+      S[S_STATE] = loop_state(S);
       break;
     case 4:
       S[S_R0SQ] = v[0];
@@ -93,7 +141,22 @@ __global__ void k_scalar(const double *__restrict__ part, int nblk, double *__re
   }
 }
 
-__global__ void k_residual(int64_t n, const float *__restrict__ b, const float *__restrict__ ax, float *__restrict__ r, float *__restrict__ r0) {
+// After a restart (which 4 above): the first one sets the iteration count back to zero.
+__global__ void k_restart_done(double *S, int first) {
+  if (first) S[S_I] = 0.0;
+  S[S_STATE] = kIterate;
+}
+
+__global__ void k_loop_init(double *S, double tol2, double eps2, int max_iters) {
+  S[S_I] = 0.0;
+  S[S_TOL2] = tol2;
+  S[S_EPS2] = eps2;
+  S[S_MAXIT] = (double)max_iters;
+  S[S_STATE] = loop_state(S);
+}
+
+__global__ void k_residual(int64_t n, const float *__restrict__ b, const float *__restrict__ ax, float *__restrict__ r, float *__restrict__ r0, const double *__restrict__ S, int gate) {
+  if (gated_off(S, gate)) return;
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   float v = __fsub_rn(b[i], ax[i]);
@@ -103,6 +166,7 @@ __global__ void k_residual(int64_t n, const float *__restrict__ b, const float *
 
 // p = r + beta (p - w v), beta = (rho / rho_old) (alpha / w)
 __global__ void k_update_p(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ p) {
+  if (gated_off(S, kLive)) return;
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   float beta = (float)((S[S_RHO] / S[S_RHO_OLD]) * (S[S_ALPHA] / S[S_W]));
@@ -111,6 +175,7 @@ __global__ void k_update_p(int64_t n, const double *__restrict__ S, const float 
 }
 
 __global__ void k_update_s(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ s) {
+  if (gated_off(S, kLive)) return;
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   float a = (float)S[S_ALPHA];
@@ -119,6 +184,7 @@ __global__ void k_update_s(int64_t n, const double *__restrict__ S, const float 
 
 // x += alpha p + w s; r = s - w t; partials of |r|^2 and r0.r
 __global__ void k_update_xr(int64_t n, const double *__restrict__ S, const float *__restrict__ p, const float *__restrict__ s, const float *__restrict__ t, const float *__restrict__ r0, float *__restrict__ x, float *__restrict__ r, double *__restrict__ part) {
+  if (gated_off(S, kLive)) return;
   __shared__ double sh[kThreads / 32];
   float a = (float)S[S_ALPHA], w = (float)S[S_W];
   double rr = 0, r0r = 0;
@@ -152,6 +218,9 @@ __global__ void k_scal_init(double *S) {
 
 }  // namespace
 
+// Iterations enqueued between two reads of the loop's state.
+constexpr int kBicgBatch = 8;
+
 size_t bicgstab_scratch_bytes(int64_t n) {
   size_t vec = (size_t)n * sizeof(float);
   vec = (vec + 255) / 256 * 256;
@@ -159,6 +228,7 @@ size_t bicgstab_scratch_bytes(int64_t n) {
 }
 
 cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_iters, void *scratch, cudaStream_t st, BicgResult *out) {
+  static_assert(S_END <= 64, "the scalars fit the scratch's 64 doubles");
   int64_t n = A.n;
   size_t vec = ((size_t)n * sizeof(float) + 255) / 256 * 256;
   char *base = (char *)scratch;
@@ -170,20 +240,20 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
   if (eb < 1) eb = 1;
   int rb = kBicgBlocks;
   const float tol = 1.1920929e-07f;
-  double hs[S_COUNT];
-  auto spmv = [&](const float *in, float *o) { k_spmv<<<eb, kThreads, 0, st>>>(n, A.rs, A.cols, A.vals, in, o); };
+  double hs[S_END];
+  auto spmv = [&](const float *in, float *o, int gate) { k_spmv<<<eb, kThreads, 0, st>>>(n, A.rs, A.cols, A.vals, in, o, S, gate); };
   auto pull = [&]() -> cudaError_t {
     cudaError_t e = cudaMemcpyAsync(hs, S, sizeof hs, cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return e;
     return cudaStreamSynchronize(st);
   };
   cudaError_t e;
-  spmv(x, ax);
-  k_residual<<<eb, kThreads, 0, st>>>(n, b, ax, r, r0);
-  k_dots<<<rb, kThreads, 0, st>>>(n, r0, r0, b, b, r0, r, part);
-  k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 0, S_R0SQ);  // S_R0SQ, S_BB, then dot(r0, r) in S[S_COUNT]
+  spmv(x, ax, kAlways);
+  k_residual<<<eb, kThreads, 0, st>>>(n, b, ax, r, r0, S, kAlways);
+  k_dots<<<rb, kThreads, 0, st>>>(n, r0, r0, b, b, r0, r, part, S, kAlways);
+  k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 0, S_R0SQ, kAlways);  // S_R0SQ, S_BB, then dot(r0, r) in S[S_COUNT]
   if ((e = pull()) != cudaSuccess) return e;
-  double r0_sqnorm = hs[S_R0SQ], rhs_sqnorm = hs[S_BB];
+  double rhs_sqnorm = hs[S_BB];
   if (rhs_sqnorm == 0.0) {
     k_fill<<<eb, kThreads, 0, st>>>(n, x, 0.0f);
     out->iterations = max_iters;
@@ -196,37 +266,41 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
   cudaMemsetAsync(p, 0, (size_t)n * sizeof(float), st);
   double tol2 = (double)tol * (double)tol * rhs_sqnorm;
   double eps2 = (double)tol * (double)tol;
-  double rr = r0_sqnorm;       // r == r0 at the start
-  double rho_next = r0_sqnorm;  // dot(r0, r)
-  int i = 0, restarts = 0;
-  while (rr > tol2 && i < max_iters) {
-    if (std::fabs(rho_next) < eps2 * r0_sqnorm) {
+  k_loop_init<<<1, 1, 0, st>>>(S, tol2, eps2, max_iters);
+  // Every iteration counts one and only the first restart sets the count back, so the loop
+  // ends within 2 max_iters + 1 iterations; a batch that asks for a restart holds until the
+  // host has run it, and every batch but the last runs at least one iteration.
+  const int64_t max_batches = 2 * (int64_t)max_iters + 3;
+  int64_t batches = 0;
+  int restarts = 0;
+  for (;;) {
+    for (int k = 0; k < kBicgBatch; k++) {
+      k_update_p<<<eb, kThreads, 0, st>>>(n, S, r, v, p);
+      spmv(p, v, kLive);
+      k_dots<<<rb, kThreads, 0, st>>>(n, r0, v, nullptr, nullptr, nullptr, nullptr, part, S, kLive);
+      k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 1, 0, kLive);
+      k_update_s<<<eb, kThreads, 0, st>>>(n, S, r, v, s);
+      spmv(s, t, kLive);
+      k_dots<<<rb, kThreads, 0, st>>>(n, t, t, t, s, nullptr, nullptr, part, S, kLive);
+      k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 2, 0, kLive);
+      k_update_xr<<<rb, kThreads, 0, st>>>(n, S, p, s, t, r0, x, r, part);
+      k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 3, 0, kLive);
+    }
+    if ((e = pull()) != cudaSuccess) return e;
+    if (hs[S_STATE] == kEnded) break;
+    if (++batches > max_batches) return cudaErrorUnknown;  // cannot happen: the count above
+    if (hs[S_STATE] == kRestart) {
       // too orthogonal to r0: restart from the current residual
-      spmv(x, ax);
-      k_residual<<<eb, kThreads, 0, st>>>(n, b, ax, r, r0);
-      k_dots<<<rb, kThreads, 0, st>>>(n, r, r, nullptr, nullptr, nullptr, nullptr, part);
-      k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 4, 0);
-      if ((e = pull()) != cudaSuccess) return e;
-      r0_sqnorm = hs[S_R0SQ];
-      if (restarts == 0) i = 0;
+      spmv(x, ax, kAlways);
+      k_residual<<<eb, kThreads, 0, st>>>(n, b, ax, r, r0, S, kAlways);
+      k_dots<<<rb, kThreads, 0, st>>>(n, r, r, nullptr, nullptr, nullptr, nullptr, part, S, kAlways);
+      k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 4, 0, kAlways);
+      k_restart_done<<<1, 1, 0, st>>>(S, restarts == 0 ? 1 : 0);
       restarts++;
     }
-    k_update_p<<<eb, kThreads, 0, st>>>(n, S, r, v, p);
-    spmv(p, v);
-    k_dots<<<rb, kThreads, 0, st>>>(n, r0, v, nullptr, nullptr, nullptr, nullptr, part);
-    k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 1, 0);
-    k_update_s<<<eb, kThreads, 0, st>>>(n, S, r, v, s);
-    spmv(s, t);
-    k_dots<<<rb, kThreads, 0, st>>>(n, t, t, t, s, nullptr, nullptr, part);
-    k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 2, 0);
-    k_update_xr<<<rb, kThreads, 0, st>>>(n, S, p, s, t, r0, x, r, part);
-    k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 3, 0);
-    if ((e = pull()) != cudaSuccess) return e;
-    rr = hs[S_RR];
-    rho_next = hs[S_RHO];
-    i++;
   }
-  out->iterations = i;
+  double rr = hs[S_RR];
+  out->iterations = (int)hs[S_I];
   out->error = (float)std::sqrt(rr / rhs_sqnorm);
   out->converged = out->error <= tol;
   return cudaGetLastError();

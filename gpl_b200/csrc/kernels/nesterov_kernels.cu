@@ -344,14 +344,18 @@ __global__ void k_wa(WaArgs w, float cx, float cy) {
 //   1. pins' positions into shared memory (coalesced; one gather of the cell centre each);
 //   2. a thread per net: the net's box, and each pin's net;
 //   3. a thread per pin: the four exp terms (zero where the exponent is at or below -300,
-//      which leaves a sum unchanged: the reference skips those terms);
+//      which leaves a sum unchanged: the reference skips those terms), which of them the
+//      reference takes (a mask beside the pin's net), and the position as floats;
 //   4. a thread per net: the eight sums in pin order (the reference's float order);
 //   5. a thread per pin: its force.
-// The results are the thread-per-net kernel's bit for bit.
+// The engine orders its nets by degree, so a tile's nets are alike and the thread-per-net
+// phases run without divergence. The results are the thread-per-net kernel's bit for bit.
+static_assert(kWaTileNets <= 256, "a pin's net index in the tile is kept in 8 bits");
+
 __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float cy) {
-  __shared__ int2 s_pos[kWaTilePins];
+  __shared__ int2 s_pos[kWaTilePins];        // phases 1-3: the position; 3-5: its floats' bits
   __shared__ float4 s_v[kWaTilePins];
-  __shared__ uint16_t s_pnet[kWaTilePins];
+  __shared__ uint16_t s_pnet[kWaTilePins];   // the pin's net in the tile | taken-terms mask << 8
   __shared__ int32_t s_nstart[kWaTileNets + 1];
   __shared__ int4 s_box[kWaTileNets];
   __shared__ float s_sum[8][kWaTileNets];
@@ -386,15 +390,19 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
   const float BAR = -300.0f;
   for (int j = threadIdx.x; j < np; j += blockDim.x) {
     int2 q = s_pos[j];
-    int4 b = s_box[s_pnet[j]];
+    uint32_t n = s_pnet[j];
+    int4 b = s_box[n];
     float emin_x = __fmul_rn((float)(b.x - q.x), cx), emax_x = __fmul_rn((float)(q.x - b.z), cx);
     float emin_y = __fmul_rn((float)(b.y - q.y), cy), emax_y = __fmul_rn((float)(q.y - b.w), cy);
+    uint32_t m = (emin_x > BAR ? 1u : 0u) | (emax_x > BAR ? 2u : 0u) | (emin_y > BAR ? 4u : 0u) | (emax_y > BAR ? 8u : 0u);
     float4 v;
-    v.x = emin_x > BAR ? fast_exp(emin_x) : 0.0f;
-    v.y = emax_x > BAR ? fast_exp(emax_x) : 0.0f;
-    v.z = emin_y > BAR ? fast_exp(emin_y) : 0.0f;
-    v.w = emax_y > BAR ? fast_exp(emax_y) : 0.0f;
+    v.x = (m & 1u) ? fast_exp(emin_x) : 0.0f;
+    v.y = (m & 2u) ? fast_exp(emax_x) : 0.0f;
+    v.z = (m & 4u) ? fast_exp(emin_y) : 0.0f;
+    v.w = (m & 8u) ? fast_exp(emax_y) : 0.0f;
     s_v[j] = v;
+    s_pnet[j] = (uint16_t)(n | (m << 8));
+    s_pos[j] = make_int2(__float_as_int((float)q.x), __float_as_int((float)q.y));
   }
   __syncthreads();
   for (int j = threadIdx.x; j < nn; j += blockDim.x) {
@@ -402,7 +410,7 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
     for (int32_t k = s_nstart[j]; k < s_nstart[j + 1]; k++) {
       int2 q = s_pos[k];
       float4 v = s_v[k];
-      float qx = (float)q.x, qy = (float)q.y;
+      float qx = __int_as_float(q.x), qy = __int_as_float(q.y);
       s_minx = __fadd_rn(s_minx, v.x);
       s_xminx = __fadd_rn(s_xminx, __fmul_rn(qx, v.x));
       s_maxx = __fadd_rn(s_maxx, v.y);
@@ -425,15 +433,13 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
   for (int j = threadIdx.x; j < np; j += blockDim.x) {
     int2 q = s_pos[j];
     float4 v = s_v[j];
-    int n = s_pnet[j];
-    int4 b = s_box[n];
-    float qx = (float)q.x, qy = (float)q.y;
-    float emin_x = __fmul_rn((float)(b.x - q.x), cx), emax_x = __fmul_rn((float)(q.x - b.z), cx);
-    float emin_y = __fmul_rn((float)(b.y - q.y), cy), emax_y = __fmul_rn((float)(q.y - b.w), cy);
-    float gmin_x = emin_x > BAR ? wa_term_min(s_sum[0][n], s_sum[1][n], v.x, cx, qx) : 0.0f;
-    float gmax_x = emax_x > BAR ? wa_term_max(s_sum[2][n], s_sum[3][n], v.y, cx, qx) : 0.0f;
-    float gmin_y = emin_y > BAR ? wa_term_min(s_sum[4][n], s_sum[5][n], v.z, cy, qy) : 0.0f;
-    float gmax_y = emax_y > BAR ? wa_term_max(s_sum[6][n], s_sum[7][n], v.w, cy, qy) : 0.0f;
+    uint32_t pn = s_pnet[j];
+    uint32_t n = pn & 0xffu, m = pn >> 8;
+    float qx = __int_as_float(q.x), qy = __int_as_float(q.y);
+    float gmin_x = (m & 1u) ? wa_term_min(s_sum[0][n], s_sum[1][n], v.x, cx, qx) : 0.0f;
+    float gmax_x = (m & 2u) ? wa_term_max(s_sum[2][n], s_sum[3][n], v.y, cx, qx) : 0.0f;
+    float gmin_y = (m & 4u) ? wa_term_min(s_sum[4][n], s_sum[5][n], v.z, cy, qy) : 0.0f;
+    float gmax_y = (m & 8u) ? wa_term_max(s_sum[6][n], s_sum[7][n], v.w, cy, qy) : 0.0f;
     float wt = w.net_weight ? w.net_weight[t.x + n] : 1.0f;
     wa_store(w, p0 + j, make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt)));
   }

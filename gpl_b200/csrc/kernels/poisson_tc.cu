@@ -7,13 +7,15 @@
 // memory. The epilogue reads the accumulator back (tcgen05.ld) and writes the next GEMM's
 // split operand directly, or the spectral step's two operands, or the FP32 field.
 //
-// Kernel: one 128 x 128 output tile per CTA of 128 threads. Thread 0 issues the TMA loads of
-// each K-block (128B-swizzled 128x64 bf16 tiles: A_hi, A_lo, B_hi, B_lo) into a 3-stage ring;
-// thread 32 issues tcgen05.mma (M=128, N=128, K=16, kind::f16, bf16 in, f32 accumulate),
-// three per K step, as the stages land, committing each stage back to the producer; after the
-// last K-block all four warps read their 32 TMEM lanes, 32 columns at a time. Every wait is
-// bounded by the GPU's global timer (1 s): a wait that runs out records an error word, and
-// the CTA drains and returns.
+// Kernel: one 128 x BN output tile per CTA of 128 threads. Thread 0 issues the TMA loads of
+// each K-block (128B-swizzled 64-wide bf16 tiles: A_hi, A_lo, B_hi, B_lo) into a ring of
+// stages; thread 32 issues tcgen05.mma (M=128, N=BN, K=16, kind::f16, bf16 in, f32
+// accumulate), three per K step, as the stages land, committing each stage back to the
+// producer; after the last K-block all four warps read their 32 TMEM lanes, 32 columns at a
+// time. The single GEMMs use BN = 64 (a 1024-point grid gives 128 tiles for the 148 SMs), the
+// batched pairs BN = 128 (the same 128 tiles over both). Every wait is bounded by the GPU's
+// global timer (1 s): a wait that runs out records an error word, and the CTA drains and
+// returns.
 //
 // The four launches of a solve (see poisson.cu for the algebra):
 //   1  T1t = CyTs rho^T                      split out
@@ -39,12 +41,20 @@ namespace {
 // A stage holds one K-block of both halves of both operands: A_hi, A_lo (BM x BK each) and
 // B_hi, B_lo (BN x BK each); its three products hi*hi, hi*lo, lo*hi all accumulate into the
 // one TMEM tile, so each operand byte crosses from L2 once per output tile.
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3;
+constexpr int BM = 128, BK = 64;
 constexpr int A_TILE = BM * BK * 2;                    // 16 KB
-constexpr int B_TILE = BN * BK * 2;                    // 16 KB
-constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;   // 64 KB, a multiple of 1 KB
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr uint32_t TMEM_COLS = BN;                     // fp32 accumulator columns
+template <int BN>
+struct Tile {
+  static constexpr int B_TILE = BN * BK * 2;                   // 8 or 16 KB
+  static constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;  // 48 or 64 KB, multiples of 1 KB
+  static constexpr int STAGES = BN == 64 ? 4 : 3;
+  static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+  static constexpr uint32_t TMEM_COLS = BN;                    // fp32 accumulator columns
+  // kind::f16 instruction descriptor: D f32, A and B bf16, both K-major, M=BM, N=BN.
+  static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+  static_assert(BN % 16 == 0 && BN >= 32 && BN <= 256 && (BN & (BN - 1)) == 0, "an M=128 MMA shape with a power-of-two TMEM allocation");
+  static_assert(SMEM_BYTES <= 227 * 1024, "shared memory per CTA");
+};
 constexpr int EPI_COLS = 32;                           // accumulator columns per epilogue step
 constexpr uint64_t WAIT_NS = 1000000000ull;    // a wait that lasts a second is an error
 
@@ -108,15 +118,12 @@ __device__ __forceinline__ void tma_load(void *dst, const CUtensorMap *map, uint
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
-// kind::f16 instruction descriptor: D f32, A and B bf16, both K-major, M=BM, N=BN.
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-
-__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(IDESC), "r"(accumulate));
+      "l"(da), "l"(db), "r"(idesc), "r"(accumulate));
 }
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -147,9 +154,12 @@ __device__ __forceinline__ void split_store(__nv_bfloat16 *row_hi, __nv_bfloat16
   }
 }
 
-template <int EPI>
+template <int EPI, int BN>
 __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tB0,
                                                    const __grid_constant__ CUtensorMap tA1, const __grid_constant__ CUtensorMap tB1, TcArgs args) {
+  using T = Tile<BN>;
+  constexpr int STAGES = T::STAGES, STAGE_BYTES = T::STAGE_BYTES, B_TILE = T::B_TILE;
+  constexpr uint32_t TMEM_COLS = T::TMEM_COLS, IDESC = T::IDESC;
   extern __shared__ uint8_t smem_raw[];
   uint8_t *smem = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   uint64_t *full = (uint64_t *)(smem + STAGES * STAGE_BYTES);
@@ -205,9 +215,9 @@ __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUte
 #pragma unroll
       for (int kk = 0; kk < BK / 16; kk++) {
         uint32_t o = kk * 32;
-        umma(tmem, smem_desc(ahi + o), smem_desc(bhi + o), (kb > 0 || kk > 0) ? 1u : 0u);
-        umma(tmem, smem_desc(ahi + o), smem_desc(blo + o), 1u);
-        umma(tmem, smem_desc(alo + o), smem_desc(bhi + o), 1u);
+        umma(tmem, smem_desc(ahi + o), smem_desc(bhi + o), IDESC, (kb > 0 || kk > 0) ? 1u : 0u);
+        umma(tmem, smem_desc(ahi + o), smem_desc(blo + o), IDESC, 1u);
+        umma(tmem, smem_desc(alo + o), smem_desc(bhi + o), IDESC, 1u);
       }
       umma_commit(&empty[s]);
     }
@@ -304,7 +314,8 @@ struct TcState {
   __nv_bfloat16 *t1 = nullptr, *exh = nullptr, *eyh = nullptr, *t2 = nullptr, *t3 = nullptr;
   int *err = nullptr;
   CUtensorMap mCyTs, mCxTs, mCy, mSy, mSx, mCx;  // A operands (BM-row boxes)
-  CUtensorMap mDens, mT1, mExh, mEyh, mT2, mT3;  // B operands (BN-row boxes)
+  CUtensorMap mDens, mT1;                        // B operands of the single GEMMs (64-row boxes)
+  CUtensorMap mExh, mEyh, mT2, mT3;              // B operands of the batched pairs (128-row boxes)
 };
 
 static cudaError_t upload_split(const std::vector<double> &h, int rows, int k, __nv_bfloat16 **d) {
@@ -354,19 +365,20 @@ cudaError_t tc_plan_init(PoissonPlan *p, const BasisHost &b) {
   TRY(make_map(&t->mSy, t->Sy, ny, ny, BM));
   TRY(make_map(&t->mSx, t->Sx, nx, nx, BM));
   TRY(make_map(&t->mCx, t->Cx, nx, nx, BM));
-  // B operands [N][2K]: 64-row boxes
-  TRY(make_map(&t->mDens, p->tc_dens, nx, ny, BN));  // rows x, K = y
-  TRY(make_map(&t->mT1, t->t1, ny, nx, BN));         // rows v, K = x
-  TRY(make_map(&t->mExh, t->exh, nx, ny, BN));       // rows u, K = v
-  TRY(make_map(&t->mEyh, t->eyh, nx, ny, BN));
-  TRY(make_map(&t->mT2, t->t2, ny, nx, BN));         // rows y, K = u
-  TRY(make_map(&t->mT3, t->t3, ny, nx, BN));
+  // B operands [N][2K]: BN-row boxes
+  TRY(make_map(&t->mDens, p->tc_dens, nx, ny, 64));  // rows x, K = y
+  TRY(make_map(&t->mT1, t->t1, ny, nx, 64));         // rows v, K = x
+  TRY(make_map(&t->mExh, t->exh, nx, ny, 128));      // rows u, K = v
+  TRY(make_map(&t->mEyh, t->eyh, nx, ny, 128));
+  TRY(make_map(&t->mT2, t->t2, ny, nx, 128));        // rows y, K = u
+  TRY(make_map(&t->mT3, t->t3, ny, nx, 128));
 #undef TRY
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(k_tc_gemm<EPI_SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    cudaFuncSetAttribute(k_tc_gemm<EPI_SPECTRAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    cudaFuncSetAttribute(k_tc_gemm<EPI_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    cudaFuncSetAttribute(k_tc_gemm<EPI_SPLIT, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tile<64>::SMEM_BYTES);
+    cudaFuncSetAttribute(k_tc_gemm<EPI_SPECTRAL, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tile<64>::SMEM_BYTES);
+    cudaFuncSetAttribute(k_tc_gemm<EPI_SPLIT, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tile<128>::SMEM_BYTES);
+    cudaFuncSetAttribute(k_tc_gemm<EPI_F32, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, Tile<128>::SMEM_BYTES);
     attr = true;
   }
   return cudaGetLastError();
@@ -398,21 +410,21 @@ cudaError_t tc_solve(PoissonPlan *p, float *field_x, float *field_y, cudaStream_
   // 1: T1t[v][x] = sum_y CyTs[v][y] rho[x][y]      M = ny, N = nx, K = ny
   a.M = ny, a.N = nx, a.K = ny;
   a.o[0] = TcOut{t->t1, nullptr, nx};
-  k_tc_gemm<EPI_SPLIT><<<dim3(nx / BN, ny / BM, 1), 128, SMEM_BYTES, s>>>(t->mCyTs, t->mDens, t->mCyTs, t->mDens, a);
+  k_tc_gemm<EPI_SPLIT, 64><<<dim3(nx / 64, ny / BM, 1), 128, Tile<64>::SMEM_BYTES, s>>>(t->mCyTs, t->mDens, t->mCyTs, t->mDens, a);
   // 2: Ah[u][v] = sum_x CxTs[u][x] T1t[v][x]; spectral  M = nx, N = ny, K = nx
   a.M = nx, a.N = ny, a.K = nx;
   a.o[0] = TcOut{t->exh, t->eyh, ny};
-  k_tc_gemm<EPI_SPECTRAL><<<dim3(ny / BN, nx / BM, 1), 128, SMEM_BYTES, s>>>(t->mCxTs, t->mT1, t->mCxTs, t->mT1, a);
+  k_tc_gemm<EPI_SPECTRAL, 64><<<dim3(ny / 64, nx / BM, 1), 128, Tile<64>::SMEM_BYTES, s>>>(t->mCxTs, t->mT1, t->mCxTs, t->mT1, a);
   // 3: T2t[y][u] = sum_v Cy[y][v] Exh[u][v]; T3t = Sy Eyh^T   M = ny, N = nx, K = ny
   a.M = ny, a.N = nx, a.K = ny;
   a.o[0] = TcOut{t->t2, nullptr, nx};
   a.o[1] = TcOut{t->t3, nullptr, nx};
-  k_tc_gemm<EPI_SPLIT><<<dim3(nx / BN, ny / BM, 2), 128, SMEM_BYTES, s>>>(t->mCy, t->mExh, t->mSy, t->mEyh, a);
+  k_tc_gemm<EPI_SPLIT, 128><<<dim3(nx / 128, ny / BM, 2), 128, Tile<128>::SMEM_BYTES, s>>>(t->mCy, t->mExh, t->mSy, t->mEyh, a);
   // 4: Ex[x][y] = sum_u Sx[x][u] T2t[y][u]; Ey = Cx T3t^T     M = nx, N = ny, K = nx
   a.M = nx, a.N = ny, a.K = nx;
   a.o[0] = TcOut{field_x, nullptr, ny};
   a.o[1] = TcOut{field_y, nullptr, ny};
-  k_tc_gemm<EPI_F32><<<dim3(ny / BN, nx / BM, 2), 128, SMEM_BYTES, s>>>(t->mSx, t->mT2, t->mCx, t->mT3, a);
+  k_tc_gemm<EPI_F32, 128><<<dim3(ny / 128, nx / BM, 2), 128, Tile<128>::SMEM_BYTES, s>>>(t->mSx, t->mT2, t->mCx, t->mT3, a);
   return cudaGetLastError();
 }
 

@@ -115,6 +115,13 @@ int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_x
   return (int)(e != cudaSuccess ? e : e2);
 }
 
+static_assert(GPL_SPMV_ROWS == kSpmvRows && GPL_SPMV_TILED == kSpmvTiled, "the C ABI's SpMV forms");
+
+int gpl_kernel_spmv(int64_t n, const int64_t *row_start, const int32_t *cols, const float *vals, const float *x, float *y, int32_t form, void *stream) {
+  CsrDev A{n, row_start, cols, vals};
+  return (int)spmv(A, x, y, form, (cudaStream_t)stream);
+}
+
 int gpl_kernel_bicgstab(int64_t n, const int64_t *row_start, const int32_t *cols, const float *vals, const float *rhs, float *x, int32_t max_iters, int32_t *iterations, float *error, void *stream) {
   cudaStream_t s = (cudaStream_t)stream;
   void *scratch = nullptr;

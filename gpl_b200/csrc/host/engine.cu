@@ -8,6 +8,10 @@
 #include "engine.h"
 
 namespace gpl {
+void progress(const char *fmt, ...) __attribute__((format(printf, 1, 2)));
+}
+
+namespace gpl {
 
 struct Engine::Region {
   RegionArgs args{};
@@ -197,6 +201,7 @@ void Engine::upload(const EngineSetup &s) {
     check(upload_vec(&pin_base_, pb, st), "upload pins");
     check(upload_vec(&net_weight_, wt, st), "upload nets");
   }
+  progress("  upload: cells, nets and pins");
   check(dmalloc(&pin_grad_, s.cell_pins.size()), "alloc pins");
   check(dmalloc(&hpwl_acc_, 1), "alloc");
   check(dmalloc(&dev_scal_, s.regions.size()), "alloc");
@@ -249,6 +254,7 @@ void Engine::upload(const EngineSetup &s) {
       r->plan = poisson_plan_create(rs.nx, rs.ny, rs.wx.data(), rs.wy.data(), poisson_mode_, &pe);
       check(pe, poisson_mode_ == 0 ? "poisson plan (fp32)" : "poisson plan (split-bf16 tcgen05)");
       if (r->plan) r->dens_split = poisson_split_input(r->plan, &r->split_ld);
+      progress("  upload: region solver planned (%dx%d bins)", rs.nx, rs.ny);
     }
     RegionArgs &a = r->args;
     a.n_cells = (int32_t)rs.n_cells;

@@ -1778,8 +1778,11 @@ static void init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip, co
     nb.non_place_insts_area = base.non_place_insts_area;
     nb.max_phi_coef = o.max_phi_coef;
     nb.generator = Mt19937((uint32_t)o.seed);
+    progress("  region set-up: cells and pins copied");
     std::vector<GCell> fillers = init_filler_gcells(log, d, c, base, nb, o);
+    progress("  region set-up: %zu fillers", fillers.size());
     perturb_place_insts(d, c, ip, base, inst_cell, P.gcells, o, nb.generator);
+    progress("  region set-up: instances perturbed");
     nb.fillers = (int64_t)fillers.size();
     for (int k : base.place_insts) nb.cells.push_back(inst_cell[k]);
     for (auto &f : fillers) {
@@ -1787,6 +1790,7 @@ static void init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip, co
       P.gcells.push_back(f);
     }
     init_bins(log, d, c, base, nb, o);
+    progress("  region set-up: bins");
     nb.wx.resize(nb.bg.cnt_x);
     nb.wy.resize(nb.bg.cnt_y);
     for (int i = 0; i < nb.bg.cnt_x; i++) nb.wx[i] = wavenumber_x(i, nb.bg.cnt_x);
@@ -1868,6 +1872,7 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
       P.gcell_of_dev.push_back(kv.second);
     }
   }
+  progress("  device set-up: cells in Z order");
   size_t n = P.gcell_of_dev.size();
   s.hx.resize(n);
   s.hy.resize(n);
@@ -1922,7 +1927,9 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
     }
   }
   s.net_weight.assign(P.net_pins.size(), 1.0f);
+  progress("  device set-up: cells and pins");
   for (auto &nb : P.nbs) s.regions.push_back(region_setup(nb));
+  progress("  device set-up: regions");
   return s;
 }
 

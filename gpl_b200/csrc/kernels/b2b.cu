@@ -618,8 +618,12 @@ cudaError_t IpDevice::solve(int axis, int max_iters, IpAxisResult &out) {
   Axis &A = ax_[axis];
   CsrDev m{n_, A.starts, A.cols, A.vals};
   BicgResult r{};
-  cudaError_t e = bicgstab_solve(m, A.rhs, A.x, max_iters, scratch_, s_, &r);
-  launches += 4 + (int64_t)r.iterations * 10;
+  if (spmv_form_ < 0) {
+    CK(bicgstab_pick_spmv(m, A.x, scratch_, s_, &spmv_form_));
+    launches += 8;
+  }
+  cudaError_t e = bicgstab_solve(m, A.rhs, A.x, max_iters, scratch_, s_, &r, spmv_form_);
+  launches += 4 + (int64_t)r.iterations * 7;
   d2h_bytes += (int64_t)(r.iterations + 2) * 64;
   out.solve = r;
   return e;

@@ -62,6 +62,7 @@ class IpDevice {
 
  private:
   cudaStream_t s_;
+  int spmv_form_ = -1;  // the solver's SpMV form, timed on the first solve
   int64_t n_ = 0, n_pins_ = 0, n_locked_ = 0;
   int32_t n_nets_ = 0;
   IpSetup cfg_;

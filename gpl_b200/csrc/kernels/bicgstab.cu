@@ -18,12 +18,14 @@ enum Scal { S_RHO = 0, S_RHO_OLD, S_ALPHA, S_W, S_RR, S_R0R, S_R0SQ, S_BB, S_COU
 // count, the state (0 iterate, 1 waiting for a restart, 2 ended), and the bounds the tests
 // compare with. Small integers, exact in double.
 enum Loop { S_I = 10, S_STATE, S_TOL2, S_EPS2, S_MAXIT, S_END };
+constexpr int S_TICKET = 16;  // the fused reductions' arrival count (an unsigned int)
 constexpr double kIterate = 0.0, kRestart = 1.0, kEnded = 2.0;
 // Which launches run: every one (kAlways), or only while the loop iterates (kLive).
 enum Gate { kAlways = -1, kLive = 0 };
 __device__ __forceinline__ bool gated_off(const double *S, int gate) {
   return gate == kLive && S[S_STATE] != kIterate;
 }
+
 
 // The loop's tests (`while rr > tol2 && i < max_iters`, then the restart test
 // |rho| < eps^2 |r0|^2 at the head of the next iteration), in the reference's order.
@@ -32,20 +34,38 @@ __device__ __forceinline__ double loop_state(const double *S) {
   return fabs(S[S_RHO]) < S[S_EPS2] * S[S_R0SQ] ? kRestart : kIterate;
 }
 
-// y = A x, then `0 + 1 * tmp` as the library writes it. A block's rows are contiguous in
-// the CSR arrays: the block first forms every product vals[k] * x[cols[k]] of its rows with
-// coalesced loads into shared memory (four entries per thread in flight), then each thread
-// sums its row's products in column order (the reference's order). A block whose rows hold
-// more than kSpmvTile entries sums straight from memory.
+// y = A x, then `0 + 1 * tmp` as the library writes it, each row's products summed in
+// column order (the reference's order). Two forms with the same results (SpmvForm):
+//  rows:  a thread per row straight from memory;
+//  tiled: a block's rows are contiguous in the CSR arrays, so the block first forms every
+//         product vals[k] * x[cols[k]] of its rows with coalesced loads into shared memory
+//         (four entries per thread in flight), then each thread sums its row's products; a
+//         block whose rows hold more than kSpmvTile entries sums straight from memory.
 constexpr int kSpmvTile = 6144;
 constexpr int kSpmvUnroll = 4;
 
-__global__ void __launch_bounds__(kThreads) k_spmv(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
+__global__ void __launch_bounds__(kThreads) k_spmv_rows(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
+  if (gated_off(S, gate)) return;
+  const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  if (i >= n) return;
+  float tmp = 0.0f;
+  const int64_t b = rs[i], e = rs[i + 1];
+  for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, __fmul_rn(vals[k], x[cols[k]]));
+  y[i] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
+}
+
+__global__ void __launch_bounds__(kThreads) k_spmv_tiled(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
   if (gated_off(S, gate)) return;
   __shared__ float prod[kSpmvTile];
   const int64_t r0 = blockIdx.x * (int64_t)kThreads;
   const int64_t r1 = min(n, r0 + (int64_t)kThreads);
   const int64_t k0 = rs[r0], k1 = rs[r1];
+  const int64_t i = r0 + threadIdx.x;
+  int64_t b = 0, e = 0;
+  if (i < n) {
+    b = rs[i];
+    e = rs[i + 1];
+  }
   const bool tiled = k1 - k0 <= kSpmvTile;
   if (tiled) {
     const int cnt = (int)(k1 - k0);
@@ -57,11 +77,11 @@ __global__ void __launch_bounds__(kThreads) k_spmv(int64_t n, const int64_t *__r
 #pragma unroll
       for (int u = 0; u < kSpmvUnroll; u++) {
         int q = j + u * kThreads;
-        cc[u] = q < cnt ? c[q] : 0;
-        vv[u] = q < cnt ? v[q] : 0.0f;
+        cc[u] = q < cnt ? __ldg(c + q) : 0;
+        vv[u] = q < cnt ? __ldg(v + q) : 0.0f;
       }
 #pragma unroll
-      for (int u = 0; u < kSpmvUnroll; u++) xv[u] = j + u * kThreads < cnt ? x[cc[u]] : 0.0f;
+      for (int u = 0; u < kSpmvUnroll; u++) xv[u] = j + u * kThreads < cnt ? __ldg(x + cc[u]) : 0.0f;
 #pragma unroll
       for (int u = 0; u < kSpmvUnroll; u++) {
         int q = j + u * kThreads;
@@ -70,51 +90,37 @@ __global__ void __launch_bounds__(kThreads) k_spmv(int64_t n, const int64_t *__r
     }
   }
   __syncthreads();
-  const int64_t i = r0 + threadIdx.x;
   if (i >= n) return;
   float tmp = 0.0f;
-  const int64_t b = rs[i], e = rs[i + 1];
-  if (tiled)
-    for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, prod[k - k0]);
-  else
+  if (tiled) {
+    const int lb = (int)(b - k0), le = (int)(e - k0);
+    for (int k = lb; k < le; k++) tmp = __fadd_rn(tmp, prod[k]);
+  } else {
     for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, __fmul_rn(vals[k], x[cols[k]]));
+  }
   y[i] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
 }
 
-// Up to three dot products at once; partials[blk * 3 + j].
-__global__ void k_dots(int64_t n, const float *__restrict__ a0, const float *__restrict__ b0, const float *__restrict__ a1, const float *__restrict__ b1, const float *__restrict__ a2, const float *__restrict__ b2, double *__restrict__ part, const double *__restrict__ S, int gate) {
-  if (gated_off(S, gate)) return;
-  __shared__ double sh[kThreads / 32];
-  double s0 = 0, s1 = 0, s2 = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    s0 += (double)a0[i] * (double)b0[i];
-    if (a1) s1 += (double)a1[i] * (double)b1[i];
-    if (a2) s2 += (double)a2[i] * (double)b2[i];
-  }
-  double t0 = block_sum<kThreads>(s0, sh);
-  double t1 = block_sum<kThreads>(s1, sh);
-  double t2 = block_sum<kThreads>(s2, sh);
-  if (threadIdx.x == 0) {
-    part[3 * blockIdx.x] = t0;
-    part[3 * blockIdx.x + 1] = t1;
-    part[3 * blockIdx.x + 2] = t2;
-  }
+static void spmv_launch(int form, int eb, cudaStream_t st, const CsrDev &A, const float *in, float *o, const double *S, int gate) {
+  if (form == kSpmvTiled)
+    k_spmv_tiled<<<eb, kThreads, 0, st>>>(A.n, A.rs, A.cols, A.vals, in, o, S, gate);
+  else
+    k_spmv_rows<<<eb, kThreads, 0, st>>>(A.n, A.rs, A.cols, A.vals, in, o, S, gate);
 }
 
-// Reduce the partials and apply one scalar step:
+// Reduce the partials and apply one scalar step (the block's threads over the blocks'
+// partials, in a fixed order, so every launch shape gives the same sums):
 //  which 0: S[dst0..dst0+2] = sums
 //  which 1 (alpha): S_ALPHA = rho / sum0
 //  which 2 (omega): S_W = sum0 > 0 ? sum1 / sum0 : 0
 //  which 3 (end of iteration): S_RR = sum0; S_RHO_OLD = S_RHO; S_RHO = sum1; one more
 //           iteration; the loop's tests for the next one
 //  which 4 (restart): S_R0SQ = S_RHO = S_RR = sum0
-__global__ void k_scalar(const double *__restrict__ part, int nblk, double *__restrict__ S, int which, int dst0, int gate) {
-  if (gated_off(S, gate)) return;
-  __shared__ double sh[kThreads / 32];
+__device__ void scalar_step(const double *part, int nblk, double *S, int which, int dst0, double *sh) {
   double v[3];
   for (int j = 0; j < 3; j++) {
     double s = 0;
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += part[3 * b + j];
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += __ldcg(part + 3 * b + j);
     v[j] = block_sum<kThreads>(s, sh);
   }
   if (threadIdx.x != 0) return;
@@ -139,6 +145,50 @@ __global__ void k_scalar(const double *__restrict__ part, int nblk, double *__re
       S[S_RR] = v[0];
       break;
   }
+}
+
+// Whether this block is the last of its launch to finish (its partial written and fenced
+// before it counts itself); the last one then sees every block's partial. The count is left
+// at zero for the next launch.
+__device__ bool last_block(unsigned int *ticket) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    if (last) *ticket = 0;
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Up to three dot products at once; partials[blk * 3 + j]. With which >= 0 the last block to
+// finish also takes that scalar step (one launch fewer than a separate k_scalar).
+__global__ void k_dots(int64_t n, const float *__restrict__ a0, const float *__restrict__ b0, const float *__restrict__ a1, const float *__restrict__ b1, const float *__restrict__ a2, const float *__restrict__ b2, double *__restrict__ part, double *__restrict__ S, int gate, int which, unsigned int *ticket) {
+  if (gated_off(S, gate)) return;
+  __shared__ double sh[kThreads / 32];
+  double s0 = 0, s1 = 0, s2 = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    s0 += (double)a0[i] * (double)b0[i];
+    if (a1) s1 += (double)a1[i] * (double)b1[i];
+    if (a2) s2 += (double)a2[i] * (double)b2[i];
+  }
+  double t0 = block_sum<kThreads>(s0, sh);
+  double t1 = block_sum<kThreads>(s1, sh);
+  double t2 = block_sum<kThreads>(s2, sh);
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = t0;
+    part[3 * blockIdx.x + 1] = t1;
+    part[3 * blockIdx.x + 2] = t2;
+  }
+  if (which >= 0 && last_block(ticket)) scalar_step(part, gridDim.x, S, which, 0, sh);
+}
+
+__global__ void k_scalar(const double *__restrict__ part, int nblk, double *__restrict__ S, int which, int dst0, int gate) {
+  if (gated_off(S, gate)) return;
+  __shared__ double sh[kThreads / 32];
+  scalar_step(part, nblk, S, which, dst0, sh);
 }
 
 // After a restart (which 4 above): the first one sets the iteration count back to zero.
@@ -182,8 +232,9 @@ __global__ void k_update_s(int64_t n, const double *__restrict__ S, const float 
   s[i] = __fsub_rn(r[i], __fmul_rn(a, v[i]));
 }
 
-// x += alpha p + w s; r = s - w t; partials of |r|^2 and r0.r
-__global__ void k_update_xr(int64_t n, const double *__restrict__ S, const float *__restrict__ p, const float *__restrict__ s, const float *__restrict__ t, const float *__restrict__ r0, float *__restrict__ x, float *__restrict__ r, double *__restrict__ part) {
+// x += alpha p + w s; r = s - w t; partials of |r|^2 and r0.r, the last block taking the
+// iteration's end (scalar step 3)
+__global__ void k_update_xr(int64_t n, double *__restrict__ S, const float *__restrict__ p, const float *__restrict__ s, const float *__restrict__ t, const float *__restrict__ r0, float *__restrict__ x, float *__restrict__ r, double *__restrict__ part, unsigned int *ticket) {
   if (gated_off(S, kLive)) return;
   __shared__ double sh[kThreads / 32];
   float a = (float)S[S_ALPHA], w = (float)S[S_W];
@@ -202,6 +253,7 @@ __global__ void k_update_xr(int64_t n, const double *__restrict__ S, const float
     part[3 * blockIdx.x + 1] = t1;
     part[3 * blockIdx.x + 2] = 0.0;
   }
+  if (last_block(ticket)) scalar_step(part, gridDim.x, S, 3, 0, sh);  // the iteration's end
 }
 
 __global__ void k_fill(int64_t n, float *a, float v) {
@@ -227,8 +279,38 @@ size_t bicgstab_scratch_bytes(int64_t n) {
   return 7 * vec + (size_t)kBicgBlocks * 3 * sizeof(double) + 64 * sizeof(double);
 }
 
-cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_iters, void *scratch, cudaStream_t st, BicgResult *out) {
-  static_assert(S_END <= 64, "the scalars fit the scratch's 64 doubles");
+cudaError_t spmv(const CsrDev &A, const float *x, float *y, int form, cudaStream_t st) {
+  if (form != kSpmvRows && form != kSpmvTiled) return cudaErrorInvalidValue;
+  if (A.n <= 0) return cudaSuccess;
+  spmv_launch(form, (int)((A.n + kThreads - 1) / kThreads), st, A, x, y, nullptr, kAlways);
+  return cudaGetLastError();
+}
+
+cudaError_t bicgstab_pick_spmv(const CsrDev &A, const float *x, void *scratch, cudaStream_t st, int *form) {
+  *form = kSpmvRows;
+  if (A.n <= 0) return cudaSuccess;
+  int eb = (int)((A.n + kThreads - 1) / kThreads);
+  float *y = (float *)scratch;  // the first scratch vector
+  cudaEvent_t ev[2];
+  for (auto &e : ev)
+    if (cudaEventCreate(&e) != cudaSuccess) return cudaGetLastError();
+  float ms[2] = {0, 0};
+  cudaError_t err = cudaSuccess;
+  for (int f = 0; f < 2 && err == cudaSuccess; f++) {
+    spmv_launch(f, eb, st, A, x, y, nullptr, kAlways);  // warm
+    cudaEventRecord(ev[0], st);
+    for (int r = 0; r < 3; r++) spmv_launch(f, eb, st, A, x, y, nullptr, kAlways);
+    cudaEventRecord(ev[1], st);
+    err = cudaEventSynchronize(ev[1]);
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms[f], ev[0], ev[1]);
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  if (err == cudaSuccess && ms[kSpmvTiled] < ms[kSpmvRows]) *form = kSpmvTiled;
+  return err != cudaSuccess ? err : cudaGetLastError();
+}
+
+cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_iters, void *scratch, cudaStream_t st, BicgResult *out, int form) {
+  static_assert(S_END <= S_TICKET && S_TICKET < 64, "the scalars fit the scratch's 64 doubles");
   int64_t n = A.n;
   size_t vec = ((size_t)n * sizeof(float) + 255) / 256 * 256;
   char *base = (char *)scratch;
@@ -236,12 +318,13 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
   float *s = (float *)(base + 4 * vec), *t = (float *)(base + 5 * vec), *ax = (float *)(base + 6 * vec);
   double *part = (double *)(base + 7 * vec);
   double *S = part + (size_t)kBicgBlocks * 3;
+  unsigned int *ticket = (unsigned int *)(S + S_TICKET);
   int eb = (int)((n + kThreads - 1) / kThreads);
   if (eb < 1) eb = 1;
   int rb = kBicgBlocks;
   const float tol = 1.1920929e-07f;
   double hs[S_END];
-  auto spmv = [&](const float *in, float *o, int gate) { k_spmv<<<eb, kThreads, 0, st>>>(n, A.rs, A.cols, A.vals, in, o, S, gate); };
+  auto spmv = [&](const float *in, float *o, int gate) { spmv_launch(form, eb, st, A, in, o, S, gate); };
   auto pull = [&]() -> cudaError_t {
     cudaError_t e = cudaMemcpyAsync(hs, S, sizeof hs, cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return e;
@@ -250,7 +333,8 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
   cudaError_t e;
   spmv(x, ax, kAlways);
   k_residual<<<eb, kThreads, 0, st>>>(n, b, ax, r, r0, S, kAlways);
-  k_dots<<<rb, kThreads, 0, st>>>(n, r0, r0, b, b, r0, r, part, S, kAlways);
+  cudaMemsetAsync(ticket, 0, sizeof(unsigned int), st);
+  k_dots<<<rb, kThreads, 0, st>>>(n, r0, r0, b, b, r0, r, part, S, kAlways, -1, ticket);
   k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 0, S_R0SQ, kAlways);  // S_R0SQ, S_BB, then dot(r0, r) in S[S_COUNT]
   if ((e = pull()) != cudaSuccess) return e;
   double rhs_sqnorm = hs[S_BB];
@@ -277,14 +361,11 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
     for (int k = 0; k < kBicgBatch; k++) {
       k_update_p<<<eb, kThreads, 0, st>>>(n, S, r, v, p);
       spmv(p, v, kLive);
-      k_dots<<<rb, kThreads, 0, st>>>(n, r0, v, nullptr, nullptr, nullptr, nullptr, part, S, kLive);
-      k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 1, 0, kLive);
+      k_dots<<<rb, kThreads, 0, st>>>(n, r0, v, nullptr, nullptr, nullptr, nullptr, part, S, kLive, 1, ticket);
       k_update_s<<<eb, kThreads, 0, st>>>(n, S, r, v, s);
       spmv(s, t, kLive);
-      k_dots<<<rb, kThreads, 0, st>>>(n, t, t, t, s, nullptr, nullptr, part, S, kLive);
-      k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 2, 0, kLive);
-      k_update_xr<<<rb, kThreads, 0, st>>>(n, S, p, s, t, r0, x, r, part);
-      k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 3, 0, kLive);
+      k_dots<<<rb, kThreads, 0, st>>>(n, t, t, t, s, nullptr, nullptr, part, S, kLive, 2, ticket);
+      k_update_xr<<<rb, kThreads, 0, st>>>(n, S, p, s, t, r0, x, r, part, ticket);
     }
     if ((e = pull()) != cudaSuccess) return e;
     if (hs[S_STATE] == kEnded) break;
@@ -293,7 +374,7 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
       // too orthogonal to r0: restart from the current residual
       spmv(x, ax, kAlways);
       k_residual<<<eb, kThreads, 0, st>>>(n, b, ax, r, r0, S, kAlways);
-      k_dots<<<rb, kThreads, 0, st>>>(n, r, r, nullptr, nullptr, nullptr, nullptr, part, S, kAlways);
+      k_dots<<<rb, kThreads, 0, st>>>(n, r, r, nullptr, nullptr, nullptr, nullptr, part, S, kAlways, -1, ticket);
       k_scalar<<<1, kThreads, 0, st>>>(part, rb, S, 4, 0, kAlways);
       k_restart_done<<<1, 1, 0, st>>>(S, restarts == 0 ? 1 : 0);
       restarts++;

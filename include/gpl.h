@@ -232,6 +232,15 @@ int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy,
 int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy,
                   const float *net_weight, float coef_x, float coef_y, float *grad, void *stream);
 
+/* `Csr::mul` (src/bicgstab.rs:72-82): y = A x on a CSR matrix (device pointers), each row's
+ * products summed in column order, then 0 + 1 * sum, as the solver forms them. form picks the
+ * kernel: GPL_SPMV_ROWS (a thread per row) or GPL_SPMV_TILED (a block's products staged in
+ * shared memory); both give the same y, bit for bit. */
+#define GPL_SPMV_ROWS 0
+#define GPL_SPMV_TILED 1
+int gpl_kernel_spmv(int64_t n, const int64_t *row_start, const int32_t *cols, const float *vals,
+                    const float *x, float *y, int32_t form, void *stream);
+
 /* The initial placement's solver `bicgstab` (src/bicgstab.rs:615-669) on a CSR matrix (device
  * pointers) with FP64 inner products; x is the start point and the result. Writes iterations
  * and error (host pointers). Allocates its scratch vectors per call. */

@@ -131,6 +131,33 @@ def test_poisson(L, nx, ny, mode):
     assert np.max(np.abs(ey - fy)) <= tol * np.max(np.abs(fy))
 
 
+@pytest.mark.parametrize("form", [0, 1])
+def test_spmv_forms_match_the_reference_order(L, form):
+    """`Csr::mul` (src/bicgstab.rs:72-82) bit for bit: each row's products summed in float in
+    column order, then 0 + 1 * sum. Rows 512-767 hold 40 entries each (10240 in one block of
+    256 rows), past the tiled form's shared-memory tile, so its fallback runs too."""
+    rng = np.random.default_rng(21)
+    n = 5000
+    lens = rng.integers(0, 31, n)
+    lens[512:768] = 40
+    starts = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    cols = np.concatenate([np.sort(rng.choice(n, int(k), replace=False)) for k in lens]).astype(np.int32)
+    vals = rng.uniform(-2, 2, int(starts[-1])).astype(np.float32)
+    x = rng.uniform(-1e3, 1e3, n).astype(np.float32)
+    prod = (vals * x[cols]).astype(np.float32)
+    tmp = np.zeros(n, np.float32)
+    for j in range(int(lens.max())):
+        rows = np.flatnonzero(lens > j)
+        tmp[rows] = (tmp[rows] + prod[starts[rows] + j]).astype(np.float32)
+    ref = (np.float32(0.0) + np.float32(1.0) * tmp).astype(np.float32)
+    d = [dev(starts), dev(cols), dev(vals), dev(x)]  # held across the call
+    y = dev(np.full(n, np.nan, np.float32))
+    L.gpl_kernel_spmv.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
+    assert L.gpl_kernel_spmv(n, ptr(d[0]), ptr(d[1]), ptr(d[2]), ptr(d[3]), ptr(y), form, stream()) == 0
+    sync()
+    assert np.array_equal(y.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
 def test_bicgstab_matches_the_oracle(L):
     rng = np.random.default_rng(3)
     n = 3000

@@ -6,6 +6,7 @@
 #include "../kernels/bicgstab.h"
 #include "../kernels/engine_kernels.h"
 #include "engine.h"
+#include "parallel.h"
 
 namespace gpl {
 void progress(const char *fmt, ...) __attribute__((format(printf, 1, 2)));
@@ -168,24 +169,28 @@ void Engine::upload(const EngineSetup &s) {
       for (int32_t n = 0; n < n_nets_; n++) net_order_[n] = n;
       std::stable_sort(net_order_.begin(), net_order_.end(), [&](int32_t a, int32_t b) { return s.net_start[a + 1] - s.net_start[a] < s.net_start[b + 1] - s.net_start[b]; });
     }
-    // each pin's force goes to its place in its cell's pin list
+    // each pin's force goes to its place in its cell's pin list (cell_pins lists each pin once)
     std::vector<int32_t> slot(n_pins_, -1);
-    for (size_t k = 0; k < s.cell_pins.size(); k++) slot[s.cell_pins[k]] = (int32_t)k;
+    parallel_for(s.cell_pins.size(), [&](size_t a, size_t b) {
+      for (size_t k = a; k < b; k++) slot[s.cell_pins[k]] = (int32_t)k;
+    });
     std::vector<int64_t> ns(n_nets_ + 1, 0);
+    for (int32_t i = 0; i < n_nets_; i++) ns[i + 1] = ns[i] + (s.net_start[net_order_[i] + 1] - s.net_start[net_order_[i]]);
     std::vector<int32_t> pc(n_pins_), ps(n_pins_);
     std::vector<int2> pb(n_pins_);
     std::vector<float> wt(n_nets_);
-    int64_t at = 0;
-    for (int32_t i = 0; i < n_nets_; i++) {
-      int32_t n = net_order_[i];
-      for (int64_t q = s.net_start[n]; q < s.net_start[n + 1]; q++, at++) {
-        pc[at] = s.pin_cell[q];
-        ps[at] = slot[q];
-        pb[at] = make_int2(s.pin_base[2 * q], s.pin_base[2 * q + 1]);
+    parallel_for((size_t)n_nets_, [&](size_t a, size_t b) {
+      for (size_t i = a; i < b; i++) {
+        int32_t n = net_order_[i];
+        int64_t at = ns[i];
+        for (int64_t q = s.net_start[n]; q < s.net_start[n + 1]; q++, at++) {
+          pc[at] = s.pin_cell[q];
+          ps[at] = slot[q];
+          pb[at] = make_int2(s.pin_base[2 * q], s.pin_base[2 * q + 1]);
+        }
+        wt[i] = s.net_weight[n];
       }
-      ns[i + 1] = at;
-      wt[i] = s.net_weight[n];
-    }
+    });
     check(upload_vec(&net_start_, ns, st), "upload nets");
     // WA's tiles of consecutive nets, and the nets too large for a tile (already in degree
     // order, so a warp's threads walk nets of one length)

@@ -15,6 +15,7 @@
 
 #include "../kernels/engine_kernels.h"
 #include "engine.h"
+#include "parallel.h"
 #include "../kernels/b2b.h"
 #include "../kernels/rudy.h"
 #include "host.h"
@@ -804,17 +805,22 @@ static void init_bins(Log &log, const Design &d, const Common &c, const Base &ba
   bg.size_x = (double)(r.ux - r.lx) / (double)bg.cnt_x;
   bg.size_y = (double)(r.uy - r.ly) / (double)bg.cnt_y;
   log.info("GPL", 29, sfmt("%-21s %7.3f * %6.3f um", "Bin size (W * H):", bg.size_x / (double)d.dbu, bg.size_y / (double)d.dbu));
-  for (int32_t y = 0; y < bg.cnt_y; y++)
-    for (int32_t x = 0; x < bg.cnt_x; x++) {
-      Bin b;
-      b.lx = r.lx + f2i(std::round((double)x * bg.size_x));
-      b.ly = r.ly + f2i(std::round((double)y * bg.size_y));
-      b.ux = r.lx + f2i(std::round((double)(x + 1) * bg.size_x));
-      b.uy = r.ly + f2i(std::round((double)(y + 1) * bg.size_y));
-      b.target_density = nb.target_density;
-      if (b.ux - b.lx < 0 || b.uy - b.ly < 0) log.warn("GPL", 34, sfmt("Bin (center: %d,%d, index: %d) has negative size: %d, %d", (b.lx + b.ux) / 2, (b.ly + b.uy) / 2, y * bg.cnt_x + x, b.ux - b.lx, b.uy - b.ly));
-      bg.bins.push_back(b);
-    }
+  bg.bins.resize((size_t)bg.cnt_x * bg.cnt_y);
+  parallel_for((size_t)bg.cnt_y, [&](size_t y0, size_t y1) {
+    for (int32_t y = (int32_t)y0; y < (int32_t)y1; y++)
+      for (int32_t x = 0; x < bg.cnt_x; x++) {
+        Bin &b = bg.bins[(size_t)y * bg.cnt_x + x];
+        b.lx = r.lx + f2i(std::round((double)x * bg.size_x));
+        b.ly = r.ly + f2i(std::round((double)y * bg.size_y));
+        b.ux = r.lx + f2i(std::round((double)(x + 1) * bg.size_x));
+        b.uy = r.ly + f2i(std::round((double)(y + 1) * bg.size_y));
+        b.target_density = nb.target_density;
+      }
+  }, 16);
+  for (size_t k = 0; k < bg.bins.size(); k++) {
+    const Bin &b = bg.bins[k];
+    if (b.ux - b.lx < 0 || b.uy - b.ly < 0) log.warn("GPL", 34, sfmt("Bin (center: %d,%d, index: %zu) has negative size: %d, %d", (b.lx + b.ux) / 2, (b.ly + b.uy) / 2, k, b.ux - b.lx, b.uy - b.ly));
+  }
   log.info("GPL", 30, sfmt("Number of bins:             %10zu", bg.bins.size()));
   nb.bg = std::move(bg);
   nb.fixed.clear();
@@ -1738,30 +1744,35 @@ struct Placer {
 static void init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip, const std::vector<Base> &bases, Placer &P) {
   const Opts &o = P.o;
   std::vector<int> inst_cell(c.insts.size(), -1);
+  for (size_t q = 0; q < ip.place.size(); q++) inst_cell[ip.place[q]] = (int)q;
   P.gcells.reserve(ip.place.size() + ip.place.size() / 4);
-  P.gpins.reserve(ip.pins.size());
-  for (int k : ip.place) {
-    const Instance &i = c.insts[k];
-    inst_cell[k] = (int)P.gcells.size();
-    GCell g;
-    g.inst = k;
-    g.macro_ = i.macro_;
-    g.lx = g.dlx = i.lx;
-    g.ly = g.dly = i.ly;
-    g.ux = g.dux = i.ux;
-    g.uy = g.duy = i.uy;
-    g.locked = i.locked;
-    P.gcells.push_back(g);
-  }
-  for (auto &p : ip.pins) {
-    GPin q;
-    q.cx = p.cx;
-    q.cy = p.cy;
-    q.off_x = p.off_x;
-    q.off_y = p.off_y;
-    q.gcell = p.inst >= 0 ? inst_cell[p.inst] : -1;
-    P.gpins.push_back(q);
-  }
+  P.gcells.resize(ip.place.size());
+  parallel_for(ip.place.size(), [&](size_t a, size_t b) {
+    for (size_t q = a; q < b; q++) {
+      int k = ip.place[q];
+      const Instance &i = c.insts[k];
+      GCell &g = P.gcells[q];
+      g.inst = k;
+      g.macro_ = i.macro_;
+      g.lx = g.dlx = i.lx;
+      g.ly = g.dly = i.ly;
+      g.ux = g.dux = i.ux;
+      g.uy = g.duy = i.uy;
+      g.locked = i.locked;
+    }
+  });
+  P.gpins.resize(ip.pins.size());
+  parallel_for(ip.pins.size(), [&](size_t a, size_t b) {
+    for (size_t q = a; q < b; q++) {
+      const Pin &p = ip.pins[q];
+      GPin &g = P.gpins[q];
+      g.cx = p.cx;
+      g.cy = p.cy;
+      g.off_x = p.off_x;
+      g.off_y = p.off_y;
+      g.gcell = p.inst >= 0 ? inst_cell[p.inst] : -1;
+    }
+  });
   P.net_pins = std::move(ip.net_pins);  // the initial placement is done with them
   for (auto &b : bases)
     for (int k : b.place_insts)
@@ -1883,49 +1894,52 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
   s.dcx.resize(n);
   s.dcy.resize(n);
   s.cell_pin_start.assign(n + 1, 0);
-  for (size_t dv = 0; dv < n; dv++) {
-    const GCell &g = P.gcells[P.gcell_of_dev[dv]];
-    s.hx[dv] = g.d_dx() / 2;
-    s.hy[dv] = g.d_dy() / 2;
-    s.dscale[dv] = g.density_scale;
-    s.area[dv] = (float)g.dx() * (float)g.dy();
-    s.kind[dv] = g.is_filler() ? CELL_FILLER : (g.macro_ ? CELL_MACRO : CELL_STD);
-    s.locked[dv] = g.locked ? 1 : 0;
-    s.dcx[dv] = g.d_cx();
-    s.dcy[dv] = g.d_cy();
-    // a cell's pins sit where the placer copied them (before the perturbation); a rebuild
-    // keeps the current centres
-    PinLists::Span pins = g.is_filler() ? PinLists::Span{} : P.inst_pins[g.inst];
-    if (!rebuild && !pins.empty()) {
-      const GPin &q = P.gpins[pins[0]];
-      s.dcx[dv] = q.cx - q.off_x;
-      s.dcy[dv] = q.cy - q.off_y;
+  auto cell_pins = [&](const GCell &g) { return g.is_filler() ? PinLists::Span{} : P.inst_pins[g.inst]; };
+  for (size_t dv = 0; dv < n; dv++) s.cell_pin_start[dv + 1] = s.cell_pin_start[dv] + (int64_t)cell_pins(P.gcells[P.gcell_of_dev[dv]]).size();
+  s.cell_pins.resize((size_t)s.cell_pin_start[n]);
+  parallel_for(n, [&](size_t a, size_t b) {
+    for (size_t dv = a; dv < b; dv++) {
+      const GCell &g = P.gcells[P.gcell_of_dev[dv]];
+      s.hx[dv] = g.d_dx() / 2;
+      s.hy[dv] = g.d_dy() / 2;
+      s.dscale[dv] = g.density_scale;
+      s.area[dv] = (float)g.dx() * (float)g.dy();
+      s.kind[dv] = g.is_filler() ? CELL_FILLER : (g.macro_ ? CELL_MACRO : CELL_STD);
+      s.locked[dv] = g.locked ? 1 : 0;
+      s.dcx[dv] = g.d_cx();
+      s.dcy[dv] = g.d_cy();
+      // a cell's pins sit where the placer copied them (before the perturbation); a rebuild
+      // keeps the current centres
+      PinLists::Span pins = cell_pins(g);
+      if (!rebuild && !pins.empty()) {
+        const GPin &q = P.gpins[pins[0]];
+        s.dcx[dv] = q.cx - q.off_x;
+        s.dcy[dv] = q.cy - q.off_y;
+      }
+      std::copy(pins.begin(), pins.end(), s.cell_pins.begin() + s.cell_pin_start[dv]);
     }
-    s.cell_pin_start[dv + 1] = s.cell_pin_start[dv] + (int64_t)pins.size();
-    for (int p : pins) s.cell_pins.push_back(p);
-  }
-  s.net_start.assign(P.net_pins.size() + 1, 0);
+  });
+  s.net_start.assign(P.net_pins.start.begin(), P.net_pins.start.end());
   size_t np = P.gpins.size();
   s.pin_cell.assign(np, -1);
   s.pin_base.assign(2 * np, 0);
   // pins are numbered net-major already (the placer's pins are made net by net)
-  for (size_t nn = 0; nn < P.net_pins.size(); nn++) {
-    s.net_start[nn + 1] = s.net_start[nn] + (int64_t)P.net_pins[nn].size();
-    for (size_t j = 0; j < P.net_pins[nn].size(); j++)
-      if (P.net_pins[nn][j] != (int)(s.net_start[nn] + j)) refuse("pins not numbered net by net");
-  }
-  for (size_t p = 0; p < np; p++) {
-    const GPin &q = P.gpins[p];
-    int64_t dv = q.gcell >= 0 ? P.dev_of_gcell[q.gcell] : -1;
-    if (dv >= 0) {
-      s.pin_cell[p] = (int32_t)dv;
-      s.pin_base[2 * p] = q.off_x;
-      s.pin_base[2 * p + 1] = q.off_y;
-    } else {
-      s.pin_base[2 * p] = q.cx;
-      s.pin_base[2 * p + 1] = q.cy;
+  for (size_t q = 0; q < P.net_pins.items.size(); q++)
+    if (P.net_pins.items[q] != (int)q) refuse("pins not numbered net by net");
+  parallel_for(np, [&](size_t a, size_t b) {
+    for (size_t p = a; p < b; p++) {
+      const GPin &q = P.gpins[p];
+      int64_t dv = q.gcell >= 0 ? P.dev_of_gcell[q.gcell] : -1;
+      if (dv >= 0) {
+        s.pin_cell[p] = (int32_t)dv;
+        s.pin_base[2 * p] = q.off_x;
+        s.pin_base[2 * p + 1] = q.off_y;
+      } else {
+        s.pin_base[2 * p] = q.cx;
+        s.pin_base[2 * p + 1] = q.cy;
+      }
     }
-  }
+  });
   s.net_weight.assign(P.net_pins.size(), 1.0f);
   progress("  device set-up: cells and pins");
   for (auto &nb : P.nbs) s.regions.push_back(region_setup(nb));
@@ -2425,7 +2439,7 @@ int gpl_session_set_option(gpl_session *s, const char *name, const char *value) 
     s->ctx->eng->set_profile(v == "1");
     return 0;
   }
-  if (n == "overlap") {  // the WA beside the density solve (1, the default) or after it (0)
+  if (n == "overlap") {  // the WA beside the density solve (1) or after it (0, the default)
     s->ctx->eng->set_overlap(v != "0");
     return 0;
   }

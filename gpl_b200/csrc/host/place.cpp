@@ -13,6 +13,7 @@
 #include <tuple>
 
 #include "host.h"
+#include "parallel.h"
 #include "../kernels/b2b.h"
 
 namespace gpl {
@@ -603,64 +604,71 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
   for (size_t k = 0; k < c.insts.size(); k++)
     if (c.insts[k].db >= 0) inst_map[c.insts[k].db] = (int)k;
   Ip ip;
-  ip.db_bbox.reserve(d.insts.size());
-  for (auto &i : d.insts) ip.db_bbox.push_back(i.bbox);
-  // sized up front: the pins, each net's list, each instance's list
-  size_t total = 0;
+  ip.db_bbox.resize(d.insts.size());
+  parallel_for(d.insts.size(), [&](size_t a, size_t b) {
+    for (size_t i = a; i < b; i++) ip.db_bbox[i] = d.insts[i].bbox;
+  });
+  // sized up front: pins are made net by net, so net n's pins are the run of pin numbers
+  // from its start; each instance's list is counted first
+  const size_t nn = c.nets.size();
+  ip.net_pins.start.assign(nn + 1, 0);
   ip.inst_pins.start.assign(c.insts.size() + 1, 0);
-  ip.net_pins.start.reserve(c.nets.size() + 1);
-  for (auto &[net, cnt] : c.nets) {
-    const DbNet &n = d.nets[net];
-    total += n.iterms.size() + (v.skip_io ? 0 : n.bterms.size());
-    ip.net_pins.start.push_back((int64_t)total);
-    for (auto &t : n.iterms)
+  for (size_t n = 0; n < nn; n++) {
+    const DbNet &dn = d.nets[c.nets[n].first];
+    ip.net_pins.start[n + 1] = ip.net_pins.start[n] + (int64_t)(dn.iterms.size() + (v.skip_io ? 0 : dn.bterms.size()));
+    for (auto &t : dn.iterms)
       if (inst_map[t.inst] >= 0) ip.inst_pins.start[inst_map[t.inst] + 1]++;
   }
+  const size_t total = (size_t)ip.net_pins.start[nn];
   for (size_t k = 0; k < c.insts.size(); k++) ip.inst_pins.start[k + 1] += ip.inst_pins.start[k];
-  ip.inst_pins.items.resize((size_t)ip.inst_pins.start.back());
-  std::vector<int64_t> fill(ip.inst_pins.start.begin(), ip.inst_pins.start.end() - 1);
-  // pins are made net by net, so net n's list is the run of pin numbers from its start
   ip.net_pins.items.resize(total);
-  for (size_t q = 0; q < total; q++) ip.net_pins.items[q] = (int)q;
   ip.pins.resize(total);
-  size_t pk = 0;
-  for (auto &[net, cnt] : c.nets) {
-    const DbNet &n = d.nets[net];
-    for (auto &t : n.iterms) {
-      auto p4 = iterm_pin(d, t.inst, t);
-      int k = inst_map[t.inst];
-      if (k >= 0) ip.inst_pins.items[fill[k]++] = (int)pk;
-      Pin &p = ip.pins[pk++];
-      p.inst = k;
-      p.off_x = p4[0];
-      p.off_y = p4[1];
-      p.cx = p4[2];
-      p.cy = p4[3];
-    }
-    if (!v.skip_io) {
-      for (auto &pt : n.bterms) {
-        Rect b = pt.has_bbox ? pt.bbox : Rect{};
-        Pin &p = ip.pins[pk++];
-        p.port = true;
-        p.movable_io = v.place_ios && !pt.fixed;
-        p.cx = (b.lx + b.ux) / 2;
-        p.cy = (b.ly + b.uy) / 2;
+  std::vector<int> order(total, 0);
+  parallel_for(nn, [&](size_t a, size_t b) {
+    for (size_t n = a; n < b; n++) {
+      const DbNet &dn = d.nets[c.nets[n].first];
+      int64_t pk = ip.net_pins.start[n];
+      for (auto &t : dn.iterms) {
+        auto p4 = iterm_pin(d, t.inst, t);
+        Pin &p = ip.pins[pk];
+        p.inst = inst_map[t.inst];
+        p.off_x = p4[0];
+        p.off_y = p4[1];
+        p.cx = p4[2];
+        p.cy = p4[3];
+        order[pk] = t.order;
+        ip.net_pins.items[pk] = (int)pk;
+        pk++;
+      }
+      if (!v.skip_io) {
+        for (auto &pt : dn.bterms) {
+          Rect r = pt.has_bbox ? pt.bbox : Rect{};
+          Pin &p = ip.pins[pk];
+          p.port = true;
+          p.movable_io = v.place_ios && !pt.fixed;
+          p.cx = (r.lx + r.ux) / 2;
+          p.cy = (r.ly + r.uy) / 2;
+          ip.net_pins.items[pk] = (int)pk;
+          pk++;
+        }
       }
     }
+  });
+  // each instance's pins in net order, then in its iterms' order (the reference walks an
+  // instance's iterms)
+  ip.inst_pins.items.resize((size_t)ip.inst_pins.start.back());
+  std::vector<int64_t> fill(ip.inst_pins.start.begin(), ip.inst_pins.start.end() - 1);
+  for (size_t q = 0; q < total; q++) {
+    int k = ip.pins[q].inst;
+    if (k >= 0 && !ip.pins[q].port) ip.inst_pins.items[fill[k]++] = (int)q;
   }
-  // each instance's pins in its iterms' order (the reference walks an instance's iterms)
-  std::vector<int> order(total, 0);
-  size_t k = 0;
-  for (auto &[net, cnt] : c.nets) {
-    const DbNet &n = d.nets[net];
-    for (auto &t : n.iterms) order[k++] = t.order;
-    if (!v.skip_io) k += n.bterms.size();
-  }
-  auto by_order = [&](int a, int b) { return order[a] < order[b]; };
-  for (size_t q = 0; q < c.insts.size(); q++) {
-    int *b = ip.inst_pins.begin_of(q), *e = ip.inst_pins.end_of(q);
-    if (!std::is_sorted(b, e, by_order)) std::stable_sort(b, e, by_order);
-  }
+  auto by_order = [&](int x, int y) { return order[x] < order[y]; };
+  parallel_for(c.insts.size(), [&](size_t a, size_t b) {
+    for (size_t q = a; q < b; q++) {
+      int *lo = ip.inst_pins.begin_of(q), *hi = ip.inst_pins.end_of(q);
+      if (!std::is_sorted(lo, hi, by_order)) std::stable_sort(lo, hi, by_order);
+    }
+  });
   for (size_t q = 0; q < c.insts.size(); q++)
     if (!c.insts[q].fixed) ip.place.push_back((int)q);
   return ip;
@@ -748,69 +756,75 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
   std::vector<int32_t> ext(c.insts.size(), -1);
   for (size_t e = 0; e < n; e++) ext[ip.place[e]] = (int32_t)e;
   s.core = make_int4(d.core.lx, d.core.ly, d.core.ux, d.core.uy);
-  s.box.reserve(n);
-  s.locked.reserve(n);
-  s.grouped.reserve(n);
-  s.clamp.reserve(n);
-  s.db_box.reserve(n);
-  s.db_size.reserve(n);
-  const size_t np = ip.pins.size();
-  s.pin_e.reserve(np);
-  s.pin_inst.reserve(np);
-  s.pin_mio.reserve(np);
-  s.pin_off.reserve(np);
-  s.pin_xy.reserve(np);
-  s.pin_hp.reserve(np);
-  s.pin_static.reserve(np);
-  s.net_start.reserve(c.nets.size() + 1);
-  for (size_t e = 0; e < n; e++) {
-    const Instance &i = c.insts[ip.place[e]];
-    s.box.push_back(make_int4(i.lx, i.ly, i.ux, i.uy));
-    s.locked.push_back(i.locked ? 1 : 0);
-    int g = d.insts[i.db].group;
-    bool grouped = g >= 0 && d.groups[g].region >= 0;
-    Rect r = grouped ? region_box_of(d, d.groups[g].region) : Rect{};
-    s.grouped.push_back(grouped ? 1 : 0);
-    s.clamp.push_back(make_int4(r.lx, r.ly, r.ux, r.uy));
-    Rect b = ip.db_bbox[i.db];
-    s.db_box.push_back(make_int4(b.lx, b.ly, b.ux, b.uy));
-    s.db_size.push_back(make_int2(b.dx(), b.dy()));
-  }
+  s.box.resize(n);
+  s.locked.resize(n);
+  s.grouped.resize(n);
+  s.clamp.resize(n);
+  s.db_box.resize(n);
+  s.db_size.resize(n);
+  parallel_for(n, [&](size_t a, size_t b) {
+    for (size_t e = a; e < b; e++) {
+      const Instance &i = c.insts[ip.place[e]];
+      s.box[e] = make_int4(i.lx, i.ly, i.ux, i.uy);
+      s.locked[e] = i.locked ? 1 : 0;
+      int g = d.insts[i.db].group;
+      bool grouped = g >= 0 && d.groups[g].region >= 0;
+      Rect r = grouped ? region_box_of(d, d.groups[g].region) : Rect{};
+      s.grouped[e] = grouped ? 1 : 0;
+      s.clamp[e] = make_int4(r.lx, r.ly, r.ux, r.uy);
+      Rect bb = ip.db_bbox[i.db];
+      s.db_box[e] = make_int4(bb.lx, bb.ly, bb.ux, bb.uy);
+      s.db_size[e] = make_int2(bb.dx(), bb.dy());
+    }
+  });
   std::vector<int> inst_map(d.insts.size(), -1);
   for (size_t k = 0; k < c.insts.size(); k++)
     if (c.insts[k].db >= 0) inst_map[c.insts[k].db] = (int)k;
-  s.net_start.push_back(0);
-  size_t pk = 0;
-  for (auto &[net, cnt] : c.nets) {
-    const DbNet &dn = d.nets[net];
-    for (auto &t : dn.iterms) {
-      const Pin &p = ip.pins[pk++];
-      int k = inst_map[t.inst];
-      bool placed = p.inst >= 0 && !c.insts[p.inst].fixed;
-      s.pin_e.push_back(placed ? ext[p.inst] : -1);
-      s.pin_inst.push_back(p.inst);
-      s.pin_mio.push_back(p.movable_io ? 1 : 0);
-      s.pin_off.push_back(make_int2(p.off_x, p.off_y));
-      s.pin_xy.push_back(make_int2(p.cx, p.cy));
-      bool dynamic = k >= 0 && !c.insts[k].fixed;
-      Rect b = ip.db_bbox[t.inst];
-      s.pin_hp.push_back(dynamic ? 0 : 1);
-      s.pin_static.push_back(make_int4(b.lx, b.ly, b.ux, b.uy));
-    }
-    if (!v.skip_io)
-      for (auto &pt : dn.bterms) {
-        const Pin &p = ip.pins[pk++];
-        s.pin_e.push_back(-1);
-        s.pin_inst.push_back(p.inst);
-        s.pin_mio.push_back(p.movable_io ? 1 : 0);
-        s.pin_off.push_back(make_int2(p.off_x, p.off_y));
-        s.pin_xy.push_back(make_int2(p.cx, p.cy));
-        s.pin_hp.push_back(pt.has_bbox ? 1 : 2);
-        s.pin_static.push_back(make_int4(pt.bbox.lx, pt.bbox.ly, pt.bbox.ux, pt.bbox.uy));
+  // pins net by net, as make_pins numbered them (net n's run starts at net_pins.start[n])
+  const size_t np = ip.pins.size(), nn = c.nets.size();
+  if (ip.net_pins.size() != nn || (size_t)ip.net_pins.start[nn] != np) throw std::runtime_error("initial placement: pin order mismatch");
+  s.pin_e.resize(np);
+  s.pin_inst.resize(np);
+  s.pin_mio.resize(np);
+  s.pin_off.resize(np);
+  s.pin_xy.resize(np);
+  s.pin_hp.resize(np);
+  s.pin_static.resize(np);
+  s.net_start.assign(ip.net_pins.start.begin(), ip.net_pins.start.end());
+  parallel_for(nn, [&](size_t a, size_t b) {
+    for (size_t ni = a; ni < b; ni++) {
+      const DbNet &dn = d.nets[c.nets[ni].first];
+      size_t pk = (size_t)ip.net_pins.start[ni];
+      for (auto &t : dn.iterms) {
+        const Pin &p = ip.pins[pk];
+        int k = inst_map[t.inst];
+        bool placed = p.inst >= 0 && !c.insts[p.inst].fixed;
+        s.pin_e[pk] = placed ? ext[p.inst] : -1;
+        s.pin_inst[pk] = p.inst;
+        s.pin_mio[pk] = p.movable_io ? 1 : 0;
+        s.pin_off[pk] = make_int2(p.off_x, p.off_y);
+        s.pin_xy[pk] = make_int2(p.cx, p.cy);
+        bool dynamic = k >= 0 && !c.insts[k].fixed;
+        Rect bb = ip.db_bbox[t.inst];
+        s.pin_hp[pk] = dynamic ? 0 : 1;
+        s.pin_static[pk] = make_int4(bb.lx, bb.ly, bb.ux, bb.uy);
+        pk++;
       }
-    s.net_start.push_back((int64_t)pk);
-  }
-  if (pk != ip.pins.size()) throw std::runtime_error("initial placement: pin order mismatch");
+      if (!v.skip_io)
+        for (auto &pt : dn.bterms) {
+          const Pin &p = ip.pins[pk];
+          s.pin_e[pk] = -1;
+          s.pin_inst[pk] = p.inst;
+          s.pin_mio[pk] = p.movable_io ? 1 : 0;
+          s.pin_off[pk] = make_int2(p.off_x, p.off_y);
+          s.pin_xy[pk] = make_int2(p.cx, p.cy);
+          s.pin_hp[pk] = pt.has_bbox ? 1 : 2;
+          s.pin_static[pk] = make_int4(pt.bbox.lx, pt.bbox.ly, pt.bbox.ux, pt.bbox.uy);
+          pk++;
+        }
+    }
+  });
+
   progress("initial placement set up on the host");
   s.max_fanout = vars.max_fanout;
   s.min_diff = vars.min_diff_length;

@@ -221,45 +221,198 @@ __global__ void k_bucket(int64_t nt, const int32_t *row, const int32_t *col, con
   bucket[at] = ((unsigned long long)c << 32) | (unsigned long long)(uint32_t)t;
 }
 
-// Per row: keys sorted (column, then position; Shell's sort, the keys are distinct), each
-// column's run summed in position order (the first value, then the rest added to it), the
-// distinct columns compacted.
-__global__ void k_row_collapse(int64_t n, const int64_t *row_off, unsigned long long *bucket, const float *val, int32_t *ucol, float *uval, int64_t *ucount) {
-  int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  const int64_t b = row_off[r], e = row_off[r + 1], m = e - b;
-  unsigned long long *k = bucket + b;
-  const int gaps[] = {1750, 701, 301, 132, 57, 23, 10, 4, 1};
-  for (int gi = 0; gi < 9; gi++) {
-    const int64_t g = gaps[gi];
-    if (g >= m) continue;
-    for (int64_t i = g; i < m; i++) {
-      unsigned long long v = k[i];
-      int64_t j = i;
-      while (j >= g && v < k[j - g]) {
-        k[j] = k[j - g];
-        j -= g;
+// Per row: keys sorted (column, then position; the keys are distinct), each column's run
+// summed in position order (the first value, then the rest added to it), the distinct columns
+// compacted. Tiers by the row's length: a warp per row with its keys in registers (R per
+// lane, bitonic-sorted across the warp) for rows of up to 64 and then 256 keys; a block per
+// row (bitonic sort in shared memory) up to 8192; a thread per row (Shell's sort in place)
+// beyond. Every tier gives the same result.
+constexpr int kRowShort = 64, kRowMid = 256;
+
+// One column's run [p, end) of a sorted row summed in position order: the first value, then
+// the rest added to it; the values' loads go four at a time ahead of the adds.
+__device__ __forceinline__ float run_sum(const unsigned long long *sk, int p, int end, const float *val) {
+  float s = val[(uint32_t)sk[p]];
+  int q = p + 1;
+  for (; q + 4 <= end; q += 4) {
+    float t0 = val[(uint32_t)sk[q]], t1 = val[(uint32_t)sk[q + 1]], t2 = val[(uint32_t)sk[q + 2]], t3 = val[(uint32_t)sk[q + 3]];
+    s = __fadd_rn(s, t0);
+    s = __fadd_rn(s, t1);
+    s = __fadd_rn(s, t2);
+    s = __fadd_rn(s, t3);
+  }
+  for (; q < end; q++) s = __fadd_rn(s, val[(uint32_t)sk[q]]);
+  return s;
+}
+
+// Sums and compacts a sorted row held in shared memory (sk: m keys), a warp's lanes taking
+// the run starts; returns the row's distinct columns.
+__device__ __forceinline__ int64_t warp_runs(const unsigned long long *sk, int m, int64_t b, const float *val, int32_t *ucol, float *uval) {
+  const int lane = threadIdx.x & 31;
+  int64_t base = 0;
+  for (int p0 = 0; p0 < m; p0 += 32) {
+    int p = p0 + lane;
+    bool start = p < m && (p == 0 || (uint32_t)(sk[p] >> 32) != (uint32_t)(sk[p - 1] >> 32));
+    unsigned mask = __ballot_sync(0xffffffffu, start);
+    if (start) {
+      unsigned long long key = sk[p];
+      uint32_t c = (uint32_t)(key >> 32);
+      int end = p + 1;
+      while (end < m && (uint32_t)(sk[end] >> 32) == c) end++;
+      float s = run_sum(sk, p, end, val);
+      int64_t u = base + __popc(mask & ((1u << lane) - 1u));
+      ucol[b + u] = (int32_t)c;
+      uval[b + u] = s;
+    }
+    base += __popc(mask);
+  }
+  return base;
+}
+
+// A warp per row of at most 32 R keys: element i = j * 32 + lane lives in register j.
+template <int R>
+__device__ __forceinline__ void warp_bitonic(unsigned long long (&v)[R]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 2; k <= 32 * R; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const int jr = j >> 5;
+#pragma unroll
+        for (int a = 0; a < R; a++) {
+          const int bb = a ^ jr;
+          if (bb > a) {
+            const int i = a * 32 + lane;
+            const bool up = (i & k) == 0;
+            unsigned long long x = v[a], y = v[bb];
+            bool sw = up ? (x > y) : (x < y);
+            v[a] = sw ? y : x;
+            v[bb] = sw ? x : y;
+          }
+        }
+      } else {
+#pragma unroll
+        for (int a = 0; a < R; a++) {
+          const int i = a * 32 + lane;
+          const bool up = (i & k) == 0, lower = (lane & j) == 0;
+          unsigned long long o = __shfl_xor_sync(0xffffffffu, v[a], j);
+          unsigned long long mn = v[a] < o ? v[a] : o, mx = v[a] < o ? o : v[a];
+          v[a] = (lower == up) ? mn : mx;
+        }
       }
-      k[j] = v;
     }
   }
-  int64_t u = 0, i = 0;
-  while (i < m) {
-    unsigned long long key = k[i];
-    uint32_t c = (uint32_t)(key >> 32);
-    float s = val[(uint32_t)key];
-    int64_t j = i + 1;
-    for (; j < m; j++) {
-      unsigned long long k2 = k[j];
-      if ((uint32_t)(k2 >> 32) != c) break;
-      s = __fadd_rn(s, val[(uint32_t)k2]);
+}
+
+// Rows of up to 32 R keys, a warp each: rows [0, n) when `list` is null, else the `*count`
+// rows of `list`; longer rows go to `next` (with `next_count`) for the next tier.
+template <int R>
+__global__ void __launch_bounds__(kThreads) k_row_collapse_warp(int64_t n, const int32_t *list, const int *count, const int64_t *row_off, const unsigned long long *bucket, const float *val, int32_t *ucol, float *uval, int64_t *ucount, int32_t *next, int *next_count) {
+  __shared__ unsigned long long sk[kThreads / 32][32 * R];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int64_t total = list ? (int64_t)*count : n;
+  const int64_t warps = (int64_t)gridDim.x * (kThreads / 32);
+  for (int64_t w = blockIdx.x * (int64_t)(kThreads / 32) + wib; w < total; w += warps) {
+    const int64_t r = list ? (int64_t)list[w] : w;
+    const int64_t b = row_off[r], e = row_off[r + 1];
+    const int64_t m = e - b;
+    if (m > 32 * R) {
+      if (lane == 0) next[atomicAdd(next_count, 1)] = (int32_t)r;
+      continue;
     }
-    ucol[b + u] = (int32_t)c;
-    uval[b + u] = s;
-    u++;
-    i = j;
+    unsigned long long v[R];
+#pragma unroll
+    for (int a = 0; a < R; a++) {
+      const int i = a * 32 + lane;
+      v[a] = i < m ? bucket[b + i] : ~0ull;
+    }
+    warp_bitonic<R>(v);
+#pragma unroll
+    for (int a = 0; a < R; a++) sk[wib][a * 32 + lane] = v[a];
+    __syncwarp();
+    int64_t u = warp_runs(sk[wib], (int)m, b, val, ucol, uval);
+    if (lane == 0) ucount[r] = u;
+    __syncwarp();
   }
-  ucount[r] = u;
+}
+
+// Rows of up to kRowLong keys, a block each: the keys bitonic-sorted in shared memory
+// (padded to a power of two), then one warp walks the runs. Longer rows go to `next`.
+constexpr int kRowLong = 8192;
+__global__ void __launch_bounds__(kThreads) k_row_collapse_block(const int32_t *list, const int *count, const int64_t *row_off, const unsigned long long *bucket, const float *val, int32_t *ucol, float *uval, int64_t *ucount, int32_t *next, int *next_count) {
+  extern __shared__ unsigned long long skb[];
+  const int64_t total = *count;
+  for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
+    const int64_t r = list[w];
+    const int64_t b = row_off[r], e = row_off[r + 1];
+    const int64_t m = e - b;
+    if (m > kRowLong) {
+      if (threadIdx.x == 0) next[atomicAdd(next_count, 1)] = (int32_t)r;
+      continue;
+    }
+    int N = 1;
+    while (N < m) N <<= 1;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) skb[i] = i < m ? bucket[b + i] : ~0ull;
+    __syncthreads();
+    for (int k = 2; k <= N; k <<= 1)
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int i = threadIdx.x; i < N; i += blockDim.x) {
+          const int o = i ^ j;
+          if (o > i) {
+            const bool up = (i & k) == 0;
+            unsigned long long x = skb[i], y = skb[o];
+            if (up ? (x > y) : (x < y)) {
+              skb[i] = y;
+              skb[o] = x;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    if (threadIdx.x < 32) {
+      int64_t u = warp_runs(skb, (int)m, b, val, ucol, uval);
+      if (threadIdx.x == 0) ucount[r] = u;
+    }
+    __syncthreads();
+  }
+}
+
+// The longest rows, a thread each: Shell's sort in place, then the runs.
+__global__ void k_row_collapse_long(const int32_t *list, const int *count, const int64_t *row_off, unsigned long long *bucket, const float *val, int32_t *ucol, float *uval, int64_t *ucount) {
+  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < *count; w += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = list[w];
+    const int64_t b = row_off[r], e = row_off[r + 1], m = e - b;
+    unsigned long long *k = bucket + b;
+    const int gaps[] = {1750, 701, 301, 132, 57, 23, 10, 4, 1};
+    for (int gi = 0; gi < 9; gi++) {
+      const int64_t g = gaps[gi];
+      if (g >= m) continue;
+      for (int64_t i = g; i < m; i++) {
+        unsigned long long v = k[i];
+        int64_t j = i;
+        while (j >= g && v < k[j - g]) {
+          k[j] = k[j - g];
+          j -= g;
+        }
+        k[j] = v;
+      }
+    }
+    int64_t u = 0, i = 0;
+    while (i < m) {
+      unsigned long long key = k[i];
+      uint32_t c = (uint32_t)(key >> 32);
+      int64_t j = i + 1;
+      while (j < m && (uint32_t)(k[j] >> 32) == c) j++;
+      float s = val[(uint32_t)key];
+      for (int64_t q = i + 1; q < j; q++) s = __fadd_rn(s, val[(uint32_t)k[q]]);
+      ucol[b + u] = (int32_t)c;
+      uval[b + u] = s;
+      u++;
+      i = j;
+    }
+    ucount[r] = u;
+  }
 }
 
 __global__ void k_row_fill(int64_t n, const int64_t *row_off, const int64_t *starts, const int32_t *ucol, const float *uval, int32_t *cols, float *vals) {
@@ -442,7 +595,7 @@ IpDevice::~IpDevice() { release(); }
 
 void IpDevice::release() {
   void *ptrs[] = {box_, clamp_, db_box_, pin_static_, db_size_, pin_off_, pin_xy_, locked_, grouped_, pin_mio_, pin_hp_, pin_flag_, pin_e_, pin_inst_, locked_rank_,
-                  net_start_, cnt_, scan_tmp_, t_row_, t_col_, t_val_, r_row_, r_val_, bucket_, fill_, row_off_, ucount_, ucol_, uval_, scratch_, hpwl_acc_};
+                  net_start_, cnt_, scan_tmp_, t_row_, t_col_, t_val_, r_row_, r_val_, bucket_, fill_, row_off_, ucount_, ucol_, uval_, scratch_, hpwl_acc_, tier_rows_, tier_n_};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto &a : ax_) {
@@ -461,6 +614,8 @@ void IpDevice::release() {
   bucket_ = nullptr;
   scratch_ = nullptr;
   hpwl_acc_ = nullptr;
+  tier_rows_ = nullptr;
+  tier_n_ = nullptr;
   t_cap_ = r_cap_ = w_cap_ = scan_tmp_n_ = 0;
 }
 
@@ -497,6 +652,9 @@ cudaError_t IpDevice::upload(const IpSetup &s) {
   CK(alloc(&cnt_, 4 * ((size_t)n_nets_ + 1)));
   CK(alloc(&row_off_, n_ + 1));
   CK(alloc(&ucount_, n_ + 1));
+  CK(cudaFuncSetAttribute(k_row_collapse_block, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
+  CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1)));
+  CK(alloc(&tier_n_, 3));
   CK(alloc(&fill_, n_));
   CK(alloc(&hpwl_acc_, 1));
   for (auto &a : ax_) {
@@ -532,8 +690,18 @@ cudaError_t IpDevice::collapse(int64_t n_trip, const int32_t *row, const int32_t
   if (n_trip) k_row_count<<<grid(n_trip), kThreads, 0, s_>>>(n_trip, row, (unsigned long long *)row_off_);
   CK(scan(row_off_, n_));
   if (n_trip) k_bucket<<<grid(n_trip), kThreads, 0, s_>>>(n_trip, row, col, row_off_, fill_, bucket_);
-  if (n_) k_row_collapse<<<grid(n_), kThreads, 0, s_>>>(n_, row_off_, bucket_, val, ucol_, uval_, ucount_);
-  launches += 3;
+  if (n_) {
+    // tiers: a warp per row up to 64 keys, then up to 256, a block per row up to 8192, then
+    // a thread per row
+    CK(cudaMemsetAsync(tier_n_, 0, 3 * sizeof(int), s_));
+    const int wblocks = (int)std::min<int64_t>((n_ + kThreads / 32 - 1) / (kThreads / 32), 148 * 64);
+    k_row_collapse_warp<kRowShort / 32><<<wblocks, kThreads, 0, s_>>>(n_, nullptr, nullptr, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_, tier_n_);
+    k_row_collapse_warp<kRowMid / 32><<<148 * 4, kThreads, 0, s_>>>(n_, tier_rows_, tier_n_, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_ + n_, tier_n_ + 1);
+    k_row_collapse_block<<<148 * 2, kThreads, kRowLong * sizeof(unsigned long long), s_>>>(tier_rows_ + n_, tier_n_ + 1, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_ + 2 * n_, tier_n_ + 2);
+    k_row_collapse_long<<<148, kThreads, 0, s_>>>(tier_rows_ + 2 * n_, tier_n_ + 2, row_off_, bucket_, val, ucol_, uval_, ucount_);
+    launches += 4;
+  }
+  launches += 2;
   if (!cols) return cudaGetLastError();
   CK(cudaMemcpyAsync(starts_out, ucount_, n_ * sizeof(int64_t), cudaMemcpyDeviceToDevice, s_));
   CK(scan(starts_out, n_));

@@ -82,6 +82,8 @@ class IpDevice {
   unsigned long long *bucket_ = nullptr;  // (column << 32 | position) per triplet, by row
   int32_t *fill_ = nullptr;
   int64_t *row_off_ = nullptr, *ucount_ = nullptr;
+  int32_t *tier_rows_ = nullptr;  // [3][n]: rows handed to the collapse's later tiers
+  int *tier_n_ = nullptr;         // their counts
   int32_t *ucol_ = nullptr;
   float *uval_ = nullptr;
   struct Axis {

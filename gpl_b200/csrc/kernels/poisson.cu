@@ -24,6 +24,7 @@
 #include "common.cuh"
 #include "engine_kernels.h"
 #include "poisson_internal.h"
+#include "parallel.h"
 
 namespace gpl {
 
@@ -131,23 +132,27 @@ void build_basis(int nx, int ny, BasisHost &b) {
   b.CyTs.assign((size_t)ny * ny, 0);
   b.Cy.assign((size_t)ny * ny, 0);
   b.Sy.assign((size_t)ny * ny, 0);
-  for (int v = 0; v < ny; v++)
-    for (int y = 0; y < ny; y++) {
-      double h = (v == 0 ? 0.5 : 1.0) * 2.0 / (double)ny;
-      b.CyTs[(size_t)v * ny + y] = h * cosv(v, y, ny);
-      b.Cy[(size_t)y * ny + v] = cosv(v, y, ny);
-      b.Sy[(size_t)y * ny + v] = sinv(v, y, ny);
-    }
+  parallel_for((size_t)ny, [&](size_t v0, size_t v1) {
+    for (int v = (int)v0; v < (int)v1; v++)
+      for (int y = 0; y < ny; y++) {
+        double h = (v == 0 ? 0.5 : 1.0) * 2.0 / (double)ny;
+        b.CyTs[(size_t)v * ny + y] = h * cosv(v, y, ny);
+        b.Cy[(size_t)y * ny + v] = cosv(v, y, ny);
+        b.Sy[(size_t)y * ny + v] = sinv(v, y, ny);
+      }
+  }, 16);
   b.CxTs.assign((size_t)nx * nx, 0);
   b.Cx.assign((size_t)nx * nx, 0);
   b.Sx.assign((size_t)nx * nx, 0);
-  for (int u = 0; u < nx; u++)
-    for (int x = 0; x < nx; x++) {
-      double h = (u == 0 ? 0.5 : 1.0) * 2.0 / (double)nx;
-      b.CxTs[(size_t)u * nx + x] = h * cosv(u, x, nx);
-      b.Cx[(size_t)x * nx + u] = cosv(u, x, nx);
-      b.Sx[(size_t)x * nx + u] = sinv(u, x, nx);
-    }
+  parallel_for((size_t)nx, [&](size_t u0, size_t u1) {
+    for (int u = (int)u0; u < (int)u1; u++)
+      for (int x = 0; x < nx; x++) {
+        double h = (u == 0 ? 0.5 : 1.0) * 2.0 / (double)nx;
+        b.CxTs[(size_t)u * nx + x] = h * cosv(u, x, nx);
+        b.Cx[(size_t)x * nx + u] = cosv(u, x, nx);
+        b.Sx[(size_t)x * nx + u] = sinv(u, x, nx);
+      }
+  }, 16);
 }
 
 static cudaError_t upload_f32(const std::vector<double> &h, float **d) {

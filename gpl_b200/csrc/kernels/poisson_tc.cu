@@ -33,6 +33,7 @@
 #include "common.cuh"
 #include "engine_kernels.h"
 #include "poisson_internal.h"
+#include "parallel.h"
 
 namespace gpl {
 
@@ -320,13 +321,15 @@ struct TcState {
 
 static cudaError_t upload_split(const std::vector<double> &h, int rows, int k, __nv_bfloat16 **d) {
   std::vector<__nv_bfloat16> v((size_t)rows * 2 * k);
-  for (int r = 0; r < rows; r++)
-    for (int c = 0; c < k; c++) {
-      float x = (float)h[(size_t)r * k + c];
-      __nv_bfloat16 hi = __float2bfloat16_rn(x);
-      v[(size_t)r * 2 * k + c] = hi;
-      v[(size_t)r * 2 * k + k + c] = __float2bfloat16_rn(x - __bfloat162float(hi));
-    }
+  parallel_for((size_t)rows, [&](size_t r0, size_t r1) {
+    for (size_t r = r0; r < r1; r++)
+      for (int c = 0; c < k; c++) {
+        float x = (float)h[r * k + c];
+        __nv_bfloat16 hi = __float2bfloat16_rn(x);
+        v[r * 2 * k + c] = hi;
+        v[r * 2 * k + k + c] = __float2bfloat16_rn(x - __bfloat162float(hi));
+      }
+  }, 16);
   cudaError_t e = cudaMalloc(d, v.size() * sizeof(__nv_bfloat16));
   if (e != cudaSuccess) return e;
   return cudaMemcpy(*d, v.data(), v.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice);

@@ -102,6 +102,24 @@ def test_wa_bit_exact(L, coef):
     np.testing.assert_array_equal(g.cpu().numpy(), want)
 
 
+@pytest.mark.parametrize("coef,offset", [(1e-5, 0), (3e-4, -100000), (4e-3, 0), (2e-2, -7000000)])
+def test_wa_quotients_bit_exact_at_scale(L, coef, offset):
+    """The forces' double quotients at scale: 100k nets, about 2M quotients per case, against
+    the oracle's IEEE division, bit for bit (signed zeros included); coordinates shifted
+    negative in two cases (negative numerators)."""
+    rng = np.random.default_rng(17 + int(coef * 1e6))
+    start, xy, w = random_nets(rng, 100000, span=4000000)
+    xy = (xy.astype(np.int64) + offset).astype(np.int32)
+    want = np.zeros(2 * len(xy), np.float32)
+    oracle.lib().oracle_wa(C.c_int64(len(start) - 1), start.ctypes.data_as(C.c_void_p), xy.ctypes.data_as(C.c_void_p),
+                           w.ctypes.data_as(C.c_void_p), C.c_float(coef), C.c_float(coef * 0.8), want.ctypes.data_as(C.c_void_p))
+    ds, dxy, dw = dev(start), dev(xy), dev(w)
+    g = dev(np.zeros(2 * len(xy), np.float32))
+    assert L.gpl_kernel_wa(len(start) - 1, ptr(ds), ptr(dxy), ptr(dw), coef, coef * 0.8, ptr(g), stream()) == 0
+    sync()
+    np.testing.assert_array_equal(g.cpu().numpy().view(np.uint32), want.view(np.uint32))
+
+
 def _poisson_oracle(nx, ny, bin_x, bin_y, dens):
     O = oracle.lib()
     phi, fx, fy = (np.zeros(nx * ny, np.float32) for _ in range(3))

@@ -195,12 +195,14 @@ def ours(a):
         return {"ms": ms, "iters": done, "wall_s": wall, "clocks": clk.summary(), "launches": c1["launches"] - c0["launches"]}
 
     def phase_times(k):
-        # each phase's own device time: events around each phase's launches (outside the
-        # timed region above)
+        # each phase's own device time: events around each phase's launches, with the WA after
+        # the density solve instead of beside it (outside the timed region above)
+        sess.set_option("overlap", "0")
         sess.set_option("profile", "1")
         sess.iterate(k)
         prof = sess.profile()
         sess.set_option("profile", "0")
+        sess.set_option("overlap", "1")
         return prof
 
     cells_total = sess.counters()["cells"]

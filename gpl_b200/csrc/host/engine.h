@@ -151,14 +151,14 @@ class Engine {
   size_t pinned_bytes_ = 0;
   bool hpwl_fetched_ = false;
   unsigned long long hpwl_host_ = 0;
-  // With overlap on, the WA runs on its own stream beside the density solve (it needs the
-  // centres, not the field) and everything that reads its forces or moves the centres joins
-  // it first. Off by default: both kernels fill every SM, the solve's CTAs (about 200 KB of
-  // shared memory each) wait for WA blocks to drain, and the trial measured slower that way.
+  // With overlap on (the default), the WA runs on its own stream beside the density solve
+  // (it needs the centres, not the field) and everything that reads its forces or moves the
+  // centres joins it first. Both kernels fill every SM, so the gain is small (a few percent
+  // of a trial, measured); off runs them one after the other.
   cudaStream_t wa_stream_ = nullptr;
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   bool wa_pending_ = false;
-  bool overlap_ = false;
+  bool overlap_ = true;
   void join();
   void free_globals();
   WaArgs wa_args() const;

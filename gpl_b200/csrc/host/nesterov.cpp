@@ -2439,7 +2439,7 @@ int gpl_session_set_option(gpl_session *s, const char *name, const char *value) 
     s->ctx->eng->set_profile(v == "1");
     return 0;
   }
-  if (n == "overlap") {  // the WA beside the density solve (1) or after it (0, the default)
+  if (n == "overlap") {  // the WA beside the density solve (1, the default) or after it (0)
     s->ctx->eng->set_overlap(v != "0");
     return 0;
   }

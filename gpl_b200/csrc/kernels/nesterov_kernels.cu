@@ -135,7 +135,13 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
     return;
   }
   const int nt = tw * th;
-  for (int k = threadIdx.x; k < 2 * kTileBins; k += blockDim.x) s_tile[k] = 0;
+  // only the slots this block's bins use: [0, nt) for cells and [kTileBins, kTileBins + nt)
+  // for fillers, in the tile's element width
+  if (narrow) {
+    for (int k = threadIdx.x; k < nt; k += blockDim.x) t32[k] = t32[kTileBins + k] = 0u;
+  } else {
+    for (int k = threadIdx.x; k < nt; k += blockDim.x) s_tile[k] = s_tile[kTileBins + k] = 0ull;
+  }
   __syncthreads();
   // the warp's lanes in step over their bins (x outer, y inner); key = tile slot * 2 + filler
   const int nb = any ? (x1 - x0) * (y1 - y0) : 0;
@@ -449,16 +455,39 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
 // the density force over its bins (x outer, y inner), the preconditioned sum; block partials
 // of |wl|, |density| and the two step-length distances (getDistance :319-330):
 // |a1 - b1|^2 and |out - b2|^2.
+// A block's cells are consecutive, so their pins' forces (cell-major) are one run: staged in
+// shared memory with coalesced loads when the run fits kGradPinTile, then each cell sums its
+// own in order. A cell over at most 2 x 2 bins loads its bins' boundaries and fields before
+// the ordered sums; larger cells walk their bins.
+constexpr int kGradPinTile = 2048;
+
 __global__ void __launch_bounds__(kThreads, 5) k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials) {
   __shared__ double4 sh[kThreads / 32];
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ float2 s_pg[kGradPinTile];
+  const int i0 = blockIdx.x * blockDim.x;
+  const int i = i0 + threadIdx.x;
+  const int i1 = min(r.n_cells, i0 + (int)blockDim.x);
+  const int64_t p0 = c.pin_start[i0], p1 = c.pin_start[i1];
+  const bool staged = p1 - p0 <= kGradPinTile;
+  if (staged)
+    for (int k = threadIdx.x; k < (int)(p1 - p0); k += blockDim.x) s_pg[k] = pin_grad[p0 + k];
+  __syncthreads();
   double s_wl = 0, s_den = 0, s_d1 = 0, s_d2 = 0;
   if (i < r.n_cells) {
+    const int64_t pb = c.pin_start[i], pe = c.pin_start[i + 1];
     float wlx = 0.0f, wly = 0.0f;
-    for (int64_t k = c.pin_start[i]; k < c.pin_start[i + 1]; k++) {
-      float2 t = pin_grad[k];
-      wlx = __fadd_rn(wlx, t.x);
-      wly = __fadd_rn(wly, t.y);
+    if (staged) {
+      for (int k = (int)(pb - p0); k < (int)(pe - p0); k++) {
+        float2 t = s_pg[k];
+        wlx = __fadd_rn(wlx, t.x);
+        wly = __fadd_rn(wly, t.y);
+      }
+    } else {
+      for (int64_t k = pb; k < pe; k++) {
+        float2 t = pin_grad[k];
+        wlx = __fadd_rn(wlx, t.x);
+        wly = __fadd_rn(wly, t.y);
+      }
     }
     int2 d = c.dc[i];
     int32_t cx = d.x, cy = d.y, hx = c.hx[i], hy = c.hy[i];
@@ -468,23 +497,43 @@ __global__ void __launch_bounds__(kThreads, 5) k_gradients(RegionArgs r, CellArg
     bin_span(dly, duy, r.ly, r.size_y, r.inv_size_y, r.ny, y0, y1);
     float scale = c.dscale[i];
     float fx = 0.0f, fy = 0.0f;
-    for (int32_t x = x0; x < x1; x++) {
-      int32_t blx = r.bx[x], bux = r.bx[x + 1];
+    // one bin's term in the reference's order: overlap area (float), times the scale, times
+    // the field, added to the running sums
+    auto term = [&](int32_t blx, int32_t bux, int32_t bly, int32_t buy, float ex, float ey) {
       int32_t olx = dlx > blx ? dlx : blx, oux = dux < bux ? dux : bux;
-      for (int32_t y = y0; y < y1; y++) {
-        int32_t bly = r.by[y], buy = r.by[y + 1];
-        int32_t oly = dly > bly ? dly : bly, ouy = duy < buy ? duy : buy;
-        float a = 0.0f;
-        if (olx < oux && oly < ouy) a = __fmul_rn((float)(oux - olx), (float)(ouy - oly));
-        a = __fmul_rn(a, scale);
-        size_t k = (size_t)x * r.ny + y;
-        fx = __fadd_rn(fx, __fmul_rn(a, r.field_x[k]));
-        fy = __fadd_rn(fy, __fmul_rn(a, r.field_y[k]));
+      int32_t oly = dly > bly ? dly : bly, ouy = duy < buy ? duy : buy;
+      float a = 0.0f;
+      if (olx < oux && oly < ouy) a = __fmul_rn((float)(oux - olx), (float)(ouy - oly));
+      a = __fmul_rn(a, scale);
+      fx = __fadd_rn(fx, __fmul_rn(a, ex));
+      fy = __fadd_rn(fy, __fmul_rn(a, ey));
+    };
+    if (x1 - x0 <= 2 && y1 - y0 <= 2 && x1 > x0 && y1 > y0) {
+      // every load first (the boundaries and up to four bins' fields), then the sums in order
+      const int xb = min(x0 + 1, x1 - 1), yb = min(y0 + 1, y1 - 1);
+      const int32_t bx0 = r.bx[x0], bx1 = r.bx[x0 + 1], bx2 = r.bx[xb + 1];
+      const int32_t by0 = r.by[y0], by1 = r.by[y0 + 1], by2 = r.by[yb + 1];
+      const size_t k00 = (size_t)x0 * r.ny + y0, k01 = (size_t)x0 * r.ny + yb, k10 = (size_t)xb * r.ny + y0, k11 = (size_t)xb * r.ny + yb;
+      const float e00x = r.field_x[k00], e00y = r.field_y[k00], e01x = r.field_x[k01], e01y = r.field_y[k01];
+      const float e10x = r.field_x[k10], e10y = r.field_y[k10], e11x = r.field_x[k11], e11y = r.field_y[k11];
+      term(bx0, bx1, by0, by1, e00x, e00y);
+      if (y1 - y0 == 2) term(bx0, bx1, by1, by2, e01x, e01y);
+      if (x1 - x0 == 2) {
+        term(bx1, bx2, by0, by1, e10x, e10y);
+        if (y1 - y0 == 2) term(bx1, bx2, by1, by2, e11x, e11y);
+      }
+    } else {
+      for (int32_t x = x0; x < x1; x++) {
+        int32_t blx = r.bx[x], bux = r.bx[x + 1];
+        for (int32_t y = y0; y < y1; y++) {
+          size_t k = (size_t)x * r.ny + y;
+          term(blx, bux, r.by[y], r.by[y + 1], r.field_x[k], r.field_y[k]);
+        }
       }
     }
     float sx = __fadd_rn(wlx, __fmul_rn(penalty, fx));
     float sy = __fadd_rn(wly, __fmul_rn(penalty, fy));
-    float wl_pre = (float)(c.pin_start[i + 1] - c.pin_start[i]);
+    float wl_pre = (float)(pe - pb);
     float pre = fmaxf(__fadd_rn(wl_pre, __fmul_rn(penalty, c.area[i])), 1.0f);
     sx = __fdiv_rn(sx, pre);
     sy = __fdiv_rn(sy, pre);

@@ -24,6 +24,7 @@ struct Engine::Region {
   int64_t cell_off = 0, n_cells = 0;
   PoissonPlan *plan = nullptr;
   double *part = nullptr;
+  unsigned int *ticket = nullptr;  // arrivals of the finalize's and the gradients' blocks
   int nb_bins = 0, nb_cells = 0;
   __nv_bfloat16 *dens_split = nullptr;
   int split_ld = 0;
@@ -118,7 +119,7 @@ void Engine::free_globals() {
 void Engine::release() {
   join();
   for (Region *r : regions_) {
-    void *ptrs[] = {r->bx, r->by, r->scaled, r->density, r->fx, r->fy, r->np, r->npu, r->acc_inst, r->acc_fill, r->part};
+    void *ptrs[] = {r->bx, r->by, r->scaled, r->density, r->fx, r->fy, r->np, r->npu, r->acc_inst, r->acc_fill, r->part, r->ticket};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     for (int k = 0; k < S_NUM; k++)
@@ -254,6 +255,8 @@ void Engine::upload(const EngineSetup &s) {
     r->nb_bins = rs.nx;  // the bin finalize runs one block per x row
     r->nb_cells = blocks_for(rs.n_cells);
     check(dmalloc(&r->part, (size_t)std::max(r->nb_bins * 2, r->nb_cells * 4)), "alloc partials");
+    check(dmalloc(&r->ticket, 1), "alloc partials");
+    if (!failed()) check(cudaMemsetAsync(r->ticket, 0, sizeof(unsigned int), st), "memset");
     if (!failed()) {
       cudaError_t pe = cudaSuccess;
       r->plan = poisson_plan_create(rs.nx, rs.ny, rs.wx.data(), rs.wy.data(), poisson_mode_, &pe);
@@ -367,12 +370,11 @@ void Engine::place_at(int b, SlotId slot) {
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
   ph_begin(PH_PLACE);
-  launches += (r->n_cells ? 1 : 0) + 2;
+  launches += (r->n_cells ? 1 : 0) + 1;
   if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, c, PLACE_AT, 0.0f, 0.0f, r->slot[slot]);
   ph_end(PH_PLACE);
   ph_begin(PH_FINALIZE);
-  k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld);
-  k_reduce_partials<<<1, kThreadsPerBlock, 0, stream_>>>(r->part, r->nb_bins, 2, &dev_scal_[b].overflow);
+  k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld, r->ticket, &dev_scal_[b].overflow);
   ph_end(PH_FINALIZE);
   check(cudaGetLastError(), "place_at");
 }
@@ -384,12 +386,11 @@ void Engine::nesterov_step(int b, float step, float coeff) {
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
   ph_begin(PH_PLACE);
-  launches += (r->n_cells ? 1 : 0) + 2;
+  launches += (r->n_cells ? 1 : 0) + 1;
   if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, c, PLACE_NESTEROV, step, coeff, nullptr);
   ph_end(PH_PLACE);
   ph_begin(PH_FINALIZE);
-  k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld);
-  k_reduce_partials<<<1, kThreadsPerBlock, 0, stream_>>>(r->part, r->nb_bins, 2, &dev_scal_[b].overflow);
+  k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld, r->ticket, &dev_scal_[b].overflow);
   ph_end(PH_FINALIZE);
   check(cudaGetLastError(), "nesterov_step");
 }
@@ -461,9 +462,8 @@ void Engine::gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, S
   const float2 *pb2 = b2 == S_NUM ? nullptr : r->slot[b2];
   if (r->n_cells) {
     ph_begin(PH_GRAD);
-    launches += 2;
-    k_gradients<<<r->nb_cells, kThreadsPerBlock, 0, stream_>>>(r->args, c, pin_grad_, penalty, r->slot[out], pa1, pb1, pb2, r->part);
-    k_reduce_partials<<<1, kThreadsPerBlock, 0, stream_>>>(r->part, r->nb_cells, 4, &dev_scal_[b].wl_sum);
+    launches += 1;
+    k_gradients<<<r->nb_cells, kThreadsPerBlock, 0, stream_>>>(r->args, c, pin_grad_, penalty, r->slot[out], pa1, pb1, pb2, r->part, r->ticket, &dev_scal_[b].wl_sum);
     ph_end(PH_GRAD);
   } else {
     check(cudaMemsetAsync(&dev_scal_[b].wl_sum, 0, 4 * sizeof(double), stream_), "gradients");

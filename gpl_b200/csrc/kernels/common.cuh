@@ -67,6 +67,34 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return s;
 }
 
+// Whether this block is the last of its launch to finish: its partials written and fenced
+// before it counts itself, so the last one sees every block's partials. The count is left at
+// zero for the next launch.
+__device__ __forceinline__ bool last_block_done(unsigned int *ticket) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    if (last) *ticket = 0;
+  }
+  __syncthreads();
+  if (last) __threadfence();
+  return last;
+}
+
+// Sums `nblk` rows of `width` partials into out[0..width): each thread over rows t,
+// t + NT, ... then the block's sum, so the order is fixed for a block of NT threads.
+template <int NT>
+__device__ __forceinline__ void reduce_rows(const double *partials, int nblk, int width, double *out, double *sh) {
+  for (int j = 0; j < width; j++) {
+    double s = 0;
+    for (int b = threadIdx.x; b < nblk; b += NT) s += __ldcg(partials + (size_t)b * width + j);
+    double t = block_sum<NT>(s, sh);
+    if (threadIdx.x == 0) out[j] = t;
+  }
+}
+
 // A block's sums of four doubles at once (one barrier pass), valid in thread 0. Fixed order
 // for a fixed launch shape.
 template <int NT>

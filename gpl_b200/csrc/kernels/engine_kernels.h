@@ -64,11 +64,11 @@ struct WaArgs {
 };
 
 __global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *coords);
-__global__ void k_bins_finalize(RegionArgs r, double *partials, __nv_bfloat16 *dens_split, int split_ld);
+__global__ void k_bins_finalize(RegionArgs r, double *partials, __nv_bfloat16 *dens_split, int split_ld, unsigned int *ticket, double *out);
 __global__ void k_wa(WaArgs w, float cx, float cy);
 __global__ void k_wa_tiles(WaArgs w, float cx, float cy);
 __global__ void k_gradients(RegionArgs r, CellArgs c, const float2 *pin_grad, float penalty, float2 *out_sum,
-                            const float2 *a1, const float2 *b1, const float2 *b2, double *partials);
+                            const float2 *a1, const float2 *b1, const float2 *b2, double *partials, unsigned int *ticket, double *out);
 __global__ void k_prev_slp(RegionArgs r, CellArgs c, float coef);
 __global__ void k_hpwl(WaArgs w, unsigned long long *out);
 __global__ void k_hpwl_tiles(WaArgs w, unsigned long long *out);

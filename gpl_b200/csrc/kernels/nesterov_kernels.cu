@@ -34,15 +34,29 @@ __device__ __forceinline__ float inside_axis(float c, float half, float lo, floa
 // Integer adds throughout: the same accumulators in any order.
 constexpr int kTileBins = 2048;
 
+// Exact conversions on the FMA and integer pipes for the small values the addends take (the
+// conversion pipe is the scatter's busiest): an int in [0, 2^23) to float through the
+// 2^23 exponent pattern; a float in [0, 2^23) truncated through a round-down add of 2^23
+// (every float in [2^23, 2^24) is an integer). Larger values take the conversion pipe.
+__device__ __forceinline__ float small_i2f(int32_t v) {
+  return v < (1 << 23) ? __fsub_rn(__int_as_float(0x4B000000 | v), 8388608.0f) : (float)v;
+}
+__device__ __forceinline__ int64_t small_f2l_rz(float a) {
+  return a < 8388608.0f ? (int64_t)(__float_as_int(__fadd_rd(a, 8388608.0f)) - 0x4B000000) : f2l_rz(a);
+}
+
+// One cell's addend to one bin (N4): the overlap area in float (the widths converted, then
+// multiplied), times the cell's density scale (and the bin's target density for a macro),
+// truncated to int64. Areas and widths are non-negative.
 __device__ __forceinline__ int64_t cell_bin_addend(const RegionArgs &r, int32_t dlx, int32_t dux, int32_t dly, int32_t duy, int32_t x, int32_t y, float scale, uint8_t kind) {
   int32_t blx = r.bx[x], bux = r.bx[x + 1], bly = r.by[y], buy = r.by[y + 1];
   int32_t olx = dlx > blx ? dlx : blx, oux = dux < bux ? dux : bux;
   int32_t oly = dly > bly ? dly : bly, ouy = duy < buy ? duy : buy;
   float a = 0.0f;
-  if (olx < oux && oly < ouy) a = __fmul_rn((float)(oux - olx), (float)(ouy - oly));
+  if (olx < oux && oly < ouy) a = __fmul_rn(small_i2f(oux - olx), small_i2f(ouy - oly));
   a = __fmul_rn(a, scale);
   if (kind == CELL_MACRO) a = __fmul_rn(a, r.target_density);
-  return f2l_rz(a);
+  return small_f2l_rz(a);
 }
 
 __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
@@ -162,18 +176,21 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
       }
     }
     const unsigned peers = __match_any_sync(0xffffffffu, key);
-    s_red[threadIdx.x] = v;
-    __syncwarp();
-    if (key >= 0 && lane == __ffs(peers) - 1) {
-      unsigned long long sum = 0;
-      for (unsigned m = peers; m; m &= m - 1) sum += s_red[(threadIdx.x & ~31) + __ffs(m) - 1];
-      int slot = (key & 1) * kTileBins + (key >> 1);
-      if (narrow)
-        atomicAdd(&t32[slot], (unsigned int)sum);
-      else
-        atomicAdd(&s_tile[slot], sum);
+    if (narrow) {
+      // a block's sum for one bin stays below 2^32: each group of same-bin lanes adds its
+      // addends with one warp reduction, its first lane one shared atomic
+      const unsigned sum = __reduce_add_sync(peers, (unsigned)v);
+      if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&t32[(key & 1) * kTileBins + (key >> 1)], sum);
+    } else {
+      s_red[threadIdx.x] = v;
+      __syncwarp();
+      if (key >= 0 && lane == __ffs(peers) - 1) {
+        unsigned long long sum = 0;
+        for (unsigned m = peers; m; m &= m - 1) sum += s_red[(threadIdx.x & ~31) + __ffs(m) - 1];
+        atomicAdd(&s_tile[(key & 1) * kTileBins + (key >> 1)], sum);
+      }
+      __syncwarp();
     }
-    __syncwarp();
   }
   __syncthreads();
   for (int k = threadIdx.x; k < nt; k += blockDim.x) {
@@ -191,7 +208,7 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
 // index is divided; block partials of the two overflow sums.
 constexpr int kBinsPerThread = 4;
 
-__global__ void __launch_bounds__(kThreads) k_bins_finalize(RegionArgs r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld) {
+__global__ void __launch_bounds__(kThreads) k_bins_finalize(RegionArgs r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld, unsigned int *ticket, double *out) {
   __shared__ double sh[kThreads / 32];
   double o_sum = 0.0, ou_sum = 0.0;
   const int32_t x = blockIdx.x;
@@ -239,6 +256,8 @@ __global__ void __launch_bounds__(kThreads) k_bins_finalize(RegionArgs r, double
     partials[2 * blockIdx.x] = a;
     partials[2 * blockIdx.x + 1] = b;
   }
+  // the last block to finish sums the blocks' partials (the overflow sums)
+  if (last_block_done(ticket)) reduce_rows<kThreads>(partials, gridDim.x, 2, out, sh);
 }
 
 // ---- WA wirelength (updateWireLengthForceWA :2325-2388 + getWireLengthGradientPinWA
@@ -371,7 +390,19 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
   for (int j = threadIdx.x; j <= nn; j += blockDim.x) s_nstart[j] = (int32_t)(w.net_start[t.x + j] - p0);
   __syncthreads();
   const int32_t np = s_nstart[nn];
-  for (int j = threadIdx.x; j < np; j += blockDim.x) s_pos[j] = pin_pos(w, p0 + j);
+  // two pins per thread per step, their loads and cell gathers issued together
+  for (int j = threadIdx.x; j < np; j += 2 * blockDim.x) {
+    const int j2 = j + blockDim.x;
+    const bool two = j2 < np;
+    const int32_t ca = w.pin_cell ? w.pin_cell[p0 + j] : -1;
+    const int32_t cb = (two && w.pin_cell) ? w.pin_cell[p0 + j2] : -1;
+    int2 ba = w.pin_base[p0 + j];
+    int2 bb = two ? w.pin_base[p0 + j2] : make_int2(0, 0);
+    const int2 da = ca >= 0 ? w.dc[ca] : make_int2(0, 0);
+    const int2 db = cb >= 0 ? w.dc[cb] : make_int2(0, 0);
+    s_pos[j] = make_int2(ba.x + da.x, ba.y + da.y);
+    if (two) s_pos[j2] = make_int2(bb.x + db.x, bb.y + db.y);
+  }
   __syncthreads();
   long long h = 0;  // the same pins' HPWL, for the iteration's report
   for (int j = threadIdx.x; j < nn; j += blockDim.x) {
@@ -461,7 +492,7 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
 // the ordered sums; larger cells walk their bins.
 constexpr int kGradPinTile = 2048;
 
-__global__ void __launch_bounds__(kThreads, 5) k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials) {
+__global__ void __launch_bounds__(kThreads, 5) k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials, unsigned int *ticket, double *out) {
   __shared__ double4 sh[kThreads / 32];
   __shared__ float2 s_pg[kGradPinTile];
   const int i0 = blockIdx.x * blockDim.x;
@@ -558,6 +589,9 @@ __global__ void __launch_bounds__(kThreads, 5) k_gradients(RegionArgs r, CellArg
     partials[4 * blockIdx.x + 2] = v.z;
     partials[4 * blockIdx.x + 3] = v.w;
   }
+  // the last block to finish sums the blocks' partials (|wl|, |density|, the two distances)
+  __shared__ double shr[kThreads / 32];
+  if (last_block_done(ticket)) reduce_rows<kThreads>(partials, gridDim.x, 4, out, shr);
 }
 
 // ---- updateInitialPrevSLPCoordi (:2583-2595): a back-step along the current gradient.

@@ -86,14 +86,15 @@ int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_x
   cudaError_t e = cudaMemcpyAsync(starts.data(), net_start, starts.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return (int)e;
-  std::vector<int2> tiles;
+  if (starts[n_nets] >= ((int64_t)1 << 31)) return (int)cudaErrorInvalidValue;  // pin numbers are 32-bit
+  std::vector<int4> tiles;
   std::vector<int32_t> big;
   wa_tiles(starts.data(), (int32_t)n_nets, tiles, big);
-  int2 *d_tiles = nullptr;
+  int4 *d_tiles = nullptr;
   int32_t *d_big = nullptr;
-  e = cudaMalloc((void **)&d_tiles, std::max<size_t>(tiles.size(), 1) * sizeof(int2));
+  e = cudaMalloc((void **)&d_tiles, std::max<size_t>(tiles.size(), 1) * sizeof(int4));
   if (e == cudaSuccess) e = cudaMalloc((void **)&d_big, std::max<size_t>(big.size(), 1) * sizeof(int32_t));
-  if (e == cudaSuccess && !tiles.empty()) e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && !tiles.empty()) e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess && !big.empty()) e = cudaMemcpyAsync(d_big, big.data(), big.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
   if (e == cudaSuccess) {
     WaArgs w{};

@@ -59,8 +59,12 @@ void Engine::check(cudaError_t e, const char *where) {
 
 Engine::Engine(int device) : device_(device) {
   check(cudaSetDevice(device), "cudaSetDevice");
-  if (!failed()) check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-  if (!failed()) check(cudaStreamCreateWithFlags(&wa_stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  // the trial's own stream at the highest priority and the WA's beside it at the lowest: when
+  // both have blocks waiting, an SM that frees up takes the density solve's first
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  if (!failed()) check(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_hi), "cudaStreamCreate");
+  if (!failed()) check(cudaStreamCreateWithPriority(&wa_stream_, cudaStreamNonBlocking, prio_lo), "cudaStreamCreate");
   if (!failed()) check(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming), "cudaEventCreate");
   if (!failed()) check(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming), "cudaEventCreate");
 }
@@ -108,7 +112,8 @@ void Engine::free_globals() {
   cell_pin_start_ = nullptr;
   net_start_ = nullptr;
   pin_cell_ = pin_slot_ = big_nets_ = nullptr;
-  pin_base_ = tiles_ = nullptr;
+  pin_base_ = nullptr;
+  tiles_ = nullptr;
   n_tiles_ = n_big_ = 0;
   net_weight_ = nullptr;
   pin_grad_ = nullptr;
@@ -192,10 +197,11 @@ void Engine::upload(const EngineSetup &s) {
         wt[i] = s.net_weight[n];
       }
     });
+    if (ns[n_nets_] >= ((int64_t)1 << 31)) check(cudaErrorInvalidValue, "upload nets: 2^31 pins or more");
     check(upload_vec(&net_start_, ns, st), "upload nets");
     // WA's tiles of consecutive nets, and the nets too large for a tile (already in degree
     // order, so a warp's threads walk nets of one length)
-    std::vector<int2> tiles;
+    std::vector<int4> tiles;
     std::vector<int32_t> big;
     wa_tiles(ns.data(), n_nets_, tiles, big);
     n_tiles_ = (int32_t)tiles.size();
@@ -206,6 +212,7 @@ void Engine::upload(const EngineSetup &s) {
     check(upload_vec(&pin_cell_, pc, st), "upload pins");
     check(upload_vec(&pin_base_, pb, st), "upload pins");
     check(upload_vec(&net_weight_, wt, st), "upload nets");
+    unit_weights_ = std::all_of(wt.begin(), wt.end(), [](float v) { return v == 1.0f; });
   }
   progress("  upload: cells, nets and pins");
   check(dmalloc(&pin_grad_, s.cell_pins.size()), "alloc pins");
@@ -409,7 +416,7 @@ WaArgs Engine::wa_args() const {
   w.n_nets = n_big_;
   w.net_start = net_start_;
   w.net_order = big_nets_;
-  w.net_weight = net_weight_;
+  w.net_weight = unit_weights_ ? nullptr : net_weight_;  // x * 1.0f is x, bit for bit
   w.pin_cell = pin_cell_;
   w.pin_base = pin_base_;
   w.dc = dc_;
@@ -575,6 +582,7 @@ void Engine::set_net_weights(const std::vector<float> &w) {
   // in the device's net order (a copy from pageable memory returns once the data is staged)
   std::vector<float> dw(w.size());
   for (size_t i = 0; i < w.size(); i++) dw[i] = w[net_order_[i]];
+  unit_weights_ = std::all_of(dw.begin(), dw.end(), [](float v) { return v == 1.0f; });
   check(cudaMemcpyAsync(net_weight_, dw.data(), dw.size() * sizeof(float), cudaMemcpyHostToDevice, stream_), "net weights");
 }
 

@@ -138,9 +138,11 @@ class Engine {
   std::vector<int32_t> net_order_;
   int64_t *net_start_ = nullptr;
   int32_t *pin_cell_ = nullptr, *pin_slot_ = nullptr, *big_nets_ = nullptr;
-  int2 *pin_base_ = nullptr, *tiles_ = nullptr;
+  int2 *pin_base_ = nullptr;
+  int4 *tiles_ = nullptr;
   int32_t n_tiles_ = 0, n_big_ = 0;
   float *net_weight_ = nullptr;
+  bool unit_weights_ = true;  // every net weight is 1: the WA kernels skip the weight loads
   float2 *pin_grad_ = nullptr;  // the WA force of every pin of a cell, cell-major (cell_pins order)
   unsigned long long *hpwl_acc_ = nullptr;
   bool hpwl_ready_ = false;  // hpwl_acc_ holds the HPWL of the current centres (from the WA)

@@ -58,8 +58,8 @@ struct WaArgs {
   const int2 *dc;                // global device cell centres
   const int32_t *pin_slot;       // where a pin's force goes (-1: nowhere); NULL: at the pin
   float2 *pin_grad;
-  int32_t n_tiles;               // tiles of consecutive nets: [first, last) per tile
-  const int2 *tiles;
+  int32_t n_tiles;               // tiles of consecutive nets: first net, end net, first pin, pins
+  const int4 *tiles;
   unsigned long long *hpwl_out;  // WA adds the HPWL of the same pin positions here (NULL: not)
 };
 
@@ -79,7 +79,7 @@ bool narrow_tile(const std::vector<int32_t> &bx, const std::vector<int32_t> &by)
 
 // Tiles of consecutive nets (at most kWaTilePins pins and kWaTileNets nets each) and the nets
 // too large for a tile, from the nets' pin starts.
-void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int2> &tiles, std::vector<int32_t> &big);
+void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int4> &tiles, std::vector<int32_t> &big);
 __global__ void k_hold_locked(RegionArgs r, CellArgs c);
 __global__ void k_reduce_partials(const double *partials, int nblk, int width, double *out);
 

@@ -376,6 +376,7 @@ __global__ void k_wa(WaArgs w, float cx, float cy) {
 // The engine orders its nets by degree, so a tile's nets are alike and the thread-per-net
 // phases run without divergence. The results are the thread-per-net kernel's bit for bit.
 static_assert(kWaTileNets <= 256, "a pin's net index in the tile is kept in 8 bits");
+static_assert(kWaTilePins <= 2 * kThreads, "a thread holds at most two of a tile's pins");
 
 __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float cy) {
   __shared__ int2 s_pos[kWaTilePins];        // phases 1-3: the position; 3-5: its floats' bits
@@ -384,24 +385,26 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
   __shared__ int32_t s_nstart[kWaTileNets + 1];
   __shared__ int4 s_box[kWaTileNets];
   __shared__ float s_sum[8][kWaTileNets];
-  const int2 t = w.tiles[blockIdx.x];
-  const int32_t nn = t.y - t.x;
-  const int64_t p0 = w.net_start[t.x];
+  const int4 t = w.tiles[blockIdx.x];
+  const int32_t nn = t.y - t.x, np = t.w;
+  const int64_t p0 = t.z;
+  // the nets' starts and the pins' positions load together (a thread's two pins, their loads
+  // and cell gathers issued at once), and each pin's place in its cell's list for the end
   for (int j = threadIdx.x; j <= nn; j += blockDim.x) s_nstart[j] = (int32_t)(w.net_start[t.x + j] - p0);
-  __syncthreads();
-  const int32_t np = s_nstart[nn];
-  // two pins per thread per step, their loads and cell gathers issued together
-  for (int j = threadIdx.x; j < np; j += 2 * blockDim.x) {
-    const int j2 = j + blockDim.x;
-    const bool two = j2 < np;
-    const int32_t ca = w.pin_cell ? w.pin_cell[p0 + j] : -1;
-    const int32_t cb = (two && w.pin_cell) ? w.pin_cell[p0 + j2] : -1;
-    int2 ba = w.pin_base[p0 + j];
-    int2 bb = two ? w.pin_base[p0 + j2] : make_int2(0, 0);
+  const int ja = threadIdx.x, jb = threadIdx.x + kThreads;
+  int32_t slot_a = -1, slot_b = -1;
+  if (ja < np) {
+    const bool two = jb < np;
+    const int32_t ca = w.pin_cell ? w.pin_cell[p0 + ja] : -1;
+    const int32_t cb = (two && w.pin_cell) ? w.pin_cell[p0 + jb] : -1;
+    slot_a = w.pin_slot ? w.pin_slot[p0 + ja] : (int32_t)(p0 + ja);
+    if (two) slot_b = w.pin_slot ? w.pin_slot[p0 + jb] : (int32_t)(p0 + jb);
+    int2 ba = w.pin_base[p0 + ja];
+    int2 bb = two ? w.pin_base[p0 + jb] : make_int2(0, 0);
     const int2 da = ca >= 0 ? w.dc[ca] : make_int2(0, 0);
     const int2 db = cb >= 0 ? w.dc[cb] : make_int2(0, 0);
-    s_pos[j] = make_int2(ba.x + da.x, ba.y + da.y);
-    if (two) s_pos[j2] = make_int2(bb.x + db.x, bb.y + db.y);
+    s_pos[ja] = make_int2(ba.x + da.x, ba.y + da.y);
+    if (two) s_pos[jb] = make_int2(bb.x + db.x, bb.y + db.y);
   }
   __syncthreads();
   long long h = 0;  // the same pins' HPWL, for the iteration's report
@@ -478,7 +481,8 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
     float gmin_y = (m & 4u) ? wa_term_min(s_sum[4][n], s_sum[5][n], v.z, cy, qy) : 0.0f;
     float gmax_y = (m & 8u) ? wa_term_max(s_sum[6][n], s_sum[7][n], v.w, cy, qy) : 0.0f;
     float wt = w.net_weight ? w.net_weight[t.x + n] : 1.0f;
-    wa_store(w, p0 + j, make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt)));
+    const int32_t at = j == ja ? slot_a : slot_b;
+    if (at >= 0) w.pin_grad[at] = make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt));
   }
 }
 
@@ -636,12 +640,10 @@ __global__ void k_hpwl(WaArgs w, unsigned long long *__restrict__ out) {
 __global__ void __launch_bounds__(kThreads) k_hpwl_tiles(WaArgs w, unsigned long long *__restrict__ out) {
   __shared__ int2 s_pos[kWaTilePins];
   __shared__ int32_t s_nstart[kWaTileNets + 1];
-  const int2 t = w.tiles[blockIdx.x];
-  const int32_t nn = t.y - t.x;
-  const int64_t p0 = w.net_start[t.x];
+  const int4 t = w.tiles[blockIdx.x];
+  const int32_t nn = t.y - t.x, np = t.w;
+  const int64_t p0 = t.z;
   for (int j = threadIdx.x; j <= nn; j += blockDim.x) s_nstart[j] = (int32_t)(w.net_start[t.x + j] - p0);
-  __syncthreads();
-  const int32_t np = s_nstart[nn];
   for (int j = threadIdx.x; j < np; j += blockDim.x) s_pos[j] = pin_pos(w, p0 + j);
   __syncthreads();
   long long h = 0;
@@ -666,12 +668,13 @@ __global__ void k_pack_centres(int64_t n, const int32_t *__restrict__ x, const i
   if (i < n) out[i] = make_int2(x[i], y[i]);
 }
 
-void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int2> &tiles, std::vector<int32_t> &big) {
+void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int4> &tiles, std::vector<int32_t> &big) {
   tiles.clear();
   big.clear();
   int32_t first = 0;
+  // a tile: its nets [first, end), its first pin and its pin count (pin numbers below 2^31)
   auto close = [&](int32_t end) {
-    if (end > first) tiles.push_back(make_int2(first, end));
+    if (end > first) tiles.push_back(make_int4(first, end, (int32_t)net_start[first], (int32_t)(net_start[end] - net_start[first])));
   };
   for (int32_t n = 0; n < n_nets; n++) {
     int64_t deg = net_start[n + 1] - net_start[n];

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "../../../include/gpl.h"
+#include "../kernels/b2b.h"
 #include "../kernels/bicgstab.h"
 #include "../kernels/engine_kernels.h"
 #include "../kernels/rudy.h"
@@ -114,6 +115,12 @@ int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_x
   cudaFree(d_tiles);
   cudaFree(d_big);
   return (int)(e != cudaSuccess ? e : e2);
+}
+
+int gpl_kernel_csr_from_triplets(int64_t n, int64_t nt, const int32_t *rows, const int32_t *cols, const float *vals, int64_t *row_start, int32_t *out_cols, float *out_vals, int64_t *nnz, void *stream) {
+  if (n < 0 || nt < 0 || nt >= ((int64_t)1 << 32)) return (int)cudaErrorInvalidValue;  // positions are 32-bit
+  IpDevice dev((cudaStream_t)stream);
+  return (int)dev.csr_from_triplets(n, nt, rows, cols, vals, row_start, out_cols, out_vals, nnz);
 }
 
 static_assert(GPL_SPMV_ROWS == kSpmvRows && GPL_SPMV_TILED == kSpmvTiled, "the C ABI's SpMV forms");

@@ -722,6 +722,24 @@ cudaError_t IpDevice::collapse(int64_t n_trip, const int32_t *row, const int32_t
   return cudaGetLastError();
 }
 
+cudaError_t IpDevice::csr_from_triplets(int64_t n, int64_t nt, const int32_t *row, const int32_t *col, const float *val, int64_t *starts, int32_t *cols, float *vals, int64_t *nnz) {
+  release();
+  n_ = n;
+  CK(cudaFuncSetAttribute(k_row_collapse_block, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
+  CK(alloc(&row_off_, n_ + 1));
+  CK(alloc(&ucount_, n_ + 1));
+  CK(alloc(&fill_, n_));
+  CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1)));
+  CK(alloc(&tier_n_, 3));
+  CK(grow((size_t)std::max<int64_t>(nt, 1), w_cap_, &bucket_, &ucol_, &uval_));
+  size_t cap = (size_t)std::max<int64_t>(nt, 1);  // nnz <= nt: the caller's buffers suffice
+  int32_t *c = cols;
+  float *v = vals;
+  CK(collapse(nt, row, col, val, starts, &c, &v, &cap, nnz));
+  if (c != cols || v != vals) return cudaErrorUnknown;  // cannot happen: nnz <= nt
+  return cudaStreamSynchronize(s_);
+}
+
 cudaError_t IpDevice::assemble(IpAxisResult out[2]) {
   IpArgs a{};
   a.n_nets = n_nets_;

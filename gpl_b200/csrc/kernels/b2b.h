@@ -58,6 +58,10 @@ class IpDevice {
   cudaError_t solution(int axis, std::vector<float> &x);
   // The placed instances' boxes and database boxes.
   cudaError_t download(std::vector<int4> &box, std::vector<int4> &db_box);
+  // `Csr::from_triplets` (src/bicgstab.rs:501-541) on its own, on device triplets: n rows,
+  // nt triplets (row, col, val) in order; writes starts[n + 1] and the *nnz (host) entries of
+  // cols and vals (device buffers of at least nt entries). For a device that holds no design.
+  cudaError_t csr_from_triplets(int64_t n, int64_t nt, const int32_t *row, const int32_t *col, const float *val, int64_t *starts, int32_t *cols, float *vals, int64_t *nnz);
   int64_t launches = 0, h2d_bytes = 0, d2h_bytes = 0;
 
  private:

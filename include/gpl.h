@@ -232,6 +232,15 @@ int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy,
 int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy,
                   const float *net_weight, float coef_x, float coef_y, float *grad, void *stream);
 
+/* `Csr::from_triplets` (src/bicgstab.rs:501-541, the initial placement's collapse) on device
+ * arrays: n rows, nt triplets (row, col, val) in their order; duplicates summed in that order,
+ * each row's columns ascending. Writes row_start[n+1], and *nnz (host) entries into cols and
+ * vals (device buffers of at least nt entries). Rows of any length: a warp, a block or a
+ * thread per row by length, the same result from each. */
+int gpl_kernel_csr_from_triplets(int64_t n, int64_t nt, const int32_t *rows, const int32_t *cols,
+                                 const float *vals, int64_t *row_start, int32_t *out_cols,
+                                 float *out_vals, int64_t *nnz, void *stream);
+
 /* `Csr::mul` (src/bicgstab.rs:72-82): y = A x on a CSR matrix (device pointers), each row's
  * products summed in column order, then 0 + 1 * sum, as the solver forms them. form picks the
  * kernel: GPL_SPMV_ROWS (a thread per row) or GPL_SPMV_TILED (a block's products staged in

@@ -176,6 +176,42 @@ def test_spmv_forms_match_the_reference_order(L, form):
     assert np.array_equal(y.cpu().numpy().view(np.uint32), ref.view(np.uint32))
 
 
+def test_csr_from_triplets_matches_the_oracle_at_every_row_length(L):
+    """`Csr::from_triplets` (src/bicgstab.rs:501-541) bit for bit: the same row starts, columns
+    and summed values. Row lengths reach every tier of the device collapse: up to 64 keys (a
+    warp, registers), 256 (a warp, eight per lane), 8192 (a block, shared memory) and beyond (a
+    thread); narrow column ranges force many duplicates, summed in triplet order."""
+    rng = np.random.default_rng(23)
+    n = 4000
+    lens = rng.integers(0, 40, n)
+    lens[rng.choice(n, 60, replace=False)] = rng.integers(65, 257, 60)
+    lens[rng.choice(n, 12, replace=False)] = rng.integers(300, 8193, 12)
+    lens[rng.choice(n, 2, replace=False)] = [9000, 20000]
+    rows = np.repeat(np.arange(n), lens)
+    span = np.where(rng.random(n) < 0.5, 8, n)  # half the rows draw from 8 columns only
+    cols = (rng.integers(0, 1 << 30, len(rows)) % np.repeat(span, lens)).astype(np.int64)
+    order = rng.permutation(len(rows))  # triplets in no particular order
+    rows, cols = rows[order].astype(np.int64), cols[order]
+    vals = rng.uniform(-1, 1, len(rows)).astype(np.float32)
+    O = oracle.lib()
+    ws = np.zeros(n + 1, np.int64)
+    wc = np.zeros(len(rows), np.int32)
+    wv = np.zeros(len(rows), np.float32)
+    nnz = O.oracle_csr_from_triplets(n, len(rows), rows.ctypes.data, cols.ctypes.data, vals.ctypes.data, ws.ctypes.data, wc.ctypes.data, wv.ctypes.data)
+    d = [dev(rows.astype(np.int32)), dev(cols.astype(np.int32)), dev(vals)]  # held across the call
+    gs = dev(np.zeros(n + 1, np.int64))
+    gc = dev(np.zeros(len(rows), np.int32))
+    gv = dev(np.zeros(len(rows), np.float32))
+    gn = C.c_int64()
+    L.gpl_kernel_csr_from_triplets.argtypes = [C.c_int64, C.c_int64] + [C.c_void_p] * 6 + [C.POINTER(C.c_int64), C.c_void_p]
+    assert L.gpl_kernel_csr_from_triplets(n, len(rows), ptr(d[0]), ptr(d[1]), ptr(d[2]), ptr(gs), ptr(gc), ptr(gv), C.byref(gn), stream()) == 0
+    sync()
+    assert gn.value == nnz
+    np.testing.assert_array_equal(gs.cpu().numpy(), ws)
+    np.testing.assert_array_equal(gc.cpu().numpy()[:nnz], wc[:nnz])
+    np.testing.assert_array_equal(gv.cpu().numpy()[:nnz].view(np.uint32), wv[:nnz].view(np.uint32))
+
+
 def test_bicgstab_matches_the_oracle(L):
     rng = np.random.default_rng(3)
     n = 3000

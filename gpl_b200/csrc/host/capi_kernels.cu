@@ -107,7 +107,7 @@ int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_x
     w.pin_grad = reinterpret_cast<float2 *>(grad);
     w.n_tiles = (int32_t)tiles.size();
     w.tiles = d_tiles;
-    if (!tiles.empty()) k_wa_tiles<<<(unsigned)tiles.size(), kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y);
+    if (!tiles.empty()) launch_wa_tiles(w, coef_x, coef_y, s);
     if (!big.empty()) k_wa<<<(unsigned)((big.size() + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y);
     e = cudaGetLastError();
   }

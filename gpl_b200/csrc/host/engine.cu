@@ -445,7 +445,7 @@ void Engine::wa(float cx, float cy) {
   ph_begin(PH_WA, st);
   if (n_tiles_) {
     launches += 1;
-    k_wa_tiles<<<n_tiles_, kThreadsPerBlock, 0, st>>>(w, cx, cy);
+    launch_wa_tiles(w, cx, cy, st);
   }
   if (n_big_) {
     launches += 1;

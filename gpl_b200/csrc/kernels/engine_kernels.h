@@ -67,6 +67,8 @@ __global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, fl
 __global__ void k_bins_finalize(RegionArgs r, double *partials, __nv_bfloat16 *dens_split, int split_ld, unsigned int *ticket, double *out);
 __global__ void k_wa(WaArgs w, float cx, float cy);
 __global__ void k_wa_tiles(WaArgs w, float cx, float cy);
+// k_wa_tiles over every tile: a persistent grid of the blocks the device holds at once.
+void launch_wa_tiles(const WaArgs &w, float cx, float cy, cudaStream_t s);
 __global__ void k_gradients(RegionArgs r, CellArgs c, const float2 *pin_grad, float penalty, float2 *out_sum,
                             const float2 *a1, const float2 *b1, const float2 *b2, double *partials, unsigned int *ticket, double *out);
 __global__ void k_prev_slp(RegionArgs r, CellArgs c, float coef);

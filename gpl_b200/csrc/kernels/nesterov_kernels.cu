@@ -385,105 +385,143 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
   __shared__ int32_t s_nstart[kWaTileNets + 1];
   __shared__ int4 s_box[kWaTileNets];
   __shared__ float s_sum[8][kWaTileNets];
-  const int4 t = w.tiles[blockIdx.x];
-  const int32_t nn = t.y - t.x, np = t.w;
-  const int64_t p0 = t.z;
-  // the nets' starts and the pins' positions load together (a thread's two pins, their loads
-  // and cell gathers issued at once), and each pin's place in its cell's list for the end
-  for (int j = threadIdx.x; j <= nn; j += blockDim.x) s_nstart[j] = (int32_t)(w.net_start[t.x + j] - p0);
+  // Persistent: the block walks tiles blockIdx.x, + gridDim.x, ...; the next tile's record and
+  // its pins' cells load while this tile computes, so a tile starts with one round trip (the
+  // cell centres) instead of three.
   const int ja = threadIdx.x, jb = threadIdx.x + kThreads;
-  int32_t slot_a = -1, slot_b = -1;
-  if (ja < np) {
-    const bool two = jb < np;
-    const int32_t ca = w.pin_cell ? w.pin_cell[p0 + ja] : -1;
-    const int32_t cb = (two && w.pin_cell) ? w.pin_cell[p0 + jb] : -1;
-    slot_a = w.pin_slot ? w.pin_slot[p0 + ja] : (int32_t)(p0 + ja);
-    if (two) slot_b = w.pin_slot ? w.pin_slot[p0 + jb] : (int32_t)(p0 + jb);
-    int2 ba = w.pin_base[p0 + ja];
-    int2 bb = two ? w.pin_base[p0 + jb] : make_int2(0, 0);
-    const int2 da = ca >= 0 ? w.dc[ca] : make_int2(0, 0);
-    const int2 db = cb >= 0 ? w.dc[cb] : make_int2(0, 0);
-    s_pos[ja] = make_int2(ba.x + da.x, ba.y + da.y);
-    if (two) s_pos[jb] = make_int2(bb.x + db.x, bb.y + db.y);
+  int tile = blockIdx.x;
+  if (tile >= w.n_tiles) return;
+  int4 t = w.tiles[tile];
+  int32_t ca = -1, cb = -1;  // this tile's pins' cells
+  if (w.pin_cell) {
+    if (ja < t.w) ca = w.pin_cell[t.z + ja];
+    if (jb < t.w) cb = w.pin_cell[t.z + jb];
   }
-  __syncthreads();
-  long long h = 0;  // the same pins' HPWL, for the iteration's report
-  for (int j = threadIdx.x; j < nn; j += blockDim.x) {
-    int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
-    for (int32_t k = s_nstart[j]; k < s_nstart[j + 1]; k++) {
-      int2 q = s_pos[k];
-      lx = min(lx, q.x);
-      ly = min(ly, q.y);
-      ux = max(ux, q.x);
-      uy = max(uy, q.y);
-      s_pnet[k] = (uint16_t)j;
+  for (;;) {
+    const int32_t nn = t.y - t.x, np = t.w;
+    const int64_t p0 = t.z;
+    // the nets' starts and the pins' positions load together, and each pin's place in its
+    // cell's list for the end
+    for (int j = threadIdx.x; j <= nn; j += blockDim.x) s_nstart[j] = (int32_t)(w.net_start[t.x + j] - p0);
+    int32_t slot_a = -1, slot_b = -1;
+    if (ja < np) {
+      const bool two = jb < np;
+      slot_a = w.pin_slot ? w.pin_slot[p0 + ja] : (int32_t)(p0 + ja);
+      if (two) slot_b = w.pin_slot ? w.pin_slot[p0 + jb] : (int32_t)(p0 + jb);
+      int2 ba = w.pin_base[p0 + ja];
+      int2 bb = two ? w.pin_base[p0 + jb] : make_int2(0, 0);
+      const int2 da = ca >= 0 ? w.dc[ca] : make_int2(0, 0);
+      const int2 db = cb >= 0 ? w.dc[cb] : make_int2(0, 0);
+      s_pos[ja] = make_int2(ba.x + da.x, ba.y + da.y);
+      if (two) s_pos[jb] = make_int2(bb.x + db.x, bb.y + db.y);
     }
-    s_box[j] = make_int4(lx, ly, ux, uy);
-    if (ux >= lx) h += ((long long)ux - lx) + ((long long)uy - ly);
-  }
-  if (w.hpwl_out) {
+    __syncthreads();
+    const int next = tile + gridDim.x;
+    const int4 tn = next < w.n_tiles ? w.tiles[next] : make_int4(0, 0, 0, 0);
+    long long h = 0;  // the same pins' HPWL, for the iteration's report
+    for (int j = threadIdx.x; j < nn; j += blockDim.x) {
+      int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+      for (int32_t k = s_nstart[j]; k < s_nstart[j + 1]; k++) {
+        int2 q = s_pos[k];
+        lx = min(lx, q.x);
+        ly = min(ly, q.y);
+        ux = max(ux, q.x);
+        uy = max(uy, q.y);
+        s_pnet[k] = (uint16_t)j;
+      }
+      s_box[j] = make_int4(lx, ly, ux, uy);
+      if (ux >= lx) h += ((long long)ux - lx) + ((long long)uy - ly);
+    }
+    if (w.hpwl_out) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
-    if ((threadIdx.x & 31) == 0 && h) atomicAdd(w.hpwl_out, (unsigned long long)h);
-  }
-  __syncthreads();
-  const float BAR = -300.0f;
-  for (int j = threadIdx.x; j < np; j += blockDim.x) {
-    int2 q = s_pos[j];
-    uint32_t n = s_pnet[j];
-    int4 b = s_box[n];
-    float emin_x = __fmul_rn((float)(b.x - q.x), cx), emax_x = __fmul_rn((float)(q.x - b.z), cx);
-    float emin_y = __fmul_rn((float)(b.y - q.y), cy), emax_y = __fmul_rn((float)(q.y - b.w), cy);
-    uint32_t m = (emin_x > BAR ? 1u : 0u) | (emax_x > BAR ? 2u : 0u) | (emin_y > BAR ? 4u : 0u) | (emax_y > BAR ? 8u : 0u);
-    float4 v;
-    v.x = (m & 1u) ? fast_exp(emin_x) : 0.0f;
-    v.y = (m & 2u) ? fast_exp(emax_x) : 0.0f;
-    v.z = (m & 4u) ? fast_exp(emin_y) : 0.0f;
-    v.w = (m & 8u) ? fast_exp(emax_y) : 0.0f;
-    s_v[j] = v;
-    s_pnet[j] = (uint16_t)(n | (m << 8));
-    s_pos[j] = make_int2(__float_as_int((float)q.x), __float_as_int((float)q.y));
-  }
-  __syncthreads();
-  for (int j = threadIdx.x; j < nn; j += blockDim.x) {
-    float s_minx = 0, s_xminx = 0, s_maxx = 0, s_xmaxx = 0, s_miny = 0, s_yminy = 0, s_maxy = 0, s_ymaxy = 0;
-    for (int32_t k = s_nstart[j]; k < s_nstart[j + 1]; k++) {
-      int2 q = s_pos[k];
-      float4 v = s_v[k];
-      float qx = __int_as_float(q.x), qy = __int_as_float(q.y);
-      s_minx = __fadd_rn(s_minx, v.x);
-      s_xminx = __fadd_rn(s_xminx, __fmul_rn(qx, v.x));
-      s_maxx = __fadd_rn(s_maxx, v.y);
-      s_xmaxx = __fadd_rn(s_xmaxx, __fmul_rn(qx, v.y));
-      s_miny = __fadd_rn(s_miny, v.z);
-      s_yminy = __fadd_rn(s_yminy, __fmul_rn(qy, v.z));
-      s_maxy = __fadd_rn(s_maxy, v.w);
-      s_ymaxy = __fadd_rn(s_ymaxy, __fmul_rn(qy, v.w));
+      for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+      if ((threadIdx.x & 31) == 0 && h) atomicAdd(w.hpwl_out, (unsigned long long)h);
     }
-    s_sum[0][j] = s_minx;
-    s_sum[1][j] = s_xminx;
-    s_sum[2][j] = s_maxx;
-    s_sum[3][j] = s_xmaxx;
-    s_sum[4][j] = s_miny;
-    s_sum[5][j] = s_yminy;
-    s_sum[6][j] = s_maxy;
-    s_sum[7][j] = s_ymaxy;
+    __syncthreads();
+    const float BAR = -300.0f;
+    for (int j = threadIdx.x; j < np; j += blockDim.x) {
+      int2 q = s_pos[j];
+      uint32_t n = s_pnet[j];
+      int4 b = s_box[n];
+      float emin_x = __fmul_rn((float)(b.x - q.x), cx), emax_x = __fmul_rn((float)(q.x - b.z), cx);
+      float emin_y = __fmul_rn((float)(b.y - q.y), cy), emax_y = __fmul_rn((float)(q.y - b.w), cy);
+      uint32_t m = (emin_x > BAR ? 1u : 0u) | (emax_x > BAR ? 2u : 0u) | (emin_y > BAR ? 4u : 0u) | (emax_y > BAR ? 8u : 0u);
+      float4 v;
+      v.x = (m & 1u) ? fast_exp(emin_x) : 0.0f;
+      v.y = (m & 2u) ? fast_exp(emax_x) : 0.0f;
+      v.z = (m & 4u) ? fast_exp(emin_y) : 0.0f;
+      v.w = (m & 8u) ? fast_exp(emax_y) : 0.0f;
+      s_v[j] = v;
+      s_pnet[j] = (uint16_t)(n | (m << 8));
+      s_pos[j] = make_int2(__float_as_int((float)q.x), __float_as_int((float)q.y));
+    }
+    __syncthreads();
+    // the next tile's pins' cells (its record has arrived)
+    int32_t can = -1, cbn = -1;
+    if (w.pin_cell) {
+      if (ja < tn.w) can = w.pin_cell[tn.z + ja];
+      if (jb < tn.w) cbn = w.pin_cell[tn.z + jb];
+    }
+    for (int j = threadIdx.x; j < nn; j += blockDim.x) {
+      float s_minx = 0, s_xminx = 0, s_maxx = 0, s_xmaxx = 0, s_miny = 0, s_yminy = 0, s_maxy = 0, s_ymaxy = 0;
+      for (int32_t k = s_nstart[j]; k < s_nstart[j + 1]; k++) {
+        int2 q = s_pos[k];
+        float4 v = s_v[k];
+        float qx = __int_as_float(q.x), qy = __int_as_float(q.y);
+        s_minx = __fadd_rn(s_minx, v.x);
+        s_xminx = __fadd_rn(s_xminx, __fmul_rn(qx, v.x));
+        s_maxx = __fadd_rn(s_maxx, v.y);
+        s_xmaxx = __fadd_rn(s_xmaxx, __fmul_rn(qx, v.y));
+        s_miny = __fadd_rn(s_miny, v.z);
+        s_yminy = __fadd_rn(s_yminy, __fmul_rn(qy, v.z));
+        s_maxy = __fadd_rn(s_maxy, v.w);
+        s_ymaxy = __fadd_rn(s_ymaxy, __fmul_rn(qy, v.w));
+      }
+      s_sum[0][j] = s_minx;
+      s_sum[1][j] = s_xminx;
+      s_sum[2][j] = s_maxx;
+      s_sum[3][j] = s_xmaxx;
+      s_sum[4][j] = s_miny;
+      s_sum[5][j] = s_yminy;
+      s_sum[6][j] = s_maxy;
+      s_sum[7][j] = s_ymaxy;
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < np; j += blockDim.x) {
+      int2 q = s_pos[j];
+      float4 v = s_v[j];
+      uint32_t pn = s_pnet[j];
+      uint32_t n = pn & 0xffu, m = pn >> 8;
+      float qx = __int_as_float(q.x), qy = __int_as_float(q.y);
+      float gmin_x = (m & 1u) ? wa_term_min(s_sum[0][n], s_sum[1][n], v.x, cx, qx) : 0.0f;
+      float gmax_x = (m & 2u) ? wa_term_max(s_sum[2][n], s_sum[3][n], v.y, cx, qx) : 0.0f;
+      float gmin_y = (m & 4u) ? wa_term_min(s_sum[4][n], s_sum[5][n], v.z, cy, qy) : 0.0f;
+      float gmax_y = (m & 8u) ? wa_term_max(s_sum[6][n], s_sum[7][n], v.w, cy, qy) : 0.0f;
+      float wt = w.net_weight ? w.net_weight[t.x + n] : 1.0f;
+      const int32_t at = j == ja ? slot_a : slot_b;
+      if (at >= 0) w.pin_grad[at] = make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt));
+    }
+    if (next >= w.n_tiles) break;
+    __syncthreads();  // every read of this tile's shared arrays ends before the next tile's writes
+    tile = next;
+    t = tn;
+    ca = can;
+    cb = cbn;
   }
-  __syncthreads();
-  for (int j = threadIdx.x; j < np; j += blockDim.x) {
-    int2 q = s_pos[j];
-    float4 v = s_v[j];
-    uint32_t pn = s_pnet[j];
-    uint32_t n = pn & 0xffu, m = pn >> 8;
-    float qx = __int_as_float(q.x), qy = __int_as_float(q.y);
-    float gmin_x = (m & 1u) ? wa_term_min(s_sum[0][n], s_sum[1][n], v.x, cx, qx) : 0.0f;
-    float gmax_x = (m & 2u) ? wa_term_max(s_sum[2][n], s_sum[3][n], v.y, cx, qx) : 0.0f;
-    float gmin_y = (m & 4u) ? wa_term_min(s_sum[4][n], s_sum[5][n], v.z, cy, qy) : 0.0f;
-    float gmax_y = (m & 8u) ? wa_term_max(s_sum[6][n], s_sum[7][n], v.w, cy, qy) : 0.0f;
-    float wt = w.net_weight ? w.net_weight[t.x + n] : 1.0f;
-    const int32_t at = j == ja ? slot_a : slot_b;
-    if (at >= 0) w.pin_grad[at] = make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt));
+}
+
+// The WA tiles' launch: a persistent grid of as many blocks as fit on the device at once.
+void launch_wa_tiles(const WaArgs &w, float cx, float cy, cudaStream_t s) {
+  if (w.n_tiles <= 0) return;
+  static int resident = 0;  // blocks per device at once (the devices of a run are alike)
+  if (!resident) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_wa_tiles, kThreads, 0);
+    resident = std::max(1, sms * std::max(per, 1));
   }
+  k_wa_tiles<<<std::min(w.n_tiles, resident), kThreads, 0, s>>>(w, cx, cy);
 }
 
 // ---- cells: updateGradients (:2455-2507): the WA force over the cell's pins in its order,

@@ -836,8 +836,7 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
     IpAxisResult r[2];
     device(dev.assemble(r), "initial placement assembly");
     progress("  round %d: B2B assembled and collapsed (%lld + %lld triplets)", iter, (long long)r[0].triplets, (long long)r[1].triplets);
-    device(dev.solve(0, vars.max_solver_iter, r[0]), "initial placement solve x");
-    device(dev.solve(1, vars.max_solver_iter, r[1]), "initial placement solve y");
+    device(dev.solve(vars.max_solver_iter, r), "initial placement solves");
     const BicgResult &ex = r[0].solve, &ey = r[1].solve;
     progress("  round %d: solved (%d + %d iterations)", iter, ex.iterations, ey.iterations);
     if (log.trace_on) {

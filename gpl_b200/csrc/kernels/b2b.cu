@@ -662,8 +662,9 @@ cudaError_t IpDevice::upload(const IpSetup &s) {
     CK(alloc(&a.rhs, n_));
     CK(alloc(&a.x, n_));
   }
-  scratch_bytes_ = bicgstab_scratch_bytes(n_);
-  CK(cudaMalloc(&scratch_, scratch_bytes_));
+  // the two axes' solver scratch, side by side (256-byte aligned halves)
+  scratch_bytes_ = (bicgstab_scratch_bytes(n_) + 255) / 256 * 256;
+  CK(cudaMalloc(&scratch_, 2 * scratch_bytes_));
   return cudaStreamSynchronize(s_);
 }
 
@@ -800,18 +801,29 @@ cudaError_t IpDevice::assemble(IpAxisResult out[2]) {
   return cudaStreamSynchronize(s_);
 }
 
-cudaError_t IpDevice::solve(int axis, int max_iters, IpAxisResult &out) {
-  Axis &A = ax_[axis];
-  CsrDev m{n_, A.starts, A.cols, A.vals};
-  BicgResult r{};
+cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
+  CsrDev m[2];
+  const float *b[2];
+  float *x[2];
+  void *scratch[2];
+  for (int a = 0; a < 2; a++) {
+    Axis &A = ax_[a];
+    m[a] = CsrDev{n_, A.starts, A.cols, A.vals};
+    b[a] = A.rhs;
+    x[a] = A.x;
+    scratch[a] = (char *)scratch_ + a * scratch_bytes_;
+  }
   if (spmv_form_ < 0) {
-    CK(bicgstab_pick_spmv(m, A.x, scratch_, s_, &spmv_form_));
+    CK(bicgstab_pick_spmv(m[0], x[0], scratch[0], s_, &spmv_form_));
     launches += 8;
   }
-  cudaError_t e = bicgstab_solve(m, A.rhs, A.x, max_iters, scratch_, s_, &r, spmv_form_);
-  launches += 4 + (int64_t)r.iterations * 7;
-  d2h_bytes += (int64_t)(r.iterations + 2) * 64;
-  out.solve = r;
+  BicgResult r[2]{};
+  cudaError_t e = bicgstab_solve_pair(m, b, x, max_iters, scratch, s_, r, spmv_form_);
+  const int iters = std::max(r[0].iterations, r[1].iterations);
+  launches += 10 + (int64_t)iters * 7;
+  d2h_bytes += (int64_t)(iters / 8 + 2) * 2 * 120;
+  out[0].solve = r[0];
+  out[1].solve = r[1];
   return e;
 }
 

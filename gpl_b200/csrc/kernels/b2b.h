@@ -48,8 +48,8 @@ class IpDevice {
   // `updatePinInfo` then `createSparseMatrix` for both axes, each collapsed to CSR
   // (`Csr::from_triplets`), with its right-hand side and start vector.
   cudaError_t assemble(IpAxisResult out[2]);
-  // One axis's BiCGSTAB (src/bicgstab.rs:615-669).
-  cudaError_t solve(int axis, int max_iters, IpAxisResult &out);
+  // Both axes' BiCGSTAB (src/bicgstab.rs:615-669), solved side by side.
+  cudaError_t solve(int max_iters, IpAxisResult out[2]);
   // The report's HPWL over the database boxes (src/initial_place.rs:359-386).
   cudaError_t hpwl(int64_t *out);
   // `updateCoordi` (src/initial_place.rs:391-417) from both solutions.

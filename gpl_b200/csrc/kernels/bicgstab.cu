@@ -44,7 +44,7 @@ __device__ __forceinline__ double loop_state(const double *S) {
 constexpr int kSpmvTile = 6144;
 constexpr int kSpmvUnroll = 4;
 
-__global__ void __launch_bounds__(kThreads) k_spmv_rows(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
+__device__ __forceinline__ void spmv_rows_body(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
   if (gated_off(S, gate)) return;
   const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
   if (i >= n) return;
@@ -53,8 +53,9 @@ __global__ void __launch_bounds__(kThreads) k_spmv_rows(int64_t n, const int64_t
   for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, __fmul_rn(vals[k], x[cols[k]]));
   y[i] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
 }
+__global__ void __launch_bounds__(kThreads) k_spmv_rows(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) { spmv_rows_body(n, rs, cols, vals, x, y, S, gate); }
 
-__global__ void __launch_bounds__(kThreads) k_spmv_tiled(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
+__device__ __forceinline__ void spmv_tiled_body(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
   if (gated_off(S, gate)) return;
   __shared__ float prod[kSpmvTile];
   const int64_t r0 = blockIdx.x * (int64_t)kThreads;
@@ -100,6 +101,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_tiled(int64_t n, const int64_
   }
   y[i] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
 }
+__global__ void __launch_bounds__(kThreads) k_spmv_tiled(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) { spmv_tiled_body(n, rs, cols, vals, x, y, S, gate); }
 
 static void spmv_launch(int form, int eb, cudaStream_t st, const CsrDev &A, const float *in, float *o, const double *S, int gate) {
   if (form == kSpmvTiled)
@@ -165,7 +167,7 @@ __device__ bool last_block(unsigned int *ticket) {
 
 // Up to three dot products at once; partials[blk * 3 + j]. With which >= 0 the last block to
 // finish also takes that scalar step (one launch fewer than a separate k_scalar).
-__global__ void k_dots(int64_t n, const float *__restrict__ a0, const float *__restrict__ b0, const float *__restrict__ a1, const float *__restrict__ b1, const float *__restrict__ a2, const float *__restrict__ b2, double *__restrict__ part, double *__restrict__ S, int gate, int which, unsigned int *ticket) {
+__device__ __forceinline__ void dots_body(int64_t n, const float *__restrict__ a0, const float *__restrict__ b0, const float *__restrict__ a1, const float *__restrict__ b1, const float *__restrict__ a2, const float *__restrict__ b2, double *__restrict__ part, double *__restrict__ S, int gate, int which, unsigned int *ticket) {
   if (gated_off(S, gate)) return;
   __shared__ double sh[kThreads / 32];
   double s0 = 0, s1 = 0, s2 = 0;
@@ -184,6 +186,7 @@ __global__ void k_dots(int64_t n, const float *__restrict__ a0, const float *__r
   }
   if (which >= 0 && last_block(ticket)) scalar_step(part, gridDim.x, S, which, 0, sh);
 }
+__global__ void k_dots(int64_t n, const float *__restrict__ a0, const float *__restrict__ b0, const float *__restrict__ a1, const float *__restrict__ b1, const float *__restrict__ a2, const float *__restrict__ b2, double *__restrict__ part, double *__restrict__ S, int gate, int which, unsigned int *ticket) { dots_body(n, a0, b0, a1, b1, a2, b2, part, S, gate, which, ticket); }
 
 __global__ void k_scalar(const double *__restrict__ part, int nblk, double *__restrict__ S, int which, int dst0, int gate) {
   if (gated_off(S, gate)) return;
@@ -215,7 +218,7 @@ __global__ void k_residual(int64_t n, const float *__restrict__ b, const float *
 }
 
 // p = r + beta (p - w v), beta = (rho / rho_old) (alpha / w)
-__global__ void k_update_p(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ p) {
+__device__ __forceinline__ void update_p_body(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ p) {
   if (gated_off(S, kLive)) return;
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -223,18 +226,20 @@ __global__ void k_update_p(int64_t n, const double *__restrict__ S, const float 
   float w = (float)S[S_W];
   p[i] = __fadd_rn(r[i], __fmul_rn(beta, __fsub_rn(p[i], __fmul_rn(w, v[i]))));
 }
+__global__ void k_update_p(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ p) { update_p_body(n, S, r, v, p); }
 
-__global__ void k_update_s(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ s) {
+__device__ __forceinline__ void update_s_body(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ s) {
   if (gated_off(S, kLive)) return;
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
   float a = (float)S[S_ALPHA];
   s[i] = __fsub_rn(r[i], __fmul_rn(a, v[i]));
 }
+__global__ void k_update_s(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ s) { update_s_body(n, S, r, v, s); }
 
 // x += alpha p + w s; r = s - w t; partials of |r|^2 and r0.r, the last block taking the
 // iteration's end (scalar step 3)
-__global__ void k_update_xr(int64_t n, double *__restrict__ S, const float *__restrict__ p, const float *__restrict__ s, const float *__restrict__ t, const float *__restrict__ r0, float *__restrict__ x, float *__restrict__ r, double *__restrict__ part, unsigned int *ticket) {
+__device__ __forceinline__ void update_xr_body(int64_t n, double *__restrict__ S, const float *__restrict__ p, const float *__restrict__ s, const float *__restrict__ t, const float *__restrict__ r0, float *__restrict__ x, float *__restrict__ r, double *__restrict__ part, unsigned int *ticket) {
   if (gated_off(S, kLive)) return;
   __shared__ double sh[kThreads / 32];
   float a = (float)S[S_ALPHA], w = (float)S[S_W];
@@ -255,6 +260,56 @@ __global__ void k_update_xr(int64_t n, double *__restrict__ S, const float *__re
   }
   if (last_block(ticket)) scalar_step(part, gridDim.x, S, 3, 0, sh);  // the iteration's end
 }
+__global__ void k_update_xr(int64_t n, double *__restrict__ S, const float *__restrict__ p, const float *__restrict__ s, const float *__restrict__ t, const float *__restrict__ r0, float *__restrict__ x, float *__restrict__ r, double *__restrict__ part, unsigned int *ticket) { update_xr_body(n, S, p, s, t, r0, x, r, part, ticket); }
+
+// Both axes' systems in one launch (blockIdx.y picks the system): the initial placement solves
+// its x and y systems side by side, so each launch carries twice the work and the loop half
+// the launches. Each system keeps its own scalars, state and arrival count, so every one
+// takes exactly the steps it would take alone.
+struct SysDev {
+  int64_t n;
+  const int64_t *rs;
+  const int32_t *cols;
+  const float *vals;
+  float *x, *r, *r0, *v, *p, *s, *t;
+  double *part, *S;
+  unsigned int *ticket;
+};
+struct SysPair {
+  SysDev a[2];
+};
+__device__ __forceinline__ SysDev pick(const SysPair &P) { return blockIdx.y ? P.a[1] : P.a[0]; }
+
+__global__ void __launch_bounds__(kThreads) k2_update_p(SysPair P) {
+  SysDev q = pick(P);
+  update_p_body(q.n, q.S, q.r, q.v, q.p);
+}
+// sel 0: v = A p; sel 1: t = A s
+__global__ void __launch_bounds__(kThreads) k2_spmv_rows(SysPair P, int sel) {
+  SysDev q = pick(P);
+  spmv_rows_body(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
+}
+__global__ void __launch_bounds__(kThreads) k2_spmv_tiled(SysPair P, int sel) {
+  SysDev q = pick(P);
+  spmv_tiled_body(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
+}
+// sel 0: r0.v, then alpha; sel 1: t.t and t.s, then omega
+__global__ void k2_dots(SysPair P, int sel) {
+  SysDev q = pick(P);
+  if (sel == 0)
+    dots_body(q.n, q.r0, q.v, nullptr, nullptr, nullptr, nullptr, q.part, q.S, kLive, 1, q.ticket);
+  else
+    dots_body(q.n, q.t, q.t, q.t, q.s, nullptr, nullptr, q.part, q.S, kLive, 2, q.ticket);
+}
+__global__ void __launch_bounds__(kThreads) k2_update_s(SysPair P) {
+  SysDev q = pick(P);
+  update_s_body(q.n, q.S, q.r, q.v, q.s);
+}
+__global__ void k2_update_xr(SysPair P) {
+  SysDev q = pick(P);
+  update_xr_body(q.n, q.S, q.p, q.s, q.t, q.r0, q.x, q.r, q.part, q.ticket);
+}
+__global__ void k_set_ended(double *S) { S[S_STATE] = kEnded; }
 
 __global__ void k_fill(int64_t n, float *a, float v) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -384,6 +439,120 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
   out->iterations = (int)hs[S_I];
   out->error = (float)std::sqrt(rr / rhs_sqnorm);
   out->converged = out->error <= tol;
+  return cudaGetLastError();
+}
+
+cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], float *const x[2], int max_iters, void *const scratch[2], cudaStream_t st, BicgResult out[2], int form) {
+  const int64_t n = A[0].n;
+  if (A[1].n != n) return cudaErrorInvalidValue;
+  const size_t vec = ((size_t)n * sizeof(float) + 255) / 256 * 256;
+  SysPair P{};
+  for (int a = 0; a < 2; a++) {
+    char *base = (char *)scratch[a];
+    SysDev &q = P.a[a];
+    q.n = n;
+    q.rs = A[a].rs;
+    q.cols = A[a].cols;
+    q.vals = A[a].vals;
+    q.x = x[a];
+    q.r = (float *)base;
+    q.r0 = (float *)(base + vec);
+    q.v = (float *)(base + 2 * vec);
+    q.p = (float *)(base + 3 * vec);
+    q.s = (float *)(base + 4 * vec);
+    q.t = (float *)(base + 5 * vec);
+    q.part = (double *)(base + 7 * vec);
+    q.S = q.part + (size_t)kBicgBlocks * 3;
+    q.ticket = (unsigned int *)(q.S + S_TICKET);
+  }
+  auto ax_of = [&](int a) { return (float *)((char *)scratch[a] + 6 * vec); };
+  int eb = (int)((n + kThreads - 1) / kThreads);
+  if (eb < 1) eb = 1;
+  const int rb = kBicgBlocks;
+  const float tol = 1.1920929e-07f;
+  double hs[2][S_END];
+  auto pull = [&]() -> cudaError_t {
+    for (int a = 0; a < 2; a++) {
+      cudaError_t e = cudaMemcpyAsync(hs[a], P.a[a].S, sizeof hs[a], cudaMemcpyDeviceToHost, st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaStreamSynchronize(st);
+  };
+  auto restart = [&](int a, bool first) {
+    // too orthogonal to r0: restart from the current residual (that system alone)
+    const SysDev &q = P.a[a];
+    spmv_launch(form, eb, st, A[a], q.x, ax_of(a), q.S, kAlways);
+    k_residual<<<eb, kThreads, 0, st>>>(n, b[a], ax_of(a), q.r, q.r0, q.S, kAlways);
+    k_dots<<<rb, kThreads, 0, st>>>(n, q.r, q.r, nullptr, nullptr, nullptr, nullptr, q.part, q.S, kAlways, -1, q.ticket);
+    k_scalar<<<1, kThreads, 0, st>>>(q.part, rb, q.S, 4, 0, kAlways);
+    k_restart_done<<<1, 1, 0, st>>>(q.S, first ? 1 : 0);
+  };
+  cudaError_t e;
+  // each system's start, as the single solve takes it
+  for (int a = 0; a < 2; a++) {
+    const SysDev &q = P.a[a];
+    spmv_launch(form, eb, st, A[a], q.x, ax_of(a), q.S, kAlways);
+    k_residual<<<eb, kThreads, 0, st>>>(n, b[a], ax_of(a), q.r, q.r0, q.S, kAlways);
+    cudaMemsetAsync(q.ticket, 0, sizeof(unsigned int), st);
+    k_dots<<<rb, kThreads, 0, st>>>(n, q.r0, q.r0, b[a], b[a], q.r0, q.r, q.part, q.S, kAlways, -1, q.ticket);
+    k_scalar<<<1, kThreads, 0, st>>>(q.part, rb, q.S, 0, S_R0SQ, kAlways);
+  }
+  if ((e = pull()) != cudaSuccess) return e;
+  double rhs_sqnorm[2];
+  bool live[2];
+  for (int a = 0; a < 2; a++) {
+    const SysDev &q = P.a[a];
+    rhs_sqnorm[a] = hs[a][S_BB];
+    live[a] = rhs_sqnorm[a] != 0.0;
+    if (!live[a]) {
+      k_fill<<<eb, kThreads, 0, st>>>(n, q.x, 0.0f);
+      k_set_ended<<<1, 1, 0, st>>>(q.S);
+      out[a].iterations = max_iters;
+      out[a].error = tol;
+      out[a].converged = true;
+      continue;
+    }
+    k_scal_init<<<1, 1, 0, st>>>(q.S);
+    cudaMemsetAsync(q.v, 0, (size_t)n * sizeof(float), st);
+    cudaMemsetAsync(q.p, 0, (size_t)n * sizeof(float), st);
+    double tol2 = (double)tol * (double)tol * rhs_sqnorm[a];
+    double eps2 = (double)tol * (double)tol;
+    k_loop_init<<<1, 1, 0, st>>>(q.S, tol2, eps2, max_iters);
+  }
+  if (!live[0] && !live[1]) return cudaGetLastError();
+  // both systems' iterations in each launch; the bound on batches is the single solve's
+  const int64_t max_batches = 2 * (int64_t)max_iters + 3;
+  int64_t batches = 0;
+  int restarts[2] = {0, 0};
+  const dim3 ge(eb, 2), gr(rb, 2);
+  for (;;) {
+    for (int k = 0; k < kBicgBatch; k++) {
+      k2_update_p<<<ge, kThreads, 0, st>>>(P);
+      if (form == kSpmvTiled)
+        k2_spmv_tiled<<<ge, kThreads, 0, st>>>(P, 0);
+      else
+        k2_spmv_rows<<<ge, kThreads, 0, st>>>(P, 0);
+      k2_dots<<<gr, kThreads, 0, st>>>(P, 0);
+      k2_update_s<<<ge, kThreads, 0, st>>>(P);
+      if (form == kSpmvTiled)
+        k2_spmv_tiled<<<ge, kThreads, 0, st>>>(P, 1);
+      else
+        k2_spmv_rows<<<ge, kThreads, 0, st>>>(P, 1);
+      k2_dots<<<gr, kThreads, 0, st>>>(P, 1);
+      k2_update_xr<<<gr, kThreads, 0, st>>>(P);
+    }
+    if ((e = pull()) != cudaSuccess) return e;
+    if (hs[0][S_STATE] == kEnded && hs[1][S_STATE] == kEnded) break;
+    if (++batches > max_batches) return cudaErrorUnknown;  // cannot happen: the single solve's count
+    for (int a = 0; a < 2; a++)
+      if (hs[a][S_STATE] == kRestart) restart(a, restarts[a]++ == 0);
+  }
+  for (int a = 0; a < 2; a++) {
+    if (!live[a]) continue;
+    out[a].iterations = (int)hs[a][S_I];
+    out[a].error = (float)std::sqrt(hs[a][S_RR] / rhs_sqnorm[a]);
+    out[a].converged = out[a].error <= tol;
+  }
   return cudaGetLastError();
 }
 

@@ -3,6 +3,7 @@
 #include <cstring>
 #include <numeric>
 
+#include "../kernels/b2b.h"
 #include "../kernels/bicgstab.h"
 #include "../kernels/engine_kernels.h"
 #include "engine.h"
@@ -59,6 +60,8 @@ void Engine::check(cudaError_t e, const char *where) {
 
 Engine::Engine(int device) : device_(device) {
   check(cudaSetDevice(device), "cudaSetDevice");
+  // device buffers come from the device's pool, which keeps freed memory for the next run
+  if (!failed()) keep_device_pool();
   // the trial's own stream at the highest priority and the WA's beside it at the lowest: when
   // both have blocks waiting, an SM that frees up takes the density solve's first
   int prio_lo = 0, prio_hi = 0;
@@ -86,15 +89,15 @@ Engine::~Engine() {
 }
 
 template <class T>
-static cudaError_t dmalloc(T **p, size_t n) {
+static cudaError_t dmalloc(T **p, size_t n, cudaStream_t s) {
   *p = nullptr;
   if (n == 0) n = 1;
-  return cudaMalloc((void **)p, n * sizeof(T));
+  return cudaMallocAsync((void **)p, n * sizeof(T), s);  // from the device's pool (kept)
 }
 static int64_t g_h2d = 0;  // bytes the uploads below copied (folded into the engine's counter)
 template <class T>
 static cudaError_t upload_vec(T **p, const std::vector<T> &v, cudaStream_t s) {
-  cudaError_t e = dmalloc(p, v.size());
+  cudaError_t e = dmalloc(p, v.size(), s);
   if (e != cudaSuccess || v.empty()) return e;
   g_h2d += (int64_t)(v.size() * sizeof(T));
   return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
@@ -104,7 +107,7 @@ static cudaError_t upload_vec(T **p, const std::vector<T> &v, cudaStream_t s) {
 void Engine::free_globals() {
   void *ptrs[] = {dc_, hx_, hy_, dscale_, area_, kind_, locked_, cell_pin_start_, net_start_, pin_cell_, pin_slot_, big_nets_, pin_base_, tiles_, net_weight_, pin_grad_, hpwl_acc_, dev_scal_};
   for (void *p : ptrs)
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, stream_);
   dc_ = nullptr;
   hx_ = hy_ = nullptr;
   dscale_ = area_ = nullptr;
@@ -126,9 +129,9 @@ void Engine::release() {
   for (Region *r : regions_) {
     void *ptrs[] = {r->bx, r->by, r->scaled, r->density, r->fx, r->fy, r->np, r->npu, r->acc_inst, r->acc_fill, r->part, r->ticket};
     for (void *p : ptrs)
-      if (p) cudaFree(p);
+      if (p) cudaFreeAsync(p, stream_);
     for (int k = 0; k < S_NUM; k++)
-      if (r->slot[k]) cudaFree(r->slot[k]);
+      if (r->slot[k]) cudaFreeAsync(r->slot[k], stream_);
     poisson_plan_destroy(r->plan);
     delete r;
   }
@@ -215,9 +218,9 @@ void Engine::upload(const EngineSetup &s) {
     unit_weights_ = std::all_of(wt.begin(), wt.end(), [](float v) { return v == 1.0f; });
   }
   progress("  upload: cells, nets and pins");
-  check(dmalloc(&pin_grad_, s.cell_pins.size()), "alloc pins");
-  check(dmalloc(&hpwl_acc_, 1), "alloc");
-  check(dmalloc(&dev_scal_, s.regions.size()), "alloc");
+  check(dmalloc(&pin_grad_, s.cell_pins.size(), st), "alloc pins");
+  check(dmalloc(&hpwl_acc_, 1, st), "alloc");
+  check(dmalloc(&dev_scal_, s.regions.size(), st), "alloc");
   host_scal_.assign(s.regions.size(), RegionScalars{});
   {
     size_t need = s.regions.size() * sizeof(RegionScalars) + sizeof(unsigned long long);
@@ -246,23 +249,23 @@ void Engine::upload(const EngineSetup &s) {
     check(upload_vec(&r->scaled, rs.scaled, st), "upload bins");
     check(upload_vec(&r->np, as_float(rs.non_place), st), "upload bins");
     check(upload_vec(&r->npu, as_float(rs.non_place_u), st), "upload bins");
-    check(dmalloc(&r->acc_inst, nb), "alloc bins");
-    check(dmalloc(&r->acc_fill, nb), "alloc bins");
-    check(dmalloc(&r->density, nb), "alloc bins");
-    check(dmalloc(&r->fx, nb), "alloc bins");
-    check(dmalloc(&r->fy, nb), "alloc bins");
+    check(dmalloc(&r->acc_inst, nb, st), "alloc bins");
+    check(dmalloc(&r->acc_fill, nb, st), "alloc bins");
+    check(dmalloc(&r->density, nb, st), "alloc bins");
+    check(dmalloc(&r->fx, nb, st), "alloc bins");
+    check(dmalloc(&r->fy, nb, st), "alloc bins");
     if (!failed()) {
       check(cudaMemsetAsync(r->acc_inst, 0, nb * sizeof(int64_t), st), "memset");
       check(cudaMemsetAsync(r->acc_fill, 0, nb * sizeof(int64_t), st), "memset");
     }
     for (int k = 0; k < S_NUM; k++) {
-      check(dmalloc(&r->slot[k], rs.n_cells), "alloc slots");
+      check(dmalloc(&r->slot[k], rs.n_cells, st), "alloc slots");
       if (!failed()) check(cudaMemsetAsync(r->slot[k], 0, std::max<int64_t>(rs.n_cells, 1) * sizeof(float2), st), "memset");
     }
     r->nb_bins = rs.nx;  // the bin finalize runs one block per x row
     r->nb_cells = blocks_for(rs.n_cells);
-    check(dmalloc(&r->part, (size_t)std::max(r->nb_bins * 2, r->nb_cells * 4)), "alloc partials");
-    check(dmalloc(&r->ticket, 1), "alloc partials");
+    check(dmalloc(&r->part, (size_t)std::max(r->nb_bins * 2, r->nb_cells * 4), st), "alloc partials");
+    check(dmalloc(&r->ticket, 1, st), "alloc partials");
     if (!failed()) check(cudaMemsetAsync(r->ticket, 0, sizeof(unsigned int), st), "memset");
     if (!failed()) {
       cudaError_t pe = cudaSuccess;

@@ -2383,21 +2383,25 @@ static void reset_counters(Engine &e) {
 int gpl_global_placement(gpl_ctx *ctx, const gpl_design_t *cd, int argc, const char *const *argv, const gpl_router_t *router, gpl_result_t *out) {
   ctx->eng->set_poisson_mode(ctx->poisson_mode);
   reset_counters(*ctx->eng);
-  Run run(*ctx->eng);
-  run.res.log.trace_on = ctx->trace;
-  guarded(run.res, [&] {
+  auto run = std::make_unique<Run>(*ctx->eng);
+  run->res.log.trace_on = ctx->trace;
+  guarded(run->res, [&] {
     progress("command start");
-    run.d = design_from_c(cd);
-    progress("design read: %zu instances, %zu nets", run.d.insts.size(), run.d.nets.size());
-    run.open(std::vector<std::string>(argv, argv + argc), router);
-    run.close();
+    run->d = design_from_c(cd);
+    progress("design read: %zu instances, %zu nets", run->d.insts.size(), run->d.nets.size());
+    run->open(std::vector<std::string>(argv, argv + argc), router);
+    run->close();
     progress("command done");
   });
-  run.res.h2d = ctx->eng->h2d_bytes + run.res.locations.size() * 0;
-  run.res.d2h = ctx->eng->d2h_bytes;
-  run.res.launches = ctx->eng->launches;
+  run->res.h2d = ctx->eng->h2d_bytes;
+  run->res.d2h = ctx->eng->d2h_bytes;
+  run->res.launches = ctx->eng->launches;
   ctx->eng->release();
-  fill_result(run.res, out);
+  progress("device memory released");
+  fill_result(run->res, out);
+  progress("result written");
+  run.reset();
+  progress("host state released");
   return out->status;
 }
 

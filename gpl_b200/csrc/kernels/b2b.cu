@@ -554,14 +554,26 @@ __global__ void k_db_hpwl(int32_t n_nets, const int64_t *net_start, const int32_
 
 unsigned grid(int64_t n) { return (unsigned)std::max<int64_t>(1, (n + kThreads - 1) / kThreads); }
 
+// The initial placement's buffers come from the device's stream-ordered pool, which keeps
+// what they free (the release threshold is raised once per device): freeing a few GB at the
+// end of the initial placement then costs no unmapping, and the next run reuses the memory.
+void keep_pool_once() {
+  static bool kept[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 || kept[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+  uint64_t keep = UINT64_MAX;
+  if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess) kept[dev] = true;
+}
 template <class T>
-cudaError_t alloc(T **p, size_t n) {
+cudaError_t alloc(T **p, size_t n, cudaStream_t s) {
   *p = nullptr;
-  return cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+  return cudaMallocAsync((void **)p, std::max<size_t>(n, 1) * sizeof(T), s);
 }
 template <class T>
 cudaError_t put(T **p, const std::vector<T> &v, cudaStream_t s, int64_t &bytes) {
-  cudaError_t e = alloc(p, v.size());
+  cudaError_t e = alloc(p, v.size(), s);
   if (e != cudaSuccess || v.empty()) return e;
   bytes += (int64_t)(v.size() * sizeof(T));
   return cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
@@ -569,14 +581,14 @@ cudaError_t put(T **p, const std::vector<T> &v, cudaStream_t s, int64_t &bytes) 
 
 // Grows a set of buffers to hold n entries each.
 template <class... T>
-cudaError_t grow(size_t n, size_t &cap, T **...bufs) {
+cudaError_t grow(cudaStream_t s, size_t n, size_t &cap, T **...bufs) {
   if (n <= cap) return cudaSuccess;
   size_t c = (size_t)(n * 1.1) + 16;
   cudaError_t e = cudaSuccess;
   auto one = [&](auto **p) {
-    if (*p) cudaFree(*p);
+    if (*p) cudaFreeAsync(*p, s);
     *p = nullptr;
-    if (e == cudaSuccess) e = alloc(p, c);
+    if (e == cudaSuccess) e = alloc(p, c, s);
   };
   (one(bufs), ...);
   cap = e == cudaSuccess ? c : 0;
@@ -597,11 +609,11 @@ void IpDevice::release() {
   void *ptrs[] = {box_, clamp_, db_box_, pin_static_, db_size_, pin_off_, pin_xy_, locked_, grouped_, pin_mio_, pin_hp_, pin_flag_, pin_e_, pin_inst_, locked_rank_,
                   net_start_, cnt_, scan_tmp_, t_row_, t_col_, t_val_, r_row_, r_val_, bucket_, fill_, row_off_, ucount_, ucol_, uval_, scratch_, hpwl_acc_, tier_rows_, tier_n_};
   for (void *p : ptrs)
-    if (p) cudaFree(p);
+    if (p) cudaFreeAsync(p, s_);
   for (auto &a : ax_) {
     void *q[] = {a.starts, a.cols, a.vals, a.rhs, a.x};
     for (void *p : q)
-      if (p) cudaFree(p);
+      if (p) cudaFreeAsync(p, s_);
     a = Axis{};
   }
   box_ = clamp_ = db_box_ = pin_static_ = nullptr;
@@ -621,6 +633,7 @@ void IpDevice::release() {
 
 cudaError_t IpDevice::upload(const IpSetup &s) {
   release();
+  keep_pool_once();
   cfg_.max_fanout = s.max_fanout;
   cfg_.min_diff = s.min_diff;
   cfg_.weight_scale = s.weight_scale;
@@ -648,32 +661,32 @@ cudaError_t IpDevice::upload(const IpSetup &s) {
   CK(put(&pin_hp_, s.pin_hp, s_, b));
   CK(put(&pin_static_, s.pin_static, s_, b));
   CK(put(&net_start_, s.net_start, s_, b));
-  CK(alloc(&pin_flag_, n_pins_));
-  CK(alloc(&cnt_, 4 * ((size_t)n_nets_ + 1)));
-  CK(alloc(&row_off_, n_ + 1));
-  CK(alloc(&ucount_, n_ + 1));
+  CK(alloc(&pin_flag_, n_pins_, s_));
+  CK(alloc(&cnt_, 4 * ((size_t)n_nets_ + 1), s_));
+  CK(alloc(&row_off_, n_ + 1, s_));
+  CK(alloc(&ucount_, n_ + 1, s_));
   CK(cudaFuncSetAttribute(k_row_collapse_block, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
-  CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1)));
-  CK(alloc(&tier_n_, 3));
-  CK(alloc(&fill_, n_));
-  CK(alloc(&hpwl_acc_, 1));
+  CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1), s_));
+  CK(alloc(&tier_n_, 3, s_));
+  CK(alloc(&fill_, n_, s_));
+  CK(alloc(&hpwl_acc_, 1, s_));
   for (auto &a : ax_) {
-    CK(alloc(&a.starts, n_ + 1));
-    CK(alloc(&a.rhs, n_));
-    CK(alloc(&a.x, n_));
+    CK(alloc(&a.starts, n_ + 1, s_));
+    CK(alloc(&a.rhs, n_, s_));
+    CK(alloc(&a.x, n_, s_));
   }
   // the two axes' solver scratch, side by side (256-byte aligned halves)
   scratch_bytes_ = (bicgstab_scratch_bytes(n_) + 255) / 256 * 256;
-  CK(cudaMalloc(&scratch_, 2 * scratch_bytes_));
+  CK(cudaMallocAsync(&scratch_, 2 * scratch_bytes_, s_));
   return cudaStreamSynchronize(s_);
 }
 
 cudaError_t IpDevice::scan(int64_t *data, int64_t n) {
   int64_t nb = (n + kScanBlock - 1) / kScanBlock;
   if ((size_t)(nb + 1) > scan_tmp_n_) {
-    if (scan_tmp_) cudaFree(scan_tmp_);
+    if (scan_tmp_) cudaFreeAsync(scan_tmp_, s_);
     scan_tmp_n_ = (size_t)(nb + 1);
-    CK(alloc(&scan_tmp_, scan_tmp_n_));
+    CK(alloc(&scan_tmp_, scan_tmp_n_, s_));
   }
   if (nb == 0) return cudaMemsetAsync(data, 0, sizeof(int64_t), s_);
   k_scan_block<<<(unsigned)nb, kScanBlock, 0, s_>>>(data, n, scan_tmp_);
@@ -710,13 +723,13 @@ cudaError_t IpDevice::collapse(int64_t n_trip, const int32_t *row, const int32_t
   CK(cudaStreamSynchronize(s_));
   d2h_bytes += 8;
   if ((size_t)*nnz > *cap) {
-    if (*cols) cudaFree(*cols);
-    if (*vals) cudaFree(*vals);
+    if (*cols) cudaFreeAsync(*cols, s_);
+    if (*vals) cudaFreeAsync(*vals, s_);
     *cols = nullptr;
     *vals = nullptr;
     *cap = (size_t)(*nnz * 1.25) + 16;
-    CK(alloc(cols, *cap));
-    CK(alloc(vals, *cap));
+    CK(alloc(cols, *cap, s_));
+    CK(alloc(vals, *cap, s_));
   }
   if (n_) k_row_fill<<<grid(n_), kThreads, 0, s_>>>(n_, row_off_, starts_out, ucol_, uval_, *cols, *vals);
   launches += 1;
@@ -725,14 +738,15 @@ cudaError_t IpDevice::collapse(int64_t n_trip, const int32_t *row, const int32_t
 
 cudaError_t IpDevice::csr_from_triplets(int64_t n, int64_t nt, const int32_t *row, const int32_t *col, const float *val, int64_t *starts, int32_t *cols, float *vals, int64_t *nnz) {
   release();
+  keep_pool_once();
   n_ = n;
   CK(cudaFuncSetAttribute(k_row_collapse_block, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
-  CK(alloc(&row_off_, n_ + 1));
-  CK(alloc(&ucount_, n_ + 1));
-  CK(alloc(&fill_, n_));
-  CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1)));
-  CK(alloc(&tier_n_, 3));
-  CK(grow((size_t)std::max<int64_t>(nt, 1), w_cap_, &bucket_, &ucol_, &uval_));
+  CK(alloc(&row_off_, n_ + 1, s_));
+  CK(alloc(&ucount_, n_ + 1, s_));
+  CK(alloc(&fill_, n_, s_));
+  CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1), s_));
+  CK(alloc(&tier_n_, 3, s_));
+  CK(grow(s_, (size_t)std::max<int64_t>(nt, 1), w_cap_, &bucket_, &ucol_, &uval_));
   size_t cap = (size_t)std::max<int64_t>(nt, 1);  // nnz <= nt: the caller's buffers suffice
   int32_t *c = cols;
   float *v = vals;
@@ -769,9 +783,9 @@ cudaError_t IpDevice::assemble(IpAxisResult out[2]) {
   // both axes side by side: x's triplets (the locked diagonal first) then y's; the same
   // for the right-hand-side terms
   const int64_t nt[2] = {n_locked_ + tot[0], n_locked_ + tot[1]}, nr[2] = {tot[2], tot[3]};
-  CK(grow((size_t)(nt[0] + nt[1]), t_cap_, &t_row_, &t_col_, &t_val_));
-  CK(grow((size_t)(nr[0] + nr[1]), r_cap_, &r_row_, &r_val_));
-  CK(grow((size_t)std::max({nt[0], nt[1], nr[0], nr[1]}), w_cap_, &bucket_, &ucol_, &uval_));
+  CK(grow(s_, (size_t)(nt[0] + nt[1]), t_cap_, &t_row_, &t_col_, &t_val_));
+  CK(grow(s_, (size_t)(nr[0] + nr[1]), r_cap_, &r_row_, &r_val_));
+  CK(grow(s_, (size_t)std::max({nt[0], nt[1], nr[0], nr[1]}), w_cap_, &bucket_, &ucol_, &uval_));
   AxisOut ox{}, oy{};
   ox.t_row = t_row_, ox.t_col = t_col_, ox.t_val = t_val_;
   oy.t_row = t_row_ + nt[0], oy.t_col = t_col_ + nt[0], oy.t_val = t_val_ + nt[0];
@@ -867,5 +881,7 @@ cudaError_t IpDevice::download(std::vector<int4> &box, std::vector<int4> &db_box
   d2h_bytes += n_ * 32;
   return cudaStreamSynchronize(s_);
 }
+
+void keep_device_pool() { keep_pool_once(); }
 
 }  // namespace gpl

@@ -35,6 +35,11 @@ struct IpSetup {
   float weight_scale = 800.0f;
 };
 
+// Raises the current device's stream-ordered pool's release threshold (once per device), so
+// memory freed with cudaFreeAsync stays in the pool for the next allocation instead of being
+// unmapped.
+void keep_device_pool();
+
 struct IpAxisResult {
   int64_t triplets = 0;  // triplets assembled (the locked diagonal included)
   BicgResult solve{};

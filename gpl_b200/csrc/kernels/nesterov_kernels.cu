@@ -534,7 +534,7 @@ void launch_wa_tiles(const WaArgs &w, float cx, float cy, cudaStream_t s) {
 // the ordered sums; larger cells walk their bins.
 constexpr int kGradPinTile = 2048;
 
-__global__ void __launch_bounds__(kThreads, 5) k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials, unsigned int *ticket, double *out) {
+__global__ void __launch_bounds__(kThreads, 6) k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials, unsigned int *ticket, double *out) {
   __shared__ double4 sh[kThreads / 32];
   __shared__ float2 s_pg[kGradPinTile];
   const int i0 = blockIdx.x * blockDim.x;

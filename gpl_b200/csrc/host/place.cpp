@@ -203,47 +203,52 @@ Design design_from_c(const gpl_design_t *c) {
   d.core = rect4(c->core);
   for (int r = 0; r < c->n_rows; r++) d.rows.push_back(RowRec{rect4(c->row_box + 4 * r), c->row_pad[r] != 0, c->row_site[2 * r], c->row_site[2 * r + 1]});
   d.insts.resize(c->n_insts);
-  for (int k = 0; k < c->n_insts; k++) {
-    DbInst &i = d.insts[k];
-    // names the caller did not give are generated when a message needs them (inst_label)
-    if (c->inst_name) i.name = c->inst_name[k];
-    if (c->inst_master_name) i.master = c->inst_master_name[k];
-    uint32_t f = c->inst_flags[k];
-    i.core_auto_placeable = f & GPL_INST_CORE_AUTO_PLACEABLE;
-    i.master_is_block = f & GPL_INST_BLOCK;
-    i.fixed = f & GPL_INST_FIXED;
-    i.placed = f & GPL_INST_PLACED;
-    i.bbox = rect4(c->inst_box + 4 * k);
-    i.group = c->inst_group ? c->inst_group[k] : -1;
-    i.has_halo = (f & GPL_INST_HAS_HALO) && c->inst_halo;
-    if (i.has_halo) i.halo = rect4(c->inst_halo + 4 * k);
-    i.signal_pins = c->inst_signal_pins[k];
-    i.orient = c->inst_orient ? c->inst_orient[k] : GPL_R0;
-    i.master_w = c->inst_master[2 * k];
-    i.master_h = c->inst_master[2 * k + 1];
-  }
+  parallel_for((size_t)std::max(c->n_insts, 0), [&](size_t k0, size_t k1) {
+    for (int k = (int)k0; k < (int)k1; k++) {
+      DbInst &i = d.insts[k];
+      // names the caller did not give are generated when a message needs them (inst_label)
+      if (c->inst_name) i.name = c->inst_name[k];
+      if (c->inst_master_name) i.master = c->inst_master_name[k];
+      uint32_t f = c->inst_flags[k];
+      i.core_auto_placeable = f & GPL_INST_CORE_AUTO_PLACEABLE;
+      i.master_is_block = f & GPL_INST_BLOCK;
+      i.fixed = f & GPL_INST_FIXED;
+      i.placed = f & GPL_INST_PLACED;
+      i.bbox = rect4(c->inst_box + 4 * k);
+      i.group = c->inst_group ? c->inst_group[k] : -1;
+      i.has_halo = (f & GPL_INST_HAS_HALO) && c->inst_halo;
+      if (i.has_halo) i.halo = rect4(c->inst_halo + 4 * k);
+      i.signal_pins = c->inst_signal_pins[k];
+      i.orient = c->inst_orient ? c->inst_orient[k] : GPL_R0;
+      i.master_w = c->inst_master[2 * k];
+      i.master_h = c->inst_master[2 * k + 1];
+    }
+  });
   d.nets.resize(c->n_nets);
-  for (int n = 0; n < c->n_nets; n++) {
-    DbNet &net = d.nets[n];
-    if (c->net_name) net.name = c->net_name[n];
-    net.signal_or_clock = c->net_signal[n] != 0;
-    for (int64_t t = c->net_iterm_start[n]; t < c->net_iterm_start[n + 1]; t++) {
-      Term tm;
-      tm.inst = c->iterm_inst[t];
-      tm.has_shape = c->iterm_has_shape[t] != 0;
-      tm.shape = rect4(c->iterm_shape + 4 * t);
-      tm.order = c->iterm_order[t];
-      net.iterms.push_back(tm);
+  parallel_for((size_t)std::max(c->n_nets, 0), [&](size_t n0, size_t n1) {
+    for (int n = (int)n0; n < (int)n1; n++) {
+      DbNet &net = d.nets[n];
+      if (c->net_name) net.name = c->net_name[n];
+      net.signal_or_clock = c->net_signal[n] != 0;
+      net.iterms.reserve((size_t)(c->net_iterm_start[n + 1] - c->net_iterm_start[n]));
+      for (int64_t t = c->net_iterm_start[n]; t < c->net_iterm_start[n + 1]; t++) {
+        Term tm;
+        tm.inst = c->iterm_inst[t];
+        tm.has_shape = c->iterm_has_shape[t] != 0;
+        tm.shape = rect4(c->iterm_shape + 4 * t);
+        tm.order = c->iterm_order[t];
+        net.iterms.push_back(tm);
+      }
+      for (int64_t t = c->net_bterm_start[n]; t < c->net_bterm_start[n + 1]; t++) {
+        Port p;
+        p.name = c->bterm_name ? c->bterm_name[t] : sfmt("p%ld", (long)t);
+        p.has_bbox = c->bterm_flags[t] & GPL_BTERM_PLACED;
+        p.bbox = rect4(c->bterm_box + 4 * t);
+        p.fixed = c->bterm_flags[t] & GPL_BTERM_FIXED;
+        net.bterms.push_back(p);
+      }
     }
-    for (int64_t t = c->net_bterm_start[n]; t < c->net_bterm_start[n + 1]; t++) {
-      Port p;
-      p.name = c->bterm_name ? c->bterm_name[t] : sfmt("p%ld", (long)t);
-      p.has_bbox = c->bterm_flags[t] & GPL_BTERM_PLACED;
-      p.bbox = rect4(c->bterm_box + 4 * t);
-      p.fixed = c->bterm_flags[t] & GPL_BTERM_FIXED;
-      net.bterms.push_back(p);
-    }
-  }
+  });
   for (int g = 0; g < c->n_groups; g++) d.groups.push_back(Group{c->group_name ? c->group_name[g] : sfmt("g%d", g), c->group_visual_debug[g] != 0, c->group_region[g]});
   for (int r = 0; r < c->n_regions; r++) {
     Region reg;

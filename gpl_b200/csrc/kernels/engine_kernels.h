@@ -83,7 +83,6 @@ bool narrow_tile(const std::vector<int32_t> &bx, const std::vector<int32_t> &by)
 // too large for a tile, from the nets' pin starts.
 void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int4> &tiles, std::vector<int32_t> &big);
 __global__ void k_hold_locked(RegionArgs r, CellArgs c);
-__global__ void k_reduce_partials(const double *partials, int nblk, int width, double *out);
 
 // The density solver (Fft::solve without the potential): FP32 SIMT GEMMs or split-BF16
 // tcgen05 GEMMs. Workspace layout and basis matrices are the solver's own.

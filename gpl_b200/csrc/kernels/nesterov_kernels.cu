@@ -730,24 +730,13 @@ void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int4> &tiles
   close(n_nets);
 }
 
-// ---- the locked cells' next state (:2848-2859) and a deterministic reduction of partials.
+// ---- the locked cells' next state (:2848-2859).
 __global__ void k_hold_locked(RegionArgs r, CellArgs c) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r.n_cells || !c.locked || !c.locked[i] || c.kind[i] == CELL_FILLER) return;
   c.next_slp[i] = c.cur_slp[i];
   c.next_slp_sum[i] = c.cur_slp_sum[i];
   c.next[i] = c.cur[i];
-}
-
-// Sums `nblk` rows of `width` partials in a fixed order into out[0..width).
-__global__ void k_reduce_partials(const double *__restrict__ partials, int nblk, int width, double *__restrict__ out) {
-  __shared__ double sh[kThreads / 32];
-  for (int j = 0; j < width; j++) {
-    double s = 0;
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partials[(size_t)b * width + j];
-    double t = block_sum<kThreads>(s, sh);
-    if (threadIdx.x == 0) out[j] = t;
-  }
 }
 
 }  // namespace gpl

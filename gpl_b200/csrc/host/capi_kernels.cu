@@ -82,38 +82,80 @@ int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy,
 int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, const float *net_weight, float coef_x, float coef_y, float *grad, void *stream) {
   if (n_nets <= 0) return 0;
   cudaStream_t s = (cudaStream_t)stream;
-  // the engine's tiles of consecutive nets, built from the pin starts
   std::vector<int64_t> starts((size_t)n_nets + 1);
   cudaError_t e = cudaMemcpyAsync(starts.data(), net_start, starts.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return (int)e;
-  if (starts[n_nets] >= ((int64_t)1 << 31)) return (int)cudaErrorInvalidValue;  // pin numbers are 32-bit
+  const int64_t np = starts[n_nets];
+  if (np >= ((int64_t)1 << 31)) return (int)cudaErrorInvalidValue;  // pin numbers are 32-bit
+  // the nets in degree order (stable), as the engine holds them, their pins following them;
+  // each pin's force goes back to its own place (its slot is its index in the caller's order)
+  std::vector<int32_t> order((size_t)n_nets);
+  for (int64_t n = 0; n < n_nets; n++) order[n] = (int32_t)n;
+  std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return starts[x + 1] - starts[x] < starts[y + 1] - starts[y]; });
+  std::vector<int32_t> xy((size_t)np * 2), xy2((size_t)np * 2), slot((size_t)np);
+  std::vector<float> wt, wt2;
+  if (np) e = cudaMemcpyAsync(xy.data(), pin_xy, xy.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && net_weight) {
+    wt.resize((size_t)n_nets);
+    wt2.resize((size_t)n_nets);
+    e = cudaMemcpyAsync(wt.data(), net_weight, wt.size() * sizeof(float), cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return (int)e;
+  std::vector<int64_t> ns((size_t)n_nets + 1, 0);
+  int64_t at = 0;
+  for (int64_t i = 0; i < n_nets; i++) {
+    const int32_t n = order[i];
+    for (int64_t q = starts[n]; q < starts[n + 1]; q++, at++) {
+      xy2[2 * at] = xy[2 * q];
+      xy2[2 * at + 1] = xy[2 * q + 1];
+      slot[at] = (int32_t)q;
+    }
+    ns[i + 1] = at;
+    if (net_weight) wt2[i] = wt[n];
+  }
   std::vector<int4> tiles;
   std::vector<int32_t> big;
-  wa_tiles(starts.data(), (int32_t)n_nets, tiles, big);
+  const WaSmall small = wa_small_ranges(ns.data(), (int32_t)n_nets);
+  wa_tiles(ns.data(), 0, small.first[0], tiles, big);
+  wa_tiles(ns.data(), small.first[2] + small.count[2], (int32_t)n_nets, tiles, big);
+  int64_t *d_ns = nullptr;
+  int32_t *d_xy = nullptr, *d_slot = nullptr, *d_big = nullptr;
   int4 *d_tiles = nullptr;
-  int32_t *d_big = nullptr;
-  e = cudaMalloc((void **)&d_tiles, std::max<size_t>(tiles.size(), 1) * sizeof(int4));
-  if (e == cudaSuccess) e = cudaMalloc((void **)&d_big, std::max<size_t>(big.size(), 1) * sizeof(int32_t));
-  if (e == cudaSuccess && !tiles.empty()) e = cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess && !big.empty()) e = cudaMemcpyAsync(d_big, big.data(), big.size() * sizeof(int32_t), cudaMemcpyHostToDevice, s);
+  float *d_wt = nullptr;
+  auto put = [&](auto **d, const auto &v) {
+    if (e != cudaSuccess) return;
+    e = cudaMallocAsync((void **)d, std::max<size_t>(v.size(), 1) * sizeof(v[0]), s);
+    if (e == cudaSuccess && !v.empty()) e = cudaMemcpyAsync(*d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, s);
+  };
+  put(&d_ns, ns);
+  put(&d_xy, xy2);
+  put(&d_slot, slot);
+  put(&d_tiles, tiles);
+  put(&d_big, big);
+  if (net_weight) put(&d_wt, wt2);
   if (e == cudaSuccess) {
     WaArgs w{};
     w.n_nets = (int32_t)big.size();
-    w.net_start = net_start;
+    w.net_start = d_ns;
     w.net_order = d_big;
-    w.net_weight = net_weight;
-    w.pin_base = reinterpret_cast<const int2 *>(pin_xy);
+    w.net_weight = d_wt;
+    w.pin_base = reinterpret_cast<const int2 *>(d_xy);
+    w.pin_slot = d_slot;
     w.pin_grad = reinterpret_cast<float2 *>(grad);
     w.n_tiles = (int32_t)tiles.size();
     w.tiles = d_tiles;
+    w.small = small;
+    if (const int nb = wa_small_blocks(small)) k_wa_small<<<nb, kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y, 1);
     if (!tiles.empty()) launch_wa_tiles(w, coef_x, coef_y, s);
     if (!big.empty()) k_wa<<<(unsigned)((big.size() + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y);
     e = cudaGetLastError();
   }
+  void *bufs[] = {d_ns, d_xy, d_slot, d_tiles, d_big, d_wt};
+  for (void *p : bufs)
+    if (p) cudaFreeAsync(p, s);
   cudaError_t e2 = cudaStreamSynchronize(s);
-  cudaFree(d_tiles);
-  cudaFree(d_big);
   return (int)(e != cudaSuccess ? e : e2);
 }
 

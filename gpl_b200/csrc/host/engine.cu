@@ -118,6 +118,7 @@ void Engine::free_globals() {
   pin_base_ = nullptr;
   tiles_ = nullptr;
   n_tiles_ = n_big_ = 0;
+  small_ = WaSmall{};
   net_weight_ = nullptr;
   pin_grad_ = nullptr;
   hpwl_acc_ = nullptr;
@@ -204,9 +205,14 @@ void Engine::upload(const EngineSetup &s) {
     check(upload_vec(&net_start_, ns, st), "upload nets");
     // WA's tiles of consecutive nets, and the nets too large for a tile (already in degree
     // order, so a warp's threads walk nets of one length)
+    // the degree-2..4 nets run a thread per net (k_wa_small); the tiles take the rest: the
+    // nets below degree 2 and those above 4
+    small_ = wa_small_ranges(ns.data(), n_nets_);
+    const int32_t small_lo = small_.first[0], small_hi = small_.first[2] + small_.count[2];
     std::vector<int4> tiles;
     std::vector<int32_t> big;
-    wa_tiles(ns.data(), n_nets_, tiles, big);
+    wa_tiles(ns.data(), 0, small_lo, tiles, big);
+    wa_tiles(ns.data(), small_hi, n_nets_, tiles, big);
     n_tiles_ = (int32_t)tiles.size();
     n_big_ = (int32_t)big.size();
     check(upload_vec(&tiles_, tiles, st), "upload nets");
@@ -427,6 +433,7 @@ WaArgs Engine::wa_args() const {
   w.pin_grad = pin_grad_;
   w.n_tiles = n_tiles_;
   w.tiles = tiles_;
+  w.small = small_;
   return w;
 }
 
@@ -446,6 +453,10 @@ void Engine::wa(float cx, float cy) {
   hpwl_ready_ = true;
   hpwl_fetched_ = false;
   ph_begin(PH_WA, st);
+  if (const int nb = wa_small_blocks(small_)) {
+    launches += 1;
+    k_wa_small<<<nb, kThreadsPerBlock, 0, st>>>(w, cx, cy, 1);
+  }
   if (n_tiles_) {
     launches += 1;
     launch_wa_tiles(w, cx, cy, st);
@@ -536,6 +547,12 @@ int64_t Engine::hpwl() {
   if (!hpwl_ready_) {
   check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), stream_), "hpwl");
   ph_begin(PH_HPWL);
+  if (const int nb = wa_small_blocks(small_)) {
+    launches += 1;
+    WaArgs wh = w;
+    wh.hpwl_out = hpwl_acc_;
+    k_wa_small<<<nb, kThreadsPerBlock, 0, stream_>>>(wh, 0.0f, 0.0f, 0);
+  }
   if (n_tiles_) {
     launches += 1;
     k_hpwl_tiles<<<n_tiles_, kThreadsPerBlock, 0, stream_>>>(w, hpwl_acc_);

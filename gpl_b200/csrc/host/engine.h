@@ -141,6 +141,7 @@ class Engine {
   int2 *pin_base_ = nullptr;
   int4 *tiles_ = nullptr;
   int32_t n_tiles_ = 0, n_big_ = 0;
+  WaSmall small_{};  // the degree-2..4 net ranges the thread-per-net WA takes
   float *net_weight_ = nullptr;
   bool unit_weights_ = true;  // every net weight is 1: the WA kernels skip the weight loads
   float2 *pin_grad_ = nullptr;  // the WA force of every pin of a cell, cell-major (cell_pins order)

@@ -48,6 +48,13 @@ struct CellArgs {
 };
 
 // The nets and pins (all regions): pins net-major.
+// Nets of degree 2, 3 and 4 (most of a netlist) run a thread per net with their pins in
+// registers (k_wa_small, no shared memory and no barriers): one range of consecutive device
+// nets per degree (the device orders its nets by degree).
+struct WaSmall {
+  int32_t first[3], count[3];  // degree 2 + k: nets [first[k], first[k] + count[k])
+};
+
 struct WaArgs {
   int32_t n_nets;                // nets the thread-per-net kernels walk (net_order, or 0..n)
   const int64_t *net_start;
@@ -61,12 +68,19 @@ struct WaArgs {
   int32_t n_tiles;               // tiles of consecutive nets: first net, end net, first pin, pins
   const int4 *tiles;
   unsigned long long *hpwl_out;  // WA adds the HPWL of the same pin positions here (NULL: not)
+  WaSmall small;                 // the degree-2..4 ranges (zero counts: none)
 };
 
 __global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *coords);
 __global__ void k_bins_finalize(RegionArgs r, double *partials, __nv_bfloat16 *dens_split, int split_ld, unsigned int *ticket, double *out);
 __global__ void k_wa(WaArgs w, float cx, float cy);
 __global__ void k_wa_tiles(WaArgs w, float cx, float cy);
+// The nets of w.small, a thread per net: their forces (forces != 0) and their HPWL into
+// w.hpwl_out. Launch with wa_small_blocks(w.small) blocks.
+__global__ void k_wa_small(WaArgs w, float cx, float cy, int forces);
+int wa_small_blocks(const WaSmall &s);
+// The degree-2..4 ranges of nets already in degree order.
+WaSmall wa_small_ranges(const int64_t *net_start, int32_t n_nets);
 // k_wa_tiles over every tile: a persistent grid of the blocks the device holds at once.
 void launch_wa_tiles(const WaArgs &w, float cx, float cy, cudaStream_t s);
 __global__ void k_gradients(RegionArgs r, CellArgs c, const float2 *pin_grad, float penalty, float2 *out_sum,
@@ -79,9 +93,9 @@ __global__ void k_pack_centres(int64_t n, const int32_t *x, const int32_t *y, in
 // Whether a grid's bins are small enough for the scatter's 32-bit shared tile.
 bool narrow_tile(const std::vector<int32_t> &bx, const std::vector<int32_t> &by);
 
-// Tiles of consecutive nets (at most kWaTilePins pins and kWaTileNets nets each) and the nets
-// too large for a tile, from the nets' pin starts.
-void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int4> &tiles, std::vector<int32_t> &big);
+// Tiles of the consecutive nets [first, last) (at most kWaTilePins pins and kWaTileNets nets
+// each) and the nets too large for a tile, from the nets' pin starts; appended to both lists.
+void wa_tiles(const int64_t *net_start, int32_t first, int32_t last, std::vector<int4> &tiles, std::vector<int32_t> &big);
 __global__ void k_hold_locked(RegionArgs r, CellArgs c);
 
 // The density solver (Fft::solve without the potential): FP32 SIMT GEMMs or split-BF16

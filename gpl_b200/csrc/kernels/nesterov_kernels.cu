@@ -510,6 +510,97 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
   }
 }
 
+// One net of degree D, a thread's own (the nets of the small ranges): its positions in
+// registers, the box and the HPWL, the exp terms, the sums in pin order and each pin's force,
+// the same operations in the same order as the tiles' phases.
+template <int D>
+__device__ __forceinline__ long long wa_net(const WaArgs &w, int32_t n, float cx, float cy, bool forces) {
+  const int64_t p0 = w.net_start[n];
+  int2 q[D];
+#pragma unroll
+  for (int k = 0; k < D; k++) q[k] = pin_pos(w, p0 + k);
+  int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
+#pragma unroll
+  for (int k = 0; k < D; k++) {
+    lx = min(lx, q[k].x);
+    ly = min(ly, q[k].y);
+    ux = max(ux, q[k].x);
+    uy = max(uy, q[k].y);
+  }
+  const long long h = ((long long)ux - lx) + ((long long)uy - ly);  // ux >= lx: D >= 1 pins
+  if (!forces) return h;
+  const float BAR = -300.0f;
+  float4 v[D];
+  uint32_t m[D];
+#pragma unroll
+  for (int k = 0; k < D; k++) {
+    float emin_x = __fmul_rn((float)(lx - q[k].x), cx), emax_x = __fmul_rn((float)(q[k].x - ux), cx);
+    float emin_y = __fmul_rn((float)(ly - q[k].y), cy), emax_y = __fmul_rn((float)(q[k].y - uy), cy);
+    m[k] = (emin_x > BAR ? 1u : 0u) | (emax_x > BAR ? 2u : 0u) | (emin_y > BAR ? 4u : 0u) | (emax_y > BAR ? 8u : 0u);
+    v[k].x = (m[k] & 1u) ? fast_exp(emin_x) : 0.0f;
+    v[k].y = (m[k] & 2u) ? fast_exp(emax_x) : 0.0f;
+    v[k].z = (m[k] & 4u) ? fast_exp(emin_y) : 0.0f;
+    v[k].w = (m[k] & 8u) ? fast_exp(emax_y) : 0.0f;
+  }
+  float s_minx = 0, s_xminx = 0, s_maxx = 0, s_xmaxx = 0, s_miny = 0, s_yminy = 0, s_maxy = 0, s_ymaxy = 0;
+#pragma unroll
+  for (int k = 0; k < D; k++) {
+    float qx = (float)q[k].x, qy = (float)q[k].y;
+    s_minx = __fadd_rn(s_minx, v[k].x);
+    s_xminx = __fadd_rn(s_xminx, __fmul_rn(qx, v[k].x));
+    s_maxx = __fadd_rn(s_maxx, v[k].y);
+    s_xmaxx = __fadd_rn(s_xmaxx, __fmul_rn(qx, v[k].y));
+    s_miny = __fadd_rn(s_miny, v[k].z);
+    s_yminy = __fadd_rn(s_yminy, __fmul_rn(qy, v[k].z));
+    s_maxy = __fadd_rn(s_maxy, v[k].w);
+    s_ymaxy = __fadd_rn(s_ymaxy, __fmul_rn(qy, v[k].w));
+  }
+  const float wt = w.net_weight ? w.net_weight[n] : 1.0f;
+#pragma unroll
+  for (int k = 0; k < D; k++) {
+    float qx = (float)q[k].x, qy = (float)q[k].y;
+    float gmin_x = (m[k] & 1u) ? wa_term_min(s_minx, s_xminx, v[k].x, cx, qx) : 0.0f;
+    float gmax_x = (m[k] & 2u) ? wa_term_max(s_maxx, s_xmaxx, v[k].y, cx, qx) : 0.0f;
+    float gmin_y = (m[k] & 4u) ? wa_term_min(s_miny, s_yminy, v[k].z, cy, qy) : 0.0f;
+    float gmax_y = (m[k] & 8u) ? wa_term_max(s_maxy, s_ymaxy, v[k].w, cy, qy) : 0.0f;
+    wa_store(w, p0 + k, make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt)));
+  }
+  return h;
+}
+
+__global__ void __launch_bounds__(kThreads) k_wa_small(WaArgs w, float cx, float cy, int forces) {
+  // blocks of degree-2 nets, then degree 3, then degree 4 (the ranges read with constant
+  // indices: the kernel's parameters stay out of local memory)
+  const int nb0 = (w.small.count[0] + kThreads - 1) / kThreads, nb1 = (w.small.count[1] + kThreads - 1) / kThreads;
+  const int b = blockIdx.x;
+  const int k = b < nb0 ? 0 : b < nb0 + nb1 ? 1 : 2;
+  const int t = (b - (k == 0 ? 0 : k == 1 ? nb0 : nb0 + nb1)) * kThreads + threadIdx.x;
+  const int32_t count = k == 0 ? w.small.count[0] : k == 1 ? w.small.count[1] : w.small.count[2];
+  const int32_t first = k == 0 ? w.small.first[0] : k == 1 ? w.small.first[1] : w.small.first[2];
+  long long h = 0;
+  if (t < count) {
+    const int32_t n = first + t;
+    if (k == 0)
+      h = wa_net<2>(w, n, cx, cy, forces != 0);
+    else if (k == 1)
+      h = wa_net<3>(w, n, cx, cy, forces != 0);
+    else
+      h = wa_net<4>(w, n, cx, cy, forces != 0);
+  }
+  // the block's HPWL: warp sums, then one atomic per block (integer: any order)
+  __shared__ long long s_h[kThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+  if ((threadIdx.x & 31) == 0) s_h[threadIdx.x >> 5] = h;
+  __syncthreads();
+  if (threadIdx.x == 0 && w.hpwl_out) {
+    long long sum = 0;
+#pragma unroll
+    for (int j = 0; j < kThreads / 32; j++) sum += s_h[j];
+    if (sum) atomicAdd(w.hpwl_out, (unsigned long long)sum);
+  }
+}
+
 // The WA tiles' launch: a persistent grid of as many blocks as fit on the device at once.
 void launch_wa_tiles(const WaArgs &w, float cx, float cy, cudaStream_t s) {
   if (w.n_tiles <= 0) return;
@@ -706,15 +797,13 @@ __global__ void k_pack_centres(int64_t n, const int32_t *__restrict__ x, const i
   if (i < n) out[i] = make_int2(x[i], y[i]);
 }
 
-void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int4> &tiles, std::vector<int32_t> &big) {
-  tiles.clear();
-  big.clear();
-  int32_t first = 0;
+void wa_tiles(const int64_t *net_start, int32_t lo, int32_t hi, std::vector<int4> &tiles, std::vector<int32_t> &big) {
+  int32_t first = lo;
   // a tile: its nets [first, end), its first pin and its pin count (pin numbers below 2^31)
   auto close = [&](int32_t end) {
     if (end > first) tiles.push_back(make_int4(first, end, (int32_t)net_start[first], (int32_t)(net_start[end] - net_start[first])));
   };
-  for (int32_t n = 0; n < n_nets; n++) {
+  for (int32_t n = lo; n < hi; n++) {
     int64_t deg = net_start[n + 1] - net_start[n];
     if (deg > kWaTilePins) {
       close(n);
@@ -727,7 +816,26 @@ void wa_tiles(const int64_t *net_start, int32_t n_nets, std::vector<int4> &tiles
       first = n;
     }
   }
-  close(n_nets);
+  close(hi);
+}
+
+WaSmall wa_small_ranges(const int64_t *net_start, int32_t n_nets) {
+  WaSmall s{};
+  for (int k = 0; k < 3; k++) {
+    const int64_t d = 2 + k;
+    int32_t n = 0;
+    while (n < n_nets && net_start[n + 1] - net_start[n] < d) n++;
+    s.first[k] = n;
+    while (n < n_nets && net_start[n + 1] - net_start[n] == d) n++;
+    s.count[k] = n - s.first[k];
+  }
+  return s;
+}
+
+int wa_small_blocks(const WaSmall &s) {
+  int b = 0;
+  for (int k = 0; k < 3; k++) b += (s.count[k] + kThreads - 1) / kThreads;
+  return b;
 }
 
 // ---- the locked cells' next state (:2848-2859).

@@ -53,6 +53,7 @@ struct CellArgs {
 // nets per degree (the device orders its nets by degree).
 struct WaSmall {
   int32_t first[3], count[3];  // degree 2 + k: nets [first[k], first[k] + count[k])
+  int64_t pin0[3];             // and their pins from pin0[k], 2 + k a net in net order
 };
 
 struct WaArgs {

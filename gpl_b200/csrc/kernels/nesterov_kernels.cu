@@ -514,8 +514,7 @@ __global__ void __launch_bounds__(kThreads) k_wa_tiles(WaArgs w, float cx, float
 // registers, the box and the HPWL, the exp terms, the sums in pin order and each pin's force,
 // the same operations in the same order as the tiles' phases.
 template <int D>
-__device__ __forceinline__ long long wa_net(const WaArgs &w, int32_t n, float cx, float cy, bool forces) {
-  const int64_t p0 = w.net_start[n];
+__device__ __forceinline__ long long wa_net(const WaArgs &w, int32_t n, int64_t p0, float cx, float cy, bool forces) {
   int2 q[D];
 #pragma unroll
   for (int k = 0; k < D; k++) q[k] = pin_pos(w, p0 + k);
@@ -577,15 +576,18 @@ __global__ void __launch_bounds__(kThreads) k_wa_small(WaArgs w, float cx, float
   const int t = (b - (k == 0 ? 0 : k == 1 ? nb0 : nb0 + nb1)) * kThreads + threadIdx.x;
   const int32_t count = k == 0 ? w.small.count[0] : k == 1 ? w.small.count[1] : w.small.count[2];
   const int32_t first = k == 0 ? w.small.first[0] : k == 1 ? w.small.first[1] : w.small.first[2];
+  const int64_t pin0 = k == 0 ? w.small.pin0[0] : k == 1 ? w.small.pin0[1] : w.small.pin0[2];
   long long h = 0;
   if (t < count) {
+    // a range's nets all have 2 + k pins, in net order: the net's first pin without a load
     const int32_t n = first + t;
+    const int64_t p0 = pin0 + (int64_t)t * (2 + k);
     if (k == 0)
-      h = wa_net<2>(w, n, cx, cy, forces != 0);
+      h = wa_net<2>(w, n, p0, cx, cy, forces != 0);
     else if (k == 1)
-      h = wa_net<3>(w, n, cx, cy, forces != 0);
+      h = wa_net<3>(w, n, p0, cx, cy, forces != 0);
     else
-      h = wa_net<4>(w, n, cx, cy, forces != 0);
+      h = wa_net<4>(w, n, p0, cx, cy, forces != 0);
   }
   // the block's HPWL: warp sums, then one atomic per block (integer: any order)
   __shared__ long long s_h[kThreads / 32];
@@ -828,6 +830,7 @@ WaSmall wa_small_ranges(const int64_t *net_start, int32_t n_nets) {
     s.first[k] = n;
     while (n < n_nets && net_start[n + 1] - net_start[n] == d) n++;
     s.count[k] = n - s.first[k];
+    s.pin0[k] = net_start[s.first[k]];
   }
   return s;
 }

@@ -169,7 +169,54 @@ static_assert(GPL_SPMV_ROWS == kSpmvRows && GPL_SPMV_TILED == kSpmvTiled, "the C
 
 int gpl_kernel_spmv(int64_t n, const int64_t *row_start, const int32_t *cols, const float *vals, const float *x, float *y, int32_t form, void *stream) {
   CsrDev A{n, row_start, cols, vals};
-  return (int)spmv(A, x, y, form, (cudaStream_t)stream);
+  cudaStream_t s = (cudaStream_t)stream;
+  if (form != kSpmvSliced || n <= 0) return (int)spmv(A, x, y, form, s);
+  // the sliced copy: the order by length and the slice widths on the device, their
+  // exclusive scan here, the entries
+  int64_t *starts = nullptr;
+  int32_t *row = nullptr, *len = nullptr, *count = nullptr, *sc = nullptr;
+  float *sv = nullptr;
+  int32_t n_long = 0;
+  cudaError_t e = cudaMalloc(&row, (size_t)n * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&len, (size_t)n * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&count, (size_t)(kSliceLenCap + 1) * sizeof(int32_t));
+  if (e == cudaSuccess) e = csr_slice_order(A, row, len, count, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&n_long, count + kSliceLongRow + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  const int64_t ns = (n - n_long + kSliceRows - 1) / kSliceRows;
+  std::vector<int64_t> h((size_t)ns + 1, 0);
+  if (e == cudaSuccess) e = cudaMalloc(&starts, (size_t)(ns + 1) * sizeof(int64_t));
+  if (e == cudaSuccess) e = csr_slice_widths(n, n_long, len, starts, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), starts, (size_t)ns * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) {
+    int64_t run = 0;
+    for (int64_t k = 0; k < ns; k++) {
+      const int64_t w = h[(size_t)k];
+      h[(size_t)k] = run;
+      run += w;
+    }
+    h[(size_t)ns] = run;
+    e = cudaMemcpyAsync(starts, h.data(), (size_t)(ns + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s);
+  }
+  const size_t total = (size_t)std::max<int64_t>(h[(size_t)ns], 1);
+  if (e == cudaSuccess) e = cudaMalloc(&sc, total * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&sv, total * sizeof(float));
+  if (e == cudaSuccess) {
+    A.sl_long = n_long;
+    A.sl_row = row;
+    A.sl_len = len;
+    A.sl_start = starts;
+    e = csr_slice_fill(A, sc, sv, s);
+  }
+  if (e == cudaSuccess) {
+    A.sl_cols = sc;
+    A.sl_vals = sv;
+    e = spmv(A, x, y, form, s);
+  }
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  for (void *p : {(void *)starts, (void *)row, (void *)len, (void *)count, (void *)sc, (void *)sv}) cudaFree(p);
+  return (int)(e != cudaSuccess ? e : e2);
 }
 
 int gpl_kernel_bicgstab(int64_t n, const int64_t *row_start, const int32_t *cols, const float *vals, const float *rhs, float *x, int32_t max_iters, int32_t *iterations, float *error, void *stream) {

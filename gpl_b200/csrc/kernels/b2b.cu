@@ -611,7 +611,7 @@ void IpDevice::release() {
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, s_);
   for (auto &a : ax_) {
-    void *q[] = {a.starts, a.cols, a.vals, a.rhs, a.x};
+    void *q[] = {a.starts, a.cols, a.vals, a.rhs, a.x, a.sl_row, a.sl_len, a.sl_count, a.sl_start, a.sl_cols, a.sl_vals};
     for (void *p : q)
       if (p) cudaFreeAsync(p, s_);
     a = Axis{};
@@ -815,7 +815,42 @@ cudaError_t IpDevice::assemble(IpAxisResult out[2]) {
   return cudaStreamSynchronize(s_);
 }
 
+// The sliced copy: the rows in order of length and the count of long rows read back, the
+// slice widths of the rest, their scan (the starts), the total read back to size the
+// entries, then the entries.
+cudaError_t IpDevice::slice(Axis &A) {
+  CK(grow(s_, (size_t)std::max<int64_t>(n_, 1), A.sl_row_cap, &A.sl_row, &A.sl_len));
+  CK(grow(s_, (size_t)kSliceLenCap + 1, A.sl_count_cap, &A.sl_count));
+  CsrDev m{n_, A.starts, A.cols, A.vals};
+  CK(csr_slice_order(m, A.sl_row, A.sl_len, A.sl_count, s_));
+  int32_t n_long = 0;
+  CK(cudaMemcpyAsync(&n_long, A.sl_count + kSliceLongRow + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  A.sl_long = n_long;
+  const int64_t ns = (n_ - n_long + kSliceRows - 1) / kSliceRows;
+  CK(grow(s_, (size_t)ns + 1, A.sl_start_cap, &A.sl_start));
+  CK(csr_slice_widths(n_, n_long, A.sl_len, A.sl_start, s_));
+  CK(scan(A.sl_start, ns));
+  int64_t total = 0;
+  CK(cudaMemcpyAsync(&total, A.sl_start + ns, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  d2h_bytes += sizeof(int64_t) + sizeof(int32_t);
+  CK(grow(s_, (size_t)std::max<int64_t>(total, 1), A.sl_cap, &A.sl_cols, &A.sl_vals));
+  m.sl_long = n_long;
+  m.sl_row = A.sl_row;
+  m.sl_len = A.sl_len;
+  m.sl_start = A.sl_start;
+  CK(csr_slice_fill(m, A.sl_cols, A.sl_vals, s_));
+  launches += 8;
+  return cudaSuccess;
+}
+
 cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
+  // the sliced copies when the sliced form may run: before the first solve picks a form, and
+  // while it is the form picked
+  const bool sliced = spmv_form_ < 0 || spmv_form_ == kSpmvSliced;
+  if (sliced)
+    for (Axis &A : ax_) CK(slice(A));
   CsrDev m[2];
   const float *b[2];
   float *x[2];
@@ -823,6 +858,14 @@ cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
   for (int a = 0; a < 2; a++) {
     Axis &A = ax_[a];
     m[a] = CsrDev{n_, A.starts, A.cols, A.vals};
+    if (sliced) {
+      m[a].sl_long = A.sl_long;
+      m[a].sl_row = A.sl_row;
+      m[a].sl_len = A.sl_len;
+      m[a].sl_start = A.sl_start;
+      m[a].sl_cols = A.sl_cols;
+      m[a].sl_vals = A.sl_vals;
+    }
     b[a] = A.rhs;
     x[a] = A.x;
     scratch[a] = (char *)scratch_ + a * scratch_bytes_;

@@ -101,6 +101,14 @@ class IpDevice {
     float *vals = nullptr, *rhs = nullptr, *x = nullptr;
     size_t cap = 0;
     int64_t nnz = 0;
+    // the sliced copy (bicgstab.h): row order and lengths, length counts, slice starts,
+    // entries
+    int64_t sl_long = 0;
+    int32_t *sl_row = nullptr, *sl_len = nullptr, *sl_count = nullptr;
+    int64_t *sl_start = nullptr;
+    int32_t *sl_cols = nullptr;
+    float *sl_vals = nullptr;
+    size_t sl_cap = 0, sl_start_cap = 0, sl_row_cap = 0, sl_count_cap = 0;
   } ax_[2];
   void *scratch_ = nullptr;
   size_t scratch_bytes_ = 0;
@@ -108,6 +116,7 @@ class IpDevice {
   void release();
   cudaError_t collapse(int64_t n_trip, const int32_t *row, const int32_t *col, const float *val, int64_t *starts_out, int32_t **cols, float **vals, size_t *cap, int64_t *nnz);
   cudaError_t scan(int64_t *data, int64_t n);
+  cudaError_t slice(Axis &A);  // the axis's sliced copy, from its CSR arrays
 };
 
 }  // namespace gpl

@@ -7,6 +7,9 @@
 // unless it goes on. The host enqueues iterations in batches, reads the loop's state once per
 // batch and runs a restart itself when the device asks for one.
 #include "bicgstab.h"
+
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace gpl {
@@ -103,8 +106,137 @@ __device__ __forceinline__ void spmv_tiled_body(int64_t n, const int64_t *__rest
 }
 __global__ void __launch_bounds__(kThreads) k_spmv_tiled(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) { spmv_tiled_body(n, rs, cols, vals, x, y, S, gate); }
 
+//  sliced: over the sliced copy (rows in order of length). The long rows first, a warp per
+//         row: the lanes form 32 products at a time from the CSR arrays (coalesced, several
+//         chunks in flight) and every lane adds them in column order through shuffles. Then
+//         a thread per short row: at step k a warp's rows read one coalesced run of entries
+//         (the slice's column k), each row summed in column order and stopping at its own
+//         length. y is written at the row's own index. Blocks [0, long_blocks) take the long
+//         rows, kThreads / 32 rows each.
+constexpr int kLongChunks = 4;
+__host__ __device__ __forceinline__ int64_t sliced_long_blocks(int64_t n_long) { return (n_long + kThreads / 32 - 1) / (kThreads / 32); }
+__host__ __device__ __forceinline__ int64_t sliced_blocks(int64_t n, int64_t n_long) { return sliced_long_blocks(n_long) + (n - n_long + kThreads - 1) / kThreads; }
+__device__ __forceinline__ void spmv_sliced_body(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int32_t *__restrict__ sl_cols, const float *__restrict__ sl_vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
+  if (gated_off(S, gate)) return;
+  const int64_t lb = sliced_long_blocks(n_long);
+  if (blockIdx.x < lb) {
+    const int64_t w = blockIdx.x * (int64_t)(kThreads / 32) + (threadIdx.x >> 5);
+    if (w >= n_long) return;  // the whole warp
+    const int lane = threadIdx.x & 31;
+    const int32_t row = sl_row[w];
+    const int64_t b = rs[row], e = rs[row + 1];
+    float sum = 0.0f;
+    for (int64_t m = b; m < e; m += 32 * kLongChunks) {
+      float p[kLongChunks];
+#pragma unroll
+      for (int u = 0; u < kLongChunks; u++) {
+        const int64_t k = m + 32 * u + lane;
+        p[u] = k < e ? __fmul_rn(__ldg(vals + k), __ldg(x + __ldg(cols + k))) : 0.0f;
+      }
+#pragma unroll
+      for (int u = 0; u < kLongChunks; u++) {
+        const int64_t c0 = m + 32 * u;
+        if (c0 >= e) break;  // uniform across the warp
+        if (e - c0 >= 32) {
+#pragma unroll
+          for (int t = 0; t < 32; t++) sum = __fadd_rn(sum, __shfl_sync(0xffffffffu, p[u], t));
+        } else {
+          const int cnt = (int)(e - c0);
+          for (int t = 0; t < cnt; t++) sum = __fadd_rn(sum, __shfl_sync(0xffffffffu, p[u], t));
+        }
+      }
+    }
+    if (lane == 0) y[row] = __fadd_rn(0.0f, __fmul_rn(1.0f, sum));
+    return;
+  }
+  const int64_t i = (blockIdx.x - lb) * (int64_t)kThreads + threadIdx.x;  // short position
+  const int64_t j = n_long + i;
+  if (j >= n) return;
+  const int32_t len = sl_len[j];
+  const int64_t base = sl_start[i / kSliceRows] + (i % kSliceRows);
+  const int32_t *c = sl_cols + base;
+  const float *v = sl_vals + base;
+  float tmp = 0.0f;
+  int32_t k = 0;
+  for (; k + kSpmvUnroll <= len; k += kSpmvUnroll) {
+    int cc[kSpmvUnroll];
+    float vv[kSpmvUnroll], xv[kSpmvUnroll];
+#pragma unroll
+    for (int u = 0; u < kSpmvUnroll; u++) {
+      cc[u] = __ldg(c + (int64_t)(k + u) * kSliceRows);
+      vv[u] = __ldg(v + (int64_t)(k + u) * kSliceRows);
+    }
+#pragma unroll
+    for (int u = 0; u < kSpmvUnroll; u++) xv[u] = __ldg(x + cc[u]);
+#pragma unroll
+    for (int u = 0; u < kSpmvUnroll; u++) tmp = __fadd_rn(tmp, __fmul_rn(vv[u], xv[u]));
+  }
+  for (; k < len; k++) tmp = __fadd_rn(tmp, __fmul_rn(__ldg(v + (int64_t)k * kSliceRows), __ldg(x + __ldg(c + (int64_t)k * kSliceRows))));
+  y[sl_row[j]] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
+}
+__global__ void __launch_bounds__(kThreads) k_spmv_sliced(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int32_t *__restrict__ sl_cols, const float *__restrict__ sl_vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) { spmv_sliced_body(n, n_long, rs, cols, vals, sl_row, sl_len, sl_start, sl_cols, sl_vals, x, y, S, gate); }
+
+// The order by length: a histogram of the (capped) lengths per block in shared memory, the
+// buckets' starts longest first, then each row's position from its bucket's cursor (a warp's
+// rows of one bucket take one atomic between them).
+__global__ void __launch_bounds__(kThreads) k_len_hist(int64_t n, const int64_t *__restrict__ rs, int32_t *__restrict__ count) {
+  __shared__ int32_t h[kSliceLenCap + 1];
+  for (int b = threadIdx.x; b <= kSliceLenCap; b += kThreads) h[b] = 0;
+  __syncthreads();
+  const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  if (i < n) atomicAdd(&h[(int)min(rs[i + 1] - rs[i], (int64_t)kSliceLenCap)], 1);
+  __syncthreads();
+  for (int b = threadIdx.x; b <= kSliceLenCap; b += kThreads)
+    if (h[b]) atomicAdd(&count[b], h[b]);
+}
+__global__ void k_len_starts(int32_t *count) {  // one thread: counts to starts, longest first
+  int32_t run = 0;
+  for (int b = kSliceLenCap; b >= 0; b--) {
+    const int32_t c = count[b];
+    count[b] = run;
+    run += c;
+  }
+}
+__global__ void __launch_bounds__(kThreads) k_len_scatter(int64_t n, const int64_t *__restrict__ rs, int32_t *__restrict__ cursor, int32_t *__restrict__ row, int32_t *__restrict__ len) {
+  const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  const bool live = i < n;
+  const int64_t l = live ? rs[i + 1] - rs[i] : 0;
+  const int b = live ? (int)min(l, (int64_t)kSliceLenCap) : -1;
+  const unsigned peers = __match_any_sync(0xffffffffu, b);
+  const int leader = __ffs(peers) - 1, lane = threadIdx.x & 31;
+  int32_t at = 0;
+  if (live && lane == leader) at = atomicAdd(&cursor[b], __popc(peers));
+  at = __shfl_sync(0xffffffffu, at, leader);
+  if (!live) return;
+  at += __popc(peers & ((1u << lane) - 1u));
+  row[at] = (int32_t)i;
+  len[at] = (int32_t)l;
+}
+// kSliceRows times each slice's longest row (a warp's short positions are one slice).
+__global__ void __launch_bounds__(kThreads) k_slice_widths(int64_t n, int64_t n_long, const int32_t *__restrict__ len, int64_t *__restrict__ widths) {
+  static_assert(kSliceRows == 32 && kThreads % 32 == 0, "a slice is a warp's rows");
+  const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x, ns = n - n_long;
+  if (i - (threadIdx.x & 31) >= ns) return;  // the warp's slice starts past the end
+  const unsigned l = i < ns ? (unsigned)len[n_long + i] : 0u;
+  const unsigned m = __reduce_max_sync(0xffffffffu, l);
+  if ((threadIdx.x & 31) == 0) widths[i / kSliceRows] = (int64_t)m * kSliceRows;
+}
+__global__ void __launch_bounds__(kThreads) k_slice_fill(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, int32_t *__restrict__ sl_cols, float *__restrict__ sl_vals) {
+  const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x, j = n_long + i;
+  if (j >= n) return;
+  const int64_t b = rs[sl_row[j]];
+  const int32_t len = sl_len[j];
+  const int64_t base = sl_start[i / kSliceRows] + (i % kSliceRows);
+  for (int32_t k = 0; k < len; k++) {
+    sl_cols[base + (int64_t)k * kSliceRows] = cols[b + k];
+    sl_vals[base + (int64_t)k * kSliceRows] = vals[b + k];
+  }
+}
+
 static void spmv_launch(int form, int eb, cudaStream_t st, const CsrDev &A, const float *in, float *o, const double *S, int gate) {
-  if (form == kSpmvTiled)
+  if (form == kSpmvSliced)
+    k_spmv_sliced<<<(unsigned)std::max<int64_t>(sliced_blocks(A.n, A.sl_long), 1), kThreads, 0, st>>>(A.n, A.sl_long, A.rs, A.cols, A.vals, A.sl_row, A.sl_len, A.sl_start, A.sl_cols, A.sl_vals, in, o, S, gate);
+  else if (form == kSpmvTiled)
     k_spmv_tiled<<<eb, kThreads, 0, st>>>(A.n, A.rs, A.cols, A.vals, in, o, S, gate);
   else
     k_spmv_rows<<<eb, kThreads, 0, st>>>(A.n, A.rs, A.cols, A.vals, in, o, S, gate);
@@ -271,6 +403,11 @@ struct SysDev {
   const int64_t *rs;
   const int32_t *cols;
   const float *vals;
+  int64_t sl_long;
+  const int32_t *sl_row, *sl_len;
+  const int64_t *sl_start;
+  const int32_t *sl_cols;
+  const float *sl_vals;
   float *x, *r, *r0, *v, *p, *s, *t;
   double *part, *S;
   unsigned int *ticket;
@@ -292,6 +429,10 @@ __global__ void __launch_bounds__(kThreads) k2_spmv_rows(SysPair P, int sel) {
 __global__ void __launch_bounds__(kThreads) k2_spmv_tiled(SysPair P, int sel) {
   SysDev q = pick(P);
   spmv_tiled_body(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
+}
+__global__ void __launch_bounds__(kThreads) k2_spmv_sliced(SysPair P, int sel) {
+  SysDev q = pick(P);
+  spmv_sliced_body(q.n, q.sl_long, q.rs, q.cols, q.vals, q.sl_row, q.sl_len, q.sl_start, q.sl_cols, q.sl_vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
 }
 // sel 0: r0.v, then alpha; sel 1: t.t and t.s, then omega
 __global__ void k2_dots(SysPair P, int sel) {
@@ -334,8 +475,32 @@ size_t bicgstab_scratch_bytes(int64_t n) {
   return 7 * vec + (size_t)kBicgBlocks * 3 * sizeof(double) + 64 * sizeof(double);
 }
 
+cudaError_t csr_slice_order(const CsrDev &A, int32_t *row, int32_t *len, int32_t *count, cudaStream_t st) {
+  if (A.n <= 0) return cudaSuccess;
+  const unsigned g = (unsigned)((A.n + kThreads - 1) / kThreads);
+  cudaError_t e = cudaMemsetAsync(count, 0, (kSliceLenCap + 1) * sizeof(int32_t), st);
+  if (e != cudaSuccess) return e;
+  k_len_hist<<<g, kThreads, 0, st>>>(A.n, A.rs, count);
+  k_len_starts<<<1, 1, 0, st>>>(count);
+  k_len_scatter<<<g, kThreads, 0, st>>>(A.n, A.rs, count, row, len);
+  return cudaGetLastError();
+}
+
+cudaError_t csr_slice_widths(int64_t n, int64_t n_long, const int32_t *len, int64_t *widths, cudaStream_t st) {
+  if (n - n_long <= 0) return cudaSuccess;
+  k_slice_widths<<<(unsigned)((n - n_long + kThreads - 1) / kThreads), kThreads, 0, st>>>(n, n_long, len, widths);
+  return cudaGetLastError();
+}
+
+cudaError_t csr_slice_fill(const CsrDev &A, int32_t *sl_cols, float *sl_vals, cudaStream_t st) {
+  if (A.n - A.sl_long <= 0) return cudaSuccess;
+  k_slice_fill<<<(unsigned)((A.n - A.sl_long + kThreads - 1) / kThreads), kThreads, 0, st>>>(A.n, A.sl_long, A.rs, A.cols, A.vals, A.sl_row, A.sl_len, A.sl_start, sl_cols, sl_vals);
+  return cudaGetLastError();
+}
+
 cudaError_t spmv(const CsrDev &A, const float *x, float *y, int form, cudaStream_t st) {
-  if (form != kSpmvRows && form != kSpmvTiled) return cudaErrorInvalidValue;
+  if (form != kSpmvRows && form != kSpmvTiled && form != kSpmvSliced) return cudaErrorInvalidValue;
+  if (form == kSpmvSliced && (!A.sl_start || !A.sl_row || !A.sl_len)) return cudaErrorInvalidValue;
   if (A.n <= 0) return cudaSuccess;
   spmv_launch(form, (int)((A.n + kThreads - 1) / kThreads), st, A, x, y, nullptr, kAlways);
   return cudaGetLastError();
@@ -349,9 +514,10 @@ cudaError_t bicgstab_pick_spmv(const CsrDev &A, const float *x, void *scratch, c
   cudaEvent_t ev[2];
   for (auto &e : ev)
     if (cudaEventCreate(&e) != cudaSuccess) return cudaGetLastError();
-  float ms[2] = {0, 0};
+  float ms[3] = {0, 0, 0};
+  const int forms = A.sl_start && A.sl_row && A.sl_len ? 3 : 2;
   cudaError_t err = cudaSuccess;
-  for (int f = 0; f < 2 && err == cudaSuccess; f++) {
+  for (int f = 0; f < forms && err == cudaSuccess; f++) {
     spmv_launch(f, eb, st, A, x, y, nullptr, kAlways);  // warm
     cudaEventRecord(ev[0], st);
     for (int r = 0; r < 3; r++) spmv_launch(f, eb, st, A, x, y, nullptr, kAlways);
@@ -360,12 +526,15 @@ cudaError_t bicgstab_pick_spmv(const CsrDev &A, const float *x, void *scratch, c
     if (err == cudaSuccess) err = cudaEventElapsedTime(&ms[f], ev[0], ev[1]);
   }
   for (auto &e : ev) cudaEventDestroy(e);
-  if (err == cudaSuccess && ms[kSpmvTiled] < ms[kSpmvRows]) *form = kSpmvTiled;
+  if (err == cudaSuccess)
+    for (int f = 1; f < forms; f++)
+      if (ms[f] < ms[*form]) *form = f;
   return err != cudaSuccess ? err : cudaGetLastError();
 }
 
 cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_iters, void *scratch, cudaStream_t st, BicgResult *out, int form) {
   static_assert(S_END <= S_TICKET && S_TICKET < 64, "the scalars fit the scratch's 64 doubles");
+  if (form == kSpmvSliced && (!A.sl_start || !A.sl_row || !A.sl_len)) return cudaErrorInvalidValue;
   int64_t n = A.n;
   size_t vec = ((size_t)n * sizeof(float) + 255) / 256 * 256;
   char *base = (char *)scratch;
@@ -445,6 +614,8 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
 cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], float *const x[2], int max_iters, void *const scratch[2], cudaStream_t st, BicgResult out[2], int form) {
   const int64_t n = A[0].n;
   if (A[1].n != n) return cudaErrorInvalidValue;
+  for (int a = 0; a < 2; a++)
+    if (form == kSpmvSliced && (!A[a].sl_start || !A[a].sl_row || !A[a].sl_len)) return cudaErrorInvalidValue;
   const size_t vec = ((size_t)n * sizeof(float) + 255) / 256 * 256;
   SysPair P{};
   for (int a = 0; a < 2; a++) {
@@ -454,6 +625,12 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
     q.rs = A[a].rs;
     q.cols = A[a].cols;
     q.vals = A[a].vals;
+    q.sl_long = A[a].sl_long;
+    q.sl_row = A[a].sl_row;
+    q.sl_len = A[a].sl_len;
+    q.sl_start = A[a].sl_start;
+    q.sl_cols = A[a].sl_cols;
+    q.sl_vals = A[a].sl_vals;
     q.x = x[a];
     q.r = (float *)base;
     q.r0 = (float *)(base + vec);
@@ -525,16 +702,21 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
   int64_t batches = 0;
   int restarts[2] = {0, 0};
   const dim3 ge(eb, 2), gr(rb, 2);
+  const dim3 gs((unsigned)std::max<int64_t>({sliced_blocks(n, A[0].sl_long), sliced_blocks(n, A[1].sl_long), 1}), 2);
   for (;;) {
     for (int k = 0; k < kBicgBatch; k++) {
       k2_update_p<<<ge, kThreads, 0, st>>>(P);
-      if (form == kSpmvTiled)
+      if (form == kSpmvSliced)
+        k2_spmv_sliced<<<gs, kThreads, 0, st>>>(P, 0);
+      else if (form == kSpmvTiled)
         k2_spmv_tiled<<<ge, kThreads, 0, st>>>(P, 0);
       else
         k2_spmv_rows<<<ge, kThreads, 0, st>>>(P, 0);
       k2_dots<<<gr, kThreads, 0, st>>>(P, 0);
       k2_update_s<<<ge, kThreads, 0, st>>>(P);
-      if (form == kSpmvTiled)
+      if (form == kSpmvSliced)
+        k2_spmv_sliced<<<gs, kThreads, 0, st>>>(P, 1);
+      else if (form == kSpmvTiled)
         k2_spmv_tiled<<<ge, kThreads, 0, st>>>(P, 1);
       else
         k2_spmv_rows<<<ge, kThreads, 0, st>>>(P, 1);

@@ -243,10 +243,13 @@ int gpl_kernel_csr_from_triplets(int64_t n, int64_t nt, const int32_t *rows, con
 
 /* `Csr::mul` (src/bicgstab.rs:72-82): y = A x on a CSR matrix (device pointers), each row's
  * products summed in column order, then 0 + 1 * sum, as the solver forms them. form picks the
- * kernel: GPL_SPMV_ROWS (a thread per row) or GPL_SPMV_TILED (a block's products staged in
- * shared memory); both give the same y, bit for bit. */
+ * kernel: GPL_SPMV_ROWS (a thread per row), GPL_SPMV_TILED (a block's products staged in
+ * shared memory) or GPL_SPMV_SLICED (a thread per row over a copy of the matrix in slices of
+ * 32 rows stored column-major, built by the call, which then synchronizes the stream); all
+ * give the same y, bit for bit. */
 #define GPL_SPMV_ROWS 0
 #define GPL_SPMV_TILED 1
+#define GPL_SPMV_SLICED 2
 int gpl_kernel_spmv(int64_t n, const int64_t *row_start, const int32_t *cols, const float *vals,
                     const float *x, float *y, int32_t form, void *stream);
 

@@ -149,15 +149,19 @@ def test_poisson(L, nx, ny, mode):
     assert np.max(np.abs(ey - fy)) <= tol * np.max(np.abs(fy))
 
 
-@pytest.mark.parametrize("form", [0, 1])
+@pytest.mark.parametrize("form", [0, 1, 2])
 def test_spmv_forms_match_the_reference_order(L, form):
     """`Csr::mul` (src/bicgstab.rs:72-82) bit for bit: each row's products summed in float in
     column order, then 0 + 1 * sum. Rows 512-767 hold 40 entries each (10240 in one block of
-    256 rows), past the tiled form's shared-memory tile, so its fallback runs too."""
+    256 rows), past the tiled form's shared-memory tile, so its fallback runs too; the sliced
+    form's last slice is partial (5000 rows), empty rows sit beside long ones, and rows 1000-
+    1009 run past 64 entries (its warp-per-row part), two of them past 1024 (the top length
+    class) and some with a partial last chunk of 32."""
     rng = np.random.default_rng(21)
     n = 5000
     lens = rng.integers(0, 31, n)
     lens[512:768] = 40
+    lens[1000:1010] = [65, 96, 100, 129, 200, 300, 997, 1030, 1500, 2047]
     starts = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
     cols = np.concatenate([np.sort(rng.choice(n, int(k), replace=False)) for k in lens]).astype(np.int32)
     vals = rng.uniform(-2, 2, int(starts[-1])).astype(np.float32)

@@ -609,50 +609,49 @@ static int64_t overlap_area(const Bin &b, const Instance &i, int32_t dbu) {
 // `BinGrid::updateBinsNonPlaceArea` (src/nesterov.rs:1956-2018).
 static void update_bins_non_place_area(Nb &nb) {
   auto &bg = nb.bg;
-  auto &fixed = nb.fixed;
-  for (auto &b : bg.bins) {
-    b.non_place = 0;
-    b.non_place_unscaled = 0;
-  }
-  size_t n = bg.bins.size();
-  std::vector<std::vector<int>> touching(n);
-  for (size_t k = 0; k < fixed.size(); k++) {
-    const Instance &i = fixed[k];
-    if (i.lx >= i.ux || i.ly >= i.uy) continue;
+  const auto &fixed = nb.fixed;
+  const size_t n = bg.bins.size();
+  // each bin's touching fixed instances in instance order (counts, their scan, a fill)
+  std::vector<int64_t> start(n + 1, 0);
+  auto each_bin = [&](const Instance &i, auto &&f) {
     auto [x0, x1] = bg.idx_x(i.lx, i.ux);
     auto [y0, y1] = bg.idx_y(i.ly, i.uy);
     for (int32_t y = y0; y < y1; y++)
-      for (int32_t x = x0; x < x1; x++) touching[(size_t)(y * bg.cnt_x + x)].push_back((int)k);
+      for (int32_t x = x0; x < x1; x++) f((size_t)(y * bg.cnt_x + x));
+  };
+  for (const Instance &i : fixed)
+    if (i.lx < i.ux && i.ly < i.uy) each_bin(i, [&](size_t b) { start[b + 1]++; });
+  for (size_t b = 0; b < n; b++) start[b + 1] += start[b];
+  std::vector<int32_t> touching((size_t)start[n]);
+  {
+    std::vector<int64_t> at(start.begin(), start.end() - 1);
+    for (size_t k = 0; k < fixed.size(); k++)
+      if (fixed[k].lx < fixed[k].ux && fixed[k].ly < fixed[k].uy) each_bin(fixed[k], [&](size_t b) { touching[(size_t)at[b]++] = (int32_t)k; });
   }
-  std::vector<int64_t> uni(n, 0);
-  for (size_t b = 0; b < n; b++) {
-    if (touching[b].empty()) continue;
-    const Bin &bin = bg.bins[b];
+  // per bin: the union of the touching boxes (the cap), and the sum of their overlaps (a
+  // degenerate instance overlaps nothing, so the touching ones give the whole sum)
+  parallel_for(n, [&](size_t b0, size_t b1) {
     std::vector<std::array<int32_t, 4>> rects;
-    for (int k : touching[b]) {
-      std::array<int32_t, 4> r = {std::max(fixed[k].lx, bin.lx), std::max(fixed[k].ly, bin.ly), std::min(fixed[k].ux, bin.ux), std::min(fixed[k].uy, bin.uy)};
-      if (r[0] < r[2] && r[1] < r[3]) rects.push_back(r);
-    }
-    uni[b] = union_area(rects);
-    bg.bins[b].non_place_unscaled = f2l((float)uni[b] * bg.bins[b].target_density);
-  }
-  std::vector<int64_t> raw(n, 0);
-  for (auto &i : fixed) {
-    auto [x0, x1] = bg.idx_x(i.lx, i.ux);
-    auto [y0, y1] = bg.idx_y(i.ly, i.uy);
-    for (int32_t y = y0; y < y1; y++)
-      for (int32_t x = x0; x < x1; x++) {
-        size_t b = (size_t)(y * bg.cnt_x + x);
-        raw[b] += overlap_area(bg.bins[b], i, nb.dbu);
+    for (size_t b = b0; b < b1; b++) {
+      Bin &bin = bg.bins[b];
+      bin.non_place = 0;
+      bin.non_place_unscaled = 0;
+      if (start[b] == start[b + 1]) continue;
+      rects.clear();
+      int64_t raw = 0;
+      for (int64_t t = start[b]; t < start[b + 1]; t++) {
+        const Instance &i = fixed[(size_t)touching[(size_t)t]];
+        std::array<int32_t, 4> r = {std::max(i.lx, bin.lx), std::max(i.ly, bin.ly), std::min(i.ux, bin.ux), std::min(i.uy, bin.uy)};
+        if (r[0] < r[2] && r[1] < r[3]) rects.push_back(r);
+        raw += overlap_area(bin, i, nb.dbu);
       }
-  }
-  for (size_t b = 0; b < n; b++)
-    if (raw[b] != 0) bg.bins[b].non_place += f2l((float)raw[b] * bg.bins[b].target_density);
-  for (size_t b = 0; b < n; b++) {
-    if (touching[b].empty()) continue;
-    int64_t cap = f2l((float)uni[b] * bg.bins[b].target_density * 1.10f);
-    if (bg.bins[b].non_place > cap) bg.bins[b].non_place = cap;
-  }
+      const int64_t uni = union_area(rects);
+      bin.non_place_unscaled = f2l((float)uni * bin.target_density);
+      if (raw != 0) bin.non_place += f2l((float)raw * bin.target_density);
+      const int64_t cap = f2l((float)uni * bin.target_density * 1.10f);
+      if (bin.non_place > cap) bin.non_place = cap;
+    }
+  }, 1024);
 }
 
 enum Slot { SLOT_PREV, SLOT_CUR, SLOT_NEXT };
@@ -725,40 +724,47 @@ static void perturb_place_insts(const Design &d, Common &c, Ip &ip, const Base &
   bool draws = c.site_y > 0 && dist != 0.0f;
   double r = dist > 0.0f ? (double)dist * ((double)d.dbu / 1000.0) : std::min(0.5 * (double)d.dbu, (double)c.site_y);
   double sigma = r * 0.3071963263271184;
-  for (int k : base.place_insts) {
-    int32_t xo = 0, yo = 0;
-    if (draws) {
+  // the draws in the reference's order, then each instance moved (its own instance, pins and
+  // cell: the instances are independent)
+  const size_t m = base.place_insts.size();
+  std::vector<int2> off(m, int2{0, 0});
+  if (draws)
+    for (size_t j = 0; j < m; j++) {
       double ddx = normal(rng, 0.0, sigma);
       double ddy = normal(rng, 0.0, sigma);
-      xo = f2i(std::round(ddx));
-      yo = f2i(std::round(ddy));
+      off[j] = int2{f2i(std::round(ddx)), f2i(std::round(ddy))};
     }
-    int gi = inst_cell[k];
-    if (!c.insts[k].locked) {
-      int32_t nx = c.insts[k].lx + xo, ny = c.insts[k].ly + yo;
-      Instance &i = c.insts[k];
-      int32_t w = i.dx(), h = i.dy();
-      i.lx = nx;
-      i.ly = ny;
-      i.ux = i.lx + w;
-      i.uy = i.ly + h;
-      int32_t icx = i.cx(), icy = i.cy();
-      for (int p : ip.inst_pins[k]) {
-        ip.pins[p].cx = icx + ip.pins[p].off_x;
-        ip.pins[p].cy = icy + ip.pins[p].off_y;
+  parallel_for(m, [&](size_t j0, size_t j1) {
+    for (size_t j = j0; j < j1; j++) {
+      const int k = base.place_insts[j];
+      const int32_t xo = off[j].x, yo = off[j].y;
+      int gi = inst_cell[k];
+      if (!c.insts[k].locked) {
+        int32_t nx = c.insts[k].lx + xo, ny = c.insts[k].ly + yo;
+        Instance &i = c.insts[k];
+        int32_t w = i.dx(), h = i.dy();
+        i.lx = nx;
+        i.ly = ny;
+        i.ux = i.lx + w;
+        i.uy = i.ly + h;
+        int32_t icx = i.cx(), icy = i.cy();
+        for (int p : ip.inst_pins[k]) {
+          ip.pins[p].cx = icx + ip.pins[p].off_x;
+          ip.pins[p].cy = icy + ip.pins[p].off_y;
+        }
       }
+      const Instance &i = c.insts[k];
+      GCell &cell = gcells[gi];
+      cell.lx = i.lx;
+      cell.ly = i.ly;
+      cell.ux = i.ux;
+      cell.uy = i.uy;
+      cell.dlx = i.lx;
+      cell.dly = i.ly;
+      cell.dux = i.ux;
+      cell.duy = i.uy;
     }
-    const Instance &i = c.insts[k];
-    GCell &cell = gcells[gi];
-    cell.lx = i.lx;
-    cell.ly = i.ly;
-    cell.ux = i.ux;
-    cell.uy = i.uy;
-    cell.dlx = i.lx;
-    cell.dly = i.ly;
-    cell.dux = i.ux;
-    cell.duy = i.uy;
-  }
+  }, 4096);
 }
 
 // `BinGrid::initBins` (src/nesterov.rs:1830-1898).

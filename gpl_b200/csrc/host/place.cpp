@@ -4,6 +4,7 @@
 // the solve itself on the device, and the random numbers (src/normal.rs) the Nesterov setup
 // draws.
 #include <algorithm>
+#include <atomic>
 #include <charconv>
 #include <cstdarg>
 #include <cstdio>
@@ -708,26 +709,35 @@ static Rect region_box_of(const Design &d, int r) {
 // `placeInstsInitialPositions` (src/initial_place.rs:169-199).
 static void place_insts_initial_positions(Log &log, const Design &d, Common &c, Ip &ip, const IpVars &vars) {
   int32_t ccx = (d.core.lx + d.core.ux) / 2, ccy = (d.core.ly + d.core.uy) / 2;
-  long region = 0, db = 0, core = 0;
-  std::vector<int> place = ip.place;
-  for (int k : place) {
-    if (c.insts[k].locked) continue;
-    const DbInst &di = d.insts[c.insts[k].db];
-    int reg = di.group >= 0 ? d.groups[di.group].region : -1;
-    if (reg >= 0) {
-      Rect b = region_box_of(d, reg);
-      set_center_location(c, ip, k, b.ux - (b.ux - b.lx) / 2, b.uy - (b.uy - b.ly) / 2);
-      region++;
-    } else if (!vars.force_center && di.placed) {
-      Rect b = di.bbox;
-      set_center_location(c, ip, k, (b.lx + b.ux) / 2, (b.ly + b.uy) / 2);
-      db++;
-    } else {
-      set_center_location(c, ip, k, ccx, ccy);
-      core++;
+  // each instance moves with its own pins only, so the instances go in parallel; the
+  // counters are summed over the chunks
+  std::atomic<long> region{0}, db{0}, core{0};
+  const std::vector<int> &place = ip.place;
+  parallel_for(place.size(), [&](size_t a, size_t b) {
+    long n_region = 0, n_db = 0, n_core = 0;
+    for (size_t e = a; e < b; e++) {
+      const int k = place[e];
+      if (c.insts[k].locked) continue;
+      const DbInst &di = d.insts[c.insts[k].db];
+      int reg = di.group >= 0 ? d.groups[di.group].region : -1;
+      if (reg >= 0) {
+        Rect r = region_box_of(d, reg);
+        set_center_location(c, ip, k, r.ux - (r.ux - r.lx) / 2, r.uy - (r.uy - r.ly) / 2);
+        n_region++;
+      } else if (!vars.force_center && di.placed) {
+        Rect r = di.bbox;
+        set_center_location(c, ip, k, (r.lx + r.ux) / 2, (r.ly + r.uy) / 2);
+        n_db++;
+      } else {
+        set_center_location(c, ip, k, ccx, ccy);
+        n_core++;
+      }
     }
-  }
-  log.info("GPL", 51, sfmt("Source of initial instance position counters:\n\tOdb location = %ld\tCore center = %ld\tRegion center = %ld", db, core, region));
+    region += n_region;
+    db += n_db;
+    core += n_core;
+  });
+  log.info("GPL", 51, sfmt("Source of initial instance position counters:\n\tOdb location = %ld\tCore center = %ld\tRegion center = %ld", db.load(), core.load(), region.load()));
 }
 
 static uint64_t fnv_f32(const std::vector<float> &v) {

@@ -8,6 +8,7 @@
 // entries sorted by (column, position)), the first occurrence first, as the reference sums
 // them into the first.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "b2b.h"
@@ -846,6 +847,11 @@ cudaError_t IpDevice::slice(Axis &A) {
 }
 
 cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
+  // GPL_SPMV_FORM (0 rows, 1 tiled, 2 sliced) fixes the SpMV form instead of timing them:
+  // the forms give the same products bit for bit, so it changes only the speed
+  if (spmv_form_ < 0)
+    if (const char *f = std::getenv("GPL_SPMV_FORM"))
+      if (f[0] >= '0' && f[0] <= '2' && f[1] == 0) spmv_form_ = f[0] - '0';
   // the sliced copies when the sliced form may run: before the first solve picks a form, and
   // while it is the form picked
   const bool sliced = spmv_form_ < 0 || spmv_form_ == kSpmvSliced;

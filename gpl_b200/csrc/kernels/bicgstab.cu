@@ -42,10 +42,10 @@ __device__ __forceinline__ double loop_state(const double *S) {
 //  rows:  a thread per row straight from memory;
 //  tiled: a block's rows are contiguous in the CSR arrays, so the block first forms every
 //         product vals[k] * x[cols[k]] of its rows with coalesced loads into shared memory
-//         (four entries per thread in flight), then each thread sums its row's products; a
+//         (eight entries per thread in flight), then each thread sums its row's products; a
 //         block whose rows hold more than kSpmvTile entries sums straight from memory.
 constexpr int kSpmvTile = 6144;
-constexpr int kSpmvUnroll = 4;
+constexpr int kSpmvUnroll = 8;
 
 __device__ __forceinline__ void spmv_rows_body(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
   if (gated_off(S, gate)) return;

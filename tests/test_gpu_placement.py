@@ -76,6 +76,20 @@ def test_initial_place_rounds_match_the_oracle(cfg1):
         assert abs(ha - hb) <= 1e-3 * hb
 
 
+def test_initial_place_spmv_forms_agree(cfg1, monkeypatch):
+    """The initial placement with each SpMV form forced (GPL_SPMV_FORM: a thread per row,
+    block-staged, sliced): the solves' products are the same bit for bit in every form, so the
+    placed locations and every report line are identical."""
+    d, _ = cfg1
+    runs = []
+    for form in ("0", "1", "2"):
+        monkeypatch.setenv("GPL_SPMV_FORM", form)
+        runs.append(engine.global_placement(d, ARGS + ["-skip_nesterov_place"]))
+    for r in runs[1:]:
+        assert np.array_equal(r["locations"], runs[0]["locations"])
+        assert r["lines"] == runs[0]["lines"]
+
+
 def _lines_with(lines, code):
     return [l for l in lines if f"GPL-{code}]" in l]
 

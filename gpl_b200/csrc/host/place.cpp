@@ -318,6 +318,8 @@ Common placer_base_common(Log &log, const Design &d, const Vars &v) {
   Common c;
   c.site_x = site_x;
   c.site_y = site_y;
+  c.insts.reserve(d.insts.size());
+  c.nets.reserve(d.nets.size());
   for (size_t k = 0; k < d.insts.size(); k++) {
     const DbInst &di = d.insts[k];
     if (!di.core_auto_placeable) continue;
@@ -356,21 +358,28 @@ Common placer_base_common(Log &log, const Design &d, const Vars &v) {
   log.info("GPL", 36, sfmt("Movable instances area:     %10.3f um^2", dbu_area_to_microns(d, movable_area)));
   log.info("GPL", 37, sfmt("Total instances area:       %10.3f um^2", dbu_area_to_microns(d, total_area)));
   double avg_density = movable_area > 0 ? (double)total_signal_pins / (double)movable_area : 0.0;
-  int64_t total_adjustment_area = 0;
+  // each instance grows by its own pin count alone: the instances go in parallel, and the
+  // total is an integer sum
+  std::atomic<int64_t> total_adjustment_area{0};
   if (!v.disable_pin_density_adjust) {
-    for (auto &i : c.insts) {
-      if (!i.fixed && i.db >= 0) {
-        int64_t pins = signal_pins(i);
-        if (pins > 2 && avg_density > 0.0) {
-          double target_area = (double)pins / avg_density;
-          double scale = std::sqrt(target_area / (double)i.area());
-          scale = std::min(std::max(scale, 0.95), 1.2);  // f64::clamp
-          total_adjustment_area += i.extend_size_by_scale(scale);
+    parallel_for(c.insts.size(), [&](size_t a, size_t b) {
+      int64_t part = 0;
+      for (size_t k = a; k < b; k++) {
+        Instance &i = c.insts[k];
+        if (!i.fixed && i.db >= 0) {
+          int64_t pins = signal_pins(i);
+          if (pins > 2 && avg_density > 0.0) {
+            double target_area = (double)pins / avg_density;
+            double scale = std::sqrt(target_area / (double)i.area());
+            scale = std::min(std::max(scale, 0.95), 1.2);  // f64::clamp
+            part += i.extend_size_by_scale(scale);
+          }
         }
       }
-    }
+      total_adjustment_area += part;
+    });
   }
-  log.info("GPL", 35, sfmt("Pin density area adjust:    %10.3f um^2", dbu_area_to_microns(d, total_adjustment_area)));
+  log.info("GPL", 35, sfmt("Pin density area adjust:    %10.3f um^2", dbu_area_to_microns(d, total_adjustment_area.load())));
   int64_t pins = 0;
   for (size_t k = 0; k < d.nets.size(); k++) {
     const DbNet &n = d.nets[k];

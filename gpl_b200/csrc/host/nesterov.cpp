@@ -660,12 +660,12 @@ enum Slot { SLOT_PREV, SLOT_CUR, SLOT_NEXT };
 // `initFillerGCells` (src/nesterov.rs:1690-1753).
 static std::vector<GCell> init_filler_gcells(Log &log, const Design &d, const Common &c, const Base &base, Nb &nb, const Opts &o) {
   std::vector<int32_t> dxs, dys;
+  dxs.reserve(base.place_insts.size());
+  dys.reserve(base.place_insts.size());
   for (int k : base.place_insts) {
     dxs.push_back(c.insts[k].dx());
     dys.push_back(c.insts[k].dy());
   }
-  std::sort(dxs.begin(), dxs.end());
-  std::sort(dys.begin(), dys.end());
   size_t n = dxs.size();
   int32_t lo = f2i((double)n * 0.05), hi = f2i((double)n * 0.95);
   if (lo == hi) {
@@ -673,6 +673,12 @@ static std::vector<GCell> init_filler_gcells(Log &log, const Design &d, const Co
     hi = (int32_t)n;
   }
   if (lo == hi) refuse("a region with no placeable instance (no filler size) is not modelled");
+  // the sorted sizes' ranks [lo, hi): two partitions put exactly those values there (their
+  // integer sum needs no further order)
+  for (auto *v : {&dxs, &dys}) {
+    if (lo > 0) std::nth_element(v->begin(), v->begin() + lo, v->end());
+    if ((size_t)hi < n) std::nth_element(v->begin() + lo, v->begin() + hi, v->end());
+  }
   int64_t sx = 0, sy = 0;
   for (int32_t i = lo; i < hi; i++) {
     sx += dxs[i];

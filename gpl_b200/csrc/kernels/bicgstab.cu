@@ -189,12 +189,31 @@ __global__ void __launch_bounds__(kThreads) k_len_hist(int64_t n, const int64_t 
   for (int b = threadIdx.x; b <= kSliceLenCap; b += kThreads)
     if (h[b]) atomicAdd(&count[b], h[b]);
 }
-__global__ void k_len_starts(int32_t *count) {  // one thread: counts to starts, longest first
-  int32_t run = 0;
-  for (int b = kSliceLenCap; b >= 0; b--) {
-    const int32_t c = count[b];
-    count[b] = run;
-    run += c;
+// The counts to starts, longest first: one warp, each lane a run of classes (its loads in
+// flight together), the runs' totals scanned across the warp.
+constexpr int kLenPerLane = (kSliceLenCap + 1 + 31) / 32;
+__global__ void k_len_starts(int32_t *count) {
+  const int lane = threadIdx.x;
+  int32_t c[kLenPerLane];
+  int32_t sum = 0;
+#pragma unroll
+  for (int q = 0; q < kLenPerLane; q++) {
+    const int b = kSliceLenCap - (lane * kLenPerLane + q);  // descending
+    c[q] = b >= 0 ? count[b] : 0;
+    sum += c[q];
+  }
+  int32_t run = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int32_t y = __shfl_up_sync(0xffffffffu, run, o);
+    if (lane >= o) run += y;
+  }
+  run -= sum;  // exclusive
+#pragma unroll
+  for (int q = 0; q < kLenPerLane; q++) {
+    const int b = kSliceLenCap - (lane * kLenPerLane + q);
+    if (b >= 0) count[b] = run;
+    run += c[q];
   }
 }
 __global__ void __launch_bounds__(kThreads) k_len_scatter(int64_t n, const int64_t *__restrict__ rs, int32_t *__restrict__ cursor, int32_t *__restrict__ row, int32_t *__restrict__ len) {
@@ -481,7 +500,7 @@ cudaError_t csr_slice_order(const CsrDev &A, int32_t *row, int32_t *len, int32_t
   cudaError_t e = cudaMemsetAsync(count, 0, (kSliceLenCap + 1) * sizeof(int32_t), st);
   if (e != cudaSuccess) return e;
   k_len_hist<<<g, kThreads, 0, st>>>(A.n, A.rs, count);
-  k_len_starts<<<1, 1, 0, st>>>(count);
+  k_len_starts<<<1, 32, 0, st>>>(count);
   k_len_scatter<<<g, kThreads, 0, st>>>(A.n, A.rs, count, row, len);
   return cudaGetLastError();
 }

@@ -174,8 +174,8 @@ int gpl_kernel_spmv(int64_t n, const int64_t *row_start, const int32_t *cols, co
   // the sliced copy: the order by length and the slice widths on the device, their
   // exclusive scan here, the entries
   int64_t *starts = nullptr;
-  int32_t *row = nullptr, *len = nullptr, *count = nullptr, *sc = nullptr;
-  float *sv = nullptr;
+  int32_t *row = nullptr, *len = nullptr, *count = nullptr;
+  int2 *ent = nullptr;
   int32_t n_long = 0;
   cudaError_t e = cudaMalloc(&row, (size_t)n * sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMalloc(&len, (size_t)n * sizeof(int32_t));
@@ -200,22 +200,20 @@ int gpl_kernel_spmv(int64_t n, const int64_t *row_start, const int32_t *cols, co
     e = cudaMemcpyAsync(starts, h.data(), (size_t)(ns + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s);
   }
   const size_t total = (size_t)std::max<int64_t>(h[(size_t)ns], 1);
-  if (e == cudaSuccess) e = cudaMalloc(&sc, total * sizeof(int32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&sv, total * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&ent, total * sizeof(int2));
   if (e == cudaSuccess) {
     A.sl_long = n_long;
     A.sl_row = row;
     A.sl_len = len;
     A.sl_start = starts;
-    e = csr_slice_fill(A, sc, sv, s);
+    e = csr_slice_fill(A, ent, s);
   }
   if (e == cudaSuccess) {
-    A.sl_cols = sc;
-    A.sl_vals = sv;
+    A.sl_ent = ent;
     e = spmv(A, x, y, form, s);
   }
   cudaError_t e2 = cudaStreamSynchronize(s);
-  for (void *p : {(void *)starts, (void *)row, (void *)len, (void *)count, (void *)sc, (void *)sv}) cudaFree(p);
+  for (void *p : {(void *)starts, (void *)row, (void *)len, (void *)count, (void *)ent}) cudaFree(p);
   return (int)(e != cudaSuccess ? e : e2);
 }
 

@@ -612,7 +612,7 @@ void IpDevice::release() {
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, s_);
   for (auto &a : ax_) {
-    void *q[] = {a.starts, a.cols, a.vals, a.rhs, a.x, a.sl_row, a.sl_len, a.sl_count, a.sl_start, a.sl_cols, a.sl_vals};
+    void *q[] = {a.starts, a.cols, a.vals, a.rhs, a.x, a.sl_row, a.sl_len, a.sl_count, a.sl_start, a.sl_ent};
     for (void *p : q)
       if (p) cudaFreeAsync(p, s_);
     a = Axis{};
@@ -836,12 +836,12 @@ cudaError_t IpDevice::slice(Axis &A) {
   CK(cudaMemcpyAsync(&total, A.sl_start + ns, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
   CK(cudaStreamSynchronize(s_));
   d2h_bytes += sizeof(int64_t) + sizeof(int32_t);
-  CK(grow(s_, (size_t)std::max<int64_t>(total, 1), A.sl_cap, &A.sl_cols, &A.sl_vals));
+  CK(grow(s_, (size_t)std::max<int64_t>(total, 1), A.sl_cap, &A.sl_ent));
   m.sl_long = n_long;
   m.sl_row = A.sl_row;
   m.sl_len = A.sl_len;
   m.sl_start = A.sl_start;
-  CK(csr_slice_fill(m, A.sl_cols, A.sl_vals, s_));
+  CK(csr_slice_fill(m, A.sl_ent, s_));
   launches += 8;
   return cudaSuccess;
 }
@@ -869,8 +869,7 @@ cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
       m[a].sl_row = A.sl_row;
       m[a].sl_len = A.sl_len;
       m[a].sl_start = A.sl_start;
-      m[a].sl_cols = A.sl_cols;
-      m[a].sl_vals = A.sl_vals;
+      m[a].sl_ent = A.sl_ent;
     }
     b[a] = A.rhs;
     x[a] = A.x;

@@ -106,8 +106,7 @@ class IpDevice {
     int64_t sl_long = 0;
     int32_t *sl_row = nullptr, *sl_len = nullptr, *sl_count = nullptr;
     int64_t *sl_start = nullptr;
-    int32_t *sl_cols = nullptr;
-    float *sl_vals = nullptr;
+    int2 *sl_ent = nullptr;
     size_t sl_cap = 0, sl_start_cap = 0, sl_row_cap = 0, sl_count_cap = 0;
   } ax_[2];
   void *scratch_ = nullptr;

@@ -116,7 +116,7 @@ __global__ void __launch_bounds__(kThreads) k_spmv_tiled(int64_t n, const int64_
 constexpr int kLongChunks = 4;
 __host__ __device__ __forceinline__ int64_t sliced_long_blocks(int64_t n_long) { return (n_long + kThreads / 32 - 1) / (kThreads / 32); }
 __host__ __device__ __forceinline__ int64_t sliced_blocks(int64_t n, int64_t n_long) { return sliced_long_blocks(n_long) + (n - n_long + kThreads - 1) / kThreads; }
-__device__ __forceinline__ void spmv_sliced_body(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int32_t *__restrict__ sl_cols, const float *__restrict__ sl_vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
+__device__ __forceinline__ void spmv_sliced_body(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int2 *__restrict__ sl_ent, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
   if (gated_off(S, gate)) return;
   const int64_t lb = sliced_long_blocks(n_long);
   if (blockIdx.x < lb) {
@@ -154,27 +154,26 @@ __device__ __forceinline__ void spmv_sliced_body(int64_t n, int64_t n_long, cons
   if (j >= n) return;
   const int32_t len = sl_len[j];
   const int64_t base = sl_start[i / kSliceRows] + (i % kSliceRows);
-  const int32_t *c = sl_cols + base;
-  const float *v = sl_vals + base;
+  const int2 *ent = sl_ent + base;
   float tmp = 0.0f;
   int32_t k = 0;
   for (; k + kSpmvUnroll <= len; k += kSpmvUnroll) {
-    int cc[kSpmvUnroll];
-    float vv[kSpmvUnroll], xv[kSpmvUnroll];
+    int2 cv[kSpmvUnroll];
+    float xv[kSpmvUnroll];
 #pragma unroll
-    for (int u = 0; u < kSpmvUnroll; u++) {
-      cc[u] = __ldg(c + (int64_t)(k + u) * kSliceRows);
-      vv[u] = __ldg(v + (int64_t)(k + u) * kSliceRows);
-    }
+    for (int u = 0; u < kSpmvUnroll; u++) cv[u] = __ldg(ent + (int64_t)(k + u) * kSliceRows);
 #pragma unroll
-    for (int u = 0; u < kSpmvUnroll; u++) xv[u] = __ldg(x + cc[u]);
+    for (int u = 0; u < kSpmvUnroll; u++) xv[u] = __ldg(x + cv[u].x);
 #pragma unroll
-    for (int u = 0; u < kSpmvUnroll; u++) tmp = __fadd_rn(tmp, __fmul_rn(vv[u], xv[u]));
+    for (int u = 0; u < kSpmvUnroll; u++) tmp = __fadd_rn(tmp, __fmul_rn(__int_as_float(cv[u].y), xv[u]));
   }
-  for (; k < len; k++) tmp = __fadd_rn(tmp, __fmul_rn(__ldg(v + (int64_t)k * kSliceRows), __ldg(x + __ldg(c + (int64_t)k * kSliceRows))));
+  for (; k < len; k++) {
+    const int2 cv = __ldg(ent + (int64_t)k * kSliceRows);
+    tmp = __fadd_rn(tmp, __fmul_rn(__int_as_float(cv.y), __ldg(x + cv.x)));
+  }
   y[sl_row[j]] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
 }
-__global__ void __launch_bounds__(kThreads) k_spmv_sliced(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int32_t *__restrict__ sl_cols, const float *__restrict__ sl_vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) { spmv_sliced_body(n, n_long, rs, cols, vals, sl_row, sl_len, sl_start, sl_cols, sl_vals, x, y, S, gate); }
+__global__ void __launch_bounds__(kThreads) k_spmv_sliced(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int2 *__restrict__ sl_ent, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) { spmv_sliced_body(n, n_long, rs, cols, vals, sl_row, sl_len, sl_start, sl_ent, x, y, S, gate); }
 
 // The order by length: a histogram of the (capped) lengths per block in shared memory, the
 // buckets' starts longest first, then each row's position from its bucket's cursor (a warp's
@@ -240,21 +239,18 @@ __global__ void __launch_bounds__(kThreads) k_slice_widths(int64_t n, int64_t n_
   const unsigned m = __reduce_max_sync(0xffffffffu, l);
   if ((threadIdx.x & 31) == 0) widths[i / kSliceRows] = (int64_t)m * kSliceRows;
 }
-__global__ void __launch_bounds__(kThreads) k_slice_fill(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, int32_t *__restrict__ sl_cols, float *__restrict__ sl_vals) {
+__global__ void __launch_bounds__(kThreads) k_slice_fill(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, int2 *__restrict__ sl_ent) {
   const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x, j = n_long + i;
   if (j >= n) return;
   const int64_t b = rs[sl_row[j]];
   const int32_t len = sl_len[j];
   const int64_t base = sl_start[i / kSliceRows] + (i % kSliceRows);
-  for (int32_t k = 0; k < len; k++) {
-    sl_cols[base + (int64_t)k * kSliceRows] = cols[b + k];
-    sl_vals[base + (int64_t)k * kSliceRows] = vals[b + k];
-  }
+  for (int32_t k = 0; k < len; k++) sl_ent[base + (int64_t)k * kSliceRows] = make_int2(cols[b + k], __float_as_int(vals[b + k]));
 }
 
 static void spmv_launch(int form, int eb, cudaStream_t st, const CsrDev &A, const float *in, float *o, const double *S, int gate) {
   if (form == kSpmvSliced)
-    k_spmv_sliced<<<(unsigned)std::max<int64_t>(sliced_blocks(A.n, A.sl_long), 1), kThreads, 0, st>>>(A.n, A.sl_long, A.rs, A.cols, A.vals, A.sl_row, A.sl_len, A.sl_start, A.sl_cols, A.sl_vals, in, o, S, gate);
+    k_spmv_sliced<<<(unsigned)std::max<int64_t>(sliced_blocks(A.n, A.sl_long), 1), kThreads, 0, st>>>(A.n, A.sl_long, A.rs, A.cols, A.vals, A.sl_row, A.sl_len, A.sl_start, A.sl_ent, in, o, S, gate);
   else if (form == kSpmvTiled)
     k_spmv_tiled<<<eb, kThreads, 0, st>>>(A.n, A.rs, A.cols, A.vals, in, o, S, gate);
   else
@@ -425,8 +421,7 @@ struct SysDev {
   int64_t sl_long;
   const int32_t *sl_row, *sl_len;
   const int64_t *sl_start;
-  const int32_t *sl_cols;
-  const float *sl_vals;
+  const int2 *sl_ent;
   float *x, *r, *r0, *v, *p, *s, *t;
   double *part, *S;
   unsigned int *ticket;
@@ -451,7 +446,7 @@ __global__ void __launch_bounds__(kThreads) k2_spmv_tiled(SysPair P, int sel) {
 }
 __global__ void __launch_bounds__(kThreads) k2_spmv_sliced(SysPair P, int sel) {
   SysDev q = pick(P);
-  spmv_sliced_body(q.n, q.sl_long, q.rs, q.cols, q.vals, q.sl_row, q.sl_len, q.sl_start, q.sl_cols, q.sl_vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
+  spmv_sliced_body(q.n, q.sl_long, q.rs, q.cols, q.vals, q.sl_row, q.sl_len, q.sl_start, q.sl_ent, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
 }
 // sel 0: r0.v, then alpha; sel 1: t.t and t.s, then omega
 __global__ void k2_dots(SysPair P, int sel) {
@@ -511,9 +506,9 @@ cudaError_t csr_slice_widths(int64_t n, int64_t n_long, const int32_t *len, int6
   return cudaGetLastError();
 }
 
-cudaError_t csr_slice_fill(const CsrDev &A, int32_t *sl_cols, float *sl_vals, cudaStream_t st) {
+cudaError_t csr_slice_fill(const CsrDev &A, int2 *sl_ent, cudaStream_t st) {
   if (A.n - A.sl_long <= 0) return cudaSuccess;
-  k_slice_fill<<<(unsigned)((A.n - A.sl_long + kThreads - 1) / kThreads), kThreads, 0, st>>>(A.n, A.sl_long, A.rs, A.cols, A.vals, A.sl_row, A.sl_len, A.sl_start, sl_cols, sl_vals);
+  k_slice_fill<<<(unsigned)((A.n - A.sl_long + kThreads - 1) / kThreads), kThreads, 0, st>>>(A.n, A.sl_long, A.rs, A.cols, A.vals, A.sl_row, A.sl_len, A.sl_start, sl_ent);
   return cudaGetLastError();
 }
 
@@ -648,8 +643,7 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
     q.sl_row = A[a].sl_row;
     q.sl_len = A[a].sl_len;
     q.sl_start = A[a].sl_start;
-    q.sl_cols = A[a].sl_cols;
-    q.sl_vals = A[a].sl_vals;
+    q.sl_ent = A[a].sl_ent;
     q.x = x[a];
     q.r = (float *)base;
     q.r0 = (float *)(base + vec);

@@ -21,14 +21,14 @@ struct CsrDev {
   // the rest are cut into slices of kSliceRows positions, each slice stored column-major at
   // its longest row's width: with i = j - sl_long, entry k sits at sl_start[i / kSliceRows] +
   // kSliceRows * k + i % kSliceRows, so a warp's k-th entries are one coalesced run and its
-  // rows end together. Built by csr_slice_order, csr_slice_widths, a scan, and
+  // rows end together; an entry is one 8-byte word (x: the column, y: the value's bits), so
+  // a step is one load. Built by csr_slice_order, csr_slice_widths, a scan, and
   // csr_slice_fill; NULL when not built.
   int64_t sl_long = 0;
   const int32_t *sl_row = nullptr;
   const int32_t *sl_len = nullptr;
   const int64_t *sl_start = nullptr;
-  const int32_t *sl_cols = nullptr;
-  const float *sl_vals = nullptr;
+  const int2 *sl_ent = nullptr;
 };
 struct BicgResult {
   int iterations;
@@ -52,7 +52,7 @@ cudaError_t csr_slice_order(const CsrDev &A, int32_t *row, int32_t *len, int32_t
 // exclusive scan of them (total at [slices]) gives sl_start.
 cudaError_t csr_slice_widths(int64_t n, int64_t n_long, const int32_t *len, int64_t *widths, cudaStream_t s);
 // The sliced copy's entries from A's CSR arrays (A.sl_long, sl_row, sl_len, sl_start set).
-cudaError_t csr_slice_fill(const CsrDev &A, int32_t *sl_cols, float *sl_vals, cudaStream_t s);
+cudaError_t csr_slice_fill(const CsrDev &A, int2 *sl_ent, cudaStream_t s);
 // Scratch the solve needs (seven vectors of n floats, the partials and the scalars).
 size_t bicgstab_scratch_bytes(int64_t n);
 // Solve A x = b from the start point in x; `scratch` holds bicgstab_scratch_bytes(n) bytes.

@@ -49,18 +49,62 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+    """SM clock and throttle reasons sampled during the timed region: NVML (read-only queries)
+    every 10 ms on a thread, plus one reading as the region opens and one as it closes, so a
+    region of a few milliseconds still has samples; nvidia-smi when NVML is unavailable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device):
         self.device = device
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.rows = []  # (sm MHz, max sm MHz, set of reasons)
+        self.nv = None
+        self.h = None
         self.p = None
+        self.f = None
+        self.stop = None
+        self.thread = None
+
+    def _nvml_open(self):
+        import pynvml as nv
+        import torch
+        nv.nvmlInit()
+        props = torch.cuda.get_device_properties(self.device)
+        bus = "%08x:%02x:%02x.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+        self.h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+        self.nv = nv
+        self.bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                     nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+
+    def _sample(self):
+        nv = self.nv
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+            mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            self.rows.append((float(sm), float(mx), {n for n, b in zip(self.NAMES, self.bits) if r & b}))
+        except Exception:
+            pass
 
     def __enter__(self):
         try:
+            self._nvml_open()
+        except Exception:
+            self.nv = None
+        if self.nv is not None:
+            self.stop = threading.Event()
+
+            def loop():
+                while not self.stop.wait(0.01):
+                    self._sample()
+            self._sample()
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return self
+        try:
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.p = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
@@ -69,6 +113,14 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self.nv is not None:
+            self._sample()
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
         if self.p:
             self.p.terminate()
             try:
@@ -77,21 +129,21 @@ class Clocks:
                 self.p.kill()
 
     def summary(self):
-        self.f.flush()
-        rows = []
-        for line in open(self.f.name):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 9:
-                rows.append(parts)
-        os.unlink(self.f.name)
+        rows = list(self.rows)
+        source = "nvml"
+        if self.f is not None:
+            source = "nvidia-smi"
+            self.f.flush()
+            for line in open(self.f.name):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    mx = float(parts[2]) if parts[2].replace(".", "").isdigit() else 0.0
+                    rows.append((float(parts[1]), mx, {self.NAMES[i] for i in range(4) if parts[5 + i].lower() in ("active", "1")}))
+            os.unlink(self.f.name)
         if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() in ("active", "1")})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock samples"]}
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": sorted(set().union(*(r[2] for r in rows))), "samples": len(rows), "source": source}
 
 
 def algorithmic(phase, C, P, N, B, mixed, nx):

@@ -3,9 +3,12 @@
 
 Workload (one "step" = one Nesterov iteration with its back-tracking trials): the 1M-cell
 synthetic design (about 1.05M nets, 4M pins, 32 macros over 15 % of the core) with a
-1024 x 1024 bin grid, `-density 0.70 -bin_grid_count 1024`, after construction, the initial
-placement and the Nesterov set-up (untimed). The mixed form (split-BF16 tcgen05 density
-solve) is the headline; the plain FP32 form is timed beside it on the same placement run.
+1024 x 1024 bin grid, `-density 0.70 -bin_grid_count 1024`, the loop started from the
+generator's spread placement with the initial placement skipped, after construction, the
+Nesterov set-up and W warm-up iterations (untimed). Both arms time the same iterations of the
+same loop from the same state. The mixed form (split-BF16 tcgen05 density solve) is the
+headline; the plain FP32 form is timed on the next K iterations of the same run. `e2e` is the
+whole command (construction and the device's initial placement included) through the C ABI.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -16,7 +19,8 @@ events for the phase shares and the roofline of the dominant kernel.
 N > 1 (under torchrun): one independent replica per GPU (the path has no exchange step), the
 time is the max over ranks, `value` the iterations of all ranks over it.
 --impl reference: the reference's CPU path (its restatement, single-threaded as the reference
-is) on the same workload, each step one Nesterov iteration.
+is) on the same workload, the same W warm-up and K timed iterations; the GPU line's
+cpu_baseline is the same sample.
 """
 import argparse
 import json
@@ -50,8 +54,8 @@ def peaks():
 
 class Clocks:
     """SM clock and throttle reasons sampled during the timed region: NVML (read-only queries)
-    every 10 ms on a thread, plus one reading as the region opens and one as it closes, so a
-    region of a few milliseconds still has samples; nvidia-smi when NVML is unavailable."""
+    every 2 ms on a thread; a reading as the region opens and one as it closes stand in only when
+    the region was too short for the poll; nvidia-smi when NVML cannot answer."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -71,24 +75,35 @@ class Clocks:
         import pynvml as nv
         import torch
         nv.nvmlInit()
-        props = torch.cuda.get_device_properties(self.device)
-        bus = "%08x:%02x:%02x.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
-        self.h = nv.nvmlDeviceGetHandleByPciBusId(bus)
-        self.nv = nv
-        self.bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
-                     nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
-
-    def _sample(self):
-        nv = self.nv
         try:
-            sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
-            mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
-            r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
-            self.rows.append((float(sm), float(mx), {n for n, b in zip(self.NAMES, self.bits) if r & b}))
+            props = torch.cuda.get_device_properties(self.device)
+            bus = "%08x:%02x:%02x.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+            self.h = nv.nvmlDeviceGetHandleByPciBusId(bus)
+            self.nv = nv
+            self.bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                         nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            self._read()  # one trial query: a binding that cannot answer falls back to nvidia-smi
         except Exception:
-            pass
+            self.nv = None
+            nv.nvmlShutdown()
+            raise
+
+    def _read(self):
+        nv = self.nv
+        sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        return (float(sm), float(mx), {n for n, b in zip(self.NAMES, self.bits) if r & b})
+
+    def _sample(self, into):
+        try:
+            into.append(self._read())
+        except Exception:
+            self.errors += 1
 
     def __enter__(self):
+        self.errors = 0
+        self.edge = []  # the readings as the region opens and closes
         try:
             self._nvml_open()
         except Exception:
@@ -97,9 +112,9 @@ class Clocks:
             self.stop = threading.Event()
 
             def loop():
-                while not self.stop.wait(0.01):
-                    self._sample()
-            self._sample()
+                while not self.stop.wait(0.002):
+                    self._sample(self.rows)
+            self._sample(self.edge)
             self.thread = threading.Thread(target=loop, daemon=True)
             self.thread.start()
             return self
@@ -114,7 +129,7 @@ class Clocks:
 
     def __exit__(self, *a):
         if self.nv is not None:
-            self._sample()
+            self._sample(self.edge)
             self.stop.set()
             self.thread.join(timeout=5)
             try:
@@ -129,7 +144,9 @@ class Clocks:
                 self.p.kill()
 
     def summary(self):
-        rows = list(self.rows)
+        # the readings taken while the work ran; the two edge readings only when the poll took
+        # none (the opening one can catch a clock still ramping up)
+        rows = list(self.rows) or list(getattr(self, "edge", []))
         source = "nvml"
         if self.f is not None:
             source = "nvidia-smi"
@@ -143,7 +160,8 @@ class Clocks:
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no clock samples"]}
         return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": sorted(set().union(*(r[2] for r in rows))), "samples": len(rows), "source": source}
+                "reasons": sorted(set().union(*(r[2] for r in rows))), "samples": len(rows), "source": source,
+                "edge_only": not self.rows and self.f is None}
 
 
 def algorithmic(phase, C, P, N, B, mixed, nx):
@@ -182,6 +200,41 @@ def log(msg):
 T0 = time.perf_counter()
 
 
+START = {
+    "spread": "the generator's spread placement, initial placement skipped (both arms)",
+    "ip": "after the initial placement (profiling case)",
+}
+
+
+def workload(a, design):
+    """The workload as both arms name it: the same keys and values in either line."""
+    cfg = CONFIGS[a.config]
+    nx = int(cfg["args"][cfg["args"].index("-bin_grid_count") + 1])
+    m = design.meta
+    return {"workload": cfg["name"], "args": cfg["args"], "design": m["config"], "cells": m["cells"], "nets": m["nets"],
+            "pins": m["pins"], "bins": nx * nx, "start": START[a.start] if not a.start_from else "a saved initial placement",
+            "timed": f"Nesterov iterations {a.warmup + 1}..{a.warmup + a.steps} of the loop (iteration = step)",
+            "parallelism": "replicas x1", "l2": "working set > L2 (126 MB): cells, pins and bins stream from HBM each trial"}
+
+
+def loop_design(a):
+    """The design the timed loop starts from, and the command's arguments for it."""
+    from gpl_b200 import synth
+    cfg = CONFIGS[a.config]
+    design = synth.generate(cfg["preset"], placed=a.start == "spread")
+    if a.start_from:
+        # the saved initial placement as the design's placement (lower-left corners), so the
+        # loop starts where the initial placement left it without running it again
+        loc = np.load(a.start_from)
+        box = design.inst_box
+        w, h = box[loc[:, 0], 2] - box[loc[:, 0], 0], box[loc[:, 0], 3] - box[loc[:, 0], 1]
+        box[loc[:, 0], 0], box[loc[:, 0], 1] = loc[:, 1], loc[:, 2]
+        box[loc[:, 0], 2], box[loc[:, 0], 3] = loc[:, 1] + w, loc[:, 2] + h
+        design.inst_flags[loc[:, 0]] |= synth.INST_PLACED
+    skip_ip = a.start == "spread" or bool(a.start_from)
+    return design, cfg["args"] + (["-skip_initial_place"] if skip_ip else [])
+
+
 def ours(a):
     import torch
     import torch.distributed as dist
@@ -204,21 +257,10 @@ def ours(a):
         if a.save_placement:
             np.save(a.save_placement, r["locations"])
         return
-    design = synth.generate(cfg["preset"], placed=a.start == "placed")
-    if a.start_from:
-        # the saved initial placement as the design's placement (lower-left corners), so the
-        # loop starts where the initial placement left it without running it again
-        loc = np.load(a.start_from)
-        box = design.inst_box
-        w, h = box[loc[:, 0], 2] - box[loc[:, 0], 0], box[loc[:, 0], 3] - box[loc[:, 0], 1]
-        box[loc[:, 0], 0], box[loc[:, 0], 1] = loc[:, 1], loc[:, 2]
-        box[loc[:, 0], 2], box[loc[:, 0], 3] = loc[:, 1] + w, loc[:, 2] + h
-        design.inst_flags[loc[:, 0]] |= synth.INST_PLACED
+    design, args = loop_design(a)
     log("design generated")
-    C_cells = design.meta["cells"]
     placer = engine.Placer(local, a.form)
-    skip_ip = a.start == "placed" or bool(a.start_from)
-    sess = engine.Session(placer, design, cfg["args"] + (["-skip_initial_place"] if skip_ip else []))
+    sess = engine.Session(placer, design, args)
     log("session open")
     sess.iterate(a.warmup)
     log("warm-up done")
@@ -226,7 +268,7 @@ def ours(a):
         raise SystemExit("the loop ended during warm-up: " + json.dumps(sess.close().get("reason")))
     stream = torch.cuda.ExternalStream(sess.stream, device=local)
 
-    def timed(k, label):
+    def timed(k):
         c0 = sess.counters()
         if world > 1:
             dist.barrier()
@@ -244,7 +286,8 @@ def ours(a):
         ms = e0.elapsed_time(e1)
         c1 = sess.counters()
         ms = max_over_ranks(ms, f"cuda:{local}")
-        return {"ms": ms, "iters": done, "wall_s": wall, "clocks": clk.summary(), "launches": c1["launches"] - c0["launches"]}
+        return {"ms": ms, "iters": done, "wall_s": wall, "clocks": clk.summary(), "launches": c1["launches"] - c0["launches"],
+                "trials": c1["trials"] - c0["trials"]}
 
     def phase_times(k):
         # each phase's own device time: events around each phase's launches, with the WA after
@@ -259,11 +302,11 @@ def ours(a):
 
     cells_total = sess.counters()["cells"]
     if a.form == "mixed":
-        mixed = timed(a.steps, "mixed")
+        mixed = timed(a.steps)
         mixed["profile"] = phase_times(min(a.steps, 10))
         sess.set_option("poisson", "fp32")
         sess.iterate(min(a.warmup, 3))
-    fp32 = timed(a.steps, "fp32")
+    fp32 = timed(a.steps)
     fp32["profile"] = phase_times(min(a.steps, 10))
     if a.form == "fp32":
         mixed = fp32
@@ -271,21 +314,21 @@ def ours(a):
     res = sess.close()
     log("session closed")
     P_pins, N_nets = res["pins"], res["nets"]
-    # the placement run's own figures: fillers in the cell count
     nx = int(cfg["args"][cfg["args"].index("-bin_grid_count") + 1])
     B = nx * nx
-    # e2e: the whole command through the public C ABI, host arrays in, locations out
+    # e2e: the whole command through the public C ABI, host arrays in (construction and the
+    # initial placement included), locations out
     e2e = None
     if not a.no_e2e:
-        if a.start == "placed":
-            design = synth.generate(cfg["preset"])
+        full = synth.generate(cfg["preset"])
         t0 = time.perf_counter()
-        r = engine.global_placement(design, cfg["args"], device=local, poisson=a.form)
+        r = engine.global_placement(full, cfg["args"], device=local, poisson=a.form)
         e2e_s = max_over_ranks(time.perf_counter() - t0, f"cuda:{local}")
         log("e2e run done")
         its = r["nesterov_iterations"] or 0
         e2e = {"value": its * world / e2e_s if e2e_s > 0 else 0.0, "unit": "iters/s", "seconds": e2e_s,
-               "iterations": its, "status": r["status"],
+               "iterations": its, "trials": r["trials"], "status": r["status"],
+               "what": "the whole global_placement command (construction, initial placement, Nesterov loop, written placement) through the C ABI with host arrays",
                "h2d_bytes_per_step": int(r["h2d_bytes"] / max(its, 1)), "d2h_bytes_per_step": int(r["d2h_bytes"] / max(its, 1)),
                "final_hpwl": r["final_hpwl"], "final_overflow": r["final_overflow"],
                "seconds_initial_place": r["seconds_initial_place"], "seconds_nesterov": r["seconds_nesterov"]}
@@ -325,19 +368,18 @@ def ours(a):
     phases = {k: {"ms_total": v[0], "launches": v[1], "share": v[0] / max(sum(x[0] for x in prof.values()), 1e-9)} for k, v in prof.items()}
     cpu = None
     if world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(a)
+        cpu = cpu_sample(a)
     precision = precision_report(local, nx)
+    conf = workload(a, design)
+    conf["parallelism"] = f"replicas x{world}"
     out = {
         "metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": mixed["ms"] / max(mixed["iters"], 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+bf16x3 (split-BF16 density solve), f64 reductions", "data": "synthetic",
-        "config": {"workload": cfg["name"], "args": cfg["args"], "design": design.meta["config"],
-                   "cells": C_cells, "nets": N_nets, "pins": P_pins, "bins": B, "parallelism": f"replicas x{world}",
-                   "start": ("the saved initial placement, not re-run" if a.start_from else "after the initial placement") if a.start == "ip" else "the generator's spread placement, initial placement skipped",
-                   "l2": "working set > L2 (126 MB): cells, pins and bins stream from HBM each trial"},
-        "form": a.form,
-        "forms": {"mixed": {"iters_per_s": value, "ms_per_iter": mixed["ms"] / max(mixed["iters"], 1), "iters": mixed["iters"]},
-                  "fp32": {"iters_per_s": value_fp32, "ms_per_iter": fp32["ms"] / max(fp32["iters"], 1), "iters": fp32["iters"]},
+        "config": conf, "form": a.form, "trials": mixed["trials"], "trials_per_s": mixed["trials"] * world / (mixed["ms"] / 1000.0),
+        "forms": {"mixed": {"iters_per_s": value, "ms_per_iter": mixed["ms"] / max(mixed["iters"], 1), "iters": mixed["iters"], "trials": mixed["trials"]},
+                  "fp32": {"iters_per_s": value_fp32, "ms_per_iter": fp32["ms"] / max(fp32["iters"], 1), "iters": fp32["iters"], "trials": fp32["trials"],
+                           "note": "timed on the iterations after the mixed form's, from the same run"},
                   "mixed_over_fp32": value / value_fp32 if value_fp32 else None},
         "phases": phases, "roofline": roof, "gpu_launches": mixed["launches"], "clocks": mixed["clocks"],
         "e2e": e2e, "cpu_baseline": cpu, "precision": precision,
@@ -372,38 +414,16 @@ def precision_report(local, n):
     return out
 
 
-def cpu_baseline(a):
-    """The oracle (the reference's CPU path restated, one thread) on a bounded sample."""
+def cpu_sample(a):
+    """The oracle (the reference's CPU path restated; one thread, as the reference runs) on the
+    same workload as the device's timed loop: the same design, start and arguments, the same
+    warm-up iterations untimed, then the same K iterations timed. The reference arm and the
+    GPU line's cpu_baseline are this one sample."""
     import oracle
-    from gpl_b200 import synth
-    cfg = CONFIGS[a.config]
-    design = synth.generate(cfg["preset"], placed=True)
+    design, args = loop_design(a)
     t0 = time.perf_counter()
-    s = oracle.Session(design, cfg["args"] + ["-skip_initial_place"])
+    s = oracle.Session(design, args)
     setup = time.perf_counter() - t0
-    s.iterate(1)
-    k = a.cpu_iters
-    tr0 = s.trials()
-    t0 = time.perf_counter()
-    done = s.iterate(k)
-    dt = time.perf_counter() - t0
-    trials = s.trials() - tr0
-    s.discard()
-    return {"value": done / dt if dt > 0 else 0.0, "unit": "iters/s", "cores": 1, "kind": "port",
-            "sample": f"{done} Nesterov iterations ({trials} trials) of the same netlist from the generator's spread placement after its set-up ({setup:.1f} s, initial placement skipped), single thread",
-            "seconds_per_iter": dt / max(done, 1)}
-
-
-def reference(a):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    if rank != 0:
-        return
-    import oracle
-    from gpl_b200 import synth
-    cfg = CONFIGS[a.config]
-    design = synth.generate(cfg["preset"], placed=True)
-    s = oracle.Session(design, cfg["args"] + ["-skip_initial_place"])
     s.iterate(a.warmup)
     tr0 = s.trials()
     t0 = time.perf_counter()
@@ -412,12 +432,23 @@ def reference(a):
     trials = s.trials() - tr0
     s.discard()
     v = done / dt if dt > 0 else 0.0
+    return {"value": v, "unit": "iters/s", "cores": 1, "kind": "port", "trials": trials, "trials_per_s": trials / dt if dt > 0 else 0.0,
+            "seconds_per_iter": dt / max(done, 1), "seconds": dt,
+            "sample": f"Nesterov iterations {a.warmup + 1}..{a.warmup + done} ({trials} trials) of the same design from {START[a.start]}, after {a.warmup} untimed warm-up iterations and the set-up ({setup:.1f} s); one host thread (the reference is single-threaded)"}
+
+
+def reference(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    design, _ = loop_design(a)
+    cpu = cpu_sample(a)
+    v = cpu["value"]
     out = {"metric": METRIC, "value": v, "unit": "iters/s", "impl": "reference", "n_gpus": world, "steps": a.steps,
-           "warmup": a.warmup, "ms_per_step": 1000.0 * dt / max(done, 1), "higher_is_better": True, "scaling": "weak",
+           "warmup": a.warmup, "ms_per_step": 1000.0 * cpu["seconds_per_iter"], "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32 (the reference's float order), f64 where the reference uses double", "data": "synthetic",
-           "config": {"workload": cfg["name"], "args": cfg["args"], "design": design.meta["config"], "parallelism": "1 CPU thread"},
-           "cpu_baseline": {"value": v, "unit": "iters/s", "cores": 1, "kind": "port",
-                            "sample": f"{done} Nesterov iterations ({trials} trials) over the timed steps, from the generator's spread placement (initial placement skipped); the reference runs on one thread"},
+           "config": workload(a, design), "trials": cpu["trials"], "trials_per_s": cpu["trials_per_s"], "cpu_baseline": cpu,
            "e2e": {"value": v, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
@@ -431,10 +462,9 @@ def main():
     ap.add_argument("--config", default="cfg3", choices=list(CONFIGS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-iters", type=int, default=8)
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp32"], help="the density solve timed as the headline")
-    ap.add_argument("--start", default="ip", choices=["ip", "placed"],
-                    help="time the loop after the initial placement, or from the generator's spread placement with the initial placement skipped (a short case for profiling)")
+    ap.add_argument("--start", default="spread", choices=["spread", "ip"],
+                    help="time the loop from the generator's spread placement with the initial placement skipped (both arms, the default), or after the device's initial placement (a profiling case)")
     ap.add_argument("--initial-place-only", action="store_true",
                     help="run the command through the initial placement once and print its time (a profiling case)")
     ap.add_argument("--save-placement", default="", help="with --initial-place-only: save the locations (.npy)")

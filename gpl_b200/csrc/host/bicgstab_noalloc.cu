@@ -5,8 +5,13 @@
 // plug-in hosts that forbid a library from growing the device heap behind their back, and code
 // that shares the GPU with latency-critical streams, where cudaMalloc and cudaFree may wait for
 // the whole device. This entry point gives them the same solve with
-// its scratch in one fixed array of this library's own: a file-scope device array, reserved
-// when the library is loaded and held on every device that loads it until the process exits.
+// its scratch in one fixed array of this library's own: a file-scope device array. The CUDA
+// driver reserves it when it loads this library's device code on a device: at the first use of
+// the library's kernels there under lazy module loading (CUDA's default since 12.2; possibly
+// inside the first call below, at cudaGetSymbolAddress), or when the context is made with
+// CUDA_MODULE_LOADING=EAGER. It is held on that device until the process exits. A caller that
+// budgets device memory or captures streams makes one call (or any launch of this library) on
+// each device first.
 #include <cstdint>
 #include <mutex>
 
@@ -31,6 +36,8 @@ void *g_addr[kMaxDevices] = {};
 
 // The scratch's device address on the current device, looked up once per device, by the first
 // call made with that device current; that first call should come before any stream capture.
+// The address is kept for the process: after cudaDeviceReset on a device it names freed memory,
+// so a caller that resets a device must not call this entry point on it again.
 cudaError_t scratch_address(void **out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -50,7 +57,8 @@ cudaError_t scratch_address(void **out) {
 }  // namespace
 
 extern "C" int gpl_kernel_bicgstab_noalloc(int64_t n, const int64_t *row_start, const int32_t *cols, const float *vals, const float *rhs, float *x, int32_t max_iters, int32_t *iterations, float *error, void *stream) {
-  if (n < 0 || n > kMaxRows) return GPL_NOALLOC_TOO_LARGE;
+  if (n < 0) return (int)cudaErrorInvalidValue;
+  if (n > kMaxRows) return GPL_NOALLOC_TOO_LARGE;
   if (gpl::bicgstab_scratch_bytes(n) > kScratchBytes) return GPL_NOALLOC_TOO_LARGE;
   void *scratch = nullptr;
   cudaError_t e = scratch_address(&scratch);

@@ -62,6 +62,106 @@ int gpl_kernel_density_scatter(int64_t n_cells, const int32_t *cx, const int32_t
   return (int)(e != cudaSuccess ? e : e2);
 }
 
+// A grid of the caller's bins as the trial kernels read it; its edges are read back here (the
+// scatter's 32-bit tile test and the grid's upper corner).
+static cudaError_t region_args(RegionArgs &r, int64_t n_cells, int32_t nx, int32_t ny, int32_t grid_lx, int32_t grid_ly, const int32_t *bx, const int32_t *by, double size_x, double size_y, float target_density, cudaStream_t s) {
+  if (n_cells < 0 || n_cells >= ((int64_t)1 << 31) || nx <= 0 || ny <= 0) return cudaErrorInvalidValue;
+  r = RegionArgs{};
+  r.n_cells = (int32_t)n_cells;
+  r.nx = nx;
+  r.ny = ny;
+  r.lx = grid_lx;
+  r.ly = grid_ly;
+  r.size_x = size_x;
+  r.size_y = size_y;
+  r.inv_size_x = 1.0 / size_x;
+  r.inv_size_y = 1.0 / size_y;
+  std::vector<int32_t> hbx(nx + 1), hby(ny + 1);
+  cudaError_t e = cudaMemcpyAsync(hbx.data(), bx, hbx.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hby.data(), by, hby.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  r.ux = hbx[nx];
+  r.uy = hby[ny];
+  r.narrow = narrow_tile(hbx, hby) ? 1 : 0;
+  r.target_density = target_density;
+  r.bx = bx;
+  r.by = by;
+  return cudaSuccess;
+}
+
+static bool aligned8(const void *p) { return ((uintptr_t)p & 7u) == 0; }
+
+int gpl_kernel_nesterov_step(int64_t n_cells, const float *cur_slp, const float *cur_slp_sum, const float *cur, const int32_t *hx, const int32_t *hy, const float *scale, const uint8_t *kind, const uint8_t *locked, int32_t nx, int32_t ny, int32_t grid_lx, int32_t grid_ly, const int32_t *bx, const int32_t *by, double size_x, double size_y, float target_density, float step, float coeff, float *next, float *next_slp, int32_t *centre, int64_t *inst, int64_t *filler, void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  RegionArgs r;
+  cudaError_t e = region_args(r, n_cells, nx, ny, grid_lx, grid_ly, bx, by, size_x, size_y, target_density, s);
+  if (e != cudaSuccess) return (int)e;
+  for (const void *p : {(const void *)cur_slp, (const void *)cur_slp_sum, (const void *)cur, (const void *)next, (const void *)next_slp, (const void *)centre})
+    if (!aligned8(p)) return (int)cudaErrorMisalignedAddress;  // read and written as pairs
+  size_t nb = (size_t)nx * ny;
+  e = cudaMemsetAsync(inst, 0, nb * sizeof(int64_t), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(filler, 0, nb * sizeof(int64_t), s);
+  if (e != cudaSuccess || n_cells == 0) return (int)e;
+  r.acc_inst = inst;
+  r.acc_fill = filler;
+  CellArgs c{};
+  c.dc = reinterpret_cast<int2 *>(centre);
+  c.hx = hx;
+  c.hy = hy;
+  c.dscale = scale;
+  c.kind = kind;
+  c.locked = locked;
+  // the kernel reads cur_slp, cur_slp_sum and cur and writes next and next_slp only
+  c.cur_slp = reinterpret_cast<float2 *>(const_cast<float *>(cur_slp));
+  c.cur_slp_sum = reinterpret_cast<float2 *>(const_cast<float *>(cur_slp_sum));
+  c.cur = reinterpret_cast<float2 *>(const_cast<float *>(cur));
+  c.next = reinterpret_cast<float2 *>(next);
+  c.next_slp = reinterpret_cast<float2 *>(next_slp);
+  unsigned blocks = (unsigned)((n_cells + kThreadsPerBlock - 1) / kThreadsPerBlock);
+  k_place_cells<<<blocks, kThreadsPerBlock, 0, s>>>(r, c, PLACE_NESTEROV, step, coeff, nullptr);
+  return (int)cudaGetLastError();
+}
+
+int gpl_kernel_gradients(int64_t n_cells, const int32_t *centre, const int32_t *hx, const int32_t *hy, const float *scale, const float *area, const int64_t *cell_pin_start, const float *pin_force, int32_t nx, int32_t ny, int32_t grid_lx, int32_t grid_ly, const int32_t *bx, const int32_t *by, double size_x, double size_y, const float *field_x, const float *field_y, float penalty, float *sum, const float *a1, const float *b1, const float *b2, double *sums, void *stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int k = 0; k < 4; k++) sums[k] = 0.0;
+  RegionArgs r;
+  cudaError_t e = region_args(r, n_cells, nx, ny, grid_lx, grid_ly, bx, by, size_x, size_y, 1.0f, s);
+  if (e != cudaSuccess) return (int)e;
+  for (const void *p : {(const void *)centre, (const void *)pin_force, (const void *)sum, (const void *)a1, (const void *)b1, (const void *)b2})
+    if (!aligned8(p)) return (int)cudaErrorMisalignedAddress;
+  if ((a1 == nullptr) != (b1 == nullptr)) return (int)cudaErrorInvalidValue;
+  if (n_cells == 0) return 0;
+  r.field_x = const_cast<float *>(field_x);
+  r.field_y = const_cast<float *>(field_y);
+  CellArgs c{};
+  c.dc = reinterpret_cast<int2 *>(const_cast<int32_t *>(centre));
+  c.hx = hx;
+  c.hy = hy;
+  c.dscale = scale;
+  c.area = area;
+  c.pin_start = cell_pin_start;
+  const int blocks = (int)((n_cells + kThreadsPerBlock - 1) / kThreadsPerBlock);
+  // the block partials, the arrival ticket and the four sums, in one scratch block
+  const size_t bytes = (size_t)(4 * blocks + 4) * sizeof(double) + 256;
+  uint8_t *scratch = nullptr;
+  e = cudaMallocAsync((void **)&scratch, bytes, s);
+  if (e != cudaSuccess) return (int)e;
+  double *partials = reinterpret_cast<double *>(scratch), *out = partials + 4 * blocks;
+  unsigned int *ticket = reinterpret_cast<unsigned int *>(out + 4);
+  e = cudaMemsetAsync(ticket, 0, sizeof(unsigned int), s);
+  if (e == cudaSuccess) {
+    k_gradients<<<blocks, kThreadsPerBlock, 0, s>>>(r, c, reinterpret_cast<const float2 *>(pin_force), penalty, reinterpret_cast<float2 *>(sum), reinterpret_cast<const float2 *>(a1),
+                                                    reinterpret_cast<const float2 *>(b1), reinterpret_cast<const float2 *>(b2), partials, ticket, out);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(sums, out, 4 * sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaError_t e2 = cudaFreeAsync(scratch, s);
+  return (int)(e != cudaSuccess ? e : e2);
+}
+
 int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy, const float *density, float *field_x, float *field_y, int mode, void *stream) {
   cudaStream_t s = (cudaStream_t)stream;
   cudaError_t e = cudaSuccess;
@@ -79,83 +179,154 @@ int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy,
   return (int)(e != cudaSuccess ? e : e2);
 }
 
-int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, const float *net_weight, float coef_x, float coef_y, float *grad, void *stream) {
-  if (n_nets <= 0) return 0;
-  cudaStream_t s = (cudaStream_t)stream;
-  std::vector<int64_t> starts((size_t)n_nets + 1);
-  cudaError_t e = cudaMemcpyAsync(starts.data(), net_start, starts.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return (int)e;
-  const int64_t np = starts[n_nets];
-  if (np >= ((int64_t)1 << 31)) return (int)cudaErrorInvalidValue;  // pin numbers are 32-bit
-  // the nets in degree order (stable), as the engine holds them, their pins following them;
-  // each pin's force goes back to its own place (its slot is its index in the caller's order)
-  std::vector<int32_t> order((size_t)n_nets);
-  for (int64_t n = 0; n < n_nets; n++) order[n] = (int32_t)n;
-  std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return starts[x + 1] - starts[x] < starts[y + 1] - starts[y]; });
-  std::vector<int32_t> xy((size_t)np * 2), xy2((size_t)np * 2), slot((size_t)np);
-  std::vector<float> wt, wt2;
-  if (np) e = cudaMemcpyAsync(xy.data(), pin_xy, xy.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess && net_weight) {
-    wt.resize((size_t)n_nets);
-    wt2.resize((size_t)n_nets);
-    e = cudaMemcpyAsync(wt.data(), net_weight, wt.size() * sizeof(float), cudaMemcpyDeviceToHost, s);
-  }
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return (int)e;
-  std::vector<int64_t> ns((size_t)n_nets + 1, 0);
-  int64_t at = 0;
-  for (int64_t i = 0; i < n_nets; i++) {
-    const int32_t n = order[i];
-    for (int64_t q = starts[n]; q < starts[n + 1]; q++, at++) {
-      xy2[2 * at] = xy[2 * q];
-      xy2[2 * at + 1] = xy[2 * q + 1];
-      slot[at] = (int32_t)q;
-    }
-    ns[i + 1] = at;
-    if (net_weight) wt2[i] = wt[n];
-  }
-  std::vector<int4> tiles;
-  std::vector<int32_t> big;
-  const WaSmall small = wa_small_ranges(ns.data(), (int32_t)n_nets);
-  wa_tiles(ns.data(), 0, small.first[0], tiles, big);
-  wa_tiles(ns.data(), small.first[2] + small.count[2], (int32_t)n_nets, tiles, big);
+// The caller's nets on the device as the engine holds them: in degree order (stable), their
+// pins following them, each pin's slot its index in the caller's order (so a force goes back to
+// its own place); the degree-2..4 ranges, the tiles and the nets too large for a tile.
+struct DeviceNets {
+  cudaStream_t s;
+  cudaError_t e = cudaSuccess;
   int64_t *d_ns = nullptr;
   int32_t *d_xy = nullptr, *d_slot = nullptr, *d_big = nullptr;
   int4 *d_tiles = nullptr;
   float *d_wt = nullptr;
-  auto put = [&](auto **d, const auto &v) {
-    if (e != cudaSuccess) return;
-    e = cudaMallocAsync((void **)d, std::max<size_t>(v.size(), 1) * sizeof(v[0]), s);
-    if (e == cudaSuccess && !v.empty()) e = cudaMemcpyAsync(*d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, s);
-  };
-  put(&d_ns, ns);
-  put(&d_xy, xy2);
-  put(&d_slot, slot);
-  put(&d_tiles, tiles);
-  put(&d_big, big);
-  if (net_weight) put(&d_wt, wt2);
-  if (e == cudaSuccess) {
+  WaSmall small{};
+  size_t n_tiles = 0, n_big = 0;
+  int64_t n_pins = 0;
+  explicit DeviceNets(cudaStream_t st) : s(st) {}
+  ~DeviceNets() {
+    void *bufs[] = {d_ns, d_xy, d_slot, d_tiles, d_big, d_wt};
+    for (void *p : bufs)
+      if (p) cudaFreeAsync(p, s);
+  }
+  cudaError_t build(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, const float *net_weight) {
+    std::vector<int64_t> starts((size_t)n_nets + 1);
+    e = cudaMemcpyAsync(starts.data(), net_start, starts.size() * sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    const int64_t np = starts[n_nets];
+    n_pins = np;
+    if (np >= ((int64_t)1 << 31)) return e = cudaErrorInvalidValue;  // pin numbers are 32-bit
+    std::vector<int32_t> order((size_t)n_nets);
+    for (int64_t n = 0; n < n_nets; n++) order[n] = (int32_t)n;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t x, int32_t y) { return starts[x + 1] - starts[x] < starts[y + 1] - starts[y]; });
+    std::vector<int32_t> xy((size_t)np * 2), xy2((size_t)np * 2), slot((size_t)np);
+    std::vector<float> wt, wt2;
+    if (np) e = cudaMemcpyAsync(xy.data(), pin_xy, xy.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && net_weight) {
+      wt.resize((size_t)n_nets);
+      wt2.resize((size_t)n_nets);
+      e = cudaMemcpyAsync(wt.data(), net_weight, wt.size() * sizeof(float), cudaMemcpyDeviceToHost, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    std::vector<int64_t> ns((size_t)n_nets + 1, 0);
+    int64_t at = 0;
+    for (int64_t i = 0; i < n_nets; i++) {
+      const int32_t n = order[i];
+      for (int64_t q = starts[n]; q < starts[n + 1]; q++, at++) {
+        xy2[2 * at] = xy[2 * q];
+        xy2[2 * at + 1] = xy[2 * q + 1];
+        slot[at] = (int32_t)q;
+      }
+      ns[i + 1] = at;
+      if (net_weight) wt2[i] = wt[n];
+    }
+    std::vector<int4> tiles;
+    std::vector<int32_t> big;
+    small = wa_small_ranges(ns.data(), (int32_t)n_nets);
+    wa_tiles(ns.data(), 0, small.first[0], tiles, big);
+    wa_tiles(ns.data(), small.first[2] + small.count[2], (int32_t)n_nets, tiles, big);
+    n_tiles = tiles.size();
+    n_big = big.size();
+    auto put = [&](auto **d, const auto &v) {
+      if (e != cudaSuccess) return;
+      e = cudaMallocAsync((void **)d, std::max<size_t>(v.size(), 1) * sizeof(v[0]), s);
+      if (e == cudaSuccess && !v.empty()) e = cudaMemcpyAsync(*d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, s);
+    };
+    put(&d_ns, ns);
+    put(&d_xy, xy2);
+    put(&d_slot, slot);
+    put(&d_tiles, tiles);
+    put(&d_big, big);
+    if (net_weight) put(&d_wt, wt2);
+    // the host vectors above are freed on return: the copies must have read them
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
+  }
+  WaArgs args(float *grad) const {
     WaArgs w{};
-    w.n_nets = (int32_t)big.size();
+    w.n_nets = (int32_t)n_big;
     w.net_start = d_ns;
     w.net_order = d_big;
     w.net_weight = d_wt;
     w.pin_base = reinterpret_cast<const int2 *>(d_xy);
     w.pin_slot = d_slot;
     w.pin_grad = reinterpret_cast<float2 *>(grad);
-    w.n_tiles = (int32_t)tiles.size();
+    w.n_tiles = (int32_t)n_tiles;
     w.tiles = d_tiles;
     w.small = small;
-    if (const int nb = wa_small_blocks(small)) k_wa_small<<<nb, kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y, 1);
-    if (!tiles.empty()) launch_wa_tiles(w, coef_x, coef_y, s);
-    if (!big.empty()) k_wa<<<(unsigned)((big.size() + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y);
-    e = cudaGetLastError();
+    return w;
   }
-  void *bufs[] = {d_ns, d_xy, d_slot, d_tiles, d_big, d_wt};
-  for (void *p : bufs)
-    if (p) cudaFreeAsync(p, s);
+};
+
+int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, const float *net_weight, float coef_x, float coef_y, float *grad, void *stream) {
+  if (n_nets <= 0) return 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e;
+  {
+    DeviceNets d(s);
+    e = d.build(n_nets, net_start, pin_xy, net_weight);
+    if (e == cudaSuccess) {
+      WaArgs w = d.args(grad);
+      if (const int nb = wa_small_blocks(w.small)) k_wa_small<<<nb, kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y, 1);
+      if (w.n_tiles) launch_wa_tiles(w, coef_x, coef_y, s);
+      if (w.n_nets) k_wa<<<(unsigned)((w.n_nets + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y);
+      e = cudaGetLastError();
+    }
+  }
   cudaError_t e2 = cudaStreamSynchronize(s);
+  return (int)(e != cudaSuccess ? e : e2);
+}
+
+int gpl_kernel_hpwl(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, int32_t fused, int64_t *hpwl, void *stream) {
+  *hpwl = 0;
+  if (n_nets <= 0) return 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e;
+  unsigned long long h = 0;
+  {
+    DeviceNets d(s);
+    unsigned long long *acc = nullptr;
+    float *grad = nullptr;
+    e = d.build(n_nets, net_start, pin_xy, nullptr);
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)&acc, sizeof(unsigned long long), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, sizeof(unsigned long long), s);
+    if (e == cudaSuccess && fused) e = cudaMallocAsync((void **)&grad, (size_t)std::max<int64_t>(d.n_pins, 1) * 2 * sizeof(float), s);
+    if (e == cudaSuccess) {
+      WaArgs w = d.args(grad);
+      w.hpwl_out = acc;
+      const unsigned nbig = (unsigned)((w.n_nets + kThreadsPerBlock - 1) / kThreadsPerBlock);
+      const float c = 1e-4f;  // any coefficient: the HPWL is the pins' boxes
+      if (fused) {
+        // the HPWL the WA kernels add up beside the forces (the trial's read-back)
+        if (const int nb = wa_small_blocks(w.small)) k_wa_small<<<nb, kThreadsPerBlock, 0, s>>>(w, c, c, 1);
+        if (w.n_tiles) launch_wa_tiles(w, c, c, s);
+        if (w.n_nets) k_wa<<<nbig, kThreadsPerBlock, 0, s>>>(w, c, c);
+      } else {
+        // the HPWL kernels of an iteration without a WA pass
+        if (const int nb = wa_small_blocks(w.small)) k_wa_small<<<nb, kThreadsPerBlock, 0, s>>>(w, 0.0f, 0.0f, 0);
+        if (w.n_tiles) k_hpwl_tiles<<<(unsigned)w.n_tiles, kThreadsPerBlock, 0, s>>>(w, acc);
+        if (w.n_nets) k_hpwl<<<nbig, kThreadsPerBlock, 0, s>>>(w, acc);
+      }
+      e = cudaGetLastError();
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&h, acc, sizeof h, cudaMemcpyDeviceToHost, s);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (acc) cudaFreeAsync(acc, s);
+    if (grad) cudaFreeAsync(grad, s);
+  }
+  cudaError_t e2 = cudaStreamSynchronize(s);
+  if (e == cudaSuccess && e2 == cudaSuccess) *hpwl = (int64_t)h;
   return (int)(e != cudaSuccess ? e : e2);
 }
 

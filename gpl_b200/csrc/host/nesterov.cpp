@@ -2468,11 +2468,12 @@ int gpl_session_profile(gpl_session *s, double *ms, int64_t *launches, int cap) 
 
 void *gpl_session_stream(gpl_session *s) { return (void *)s->ctx->eng->stream(); }
 
-void gpl_session_counters(gpl_session *s, int64_t out[4]) {
+void gpl_session_counters(gpl_session *s, int64_t out[5]) {
   out[0] = s->ctx->eng->launches;
   out[1] = s->ctx->eng->h2d_bytes;
   out[2] = s->ctx->eng->d2h_bytes;
   out[3] = s->run->P ? (int64_t)s->run->P->gcell_of_dev.size() : 0;
+  out[4] = s->ctx->eng->trials;
 }
 
 void gpl_session_discard(gpl_session *s) {

@@ -42,6 +42,9 @@ def lib():
         L.gpl_kernel_wa.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_void_p, C.c_void_p]
         L.gpl_kernel_bicgstab.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
         L.gpl_kernel_rudy.argtypes = [C.c_int64, C.c_void_p] + [C.c_int32] * 8 + [C.c_void_p, C.c_void_p]
+        L.gpl_kernel_nesterov_step.argtypes = [C.c_int64] + [C.c_void_p] * 8 + [C.c_int32] * 4 + [C.c_void_p] * 2 + [C.c_double, C.c_double, C.c_float, C.c_float, C.c_float] + [C.c_void_p] * 6
+        L.gpl_kernel_gradients.argtypes = [C.c_int64] + [C.c_void_p] * 7 + [C.c_int32] * 4 + [C.c_void_p] * 2 + [C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_float] + [C.c_void_p] * 6
+        L.gpl_kernel_hpwl.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -158,9 +161,9 @@ class Session:
         return {PHASES[i]: (ms[i], n[i]) for i in range(k)}
 
     def counters(self):
-        out = (C.c_int64 * 4)()
+        out = (C.c_int64 * 5)()
         _session_lib().gpl_session_counters(self._h, out)
-        return {"launches": out[0], "h2d_bytes": out[1], "d2h_bytes": out[2], "cells": out[3]}
+        return {"launches": out[0], "h2d_bytes": out[1], "d2h_bytes": out[2], "cells": out[3], "trials": out[4]}
 
     @property
     def stream(self):

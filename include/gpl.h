@@ -183,9 +183,10 @@ int gpl_session_set_option(gpl_session *s, const char *name, const char *value);
 /* Per-phase device milliseconds and launch counts since "profile" was set: scatter, bin
  * finalize, density solve, WA, gradients, HPWL. Returns the number of phases written. */
 int gpl_session_profile(gpl_session *s, double *ms, int64_t *launches, int cap);
-/* Kernel launches, host-to-device and device-to-host bytes since the session opened, and the
- * Nesterov cells (instances and fillers) on the device (4 int64). */
-void gpl_session_counters(gpl_session *s, int64_t out[4]);
+/* Kernel launches, host-to-device and device-to-host bytes since the session opened, the
+ * Nesterov cells (instances and fillers) on the device, and the back-tracking trials run
+ * (`do_back_tracking`'s passes, src/nesterov.rs:2776-2808) since the session opened (5 int64). */
+void gpl_session_counters(gpl_session *s, int64_t out[5]);
 /* The session's CUDA stream (cudaStream_t), for timing with events on it. */
 void *gpl_session_stream(gpl_session *s);
 int gpl_session_close(gpl_session *s, gpl_result_t *out);
@@ -216,6 +217,49 @@ int gpl_kernel_density_scatter(int64_t n_cells, const int32_t *cx, const int32_t
                                int32_t grid_ly, const int32_t *bx, const int32_t *by,
                                double size_x, double size_y, float target_density,
                                int64_t *inst, int64_t *filler, void *stream);
+
+/* The Nesterov step `nesterov_update_coordinates` (src/nesterov.rs:2718-2746, with
+ * `inside_x/y` :2188-2213) up to the field, as one trial runs it: per cell (float pairs x, y)
+ *   next     = clamp(cur_slp + step * cur_slp_sum),
+ *   next_slp = clamp(next' + coeff * (next' - cur))  (next' the unclamped next),
+ * each clamped so the density box (half sizes hx, hy: 2 hx wide, as `set_density_size` leaves
+ * it) stays inside the grid [grid_lx, bx[nx]] x [grid_ly, by[ny]]; a locked cell (locked may be
+ * NULL) keeps cur and cur_slp. Then the density centre at next_slp, truncated to integers
+ * (`update_gcell_density_center_location`, :2268-2276), into centre (2 per cell), and the bin
+ * scatter of those boxes as gpl_kernel_density_scatter writes it into inst and filler (zeroed
+ * first). Float pairs and centre must be 8-byte aligned. */
+int gpl_kernel_nesterov_step(int64_t n_cells, const float *cur_slp, const float *cur_slp_sum,
+                             const float *cur, const int32_t *hx, const int32_t *hy,
+                             const float *scale, const uint8_t *kind, const uint8_t *locked,
+                             int32_t nx, int32_t ny, int32_t grid_lx, int32_t grid_ly,
+                             const int32_t *bx, const int32_t *by, double size_x, double size_y,
+                             float target_density, float step, float coeff, float *next,
+                             float *next_slp, int32_t *centre, int64_t *inst, int64_t *filler,
+                             void *stream);
+
+/* `update_gradients` (src/nesterov.rs:2455-2507) with the step length's distances
+ * (`distance`, :319-330): per cell, the WA force summed over its pins in its own order
+ * (`wl_gradient`, :2418-2430; pin_force holds each pin's force times its net's weight, cell-major:
+ * the cell's pins at cell_pin_start[i] .. cell_pin_start[i+1]), the density force over its bins,
+ * x outer, y inner (`density_gradient`, :2434-2449; centre 2 per cell, fields x-major), and
+ *   sum = (wl + penalty * density) / max(pins + penalty * area, 1)
+ * into sum (2 per cell). sums (host, 4 doubles) receives sum |wl|, sum |density|,
+ * sum |a1 - b1|^2 (a1 and b1 both NULL: 0) and sum |sum - b2|^2 (b2 NULL: 0) over every cell's
+ * x and y, each in double. Float pairs and centre must be 8-byte aligned. */
+int gpl_kernel_gradients(int64_t n_cells, const int32_t *centre, const int32_t *hx,
+                         const int32_t *hy, const float *scale, const float *area,
+                         const int64_t *cell_pin_start, const float *pin_force, int32_t nx,
+                         int32_t ny, int32_t grid_lx, int32_t grid_ly, const int32_t *bx,
+                         const int32_t *by, double size_x, double size_y, const float *field_x,
+                         const float *field_y, float penalty, float *sum, const float *a1,
+                         const float *b1, const float *b2, double *sums, void *stream);
+
+/* `get_hpwl` (src/nesterov.rs:2297-2304): the sum over nets (pins net-major, net_start[n_nets+1])
+ * of each net's pin-box half perimeter, int64, into *hpwl (host). fused = 1 takes it from the WA
+ * kernels, which add it up beside the forces as each trial reads it back; 0 from the HPWL
+ * kernels an iteration runs without a WA pass. */
+int gpl_kernel_hpwl(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy,
+                    int32_t fused, int64_t *hpwl, void *stream);
 
 /* `Fft::solve` (src/nesterov.rs:412-444) without the potential: density[nx*ny] (x-major) to
  * field_x, field_y (device pointers). mode 0 = FP32 SIMT GEMMs, 1 = split-BF16 tcgen05 GEMMs.
@@ -265,11 +309,16 @@ int gpl_kernel_bicgstab(int64_t n, const int64_t *row_start, const int32_t *cols
  * sized in advance, which a library must not bypass; hosts that forbid a plug-in library to
  * allocate device memory on its own; and code that shares the GPU with latency-critical
  * streams, where cudaMalloc and cudaFree may wait for the whole device. Its scratch is one fixed device array of this
- * library (reserved when the library is loaded, on every device that loads it, until the
- * process exits), so it serves systems of at most GPL_BICGSTAB_NOALLOC_MAX_ROWS rows (about
- * 3.7 MB of scratch); a larger n returns GPL_NOALLOC_TOO_LARGE and touches nothing. The first
- * call on a device looks up the array's device address there (cudaGetSymbolAddress, with that
- * device current): make that first call before any stream capture. Every call on a device
+ * library, so it serves systems of at most GPL_BICGSTAB_NOALLOC_MAX_ROWS rows (about 3.7 MB of
+ * scratch); a larger n returns GPL_NOALLOC_TOO_LARGE and touches nothing, a negative n
+ * cudaErrorInvalidValue. The driver reserves the array on a device when it loads the library's
+ * device code there: under CUDA's default lazy module loading, at the first use of the
+ * library's kernels on that device (possibly inside this entry point's first call); with
+ * CUDA_MODULE_LOADING=EAGER, when the context is made. It is held until the process exits. The
+ * first call on a device also looks up the array's device address there (cudaGetSymbolAddress,
+ * with that device current): a caller that budgets device memory or captures streams makes one
+ * call on each device before doing so. The address is kept for the process, so after
+ * cudaDeviceReset on a device this entry point must not be called on that device again. Every call on a device
  * shares the one array, so calls that overlap on the GPU (other streams, other threads) race:
  * serialise them. Arguments and results as gpl_kernel_bicgstab's. */
 #define GPL_BICGSTAB_NOALLOC_MAX_ROWS 131072

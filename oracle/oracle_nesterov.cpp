@@ -1264,6 +1264,14 @@ struct Nesterov {
   // `nesterovUpdateCoordinates` (src/nesterov.rs:2718-2746).
   void nesterov_update_coordinates(int b, float coeff) {
     if (nbs[b].is_converged) return;
+    nesterov_next_coordinates(b, coeff);
+    std::vector<FloatPoint> ns = nbs[b].next_slp;
+    update_gcell_density_center_location(b, ns);
+    update_density_field_bin(b);
+  }
+  // The coordinate half of `nesterovUpdateCoordinates` (src/nesterov.rs:2718-2740): next and
+  // next_slp of every cell, clamped inside the region; locked cells keep their place.
+  void nesterov_next_coordinates(int b, float coeff) {
     float s = nbs[b].step_length;
     Nb &nb = nbs[b];
     for (size_t k = 0; k < nb.cells.size(); k++) {
@@ -1279,9 +1287,6 @@ struct Nesterov {
       nb.next[k] = FloatPoint{inside_x(b, k, nx), inside_y(b, k, ny)};
       nb.next_slp[k] = FloatPoint{inside_x(b, k, sx), inside_y(b, k, sy)};
     }
-    std::vector<FloatPoint> ns = nb.next_slp;
-    update_gcell_density_center_location(b, ns);
-    update_density_field_bin(b);
   }
   // `nesterovUpdateStepLength` (src/nesterov.rs:2750-2772).
   bool nesterov_update_step_length(int b) {
@@ -2840,6 +2845,132 @@ void oracle_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, 
     grad[2 * p] = t.x * w;
     grad[2 * p + 1] = t.y * w;
   }
+}
+
+// One region's cells for the per-kernel references below: the bin grid, and each cell a
+// density box of half sizes hx, hy (2 hx wide, as `set_density_size` leaves it) centred at
+// (cx, cy) (cx may be NULL: centred at 0).
+static void one_region(Nesterov &np, int64_t n, const int32_t *cx, const int32_t *cy, const int32_t *hx, const int32_t *hy, const float *scale, const uint8_t *kind, int nx, int ny, int32_t glx, int32_t gly, const int32_t *bx, const int32_t *by, double sx, double sy, float td) {
+  np.nbs.resize(1);
+  Nb &nb = np.nbs[0];
+  nb.bg = make_grid(nx, ny, glx, gly, bx, by, sx, sy, td);
+  np.gcells.resize((size_t)n);
+  nb.cells.resize((size_t)n);
+  for (int64_t i = 0; i < n; i++) {
+    np.gcells[i] = cell_at(cx ? cx[i] : 0, cy ? cy[i] : 0, hx[i], hy[i], scale[i], kind ? kind[i] : 0);
+    nb.cells[i] = (int)i;
+  }
+}
+static std::vector<FloatPoint> points(int64_t n, const float *xy) {
+  std::vector<FloatPoint> v((size_t)n);
+  for (int64_t i = 0; i < n; i++) v[i] = FloatPoint{xy[2 * i], xy[2 * i + 1]};
+  return v;
+}
+// `nesterovUpdateCoordinates` (src/nesterov.rs:2718-2746) up to the field: each cell's next and
+// next_slp (clamped inside the grid; locked cells keep cur and cur_slp), then the density
+// centres at next_slp (`updateGCellDensityCenterLocation`, :2268-2276, truncated) and the bin
+// scatter they give (:2218-2250). Writes next, next_slp (2 per cell), centre (2 per cell) and
+// the int64 accumulators (x-major).
+void oracle_nesterov_step(int64_t n, const float *cur_slp, const float *cur_slp_sum, const float *cur, const int32_t *hx, const int32_t *hy, const float *scale, const uint8_t *kind, const uint8_t *locked, int nx, int ny, int32_t glx, int32_t gly, const int32_t *bx, const int32_t *by, double sx, double sy, float td, float step, float coeff, float *next, float *next_slp, int32_t *centre, int64_t *inst, int64_t *filler) {
+  Nesterov np;
+  one_region(np, n, nullptr, nullptr, hx, hy, scale, kind, nx, ny, glx, gly, bx, by, sx, sy, td);
+  Nb &nb = np.nbs[0];
+  for (int64_t i = 0; i < n; i++) np.gcells[i].locked = locked && locked[i];
+  nb.cur_slp = points(n, cur_slp);
+  nb.cur_slp_sum = points(n, cur_slp_sum);
+  nb.cur = points(n, cur);
+  nb.next.assign((size_t)n, FloatPoint{});
+  nb.next_slp.assign((size_t)n, FloatPoint{});
+  nb.step_length = step;
+  np.nesterov_next_coordinates(0, coeff);
+  std::vector<FloatPoint> ns = nb.next_slp;
+  np.update_gcell_density_center_location(0, ns);
+  for (int64_t i = 0; i < n; i++) {
+    next[2 * i] = nb.next[i].x;
+    next[2 * i + 1] = nb.next[i].y;
+    next_slp[2 * i] = nb.next_slp[i].x;
+    next_slp[2 * i + 1] = nb.next_slp[i].y;
+    centre[2 * i] = np.gcells[i].d_cx();
+    centre[2 * i + 1] = np.gcells[i].d_cy();
+  }
+  for (int y = 0; y < ny; y++)
+    for (int x = 0; x < nx; x++) {
+      const Bin &b = nb.bg.bins[(size_t)y * nx + x];
+      inst[(size_t)x * ny + y] = b.inst_placed_unscaled;
+      filler[(size_t)x * ny + y] = b.filler;
+    }
+}
+// `NesterovBase::updateGradients` (src/nesterov.rs:2455-2507) on one region: the WA force of
+// each cell's pins (`updateWireLengthForceWA` + `getWireLengthGradientWA`, :2325-2430, over the
+// nets' pins at pin_xy, net-major, weights `weight` or 1), the density force over its bins
+// (:2434-2449, fields x-major) and the preconditioned sum with the penalty. A cell's pins are
+// cell_pins[cell_pin_start[i] .. cell_pin_start[i+1]] (pin numbers); its box is dx x dy (the
+// preconditioner's area). Writes sum, and when not NULL the WA and density forces wl and den
+// (2 per cell each), and sums[0..1] = the float |wl| and |density| sums in the reference's order.
+void oracle_gradients(int64_t n, const int32_t *cx, const int32_t *cy, const int32_t *hx, const int32_t *hy, const float *scale, const int32_t *dx, const int32_t *dy, const int64_t *cell_pin_start, const int32_t *cell_pins, int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy, const float *weight, float coef_x, float coef_y, int nx, int ny, int32_t glx, int32_t gly, const int32_t *bx, const int32_t *by, double sx, double sy, const float *fx, const float *fy, float penalty, float *sum, float *wl, float *den, float *sums) {
+  Nesterov np;
+  one_region(np, n, cx, cy, hx, hy, scale, nullptr, nx, ny, glx, gly, bx, by, sx, sy, 1.0f);
+  Nb &nb = np.nbs[0];
+  for (int y = 0; y < ny; y++)
+    for (int x = 0; x < nx; x++) {
+      nb.bg.bins[(size_t)y * nx + x].field_x = fx[(size_t)x * ny + y];
+      nb.bg.bins[(size_t)y * nx + x].field_y = fy[(size_t)x * ny + y];
+    }
+  for (int64_t i = 0; i < n; i++) {
+    GCell &g = np.gcells[i];
+    g.lx = 0;
+    g.ly = 0;
+    g.ux = dx[i];
+    g.uy = dy[i];
+    g.pins.assign(cell_pins + cell_pin_start[i], cell_pins + cell_pin_start[i + 1]);
+  }
+  int64_t n_pins = net_start[n_nets];
+  np.gpins.resize((size_t)n_pins);
+  for (int64_t p = 0; p < n_pins; p++) {
+    np.gpins[p].cx = pin_xy[2 * p];
+    np.gpins[p].cy = pin_xy[2 * p + 1];
+  }
+  np.gnets.resize((size_t)n_nets);
+  np.pin_net.resize((size_t)n_pins);
+  for (int64_t k = 0; k < n_nets; k++) {
+    for (int64_t p = net_start[k]; p < net_start[k + 1]; p++) {
+      np.gnets[k].pins.push_back((int)p);
+      np.pin_net[p] = (int)k;
+    }
+    if (weight) np.gnets[k].custom_weight = weight[k];
+  }
+  np.wl_coef_x = coef_x;
+  np.wl_coef_y = coef_y;
+  np.update_wirelength_force_wa();
+  nb.density_penalty = penalty;
+  np.update_gradients(0, SLOT_CUR);
+  for (int64_t i = 0; i < n; i++) {
+    sum[2 * i] = nb.cur_slp_sum[i].x;
+    sum[2 * i + 1] = nb.cur_slp_sum[i].y;
+    if (wl) {
+      wl[2 * i] = nb.cur_slp_wl[i].x;
+      wl[2 * i + 1] = nb.cur_slp_wl[i].y;
+    }
+    if (den) {
+      den[2 * i] = nb.cur_slp_den[i].x;
+      den[2 * i + 1] = nb.cur_slp_den[i].y;
+    }
+  }
+  sums[0] = nb.wl_grad_sum;
+  sums[1] = nb.density_grad_sum;
+}
+// `getHpwl` (src/nesterov.rs:2297-2304) over nets of pins at pin_xy (net-major).
+int64_t oracle_hpwl(int64_t n_nets, const int64_t *net_start, const int32_t *pin_xy) {
+  Nesterov np;
+  np.gpins.resize((size_t)net_start[n_nets]);
+  for (int64_t p = 0; p < net_start[n_nets]; p++) {
+    np.gpins[p].cx = pin_xy[2 * p];
+    np.gpins[p].cy = pin_xy[2 * p + 1];
+  }
+  np.gnets.resize((size_t)n_nets);
+  for (int64_t k = 0; k < n_nets; k++)
+    for (int64_t p = net_start[k]; p < net_start[k + 1]; p++) np.gnets[k].pins.push_back((int)p);
+  return np.hpwl();
 }
 
 // The 1-D transforms, for checking against direct sums. kind 0 dct2, 1 idct, 2 idst.

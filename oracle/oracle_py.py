@@ -60,6 +60,10 @@ def lib():
         _lib.oracle_density_scatter.argtypes = [C.c_int64] + [C.c_void_p] * 6 + [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_float, C.c_void_p, C.c_void_p]
         _lib.oracle_density_gradient.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.oracle_wa.argtypes = [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_void_p]
+        _lib.oracle_nesterov_step.argtypes = [C.c_int64] + [C.c_void_p] * 8 + [C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_float, C.c_float, C.c_float] + [C.c_void_p] * 5
+        _lib.oracle_gradients.argtypes = [C.c_int64] + [C.c_void_p] * 9 + [C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.oracle_hpwl.restype = C.c_int64
+        _lib.oracle_hpwl.argtypes = [C.c_int64, C.c_void_p, C.c_void_p]
         _lib.oracle_uniform_int_draws.argtypes = [C.c_uint32, C.c_int, C.c_void_p, C.c_int, C.c_void_p]
         _lib.oracle_min_max_idx.argtypes = [C.c_int32] * 6 + [C.c_void_p]
         _lib.oracle_snap_outward.argtypes = [C.c_void_p] + [C.c_int32] * 4

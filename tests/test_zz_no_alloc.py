@@ -86,3 +86,34 @@ def test_no_alloc_rejects_a_system_beyond_its_scratch():
     rc = L.gpl_kernel_bicgstab_noalloc(MAX_ROWS + 1, None, None, None, None, None, 100, C.byref(it), C.byref(err), None)
     assert rc == TOO_LARGE
     assert it.value == -7
+
+
+def test_no_alloc_solves_a_system_of_exactly_its_maximum_size():
+    """At n = GPL_BICGSTAB_NOALLOC_MAX_ROWS the solve's scratch fills the fixed array exactly."""
+    import torch
+    from gpl_b200 import engine
+    L = engine.lib()
+    L.gpl_kernel_bicgstab_noalloc.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    n = MAX_ROWS
+    rs, cols, vals, rhs, x0 = _system(n, 5)
+    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    d_rs, d_cols, d_vals, d_rhs = dev(rs), dev(cols), dev(vals), dev(rhs)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    p = lambda t: C.c_void_p(t.data_ptr())
+    x_ref, x = dev(x0), dev(x0)
+    it_ref, err_ref, it, err = C.c_int32(), C.c_float(), C.c_int32(), C.c_float()
+    assert L.gpl_kernel_bicgstab(n, p(d_rs), p(d_cols), p(d_vals), p(d_rhs), p(x_ref), 100, C.byref(it_ref), C.byref(err_ref), stream) == 0
+    assert L.gpl_kernel_bicgstab_noalloc(n, p(d_rs), p(d_cols), p(d_vals), p(d_rhs), p(x), 100, C.byref(it), C.byref(err), stream) == 0
+    want, got = x_ref.cpu().numpy(), x.cpu().numpy()
+    np.testing.assert_allclose(got, want, rtol=1e-4, atol=1e-3 * np.max(np.abs(want)))
+    assert it.value == it_ref.value and err.value < 1e-5
+
+
+def test_no_alloc_rejects_a_negative_size():
+    from gpl_b200 import engine
+    L = engine.lib()
+    L.gpl_kernel_bicgstab_noalloc.argtypes = [C.c_int64] + [C.c_void_p] * 5 + [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    it, err = C.c_int32(-7), C.c_float()
+    rc = L.gpl_kernel_bicgstab_noalloc(-1, None, None, None, None, None, 100, C.byref(it), C.byref(err), None)
+    assert rc == 1  # cudaErrorInvalidValue
+    assert it.value == -7

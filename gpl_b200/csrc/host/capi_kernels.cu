@@ -278,7 +278,7 @@ int gpl_kernel_wa(int64_t n_nets, const int64_t *net_start, const int32_t *pin_x
     e = d.build(n_nets, net_start, pin_xy, net_weight);
     if (e == cudaSuccess) {
       WaArgs w = d.args(grad);
-      if (const int nb = wa_small_blocks(w.small)) k_wa_small<<<nb, kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y, 1);
+      launch_wa_small(w, coef_x, coef_y, 1, s);
       if (w.n_tiles) launch_wa_tiles(w, coef_x, coef_y, s);
       if (w.n_nets) k_wa<<<(unsigned)((w.n_nets + kThreadsPerBlock - 1) / kThreadsPerBlock), kThreadsPerBlock, 0, s>>>(w, coef_x, coef_y);
       e = cudaGetLastError();
@@ -309,12 +309,12 @@ int gpl_kernel_hpwl(int64_t n_nets, const int64_t *net_start, const int32_t *pin
       const float c = 1e-4f;  // any coefficient: the HPWL is the pins' boxes
       if (fused) {
         // the HPWL the WA kernels add up beside the forces (the trial's read-back)
-        if (const int nb = wa_small_blocks(w.small)) k_wa_small<<<nb, kThreadsPerBlock, 0, s>>>(w, c, c, 1);
+        launch_wa_small(w, c, c, 1, s);
         if (w.n_tiles) launch_wa_tiles(w, c, c, s);
         if (w.n_nets) k_wa<<<nbig, kThreadsPerBlock, 0, s>>>(w, c, c);
       } else {
         // the HPWL kernels of an iteration without a WA pass
-        if (const int nb = wa_small_blocks(w.small)) k_wa_small<<<nb, kThreadsPerBlock, 0, s>>>(w, 0.0f, 0.0f, 0);
+        launch_wa_small(w, 0.0f, 0.0f, 0, s);
         if (w.n_tiles) k_hpwl_tiles<<<(unsigned)w.n_tiles, kThreadsPerBlock, 0, s>>>(w, acc);
         if (w.n_nets) k_hpwl<<<nbig, kThreadsPerBlock, 0, s>>>(w, acc);
       }

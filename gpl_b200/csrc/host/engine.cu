@@ -205,7 +205,7 @@ void Engine::upload(const EngineSetup &s) {
     check(upload_vec(&net_start_, ns, st), "upload nets");
     // WA's tiles of consecutive nets, and the nets too large for a tile (already in degree
     // order, so a warp's threads walk nets of one length)
-    // the degree-2..4 nets run a thread per net (k_wa_small); the tiles take the rest: the
+    // the degree-2..4 nets run a lane per pin (k_wa_pins); the tiles take the rest: the
     // nets below degree 2 and those above 4
     small_ = wa_small_ranges(ns.data(), n_nets_);
     const int32_t small_lo = small_.first[0], small_hi = small_.first[2] + small_.count[2];
@@ -453,9 +453,9 @@ void Engine::wa(float cx, float cy) {
   hpwl_ready_ = true;
   hpwl_fetched_ = false;
   ph_begin(PH_WA, st);
-  if (const int nb = wa_small_blocks(small_)) {
+  if (wa_small_blocks(small_)) {
     launches += 1;
-    k_wa_small<<<nb, kThreadsPerBlock, 0, st>>>(w, cx, cy, 1);
+    launch_wa_small(w, cx, cy, 1, st);
   }
   if (n_tiles_) {
     launches += 1;
@@ -547,11 +547,11 @@ int64_t Engine::hpwl() {
   if (!hpwl_ready_) {
   check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), stream_), "hpwl");
   ph_begin(PH_HPWL);
-  if (const int nb = wa_small_blocks(small_)) {
+  if (wa_small_blocks(small_)) {
     launches += 1;
     WaArgs wh = w;
     wh.hpwl_out = hpwl_acc_;
-    k_wa_small<<<nb, kThreadsPerBlock, 0, stream_>>>(wh, 0.0f, 0.0f, 0);
+    launch_wa_small(wh, 0.0f, 0.0f, 0, stream_);
   }
   if (n_tiles_) {
     launches += 1;

@@ -80,6 +80,13 @@ __global__ void k_wa_tiles(WaArgs w, float cx, float cy);
 // w.hpwl_out. Launch with wa_small_blocks(w.small) blocks.
 __global__ void k_wa_small(WaArgs w, float cx, float cy, int forces);
 int wa_small_blocks(const WaSmall &s);
+// The same nets, a lane per pin (32 / D nets per warp): forces and HPWL bit for bit as
+// k_wa_small's. Launch with wa_pins_blocks(w.small) blocks.
+__global__ void k_wa_pins(WaArgs w, float cx, float cy, int forces);
+int wa_pins_blocks(const WaSmall &s);
+// The degree-2..4 nets' WA (forces != 0) or HPWL alone: k_wa_pins, or k_wa_small when the
+// environment sets GPL_WA_SMALL=nets (the same results; a timing comparison).
+void launch_wa_small(const WaArgs &w, float cx, float cy, int forces, cudaStream_t s);
 // The degree-2..4 ranges of nets already in degree order.
 WaSmall wa_small_ranges(const int64_t *net_start, int32_t n_nets);
 // k_wa_tiles over every tile: a persistent grid of the blocks the device holds at once.

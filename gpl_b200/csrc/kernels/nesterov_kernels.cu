@@ -7,6 +7,9 @@
 // and WA gradients) are bit-identical to the reference's for identical inputs. Only the
 // cross-cell sums (overflow, |gradient| sums, step-length distances) are taken in double and
 // in a different order.
+#include <cstdlib>
+#include <string>
+
 #include "common.cuh"
 #include "engine_kernels.h"
 
@@ -600,6 +603,121 @@ __global__ void __launch_bounds__(kThreads) k_wa_small(WaArgs w, float cx, float
 #pragma unroll
     for (int j = 0; j < kThreads / 32; j++) sum += s_h[j];
     if (sum) atomicAdd(w.hpwl_out, (unsigned long long)sum);
+  }
+}
+
+// The same nets of degree D = 2, 3, 4, a lane per pin: a warp holds 32 / D nets, each net's D
+// lanes consecutive, so the pins' loads are coalesced and every lane waits on one chain (its
+// pin's cell, then that cell's centre) instead of D. The net's positions and exp terms reach
+// its lanes by shuffles; every lane of a net forms the net's box and its eight sums in pin
+// order itself (the reference's float order), then its own pin's force. Registers stay low
+// enough for 6 blocks per SM. Results are k_wa_small's bit for bit.
+template <int D>
+__device__ __forceinline__ long long wa_lane(const WaArgs &w, int32_t first, int32_t count, int64_t pin0, int blk, float cx, float cy, bool forces) {
+  constexpr int G = 32 / D;  // nets per warp
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane / D, j = lane - g * D;
+  const int32_t t = (blk * (kThreads / 32) + warp) * G + g;  // the net's index in its range
+  const bool active = g < G && t < count;
+  const int64_t p = pin0 + (int64_t)t * D + j;
+  int2 q = make_int2(0, 0);
+  int32_t at = -1;
+  if (active) {
+    q = pin_pos(w, p);
+    at = w.pin_slot ? w.pin_slot[p] : (int32_t)p;
+  }
+  const int base = g * D;  // the net's first lane (lanes past the last group read lane 0..: unused)
+  int32_t X[D], Y[D];
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    X[i] = __shfl_sync(0xffffffffu, q.x, (base + i) & 31);
+    Y[i] = __shfl_sync(0xffffffffu, q.y, (base + i) & 31);
+  }
+  int32_t lx = X[0], ly = Y[0], ux = X[0], uy = Y[0];
+#pragma unroll
+  for (int i = 1; i < D; i++) {
+    lx = min(lx, X[i]);
+    ly = min(ly, Y[i]);
+    ux = max(ux, X[i]);
+    uy = max(uy, Y[i]);
+  }
+  const long long h = active && j == 0 ? ((long long)ux - lx) + ((long long)uy - ly) : 0;
+  if (!forces) return h;
+  const float BAR = -300.0f;
+  float emin_x = __fmul_rn((float)(lx - q.x), cx), emax_x = __fmul_rn((float)(q.x - ux), cx);
+  float emin_y = __fmul_rn((float)(ly - q.y), cy), emax_y = __fmul_rn((float)(q.y - uy), cy);
+  const uint32_t m = (emin_x > BAR ? 1u : 0u) | (emax_x > BAR ? 2u : 0u) | (emin_y > BAR ? 4u : 0u) | (emax_y > BAR ? 8u : 0u);
+  float4 v;
+  v.x = (m & 1u) ? fast_exp(emin_x) : 0.0f;
+  v.y = (m & 2u) ? fast_exp(emax_x) : 0.0f;
+  v.z = (m & 4u) ? fast_exp(emin_y) : 0.0f;
+  v.w = (m & 8u) ? fast_exp(emax_y) : 0.0f;
+  float s_minx = 0, s_xminx = 0, s_maxx = 0, s_xmaxx = 0, s_miny = 0, s_yminy = 0, s_maxy = 0, s_ymaxy = 0;
+#pragma unroll
+  for (int i = 0; i < D; i++) {
+    const int src = (base + i) & 31;
+    const float vx = __shfl_sync(0xffffffffu, v.x, src), vy = __shfl_sync(0xffffffffu, v.y, src);
+    const float vz = __shfl_sync(0xffffffffu, v.z, src), vw = __shfl_sync(0xffffffffu, v.w, src);
+    const float qx = (float)X[i], qy = (float)Y[i];
+    s_minx = __fadd_rn(s_minx, vx);
+    s_xminx = __fadd_rn(s_xminx, __fmul_rn(qx, vx));
+    s_maxx = __fadd_rn(s_maxx, vy);
+    s_xmaxx = __fadd_rn(s_xmaxx, __fmul_rn(qx, vy));
+    s_miny = __fadd_rn(s_miny, vz);
+    s_yminy = __fadd_rn(s_yminy, __fmul_rn(qy, vz));
+    s_maxy = __fadd_rn(s_maxy, vw);
+    s_ymaxy = __fadd_rn(s_ymaxy, __fmul_rn(qy, vw));
+  }
+  if (active) {
+    const float qx = (float)q.x, qy = (float)q.y;
+    const float wt = w.net_weight ? w.net_weight[first + t] : 1.0f;
+    float gmin_x = (m & 1u) ? wa_term_min(s_minx, s_xminx, v.x, cx, qx) : 0.0f;
+    float gmax_x = (m & 2u) ? wa_term_max(s_maxx, s_xmaxx, v.y, cx, qx) : 0.0f;
+    float gmin_y = (m & 4u) ? wa_term_min(s_miny, s_yminy, v.z, cy, qy) : 0.0f;
+    float gmax_y = (m & 8u) ? wa_term_max(s_maxy, s_ymaxy, v.w, cy, qy) : 0.0f;
+    if (at >= 0) w.pin_grad[at] = make_float2(__fmul_rn(__fsub_rn(gmin_x, gmax_x), wt), __fmul_rn(__fsub_rn(gmin_y, gmax_y), wt));
+  }
+  return h;
+}
+
+// Blocks per degree range of k_wa_pins: a block holds kThreads / 32 warps of 32 / D nets.
+__host__ __device__ __forceinline__ int wa_pins_range_blocks(int32_t count, int d) { return (int)((count + (kThreads / 32) * (32 / d) - 1) / ((kThreads / 32) * (32 / d))); }
+
+__global__ void __launch_bounds__(kThreads, 6) k_wa_pins(WaArgs w, float cx, float cy, int forces) {
+  const int nb0 = wa_pins_range_blocks(w.small.count[0], 2), nb1 = wa_pins_range_blocks(w.small.count[1], 3);
+  const int b = blockIdx.x;
+  long long h;
+  if (b < nb0)
+    h = wa_lane<2>(w, w.small.first[0], w.small.count[0], w.small.pin0[0], b, cx, cy, forces != 0);
+  else if (b < nb0 + nb1)
+    h = wa_lane<3>(w, w.small.first[1], w.small.count[1], w.small.pin0[1], b - nb0, cx, cy, forces != 0);
+  else
+    h = wa_lane<4>(w, w.small.first[2], w.small.count[2], w.small.pin0[2], b - nb0 - nb1, cx, cy, forces != 0);
+  __shared__ long long s_h[kThreads / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) h += __shfl_down_sync(0xffffffffu, h, o);
+  if ((threadIdx.x & 31) == 0) s_h[threadIdx.x >> 5] = h;
+  __syncthreads();
+  if (threadIdx.x == 0 && w.hpwl_out) {
+    long long sum = 0;
+#pragma unroll
+    for (int j = 0; j < kThreads / 32; j++) sum += s_h[j];
+    if (sum) atomicAdd(w.hpwl_out, (unsigned long long)sum);
+  }
+}
+
+int wa_pins_blocks(const WaSmall &s) { return wa_pins_range_blocks(s.count[0], 2) + wa_pins_range_blocks(s.count[1], 3) + wa_pins_range_blocks(s.count[2], 4); }
+
+bool wa_small_per_net() {
+  const char *f = std::getenv("GPL_WA_SMALL");
+  return f && std::string(f) == "nets";
+}
+
+void launch_wa_small(const WaArgs &w, float cx, float cy, int forces, cudaStream_t s) {
+  if (wa_small_per_net()) {
+    if (const int nb = wa_small_blocks(w.small)) k_wa_small<<<nb, kThreads, 0, s>>>(w, cx, cy, forces);
+  } else if (const int nb = wa_pins_blocks(w.small)) {
+    k_wa_pins<<<nb, kThreads, 0, s>>>(w, cx, cy, forces);
   }
 }
 

@@ -7,7 +7,7 @@ These runs take minutes (100k cells) to about an hour (1M cells) on one CPU thre
 GPU tests compare against this summary instead of re-running the oracle. Run from the
 repository root:
 
-    python tests/golden/make_oracle_runs.py [cfg2] [cfg3]
+    python tests/golden/make_oracle_runs.py [cfg2] [cfg3] [cfg2_route]
 """
 import json
 import os
@@ -23,8 +23,16 @@ from gpl_b200 import synth  # noqa: E402
 ARGS = {
     "cfg2": ["-density", "0.70", "-bin_grid_count", "512"],
     "cfg3": ["-density", "0.70", "-bin_grid_count", "1024"],
+    # routability-driven, with the synthetic router: 3000-DBU tiles, one 1200-DBU pitch (so the
+    # RUDY map overflows and the passes inflate cells), capacity 20
+    "cfg2_route": ["-density", "0.70", "-bin_grid_count", "512", "-routability_driven"],
 }
+ROUTER = {"cfg2_route": dict(tile=3000, pitches=(1200,), capacity=20)}
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle_runs.json")
+
+
+def _codes(lines, code):
+    return [l for l in lines if f"GPL-{code}]" in l]
 
 
 def summarise(cfg, res, seconds):
@@ -45,15 +53,23 @@ def summarise(cfg, res, seconds):
         "locations": int(len(loc)),
         "location_sums": [int(loc[:, 1].astype("int64").sum()), int(loc[:, 2].astype("int64").sum())] if len(loc) else [0, 0],
         "seconds": seconds,
+        # the routability passes: the snapshot line, each pass's line, the final area line
+        "route": {"snapshot": _codes(lines, "0038"), "passes": _codes(lines, "0040"), "area": _codes(lines, "1014"),
+                  "recovery": _codes(lines, "0112")},
     }
 
 
 def main(cfgs):
     out = json.load(open(OUT)) if os.path.exists(OUT) else {}
     for cfg in cfgs:
-        d = synth.generate(cfg)
+        d = synth.generate(cfg.split("_")[0])
+        router = None
+        if cfg in ROUTER:
+            from gpl_b200 import engine  # the synthetic router only (host code, no device)
+            rt = ROUTER[cfg]
+            router = engine.SyntheticRouter(d, rt["tile"], pitches=rt["pitches"], capacity=rt["capacity"])
         t0 = time.perf_counter()
-        res = oracle.global_placement(d, ARGS[cfg])
+        res = oracle.global_placement(d, ARGS[cfg], router=router.ptr if router else None)
         out[cfg] = summarise(cfg, res, time.perf_counter() - t0)
         print(cfg, out[cfg]["status"], out[cfg]["nesterov_iterations"], out[cfg]["final_hpwl"], out[cfg]["final_overflow"], flush=True)
         with open(OUT, "w") as f:

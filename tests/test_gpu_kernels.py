@@ -304,3 +304,31 @@ def test_poisson_errors_against_the_fp64_solve(L, nx, ny):
         assert L.gpl_kernel_poisson(nx, ny, wx.ctypes.data, wy.ctypes.data, ptr(d), ptr(gx), ptr(gy), mode, stream()) == 0
         sync()
         assert err(gx.cpu().numpy(), ex64) <= tol and err(gy.cpu().numpy(), ey64) <= tol, mode
+
+
+@pytest.mark.parametrize("form", ["pins", "nets"])
+def test_wa_small_net_forms_bit_exact(L, form, monkeypatch):
+    """The degree-2..4 nets' two kernels (a lane per pin, the default; a thread per net with
+    GPL_WA_SMALL=nets) against the oracle, bit for bit: most nets of a netlist are of these
+    degrees."""
+    monkeypatch.setenv("GPL_WA_SMALL", form)
+    rng = np.random.default_rng(71)
+    n_nets = 60000
+    deg = rng.integers(2, 5, n_nets)
+    start = np.concatenate([[0], np.cumsum(deg)]).astype(np.int64)
+    xy = rng.integers(0, 400000, (int(start[-1]), 2)).astype(np.int32)
+    for k in np.flatnonzero(rng.random(n_nets) < 0.4):
+        xy[start[k]:start[k + 1]] = xy[start[k]] + rng.integers(0, 2000, (deg[k], 2))
+    w = rng.uniform(1.0, 2.0, n_nets).astype(np.float32)
+    want = np.zeros(2 * len(xy), np.float32)
+    coef = 3.1e-4
+    oracle.lib().oracle_wa(C.c_int64(n_nets), start.ctypes.data_as(C.c_void_p), xy.ctypes.data_as(C.c_void_p),
+                           w.ctypes.data_as(C.c_void_p), C.c_float(coef), C.c_float(coef * 1.3), want.ctypes.data_as(C.c_void_p))
+    ds, dxy, dw = dev(start), dev(xy), dev(w)
+    g = dev(np.zeros(2 * len(xy), np.float32))
+    assert L.gpl_kernel_wa(n_nets, ptr(ds), ptr(dxy), ptr(dw), coef, coef * 1.3, ptr(g), stream()) == 0
+    sync()
+    np.testing.assert_array_equal(g.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    got = C.c_int64()
+    assert L.gpl_kernel_hpwl(n_nets, ptr(ds), ptr(dxy), 0, C.byref(got), stream()) == 0
+    assert got.value == oracle.lib().oracle_hpwl(n_nets, start.ctypes.data_as(C.c_void_p), xy.ctypes.data_as(C.c_void_p))

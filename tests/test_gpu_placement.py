@@ -136,3 +136,35 @@ def test_region_groups_match_the_oracle():
         assert abs(a[k] - b[k]) <= 10, (k, a[k], b[k])
     assert abs(got["final_hpwl"] - ref["final_hpwl"]) <= 1e-3 * ref["final_hpwl"]
     assert abs(got["final_overflow"] - ref["final_overflow"]) <= 0.005
+
+
+DIVERGE = ("GPL-0323", "GPL-0324", "GPL-0998", "GPL-0997", "GPL-0307")
+
+
+def _divergence_course(lines):
+    return [c for l in lines for c in DIVERGE if c in l]
+
+
+@pytest.mark.parametrize("extra", [["-max_phi_coef", "1.15", "-init_density_penalty", "0.001", "-overflow", "0.03"],
+                                   ["-max_phi_coef", "1.05", "-init_density_penalty", "0.00008", "-overflow", "0.03"]])
+def test_divergence_revert_takes_the_oracles_course(cfg1, extra):
+    """An overflow target the design cannot reach (0.03) runs the loop on until it diverges
+    (`check_divergence`, src/nesterov.rs:2976-2991): the oracle then reverts to the minimum-HPWL
+    snapshot and resumes twice (GPL-0998) and reverts and stops the third time (GPL-0997,
+    :3009-3052, :4406-4414). The engine must take the same course on the device's snapshots,
+    and end at a minimum-HPWL state close to the oracle's."""
+    d, _ = cfg1
+    args = ARGS + extra
+    ref = oracle.global_placement(d, args)
+    got = engine.global_placement(d, args)
+    course = _divergence_course(ref["lines"])
+    assert course[-1] == "GPL-0997" and course.count("GPL-0998") == 2  # the oracle's course, as recorded
+    assert got["status"] == ref["status"] == "placed", got["reason"]
+    print("divergence course", _divergence_course(got["lines"]), course, "iterations", got["nesterov_iterations"], ref["nesterov_iterations"],
+          "hpwl", got["final_hpwl"], ref["final_hpwl"], "overflow", got["final_overflow"], ref["final_overflow"])
+    assert _divergence_course(got["lines"]) == course
+    # the "(k of 3 reverts allowed)" counts, in order
+    reverts = lambda r: [l.split("(")[1] for l in r["lines"] if "GPL-0998" in l]
+    assert reverts(got) == reverts(ref)
+    assert abs(got["final_hpwl"] - ref["final_hpwl"]) <= 0.02 * ref["final_hpwl"]
+    assert abs(got["final_overflow"] - ref["final_overflow"]) <= 0.01

@@ -62,3 +62,37 @@ def test_mixed_and_fp32_forms_agree_at_2m_cells():
     assert a["status"] == "placed" and b["status"] == "placed", (a["reason"], b["reason"])
     assert a["final_overflow"] <= 0.1 and b["final_overflow"] <= 0.1
     assert abs(a["final_hpwl"] - b["final_hpwl"]) <= 1e-3 * b["final_hpwl"]
+
+
+def _route_numbers(lines):
+    snap = [int(l.split("=")[-1]) for l in lines if "GPL-0038]" in l]
+    cong = [float(l.split("congestion")[1].split()[0]) for l in lines if "GPL-0040]" in l]
+    area = [float(l.split(":")[1].split("(")[0]) for l in lines if "GPL-1014]" in l]
+    return snap, cong, area
+
+
+def test_routability_at_100k_cells_matches_the_oracle():
+    """-routability_driven on the 100k-cell design with the synthetic router (3000-DBU tiles,
+    one 1200-DBU pitch: the RUDY map overflows, so every pass inflates cells and cuts fillers),
+    against the oracle's recorded run: the snapshot within 5 iterations, the same number of
+    passes, each pass's weighted congestion within 2 %, the final placement area (the cells as
+    inflated) within 0.5 %, final HPWL within 1 % and overflow within 0.005."""
+    if "cfg2_route" not in RUNS:
+        pytest.skip("no recorded oracle run for cfg2_route")
+    ref = RUNS["cfg2_route"]
+    d = synth.generate("cfg2")
+    rt = engine.SyntheticRouter(d, 3000, pitches=(1200,), capacity=20)
+    got = engine.global_placement(d, ref["args"], router=rt)
+    assert got["status"] == "placed", got["reason"]
+    assert header(got["lines"]) == ref["header"]
+    snap, cong, area = _route_numbers(got["lines"])
+    rsnap, rcong, rarea = _route_numbers(ref["route"]["snapshot"] + ref["route"]["passes"] + ref["route"]["area"])
+    print("routability at 100k cells: snapshot", snap, rsnap, "passes", cong, rcong, "area", area, rarea,
+          "hpwl", got["final_hpwl"], ref["final_hpwl"], "overflow", got["final_overflow"], ref["final_overflow"])
+    assert len(snap) == 1 and abs(snap[0] - rsnap[0]) <= 5
+    assert len(cong) == len(rcong)
+    for a, b in zip(cong, rcong):
+        assert abs(a - b) <= 0.02 * b
+    assert abs(area[0] - rarea[0]) <= 0.005 * rarea[0]
+    assert abs(got["final_hpwl"] - ref["final_hpwl"]) <= 0.01 * ref["final_hpwl"]
+    assert abs(got["final_overflow"] - ref["final_overflow"]) <= 0.005

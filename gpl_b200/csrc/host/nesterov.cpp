@@ -301,13 +301,18 @@ struct Rudy {
     if (d_boxes) cudaFree(d_boxes);
     if (d_demand) cudaFree(d_demand);
   }
-  void calculate(const std::vector<uint8_t> &cap_red, const std::vector<std::array<int32_t, 4>> &nets) {
-    std::fill(demand.begin(), demand.end(), 0.0f);
+  // `resource_reductions` (src/route_base.rs:184-188): min(reduction / capacity, 1), 1 where the
+  // capacity is 0.
+  void set_blockage(const std::vector<uint8_t> &cap_red) {
     std::fill(blockage.begin(), blockage.end(), 0.0f);
     for (size_t i = 0; i < blockage.size() && 2 * i + 1 < cap_red.size(); i++) {
       uint8_t cap = cap_red[2 * i], red = cap_red[2 * i + 1];
       blockage[i] = cap == 0 ? 1.0f : fminr((float)red / (float)cap, 1.0f);
     }
+  }
+  void calculate(const std::vector<uint8_t> &cap_red, const std::vector<std::array<int32_t, 4>> &nets) {
+    std::fill(demand.begin(), demand.end(), 0.0f);
+    set_blockage(cap_red);
     auto ok = [](cudaError_t e, const char *where) {
       if (e != cudaSuccess) throw std::runtime_error(std::string("device: ") + cudaGetErrorString(e) + " in " + where);
     };
@@ -2501,4 +2506,165 @@ void gpl_result_free(gpl_result_t *out) {
   std::memset(out, 0, sizeof *out);
 }
 
+}  // extern "C"
+
+// ---- test-only exports (not in include/gpl.h): the engine's own host rules, so the tests can
+// check them against the reference's unit-test vectors directly, not only through the oracle's
+// restatement. Each takes the same arguments as the oracle's function of the same suffix.
+extern "C" {
+using namespace gpl;
+uint32_t gpl_rules_mt19937_nth(uint32_t seed, int64_t n) {
+  Mt19937 e(seed);
+  uint32_t last = 0;
+  for (int64_t i = 0; i < n; i++) last = e.next_u32();
+  return last;
+}
+uint32_t gpl_rules_normal_draws(uint32_t seed, double sigma, int k, double *out) {
+  Mt19937 e(seed);
+  for (int i = 0; i < k; i++) {
+    double v = normal(e, 0.0, sigma);
+    if (out) out[i] = v;
+  }
+  return e.next_u32();
+}
+void gpl_rules_uniform_int_draws(uint32_t seed, int nr, const int32_t *ranges, int per, int32_t *out) {
+  Mt19937 e(seed);
+  for (int r = 0; r < nr; r++)
+    for (int i = 0; i < per; i++) out[r * per + i] = uniform_int(e, -ranges[r], ranges[r]);
+}
+void gpl_rules_min_max_idx(int32_t ll, int32_t uu, int32_t core_ll, int32_t site, int32_t mn, int32_t mx, int32_t *out2) {
+  auto [a, b] = min_max_idx(ll, uu, core_ll, site, mn, mx);
+  out2[0] = a;
+  out2[1] = b;
+}
+static Instance instance_of(const int32_t *box4) {
+  Instance i;
+  i.db = 0;
+  i.lx = box4[0];
+  i.ly = box4[1];
+  i.ux = box4[2];
+  i.uy = box4[3];
+  return i;
+}
+static void box_of(const Instance &i, int32_t *box4) {
+  box4[0] = i.lx;
+  box4[1] = i.ly;
+  box4[2] = i.ux;
+  box4[3] = i.uy;
+}
+void gpl_rules_snap_outward(int32_t *box4, int32_t ox, int32_t oy, int32_t sx, int32_t sy) {
+  Instance i = instance_of(box4);
+  i.snap_outward(ox, oy, sx, sy);
+  box_of(i, box4);
+}
+int64_t gpl_rules_extend_size_by_scale(int32_t *box4, double scale) {
+  Instance i = instance_of(box4);
+  int64_t d = i.extend_size_by_scale(scale);
+  box_of(i, box4);
+  return d;
+}
+void gpl_rules_orient_point(int orient, int32_t x, int32_t y, int32_t *out2) {
+  auto [a, b] = orient_point(orient, x, y);
+  out2[0] = a;
+  out2[1] = b;
+}
+int gpl_rules_fmt(const char *which, double v, int a, int b, char *buf, int cap) {
+  std::string s, w = which;
+  if (w == "fmt_e")
+    s = fmt_e(v, a, b);
+  else if (w == "fmt_g")
+    s = fmt_g(v);
+  else if (w == "fmt_g_prec")
+    s = fmt_g_prec(v, a);
+  else if (w == "log_f32")
+    s = log_fmt_f32((float)v);
+  else if (w == "log_f64")
+    s = log_fmt_f64(v);
+  else if (w == "log_e")
+    s = log_fmt_e(v, a);
+  else if (w == "rust_f32")
+    s = rust_f32((float)v);
+  else
+    return -1;
+  std::snprintf(buf, cap, "%s", s.c_str());
+  return (int)s.size();
+}
+int gpl_rules_diverge_fallback(int saved, int reverts, int disable) {
+  LoopSnapshots s;
+  s.diverge_saved = saved;
+  s.diverge_reverts = reverts;
+  return (int)diverge_fallback(s, disable);
+}
+int gpl_rules_routability_recovery_attempt(int route_saved, int attempts, int saved, int reverts, int need) {
+  LoopSnapshots s;
+  s.route_saved = route_saved;
+  s.route_attempts = attempts;
+  s.diverge_saved = saved;
+  s.diverge_reverts = reverts;
+  return routability_recovery_attempt(s, need);
+}
+int gpl_rules_max_iter_takes_snapshot(int iter, int max_iter, int disable, int saved, int reverts, int64_t snap_hpwl, float snap_ov, float ov, int64_t hpwl) {
+  LoopSnapshots s;
+  s.diverge_saved = saved;
+  s.diverge_reverts = reverts;
+  s.diverge_hpwl = snap_hpwl;
+  return max_iter_takes_min_hpwl_snapshot(iter, max_iter, disable, s, snap_ov, ov, hpwl);
+}
+void gpl_rules_settle_wait_step(int start, int iter, int active, int settled, int *out3) {
+  int extra = 0;
+  auto [s, e] = settle_wait_step(start, iter, active, settled, extra);
+  out3[0] = s;
+  out3[1] = e;
+  out3[2] = extra;
+}
+float gpl_rules_fast_exp(float x) { return fast_exp(x); }
+float gpl_rules_wavenumber_x(int i, int nx) { return wavenumber_x(i, nx); }
+float gpl_rules_wavenumber_y(int i, int ny, float bx, float by) { return wavenumber_y(i, ny, bx, by); }
+uint32_t gpl_rules_round_down_pow2(uint32_t x) { return round_down_to_power_of_two(x); }
+int64_t gpl_rules_union_area(int n, const int32_t *rects) {
+  std::vector<std::array<int32_t, 4>> r(n);
+  for (int i = 0; i < n; i++) r[i] = {rects[4 * i], rects[4 * i + 1], rects[4 * i + 2], rects[4 * i + 3]};
+  return union_area(r);
+}
+float gpl_rules_distance(int n, const float *a, const float *b) {
+  std::vector<FloatPoint> x(n), y(n);
+  for (int i = 0; i < n; i++) {
+    x[i] = {a[2 * i], a[2 * i + 1]};
+    y[i] = {b[2 * i], b[2 * i + 1]};
+  }
+  return distance(x, y);
+}
+float gpl_rules_derived_reference_hpwl(float user, int64_t h) { return derived_reference_hpwl(user, h); }
+void gpl_rules_set_size(int32_t *box4, int32_t dx, int32_t dy) {
+  GCell g;
+  g.lx = box4[0];
+  g.ly = box4[1];
+  g.ux = box4[2];
+  g.uy = box4[3];
+  set_size(g, dx, dy);
+  box4[0] = g.lx;
+  box4[1] = g.ly;
+  box4[2] = g.ux;
+  box4[3] = g.uy;
+}
+void gpl_rules_top_averages(int n, const double *desc, double *out4) {
+  auto a = top_averages(std::vector<double>(desc, desc + n));
+  for (int k = 0; k < 4; k++) out4[k] = a[k];
+}
+// RUDY's host half (src/route_base.rs:144-188, :257-264): wire width, tile rects (x-major),
+// blockage and congestion for the given demand.
+void gpl_rules_rudy_grid(const int32_t die4[4], int32_t xg, int32_t yg, int32_t ts, int np, const int32_t *pitches, const uint8_t *cap_red, const float *demand, int32_t *wire_width, int32_t *rects, float *blockage, float *congestion) {
+  Rudy r;
+  r.init(die4, xg, yg, ts, std::vector<int32_t>(pitches, pitches + np));
+  *wire_width = r.wire_width;
+  for (size_t k = 0; k < r.rects.size(); k++)
+    for (int q = 0; q < 4; q++) rects[4 * k + q] = r.rects[k][q];
+  r.set_blockage(std::vector<uint8_t>(cap_red, cap_red + 2 * r.blockage.size()));
+  std::copy(demand, demand + r.demand.size(), r.demand.begin());
+  for (int32_t x = 0; x < xg; x++)
+    for (int32_t y = 0; y < yg; y++) {
+      blockage[r.at(x, y)] = r.blockage[r.at(x, y)];
+      congestion[r.at(x, y)] = r.congestion(x, y);
+    }
+}
 }  // extern "C"

@@ -152,7 +152,7 @@ def test_divergence_revert_takes_the_oracles_course(cfg1):
     :3009-3052, :4406-4414). The engine must take the same course on the device's snapshots,
     and end at a minimum-HPWL state close to the oracle's. (Such a run is chaotic after the
     first reverts: with -max_phi_coef 1.05 and -init_density_penalty 8e-5 the engine's run
-    diverged differently and ended on a NaN step, so only this course is asserted.)"""
+    diverged differently and stopped with an error status, so only this course is asserted.)"""
     d, _ = cfg1
     args = ARGS + ["-max_phi_coef", "1.15", "-init_density_penalty", "0.001", "-overflow", "0.03"]
     ref = oracle.global_placement(d, args)

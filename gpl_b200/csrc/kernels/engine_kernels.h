@@ -84,8 +84,9 @@ int wa_small_blocks(const WaSmall &s);
 // k_wa_small's. Launch with wa_pins_blocks(w.small) blocks.
 __global__ void k_wa_pins(WaArgs w, float cx, float cy, int forces);
 int wa_pins_blocks(const WaSmall &s);
-// The degree-2..4 nets' WA (forces != 0) or HPWL alone: k_wa_pins, or k_wa_small when the
-// environment sets GPL_WA_SMALL=nets (the same results; a timing comparison).
+// The degree-2..4 nets' WA (forces != 0) or HPWL alone: k_wa_lean, or k_wa_small / k_wa_pins
+// when the environment sets GPL_WA_SMALL=nets / pins (the same results; a timing comparison).
+__global__ void k_wa_lean(WaArgs w, float cx, float cy, int forces);
 void launch_wa_small(const WaArgs &w, float cx, float cy, int forces, cudaStream_t s);
 // The degree-2..4 ranges of nets already in degree order.
 WaSmall wa_small_ranges(const int64_t *net_start, int32_t n_nets);

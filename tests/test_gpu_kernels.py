@@ -306,9 +306,10 @@ def test_poisson_errors_against_the_fp64_solve(L, nx, ny):
         assert err(gx.cpu().numpy(), ex64) <= tol and err(gy.cpu().numpy(), ey64) <= tol, mode
 
 
-@pytest.mark.parametrize("form", ["pins", "nets"])
+@pytest.mark.parametrize("form", ["lean", "pins", "nets"])
 def test_wa_small_net_forms_bit_exact(L, form, monkeypatch):
-    """The degree-2..4 nets' two kernels (a lane per pin, the default; a thread per net with
+    """The degree-2..4 nets' three kernels (a thread per net forming the exp terms twice, the
+    default; a lane per pin with GPL_WA_SMALL=pins; a thread per net keeping them with
     GPL_WA_SMALL=nets) against the oracle, bit for bit: most nets of a netlist are of these
     degrees."""
     monkeypatch.setenv("GPL_WA_SMALL", form)

@@ -30,6 +30,9 @@ struct Engine::Region {
   __nv_bfloat16 *dens_split = nullptr;
   int split_ld = 0;
   std::vector<float> np_host, npu_host;  // staging of an update_bins copy
+  unsigned int *spread = nullptr;  // the scatter's spread blocks (cleared by the finalize)
+  int32_t *order = nullptr;        // each device cell's index at upload (since take_order)
+  bool order_moved = false;
 };
 
 static int blocks_for(int64_t n, int per = kThreadsPerBlock) { return (int)std::max<int64_t>(1, (n + per - 1) / per); }
@@ -128,7 +131,7 @@ void Engine::free_globals() {
 void Engine::release() {
   join();
   for (Region *r : regions_) {
-    void *ptrs[] = {r->bx, r->by, r->scaled, r->density, r->fx, r->fy, r->np, r->npu, r->acc_inst, r->acc_fill, r->part, r->ticket};
+    void *ptrs[] = {r->bx, r->by, r->scaled, r->density, r->fx, r->fy, r->np, r->npu, r->acc_inst, r->acc_fill, r->part, r->ticket, r->spread, r->order};
     for (void *p : ptrs)
       if (p) cudaFreeAsync(p, stream_);
     for (int k = 0; k < S_NUM; k++)
@@ -273,6 +276,11 @@ void Engine::upload(const EngineSetup &s) {
     check(dmalloc(&r->part, (size_t)std::max(r->nb_bins * 2, r->nb_cells * 4), st), "alloc partials");
     check(dmalloc(&r->ticket, 1, st), "alloc partials");
     if (!failed()) check(cudaMemsetAsync(r->ticket, 0, sizeof(unsigned int), st), "memset");
+    check(dmalloc(&r->spread, 1, st), "alloc partials");
+    if (!failed()) check(cudaMemsetAsync(r->spread, 0, sizeof(unsigned int), st), "memset");
+    check(dmalloc(&r->order, rs.n_cells, st), "alloc order");
+    if (!failed() && rs.n_cells) k_iota<<<blocks_for(rs.n_cells), kThreadsPerBlock, 0, st>>>((int32_t)rs.n_cells, r->order);
+    r->order_moved = false;
     if (!failed()) {
       cudaError_t pe = cudaSuccess;
       r->plan = poisson_plan_create(rs.nx, rs.ny, rs.wx.data(), rs.wy.data(), poisson_mode_, &pe);
@@ -304,6 +312,7 @@ void Engine::upload(const EngineSetup &s) {
     a.density = r->density;
     a.field_x = r->fx;
     a.field_y = r->fy;
+    a.spread = r->spread;
   }
   check(cudaStreamSynchronize(st), "upload sync");
   h2d_bytes += g_h2d + n_pins_ * 8;
@@ -398,6 +407,11 @@ void Engine::place_at(int b, SlotId slot) {
 void Engine::nesterov_step(int b, float step, float coeff) {
   join();
   if (failed()) return;
+  if (reorder_on_ && host_scal_[b].spread_blocks > 0.01 * regions_[b]->nb_cells) {
+    reorder(b);
+    host_scal_[b].spread_blocks = 0;  // until the next scatter reports
+    if (failed()) return;
+  }
   hpwl_ready_ = hpwl_fetched_ = false;  // the density centres move
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
@@ -604,6 +618,112 @@ void Engine::set_net_weights(const std::vector<float> &w) {
   for (size_t i = 0; i < w.size(); i++) dw[i] = w[net_order_[i]];
   unit_weights_ = std::all_of(dw.begin(), dw.end(), [](float v) { return v == 1.0f; });
   check(cudaMemcpyAsync(net_weight_, dw.data(), dw.size() * sizeof(float), cudaMemcpyHostToDevice, stream_), "net weights");
+}
+
+// The region's cells in a new device order (cell_order.cu): sorted by a coarse Z key of
+// their density centres, stably; every per-cell array gathered through the permutation, the
+// cell-major pin lists moved with their cells (each cell's pins keep their order), the pins'
+// cell indices and slots remapped. Scratch from the device's pool, returned at the end.
+void Engine::reorder(int b) {
+  join();
+  Region *r = regions_[b];
+  const int32_t n = (int32_t)r->n_cells;
+  if (failed() || n < 2) return;
+  cudaStream_t st = stream_;
+  const int64_t off = r->cell_off;
+  uint32_t *key0 = nullptr, *key1 = nullptr;
+  int32_t *idx0 = nullptr, *idx1 = nullptr, *hist = nullptr, *inv = nullptr, *ord = nullptr, *hx = nullptr, *hy = nullptr;
+  int2 *dc = nullptr;
+  float *ds = nullptr, *ar = nullptr;
+  uint8_t *kd = nullptr, *lk = nullptr;
+  int64_t *cnt = nullptr, *tmp = nullptr;
+  float2 *slot[S_NUM] = {};
+  check(dmalloc(&key0, n, st), "reorder");
+  check(dmalloc(&key1, n, st), "reorder");
+  check(dmalloc(&idx0, n, st), "reorder");
+  check(dmalloc(&idx1, n, st), "reorder");
+  check(dmalloc(&hist, (size_t)64 * order_tiles(n), st), "reorder");
+  check(dmalloc(&inv, n, st), "reorder");
+  check(dmalloc(&ord, n, st), "reorder");
+  check(dmalloc(&dc, n, st), "reorder");
+  check(dmalloc(&hx, n, st), "reorder");
+  check(dmalloc(&hy, n, st), "reorder");
+  check(dmalloc(&ds, n, st), "reorder");
+  check(dmalloc(&ar, n, st), "reorder");
+  check(dmalloc(&kd, n, st), "reorder");
+  if (locked_) check(dmalloc(&lk, n, st), "reorder");
+  check(dmalloc(&cnt, (size_t)n + 1, st), "reorder");
+  check(dmalloc(&tmp, scan_i64_tmp(n), st), "reorder");
+  for (int k = 0; k < S_NUM; k++) check(dmalloc(&slot[k], n, st), "reorder");
+  if (!failed()) {
+    const RegionArgs &a = r->args;
+    check(order_sort(n, dc_ + off, a.lx, a.ly, std::max(1.0, (double)(a.ux - a.lx) / 64.0), std::max(1.0, (double)(a.uy - a.ly) / 64.0), key0, idx0, key1, idx1, hist, st), "reorder sort");
+    static_assert(S_NUM <= kMaxSlots, "the gather's slot table");
+    CellGather g{};
+    g.dc = dc_ + off;
+    g.hx = hx_ + off;
+    g.hy = hy_ + off;
+    g.dscale = dscale_ + off;
+    g.area = area_ + off;
+    g.kind = kind_ + off;
+    g.locked = locked_ ? locked_ + off : nullptr;
+    g.pin_start = cell_pin_start_ + off;
+    g.order = r->order;
+    g.dc_out = dc;
+    g.hx_out = hx;
+    g.hy_out = hy;
+    g.dscale_out = ds;
+    g.area_out = ar;
+    g.kind_out = kd;
+    g.locked_out = lk;
+    g.pins_out = cnt;
+    g.inv = inv;
+    g.order_out = ord;
+    g.n_slots = S_NUM;
+    for (int k = 0; k < S_NUM; k++) {
+      g.slot[k] = r->slot[k];
+      g.slot_out[k] = slot[k];
+    }
+    k_order_gather<<<blocks_for(n), kThreadsPerBlock, 0, st>>>(n, idx0, g);
+    check(cudaGetLastError(), "reorder gather");
+    // the new pin starts (relative to the region's first slot), then the pins remapped from
+    // the old starts, then the old starts overwritten
+    check(scan_i64(cnt, n, tmp, st), "reorder scan");
+    if (n_pins_) k_order_pins<<<blocks_for(n_pins_), kThreadsPerBlock, 0, st>>>(n_pins_, (int32_t)off, n, inv, cell_pin_start_ + off, cnt, pin_cell_, pin_slot_);
+    k_order_starts<<<blocks_for(n), kThreadsPerBlock, 0, st>>>(n, cnt, cell_pin_start_ + off);
+    check(cudaGetLastError(), "reorder pins");
+    auto back = [&](auto *dst, const auto *src, size_t elems) { check(cudaMemcpyAsync(dst, src, elems * sizeof(*src), cudaMemcpyDeviceToDevice, st), "reorder copy"); };
+    back(dc_ + off, dc, n);
+    back(hx_ + off, hx, n);
+    back(hy_ + off, hy, n);
+    back(dscale_ + off, ds, n);
+    back(area_ + off, ar, n);
+    back(kind_ + off, kd, n);
+    if (locked_) back(locked_ + off, lk, n);
+    std::swap(r->order, ord);
+    for (int k = 0; k < S_NUM; k++) std::swap(r->slot[k], slot[k]);
+    r->order_moved = true;
+    reorders++;
+    launches += 12;
+  }
+  void *bufs[] = {key0, key1, idx0, idx1, hist, inv, ord, dc, hx, hy, ds, ar, kd, lk, cnt, tmp};
+  for (void *p : bufs)
+    if (p) cudaFreeAsync(p, st);
+  for (int k = 0; k < S_NUM; k++)
+    if (slot[k]) cudaFreeAsync(slot[k], st);
+}
+
+bool Engine::take_order(int b, std::vector<int32_t> &order) {
+  join();
+  Region *r = regions_[b];
+  if (!r->order_moved || failed()) return false;
+  order.resize((size_t)r->n_cells);
+  if (r->n_cells) check(cudaMemcpyAsync(order.data(), r->order, r->n_cells * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_), "take_order");
+  d2h_bytes += r->n_cells * 4;
+  if (r->n_cells) k_iota<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>((int32_t)r->n_cells, r->order);
+  check(cudaStreamSynchronize(stream_), "take_order sync");
+  r->order_moved = false;
+  return !failed();
 }
 
 void Engine::rebuild_poisson(int mode) {

@@ -46,9 +46,10 @@ struct EngineSetup {
 enum SlotId { S_CUR_SLP = 0, S_CUR_SLP_SUM, S_NEXT_SLP, S_NEXT_SLP_SUM, S_PREV_SLP, S_PREV_SLP_SUM, S_CUR, S_NEXT, S_SNAP_CUR, S_SNAP_SLP, S_SNAP_SLP_SUM, S_SNAP_PREV_SLP_SUM, S_NUM };
 
 // Per-region scalars the trial reads back (doubles): the overflow sums of the last scatter,
-// the two |gradient| sums and the two step-length distances of the last gradient update.
+// the two |gradient| sums and the two step-length distances of the last gradient update, and
+// how many blocks of the last scatter found their cells spread past the shared tile.
 struct RegionScalars {
-  double overflow, overflow_u, wl_sum, den_sum, dist1, dist2, pad0, pad1;
+  double overflow, overflow_u, wl_sum, den_sum, dist1, dist2, spread_blocks, pad1;
 };
 
 struct DeviceError {
@@ -100,6 +101,14 @@ class Engine {
   int64_t launches = 0, h2d_bytes = 0, d2h_bytes = 0;  // counters for the run's report
   // The density solvers rebuilt in another mode (0 FP32, 1 split-BF16 tensor cores).
   void rebuild_poisson(int mode);
+  // The region's cells sorted again on the device by their current positions (a coarse Z
+  // order), when the last scatter found more than 1 % of its blocks spread past the shared
+  // tile; on by default ("reorder" option). take_order() gives the upload-time index of each
+  // device cell of the region since the last call (false: unchanged) and starts counting anew.
+  void set_reorder(bool on) { reorder_on_ = on; }
+  void reorder(int b);
+  bool take_order(int b, std::vector<int32_t> &order);
+  int64_t reorders = 0;
   // Per-phase device time (CUDA events on the engine's stream around each launch group).
   enum Phase { PH_PLACE = 0, PH_FINALIZE, PH_POISSON, PH_WA, PH_GRAD, PH_HPWL, PH_COUNT };
   void set_profile(bool on);
@@ -119,6 +128,7 @@ class Engine {
   struct Region;
   int device_ = 0;
   int poisson_mode_ = 1;
+  bool reorder_on_ = true;
   cudaStream_t stream_ = nullptr;
   DeviceError err_{cudaSuccess, ""};
   std::vector<Region *> regions_;

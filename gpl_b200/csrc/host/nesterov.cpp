@@ -1176,8 +1176,24 @@ struct Placer {
     nb.step_length = nb.coordi_distance / grad;
     return nb.step_length;
   }
+  // The host's map of the device's cell order, after the engine sorted cells again.
+  void apply_device_order() {
+    std::vector<int32_t> ord;
+    for (size_t b = 0; b < nbs.size(); b++) {
+      if (!eng.take_order((int)b, ord)) continue;
+      const int64_t off = nbs[b].cell_off;
+      std::vector<int> was(gcell_of_dev.begin() + off, gcell_of_dev.begin() + off + (int64_t)ord.size());
+      for (size_t i = 0; i < ord.size(); i++) {
+        const int g = was[ord[i]];
+        gcell_of_dev[off + i] = g;
+        dev_of_gcell[g] = off + (int64_t)i;
+      }
+    }
+    device_check();
+  }
   // The device's density centres into the host's density boxes.
   void sync_host_centres() {
+    apply_device_order();
     std::vector<int32_t> cx, cy;
     eng.centres(cx, cy);
     device_check();
@@ -2012,7 +2028,7 @@ struct NesterovLoop {
   // One pass of the loop's body; false once the loop has ended.
   bool step(Log &log, const Design &d, Placer &P, Routability *route) {
     if (done || iter >= P.max_iter) return !(done = true);
-    if (iter % 50 == 0) progress("iteration %d: overflow %.4f, %ld trials", iter, (double)P.average_overflow_unscaled, (long)P.trials);
+    if (iter % 50 == 0) progress("iteration %d: overflow %.4f, %ld trials, %ld cell reorders", iter, (double)P.average_overflow_unscaled, (long)P.trials, (long)P.eng.reorders);
     float prev_a = cur_a;
     cur_a = (float)((1.0 + std::sqrt(4.0 * (double)prev_a * (double)prev_a + 1.0)) * 0.5);
     float coeff = (float)(((double)prev_a - 1.0) / (double)cur_a);
@@ -2387,6 +2403,11 @@ int gpl_set_option(gpl_ctx *c, const char *name, const char *value) {
     c->trace = v == "1";
     return 0;
   }
+  if (n == "reorder") {
+    if (v != "0" && v != "1") return -1;
+    c->eng->set_reorder(v == "1");
+    return 0;
+  }
   return -1;
 }
 
@@ -2464,6 +2485,10 @@ int gpl_session_set_option(gpl_session *s, const char *name, const char *value) 
     s->ctx->eng->set_overlap(v != "0");
     return 0;
   }
+  if (n == "reorder") {  // the device cell order kept coherent (1, the default) or fixed (0)
+    s->ctx->eng->set_reorder(v != "0");
+    return 0;
+  }
   return -1;
 }
 
@@ -2473,12 +2498,13 @@ int gpl_session_profile(gpl_session *s, double *ms, int64_t *launches, int cap) 
 
 void *gpl_session_stream(gpl_session *s) { return (void *)s->ctx->eng->stream(); }
 
-void gpl_session_counters(gpl_session *s, int64_t out[5]) {
+void gpl_session_counters(gpl_session *s, int64_t out[6]) {
   out[0] = s->ctx->eng->launches;
   out[1] = s->ctx->eng->h2d_bytes;
   out[2] = s->ctx->eng->d2h_bytes;
   out[3] = s->run->P ? (int64_t)s->run->P->gcell_of_dev.size() : 0;
   out[4] = s->ctx->eng->trials;
+  out[5] = s->ctx->eng->reorders;
 }
 
 void gpl_session_discard(gpl_session *s) {

@@ -682,6 +682,17 @@ cudaError_t IpDevice::upload(const IpSetup &s) {
   return cudaStreamSynchronize(s_);
 }
 
+size_t scan_i64_tmp(int64_t n) { return (size_t)((n + kScanBlock - 1) / kScanBlock + 1); }
+
+cudaError_t scan_i64(int64_t *data, int64_t n, int64_t *tmp, cudaStream_t s) {
+  const int64_t nb = (n + kScanBlock - 1) / kScanBlock;
+  if (nb == 0) return cudaMemsetAsync(data, 0, sizeof(int64_t), s);
+  k_scan_block<<<(unsigned)nb, kScanBlock, 0, s>>>(data, n, tmp);
+  k_scan_totals<<<1, kScanBlock, 0, s>>>(tmp, nb);
+  k_scan_add<<<(unsigned)nb, kScanBlock, 0, s>>>(data, n, tmp, nb);
+  return cudaGetLastError();
+}
+
 cudaError_t IpDevice::scan(int64_t *data, int64_t n) {
   int64_t nb = (n + kScanBlock - 1) / kScanBlock;
   if ((size_t)(nb + 1) > scan_tmp_n_) {

@@ -35,6 +35,11 @@ struct IpSetup {
   float weight_scale = 800.0f;
 };
 
+// Exclusive scan of n int64 in place, data[n] receiving the total; tmp holds scan_i64_tmp(n)
+// int64 (the block totals).
+size_t scan_i64_tmp(int64_t n);
+cudaError_t scan_i64(int64_t *data, int64_t n, int64_t *tmp, cudaStream_t s);
+
 // Raises the current device's stream-ordered pool's release threshold (once per device), so
 // memory freed with cudaFreeAsync stays in the pool for the next allocation instead of being
 // unmapped.

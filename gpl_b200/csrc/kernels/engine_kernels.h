@@ -33,6 +33,9 @@ struct RegionArgs {
   const float *non_place, *non_place_u;  // the fixed areas (int64) as float, as the density reads them
   int64_t *acc_inst, *acc_fill;  // scatter accumulators (cleared by the finalize)
   float *density, *field_x, *field_y;
+  // blocks of the last scatter whose cells spread past the shared tile (NULL: not counted);
+  // the finalize reports the count (out[6]) and clears it
+  unsigned int *spread;
 };
 
 // One region's cells, SoA, region-local index.
@@ -98,6 +101,35 @@ __global__ void k_prev_slp(RegionArgs r, CellArgs c, float coef);
 __global__ void k_hpwl(WaArgs w, unsigned long long *out);
 __global__ void k_hpwl_tiles(WaArgs w, unsigned long long *out);
 __global__ void k_pack_centres(int64_t n, const int32_t *x, const int32_t *y, int2 *out);
+
+// ---- the device cell order (cell_order.cu): a region's cells sorted again by a coarse Z key
+// of their density centres, stably; the per-cell arrays gathered through the permutation.
+constexpr int kMaxSlots = 12;
+struct CellGather {
+  const int2 *dc;
+  const int32_t *hx, *hy;
+  const float *dscale, *area;
+  const uint8_t *kind, *locked;
+  const int64_t *pin_start;  // n + 1
+  const int32_t *order;
+  int2 *dc_out;
+  int32_t *hx_out, *hy_out;
+  float *dscale_out, *area_out;
+  uint8_t *kind_out, *locked_out;
+  int64_t *pins_out;          // each cell's pin count (n, scanned afterwards)
+  int32_t *inv, *order_out;   // old -> new; the upload-time index of each new cell
+  int n_slots;
+  const float2 *slot[kMaxSlots];
+  float2 *slot_out[kMaxSlots];
+};
+int order_tiles(int32_t n);
+// Sorts the cells [0, n) by their coarse Z key (64 x 64 tiles of tile_w x tile_h from (lx, ly));
+// the old indices in new order end in idx0 (key0/key1/idx1: n each; hist: 64 * order_tiles(n)).
+cudaError_t order_sort(int32_t n, const int2 *dc, int32_t lx, int32_t ly, double tile_w, double tile_h, uint32_t *key0, int32_t *idx0, uint32_t *key1, int32_t *idx1, int32_t *hist, cudaStream_t s);
+__global__ void k_order_gather(int32_t n, const int32_t *perm, CellGather g);
+__global__ void k_order_pins(int64_t n_pins, int32_t off, int32_t n, const int32_t *inv, const int64_t *old_start, const int64_t *new_start, int32_t *pin_cell, int32_t *pin_slot);
+__global__ void k_order_starts(int32_t n, const int64_t *rel, int64_t *start);
+__global__ void k_iota(int32_t n, int32_t *a);
 
 // Whether a grid's bins are small enough for the scatter's 32-bit shared tile.
 bool narrow_tile(const std::vector<int32_t> &bx, const std::vector<int32_t> &by);

@@ -141,6 +141,7 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
   const bool narrow = r.narrow != 0;
   unsigned int *t32 = reinterpret_cast<unsigned int *>(s_tile);
   if (!tile) {
+    if (threadIdx.x == 0 && r.spread) atomicAdd(r.spread, 1u);
     if (any) {
       unsigned long long *acc = (unsigned long long *)(kind == CELL_FILLER ? r.acc_fill : r.acc_inst);
       for (int32_t y = y0; y < y1; y++)
@@ -259,8 +260,15 @@ __global__ void __launch_bounds__(kThreads) k_bins_finalize(RegionArgs r, double
     partials[2 * blockIdx.x] = a;
     partials[2 * blockIdx.x + 1] = b;
   }
-  // the last block to finish sums the blocks' partials (the overflow sums)
-  if (last_block_done(ticket)) reduce_rows<kThreads>(partials, gridDim.x, 2, out, sh);
+  // the last block to finish sums the blocks' partials (the overflow sums) and reports the
+  // scatter's spread blocks
+  if (last_block_done(ticket)) {
+    reduce_rows<kThreads>(partials, gridDim.x, 2, out, sh);
+    if (threadIdx.x == 0 && r.spread) {
+      out[6] = (double)*r.spread;
+      *r.spread = 0u;
+    }
+  }
 }
 
 // ---- WA wirelength (updateWireLengthForceWA :2325-2388 + getWireLengthGradientPinWA

@@ -161,9 +161,9 @@ class Session:
         return {PHASES[i]: (ms[i], n[i]) for i in range(k)}
 
     def counters(self):
-        out = (C.c_int64 * 5)()
+        out = (C.c_int64 * 6)()
         _session_lib().gpl_session_counters(self._h, out)
-        return {"launches": out[0], "h2d_bytes": out[1], "d2h_bytes": out[2], "cells": out[3], "trials": out[4]}
+        return {"launches": out[0], "h2d_bytes": out[1], "d2h_bytes": out[2], "cells": out[3], "trials": out[4], "reorders": out[5]}
 
     @property
     def stream(self):

@@ -156,6 +156,9 @@ void gpl_destroy(gpl_ctx *ctx);
 /* Engine options with no reference counterpart (the reference runs on one thread):
  *   "poisson" = "mixed" (split-BF16 tcgen05 DCT GEMMs, the default) | "fp32" (SIMT GEMMs)
  *   "trace"   = "0" | "1" (probe lines, as the reference's `Log.trace`)
+ *   "reorder" = "1" (the default) | "0": the device's cell order sorted again by position when
+ *               the cells have moved apart (no result depends on the order but the double sums'
+ *               last bits), or kept as uploaded
  * Returns 0, or -1 for an unknown name or value. */
 int gpl_set_option(gpl_ctx *ctx, const char *name, const char *value);
 
@@ -178,15 +181,17 @@ gpl_session *gpl_session_open(gpl_ctx *ctx, const gpl_design_t *design, int argc
                               const char *const *argv, const gpl_router_t *router);
 int gpl_session_iterate(gpl_session *s, int n, int *done);
 /* "poisson" = "mixed" | "fp32" (solvers rebuilt, the field recomputed); "profile" = "0" | "1"
- * (per-phase device time from CUDA events). No reference counterpart. */
+ * (per-phase device time from CUDA events); "overlap" = "1" | "0" (the WA beside the density
+ * solve or after it); "reorder" as gpl_set_option's. No reference counterpart. */
 int gpl_session_set_option(gpl_session *s, const char *name, const char *value);
 /* Per-phase device milliseconds and launch counts since "profile" was set: scatter, bin
  * finalize, density solve, WA, gradients, HPWL. Returns the number of phases written. */
 int gpl_session_profile(gpl_session *s, double *ms, int64_t *launches, int cap);
 /* Kernel launches, host-to-device and device-to-host bytes since the session opened, the
- * Nesterov cells (instances and fillers) on the device, and the back-tracking trials run
- * (`do_back_tracking`'s passes, src/nesterov.rs:2776-2808) since the session opened (5 int64). */
-void gpl_session_counters(gpl_session *s, int64_t out[5]);
+ * Nesterov cells (instances and fillers) on the device, the back-tracking trials run
+ * (`do_back_tracking`'s passes, src/nesterov.rs:2776-2808) and the times the engine sorted its
+ * device cells again (the "reorder" option) since the session opened (6 int64). */
+void gpl_session_counters(gpl_session *s, int64_t out[6]);
 /* The session's CUDA stream (cudaStream_t), for timing with events on it. */
 void *gpl_session_stream(gpl_session *s);
 int gpl_session_close(gpl_session *s, gpl_result_t *out);

@@ -96,3 +96,29 @@ def test_routability_at_100k_cells_matches_the_oracle():
     assert abs(area[0] - rarea[0]) <= 0.005 * rarea[0]
     assert abs(got["final_hpwl"] - ref["final_hpwl"]) <= 0.01 * ref["final_hpwl"]
     assert abs(got["final_overflow"] - ref["final_overflow"]) <= 0.005
+
+
+def test_cell_reorder_keeps_the_run():
+    """The device's cell order sorted again as cells move (the default) against the order kept
+    as uploaded, on the 100k-cell design from the generator's spread placement (where cells
+    move furthest): the engine must have sorted its cells at least once, and both runs place
+    the design with final HPWL within 0.1 % and overflow within 0.005 of each other (no
+    per-cell result depends on the order; only the double sums' last bits do)."""
+    d = synth.generate("cfg2", placed=True)
+    args = ["-density", "0.70", "-bin_grid_count", "512", "-skip_initial_place"]
+    runs = {}
+    for on in ("1", "0"):
+        placer = engine.Placer(0)
+        placer.set_option("reorder", on)
+        s = engine.Session(placer, d, args)
+        while not s.done:
+            s.iterate(100)
+        reorders = s.counters()["reorders"]
+        runs[on] = (s.close(), reorders)
+        placer.close()
+    (a, na), (b, nb) = runs["1"], runs["0"]
+    print("reorders", na, nb, "hpwl", a["final_hpwl"], b["final_hpwl"], "iterations", a["nesterov_iterations"], b["nesterov_iterations"])
+    assert na >= 1 and nb == 0
+    assert a["status"] == b["status"] == "placed"
+    assert abs(a["final_hpwl"] - b["final_hpwl"]) <= 1e-3 * b["final_hpwl"]
+    assert abs(a["final_overflow"] - b["final_overflow"]) <= 0.005

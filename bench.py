@@ -260,6 +260,7 @@ def ours(a):
     design, args = loop_design(a)
     log("design generated")
     placer = engine.Placer(local, a.form)
+    placer.set_option("reorder", a.reorder)
     sess = engine.Session(placer, design, args)
     log("session open")
     sess.iterate(a.warmup)
@@ -469,6 +470,7 @@ def main():
                     help="run the command through the initial placement once and print its time (a profiling case)")
     ap.add_argument("--save-placement", default="", help="with --initial-place-only: save the locations (.npy)")
     ap.add_argument("--start-from", default="", help="start the loop from saved initial-placement locations (a profiling case)")
+    ap.add_argument("--reorder", default="1", choices=["0", "1"], help="keep the device's cell order coherent as cells move (the default) or as uploaded")
     a = ap.parse_args()
     if a.warmup < 3:
         a.warmup = 3

@@ -88,6 +88,10 @@ __device__ __forceinline__ int32_t centre(const int4 &b, int axis) { return axis
 
 // One net's pairs in the host's order (the second pin from the second solve pin on, the first
 // below it; x then y): counted (EMIT false) or written at the net's offsets (EMIT true).
+// A pair counts on an axis only when one of its pins is that axis's extreme, so a second pin
+// that is no extreme pairs only with the net's extreme pins: for it the first pin runs over
+// the (at most four) extremes below it, in index order, instead of every pin below it; the
+// pairs visited, and their order, are the reference's, in O(degree) per net.
 template <bool EMIT>
 __device__ void net_pairs(const IpArgs &a, int n, int64_t *cnt, int64_t stride, const AxisOut *out) {
   int64_t b = a.net_start[n], e = a.net_start[n + 1];
@@ -103,9 +107,18 @@ __device__ void net_pairs(const IpArgs &a, int n, int64_t *cnt, int64_t stride, 
   int64_t tc[2] = {0, 0}, rc[2] = {0, 0};
   if (deg > 1 && deg < a.max_fanout) {
     float net_weight = __fdiv_rn(a.weight_scale, (float)(deg - 1));
+    // the net's extreme pins (a pin flagged on any side), in index order; at most four
+    int64_t ext[4];
+    int n_ext = 0;
+    for (int64_t k = b; k < e && n_ext < 4; k++)
+      if (a.pin_flag[k]) ext[n_ext++] = k;
     for (int64_t k1 = b; k1 < e; k1++) {
       if (a.pin_mio[k1]) continue;
-      for (int64_t k2 = b; k2 < k1; k2++) {
+      const bool k1_ext = a.pin_flag[k1] != 0;
+      const int64_t n2 = k1_ext ? k1 - b : (int64_t)n_ext;
+      for (int64_t j = 0; j < n2; j++) {
+        const int64_t k2 = k1_ext ? b + j : ext[j];
+        if (k2 >= k1) break;  // the extremes are in index order
         if (a.pin_mio[k2]) continue;
         if (a.pin_inst[k1] == a.pin_inst[k2]) continue;
         uint8_t f = a.pin_flag[k1] | a.pin_flag[k2];
@@ -677,7 +690,7 @@ cudaError_t IpDevice::upload(const IpSetup &s) {
     CK(alloc(&a.x, n_, s_));
   }
   // the two axes' solver scratch, side by side (256-byte aligned halves)
-  scratch_bytes_ = (bicgstab_scratch_bytes(n_) + 255) / 256 * 256;
+  scratch_bytes_ = (bicgstab_pair_scratch_bytes(n_) + 255) / 256 * 256;
   CK(cudaMallocAsync(&scratch_, 2 * scratch_bytes_, s_));
   return cudaStreamSynchronize(s_);
 }

@@ -47,19 +47,26 @@ __device__ __forceinline__ double loop_state(const double *S) {
 constexpr int kSpmvTile = 6144;
 constexpr int kSpmvUnroll = 8;
 
+// Each form hands every row it forms to emit(row, value), at most one row per thread, and
+// returns nowhere early, so a block-wide step may follow.
+template <class Emit>
+__device__ __forceinline__ void spmv_rows_rows(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, Emit emit) {
+  const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
+  if (i < n) {
+    float tmp = 0.0f;
+    const int64_t b = rs[i], e = rs[i + 1];
+    for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, __fmul_rn(vals[k], x[cols[k]]));
+    emit(i, __fadd_rn(0.0f, __fmul_rn(1.0f, tmp)));
+  }
+}
 __device__ __forceinline__ void spmv_rows_body(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
   if (gated_off(S, gate)) return;
-  const int64_t i = blockIdx.x * (int64_t)kThreads + threadIdx.x;
-  if (i >= n) return;
-  float tmp = 0.0f;
-  const int64_t b = rs[i], e = rs[i + 1];
-  for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, __fmul_rn(vals[k], x[cols[k]]));
-  y[i] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
+  spmv_rows_rows(n, rs, cols, vals, x, [&](int64_t r, float v) { y[r] = v; });
 }
 __global__ void __launch_bounds__(kThreads) k_spmv_rows(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) { spmv_rows_body(n, rs, cols, vals, x, y, S, gate); }
 
-__device__ __forceinline__ void spmv_tiled_body(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
-  if (gated_off(S, gate)) return;
+template <class Emit>
+__device__ __forceinline__ void spmv_tiled_rows(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, Emit emit) {
   __shared__ float prod[kSpmvTile];
   const int64_t r0 = blockIdx.x * (int64_t)kThreads;
   const int64_t r1 = min(n, r0 + (int64_t)kThreads);
@@ -94,15 +101,20 @@ __device__ __forceinline__ void spmv_tiled_body(int64_t n, const int64_t *__rest
     }
   }
   __syncthreads();
-  if (i >= n) return;
-  float tmp = 0.0f;
-  if (tiled) {
-    const int lb = (int)(b - k0), le = (int)(e - k0);
-    for (int k = lb; k < le; k++) tmp = __fadd_rn(tmp, prod[k]);
-  } else {
-    for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, __fmul_rn(vals[k], x[cols[k]]));
+  if (i < n) {
+    float tmp = 0.0f;
+    if (tiled) {
+      const int lb = (int)(b - k0), le = (int)(e - k0);
+      for (int k = lb; k < le; k++) tmp = __fadd_rn(tmp, prod[k]);
+    } else {
+      for (int64_t k = b; k < e; k++) tmp = __fadd_rn(tmp, __fmul_rn(vals[k], x[cols[k]]));
+    }
+    emit(i, __fadd_rn(0.0f, __fmul_rn(1.0f, tmp)));
   }
-  y[i] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
+}
+__device__ __forceinline__ void spmv_tiled_body(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
+  if (gated_off(S, gate)) return;
+  spmv_tiled_rows(n, rs, cols, vals, x, [&](int64_t r, float v) { y[r] = v; });
 }
 __global__ void __launch_bounds__(kThreads) k_spmv_tiled(int64_t n, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) { spmv_tiled_body(n, rs, cols, vals, x, y, S, gate); }
 
@@ -116,12 +128,12 @@ __global__ void __launch_bounds__(kThreads) k_spmv_tiled(int64_t n, const int64_
 constexpr int kLongChunks = 4;
 __host__ __device__ __forceinline__ int64_t sliced_long_blocks(int64_t n_long) { return (n_long + kThreads / 32 - 1) / (kThreads / 32); }
 __host__ __device__ __forceinline__ int64_t sliced_blocks(int64_t n, int64_t n_long) { return sliced_long_blocks(n_long) + (n - n_long + kThreads - 1) / kThreads; }
-__device__ __forceinline__ void spmv_sliced_body(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int2 *__restrict__ sl_ent, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
-  if (gated_off(S, gate)) return;
+template <class Emit>
+__device__ __forceinline__ void spmv_sliced_rows(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int2 *__restrict__ sl_ent, const float *__restrict__ x, Emit emit) {
   const int64_t lb = sliced_long_blocks(n_long);
   if (blockIdx.x < lb) {
     const int64_t w = blockIdx.x * (int64_t)(kThreads / 32) + (threadIdx.x >> 5);
-    if (w >= n_long) return;  // the whole warp
+    if (w >= n_long) return;  // the whole warp; such a warp forms no row
     const int lane = threadIdx.x & 31;
     const int32_t row = sl_row[w];
     const int64_t b = rs[row], e = rs[row + 1];
@@ -146,7 +158,7 @@ __device__ __forceinline__ void spmv_sliced_body(int64_t n, int64_t n_long, cons
         }
       }
     }
-    if (lane == 0) y[row] = __fadd_rn(0.0f, __fmul_rn(1.0f, sum));
+    if (lane == 0) emit(row, __fadd_rn(0.0f, __fmul_rn(1.0f, sum)));
     return;
   }
   const int64_t i = (blockIdx.x - lb) * (int64_t)kThreads + threadIdx.x;  // short position
@@ -171,7 +183,11 @@ __device__ __forceinline__ void spmv_sliced_body(int64_t n, int64_t n_long, cons
     const int2 cv = __ldg(ent + (int64_t)k * kSliceRows);
     tmp = __fadd_rn(tmp, __fmul_rn(__int_as_float(cv.y), __ldg(x + cv.x)));
   }
-  y[sl_row[j]] = __fadd_rn(0.0f, __fmul_rn(1.0f, tmp));
+  emit(sl_row[j], __fadd_rn(0.0f, __fmul_rn(1.0f, tmp)));
+}
+__device__ __forceinline__ void spmv_sliced_body(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int2 *__restrict__ sl_ent, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
+  if (gated_off(S, gate)) return;
+  spmv_sliced_rows(n, n_long, rs, cols, vals, sl_row, sl_len, sl_start, sl_ent, x, [&](int64_t r, float v) { y[r] = v; });
 }
 __global__ void __launch_bounds__(kThreads) k_spmv_sliced(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int2 *__restrict__ sl_ent, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) { spmv_sliced_body(n, n_long, rs, cols, vals, sl_row, sl_len, sl_start, sl_ent, x, y, S, gate); }
 
@@ -425,6 +441,7 @@ struct SysDev {
   float *x, *r, *r0, *v, *p, *s, *t;
   double *part, *S;
   unsigned int *ticket;
+  double *spart;  // the fused SpMV launches' block partials (3 per block)
 };
 struct SysPair {
   SysDev a[2];
@@ -435,27 +452,62 @@ __global__ void __launch_bounds__(kThreads) k2_update_p(SysPair P) {
   SysDev q = pick(P);
   update_p_body(q.n, q.S, q.r, q.v, q.p);
 }
-// sel 0: v = A p; sel 1: t = A s
-__global__ void __launch_bounds__(kThreads) k2_spmv_rows(SysPair P, int sel) {
-  SysDev q = pick(P);
-  spmv_rows_body(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
+// sel 0: v = A p (then r0.v and alpha); sel 1: t = A s (then t.t, t.s and omega).
+// The SpMV with the iteration's inner products that follow it, in one launch: each thread's
+// row (if it formed one) adds its terms to the block's partials (sel 0: r0.v; sel 1: t.t and
+// t.s), and the last block to finish takes the scalar step (alpha, or omega). The sums are
+// those of k2_dots, in another fixed order.
+__device__ __forceinline__ void pair_dots_tail(const SysDev &q, int sel, bool have, int64_t row, float val) {
+  __shared__ double sh[kThreads / 32];
+  double d0 = 0.0, d1 = 0.0;
+  if (have) {
+    if (sel == 0) {
+      d0 = (double)q.r0[row] * (double)val;
+    } else {
+      d0 = (double)val * (double)val;
+      d1 = (double)val * (double)q.s[row];
+    }
+  }
+  const double t0 = block_sum<kThreads>(d0, sh);
+  const double t1 = block_sum<kThreads>(d1, sh);
+  if (threadIdx.x == 0) {
+    q.spart[3 * blockIdx.x] = t0;
+    q.spart[3 * blockIdx.x + 1] = t1;
+    q.spart[3 * blockIdx.x + 2] = 0.0;
+  }
+  if (last_block(q.ticket)) scalar_step(q.spart, gridDim.x, q.S, sel ? 2 : 1, 0, sh);
 }
-__global__ void __launch_bounds__(kThreads) k2_spmv_tiled(SysPair P, int sel) {
+__global__ void __launch_bounds__(kThreads) k2_spmv_rows_dots(SysPair P, int sel) {
   SysDev q = pick(P);
-  spmv_tiled_body(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
+  if (gated_off(q.S, kLive)) return;  // the whole system
+  float *y = sel ? q.t : q.v;
+  bool have = false;
+  int64_t row = 0;
+  float val = 0.0f;
+  spmv_rows_rows(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, [&](int64_t r, float v) { y[r] = v; have = true; row = r; val = v; });
+  pair_dots_tail(q, sel, have, row, val);
 }
-__global__ void __launch_bounds__(kThreads) k2_spmv_sliced(SysPair P, int sel) {
+__global__ void __launch_bounds__(kThreads) k2_spmv_tiled_dots(SysPair P, int sel) {
   SysDev q = pick(P);
-  spmv_sliced_body(q.n, q.sl_long, q.rs, q.cols, q.vals, q.sl_row, q.sl_len, q.sl_start, q.sl_ent, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
+  if (gated_off(q.S, kLive)) return;
+  float *y = sel ? q.t : q.v;
+  bool have = false;
+  int64_t row = 0;
+  float val = 0.0f;
+  spmv_tiled_rows(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, [&](int64_t r, float v) { y[r] = v; have = true; row = r; val = v; });
+  pair_dots_tail(q, sel, have, row, val);
 }
-// sel 0: r0.v, then alpha; sel 1: t.t and t.s, then omega
-__global__ void k2_dots(SysPair P, int sel) {
+__global__ void __launch_bounds__(kThreads) k2_spmv_sliced_dots(SysPair P, int sel) {
   SysDev q = pick(P);
-  if (sel == 0)
-    dots_body(q.n, q.r0, q.v, nullptr, nullptr, nullptr, nullptr, q.part, q.S, kLive, 1, q.ticket);
-  else
-    dots_body(q.n, q.t, q.t, q.t, q.s, nullptr, nullptr, q.part, q.S, kLive, 2, q.ticket);
+  if (gated_off(q.S, kLive)) return;
+  float *y = sel ? q.t : q.v;
+  bool have = false;
+  int64_t row = 0;
+  float val = 0.0f;
+  spmv_sliced_rows(q.n, q.sl_long, q.rs, q.cols, q.vals, q.sl_row, q.sl_len, q.sl_start, q.sl_ent, sel ? q.s : q.p, [&](int64_t r, float v) { y[r] = v; have = true; row = r; val = v; });
+  pair_dots_tail(q, sel, have, row, val);
 }
+
 __global__ void __launch_bounds__(kThreads) k2_update_s(SysPair P) {
   SysDev q = pick(P);
   update_s_body(q.n, q.S, q.r, q.v, q.s);
@@ -487,6 +539,14 @@ size_t bicgstab_scratch_bytes(int64_t n) {
   size_t vec = (size_t)n * sizeof(float);
   vec = (vec + 255) / 256 * 256;
   return 7 * vec + (size_t)kBicgBlocks * 3 * sizeof(double) + 64 * sizeof(double);
+}
+
+// The fused SpMV launches' block partials after the single solve's scratch: 3 doubles for
+// each block any SpMV form launches (the sliced form's long rows take a block per 8 rows).
+static size_t pair_spart_offset(int64_t n) { return (bicgstab_scratch_bytes(n) + 255) / 256 * 256; }
+size_t bicgstab_pair_scratch_bytes(int64_t n) {
+  const int64_t blocks = (n + 7) / 8 + (n + kThreads - 1) / kThreads + 1;
+  return pair_spart_offset(n) + (size_t)blocks * 3 * sizeof(double);
 }
 
 cudaError_t csr_slice_order(const CsrDev &A, int32_t *row, int32_t *len, int32_t *count, cudaStream_t st) {
@@ -654,6 +714,7 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
     q.part = (double *)(base + 7 * vec);
     q.S = q.part + (size_t)kBicgBlocks * 3;
     q.ticket = (unsigned int *)(q.S + S_TICKET);
+    q.spart = (double *)(base + pair_spart_offset(n));
   }
   auto ax_of = [&](int a) { return (float *)((char *)scratch[a] + 6 * vec); };
   int eb = (int)((n + kThreads - 1) / kThreads);
@@ -719,21 +780,15 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
   for (;;) {
     for (int k = 0; k < kBicgBatch; k++) {
       k2_update_p<<<ge, kThreads, 0, st>>>(P);
-      if (form == kSpmvSliced)
-        k2_spmv_sliced<<<gs, kThreads, 0, st>>>(P, 0);
-      else if (form == kSpmvTiled)
-        k2_spmv_tiled<<<ge, kThreads, 0, st>>>(P, 0);
-      else
-        k2_spmv_rows<<<ge, kThreads, 0, st>>>(P, 0);
-      k2_dots<<<gr, kThreads, 0, st>>>(P, 0);
-      k2_update_s<<<ge, kThreads, 0, st>>>(P);
-      if (form == kSpmvSliced)
-        k2_spmv_sliced<<<gs, kThreads, 0, st>>>(P, 1);
-      else if (form == kSpmvTiled)
-        k2_spmv_tiled<<<ge, kThreads, 0, st>>>(P, 1);
-      else
-        k2_spmv_rows<<<ge, kThreads, 0, st>>>(P, 1);
-      k2_dots<<<gr, kThreads, 0, st>>>(P, 1);
+      for (int sel = 0; sel < 2; sel++) {
+        if (form == kSpmvSliced)
+          k2_spmv_sliced_dots<<<gs, kThreads, 0, st>>>(P, sel);
+        else if (form == kSpmvTiled)
+          k2_spmv_tiled_dots<<<ge, kThreads, 0, st>>>(P, sel);
+        else
+          k2_spmv_rows_dots<<<ge, kThreads, 0, st>>>(P, sel);
+        if (sel == 0) k2_update_s<<<ge, kThreads, 0, st>>>(P);
+      }
       k2_update_xr<<<gr, kThreads, 0, st>>>(P);
     }
     if ((e = pull()) != cudaSuccess) return e;

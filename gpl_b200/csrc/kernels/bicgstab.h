@@ -60,8 +60,10 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
 // y = A x in the given form (SpmvForm).
 cudaError_t spmv(const CsrDev &A, const float *x, float *y, int form, cudaStream_t s);
 // Two systems of the same size solved side by side (each launch carries both): each takes
-// exactly the steps, and gives exactly the result, of bicgstab_solve on its own; scratch[a]
-// holds bicgstab_scratch_bytes(n) bytes for system a.
+// the steps of bicgstab_solve on its own, each SpMV launch also forming the inner products
+// that follow it (the same sums in another fixed order); scratch[a] holds
+// bicgstab_pair_scratch_bytes(n) bytes for system a.
+size_t bicgstab_pair_scratch_bytes(int64_t n);
 cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], float *const x[2], int max_iters, void *const scratch[2], cudaStream_t s, BicgResult out[2], int spmv = kSpmvRows);
 // The fastest SpMV form for A, timed on the device (a few products of x into the scratch);
 // the sliced form competes when A carries its sliced copy.

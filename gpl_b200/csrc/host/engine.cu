@@ -33,6 +33,9 @@ struct Engine::Region {
   unsigned int *spread = nullptr;  // the scatter's spread blocks (cleared by the finalize)
   int32_t *order = nullptr;        // each device cell's index at upload (since take_order)
   bool order_moved = false;
+  double spread_base = 0;          // the spread blocks of the order as made
+  bool need_base = true;           // the next scatter's count is that base
+  int64_t reorder_trial = -1000;   // the trial of the last reorder
 };
 
 static int blocks_for(int64_t n, int per = kThreadsPerBlock) { return (int)std::max<int64_t>(1, (n + per - 1) / per); }
@@ -407,10 +410,21 @@ void Engine::place_at(int b, SlotId slot) {
 void Engine::nesterov_step(int b, float step, float coeff) {
   join();
   if (failed()) return;
-  if (reorder_on_ && host_scal_[b].spread_blocks > 0.01 * regions_[b]->nb_cells) {
-    reorder(b);
-    host_scal_[b].spread_blocks = 0;  // until the next scatter reports
-    if (failed()) return;
+  {
+    // the cells sorted again when the blocks that spread past the scatter's shared tile have
+    // grown by 2 % of the blocks since the order was made (its own spread, in sparse patches,
+    // is its base), at most once in 8 trials
+    Region *rg = regions_[b];
+    const double sp = host_scal_[b].spread_blocks;
+    if (rg->need_base) {
+      rg->spread_base = sp;
+      rg->need_base = false;
+    } else if (reorder_on_ && trials - rg->reorder_trial >= 8 && sp > rg->spread_base + 0.02 * rg->nb_cells) {
+      reorder(b);
+      rg->reorder_trial = trials;
+      rg->need_base = true;
+      if (failed()) return;
+    }
   }
   hpwl_ready_ = hpwl_fetched_ = false;  // the density centres move
   Region *r = regions_[b];
@@ -620,7 +634,7 @@ void Engine::set_net_weights(const std::vector<float> &w) {
   check(cudaMemcpyAsync(net_weight_, dw.data(), dw.size() * sizeof(float), cudaMemcpyHostToDevice, stream_), "net weights");
 }
 
-// The region's cells in a new device order (cell_order.cu): sorted by a coarse Z key of
+// The region's cells in a new device order (cell_order.cu): sorted by the Hilbert index of
 // their density centres, stably; every per-cell array gathered through the permutation, the
 // cell-major pin lists moved with their cells (each cell's pins keep their order), the pins'
 // cell indices and slots remapped. Scratch from the device's pool, returned at the end.
@@ -657,7 +671,7 @@ void Engine::reorder(int b) {
   for (int k = 0; k < S_NUM; k++) check(dmalloc(&slot[k], n, st), "reorder");
   if (!failed()) {
     const RegionArgs &a = r->args;
-    check(order_sort(n, dc_ + off, a.lx, a.ly, std::max(1.0, (double)(a.ux - a.lx) / 64.0), std::max(1.0, (double)(a.uy - a.ly) / 64.0), key0, idx0, key1, idx1, hist, st), "reorder sort");
+    check(order_sort(n, dc_ + off, a.lx, a.ly, std::max(1.0, (double)(a.ux - a.lx) / 1024.0), std::max(1.0, (double)(a.uy - a.ly) / 1024.0), key0, idx0, key1, idx1, hist, st), "reorder sort");
     static_assert(S_NUM <= kMaxSlots, "the gather's slot table");
     CellGather g{};
     g.dc = dc_ + off;

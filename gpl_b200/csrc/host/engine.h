@@ -101,9 +101,9 @@ class Engine {
   int64_t launches = 0, h2d_bytes = 0, d2h_bytes = 0;  // counters for the run's report
   // The density solvers rebuilt in another mode (0 FP32, 1 split-BF16 tensor cores).
   void rebuild_poisson(int mode);
-  // The region's cells sorted again on the device by their current positions (a coarse Z
-  // order), when the last scatter found more than 1 % of its blocks spread past the shared
-  // tile; on by default ("reorder" option). take_order() gives the upload-time index of each
+  // The region's cells sorted again on the device by their current positions (a Hilbert
+  // order), when the blocks the scatter finds spread past its shared tile have grown by 2 % of
+  // the blocks since the order was made; on by default ("reorder" option). take_order() gives the upload-time index of each
   // device cell of the region since the last call (false: unchanged) and starts counting anew.
   void set_reorder(bool on) { reorder_on_ = on; }
   void reorder(int b);

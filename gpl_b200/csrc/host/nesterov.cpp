@@ -1887,17 +1887,27 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
   EngineSetup s;
   P.dev_of_gcell.assign(P.gcells.size(), -1);
   P.gcell_of_dev.clear();
-  // Device order: each region's cells along a Z-order curve of their density centres over
-  // its bin grid, so a warp's and a block's cells lie close together (their bins and their
-  // pins' cells share cache lines and shared-memory tiles). The order is the device's only:
-  // the region's own cell order (nb.cells) is kept for everything the reference orders by.
-  auto spread = [](uint32_t v) {
-    uint64_t x = v & 0xffff;
-    x = (x | (x << 8)) & 0x00ff00ff;
-    x = (x | (x << 4)) & 0x0f0f0f0f;
-    x = (x | (x << 2)) & 0x33333333;
-    x = (x | (x << 1)) & 0x55555555;
-    return x;
+  // Device order: each region's cells along a Hilbert curve of their density centres over
+  // its bin grid (1/16 bin steps), so a warp's and a block's cells lie close together (their
+  // bins and their pins' cells share cache lines and shared-memory tiles); a Hilbert curve's
+  // runs stay compact where a Z curve's jump across quadrant seams. The order is the
+  // device's only: the region's own cell order (nb.cells) is kept for everything the
+  // reference orders by. The engine sorts the cells again as they move (Engine::reorder).
+  auto hilbert = [](uint32_t x, uint32_t y) {
+    const uint32_t n = 1u << 16;
+    uint64_t d = 0;
+    for (uint32_t q = n >> 1; q > 0; q >>= 1) {
+      const uint32_t rx = (x & q) ? 1u : 0u, ry = (y & q) ? 1u : 0u;
+      d += (uint64_t)q * q * ((3u * rx) ^ ry);
+      if (ry == 0) {
+        if (rx == 1) {
+          x = n - 1 - x;
+          y = n - 1 - y;
+        }
+        std::swap(x, y);
+      }
+    }
+    return d;
   };
   for (auto &nb : P.nbs) {
     nb.cell_off = (int64_t)P.gcell_of_dev.size();
@@ -1905,10 +1915,10 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
     keyed.reserve(nb.cells.size());
     for (int gi : nb.cells) {
       const GCell &g = P.gcells[gi];
-      double fx = ((double)g.d_cx() - nb.bg.lx) / std::max(nb.bg.size_x, 1.0);
-      double fy = ((double)g.d_cy() - nb.bg.ly) / std::max(nb.bg.size_y, 1.0);
+      double fx = 16.0 * ((double)g.d_cx() - nb.bg.lx) / std::max(nb.bg.size_x, 1.0);
+      double fy = 16.0 * ((double)g.d_cy() - nb.bg.ly) / std::max(nb.bg.size_y, 1.0);
       uint32_t qx = (uint32_t)std::min(std::max(fx, 0.0), 65535.0), qy = (uint32_t)std::min(std::max(fy, 0.0), 65535.0);
-      keyed.push_back({spread(qx) | (spread(qy) << 1), gi});
+      keyed.push_back({hilbert(qx, qy), gi});
     }
     std::stable_sort(keyed.begin(), keyed.end(), [](const std::pair<uint64_t, int> &a, const std::pair<uint64_t, int> &b) { return a.first < b.first; });
     for (auto &kv : keyed) {
@@ -1916,7 +1926,7 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
       P.gcell_of_dev.push_back(kv.second);
     }
   }
-  progress("  device set-up: cells in Z order");
+  progress("  device set-up: cells in Hilbert order");
   size_t n = P.gcell_of_dev.size();
   s.hx.resize(n);
   s.hy.resize(n);

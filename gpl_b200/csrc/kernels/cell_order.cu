@@ -5,10 +5,11 @@
 // reads the same bins' fields. The order is a Z curve over the cells' positions when the
 // design is uploaded; as the loop moves cells (most of all from a spread start, where the
 // wirelength forces pull every cell toward its nets) a block's cells drift apart and the
-// scatter falls back to global atomics. When the scatter reports that, the engine sorts the
-// region's cells again by a coarse Z key of their current density centres (64 x 64 super-tiles
-// of bins), stably, so the sort is deterministic: two LSD passes of 6-bit digits, each a
-// per-tile digit histogram, one exclusive scan, and a stable scatter that ranks a tile's
+// scatter falls back to smaller tiles and global atomics. When the scatter reports that, the
+// engine sorts the region's cells again by the Hilbert index of their current density centres
+// on a 1024 x 1024 grid over the region, stably, so the sort is deterministic: four LSD passes
+// of 6-bit digits, each a per-tile digit histogram, one exclusive scan, and a stable scatter
+// that ranks a tile's
 // elements in input order (a warp's items round by round, lanes with the same digit ranked by
 // a warp match). Then every per-cell array is gathered through the permutation and the pins'
 // cell indices and cell-major slots are remapped. Nothing computed per cell depends on the
@@ -25,12 +26,29 @@ constexpr int kTile = kThreads * kItems;        // 2048
 constexpr int kDigits = 64;                     // 6-bit digits
 constexpr int kWarps = kThreads / 32;
 
-__device__ __forceinline__ uint32_t spread6(uint32_t v) {  // 6 bits to the even bits of 12
-  v &= 63u;
-  v = (v | (v << 4)) & 0x30Fu;
-  v = (v | (v << 2)) & 0x333u;
-  v = (v | (v << 1)) & 0x555u;
-  return v;
+constexpr int kOrderBits = 10;                  // the Hilbert grid: 1024 x 1024 cells of the region
+constexpr int kPasses = (2 * kOrderBits + 5) / 6;  // 6-bit digits of the 20-bit key (even: 4)
+static_assert(kPasses % 2 == 0, "the sorted pairs end where they started");
+
+// The distance of (x, y) along the Hilbert curve over a 2^kOrderBits square: any run of it
+// lies in a compact patch, unlike a Z curve, whose runs jump across quadrant seams.
+__device__ __forceinline__ uint32_t hilbert(uint32_t x, uint32_t y) {
+  constexpr uint32_t n = 1u << kOrderBits;
+  uint32_t d = 0;
+  for (uint32_t s = n >> 1; s > 0; s >>= 1) {
+    const uint32_t rx = (x & s) ? 1u : 0u, ry = (y & s) ? 1u : 0u;
+    d += s * s * ((3u * rx) ^ ry);
+    if (ry == 0) {
+      if (rx == 1) {
+        x = n - 1 - x;
+        y = n - 1 - y;
+      }
+      const uint32_t t = x;
+      x = y;
+      y = t;
+    }
+  }
+  return d;
 }
 
 }  // namespace
@@ -39,9 +57,9 @@ __global__ void k_order_keys(int32_t n, const int2 *__restrict__ dc, int32_t lx,
   const int32_t i = blockIdx.x * kThreads + threadIdx.x;
   if (i >= n) return;
   const int2 c = dc[i];
+  const double hi = (double)((1 << kOrderBits) - 1);
   const double fx = ((double)c.x - (double)lx) / tile_w, fy = ((double)c.y - (double)ly) / tile_h;
-  const uint32_t tx = (uint32_t)fmin(fmax(fx, 0.0), 63.0), ty = (uint32_t)fmin(fmax(fy, 0.0), 63.0);
-  key[i] = spread6(tx) | (spread6(ty) << 1);
+  key[i] = hilbert((uint32_t)fmin(fmax(fx, 0.0), hi), (uint32_t)fmin(fmax(fy, 0.0), hi));
   idx[i] = i;
 }
 
@@ -184,12 +202,13 @@ cudaError_t order_sort(int32_t n, const int2 *dc, int32_t lx, int32_t ly, double
   const int32_t tiles = order_tiles(n);
   const unsigned eb = (unsigned)((n + kThreads - 1) / kThreads);
   k_order_keys<<<eb, kThreads, 0, s>>>(n, dc, lx, ly, tile_w, tile_h, key0, idx0);
-  for (int pass = 0; pass < 2; pass++) {
+  for (int pass = 0; pass < kPasses; pass++) {
     const int shift = 6 * pass;
-    const uint32_t *ki = pass ? key1 : key0;
-    const int32_t *ii = pass ? idx1 : idx0;
-    uint32_t *ko = pass ? key0 : key1;
-    int32_t *io = pass ? idx0 : idx1;
+    const bool odd = pass & 1;
+    const uint32_t *ki = odd ? key1 : key0;
+    const int32_t *ii = odd ? idx1 : idx0;
+    uint32_t *ko = odd ? key0 : key1;
+    int32_t *io = odd ? idx0 : idx1;
     k_order_hist<<<tiles, kThreads, 0, s>>>(n, ki, shift, tiles, hist);
     k_order_scan<<<1, 1024, 0, s>>>(kDigits * tiles, hist);
     k_order_scatter<<<tiles, kThreads, 0, s>>>(n, ki, ii, shift, tiles, hist, ko, io);

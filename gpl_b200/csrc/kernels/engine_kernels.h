@@ -123,8 +123,9 @@ struct CellGather {
   float2 *slot_out[kMaxSlots];
 };
 int order_tiles(int32_t n);
-// Sorts the cells [0, n) by their coarse Z key (64 x 64 tiles of tile_w x tile_h from (lx, ly));
-// the old indices in new order end in idx0 (key0/key1/idx1: n each; hist: 64 * order_tiles(n)).
+// Sorts the cells [0, n) by the Hilbert index of their density centres on a 1024 x 1024 grid
+// of tile_w x tile_h cells from (lx, ly); the old indices in new order end in idx0
+// (key0/key1/idx1: n each; hist: 64 * order_tiles(n)).
 cudaError_t order_sort(int32_t n, const int2 *dc, int32_t lx, int32_t ly, double tile_w, double tile_h, uint32_t *key0, int32_t *idx0, uint32_t *key1, int32_t *idx1, int32_t *hist, cudaStream_t s);
 __global__ void k_order_gather(int32_t n, const int32_t *perm, CellGather g);
 __global__ void k_order_pins(int64_t n_pins, int32_t off, int32_t n, const int32_t *inv, const int64_t *old_start, const int64_t *new_start, int32_t *pin_cell, int32_t *pin_slot);

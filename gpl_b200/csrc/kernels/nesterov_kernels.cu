@@ -62,6 +62,74 @@ __device__ __forceinline__ int64_t cell_bin_addend(const RegionArgs &r, int32_t 
   return small_f2l_rz(a);
 }
 
+// The lanes' addends summed in a shared tile of th x tw bins (y fastest) from bin (tx0, ty0):
+// slots [0, cap) for cells, [cap, 2 cap) for fillers, 32-bit when narrow; then every nonzero
+// slot added to the HBM accumulators once. BLOCK: the block's threads share the tile; else
+// the warp's lanes alone (their own slice of the block's tile). The warp's lanes walk their
+// cells' bins in step (x outer, y inner), and lanes that hit the same bin in a step pool
+// their addends first (one shared atomic per distinct bin). Integer adds throughout.
+template <bool BLOCK>
+__device__ __forceinline__ void tile_scatter(const RegionArgs &r, bool narrow, unsigned long long *s64, unsigned int *s32, unsigned long long *s_red, int cap, int32_t tx0, int32_t ty0, int32_t th,
+                                             int32_t tw, bool any, int32_t x0, int32_t x1, int32_t y0, int32_t y1, int32_t dlx, int32_t dux, int32_t dly, int32_t duy, float scale, uint8_t kind) {
+  const int lane = threadIdx.x & 31;
+  const int start = BLOCK ? (int)threadIdx.x : lane, stride = BLOCK ? (int)blockDim.x : 32;
+  const int nt = tw * th;
+  if (narrow) {
+    for (int k = start; k < nt; k += stride) s32[k] = s32[cap + k] = 0u;
+  } else {
+    for (int k = start; k < nt; k += stride) s64[k] = s64[cap + k] = 0ull;
+  }
+  if (BLOCK)
+    __syncthreads();
+  else
+    __syncwarp();
+  const int nb = any ? (x1 - x0) * (y1 - y0) : 0;
+  const int rounds = __reduce_max_sync(0xffffffffu, nb);
+  int32_t x = x0, y = y0;
+  for (int q = 0; q < rounds; q++) {
+    int key = -1;
+    unsigned long long v = 0;
+    if (q < nb) {
+      int64_t a = cell_bin_addend(r, dlx, dux, dly, duy, x, y, scale, kind);
+      if (a) {
+        v = (unsigned long long)a;
+        key = (((x - tx0) * th + (y - ty0)) << 1) | (kind == CELL_FILLER ? 1 : 0);
+      }
+      if (++y == y1) {
+        y = y0;
+        x++;
+      }
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    if (narrow) {
+      // a block's sum for one bin stays below 2^32: each group of same-bin lanes adds its
+      // addends with one warp reduction, its first lane one shared atomic
+      const unsigned sum = __reduce_add_sync(peers, (unsigned)v);
+      if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&s32[(key & 1) * cap + (key >> 1)], sum);
+    } else {
+      s_red[threadIdx.x] = v;
+      __syncwarp();
+      if (key >= 0 && lane == __ffs(peers) - 1) {
+        unsigned long long sum = 0;
+        for (unsigned m = peers; m; m &= m - 1) sum += s_red[(threadIdx.x & ~31) + __ffs(m) - 1];
+        atomicAdd(&s64[(key & 1) * cap + (key >> 1)], sum);
+      }
+      __syncwarp();
+    }
+  }
+  if (BLOCK)
+    __syncthreads();
+  else
+    __syncwarp();
+  for (int k = start; k < nt; k += stride) {
+    size_t g = (size_t)(tx0 + k / th) * r.ny + (ty0 + k % th);
+    unsigned long long vi = narrow ? s32[k] : s64[k];
+    unsigned long long vf = narrow ? s32[cap + k] : s64[cap + k];
+    if (vi) atomicAdd((unsigned long long *)&r.acc_inst[g], vi);
+    if (vf) atomicAdd((unsigned long long *)&r.acc_fill[g], vf);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
   __shared__ unsigned long long s_tile[2 * kTileBins];  // cells then fillers; 32-bit when narrow
   __shared__ unsigned long long s_red[kThreads];
@@ -135,74 +203,32 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
     atomicMax(&s_box[3], wy1);
   }
   __syncthreads();
-  const int32_t tx0 = s_box[0], ty0 = s_box[2];
-  const int32_t tw = s_box[1] - tx0, th = s_box[3] - ty0;
-  const bool tile = tw > 0 && th > 0 && (int64_t)tw * th <= kTileBins;
+  // The block's cells share one tile when their bins fit it (32-bit slots hold twice as many
+  // bins); else each warp takes a slice of the tile for its own cells when their bins fit the
+  // slice, and a warp whose cells spread wider still adds straight to HBM.
   const bool narrow = r.narrow != 0;
+  const int bcap = narrow ? 2 * kTileBins : kTileBins;
+  const bool tile = s_box[1] > s_box[0] && s_box[3] > s_box[2] && (int64_t)(s_box[1] - s_box[0]) * (s_box[3] - s_box[2]) <= bcap;
   unsigned int *t32 = reinterpret_cast<unsigned int *>(s_tile);
-  if (!tile) {
-    if (threadIdx.x == 0 && r.spread) atomicAdd(r.spread, 1u);
-    if (any) {
-      unsigned long long *acc = (unsigned long long *)(kind == CELL_FILLER ? r.acc_fill : r.acc_inst);
-      for (int32_t y = y0; y < y1; y++)
-        for (int32_t x = x0; x < x1; x++) {
-          int64_t v = cell_bin_addend(r, dlx, dux, dly, duy, x, y, scale, kind);
-          if (v) atomicAdd(&acc[(size_t)x * r.ny + y], (unsigned long long)v);
-        }
-    }
+  if (tile) {
+    tile_scatter<true>(r, narrow, s_tile, t32, s_red, bcap, s_box[0], s_box[2], s_box[3] - s_box[2], s_box[1] - s_box[0], any, x0, x1, y0, y1, dlx, dux, dly, duy, scale, kind);
     return;
   }
-  const int nt = tw * th;
-  // only the slots this block's bins use: [0, nt) for cells and [kTileBins, kTileBins + nt)
-  // for fillers, in the tile's element width
-  if (narrow) {
-    for (int k = threadIdx.x; k < nt; k += blockDim.x) t32[k] = t32[kTileBins + k] = 0u;
-  } else {
-    for (int k = threadIdx.x; k < nt; k += blockDim.x) s_tile[k] = s_tile[kTileBins + k] = 0ull;
+  if (threadIdx.x == 0 && r.spread) atomicAdd(r.spread, 1u);
+  const int wcap = bcap / (kThreads / 32);
+  const bool wtile = wx1 > wx0 && wy1 > wy0 && (int64_t)(wx1 - wx0) * (wy1 - wy0) <= wcap;  // warp-uniform
+  if (wtile) {
+    const int w = threadIdx.x >> 5;
+    tile_scatter<false>(r, narrow, s_tile + (size_t)w * 2 * wcap, t32 + (size_t)w * 2 * wcap, s_red, wcap, wx0, wy0, wy1 - wy0, wx1 - wx0, any, x0, x1, y0, y1, dlx, dux, dly, duy, scale, kind);
+    return;
   }
-  __syncthreads();
-  // the warp's lanes in step over their bins (x outer, y inner); key = tile slot * 2 + filler
-  const int nb = any ? (x1 - x0) * (y1 - y0) : 0;
-  const int rounds = __reduce_max_sync(0xffffffffu, nb);
-  int32_t x = x0, y = y0;
-  for (int q = 0; q < rounds; q++) {
-    int key = -1;
-    unsigned long long v = 0;
-    if (q < nb) {
-      int64_t a = cell_bin_addend(r, dlx, dux, dly, duy, x, y, scale, kind);
-      if (a) {
-        v = (unsigned long long)a;
-        key = (((x - tx0) * th + (y - ty0)) << 1) | (kind == CELL_FILLER ? 1 : 0);
+  if (any) {
+    unsigned long long *acc = (unsigned long long *)(kind == CELL_FILLER ? r.acc_fill : r.acc_inst);
+    for (int32_t y = y0; y < y1; y++)
+      for (int32_t x = x0; x < x1; x++) {
+        int64_t v = cell_bin_addend(r, dlx, dux, dly, duy, x, y, scale, kind);
+        if (v) atomicAdd(&acc[(size_t)x * r.ny + y], (unsigned long long)v);
       }
-      if (++y == y1) {
-        y = y0;
-        x++;
-      }
-    }
-    const unsigned peers = __match_any_sync(0xffffffffu, key);
-    if (narrow) {
-      // a block's sum for one bin stays below 2^32: each group of same-bin lanes adds its
-      // addends with one warp reduction, its first lane one shared atomic
-      const unsigned sum = __reduce_add_sync(peers, (unsigned)v);
-      if (key >= 0 && lane == __ffs(peers) - 1) atomicAdd(&t32[(key & 1) * kTileBins + (key >> 1)], sum);
-    } else {
-      s_red[threadIdx.x] = v;
-      __syncwarp();
-      if (key >= 0 && lane == __ffs(peers) - 1) {
-        unsigned long long sum = 0;
-        for (unsigned m = peers; m; m &= m - 1) sum += s_red[(threadIdx.x & ~31) + __ffs(m) - 1];
-        atomicAdd(&s_tile[(key & 1) * kTileBins + (key >> 1)], sum);
-      }
-      __syncwarp();
-    }
-  }
-  __syncthreads();
-  for (int k = threadIdx.x; k < nt; k += blockDim.x) {
-    size_t g = (size_t)(tx0 + k / th) * r.ny + (ty0 + k % th);
-    unsigned long long vi = narrow ? t32[k] : s_tile[k];
-    unsigned long long vf = narrow ? t32[kTileBins + k] : s_tile[kTileBins + k];
-    if (vi) atomicAdd((unsigned long long *)&r.acc_inst[g], vi);
-    if (vf) atomicAdd((unsigned long long *)&r.acc_fill[g], vf);
   }
 }
 

@@ -2518,6 +2518,24 @@ int oracle_session_iterate(void *h, int n, int *done) {
   return k;
 }
 int64_t oracle_session_trials(void *h) { return ((OracleRun *)h)->np.trials; }
+// The first region's cells as the loop holds them: density centre (2 int32), half density
+// size (2 int32) and kind (0 std, 1 macro, 2 filler) per cell, in the region's cell order;
+// returns the cell count (out arrays sized by a first call with NULL).
+int64_t oracle_session_cells(void *h, int32_t *centre, int32_t *half, uint8_t *kind) {
+  OracleRun *run = (OracleRun *)h;
+  if (run->np.nbs.empty()) return 0;
+  const Nb &nb = run->np.nbs[0];
+  if (centre)
+    for (size_t i = 0; i < nb.cells.size(); i++) {
+      const GCell &g = run->np.gcells[nb.cells[i]];
+      centre[2 * i] = g.d_cx();
+      centre[2 * i + 1] = g.d_cy();
+      half[2 * i] = g.d_dx() / 2;
+      half[2 * i + 1] = g.d_dy() / 2;
+      kind[i] = g.is_filler() ? 2 : (g.is_macro() ? 1 : 0);
+    }
+  return (int64_t)nb.cells.size();
+}
 int oracle_session_close(void *h, gpl_result_t *out) {
   OracleRun *run = (OracleRun *)h;
   if (run->res.status == GPL_PLACED) oracle_guarded(run->res, [&] { run->close(); });

@@ -371,6 +371,8 @@ def ours(a):
     if world == 1 and not a.no_cpu_baseline:
         cpu = cpu_sample(a)
     precision = precision_report(local, nx)
+    if not a.no_precision_runs and world == 1:
+        precision["runs"] = precision_runs(local, cfg)
     conf = workload(a, design)
     conf["parallelism"] = f"replicas x{world}"
     out = {
@@ -412,6 +414,23 @@ def precision_report(local, n):
         torch.cuda.synchronize(local)
         e = max(float((gx.double() - ex).abs().max() / ex.abs().max()), float((gy.double() - ey).abs().max() / ey.abs().max()))
         out[f"field_rel_err_{name}"] = e
+    return out
+
+
+def precision_runs(local, cfg):
+    """Each form's whole command against the same command with the FP64 density solve (the
+    transforms in double throughout) on the workload's design: final HPWL and overflow, and
+    the written placement's coordinates (DBU), as errors against the FP64 run."""
+    from gpl_b200 import engine, synth
+    design = synth.generate(cfg["preset"])
+    runs = {f: engine.global_placement(design, cfg["args"], device=local, poisson=f) for f in ("fp64", "mixed", "fp32")}
+    ref = runs["fp64"]
+    out = {"yardstick": "the same command with the FP64 density solve", "fp64": {"final_hpwl": ref["final_hpwl"], "final_overflow": ref["final_overflow"], "iterations": ref["nesterov_iterations"]}}
+    for f in ("mixed", "fp32"):
+        r = runs[f]
+        d = np.abs(r["locations"][:, 1:].astype(np.int64) - ref["locations"][:, 1:].astype(np.int64)) if len(r["locations"]) == len(ref["locations"]) else np.zeros(1)
+        out[f] = {"final_hpwl_rel_err": abs(r["final_hpwl"] - ref["final_hpwl"]) / max(ref["final_hpwl"], 1), "final_overflow_err": abs(r["final_overflow"] - ref["final_overflow"]),
+                  "iterations": r["nesterov_iterations"], "coord_err_dbu": {"median": float(np.median(d)), "p99": float(np.quantile(d, 0.99)), "max": float(d.max())}}
     return out
 
 
@@ -463,6 +482,7 @@ def main():
     ap.add_argument("--config", default="cfg3", choices=list(CONFIGS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision-runs", action="store_true", help="skip the three whole commands (mixed, FP32, FP64 density solves) of the precision report")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp32"], help="the density solve timed as the headline")
     ap.add_argument("--start", default="spread", choices=["spread", "ip"],
                     help="time the loop from the generator's spread placement with the initial placement skipped (both arms, the default), or after the device's initial placement (a profiling case)")

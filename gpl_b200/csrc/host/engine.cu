@@ -287,7 +287,7 @@ void Engine::upload(const EngineSetup &s) {
     if (!failed()) {
       cudaError_t pe = cudaSuccess;
       r->plan = poisson_plan_create(rs.nx, rs.ny, rs.wx.data(), rs.wy.data(), poisson_mode_, &pe);
-      check(pe, poisson_mode_ == 0 ? "poisson plan (fp32)" : "poisson plan (split-bf16 tcgen05)");
+      check(pe, poisson_mode_ == 0 ? "poisson plan (fp32)" : poisson_mode_ == 2 ? "poisson plan (fp64)" : "poisson plan (split-bf16 tcgen05)");
       if (r->plan) r->dens_split = poisson_split_input(r->plan, &r->split_ld);
       progress("  upload: region solver planned (%dx%d bins)", rs.nx, rs.ny);
     }
@@ -752,7 +752,7 @@ void Engine::rebuild_poisson(int mode) {
     r->split_ld = 0;
     cudaError_t pe = cudaSuccess;
     r->plan = poisson_plan_create(region_dims_[b].first, region_dims_[b].second, region_wx_[b].data(), region_wy_[b].data(), mode, &pe);
-    check(pe, mode == 0 ? "poisson plan (fp32)" : "poisson plan (split-bf16 tcgen05)");
+    check(pe, mode == 0 ? "poisson plan (fp32)" : mode == 2 ? "poisson plan (fp64)" : "poisson plan (split-bf16 tcgen05)");
     if (r->plan) {
       r->dens_split = poisson_split_input(r->plan, &r->split_ld);
       // the current density into the new operand, the field recomputed

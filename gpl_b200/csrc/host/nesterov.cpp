@@ -2405,6 +2405,8 @@ int gpl_set_option(gpl_ctx *c, const char *name, const char *value) {
       c->poisson_mode = 1;
     else if (v == "fp32")
       c->poisson_mode = 0;
+    else if (v == "fp64")
+      c->poisson_mode = 2;
     else
       return -1;
     return 0;
@@ -2481,7 +2483,7 @@ int gpl_session_iterate(gpl_session *s, int n, int *done) {
 int gpl_session_set_option(gpl_session *s, const char *name, const char *value) {
   std::string n = name, v = value;
   if (n == "poisson") {
-    int mode = v == "fp32" ? 0 : v == "mixed" ? 1 : -1;
+    int mode = v == "fp32" ? 0 : v == "mixed" ? 1 : v == "fp64" ? 2 : -1;
     if (mode < 0) return -1;
     if (!s->run->nesterov) return -1;
     s->ctx->eng->rebuild_poisson(mode);

@@ -15,6 +15,7 @@
 // the reference's probes reads it.
 //
 // Mode 0 (this file): FP32 SIMT GEMMs. Mode 1: split-BF16 tcgen05 GEMMs (poisson_tc.cu).
+// Mode 2 (this file): the FP32 form's sequence in double, the precision yardstick.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -32,33 +33,34 @@ namespace gpl {
 // 128 x 64 output tile per block, K-step 8, 256 threads with 8 x 4 outputs each.
 constexpr int SG_BM = 128, SG_BN = 64, SG_BK = 8;
 
-__global__ void __launch_bounds__(256) k_sgemm_tn(GemmBatch gb) {
-  const GemmProblem P = gb.p[blockIdx.z];
+template <typename T>
+__global__ void __launch_bounds__(256) k_gemm_tn(GemmBatchT<T> gb) {
+  const GemmProblemT<T> P = gb.p[blockIdx.z];
   const int m0 = blockIdx.y * SG_BM, n0 = blockIdx.x * SG_BN;
   if (m0 >= P.M || n0 >= P.N) return;
-  __shared__ __align__(16) float As[SG_BK][SG_BM + 4];
-  __shared__ __align__(16) float Bs[SG_BK][SG_BN + 4];
+  __shared__ __align__(16) T As[SG_BK][SG_BM + 4];
+  __shared__ __align__(16) T Bs[SG_BK][SG_BN + 4];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int ar = tid >> 1, ak = (tid & 1) * 4;  // A loader: row, first k
   const int br = tid >> 2, bk = (tid & 3) * 2;  // B loader
-  float acc[8][4];
+  T acc[8][4];
 #pragma unroll
   for (int i = 0; i < 8; i++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
-  float ra[4], rb[2];
+    for (int j = 0; j < 4; j++) acc[i][j] = (T)0;
+  T ra[4], rb[2];
   auto load = [&](int k0) {
     int gm = m0 + ar;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       int gk = k0 + ak + q;
-      ra[q] = (gm < P.M && gk < P.K) ? P.A[(size_t)gm * P.lda + gk] : 0.0f;
+      ra[q] = (gm < P.M && gk < P.K) ? P.A[(size_t)gm * P.lda + gk] : (T)0;
     }
     int gn = n0 + br;
 #pragma unroll
     for (int q = 0; q < 2; q++) {
       int gk = k0 + bk + q;
-      rb[q] = (gn < P.N && gk < P.K) ? P.B[(size_t)gn * P.ldb + gk] : 0.0f;
+      rb[q] = (gn < P.N && gk < P.K) ? P.B[(size_t)gn * P.ldb + gk] : (T)0;
     }
   };
   load(0);
@@ -71,15 +73,17 @@ __global__ void __launch_bounds__(256) k_sgemm_tn(GemmBatch gb) {
     if (k0 + SG_BK < P.K) load(k0 + SG_BK);
 #pragma unroll
     for (int kk = 0; kk < SG_BK; kk++) {
-      float4 a0 = *reinterpret_cast<const float4 *>(&As[kk][ty * 4]);
-      float4 a1 = *reinterpret_cast<const float4 *>(&As[kk][64 + ty * 4]);
-      float4 b0 = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 4]);
-      float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      float b[4] = {b0.x, b0.y, b0.z, b0.w};
+      T a[8], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        a[q] = As[kk][ty * 4 + q];
+        a[4 + q] = As[kk][64 + ty * 4 + q];
+        b[q] = Bs[kk][tx * 4 + q];
+      }
 #pragma unroll
       for (int i = 0; i < 8; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     __syncthreads();
   }
@@ -95,16 +99,18 @@ __global__ void __launch_bounds__(256) k_sgemm_tn(GemmBatch gb) {
   }
 }
 
-cudaError_t sgemm_tn(const GemmBatch &gb, int count, cudaStream_t s) {
+template <typename T>
+cudaError_t gemm_tn(const GemmBatchT<T> &gb, int count, cudaStream_t s) {
   int M = 0, N = 0;
   for (int i = 0; i < count; i++) {
     M = M > gb.p[i].M ? M : gb.p[i].M;
     N = N > gb.p[i].N ? N : gb.p[i].N;
   }
   dim3 grid((N + SG_BN - 1) / SG_BN, (M + SG_BM - 1) / SG_BM, count);
-  k_sgemm_tn<<<grid, 256, 0, s>>>(gb);
+  k_gemm_tn<T><<<grid, 256, 0, s>>>(gb);
   return cudaGetLastError();
 }
+cudaError_t sgemm_tn(const GemmBatch &gb, int count, cudaStream_t s) { return gemm_tn<float>(gb, count, s); }
 
 // ---------------------------------------------------------------- the spectral step
 // (src/nesterov.rs:425-440) on the scaled forward transform: phi = Ah / (wx2 + wy2),
@@ -122,6 +128,26 @@ __global__ void k_spectral(int nx, int ny, const float *__restrict__ ah, const f
     exh[k] = ex;
     eyh[k] = ey;
   }
+}
+// The FP64 yardstick's spectral step: the same in double (wavenumbers widened from float).
+__global__ void k_spectral_d(int nx, int ny, const double *__restrict__ ah, const float *__restrict__ wx, const float *__restrict__ wy, double *__restrict__ exh, double *__restrict__ eyh) {
+  int64_t n = (int64_t)nx * ny;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    int u = (int)(k / ny), v = (int)(k % ny);
+    double ex = 0.0, ey = 0.0;
+    if (u != 0 || v != 0) {
+      const double a = (double)wx[u], b = (double)wy[v];
+      const double p = ah[k] / (a * a + b * b);
+      ex = p * a;
+      ey = p * b;
+    }
+    exh[k] = ex;
+    eyh[k] = ey;
+  }
+}
+template <typename A, typename B>
+__global__ void k_convert(int64_t n, const A *__restrict__ in, B *__restrict__ out) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) out[k] = (B)in[k];
 }
 
 // ---------------------------------------------------------------- basis matrices (host)
@@ -202,7 +228,14 @@ PoissonPlan *poisson_plan_create(int nx, int ny, const float *wx_host, const flo
   for (int i = 0; i < ny; i++) sq[i] = wy_host[i] * wy_host[i];
   TRY(cudaMemcpy(p->wy, wy_host, ny * sizeof(float), cudaMemcpyHostToDevice));
   TRY(cudaMemcpy(p->wy2, sq.data(), ny * sizeof(float), cudaMemcpyHostToDevice));
-  if (mode == 0) {
+  if (mode == 2) {
+    const std::vector<double> *mats[6] = {&b.CyTs, &b.CxTs, &b.Cy, &b.Sy, &b.Sx, &b.Cx};
+    for (int k = 0; k < 6; k++) {
+      TRY(cudaMalloc(&p->d_basis[k], mats[k]->size() * sizeof(double)));
+      TRY(cudaMemcpy(p->d_basis[k], mats[k]->data(), mats[k]->size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    for (int k = 0; k < 8; k++) TRY(cudaMalloc(&p->d_buf[k], n * sizeof(double)));
+  } else if (mode == 0) {
     TRY(upload_f32(b.CyTs, &p->CyTs));
     TRY(upload_f32(b.CxTs, &p->CxTs));
     TRY(upload_f32(b.Cy, &p->Cy));
@@ -232,12 +265,16 @@ void poisson_plan_destroy(PoissonPlan *p) {
   float *bufs[] = {p->wx, p->wx2, p->wy, p->wy2, p->CyTs, p->CxTs, p->Cy, p->Sy, p->Sx, p->Cx, p->t1, p->ah, p->exh, p->eyh, p->t2, p->t3};
   for (float *b : bufs)
     if (b) cudaFree(b);
+  for (double *b : p->d_basis)
+    if (b) cudaFree(b);
+  for (double *b : p->d_buf)
+    if (b) cudaFree(b);
   tc_plan_free(p);
   delete p;
 }
 
 __nv_bfloat16 *poisson_split_input(PoissonPlan *p, int *ld) {
-  if (p->mode == 0) return nullptr;
+  if (p->mode != 1) return nullptr;
   *ld = 2 * p->ny;
   return p->tc_dens;
 }
@@ -254,16 +291,46 @@ __global__ void k_split_density(int nx, int ny, const float *__restrict__ d, __n
 }
 
 cudaError_t poisson_split_density(PoissonPlan *p, const float *density, cudaStream_t s) {
-  if (p->mode == 0) return cudaSuccess;
+  if (p->mode != 1) return cudaSuccess;
   int64_t n = (int64_t)p->nx * p->ny;
   int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
   k_split_density<<<blocks, 256, 0, s>>>(p->nx, p->ny, density, p->tc_dens, 2 * p->ny);
   return cudaGetLastError();
 }
 
-int poisson_launches(const PoissonPlan *p) { return p->mode == 0 ? 5 : tc_launches(p); }
+int poisson_launches(const PoissonPlan *p) { return p->mode == 0 ? 5 : p->mode == 2 ? 9 : tc_launches(p); }
+
+// The FP64 form: the density widened to double, the FP32 form's six GEMMs and spectral step
+// in double throughout, the fields rounded to float once at the end. The yardstick the
+// other forms' placements are compared with; not a speed path.
+static cudaError_t solve_fp64(PoissonPlan *p, const float *density, float *field_x, float *field_y, cudaStream_t s) {
+  const int nx = p->nx, ny = p->ny;
+  const int64_t n = (int64_t)nx * ny;
+  const int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+  double *const *B = p->d_basis;
+  double *rho = p->d_buf[0], *t1 = p->d_buf[1], *ah = p->d_buf[2], *exh = p->d_buf[3], *eyh = p->d_buf[4], *t2 = p->d_buf[5], *t3 = p->d_buf[6], *f = p->d_buf[7];
+  k_convert<float, double><<<blocks, 256, 0, s>>>(n, density, rho);
+  GemmBatchT<double> g{};
+  g.p[0] = GemmProblemT<double>{ny, nx, ny, B[0], ny, rho, ny, t1, nx};
+  cudaError_t e = gemm_tn<double>(g, 1, s);
+  if (e != cudaSuccess) return e;
+  g.p[0] = GemmProblemT<double>{nx, ny, nx, B[1], nx, t1, nx, ah, ny};
+  if ((e = gemm_tn<double>(g, 1, s)) != cudaSuccess) return e;
+  k_spectral_d<<<blocks, 256, 0, s>>>(nx, ny, ah, p->wx, p->wy, exh, eyh);
+  g.p[0] = GemmProblemT<double>{ny, nx, ny, B[2], ny, exh, ny, t2, nx};
+  g.p[1] = GemmProblemT<double>{ny, nx, ny, B[3], ny, eyh, ny, t3, nx};
+  if ((e = gemm_tn<double>(g, 2, s)) != cudaSuccess) return e;
+  g.p[0] = GemmProblemT<double>{nx, ny, nx, B[4], nx, t2, nx, f, ny};
+  if ((e = gemm_tn<double>(g, 1, s)) != cudaSuccess) return e;
+  k_convert<double, float><<<blocks, 256, 0, s>>>(n, f, field_x);
+  g.p[0] = GemmProblemT<double>{nx, ny, nx, B[5], nx, t3, nx, f, ny};
+  if ((e = gemm_tn<double>(g, 1, s)) != cudaSuccess) return e;
+  k_convert<double, float><<<blocks, 256, 0, s>>>(n, f, field_y);
+  return cudaGetLastError();
+}
 
 cudaError_t poisson_solve(PoissonPlan *p, const float *density, float *field_x, float *field_y, cudaStream_t s) {
+  if (p->mode == 2) return solve_fp64(p, density, field_x, field_y, s);
   if (p->mode != 0) return tc_solve(p, field_x, field_y, s);
   int nx = p->nx, ny = p->ny;
   GemmBatch g{};

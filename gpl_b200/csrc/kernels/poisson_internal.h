@@ -9,18 +9,22 @@
 namespace gpl {
 
 // D[m][n] = sum_k A[m][k] * B[n][k], row-major, leading dimensions in elements.
-struct GemmProblem {
+template <typename T>
+struct GemmProblemT {
   int M, N, K;
-  const float *A;
+  const T *A;
   int lda;
-  const float *B;
+  const T *B;
   int ldb;
-  float *D;
+  T *D;
   int ldd;
 };
-struct GemmBatch {
-  GemmProblem p[2];
+template <typename T>
+struct GemmBatchT {
+  GemmProblemT<T> p[2];
 };
+using GemmProblem = GemmProblemT<float>;
+using GemmBatch = GemmBatchT<float>;
 cudaError_t sgemm_tn(const GemmBatch &gb, int count, cudaStream_t s);
 
 // The six basis matrices in double (see poisson.cu): CyTs[v][y], CxTs[u][x] (forward, scaled
@@ -41,6 +45,9 @@ struct PoissonPlan {
   // tensor-core path
   __nv_bfloat16 *tc_dens = nullptr;  // density as [nx][2*ny] bf16 (hi | lo)
   TcState *tc = nullptr;
+  // FP64 path (the yardstick): the FP32 path's matrices and sequence in double
+  double *d_basis[6] = {};           // CyTs, CxTs, Cy, Sy, Sx, Cx
+  double *d_buf[8] = {};             // rho, t1, ah, exh, eyh, t2, t3, and the fields' staging
 };
 
 cudaError_t tc_plan_init(PoissonPlan *p, const BasisHost &b);

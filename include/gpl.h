@@ -154,7 +154,8 @@ gpl_ctx *gpl_create(int device);
 void gpl_destroy(gpl_ctx *ctx);
 
 /* Engine options with no reference counterpart (the reference runs on one thread):
- *   "poisson" = "mixed" (split-BF16 tcgen05 DCT GEMMs, the default) | "fp32" (SIMT GEMMs)
+ *   "poisson" = "mixed" (split-BF16 tcgen05 DCT GEMMs, the default) | "fp32" (SIMT GEMMs) |
+ *               "fp64" (the same transforms in double throughout: the precision yardstick)
  *   "trace"   = "0" | "1" (probe lines, as the reference's `Log.trace`)
  *   "reorder" = "1" (the default) | "0": the device's cell order sorted again by position when
  *               the cells have moved apart (no result depends on the order but the double sums'
@@ -180,7 +181,7 @@ typedef struct gpl_session gpl_session;
 gpl_session *gpl_session_open(gpl_ctx *ctx, const gpl_design_t *design, int argc,
                               const char *const *argv, const gpl_router_t *router);
 int gpl_session_iterate(gpl_session *s, int n, int *done);
-/* "poisson" = "mixed" | "fp32" (solvers rebuilt, the field recomputed); "profile" = "0" | "1"
+/* "poisson" = "mixed" | "fp32" | "fp64" (solvers rebuilt, the field recomputed); "profile" = "0" | "1"
  * (per-phase device time from CUDA events); "overlap" = "1" | "0" (the WA beside the density
  * solve or after it); "reorder" as gpl_set_option's. No reference counterpart. */
 int gpl_session_set_option(gpl_session *s, const char *name, const char *value);
@@ -267,7 +268,8 @@ int gpl_kernel_hpwl(int64_t n_nets, const int64_t *net_start, const int32_t *pin
                     int32_t fused, int64_t *hpwl, void *stream);
 
 /* `Fft::solve` (src/nesterov.rs:412-444) without the potential: density[nx*ny] (x-major) to
- * field_x, field_y (device pointers). mode 0 = FP32 SIMT GEMMs, 1 = split-BF16 tcgen05 GEMMs.
+ * field_x, field_y (device pointers). mode 0 = FP32 SIMT GEMMs, 1 = split-BF16 tcgen05 GEMMs,
+ * 2 = the FP32 form's transforms in double (fields rounded to float once).
  * wx[nx], wy[ny] are the wavenumbers (host pointers). Builds its basis matrices and workspace
  * per call, so it allocates. */
 int gpl_kernel_poisson(int32_t nx, int32_t ny, const float *wx, const float *wy,

@@ -333,3 +333,23 @@ def test_wa_small_net_forms_bit_exact(L, form, monkeypatch):
     got = C.c_int64()
     assert L.gpl_kernel_hpwl(n_nets, ptr(ds), ptr(dxy), 0, C.byref(got), stream()) == 0
     assert got.value == oracle.lib().oracle_hpwl(n_nets, start.ctypes.data_as(C.c_void_p), xy.ctypes.data_as(C.c_void_p))
+
+
+@pytest.mark.parametrize("nx,ny", [(64, 64), (256, 128)])
+def test_poisson_fp64_form_against_the_fp64_solve(L, nx, ny):
+    """The engine's FP64 solve form (mode 2, the yardstick its placements are compared with):
+    the FP32 form's transforms in double, against the separate double solve
+    gpl_kernel_poisson_fp64; the fields agree to float rounding (1e-6 of the largest)."""
+    rng = np.random.default_rng(nx * 3 + ny)
+    dens = (rng.random(nx * ny) * 1.5).astype(np.float32)
+    _, _, wx, wy = _poisson_oracle(nx, ny, 900.0, 1400.0, dens)
+    d = dev(dens)
+    gx, gy = dev(np.zeros(nx * ny, np.float32)), dev(np.zeros(nx * ny, np.float32))
+    assert L.gpl_kernel_poisson(nx, ny, wx.ctypes.data, wy.ctypes.data, ptr(d), ptr(gx), ptr(gy), 2, stream()) == 0
+    L.gpl_kernel_poisson_fp64.argtypes = [C.c_int32, C.c_int32] + [C.c_void_p] * 6
+    hx, hy = dev(np.zeros(nx * ny, np.float64)), dev(np.zeros(nx * ny, np.float64))
+    assert L.gpl_kernel_poisson_fp64(nx, ny, wx.ctypes.data, wy.ctypes.data, ptr(d), ptr(hx), ptr(hy), stream()) == 0
+    sync()
+    for got, want in ((gx, hx), (gy, hy)):
+        g, w = got.cpu().numpy().astype(np.float64), want.cpu().numpy()
+        assert np.max(np.abs(g - w)) <= 1e-6 * np.max(np.abs(w))

@@ -74,10 +74,12 @@ __device__ __forceinline__ void tile_scatter(const RegionArgs &r, bool narrow, u
   const int lane = threadIdx.x & 31;
   const int start = BLOCK ? (int)threadIdx.x : lane, stride = BLOCK ? (int)blockDim.x : 32;
   const int nt = tw * th;
-  if (narrow) {
-    for (int k = start; k < nt; k += stride) s32[k] = s32[cap + k] = 0u;
-  } else {
-    for (int k = start; k < nt; k += stride) s64[k] = s64[cap + k] = 0ull;
+  {
+    // zeroed 16 bytes a store (the slots this tile uses, rounded up to a multiple of 16 bytes)
+    uint4 *c4 = reinterpret_cast<uint4 *>(narrow ? (void *)s32 : (void *)s64);
+    uint4 *f4 = reinterpret_cast<uint4 *>(narrow ? (void *)(s32 + cap) : (void *)(s64 + cap));
+    const int n4 = narrow ? (nt + 3) / 4 : (nt + 1) / 2;
+    for (int k = start; k < n4; k += stride) c4[k] = f4[k] = make_uint4(0u, 0u, 0u, 0u);
   }
   if (BLOCK)
     __syncthreads();
@@ -121,19 +123,30 @@ __device__ __forceinline__ void tile_scatter(const RegionArgs &r, bool narrow, u
     __syncthreads();
   else
     __syncwarp();
+  // the slot's bin (x, y) followed step by step (one division per thread, not per slot)
+  const int dxs = stride / th, dys = stride - dxs * th;
+  int xk = start / th, yk = start - xk * th;
   for (int k = start; k < nt; k += stride) {
-    size_t g = (size_t)(tx0 + k / th) * r.ny + (ty0 + k % th);
     unsigned long long vi = narrow ? s32[k] : s64[k];
     unsigned long long vf = narrow ? s32[cap + k] : s64[cap + k];
-    if (vi) atomicAdd((unsigned long long *)&r.acc_inst[g], vi);
-    if (vf) atomicAdd((unsigned long long *)&r.acc_fill[g], vf);
+    if (vi | vf) {
+      const size_t g = (size_t)(tx0 + xk) * r.ny + (ty0 + yk);
+      if (vi) atomicAdd((unsigned long long *)&r.acc_inst[g], vi);
+      if (vf) atomicAdd((unsigned long long *)&r.acc_fill[g], vf);
+    }
+    xk += dxs;
+    yk += dys;
+    if (yk >= th) {
+      yk -= th;
+      xk++;
+    }
   }
 }
 
 __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
-  __shared__ unsigned long long s_tile[2 * kTileBins];  // cells then fillers; 32-bit when narrow
+  __shared__ __align__(16) unsigned long long s_tile[2 * kTileBins];  // cells then fillers; 32-bit when narrow
   __shared__ unsigned long long s_red[kThreads];
-  __shared__ int s_box[4];
+  __shared__ int s_box[5];  // the block's bin box, and its cells' (cell, bin) addends
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < r.n_cells;
   int32_t x0 = INT32_MAX, x1 = INT32_MIN, y0 = INT32_MAX, y1 = INT32_MIN;
@@ -190,9 +203,12 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
     s_box[1] = INT32_MIN;
     s_box[2] = INT32_MAX;
     s_box[3] = INT32_MIN;
+    s_box[4] = 0;
   }
   __syncthreads();
   const bool any = valid && x0 < x1 && y0 < y1;
+  const int nb_cell = any ? (x1 - x0) * (y1 - y0) : 0;
+  const int w_addends = __reduce_add_sync(0xffffffffu, nb_cell);
   int32_t wx0 = __reduce_min_sync(0xffffffffu, any ? x0 : INT32_MAX), wx1 = __reduce_max_sync(0xffffffffu, any ? x1 : INT32_MIN);
   int32_t wy0 = __reduce_min_sync(0xffffffffu, any ? y0 : INT32_MAX), wy1 = __reduce_max_sync(0xffffffffu, any ? y1 : INT32_MIN);
   const int lane = threadIdx.x & 31;
@@ -201,14 +217,18 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
     atomicMax(&s_box[1], wx1);
     atomicMin(&s_box[2], wy0);
     atomicMax(&s_box[3], wy1);
+    atomicAdd(&s_box[4], w_addends);
   }
   __syncthreads();
   // The block's cells share one tile when their bins fit it (32-bit slots hold twice as many
-  // bins); else each warp takes a slice of the tile for its own cells when their bins fit the
-  // slice, and a warp whose cells spread wider still adds straight to HBM.
+  // bins) and the tile is not mostly empty (at most twice as many slots as addends: a sparse
+  // block's slots would cost more to clear and flush than its addends); else each warp takes a
+  // slice of the tile for its own cells on the same terms, and a warp whose cells spread
+  // wider adds straight to HBM.
   const bool narrow = r.narrow != 0;
   const int bcap = narrow ? 2 * kTileBins : kTileBins;
-  const bool tile = s_box[1] > s_box[0] && s_box[3] > s_box[2] && (int64_t)(s_box[1] - s_box[0]) * (s_box[3] - s_box[2]) <= bcap;
+  const int64_t b_nt = (int64_t)(s_box[1] - s_box[0]) * (s_box[3] - s_box[2]);
+  const bool tile = s_box[1] > s_box[0] && s_box[3] > s_box[2] && b_nt <= bcap && b_nt <= 2 * (int64_t)s_box[4];
   unsigned int *t32 = reinterpret_cast<unsigned int *>(s_tile);
   if (tile) {
     tile_scatter<true>(r, narrow, s_tile, t32, s_red, bcap, s_box[0], s_box[2], s_box[3] - s_box[2], s_box[1] - s_box[0], any, x0, x1, y0, y1, dlx, dux, dly, duy, scale, kind);
@@ -216,7 +236,8 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
   }
   if (threadIdx.x == 0 && r.spread) atomicAdd(r.spread, 1u);
   const int wcap = bcap / (kThreads / 32);
-  const bool wtile = wx1 > wx0 && wy1 > wy0 && (int64_t)(wx1 - wx0) * (wy1 - wy0) <= wcap;  // warp-uniform
+  const int64_t w_nt = (int64_t)(wx1 - wx0) * (wy1 - wy0);
+  const bool wtile = wx1 > wx0 && wy1 > wy0 && w_nt <= wcap && w_nt <= 2 * (int64_t)w_addends;  // warp-uniform
   if (wtile) {
     const int w = threadIdx.x >> 5;
     tile_scatter<false>(r, narrow, s_tile + (size_t)w * 2 * wcap, t32 + (size_t)w * 2 * wcap, s_red, wcap, wx0, wy0, wy1 - wy0, wx1 - wx0, any, x0, x1, y0, y1, dlx, dux, dly, duy, scale, kind);

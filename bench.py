@@ -311,6 +311,7 @@ def ours(a):
     fp32["profile"] = phase_times(min(a.steps, 10))
     if a.form == "fp32":
         mixed = fp32
+    tuning = sess.tuning()
     log("timed")
     res = sess.close()
     log("session closed")
@@ -385,7 +386,7 @@ def ours(a):
                            "note": "timed on the iterations after the mixed form's, from the same run"},
                   "mixed_over_fp32": value / value_fp32 if value_fp32 else None},
         "phases": phases, "roofline": roof, "gpu_launches": mixed["launches"], "clocks": mixed["clocks"],
-        "e2e": e2e, "cpu_baseline": cpu, "precision": precision,
+        "e2e": e2e, "cpu_baseline": cpu, "precision": precision, "tuning": tuning,
     }
     print(json.dumps(out))
 

@@ -20,7 +20,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 CU = [("kernels/nesterov_kernels.cu", True), ("kernels/bicgstab.cu", True), ("kernels/rudy.cu", True),
       ("kernels/poisson.cu", False), ("kernels/b2b.cu", True), ("kernels/adjoint.cu", False), ("kernels/poisson_tc.cu", False), ("kernels/cell_order.cu", True), ("host/engine.cu", True),
       ("host/capi_kernels.cu", True), ("host/bicgstab_noalloc.cu", True)]
-CPP = ["host/place.cpp", "host/nesterov.cpp"]
+CPP = ["host/place.cpp", "host/nesterov.cpp", "host/tune.cpp"]
 
 
 def _run(cmd):

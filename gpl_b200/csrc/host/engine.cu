@@ -8,6 +8,7 @@
 #include "../kernels/engine_kernels.h"
 #include "engine.h"
 #include "parallel.h"
+#include "tune.h"
 
 namespace gpl {
 void progress(const char *fmt, ...) __attribute__((format(printf, 1, 2)));
@@ -36,6 +37,9 @@ struct Engine::Region {
   double spread_base = 0;          // the spread blocks of the order as made
   bool need_base = true;           // the next scatter's count is that base
   int64_t reorder_trial = -1000;   // the trial of the last reorder
+  // the scatter's form (shared tiles, or straight to HBM: the same int64 sums either way),
+  // timed in place; GPL_SCATTER=tiles|global fixes it
+  std::unique_ptr<Tuner> scatter_tune = std::make_unique<Tuner>("scatter", std::vector<std::string>{"tiles", "global"}, "GPL_SCATTER", 3, 128);
 };
 
 static int blocks_for(int64_t n, int per = kThreadsPerBlock) { return (int)std::max<int64_t>(1, (n + per - 1) / per); }
@@ -76,6 +80,8 @@ Engine::Engine(int device) : device_(device) {
   if (!failed()) check(cudaStreamCreateWithPriority(&wa_stream_, cudaStreamNonBlocking, prio_lo), "cudaStreamCreate");
   if (!failed()) check(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming), "cudaEventCreate");
   if (!failed()) check(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming), "cudaEventCreate");
+  // the degree-2..4 nets' WA form, timed in place; GPL_WA_SMALL=lean|nets|pins fixes it
+  if (!failed()) wa_tune_ = std::make_unique<Tuner>("small-net WA", std::vector<std::string>{"lean", "nets", "pins"}, "GPL_WA_SMALL", 3, 256);
 }
 
 void Engine::join() {
@@ -399,7 +405,9 @@ void Engine::place_at(int b, SlotId slot) {
   CellArgs c = CELLS(r);
   ph_begin(PH_PLACE);
   launches += (r->n_cells ? 1 : 0) + 1;
-  if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, c, PLACE_AT, 0.0f, 0.0f, r->slot[slot]);
+  RegionArgs a = r->args;
+  a.global = r->scatter_tune->best();
+  if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(a, c, PLACE_AT, 0.0f, 0.0f, r->slot[slot]);
   ph_end(PH_PLACE);
   ph_begin(PH_FINALIZE);
   k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld, r->ticket, &dev_scal_[b].overflow);
@@ -431,7 +439,12 @@ void Engine::nesterov_step(int b, float step, float coeff) {
   CellArgs c = CELLS(r);
   ph_begin(PH_PLACE);
   launches += (r->n_cells ? 1 : 0) + 1;
-  if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(r->args, c, PLACE_NESTEROV, step, coeff, nullptr);
+  if (r->n_cells) {
+    RegionArgs a = r->args;
+    a.global = r->scatter_tune->start(stream_);
+    k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(a, c, PLACE_NESTEROV, step, coeff, nullptr);
+    r->scatter_tune->stop(stream_);
+  }
   ph_end(PH_PLACE);
   ph_begin(PH_FINALIZE);
   k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld, r->ticket, &dev_scal_[b].overflow);
@@ -483,7 +496,9 @@ void Engine::wa(float cx, float cy) {
   ph_begin(PH_WA, st);
   if (wa_small_blocks(small_)) {
     launches += 1;
-    launch_wa_small(w, cx, cy, 1, st);
+    const int form = wa_tune_->start(st);
+    launch_wa_small(w, cx, cy, 1, st, form);
+    wa_tune_->stop(st);
   }
   if (n_tiles_) {
     launches += 1;
@@ -565,6 +580,16 @@ void Engine::fetch() {
     hpwl_fetched_ = true;
   }
   ph_flush();
+  // the trial's timed launches have ended (the WA joined the stream before the copy)
+  for (Region *r : regions_) r->scatter_tune->finish();
+  wa_tune_->finish();
+}
+
+std::string Engine::tuning() const {
+  std::string s = wa_tune_ ? wa_tune_->report() : std::string();
+  for (size_t b = 0; b < regions_.size(); b++)
+    if (regions_[b]->n_cells) s += "; region " + std::to_string(b) + " " + regions_[b]->scatter_tune->report();
+  return s;
 }
 
 int64_t Engine::hpwl() {
@@ -579,7 +604,7 @@ int64_t Engine::hpwl() {
     launches += 1;
     WaArgs wh = w;
     wh.hpwl_out = hpwl_acc_;
-    launch_wa_small(wh, 0.0f, 0.0f, 0, stream_);
+    launch_wa_small(wh, 0.0f, 0.0f, 0, stream_, wa_tune_->best());
   }
   if (n_tiles_) {
     launches += 1;

@@ -3,6 +3,7 @@
 // overflow and gradient sums, the step-length distances and the HPWL, read once per trial.
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -14,6 +15,7 @@ namespace gpl {
 
 struct PoissonPlan;
 struct WaArgs;
+class Tuner;
 
 // What the device needs of one region (a `NesterovBase`'s bin grid).
 struct RegionSetup {
@@ -117,6 +119,9 @@ class Engine {
     overlap_ = on;
   }
   int profile_read(double *ms, int64_t *launches, int cap);
+  // The tuners' choices and their candidates' median times: the small nets' WA form, each
+  // region's scatter form.
+  std::string tuning() const;
   bool failed() const { return err_.code != cudaSuccess; }
   const DeviceError &error() const { return err_; }
   void check(cudaError_t e, const char *where);
@@ -170,6 +175,7 @@ class Engine {
   // of a trial, measured); off runs them one after the other.
   cudaStream_t wa_stream_ = nullptr;
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+  std::unique_ptr<Tuner> wa_tune_;
   bool wa_pending_ = false;
   bool overlap_ = true;
   void join();

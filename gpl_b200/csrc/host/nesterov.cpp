@@ -2441,7 +2441,7 @@ int gpl_global_placement(gpl_ctx *ctx, const gpl_design_t *cd, int argc, const c
     progress("design read: %zu instances, %zu nets", run->d.insts.size(), run->d.nets.size());
     run->open(std::vector<std::string>(argv, argv + argc), router);
     run->close();
-    progress("command done");
+    progress("command done (%s)", ctx->eng->tuning().substr(0, 400).c_str());
   });
   run->res.h2d = ctx->eng->h2d_bytes;
   run->res.d2h = ctx->eng->d2h_bytes;
@@ -2517,6 +2517,12 @@ void gpl_session_counters(gpl_session *s, int64_t out[6]) {
   out[3] = s->run->P ? (int64_t)s->run->P->gcell_of_dev.size() : 0;
   out[4] = s->ctx->eng->trials;
   out[5] = s->ctx->eng->reorders;
+}
+
+int gpl_session_tuning(gpl_session *s, char *buf, int cap) {
+  const std::string t = s->ctx->eng->tuning();
+  if (buf && cap > 0) std::snprintf(buf, (size_t)cap, "%s", t.c_str());
+  return (int)t.size();
 }
 
 void gpl_session_discard(gpl_session *s) {

@@ -883,7 +883,7 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
     device(dev.update(), "initial placement update");
     if ((double)error_max <= 1e-5 && iter >= 5) break;
   }
-  progress("initial placement rounds done");
+  progress("initial placement rounds done (%s)", dev.tuning().c_str());
   // the placed instances, their database boxes and their pins back on the host
   std::vector<int4> box, db_box;
   device(dev.download(box, db_box), "initial placement download");

@@ -871,14 +871,10 @@ cudaError_t IpDevice::slice(Axis &A) {
 }
 
 cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
-  // GPL_SPMV_FORM (0 rows, 1 tiled, 2 sliced) fixes the SpMV form instead of timing them:
-  // the forms give the same products bit for bit, so it changes only the speed
-  if (spmv_form_ < 0)
-    if (const char *f = std::getenv("GPL_SPMV_FORM"))
-      if (f[0] >= '0' && f[0] <= '2' && f[1] == 0) spmv_form_ = f[0] - '0';
-  // the sliced copies when the sliced form may run: before the first solve picks a form, and
-  // while it is the form picked
-  const bool sliced = spmv_form_ < 0 || spmv_form_ == kSpmvSliced;
+  // the forms give the same products bit for bit, so the choice changes only the speed
+  if (!spmv_tune_) spmv_tune_ = std::make_unique<Tuner>("initial placement SpMV", std::vector<std::string>{"0", "1", "2"}, "GPL_SPMV_FORM", 2, 48);
+  // the sliced copies whenever the sliced form may run
+  const bool sliced = !spmv_tune_->fixed() || spmv_tune_->best() == kSpmvSliced;
   if (sliced)
     for (Axis &A : ax_) CK(slice(A));
   CsrDev m[2];
@@ -899,14 +895,11 @@ cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
     x[a] = A.x;
     scratch[a] = (char *)scratch_ + a * scratch_bytes_;
   }
-  if (spmv_form_ < 0) {
-    CK(bicgstab_pick_spmv(m[0], x[0], scratch[0], s_, &spmv_form_));
-    launches += 8;
-  }
   BicgResult r[2]{};
-  cudaError_t e = bicgstab_solve_pair(m, b, x, max_iters, scratch, s_, r, spmv_form_);
+  Tuner *t = spmv_tune_->fixed() ? nullptr : spmv_tune_.get();
+  cudaError_t e = bicgstab_solve_pair(m, b, x, max_iters, scratch, s_, r, spmv_tune_->best(), t);
   const int iters = std::max(r[0].iterations, r[1].iterations);
-  launches += 10 + (int64_t)iters * 7;
+  launches += 10 + (int64_t)iters * 5;
   d2h_bytes += (int64_t)(iters / 8 + 2) * 2 * 120;
   out[0].solve = r[0];
   out[1].solve = r[1];

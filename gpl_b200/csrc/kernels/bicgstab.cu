@@ -11,6 +11,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "tune.h"
 
 namespace gpl {
 
@@ -580,32 +581,6 @@ cudaError_t spmv(const CsrDev &A, const float *x, float *y, int form, cudaStream
   return cudaGetLastError();
 }
 
-cudaError_t bicgstab_pick_spmv(const CsrDev &A, const float *x, void *scratch, cudaStream_t st, int *form) {
-  *form = kSpmvRows;
-  if (A.n <= 0) return cudaSuccess;
-  int eb = (int)((A.n + kThreads - 1) / kThreads);
-  float *y = (float *)scratch;  // the first scratch vector
-  cudaEvent_t ev[2];
-  for (auto &e : ev)
-    if (cudaEventCreate(&e) != cudaSuccess) return cudaGetLastError();
-  float ms[3] = {0, 0, 0};
-  const int forms = A.sl_start && A.sl_row && A.sl_len ? 3 : 2;
-  cudaError_t err = cudaSuccess;
-  for (int f = 0; f < forms && err == cudaSuccess; f++) {
-    spmv_launch(f, eb, st, A, x, y, nullptr, kAlways);  // warm
-    cudaEventRecord(ev[0], st);
-    for (int r = 0; r < 3; r++) spmv_launch(f, eb, st, A, x, y, nullptr, kAlways);
-    cudaEventRecord(ev[1], st);
-    err = cudaEventSynchronize(ev[1]);
-    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms[f], ev[0], ev[1]);
-  }
-  for (auto &e : ev) cudaEventDestroy(e);
-  if (err == cudaSuccess)
-    for (int f = 1; f < forms; f++)
-      if (ms[f] < ms[*form]) *form = f;
-  return err != cudaSuccess ? err : cudaGetLastError();
-}
-
 cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_iters, void *scratch, cudaStream_t st, BicgResult *out, int form) {
   static_assert(S_END <= S_TICKET && S_TICKET < 64, "the scalars fit the scratch's 64 doubles");
   if (form == kSpmvSliced && (!A.sl_start || !A.sl_row || !A.sl_len)) return cudaErrorInvalidValue;
@@ -685,11 +660,11 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
   return cudaGetLastError();
 }
 
-cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], float *const x[2], int max_iters, void *const scratch[2], cudaStream_t st, BicgResult out[2], int form) {
+cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], float *const x[2], int max_iters, void *const scratch[2], cudaStream_t st, BicgResult out[2], int form, Tuner *tune) {
   const int64_t n = A[0].n;
   if (A[1].n != n) return cudaErrorInvalidValue;
   for (int a = 0; a < 2; a++)
-    if (form == kSpmvSliced && (!A[a].sl_start || !A[a].sl_row || !A[a].sl_len)) return cudaErrorInvalidValue;
+    if ((form == kSpmvSliced || tune) && (!A[a].sl_start || !A[a].sl_row || !A[a].sl_len)) return cudaErrorInvalidValue;
   const size_t vec = ((size_t)n * sizeof(float) + 255) / 256 * 256;
   SysPair P{};
   for (int a = 0; a < 2; a++) {
@@ -778,12 +753,13 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
   const dim3 ge(eb, 2), gr(rb, 2);
   const dim3 gs((unsigned)std::max<int64_t>({sliced_blocks(n, A[0].sl_long), sliced_blocks(n, A[1].sl_long), 1}), 2);
   for (;;) {
+    const int f = tune ? tune->start(st) : form;
     for (int k = 0; k < kBicgBatch; k++) {
       k2_update_p<<<ge, kThreads, 0, st>>>(P);
       for (int sel = 0; sel < 2; sel++) {
-        if (form == kSpmvSliced)
+        if (f == kSpmvSliced)
           k2_spmv_sliced_dots<<<gs, kThreads, 0, st>>>(P, sel);
-        else if (form == kSpmvTiled)
+        else if (f == kSpmvTiled)
           k2_spmv_tiled_dots<<<ge, kThreads, 0, st>>>(P, sel);
         else
           k2_spmv_rows_dots<<<ge, kThreads, 0, st>>>(P, sel);
@@ -791,7 +767,10 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
       }
       k2_update_xr<<<gr, kThreads, 0, st>>>(P);
     }
+    if (tune) tune->stop(st);
     if ((e = pull()) != cudaSuccess) return e;
+    // a batch counts for the tuner when both systems ran all of it
+    if (tune) tune->finish(hs[0][S_STATE] == kIterate && hs[1][S_STATE] == kIterate);
     if (hs[0][S_STATE] == kEnded && hs[1][S_STATE] == kEnded) break;
     if (++batches > max_batches) return cudaErrorUnknown;  // cannot happen: the single solve's count
     for (int a = 0; a < 2; a++)

@@ -6,6 +6,8 @@
 
 namespace gpl {
 
+class Tuner;
+
 constexpr int kBicgBlocks = 296;  // two blocks per SM for the reductions
 
 // Rows per slice of the sliced copy of a matrix (below).
@@ -64,9 +66,8 @@ cudaError_t spmv(const CsrDev &A, const float *x, float *y, int form, cudaStream
 // that follow it (the same sums in another fixed order); scratch[a] holds
 // bicgstab_pair_scratch_bytes(n) bytes for system a.
 size_t bicgstab_pair_scratch_bytes(int64_t n);
-cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], float *const x[2], int max_iters, void *const scratch[2], cudaStream_t s, BicgResult out[2], int spmv = kSpmvRows);
-// The fastest SpMV form for A, timed on the device (a few products of x into the scratch);
-// the sliced form competes when A carries its sliced copy.
-cudaError_t bicgstab_pick_spmv(const CsrDev &A, const float *x, void *scratch, cudaStream_t s, int *form);
+// With `tune`, each batch of iterations runs the SpMV form the tuner picks (every form then
+// needs A's sliced copy), timed in place; `spmv` is then the form of the start and restarts.
+cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], float *const x[2], int max_iters, void *const scratch[2], cudaStream_t s, BicgResult out[2], int spmv = kSpmvRows, Tuner *tune = nullptr);
 
 }  // namespace gpl

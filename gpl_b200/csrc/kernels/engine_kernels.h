@@ -28,6 +28,7 @@ struct RegionArgs {
   double inv_size_x, inv_size_y; // 1 / size, rounded (the bin span's fast path)
   int32_t narrow;                // a block's sum into one bin fits 32 bits (the scatter's tile)
   float target_density;
+  int32_t global;                // the scatter adds every addend straight to HBM (no shared tile)
   const int32_t *bx, *by;        // bin edges, nx+1 and ny+1
   const float *scaled;           // bin area * target density (float)
   const float *non_place, *non_place_u;  // the fixed areas (int64) as float, as the density reads them
@@ -90,7 +91,9 @@ int wa_pins_blocks(const WaSmall &s);
 // The degree-2..4 nets' WA (forces != 0) or HPWL alone: k_wa_lean, or k_wa_small / k_wa_pins
 // when the environment sets GPL_WA_SMALL=nets / pins (the same results; a timing comparison).
 __global__ void k_wa_lean(WaArgs w, float cx, float cy, int forces);
-void launch_wa_small(const WaArgs &w, float cx, float cy, int forces, cudaStream_t s);
+// The degree-2..4 nets' WA in one of its three forms (0 k_wa_lean, 1 k_wa_small, 2 k_wa_pins;
+// -1: GPL_WA_SMALL's "nets" / "pins", else the first), which give the same forces and HPWL.
+void launch_wa_small(const WaArgs &w, float cx, float cy, int forces, cudaStream_t s, int form = -1);
 // The degree-2..4 ranges of nets already in degree order.
 WaSmall wa_small_ranges(const int64_t *net_start, int32_t n_nets);
 // k_wa_tiles over every tile: a persistent grid of the blocks the device holds at once.

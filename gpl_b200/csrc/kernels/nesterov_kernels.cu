@@ -228,17 +228,18 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
   const bool narrow = r.narrow != 0;
   const int bcap = narrow ? 2 * kTileBins : kTileBins;
   const int64_t b_nt = (int64_t)(s_box[1] - s_box[0]) * (s_box[3] - s_box[2]);
+  // (with r.global every addend goes straight to HBM; the spread count is the same either way)
   const bool tile = s_box[1] > s_box[0] && s_box[3] > s_box[2] && b_nt <= bcap && b_nt <= 2 * (int64_t)s_box[4];
   unsigned int *t32 = reinterpret_cast<unsigned int *>(s_tile);
-  if (tile) {
+  if (tile && !r.global) {
     tile_scatter<true>(r, narrow, s_tile, t32, s_red, bcap, s_box[0], s_box[2], s_box[3] - s_box[2], s_box[1] - s_box[0], any, x0, x1, y0, y1, dlx, dux, dly, duy, scale, kind);
     return;
   }
-  if (threadIdx.x == 0 && r.spread) atomicAdd(r.spread, 1u);
+  if (!tile && threadIdx.x == 0 && r.spread) atomicAdd(r.spread, 1u);
   const int wcap = bcap / (kThreads / 32);
   const int64_t w_nt = (int64_t)(wx1 - wx0) * (wy1 - wy0);
   const bool wtile = wx1 > wx0 && wy1 > wy0 && w_nt <= wcap && w_nt <= 2 * (int64_t)w_addends;  // warp-uniform
-  if (wtile) {
+  if (wtile && !r.global) {
     const int w = threadIdx.x >> 5;
     tile_scatter<false>(r, narrow, s_tile + (size_t)w * 2 * wcap, t32 + (size_t)w * 2 * wcap, s_red, wcap, wx0, wy0, wy1 - wy0, wx1 - wx0, any, x0, x1, y0, y1, dlx, dux, dly, duy, scale, kind);
     return;
@@ -861,8 +862,8 @@ static int wa_small_form() {
   return 0;
 }
 
-void launch_wa_small(const WaArgs &w, float cx, float cy, int forces, cudaStream_t s) {
-  const int form = wa_small_form();
+void launch_wa_small(const WaArgs &w, float cx, float cy, int forces, cudaStream_t s, int form) {
+  if (form < 0) form = wa_small_form();
   if (form == 2) {
     if (const int nb = wa_pins_blocks(w.small)) k_wa_pins<<<nb, kThreads, 0, s>>>(w, cx, cy, forces);
   } else if (const int nb = wa_small_blocks(w.small)) {

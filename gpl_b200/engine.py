@@ -126,6 +126,7 @@ def _session_lib():
         L.gpl_session_stream.restype = C.c_void_p
         L.gpl_session_stream.argtypes = [C.c_void_p]
         L.gpl_session_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
+        L.gpl_session_tuning.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
         L.gpl_session_close.argtypes = [C.c_void_p, C.POINTER(gpl_result_t)]
         L._session_ready = True
     return L
@@ -164,6 +165,14 @@ class Session:
         out = (C.c_int64 * 6)()
         _session_lib().gpl_session_counters(self._h, out)
         return {"launches": out[0], "h2d_bytes": out[1], "d2h_bytes": out[2], "cells": out[3], "trials": out[4], "reorders": out[5]}
+
+    def tuning(self) -> str:
+        """The autotuner's choices so far and its candidates' median times (text)."""
+        L = _session_lib()
+        n = L.gpl_session_tuning(self._h, None, 0)
+        buf = C.create_string_buffer(n + 1)
+        L.gpl_session_tuning(self._h, buf, n + 1)
+        return buf.value.decode()
 
     @property
     def stream(self):

@@ -22,6 +22,11 @@ generator for every size):
   grid and the first k tiles (row by row) become regions, one group each; a cell joins the
   group whose tile holds its latent position, the rest stay top-level. No fixed instance
   then (a fixed instance against a region's boundary is outside the placer's model).
+* Uneven region groups (`region_cells=(k, lo, hi)`): k cell counts drawn log-uniform in
+  [lo, hi] (seeded; drawn again while they leave under 2 % of the cells to the top level),
+  and the core cut into k + 1 boxes whose areas follow the counts (a squarified treemap on
+  the site/row grid; the last box is the top level's). Since the latent positions are
+  uniform, each region then holds about its drawn count.
 """
 from __future__ import annotations
 
@@ -48,6 +53,11 @@ PRESETS = {
     # multi-region case the parity tests run on both sides.
     "cfg4s": dict(cells=2000, nets=2100, w_min=2, w_max=12, util=0.55, n_io=32,
                   macros=0, macro_frac=0.0, max_degree=16, seed=4, regions=(3, 2, 4)),
+    # 48 region groups of uneven size (log-uniform 2k..200k cells) beside the top level, 2.4M
+    # cells in all, no macro. The placer's own bin-count rule gives each region a grid of
+    # 32..256 bins a side, rising with its count, and the top level 1024 x 1024.
+    "cfg4": dict(cells=2_400_000, nets=2_520_000, w_min=2, w_max=24, util=0.60, n_io=256,
+                 macros=0, macro_frac=0.0, max_degree=64, seed=4, region_cells=(48, 2_000, 200_000)),
     # 2M cells, ~2.1M nets, ~8M pins, as cfg3.
     "cfg5": dict(cells=2_000_000, nets=2_100_000, w_min=2, w_max=24, util=0.60, n_io=256,
                  macros=32, macro_frac=0.15, max_degree=64, seed=5),
@@ -99,6 +109,64 @@ def _place_macros(rng, n, frac, core_w, core_h):
         else:
             raise RuntimeError("could not place the macros without overlap")
     return np.array(boxes, np.int64)
+
+
+def _region_counts(rng, k, lo, hi, total):
+    """k counts log-uniform in [lo, hi] that leave at least 2 % of `total` to the top level."""
+    for _ in range(1000):
+        c = np.exp(rng.uniform(np.log(lo), np.log(hi), k)).astype(np.int64)
+        if c.sum() <= 0.98 * total:
+            return c
+    raise ValueError("region counts do not fit the cell total")
+
+
+def _treemap_boxes(areas, box):
+    """Boxes on the site/row grid whose areas follow `areas`: the squarified treemap (Bruls,
+    Huizing and van Wijk, 2000). Items in falling area fill strips along the shorter side of
+    the box still free, a strip taking items while that does not worsen its worst aspect
+    ratio; each strip's cut and each item's edge inside a strip land on the site/row grid."""
+    order = sorted(range(len(areas)), key=lambda i: -areas[i])
+    out = [None] * len(areas)
+    lx, ly, ux, uy = box
+    left = float(sum(areas))
+
+    def worst(row, side, scale):
+        s = sum(row) * scale
+        t = s / side  # the strip's thickness
+        return max(max(t / (a * scale / t), (a * scale / t) / t) for a in row)
+
+    k = 0
+    while k < len(order):
+        w, h = ux - lx, uy - ly
+        scale = w * h / left  # area units per input unit
+        side = min(w, h)
+        row = [areas[order[k]]]
+        while k + len(row) < len(order) and worst(row + [areas[order[k + len(row)]]], side, scale) <= worst(row, side, scale):
+            row.append(areas[order[k + len(row)]])
+        last = k + len(row) == len(order)
+        frac = sum(row) / left
+        items = order[k:k + len(row)]
+        if w >= h:  # a vertical strip at the left
+            x = ux if last else min(max(lx + int(round(w * frac / SITE_W)) * SITE_W, lx + SITE_W), ux - SITE_W)
+            cum, y0 = 0.0, ly
+            for n, i in enumerate(items):
+                cum += areas[i]
+                y1 = uy if n == len(items) - 1 else min(max(ly + int(round(h * cum / sum(row) / ROW_H)) * ROW_H, y0 + ROW_H), uy - ROW_H)
+                out[i] = (lx, y0, x, y1)
+                y0 = y1
+            lx = x
+        else:  # a horizontal strip at the bottom
+            y = uy if last else min(max(ly + int(round(h * frac / ROW_H)) * ROW_H, ly + ROW_H), uy - ROW_H)
+            cum, x0 = 0.0, lx
+            for n, i in enumerate(items):
+                cum += areas[i]
+                x1 = ux if n == len(items) - 1 else min(max(lx + int(round(w * cum / sum(row) / SITE_W)) * SITE_W, x0 + SITE_W), ux - SITE_W)
+                out[i] = (x0, ly, x1, y)
+                x0 = x1
+            ly = y
+        left -= sum(row)
+        k += len(row)
+    return out
 
 
 def generate(cfg="cfg1", **over) -> Design:
@@ -236,7 +304,24 @@ def generate(cfg="cfg1", **over) -> Design:
     row_site = np.tile(np.array([SITE_W, ROW_H], np.int32), (n_rows, 1))
 
     groups = {}
-    if p.get("regions"):
+    if p.get("region_cells"):
+        k, lo, hi = p["region_cells"]
+        if n_mac:
+            raise ValueError("region groups and fixed macros do not mix")
+        counts_r = _region_counts(np.random.default_rng([p["seed"], 1]), int(k), lo, hi, m)
+        areas = np.r_[counts_r, m - counts_r.sum()].astype(np.float64)
+        boxes = _treemap_boxes(areas, (0, 0, core_w, core_h))
+        inst_group = np.full(n_inst, -1, np.int32)
+        gi = np.full(m, -1, np.int64)
+        for t, (x0, y0, x1, y1) in enumerate(boxes[:k]):
+            gi[(lat_x >= x0) & (lat_x < x1) & (lat_y >= y0) & (lat_y < y1)] = t
+        inst_group[:m] = gi
+        groups = dict(
+            inst_group=inst_group, group_names=[f"region{g}" for g in range(k)],
+            group_region=np.arange(k, dtype=np.int32),
+            region_bound_start=np.arange(k + 1, dtype=np.int32), region_bounds=np.array(boxes[:k], np.int32).reshape(k, 4),
+            region_group_start=np.arange(k + 1, dtype=np.int32), region_groups=np.arange(k, dtype=np.int32))
+    elif p.get("regions"):
         kx, ky, k = p["regions"]
         if n_mac:
             raise ValueError("region groups and fixed macros do not mix")

@@ -193,6 +193,10 @@ int gpl_session_profile(gpl_session *s, double *ms, int64_t *launches, int cap);
  * (`do_back_tracking`'s passes, src/nesterov.rs:2776-2808) and the times the engine sorted its
  * device cells again (the "reorder" option) since the session opened (6 int64). */
 void gpl_session_counters(gpl_session *s, int64_t out[6]);
+/* The engine's autotuner so far, as text: for each tuned launch group (the small nets' WA
+ * form, each region's scatter form) the form in use and its candidates' median times in
+ * microseconds. Writes at most cap bytes (NUL included) to buf; returns the text's length. */
+int gpl_session_tuning(gpl_session *s, char *buf, int cap);
 /* The session's CUDA stream (cudaStream_t), for timing with events on it. */
 void *gpl_session_stream(gpl_session *s);
 int gpl_session_close(gpl_session *s, gpl_result_t *out);

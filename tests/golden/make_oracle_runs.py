@@ -1,5 +1,5 @@
 """Writes tests/golden/oracle_runs.json: the oracle's whole `global_placement` run on the
-100k-cell and 1M-cell synthetic designs, summarised (the report's construction lines, the
+100k-cell, 1M-cell and 2.4M-cell (48 region groups) synthetic designs, summarised (the report's construction lines, the
 `[InitialPlace]` rows, the iteration count, final HPWL and overflow, and a checksum of the
 written placement).
 
@@ -7,7 +7,7 @@ These runs take minutes (100k cells) to about an hour (1M cells) on one CPU thre
 GPU tests compare against this summary instead of re-running the oracle. Run from the
 repository root:
 
-    python tests/golden/make_oracle_runs.py [cfg2] [cfg3] [cfg2_route]
+    python tests/golden/make_oracle_runs.py [cfg2] [cfg3] [cfg2_route] [cfg4]
 """
 import json
 import os
@@ -26,6 +26,8 @@ ARGS = {
     # routability-driven, with the synthetic router: 3000-DBU tiles, one 1200-DBU pitch (so the
     # RUDY map overflows and the passes inflate cells), capacity 20
     "cfg2_route": ["-density", "0.70", "-bin_grid_count", "512", "-routability_driven"],
+    # 48 uneven region groups and the top level, each with the bin grid the placer's rule gives
+    "cfg4": ["-density", "0.70"],
 }
 ROUTER = {"cfg2_route": dict(tile=3000, pitches=(1200,), capacity=20)}
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "oracle_runs.json")
@@ -72,8 +74,11 @@ def main(cfgs):
         res = oracle.global_placement(d, ARGS[cfg], router=router.ptr if router else None)
         out[cfg] = summarise(cfg, res, time.perf_counter() - t0)
         print(cfg, out[cfg]["status"], out[cfg]["nesterov_iterations"], out[cfg]["final_hpwl"], out[cfg]["final_overflow"], flush=True)
+        # merged into the file as it is now (another configuration may have been written since)
+        now = json.load(open(OUT)) if os.path.exists(OUT) else {}
+        now[cfg] = out[cfg]
         with open(OUT, "w") as f:
-            json.dump(out, f, indent=1)
+            json.dump(now, f, indent=1)
 
 
 if __name__ == "__main__":

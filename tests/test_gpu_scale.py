@@ -122,3 +122,27 @@ def test_cell_reorder_keeps_the_run():
     assert a["status"] == b["status"] == "placed"
     assert abs(a["final_hpwl"] - b["final_hpwl"]) <= 1e-3 * b["final_hpwl"]
     assert abs(a["final_overflow"] - b["final_overflow"]) <= 0.005
+
+
+def test_tuned_forms_give_the_same_run(monkeypatch):
+    """The autotuner picks among forms that give the same results bit for bit (the initial
+    placement's SpMV: a thread per row, block-staged, sliced; the scatter: shared tiles or
+    straight to HBM; the small nets' WA: lean, a thread per net, a lane per pin), so the tuned
+    run on the 100k-cell design and runs with each form fixed end identically: the same
+    initial placement rows, iteration count, final HPWL and overflow, and written placement."""
+    d = synth.generate("cfg2")
+    args = ["-density", "0.70", "-bin_grid_count", "512"]
+    base = engine.global_placement(d, args)
+    assert base["status"] == "placed", base["reason"]
+    for fixed in ({"GPL_SPMV_FORM": "0", "GPL_SCATTER": "global", "GPL_WA_SMALL": "nets"},
+                  {"GPL_SPMV_FORM": "2", "GPL_SCATTER": "tiles", "GPL_WA_SMALL": "pins"},
+                  {"GPL_SPMV_FORM": "1", "GPL_SCATTER": "tiles", "GPL_WA_SMALL": "lean"}):
+        for k, v in fixed.items():
+            monkeypatch.setenv(k, v)
+        got = engine.global_placement(d, args)
+        assert got["status"] == "placed", got["reason"]
+        assert ip_hpwl(got["lines"]) == ip_hpwl(base["lines"]), fixed
+        assert got["nesterov_iterations"] == base["nesterov_iterations"], fixed
+        assert got["final_hpwl"] == base["final_hpwl"], fixed
+        assert got["final_overflow"] == base["final_overflow"], fixed
+        assert (got["locations"] == base["locations"]).all(), fixed

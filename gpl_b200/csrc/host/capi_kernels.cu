@@ -42,8 +42,8 @@ int gpl_kernel_density_scatter(int64_t n_cells, const int32_t *cx, const int32_t
     r.narrow = narrow_tile(hbx, hby) ? 1 : 0;
   }
   r.target_density = target_density;
-  // GPL_SCATTER=global: every addend straight to HBM (the engine's tuner picks per region)
-  if (const char *f = std::getenv("GPL_SCATTER")) r.global = std::string(f) == "global" ? 1 : 0;
+  // GPL_SCATTER=global|pooled: the scatter's other forms (the engine's tuner picks per region)
+  if (const char *f = std::getenv("GPL_SCATTER")) r.scatter_form = std::string(f) == "global" ? 1 : std::string(f) == "pooled" ? 2 : 0;
   r.bx = bx;
   r.by = by;
   r.acc_inst = inst;
@@ -89,8 +89,8 @@ static cudaError_t region_args(RegionArgs &r, int64_t n_cells, int32_t nx, int32
   r.uy = hby[ny];
   r.narrow = narrow_tile(hbx, hby) ? 1 : 0;
   r.target_density = target_density;
-  // GPL_SCATTER=global: every addend straight to HBM (the engine's tuner picks per region)
-  if (const char *f = std::getenv("GPL_SCATTER")) r.global = std::string(f) == "global" ? 1 : 0;
+  // GPL_SCATTER=global|pooled: the scatter's other forms (the engine's tuner picks per region)
+  if (const char *f = std::getenv("GPL_SCATTER")) r.scatter_form = std::string(f) == "global" ? 1 : std::string(f) == "pooled" ? 2 : 0;
   r.bx = bx;
   r.by = by;
   return cudaSuccess;

@@ -37,9 +37,9 @@ struct Engine::Region {
   double spread_base = 0;          // the spread blocks of the order as made
   bool need_base = true;           // the next scatter's count is that base
   int64_t reorder_trial = -1000;   // the trial of the last reorder
-  // the scatter's form (shared tiles, or straight to HBM: the same int64 sums either way),
-  // timed in place; GPL_SCATTER=tiles|global fixes it
-  std::unique_ptr<Tuner> scatter_tune = std::make_unique<Tuner>("scatter", std::vector<std::string>{"tiles", "global"}, "GPL_SCATTER", 3, 128);
+  // the scatter's form (shared tiles, straight to HBM, or straight to HBM pooled by bin: the
+  // same int64 sums every way), timed in place; GPL_SCATTER=tiles|global|pooled fixes it
+  std::unique_ptr<Tuner> scatter_tune = std::make_unique<Tuner>("scatter", std::vector<std::string>{"tiles", "global", "pooled"}, "GPL_SCATTER", 3, 64);
 };
 
 static int blocks_for(int64_t n, int per = kThreadsPerBlock) { return (int)std::max<int64_t>(1, (n + per - 1) / per); }
@@ -406,7 +406,7 @@ void Engine::place_at(int b, SlotId slot) {
   ph_begin(PH_PLACE);
   launches += (r->n_cells ? 1 : 0) + 1;
   RegionArgs a = r->args;
-  a.global = r->scatter_tune->best();
+  a.scatter_form = r->scatter_tune->best();
   if (r->n_cells) k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(a, c, PLACE_AT, 0.0f, 0.0f, r->slot[slot]);
   ph_end(PH_PLACE);
   ph_begin(PH_FINALIZE);
@@ -441,7 +441,7 @@ void Engine::nesterov_step(int b, float step, float coeff) {
   launches += (r->n_cells ? 1 : 0) + 1;
   if (r->n_cells) {
     RegionArgs a = r->args;
-    a.global = r->scatter_tune->start(stream_);
+    a.scatter_form = r->scatter_tune->start(stream_);
     k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(a, c, PLACE_NESTEROV, step, coeff, nullptr);
     r->scatter_tune->stop(stream_);
   }

@@ -13,6 +13,7 @@
 
 #include "b2b.h"
 #include "common.cuh"
+#include "engine_kernels.h"
 
 namespace gpl {
 
@@ -514,6 +515,43 @@ __global__ void k_scan_add(int64_t *data, int64_t n, const int64_t *totals, int6
   if (i == 0) data[n] = totals[nb];
 }
 
+// ---- the solver's row order
+// Row i' of the renumbered system is row perm[i'] with its entries in their own order and each
+// column j renumbered inv[j], so each product y'[i'] sums the same terms in the same order as
+// y[perm[i']]; only the cross-row sums (the inner products) see their terms in another order.
+__global__ void k_perm_len(int64_t n, const int32_t *__restrict__ perm, const int64_t *__restrict__ starts, int64_t *__restrict__ len) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t r = perm[i];
+  len[i] = starts[r + 1] - starts[r];
+}
+__global__ void k_perm_inv(int64_t n, const int32_t *__restrict__ perm, int32_t *__restrict__ inv) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) inv[perm[i]] = (int32_t)i;
+}
+// A warp per row: the row's entries copied in order, 32 at a time.
+__global__ void k_perm_rows(int64_t n, const int32_t *__restrict__ perm, const int32_t *__restrict__ inv, const int64_t *__restrict__ starts, const int32_t *__restrict__ cols, const float *__restrict__ vals,
+                            const int64_t *__restrict__ pstarts, int32_t *__restrict__ pcols, float *__restrict__ pvals) {
+  const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= n) return;
+  const int32_t r = perm[w];
+  const int64_t s0 = starts[r], len = starts[r + 1] - s0, d0 = pstarts[w];
+  for (int64_t k = lane; k < len; k += 32) {
+    pcols[d0 + k] = inv[cols[s0 + k]];
+    pvals[d0 + k] = vals[s0 + k];
+  }
+}
+// out[i'] = in[perm[i']] (into the solver's order), and back: out[perm[i']] = in[i'].
+__global__ void k_perm_gather(int64_t n, const int32_t *__restrict__ perm, const float *__restrict__ in, float *__restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[perm[i]];
+}
+__global__ void k_perm_scatter(int64_t n, const int32_t *__restrict__ perm, const float *__restrict__ in, float *__restrict__ out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[perm[i]] = in[i];
+}
+
 // ---- updateCoordi (src/initial_place.rs:391-417) and setCenterLocation (:152-165)
 __global__ void k_update(int64_t n, const float *x, const float *y, int4 core, const int4 *region, const uint8_t *grouped, const uint8_t *locked, int4 *box, int4 *db_box, const int2 *db_size) {
   int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -624,8 +662,13 @@ void IpDevice::release() {
                   net_start_, cnt_, scan_tmp_, t_row_, t_col_, t_val_, r_row_, r_val_, bucket_, fill_, row_off_, ucount_, ucol_, uval_, scratch_, hpwl_acc_, tier_rows_, tier_n_};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, s_);
+  for (void *p : {(void *)perm_, (void *)inv_, (void *)ord_idx_, (void *)ord_hist_, (void *)ord_key0_, (void *)ord_key1_})
+    if (p) cudaFreeAsync(p, s_);
+  perm_ = inv_ = ord_idx_ = ord_hist_ = nullptr;
+  ord_key0_ = ord_key1_ = nullptr;
+  solves_ = 0;
   for (auto &a : ax_) {
-    void *q[] = {a.starts, a.cols, a.vals, a.rhs, a.x, a.sl_row, a.sl_len, a.sl_count, a.sl_start, a.sl_ent};
+    void *q[] = {a.starts, a.cols, a.vals, a.rhs, a.x, a.sl_row, a.sl_len, a.sl_count, a.sl_start, a.sl_ent, a.p_starts, a.p_cols, a.p_vals, a.p_rhs, a.p_x};
     for (void *p : q)
       if (p) cudaFreeAsync(p, s_);
     a = Axis{};
@@ -843,10 +886,9 @@ cudaError_t IpDevice::assemble(IpAxisResult out[2]) {
 // The sliced copy: the rows in order of length and the count of long rows read back, the
 // slice widths of the rest, their scan (the starts), the total read back to size the
 // entries, then the entries.
-cudaError_t IpDevice::slice(Axis &A) {
+cudaError_t IpDevice::slice(Axis &A, CsrDev m) {
   CK(grow(s_, (size_t)std::max<int64_t>(n_, 1), A.sl_row_cap, &A.sl_row, &A.sl_len));
   CK(grow(s_, (size_t)kSliceLenCap + 1, A.sl_count_cap, &A.sl_count));
-  CsrDev m{n_, A.starts, A.cols, A.vals};
   CK(csr_slice_order(m, A.sl_row, A.sl_len, A.sl_count, s_));
   int32_t n_long = 0;
   CK(cudaMemcpyAsync(&n_long, A.sl_count + kSliceLongRow + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
@@ -870,29 +912,71 @@ cudaError_t IpDevice::slice(Axis &A) {
   return cudaSuccess;
 }
 
+// The rows sorted by the Hilbert index of their centres (the solve's start point) on a
+// 1024 x 1024 grid over the core, and each axis's system and vectors renumbered.
+cudaError_t IpDevice::solver_order() {
+  const int64_t n = n_;
+  if (!perm_) {
+    const size_t tiles = (size_t)order_tiles((int32_t)n);
+    CK(alloc(&perm_, (size_t)n, s_));
+    CK(alloc(&inv_, (size_t)n, s_));
+    CK(alloc(&ord_idx_, (size_t)n, s_));
+    CK(alloc(&ord_hist_, 64 * tiles, s_));
+    CK(alloc(&ord_key0_, (size_t)n, s_));
+    CK(alloc(&ord_key1_, (size_t)n, s_));
+  }
+  const int4 c = cfg_.core;
+  const double tw = std::max(1.0, (double)(c.z - c.x) / 1024.0), th = std::max(1.0, (double)(c.w - c.y) / 1024.0);
+  CK(order_sort_xy((int32_t)n, ax_[0].x, ax_[1].x, (double)c.x, (double)c.y, tw, th, ord_key0_, perm_, ord_key1_, ord_idx_, ord_hist_, s_));
+  k_perm_inv<<<grid(n), kThreads, 0, s_>>>(n, perm_, inv_);
+  launches += 14;
+  for (Axis &A : ax_) {
+    CK(grow(s_, (size_t)std::max<int64_t>(A.nnz, 1), A.p_cap, &A.p_cols, &A.p_vals));
+    if (!A.p_starts) {
+      CK(alloc(&A.p_starts, (size_t)n + 1, s_));
+      CK(alloc(&A.p_rhs, (size_t)n, s_));
+      CK(alloc(&A.p_x, (size_t)n, s_));
+    }
+    k_perm_len<<<grid(n), kThreads, 0, s_>>>(n, perm_, A.starts, A.p_starts);
+    CK(scan(A.p_starts, n));
+    k_perm_rows<<<grid(n * 32), kThreads, 0, s_>>>(n, perm_, inv_, A.starts, A.cols, A.vals, A.p_starts, A.p_cols, A.p_vals);
+    k_perm_gather<<<grid(n), kThreads, 0, s_>>>(n, perm_, A.rhs, A.p_rhs);
+    k_perm_gather<<<grid(n), kThreads, 0, s_>>>(n, perm_, A.x, A.p_x);
+    launches += 7;
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
   // the forms give the same products bit for bit, so the choice changes only the speed
   if (!spmv_tune_) spmv_tune_ = std::make_unique<Tuner>("initial placement SpMV", std::vector<std::string>{"0", "1", "2"}, "GPL_SPMV_FORM", 2, 48);
+  if (ip_order_ < 0) {
+    const char *f = std::getenv("GPL_IP_ORDER");
+    ip_order_ = f && f[0] == '0' ? 0 : 1;
+  }
+  // the first solve starts every row at one point (the core centre): no order to take yet
+  const bool ordered = ip_order_ && solves_ > 0 && n_ > 0;
+  solves_++;
+  if (ordered) CK(solver_order());
   // the sliced copies whenever the sliced form may run
   const bool sliced = !spmv_tune_->fixed() || spmv_tune_->best() == kSpmvSliced;
-  if (sliced)
-    for (Axis &A : ax_) CK(slice(A));
   CsrDev m[2];
   const float *b[2];
   float *x[2];
   void *scratch[2];
   for (int a = 0; a < 2; a++) {
     Axis &A = ax_[a];
-    m[a] = CsrDev{n_, A.starts, A.cols, A.vals};
+    m[a] = ordered ? CsrDev{n_, A.p_starts, A.p_cols, A.p_vals} : CsrDev{n_, A.starts, A.cols, A.vals};
     if (sliced) {
+      CK(slice(A, m[a]));
       m[a].sl_long = A.sl_long;
       m[a].sl_row = A.sl_row;
       m[a].sl_len = A.sl_len;
       m[a].sl_start = A.sl_start;
       m[a].sl_ent = A.sl_ent;
     }
-    b[a] = A.rhs;
-    x[a] = A.x;
+    b[a] = ordered ? A.p_rhs : A.rhs;
+    x[a] = ordered ? A.p_x : A.x;
     scratch[a] = (char *)scratch_ + a * scratch_bytes_;
   }
   BicgResult r[2]{};
@@ -903,6 +987,11 @@ cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
   d2h_bytes += (int64_t)(iters / 8 + 2) * 2 * 120;
   out[0].solve = r[0];
   out[1].solve = r[1];
+  if (e == cudaSuccess && ordered) {
+    for (Axis &A : ax_) k_perm_scatter<<<grid(n_), kThreads, 0, s_>>>(n_, perm_, A.p_x, A.x);
+    launches += 2;
+    e = cudaGetLastError();
+  }
   return e;
 }
 

@@ -119,14 +119,27 @@ class IpDevice {
     int64_t *sl_start = nullptr;
     int2 *sl_ent = nullptr;
     size_t sl_cap = 0, sl_start_cap = 0, sl_row_cap = 0, sl_count_cap = 0;
+    // the system in the solver's row order (see solve): rows, columns and vectors renumbered
+    int64_t *p_starts = nullptr;
+    int32_t *p_cols = nullptr;
+    float *p_vals = nullptr, *p_rhs = nullptr, *p_x = nullptr;
+    size_t p_cap = 0;
   } ax_[2];
+  // The solver's row order: perm_[i'] = the row solved as row i', inv_ its inverse; sorted
+  // again each round by the Hilbert index of the rows' centres (the start point), so a warp's
+  // rows gather their x entries from a compact patch (off: GPL_IP_ORDER=0).
+  int32_t *perm_ = nullptr, *inv_ = nullptr, *ord_idx_ = nullptr, *ord_hist_ = nullptr;
+  uint32_t *ord_key0_ = nullptr, *ord_key1_ = nullptr;
+  int64_t solves_ = 0;
+  int ip_order_ = -1;
+  cudaError_t solver_order();
   void *scratch_ = nullptr;
   size_t scratch_bytes_ = 0;
   int64_t *hpwl_acc_ = nullptr;
   void release();
   cudaError_t collapse(int64_t n_trip, const int32_t *row, const int32_t *col, const float *val, int64_t *starts_out, int32_t **cols, float **vals, size_t *cap, int64_t *nnz);
   cudaError_t scan(int64_t *data, int64_t n);
-  cudaError_t slice(Axis &A);  // the axis's sliced copy, from its CSR arrays
+  cudaError_t slice(Axis &A, CsrDev m);  // the axis's sliced copy of m (its CSR, as solved)
 };
 
 }  // namespace gpl

@@ -195,13 +195,37 @@ __global__ void k_iota(int32_t n, int32_t *__restrict__ a) {
   if (i < n) a[i] = i;
 }
 
+// The same key from float centres (the initial placement's solution vectors).
+__global__ void k_order_keys_xy(int32_t n, const float *__restrict__ x, const float *__restrict__ y, double lx, double ly, double tile_w, double tile_h, uint32_t *__restrict__ key, int32_t *__restrict__ idx) {
+  const int32_t i = blockIdx.x * kThreads + threadIdx.x;
+  if (i >= n) return;
+  const double hi = (double)((1 << kOrderBits) - 1);
+  const double fx = ((double)x[i] - lx) / tile_w, fy = ((double)y[i] - ly) / tile_h;
+  // a NaN centre takes key 0 (fmax and fmin return the number)
+  key[i] = hilbert((uint32_t)fmin(fmax(fx, 0.0), hi), (uint32_t)fmin(fmax(fy, 0.0), hi));
+  idx[i] = i;
+}
+
 int order_tiles(int32_t n) { return (n + kTile - 1) / kTile; }
+
+static cudaError_t order_passes(int32_t n, uint32_t *key0, int32_t *idx0, uint32_t *key1, int32_t *idx1, int32_t *hist, cudaStream_t s);
 
 cudaError_t order_sort(int32_t n, const int2 *dc, int32_t lx, int32_t ly, double tile_w, double tile_h, uint32_t *key0, int32_t *idx0, uint32_t *key1, int32_t *idx1, int32_t *hist, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  const int32_t tiles = order_tiles(n);
   const unsigned eb = (unsigned)((n + kThreads - 1) / kThreads);
   k_order_keys<<<eb, kThreads, 0, s>>>(n, dc, lx, ly, tile_w, tile_h, key0, idx0);
+  return order_passes(n, key0, idx0, key1, idx1, hist, s);
+}
+
+cudaError_t order_sort_xy(int32_t n, const float *x, const float *y, double lx, double ly, double tile_w, double tile_h, uint32_t *key0, int32_t *idx0, uint32_t *key1, int32_t *idx1, int32_t *hist, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  const unsigned eb = (unsigned)((n + kThreads - 1) / kThreads);
+  k_order_keys_xy<<<eb, kThreads, 0, s>>>(n, x, y, lx, ly, tile_w, tile_h, key0, idx0);
+  return order_passes(n, key0, idx0, key1, idx1, hist, s);
+}
+
+static cudaError_t order_passes(int32_t n, uint32_t *key0, int32_t *idx0, uint32_t *key1, int32_t *idx1, int32_t *hist, cudaStream_t s) {
+  const int32_t tiles = order_tiles(n);
   for (int pass = 0; pass < kPasses; pass++) {
     const int shift = 6 * pass;
     const bool odd = pass & 1;

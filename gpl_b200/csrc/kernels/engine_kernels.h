@@ -28,7 +28,9 @@ struct RegionArgs {
   double inv_size_x, inv_size_y; // 1 / size, rounded (the bin span's fast path)
   int32_t narrow;                // a block's sum into one bin fits 32 bits (the scatter's tile)
   float target_density;
-  int32_t global;                // the scatter adds every addend straight to HBM (no shared tile)
+  // the scatter's form: 0 shared tiles (a block's or a warp's, else straight to HBM); 1 every
+  // addend straight to HBM; 2 straight to HBM, a warp's lanes that hit one bin pooled first
+  int32_t scatter_form;
   const int32_t *bx, *by;        // bin edges, nx+1 and ny+1
   const float *scaled;           // bin area * target density (float)
   const float *non_place, *non_place_u;  // the fixed areas (int64) as float, as the density reads them
@@ -130,6 +132,9 @@ int order_tiles(int32_t n);
 // of tile_w x tile_h cells from (lx, ly); the old indices in new order end in idx0
 // (key0/key1/idx1: n each; hist: 64 * order_tiles(n)).
 cudaError_t order_sort(int32_t n, const int2 *dc, int32_t lx, int32_t ly, double tile_w, double tile_h, uint32_t *key0, int32_t *idx0, uint32_t *key1, int32_t *idx1, int32_t *hist, cudaStream_t s);
+// The same sort of n float centres (x[i], y[i]) over the box from (lx, ly), tile_w x tile_h a
+// grid step.
+cudaError_t order_sort_xy(int32_t n, const float *x, const float *y, double lx, double ly, double tile_w, double tile_h, uint32_t *key0, int32_t *idx0, uint32_t *key1, int32_t *idx1, int32_t *hist, cudaStream_t s);
 __global__ void k_order_gather(int32_t n, const int32_t *perm, CellGather g);
 __global__ void k_order_pins(int64_t n_pins, int32_t off, int32_t n, const int32_t *inv, const int64_t *old_start, const int64_t *new_start, int32_t *pin_cell, int32_t *pin_slot);
 __global__ void k_order_starts(int32_t n, const int64_t *rel, int64_t *start);

@@ -143,6 +143,52 @@ __device__ __forceinline__ void tile_scatter(const RegionArgs &r, bool narrow, u
   }
 }
 
+// Every addend straight to the HBM accumulators, the warp's lanes walking their cells' bins in
+// step (x outer, y inner) and lanes that hit the same bin in a step pooling their addends first
+// (one global atomic per distinct bin and step): the form for cells piled on few bins, where
+// the atomics on one address would queue. Integer adds throughout.
+__device__ __forceinline__ void pooled_scatter(const RegionArgs &r, bool narrow, unsigned long long *s_red, bool any, int32_t x0, int32_t x1, int32_t y0, int32_t y1, int32_t dlx, int32_t dux,
+                                               int32_t dly, int32_t duy, float scale, uint8_t kind) {
+  const int lane = threadIdx.x & 31;
+  const int nb = any ? (x1 - x0) * (y1 - y0) : 0;
+  const int rounds = __reduce_max_sync(0xffffffffu, nb);
+  unsigned long long *acc = (unsigned long long *)(kind == CELL_FILLER ? r.acc_fill : r.acc_inst);
+  int32_t x = x0, y = y0;
+  for (int q = 0; q < rounds; q++) {
+    long long key = -1;  // the accumulator slot, fillers' apart
+    unsigned long long v = 0;
+    size_t at = 0;
+    if (q < nb) {
+      const int64_t a = cell_bin_addend(r, dlx, dux, dly, duy, x, y, scale, kind);
+      if (a) {
+        v = (unsigned long long)a;
+        at = (size_t)x * r.ny + y;
+        key = ((long long)at << 1) | (kind == CELL_FILLER ? 1 : 0);
+      }
+      if (++y == y1) {
+        y = y0;
+        x++;
+      }
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const bool lead = key >= 0 && lane == __ffs(peers) - 1;
+    if (narrow) {
+      // a block's sum for one bin stays below 2^32, so a warp's does
+      const unsigned sum = __reduce_add_sync(peers, (unsigned)v);
+      if (lead) atomicAdd(&acc[at], (unsigned long long)sum);
+    } else {
+      s_red[threadIdx.x] = v;
+      __syncwarp();
+      if (lead) {
+        unsigned long long sum = 0;
+        for (unsigned m = peers; m; m &= m - 1) sum += s_red[(threadIdx.x & ~31) + __ffs(m) - 1];
+        atomicAdd(&acc[at], sum);
+      }
+      __syncwarp();
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
   __shared__ __align__(16) unsigned long long s_tile[2 * kTileBins];  // cells then fillers; 32-bit when narrow
   __shared__ unsigned long long s_red[kThreads];
@@ -228,10 +274,11 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
   const bool narrow = r.narrow != 0;
   const int bcap = narrow ? 2 * kTileBins : kTileBins;
   const int64_t b_nt = (int64_t)(s_box[1] - s_box[0]) * (s_box[3] - s_box[2]);
-  // (with r.global every addend goes straight to HBM; the spread count is the same either way)
+  // (the other forms add straight to HBM; the spread count is the same in every form)
   const bool tile = s_box[1] > s_box[0] && s_box[3] > s_box[2] && b_nt <= bcap && b_nt <= 2 * (int64_t)s_box[4];
   unsigned int *t32 = reinterpret_cast<unsigned int *>(s_tile);
-  if (tile && !r.global) {
+  const bool tiles = r.scatter_form == 0;
+  if (tile && tiles) {
     tile_scatter<true>(r, narrow, s_tile, t32, s_red, bcap, s_box[0], s_box[2], s_box[3] - s_box[2], s_box[1] - s_box[0], any, x0, x1, y0, y1, dlx, dux, dly, duy, scale, kind);
     return;
   }
@@ -239,9 +286,13 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
   const int wcap = bcap / (kThreads / 32);
   const int64_t w_nt = (int64_t)(wx1 - wx0) * (wy1 - wy0);
   const bool wtile = wx1 > wx0 && wy1 > wy0 && w_nt <= wcap && w_nt <= 2 * (int64_t)w_addends;  // warp-uniform
-  if (wtile && !r.global) {
+  if (wtile && tiles) {
     const int w = threadIdx.x >> 5;
     tile_scatter<false>(r, narrow, s_tile + (size_t)w * 2 * wcap, t32 + (size_t)w * 2 * wcap, s_red, wcap, wx0, wy0, wy1 - wy0, wx1 - wx0, any, x0, x1, y0, y1, dlx, dux, dly, duy, scale, kind);
+    return;
+  }
+  if (r.scatter_form == 2) {
+    pooled_scatter(r, narrow, s_red, any, x0, x1, y0, y1, dlx, dux, dly, duy, scale, kind);
     return;
   }
   if (any) {

@@ -37,11 +37,12 @@ def random_cells(rng, n, bx, by, macro_frac=0.02, filler_frac=0.2):
 
 
 # (8, 8): bins so large that the scatter's shared tile sums in 64 bits
-@pytest.mark.parametrize("form", ["tiles", "global"])
+@pytest.mark.parametrize("form", ["tiles", "global", "pooled"])
 @pytest.mark.parametrize("nx,ny,aligned", [(64, 64, False), (96, 40, False), (64, 64, True), (40, 80, True), (8, 8, False)])
 def test_density_scatter_bit_exact(L, nx, ny, aligned, form, monkeypatch):
-    """Both scatter forms (shared tiles, the default; every addend straight to HBM with
-    GPL_SCATTER=global) against the oracle's int64 bin sums."""
+    """The scatter's three forms (shared tiles, the default; every addend straight to HBM with
+    GPL_SCATTER=global; straight to HBM pooled by bin within a warp with GPL_SCATTER=pooled)
+    against the oracle's int64 bin sums."""
     monkeypatch.setenv("GPL_SCATTER", form)
     rng = np.random.default_rng(nx * 1000 + ny + aligned)
     if aligned:

@@ -127,7 +127,7 @@ def test_cell_reorder_keeps_the_run():
 def test_tuned_forms_give_the_same_run(monkeypatch):
     """The autotuner picks among forms that give the same results bit for bit (the initial
     placement's SpMV: a thread per row, block-staged, sliced; the scatter: shared tiles or
-    straight to HBM; the small nets' WA: lean, a thread per net, a lane per pin), so the tuned
+    straight to HBM, alone or pooled by bin; the small nets' WA: lean, a thread per net, a lane per pin), so the tuned
     run on the 100k-cell design and runs with each form fixed end identically: the same
     initial placement rows, iteration count, final HPWL and overflow, and written placement."""
     d = synth.generate("cfg2")
@@ -135,7 +135,7 @@ def test_tuned_forms_give_the_same_run(monkeypatch):
     base = engine.global_placement(d, args)
     assert base["status"] == "placed", base["reason"]
     for fixed in ({"GPL_SPMV_FORM": "0", "GPL_SCATTER": "global", "GPL_WA_SMALL": "nets"},
-                  {"GPL_SPMV_FORM": "2", "GPL_SCATTER": "tiles", "GPL_WA_SMALL": "pins"},
+                  {"GPL_SPMV_FORM": "2", "GPL_SCATTER": "pooled", "GPL_WA_SMALL": "pins"},
                   {"GPL_SPMV_FORM": "1", "GPL_SCATTER": "tiles", "GPL_WA_SMALL": "lean"}):
         for k, v in fixed.items():
             monkeypatch.setenv(k, v)

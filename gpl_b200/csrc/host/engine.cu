@@ -42,6 +42,21 @@ struct Engine::Region {
   std::unique_ptr<Tuner> scatter_tune = std::make_unique<Tuner>("scatter", std::vector<std::string>{"tiles", "global", "pooled"}, "GPL_SCATTER", 3, 64);
 };
 
+struct Engine::QueueEntry {
+  int kind;
+  int region;
+  PackedRegion e;  // the phase's arguments as queued (the slots as they were then)
+};
+
+// Page-locked table slots between two trial reads (each packed launch's tables in a slot of
+// their own, as the copies out of them may still be queued).
+constexpr int kTableSlots = 8;
+
+// A region's density solver: the split-BF16 tensor-core form takes grids of at least 512 bins
+// a side; a smaller grid's GEMMs are a few tiles each, too few to fill the tensor cores, so it
+// runs the FP32 form (which packed launches then solve with every other such region at once).
+static int region_plan_mode(int mode, int nx, int ny) { return mode == 1 && (nx < 512 || ny < 512) ? 0 : mode; }
+
 static int blocks_for(int64_t n, int per = kThreadsPerBlock) { return (int)std::max<int64_t>(1, (n + per - 1) / per); }
 
 // Whether the scatter's shared tile can sum in 32 bits: a cell adds at most a bin's area to a
@@ -82,6 +97,8 @@ Engine::Engine(int device) : device_(device) {
   if (!failed()) check(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming), "cudaEventCreate");
   // the degree-2..4 nets' WA form, timed in place; GPL_WA_SMALL=lean|nets|pins fixes it
   if (!failed()) wa_tune_ = std::make_unique<Tuner>("small-net WA", std::vector<std::string>{"lean", "nets", "pins"}, "GPL_WA_SMALL", 3, 256);
+  if (!failed()) pk_scatter_tune_ = std::make_unique<Tuner>("packed scatter", std::vector<std::string>{"tiles", "global", "pooled"}, "GPL_SCATTER", 3, 64);
+  queue_ = new std::vector<QueueEntry>();
 }
 
 void Engine::join() {
@@ -92,6 +109,9 @@ void Engine::join() {
 
 Engine::~Engine() {
   release();
+  delete queue_;
+  if (pk_host_) cudaFreeHost(pk_host_);
+  if (pk_dev_) cudaFree(pk_dev_);
   if (pinned_) cudaFreeHost(pinned_);
   if (wa_stream_) cudaStreamSynchronize(wa_stream_);
   if (stream_) cudaStreamDestroy(stream_);
@@ -138,7 +158,11 @@ void Engine::free_globals() {
 }
 
 void Engine::release() {
+  flush();
   join();
+  poisson_group_destroy(group_);
+  group_ = nullptr;
+  group_set_.clear();
   for (Region *r : regions_) {
     void *ptrs[] = {r->bx, r->by, r->scaled, r->density, r->fx, r->fy, r->np, r->npu, r->acc_inst, r->acc_fill, r->part, r->ticket, r->spread, r->order};
     for (void *p : ptrs)
@@ -292,8 +316,9 @@ void Engine::upload(const EngineSetup &s) {
     r->order_moved = false;
     if (!failed()) {
       cudaError_t pe = cudaSuccess;
-      r->plan = poisson_plan_create(rs.nx, rs.ny, rs.wx.data(), rs.wy.data(), poisson_mode_, &pe);
-      check(pe, poisson_mode_ == 0 ? "poisson plan (fp32)" : poisson_mode_ == 2 ? "poisson plan (fp64)" : "poisson plan (split-bf16 tcgen05)");
+      const int mode = region_plan_mode(poisson_mode_, rs.nx, rs.ny);
+      r->plan = poisson_plan_create(rs.nx, rs.ny, rs.wx.data(), rs.wy.data(), mode, &pe);
+      check(pe, mode == 0 ? "poisson plan (fp32)" : mode == 2 ? "poisson plan (fp64)" : "poisson plan (split-bf16 tcgen05)");
       if (r->plan) r->dens_split = poisson_split_input(r->plan, &r->split_ld);
       progress("  upload: region solver planned (%dx%d bins)", rs.nx, rs.ny);
     }
@@ -329,6 +354,7 @@ void Engine::upload(const EngineSetup &s) {
 }
 
 void Engine::update_bins(int b, const RegionSetup &rs) {
+  flush();
   join();
   Region *r = regions_[b];
   r->args.target_density = rs.target_density;
@@ -343,6 +369,7 @@ void Engine::update_bins(int b, const RegionSetup &rs) {
 }
 
 void Engine::rewrite_cells(const EngineSetup &s) {
+  flush();
   join();
   // sizes and density sizes of every cell (routability's inflation and filler changes keep
   // the cell count of a region's block only when no filler moved; the caller re-uploads then)
@@ -381,6 +408,7 @@ static CellArgs cell_args(const int64_t off, int2 *dc, int32_t *hx, int32_t *hy,
 #define CELLS(r) cell_args((r)->cell_off, dc_, hx_, hy_, dscale_, kind_, locked_, area_, cell_pin_start_, (r)->slot)
 
 void Engine::set_coords(int b, SlotId slot, const std::vector<float> &xy) {
+  flush();
   join();
   Region *r = regions_[b];
   if (r->n_cells) check(cudaMemcpyAsync(r->slot[slot], xy.data(), r->n_cells * sizeof(float2), cudaMemcpyHostToDevice, stream_), "set_coords");
@@ -388,6 +416,7 @@ void Engine::set_coords(int b, SlotId slot, const std::vector<float> &xy) {
 }
 
 std::vector<float> Engine::get_coords(int b, SlotId slot) {
+  flush();
   join();
   Region *r = regions_[b];
   std::vector<float> xy(2 * r->n_cells);
@@ -398,6 +427,7 @@ std::vector<float> Engine::get_coords(int b, SlotId slot) {
 }
 
 void Engine::place_at(int b, SlotId slot) {
+  flush();
   join();
   if (failed()) return;
   hpwl_ready_ = hpwl_fetched_ = false;  // the density centres move
@@ -437,6 +467,22 @@ void Engine::nesterov_step(int b, float step, float coeff) {
   hpwl_ready_ = hpwl_fetched_ = false;  // the density centres move
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
+  if (packed()) {
+    QueueEntry q{};
+    q.kind = Q_PLACE;
+    q.region = b;
+    q.e.r = r->args;
+    q.e.c = c;
+    q.e.step = step;
+    q.e.coeff = coeff;
+    q.e.partials = r->part;
+    q.e.ticket = r->ticket;
+    q.e.out = &dev_scal_[b].overflow;
+    q.e.dens_split = r->dens_split;
+    q.e.split_ld = r->split_ld;
+    queue_->push_back(q);
+    return;
+  }
   ph_begin(PH_PLACE);
   launches += (r->n_cells ? 1 : 0) + 1;
   if (r->n_cells) {
@@ -454,6 +500,13 @@ void Engine::nesterov_step(int b, float step, float coeff) {
 
 void Engine::field(int b) {
   if (failed()) return;
+  if (packed()) {
+    QueueEntry q{};
+    q.kind = Q_FIELD;
+    q.region = b;
+    queue_->push_back(q);
+    return;
+  }
   Region *r = regions_[b];
   ph_begin(PH_POISSON);
   check(poisson_solve(r->plan, r->density, r->fx, r->fy, stream_), "poisson");
@@ -479,6 +532,7 @@ WaArgs Engine::wa_args() const {
 }
 
 void Engine::wa(float cx, float cy) {
+  flush();
   if (failed() || n_nets_ == 0) return;
   join();
   WaArgs w = wa_args();
@@ -517,13 +571,31 @@ void Engine::wa(float cx, float cy) {
 }
 
 void Engine::gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, SlotId b2) {
-  join();
   if (failed()) return;
   Region *r = regions_[b];
   CellArgs c = CELLS(r);
   const float2 *pa1 = a1 == S_NUM ? nullptr : r->slot[a1];
   const float2 *pb1 = b1 == S_NUM ? nullptr : r->slot[b1];
   const float2 *pb2 = b2 == S_NUM ? nullptr : r->slot[b2];
+  if (packed()) {
+    QueueEntry q{};
+    q.kind = Q_GRAD;
+    q.region = b;
+    q.e.r = r->args;
+    q.e.c = c;
+    q.e.pin_grad = pin_grad_;
+    q.e.penalty = penalty;
+    q.e.out_sum = r->slot[out];
+    q.e.a1 = pa1;
+    q.e.b1 = pb1;
+    q.e.b2 = pb2;
+    q.e.partials = r->part;
+    q.e.ticket = r->ticket;
+    q.e.out = &dev_scal_[b].wl_sum;
+    queue_->push_back(q);
+    return;
+  }
+  join();
   if (r->n_cells) {
     ph_begin(PH_GRAD);
     launches += 1;
@@ -536,6 +608,7 @@ void Engine::gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, S
 }
 
 void Engine::prev_slp(int b, float coef) {
+  flush();
   join();
   if (failed()) return;
   Region *r = regions_[b];
@@ -545,6 +618,7 @@ void Engine::prev_slp(int b, float coef) {
 }
 
 void Engine::hold_locked(int b) {
+  flush();
   join();
   if (failed() || !any_locked_) return;
   Region *r = regions_[b];
@@ -556,12 +630,14 @@ void Engine::hold_locked(int b) {
 void Engine::swap_slots(int b, SlotId a, SlotId c) { std::swap(regions_[b]->slot[a], regions_[b]->slot[c]); }
 
 void Engine::copy_slot(int b, SlotId dst, SlotId src) {
+  flush();
   join();
   Region *r = regions_[b];
   if (r->n_cells) check(cudaMemcpyAsync(r->slot[dst], r->slot[src], r->n_cells * sizeof(float2), cudaMemcpyDeviceToDevice, stream_), "copy_slot");
 }
 
 void Engine::fetch() {
+  flush();
   join();
   if (failed() || host_scal_.empty()) return;
   const size_t bytes = host_scal_.size() * sizeof(RegionScalars);
@@ -583,16 +659,190 @@ void Engine::fetch() {
   // the trial's timed launches have ended (the WA joined the stream before the copy)
   for (Region *r : regions_) r->scatter_tune->finish();
   wa_tune_->finish();
+  pk_scatter_tune_->finish();
+  pk_slot_ = 0;  // the stream has drained: every table slot is free
+}
+
+// ---- packed launches
+bool Engine::stage_tables(size_t n) {
+  const size_t need = (size_t)kTableSlots * n;
+  if (need > pk_cap_) {
+    check(cudaStreamSynchronize(stream_), "packed tables");
+    if (pk_host_) cudaFreeHost(pk_host_);
+    if (pk_dev_) cudaFree(pk_dev_);
+    pk_host_ = nullptr;
+    pk_dev_ = nullptr;
+    pk_cap_ = 0;
+    check(cudaMallocHost(&pk_host_, need * sizeof(PackedRegion)), "packed tables");
+    check(cudaMalloc(&pk_dev_, need * sizeof(PackedRegion)), "packed tables");
+    if (failed()) return false;
+    pk_cap_ = need;
+    pk_slot_ = 0;
+  }
+  if (pk_slot_ >= kTableSlots) {
+    // every slot used since the last trial read: wait for the copies out of them
+    check(cudaStreamSynchronize(stream_), "packed tables");
+    pk_slot_ = 0;
+  }
+  return !failed();
+}
+
+void Engine::flush() {
+  if (!queue_ || queue_->empty() || failed()) {
+    if (queue_) queue_->clear();
+    return;
+  }
+  std::vector<QueueEntry> q;
+  q.swap(*queue_);
+  size_t a = 0;
+  while (a < q.size()) {
+    // a run of one phase, each region at most once
+    std::vector<char> seen(regions_.size(), 0);
+    size_t b = a;
+    while (b < q.size() && q[b].kind == q[a].kind && !seen[q[b].region]) seen[q[b].region] = 1, b++;
+    if (q[a].kind == Q_PLACE)
+      flush_place(q, a, b);
+    else if (q[a].kind == Q_FIELD)
+      flush_field(q, a, b);
+    else
+      flush_grad(q, a, b);
+    a = b;
+  }
+}
+
+// Table entries [first, first + n) of a slot copied to the device: the slot's device address.
+static PackedRegion *copy_tables(Engine &eng, PackedRegion *host, PackedRegion *dev, size_t n, cudaStream_t s, int64_t &h2d) {
+  eng.check(cudaMemcpyAsync(dev, host, n * sizeof(PackedRegion), cudaMemcpyHostToDevice, s), "packed tables");
+  h2d += (int64_t)(n * sizeof(PackedRegion));
+  return dev;
+}
+
+void Engine::flush_place(const std::vector<QueueEntry> &q, size_t a, size_t b) {
+  join();  // the WA has read the centres this moves
+  const size_t n = b - a;
+  if (!stage_tables(2 * regions_.size())) return;
+  PackedRegion *h = pk_host_ + (size_t)pk_slot_ * 2 * regions_.size(), *d = pk_dev_ + (size_t)pk_slot_ * 2 * regions_.size();
+  pk_slot_++;
+  // the scatter's table (regions with cells), then the finalize's (every region); the
+  // scatter's form for every region (timed from the table's copy, the same for each form)
+  bool any = false;
+  for (size_t k = a; k < b; k++) any |= q[k].e.r.n_cells > 0;
+  ph_begin(PH_PLACE);
+  const int form = any ? pk_scatter_tune_->start(stream_) : 0;
+  int ns = 0, blocks = 0;
+  for (size_t k = a; k < b; k++) {
+    const PackedRegion &e = q[k].e;
+    if (e.r.n_cells <= 0) continue;
+    h[ns] = e;
+    h[ns].r.scatter_form = form;
+    h[ns].first = blocks;
+    h[ns].blocks = blocks_for(e.r.n_cells);
+    blocks += h[ns].blocks;
+    ns++;
+  }
+  int fb = 0;
+  for (size_t k = a; k < b; k++) {
+    PackedRegion &f = h[ns + (k - a)];
+    f = q[k].e;
+    f.first = fb;
+    f.blocks = f.r.nx;  // one block per x row
+    fb += f.blocks;
+  }
+  copy_tables(*this, h, d, ns + n, stream_, h2d_bytes);
+  if (ns) {
+    k_place_packed<<<blocks, kThreadsPerBlock, 0, stream_>>>(d, ns);
+    pk_scatter_tune_->stop(stream_);
+    launches += 1;
+  }
+  ph_end(PH_PLACE);
+  ph_begin(PH_FINALIZE);
+  k_finalize_packed<<<fb, kThreadsPerBlock, 0, stream_>>>(d + ns, (int)n);
+  launches += 1;
+  ph_end(PH_FINALIZE);
+  check(cudaGetLastError(), "packed place");
+}
+
+void Engine::flush_field(const std::vector<QueueEntry> &q, size_t a, size_t b) {
+  // the FP32 solves as one group (made again when the set of regions changes), the others
+  // one region a launch
+  std::vector<char> set(regions_.size(), 0);
+  std::vector<int> alone;
+  for (size_t k = a; k < b; k++) {
+    Region *r = regions_[q[k].region];
+    if (r->plan && poisson_plan_mode(r->plan) == 0)
+      set[q[k].region] = 1;
+    else
+      alone.push_back(q[k].region);
+  }
+  ph_begin(PH_POISSON);
+  if (std::count(set.begin(), set.end(), 1)) {
+    if (!group_ || set != group_set_) {
+      check(cudaStreamSynchronize(stream_), "poisson group");
+      poisson_group_destroy(group_);
+      group_ = nullptr;
+      std::vector<PoissonPlan *> plans;
+      std::vector<const float *> dens;
+      std::vector<float *> fx, fy;
+      for (size_t k = 0; k < regions_.size(); k++)
+        if (set[k]) {
+          plans.push_back(regions_[k]->plan);
+          dens.push_back(regions_[k]->density);
+          fx.push_back(regions_[k]->fx);
+          fy.push_back(regions_[k]->fy);
+        }
+      cudaError_t pe = cudaSuccess;
+      group_ = poisson_group_create(plans.data(), dens.data(), fx.data(), fy.data(), (int)plans.size(), &pe);
+      check(pe, "poisson group");
+      group_set_ = set;
+    }
+    check(poisson_group_solve(group_, stream_), "poisson group");
+    launches += poisson_group_launches(group_);
+  }
+  for (int k : alone) {
+    Region *r = regions_[k];
+    check(poisson_solve(r->plan, r->density, r->fx, r->fy, stream_), "poisson");
+    launches += poisson_launches(r->plan);
+  }
+  ph_end(PH_POISSON);
+}
+
+void Engine::flush_grad(const std::vector<QueueEntry> &q, size_t a, size_t b) {
+  join();  // the forces are the WA's
+  if (!stage_tables(2 * regions_.size())) return;
+  PackedRegion *h = pk_host_ + (size_t)pk_slot_ * 2 * regions_.size(), *d = pk_dev_ + (size_t)pk_slot_ * 2 * regions_.size();
+  pk_slot_++;
+  int n = 0, blocks = 0;
+  for (size_t k = a; k < b; k++) {
+    const PackedRegion &e = q[k].e;
+    if (e.r.n_cells <= 0) {
+      check(cudaMemsetAsync(e.out, 0, 4 * sizeof(double), stream_), "gradients");
+      continue;
+    }
+    h[n] = e;
+    h[n].first = blocks;
+    h[n].blocks = blocks_for(e.r.n_cells);
+    blocks += h[n].blocks;
+    n++;
+  }
+  if (!n) return;
+  copy_tables(*this, h, d, n, stream_, h2d_bytes);
+  ph_begin(PH_GRAD);
+  k_gradients_packed<<<blocks, kThreadsPerBlock, 0, stream_>>>(d, n);
+  launches += 1;
+  ph_end(PH_GRAD);
+  check(cudaGetLastError(), "packed gradients");
 }
 
 std::string Engine::tuning() const {
   std::string s = wa_tune_ ? wa_tune_->report() : std::string();
+  if (packed()) return s + "; " + pk_scatter_tune_->report();
   for (size_t b = 0; b < regions_.size(); b++)
     if (regions_[b]->n_cells) s += "; region " + std::to_string(b) + " " + regions_[b]->scatter_tune->report();
   return s;
 }
 
 int64_t Engine::hpwl() {
+  flush();
   join();
   if (failed()) return 0;
   if (hpwl_ready_ && hpwl_fetched_) return (int64_t)hpwl_host_;  // read with the trial's scalars
@@ -630,6 +880,7 @@ int64_t Engine::hpwl() {
 }
 
 void Engine::centres(std::vector<int32_t> &dcx, std::vector<int32_t> &dcy) {
+  flush();
   join();
   std::vector<int2> dc(n_cells_);
   if (n_cells_) {
@@ -646,6 +897,7 @@ void Engine::centres(std::vector<int32_t> &dcx, std::vector<int32_t> &dcy) {
 }
 
 void Engine::set_net_weights(const std::vector<float> &w) {
+  flush();
   join();
   if (w.empty()) return;
   if (w.size() != net_order_.size()) {
@@ -664,6 +916,7 @@ void Engine::set_net_weights(const std::vector<float> &w) {
 // cell-major pin lists moved with their cells (each cell's pins keep their order), the pins'
 // cell indices and slots remapped. Scratch from the device's pool, returned at the end.
 void Engine::reorder(int b) {
+  flush();
   join();
   Region *r = regions_[b];
   const int32_t n = (int32_t)r->n_cells;
@@ -753,6 +1006,7 @@ void Engine::reorder(int b) {
 }
 
 bool Engine::take_order(int b, std::vector<int32_t> &order) {
+  flush();
   join();
   Region *r = regions_[b];
   if (!r->order_moved || failed()) return false;
@@ -766,8 +1020,13 @@ bool Engine::take_order(int b, std::vector<int32_t> &order) {
 }
 
 void Engine::rebuild_poisson(int mode) {
+  flush();
   join();
   poisson_mode_ = mode;
+  check(cudaStreamSynchronize(stream_), "rebuild sync");
+  poisson_group_destroy(group_);
+  group_ = nullptr;
+  group_set_.clear();
   for (size_t b = 0; b < regions_.size(); b++) {
     Region *r = regions_[b];
     check(cudaStreamSynchronize(stream_), "rebuild sync");
@@ -776,8 +1035,9 @@ void Engine::rebuild_poisson(int mode) {
     r->dens_split = nullptr;
     r->split_ld = 0;
     cudaError_t pe = cudaSuccess;
-    r->plan = poisson_plan_create(region_dims_[b].first, region_dims_[b].second, region_wx_[b].data(), region_wy_[b].data(), mode, &pe);
-    check(pe, mode == 0 ? "poisson plan (fp32)" : mode == 2 ? "poisson plan (fp64)" : "poisson plan (split-bf16 tcgen05)");
+    const int rmode = region_plan_mode(mode, region_dims_[b].first, region_dims_[b].second);
+    r->plan = poisson_plan_create(region_dims_[b].first, region_dims_[b].second, region_wx_[b].data(), region_wy_[b].data(), rmode, &pe);
+    check(pe, rmode == 0 ? "poisson plan (fp32)" : rmode == 2 ? "poisson plan (fp64)" : "poisson plan (split-bf16 tcgen05)");
     if (r->plan) {
       r->dens_split = poisson_split_input(r->plan, &r->split_ld);
       // the current density into the new operand, the field recomputed

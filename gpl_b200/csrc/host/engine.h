@@ -14,7 +14,9 @@
 namespace gpl {
 
 struct PoissonPlan;
+struct PoissonGroup;
 struct WaArgs;
+struct PackedRegion;
 class Tuner;
 
 // What the device needs of one region (a `NesterovBase`'s bin grid).
@@ -122,6 +124,15 @@ class Engine {
   // The tuners' choices and their candidates' median times: the small nets' WA form, each
   // region's scatter form.
   std::string tuning() const;
+  // Packed launches (the default with more than one region): each region's scatter, bin
+  // finalize, FP32 density solve and gradient update are queued and run as one launch per
+  // phase over every region queued (the split-BF16 and FP64 solves stay one region a launch);
+  // every result is the same as the region-by-region launches' bit for bit.
+  void set_packed(int on) {
+    flush();
+    packed_opt_ = on;
+  }
+  bool packed() const { return packed_opt_ < 0 ? regions_.size() > 1 : packed_opt_ != 0; }
   bool failed() const { return err_.code != cudaSuccess; }
   const DeviceError &error() const { return err_; }
   void check(cudaError_t e, const char *where);
@@ -176,6 +187,23 @@ class Engine {
   cudaStream_t wa_stream_ = nullptr;
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   std::unique_ptr<Tuner> wa_tune_;
+  // packed launches: the queue of (phase, region) with each entry's arguments as queued, the
+  // tables' page-locked staging and device copy, the grouped FP32 solves of the live set
+  enum Queued { Q_PLACE = 0, Q_FIELD, Q_GRAD };
+  struct QueueEntry;
+  std::vector<QueueEntry> *queue_ = nullptr;
+  int packed_opt_ = -1;  // -1: by the region count
+  PackedRegion *pk_host_ = nullptr, *pk_dev_ = nullptr;
+  size_t pk_cap_ = 0;
+  int pk_slot_ = 0;
+  PoissonGroup *group_ = nullptr;
+  std::vector<char> group_set_;  // the regions group_ solves
+  std::unique_ptr<Tuner> pk_scatter_tune_;
+  void flush();
+  void flush_place(const std::vector<QueueEntry> &q, size_t a, size_t b);
+  void flush_field(const std::vector<QueueEntry> &q, size_t a, size_t b);
+  void flush_grad(const std::vector<QueueEntry> &q, size_t a, size_t b);
+  bool stage_tables(size_t n);
   bool wa_pending_ = false;
   bool overlap_ = true;
   void join();

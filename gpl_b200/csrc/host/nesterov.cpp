@@ -2420,6 +2420,11 @@ int gpl_set_option(gpl_ctx *c, const char *name, const char *value) {
     c->eng->set_reorder(v == "1");
     return 0;
   }
+  if (n == "packed") {
+    if (v != "0" && v != "1" && v != "auto") return -1;
+    c->eng->set_packed(v == "auto" ? -1 : v == "1" ? 1 : 0);
+    return 0;
+  }
   return -1;
 }
 
@@ -2499,6 +2504,11 @@ int gpl_session_set_option(gpl_session *s, const char *name, const char *value) 
   }
   if (n == "reorder") {  // the device cell order kept coherent (1, the default) or fixed (0)
     s->ctx->eng->set_reorder(v != "0");
+    return 0;
+  }
+  if (n == "packed") {  // every region's phase in one launch ("auto", the default: with regions)
+    if (v != "0" && v != "1" && v != "auto") return -1;
+    s->ctx->eng->set_packed(v == "auto" ? -1 : v == "1" ? 1 : 0);
     return 0;
   }
   return -1;

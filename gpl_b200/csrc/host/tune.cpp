@@ -8,7 +8,7 @@
 namespace gpl {
 
 Tuner::Tuner(std::string what, std::vector<std::string> names, const char *env, int probe, int period)
-    : what_(std::move(what)), names_(std::move(names)), probe_(std::max(1, probe)), period_(std::max(1, period)) {
+    : what_(std::move(what)), names_(std::move(names)), probe_(std::max(1, probe)), base_period_(std::max(1, period)), period_(std::max(1, period)) {
   n_ = (int)names_.size();
   samples_.assign(n_, {});
   median_.assign(n_, -1.0f);
@@ -81,7 +81,10 @@ void Tuner::decide() {
     median_[k] = v[v.size() / 2];
     if (pick < 0 || median_[k] < median_[pick]) pick = k;
   }
-  if (pick >= 0) best_ = pick;
+  if (pick >= 0) {
+    period_ = pick == best_ && probes_ > 0 ? std::min(2 * period_, 16 * base_period_) : base_period_;
+    best_ = pick;
+  }
   probing_ = false;
   since_ = 0;
   probes_++;

@@ -7,7 +7,8 @@
 // time, and the probe again every `period` uses. A use is bracketed by start() and stop();
 // finish() is called once the stream has synchronised (the trial's read-back, the solver's
 // batch read), reads the use's time and counts it or, for a use that did less work than the
-// others (a solver batch that ended part-way), drops it.
+// others (a solver batch that ended part-way), drops it. A probe that keeps the form in use
+// doubles the period to the next (up to 16 times `period`); one that changes it starts over.
 //
 // An environment variable can fix the form instead (its accepted values name the candidates
 // in order): the forms give the same results, so it changes only the speed.
@@ -43,7 +44,7 @@ class Tuner {
  private:
   std::string what_;
   std::vector<std::string> names_;
-  int n_ = 0, probe_ = 3, period_ = 256;
+  int n_ = 0, probe_ = 3, base_period_ = 256, period_ = 256;
   int fixed_ = -1;
   int best_ = 0;
   int cur_ = 0;              // the candidate of the use in flight

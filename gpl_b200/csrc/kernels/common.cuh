@@ -67,21 +67,22 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
   return s;
 }
 
-// Whether this block is the last of its launch to finish: its partials written and fenced
-// before it counts itself, so the last one sees every block's partials. The count is left at
-// zero for the next launch.
-__device__ __forceinline__ bool last_block_done(unsigned int *ticket) {
+// Whether this block is the last of its nblk (by default the launch's blocks) to finish: its
+// partials written and fenced before it counts itself, so the last one sees every block's
+// partials. The count is left at zero for the next launch.
+__device__ __forceinline__ bool last_block_done(unsigned int *ticket, unsigned int nblk) {
   __shared__ bool last;
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
-    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    last = atomicAdd(ticket, 1u) == nblk - 1;
     if (last) *ticket = 0;
   }
   __syncthreads();
   if (last) __threadfence();
   return last;
 }
+__device__ __forceinline__ bool last_block_done(unsigned int *ticket) { return last_block_done(ticket, gridDim.x); }
 
 // Sums `nblk` rows of `width` partials into out[0..width): each thread over rows t,
 // t + NT, ... then the block's sum, so the order is fixed for a block of NT threads.

@@ -78,6 +78,27 @@ struct WaArgs {
   WaSmall small;                 // the degree-2..4 ranges (zero counts: none)
 };
 
+// One region's entry in a packed launch (a phase of every live region in one launch): its
+// arguments, and its first block and block count in the launch's grid.
+struct PackedRegion {
+  RegionArgs r;
+  CellArgs c;
+  int32_t first, blocks;
+  float step, coeff;                 // the scatter (PLACE_NESTEROV)
+  double *partials, *out;            // the finalize's or the gradients' partials and sums
+  unsigned int *ticket;
+  __nv_bfloat16 *dens_split;         // the finalize
+  int32_t split_ld;
+  float penalty;                     // the gradients
+  const float2 *pin_grad;
+  float2 *out_sum;
+  const float2 *a1, *b1, *b2;
+};
+// The packed phases: k_place_cells (PLACE_NESTEROV), k_bins_finalize and k_gradients of n
+// regions, each region's blocks doing exactly what its own launch's would.
+__global__ void k_place_packed(const PackedRegion *t, int n);
+__global__ void k_finalize_packed(const PackedRegion *t, int n);
+__global__ void k_gradients_packed(const PackedRegion *t, int n);
 __global__ void k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *coords);
 __global__ void k_bins_finalize(RegionArgs r, double *partials, __nv_bfloat16 *dens_split, int split_ld, unsigned int *ticket, double *out);
 __global__ void k_wa(WaArgs w, float cx, float cy);
@@ -161,5 +182,14 @@ cudaError_t poisson_split_density(PoissonPlan *p, const float *density, cudaStre
 size_t poisson_workspace_bytes(int nx, int ny);
 // Kernel launches one poisson_solve makes.
 int poisson_launches(const PoissonPlan *p);
+// The FP32 solves of n plans (mode 0) with their densities and fields fixed, as five
+// launches in all: each GEMM stage over every plan's problems, the spectral step over every
+// plan's spectrum (the fields equal poisson_solve's bit for bit).
+struct PoissonGroup;
+PoissonGroup *poisson_group_create(PoissonPlan *const *plans, const float *const *density, float *const *field_x, float *const *field_y, int n, cudaError_t *err);
+void poisson_group_destroy(PoissonGroup *g);
+cudaError_t poisson_group_solve(const PoissonGroup *g, cudaStream_t s);
+int poisson_group_launches(const PoissonGroup *g);
+int poisson_plan_mode(const PoissonPlan *p);
 
 }  // namespace gpl

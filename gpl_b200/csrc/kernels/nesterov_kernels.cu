@@ -189,11 +189,12 @@ __device__ __forceinline__ void pooled_scatter(const RegionArgs &r, bool narrow,
   }
 }
 
-__global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
+// One block of a region's scatter: block `blk` of the region's cells.
+__device__ __forceinline__ void place_cells_block(const RegionArgs &r, const CellArgs &c, int mode, float step, float coeff, const float2 *__restrict__ coords, int blk) {
   __shared__ __align__(16) unsigned long long s_tile[2 * kTileBins];  // cells then fillers; 32-bit when narrow
   __shared__ unsigned long long s_red[kThreads];
   __shared__ int s_box[5];  // the block's bin box, and its cells' (cell, bin) addends
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int i = blk * blockDim.x + threadIdx.x;
   const bool valid = i < r.n_cells;
   int32_t x0 = INT32_MAX, x1 = INT32_MIN, y0 = INT32_MAX, y1 = INT32_MIN;
   int32_t dlx = 0, dux = 0, dly = 0, duy = 0;
@@ -305,16 +306,47 @@ __global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs
   }
 }
 
+__global__ void __launch_bounds__(kThreads) k_place_cells(RegionArgs r, CellArgs c, int mode, float step, float coeff, const float2 *__restrict__ coords) {
+  place_cells_block(r, c, mode, step, coeff, coords, blockIdx.x);
+}
+
+// A packed launch's block: its region's entry (the last whose first block is at most this
+// block) copied into shared memory.
+__device__ __forceinline__ void packed_entry(const PackedRegion *__restrict__ t, int n, PackedRegion &e) {
+  __shared__ int s_k;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (t[mid].first <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    s_k = lo;
+  }
+  __syncthreads();
+  static_assert(sizeof(PackedRegion) % 8 == 0, "copied as 8-byte words");
+  const unsigned long long *src = reinterpret_cast<const unsigned long long *>(t + s_k);
+  unsigned long long *dst = reinterpret_cast<unsigned long long *>(&e);
+  for (int k = threadIdx.x; k < (int)(sizeof(PackedRegion) / 8); k += blockDim.x) dst[k] = src[k];
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kThreads) k_place_packed(const PackedRegion *__restrict__ t, int n) {
+  __shared__ PackedRegion e;
+  packed_entry(t, n, e);
+  place_cells_block(e.r, e.c, PLACE_NESTEROV, e.step, e.coeff, nullptr, (int)blockIdx.x - e.first);
+}
+
 // ---- bins: density and overflow (:2252-2262), accumulators cleared for the next scatter.
 // Optionally the density split into bf16 hi/lo for the tensor-core solver. One block per x
 // row (threads along y, kBinsPerThread bins each with their loads issued together), so no
 // index is divided; block partials of the two overflow sums.
 constexpr int kBinsPerThread = 4;
 
-__global__ void __launch_bounds__(kThreads) k_bins_finalize(RegionArgs r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld, unsigned int *ticket, double *out) {
+// One block (bin row x = blk) of a region's finalize over nblk rows.
+__device__ __forceinline__ void bins_finalize_block(const RegionArgs &r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld, unsigned int *ticket, double *out, int blk, int nblk) {
   __shared__ double sh[kThreads / 32];
   double o_sum = 0.0, ou_sum = 0.0;
-  const int32_t x = blockIdx.x;
+  const int32_t x = blk;
   const size_t row = (size_t)x * r.ny;
   for (int32_t y0 = threadIdx.x; y0 < r.ny; y0 += blockDim.x * kBinsPerThread) {
     int64_t inst[kBinsPerThread], fill[kBinsPerThread];
@@ -356,18 +388,28 @@ __global__ void __launch_bounds__(kThreads) k_bins_finalize(RegionArgs r, double
   double a = block_sum<kThreads>(o_sum, sh);
   double b = block_sum<kThreads>(ou_sum, sh);
   if (threadIdx.x == 0) {
-    partials[2 * blockIdx.x] = a;
-    partials[2 * blockIdx.x + 1] = b;
+    partials[2 * blk] = a;
+    partials[2 * blk + 1] = b;
   }
   // the last block to finish sums the blocks' partials (the overflow sums) and reports the
   // scatter's spread blocks
-  if (last_block_done(ticket)) {
-    reduce_rows<kThreads>(partials, gridDim.x, 2, out, sh);
+  if (last_block_done(ticket, nblk)) {
+    reduce_rows<kThreads>(partials, nblk, 2, out, sh);
     if (threadIdx.x == 0 && r.spread) {
       out[6] = (double)*r.spread;
       *r.spread = 0u;
     }
   }
+}
+
+__global__ void __launch_bounds__(kThreads) k_bins_finalize(RegionArgs r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld, unsigned int *ticket, double *out) {
+  bins_finalize_block(r, partials, dens_split, split_ld, ticket, out, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(kThreads) k_finalize_packed(const PackedRegion *__restrict__ t, int n) {
+  __shared__ PackedRegion e;
+  packed_entry(t, n, e);
+  bins_finalize_block(e.r, e.partials, e.dens_split, e.split_ld, e.ticket, e.out, (int)blockIdx.x - e.first, e.blocks);
 }
 
 // ---- WA wirelength (updateWireLengthForceWA :2325-2388 + getWireLengthGradientPinWA
@@ -949,10 +991,12 @@ void launch_wa_tiles(const WaArgs &w, float cx, float cy, cudaStream_t s) {
 // the ordered sums; larger cells walk their bins.
 constexpr int kGradPinTile = 2048;
 
-__global__ void __launch_bounds__(kThreads, 6) k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials, unsigned int *ticket, double *out) {
+// One block (cells blk * 256 ..) of a region's gradient update over nblk blocks.
+__device__ __forceinline__ void gradients_block(const RegionArgs &r, const CellArgs &c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1,
+                                                const float2 *__restrict__ b2, double *__restrict__ partials, unsigned int *ticket, double *out, int blk, int nblk) {
   __shared__ double4 sh[kThreads / 32];
   __shared__ float2 s_pg[kGradPinTile];
-  const int i0 = blockIdx.x * blockDim.x;
+  const int i0 = blk * blockDim.x;
   const int i = i0 + threadIdx.x;
   const int i1 = min(r.n_cells, i0 + (int)blockDim.x);
   const int64_t p0 = c.pin_start[i0], p1 = c.pin_start[i1];
@@ -1041,14 +1085,24 @@ __global__ void __launch_bounds__(kThreads, 6) k_gradients(RegionArgs r, CellArg
   }
   double4 v = block_sum4<kThreads>(make_double4(s_wl, s_den, s_d1, s_d2), sh);
   if (threadIdx.x == 0) {
-    partials[4 * blockIdx.x + 0] = v.x;
-    partials[4 * blockIdx.x + 1] = v.y;
-    partials[4 * blockIdx.x + 2] = v.z;
-    partials[4 * blockIdx.x + 3] = v.w;
+    partials[4 * blk + 0] = v.x;
+    partials[4 * blk + 1] = v.y;
+    partials[4 * blk + 2] = v.z;
+    partials[4 * blk + 3] = v.w;
   }
   // the last block to finish sums the blocks' partials (|wl|, |density|, the two distances)
   __shared__ double shr[kThreads / 32];
-  if (last_block_done(ticket)) reduce_rows<kThreads>(partials, gridDim.x, 4, out, shr);
+  if (last_block_done(ticket, nblk)) reduce_rows<kThreads>(partials, nblk, 4, out, shr);
+}
+
+__global__ void __launch_bounds__(kThreads, 6) k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials, unsigned int *ticket, double *out) {
+  gradients_block(r, c, pin_grad, penalty, out_sum, a1, b1, b2, partials, ticket, out, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(kThreads, 6) k_gradients_packed(const PackedRegion *__restrict__ t, int n) {
+  __shared__ PackedRegion e;
+  packed_entry(t, n, e);
+  gradients_block(e.r, e.c, e.pin_grad, e.penalty, e.out_sum, e.a1, e.b1, e.b2, e.partials, e.ticket, e.out, (int)blockIdx.x - e.first, e.blocks);
 }
 
 // ---- updateInitialPrevSLPCoordi (:2583-2595): a back-step along the current gradient.

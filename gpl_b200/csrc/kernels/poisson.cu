@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -33,11 +34,9 @@ namespace gpl {
 // 128 x 64 output tile per block, K-step 8, 256 threads with 8 x 4 outputs each.
 constexpr int SG_BM = 128, SG_BN = 64, SG_BK = 8;
 
+// One 128 x 64 output tile of D = A B^T from (m0, n0).
 template <typename T>
-__global__ void __launch_bounds__(256) k_gemm_tn(GemmBatchT<T> gb) {
-  const GemmProblemT<T> P = gb.p[blockIdx.z];
-  const int m0 = blockIdx.y * SG_BM, n0 = blockIdx.x * SG_BN;
-  if (m0 >= P.M || n0 >= P.N) return;
+__device__ __forceinline__ void gemm_tile(const GemmProblemT<T> &P, const int m0, const int n0) {
   __shared__ __align__(16) T As[SG_BK][SG_BM + 4];
   __shared__ __align__(16) T Bs[SG_BK][SG_BN + 4];
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
@@ -97,6 +96,33 @@ __global__ void __launch_bounds__(256) k_gemm_tn(GemmBatchT<T> gb) {
       if (gn < P.N) P.D[(size_t)gm * P.ldd + gn] = acc[i][j];
     }
   }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_gemm_tn(GemmBatchT<T> gb) {
+  const GemmProblemT<T> P = gb.p[blockIdx.z];
+  const int m0 = blockIdx.y * SG_BM, n0 = blockIdx.x * SG_BN;
+  if (m0 >= P.M || n0 >= P.N) return;
+  gemm_tile<T>(P, m0, n0);
+}
+
+// Many problems in one launch: block b takes tile b - first[k] of problem k (the last with
+// first[k] <= b), tiles row-major over the problem's (M / 128) x (N / 64) grid.
+__global__ void __launch_bounds__(256) k_gemm_grouped(const GemmProblem *__restrict__ probs, const int *__restrict__ first, int n) {
+  __shared__ int s_k;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (first[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    s_k = lo;
+  }
+  __syncthreads();
+  const GemmProblem P = probs[s_k];
+  const int t = (int)blockIdx.x - first[s_k];
+  const int tn = (P.N + SG_BN - 1) / SG_BN;
+  gemm_tile<float>(P, (t / tn) * SG_BM, (t % tn) * SG_BN);
 }
 
 template <typename T>
@@ -298,6 +324,8 @@ cudaError_t poisson_split_density(PoissonPlan *p, const float *density, cudaStre
   return cudaGetLastError();
 }
 
+int poisson_plan_mode(const PoissonPlan *p) { return p->mode; }
+
 int poisson_launches(const PoissonPlan *p) { return p->mode == 0 ? 5 : p->mode == 2 ? 9 : tc_launches(p); }
 
 // The FP64 form: the density widened to double, the FP32 form's six GEMMs and spectral step
@@ -328,6 +356,124 @@ static cudaError_t solve_fp64(PoissonPlan *p, const float *density, float *field
   k_convert<double, float><<<blocks, 256, 0, s>>>(n, f, field_y);
   return cudaGetLastError();
 }
+
+// ---------------------------------------------------------------- many FP32 solves at once
+// The FP32 solves of several regions (each its own grid) as five launches: each GEMM stage
+// over every region's problems, the spectral step over every region's spectrum. Each
+// problem's tiles are those poisson_solve computes, so every field is the same bit for bit.
+struct SpectralJob {
+  int nx, ny, first, blocks;
+  const float *ah, *wx, *wx2, *wy, *wy2;
+  float *exh, *eyh;
+};
+__global__ void k_spectral_grouped(const SpectralJob *__restrict__ jobs, int n) {
+  __shared__ int s_k;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (jobs[mid].first <= (int)blockIdx.x) lo = mid; else hi = mid - 1;
+    }
+    s_k = lo;
+  }
+  __syncthreads();
+  const SpectralJob J = jobs[s_k];
+  const int64_t cnt = (int64_t)J.nx * J.ny;
+  for (int64_t k = ((int64_t)blockIdx.x - J.first) * blockDim.x + threadIdx.x; k < cnt; k += (int64_t)J.blocks * blockDim.x) {
+    int u = (int)(k / J.ny), v = (int)(k % J.ny);
+    float ex = 0.0f, ey = 0.0f;
+    if (u != 0 || v != 0) {
+      float p = __fdiv_rn(J.ah[k], __fadd_rn(J.wx2[u], J.wy2[v]));
+      ex = __fmul_rn(p, J.wx[u]);
+      ey = __fmul_rn(p, J.wy[v]);
+    }
+    J.exh[k] = ex;
+    J.eyh[k] = ey;
+  }
+}
+
+struct PoissonGroup {
+  // per stage: problems and each one's first tile; the spectral jobs
+  GemmProblem *probs[4] = {};
+  int *first[4] = {};
+  int count[4] = {}, tiles[4] = {};
+  SpectralJob *jobs = nullptr;
+  int n_jobs = 0, job_blocks = 0;
+};
+
+PoissonGroup *poisson_group_create(PoissonPlan *const *plans, const float *const *density, float *const *field_x, float *const *field_y, int n, cudaError_t *err) {
+  *err = cudaSuccess;
+  PoissonGroup *g = new PoissonGroup();
+  std::vector<GemmProblem> st[4];
+  std::vector<SpectralJob> jobs;
+  int jb = 0;
+  for (int k = 0; k < n; k++) {
+    PoissonPlan *p = plans[k];
+    if (p->mode != 0) {
+      *err = cudaErrorInvalidValue;  // the FP32 form's plans only
+      poisson_group_destroy(g);
+      return nullptr;
+    }
+    const int nx = p->nx, ny = p->ny;
+    st[0].push_back(GemmProblem{ny, nx, ny, p->CyTs, ny, density[k], ny, p->t1, nx});
+    st[1].push_back(GemmProblem{nx, ny, nx, p->CxTs, nx, p->t1, nx, p->ah, ny});
+    st[2].push_back(GemmProblem{ny, nx, ny, p->Cy, ny, p->exh, ny, p->t2, nx});
+    st[2].push_back(GemmProblem{ny, nx, ny, p->Sy, ny, p->eyh, ny, p->t3, nx});
+    st[3].push_back(GemmProblem{nx, ny, nx, p->Sx, nx, p->t2, nx, field_x[k], ny});
+    st[3].push_back(GemmProblem{nx, ny, nx, p->Cx, nx, p->t3, nx, field_y[k], ny});
+    const int64_t cells = (int64_t)nx * ny;
+    const int blocks = (int)std::min<int64_t>((cells + 255) / 256, 148 * 8);
+    jobs.push_back(SpectralJob{nx, ny, jb, blocks, p->ah, p->wx, p->wx2, p->wy, p->wy2, p->exh, p->eyh});
+    jb += blocks;
+  }
+  auto put = [&](auto **d, const auto &v) {
+    if (*err != cudaSuccess || v.empty()) return;
+    using E = typename std::remove_reference<decltype(v)>::type::value_type;
+    *err = cudaMalloc((void **)d, v.size() * sizeof(E));
+    if (*err == cudaSuccess) *err = cudaMemcpy(*d, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice);
+  };
+  for (int q = 0; q < 4; q++) {
+    std::vector<int> first;
+    int t = 0;
+    for (const GemmProblem &P : st[q]) {
+      first.push_back(t);
+      t += ((P.M + SG_BM - 1) / SG_BM) * ((P.N + SG_BN - 1) / SG_BN);
+    }
+    g->count[q] = (int)st[q].size();
+    g->tiles[q] = t;
+    put(&g->probs[q], st[q]);
+    put(&g->first[q], first);
+  }
+  g->n_jobs = (int)jobs.size();
+  g->job_blocks = jb;
+  put(&g->jobs, jobs);
+  if (*err != cudaSuccess) {
+    poisson_group_destroy(g);
+    return nullptr;
+  }
+  return g;
+}
+
+void poisson_group_destroy(PoissonGroup *g) {
+  if (!g) return;
+  for (int q = 0; q < 4; q++) {
+    if (g->probs[q]) cudaFree(g->probs[q]);
+    if (g->first[q]) cudaFree(g->first[q]);
+  }
+  if (g->jobs) cudaFree(g->jobs);
+  delete g;
+}
+
+cudaError_t poisson_group_solve(const PoissonGroup *g, cudaStream_t s) {
+  if (!g || g->n_jobs == 0) return cudaSuccess;
+  for (int q = 0; q < 4; q++) {
+    k_gemm_grouped<<<g->tiles[q], 256, 0, s>>>(g->probs[q], g->first[q], g->count[q]);
+    if (q == 1) k_spectral_grouped<<<g->job_blocks, 256, 0, s>>>(g->jobs, g->n_jobs);
+  }
+  return cudaGetLastError();
+}
+
+int poisson_group_launches(const PoissonGroup *g) { return g && g->n_jobs ? 5 : 0; }
 
 cudaError_t poisson_solve(PoissonPlan *p, const float *density, float *field_x, float *field_y, cudaStream_t s) {
   if (p->mode == 2) return solve_fp64(p, density, field_x, field_y, s);

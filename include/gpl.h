@@ -160,6 +160,10 @@ void gpl_destroy(gpl_ctx *ctx);
  *   "reorder" = "1" (the default) | "0": the device's cell order sorted again by position when
  *               the cells have moved apart (no result depends on the order but the double sums'
  *               last bits), or kept as uploaded
+ *   "packed"  = "auto" (the default: on with more than one region) | "1" | "0": each Nesterov
+ *               phase (scatter, bin finalize, FP32 density solve, gradient update) of every
+ *               region in one launch, or one launch a region; the results are the same bit
+ *               for bit
  * Returns 0, or -1 for an unknown name or value. */
 int gpl_set_option(gpl_ctx *ctx, const char *name, const char *value);
 
@@ -183,7 +187,7 @@ gpl_session *gpl_session_open(gpl_ctx *ctx, const gpl_design_t *design, int argc
 int gpl_session_iterate(gpl_session *s, int n, int *done);
 /* "poisson" = "mixed" | "fp32" | "fp64" (solvers rebuilt, the field recomputed); "profile" = "0" | "1"
  * (per-phase device time from CUDA events); "overlap" = "1" | "0" (the WA beside the density
- * solve or after it); "reorder" as gpl_set_option's. No reference counterpart. */
+ * solve or after it); "reorder" and "packed" as gpl_set_option's. No reference counterpart. */
 int gpl_session_set_option(gpl_session *s, const char *name, const char *value);
 /* Per-phase device milliseconds and launch counts since "profile" was set: scatter, bin
  * finalize, density solve, WA, gradients, HPWL. Returns the number of phases written. */

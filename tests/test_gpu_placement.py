@@ -161,6 +161,34 @@ def test_region_groups_match_the_oracle():
     assert abs(got["final_overflow"] - ref["final_overflow"]) <= 0.005
 
 
+def _run_packed(d, args, packed):
+    p = engine.Placer(0)
+    try:
+        p.set_option("packed", packed)
+        return p.global_placement(d, args)
+    finally:
+        p.close()
+
+
+@pytest.mark.parametrize("cfg,over", [("cfg4s", {}), ("cfg4", dict(cells=120_000, nets=126_000, region_cells=(48, 300, 8_000)))])
+def test_packed_launches_give_the_same_run(cfg, over):
+    """Every region's scatter, bin finalize, FP32 density solve and gradient update as one
+    launch per phase (the default with regions) against one launch per region: each region's
+    blocks do what its own launch's would, so the runs are identical bit for bit (report lines,
+    iterations, final HPWL and overflow, written placement). The second design has 48 uneven
+    region groups beside the top level (bin grids from 16 to 128 a side)."""
+    d = synth.generate(cfg, **over)
+    args = ["-density", "0.70"]
+    a = _run_packed(d, args, "1")
+    b = _run_packed(d, args, "0")
+    assert a["status"] == b["status"] == "placed", (a["reason"], b["reason"])
+    assert a["lines"] == b["lines"]
+    assert a["nesterov_iterations"] == b["nesterov_iterations"]
+    assert a["final_hpwl"] == b["final_hpwl"] and a["final_overflow"] == b["final_overflow"]
+    assert np.array_equal(a["locations"], b["locations"])
+    assert a["launches"] < b["launches"]
+
+
 DIVERGE = ("GPL-0323", "GPL-0324", "GPL-0998", "GPL-0997", "GPL-0307")
 
 

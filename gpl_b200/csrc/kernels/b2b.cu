@@ -16,6 +16,7 @@
 #include "engine_kernels.h"
 
 namespace gpl {
+void progress(const char *fmt, ...) __attribute__((format(printf, 1, 2)));
 
 namespace {
 
@@ -393,40 +394,77 @@ __global__ void __launch_bounds__(kThreads) k_row_collapse_block(const int32_t *
   }
 }
 
-// The longest rows, a thread each: Shell's sort in place, then the runs.
-__global__ void k_row_collapse_long(const int32_t *list, const int *count, const int64_t *row_off, unsigned long long *bucket, const float *val, int32_t *ucol, float *uval, int64_t *ucount) {
-  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < *count; w += (int64_t)gridDim.x * blockDim.x) {
+// The longest rows, a block each: chunks of kRowLong keys bitonic-sorted in shared memory and
+// written back, then runs merged pairwise between the bucket and a scratch of the same span
+// (merge path: each thread's share of a merged run starts where a binary search on its
+// diagonal puts it, then it merges that share in order) until one run remains, which a warp
+// walks as the other tiers do.
+__device__ __forceinline__ void merge_share(const unsigned long long *A, int64_t la, const unsigned long long *B, int64_t lb, unsigned long long *out) {
+  const int64_t total = la + lb, per = (total + blockDim.x - 1) / blockDim.x;
+  const int64_t d = (int64_t)threadIdx.x * per;
+  if (d >= total) return;
+  int64_t lo = d > lb ? d - lb : 0, hi = d < la ? d : la;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (A[mid] < B[d - 1 - mid]) lo = mid + 1; else hi = mid;
+  }
+  int64_t i = lo, j = d - lo;
+  const int64_t end = d + per < total ? d + per : total;
+  for (int64_t k = d; k < end; k++) out[k] = (j >= lb || (i < la && A[i] < B[j])) ? A[i++] : B[j++];
+}
+
+__global__ void __launch_bounds__(kThreads) k_row_collapse_long(const int32_t *list, const int *count, const int64_t *row_off, unsigned long long *bucket, unsigned long long *scratch, const float *val, int32_t *ucol, float *uval, int64_t *ucount) {
+  extern __shared__ unsigned long long skl[];
+  const int64_t total = *count;
+  for (int64_t w = blockIdx.x; w < total; w += gridDim.x) {
     const int64_t r = list[w];
     const int64_t b = row_off[r], e = row_off[r + 1], m = e - b;
-    unsigned long long *k = bucket + b;
-    const int gaps[] = {1750, 701, 301, 132, 57, 23, 10, 4, 1};
-    for (int gi = 0; gi < 9; gi++) {
-      const int64_t g = gaps[gi];
-      if (g >= m) continue;
-      for (int64_t i = g; i < m; i++) {
-        unsigned long long v = k[i];
-        int64_t j = i;
-        while (j >= g && v < k[j - g]) {
-          k[j] = k[j - g];
-          j -= g;
+    unsigned long long *keys = bucket + b, *tmp = scratch + b;
+    for (int64_t c0 = 0; c0 < m; c0 += kRowLong) {
+      const int cm = (int)(m - c0 < kRowLong ? m - c0 : kRowLong);
+      int N = 1;
+      while (N < cm) N <<= 1;
+      for (int i = threadIdx.x; i < N; i += blockDim.x) skl[i] = i < cm ? keys[c0 + i] : ~0ull;
+      __syncthreads();
+      for (int k = 2; k <= N; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+          for (int i = threadIdx.x; i < N; i += blockDim.x) {
+            const int o = i ^ j;
+            if (o > i) {
+              const bool up = (i & k) == 0;
+              unsigned long long x = skl[i], y = skl[o];
+              if (up ? (x > y) : (x < y)) {
+                skl[i] = y;
+                skl[o] = x;
+              }
+            }
+          }
+          __syncthreads();
         }
-        k[j] = v;
+      for (int i = threadIdx.x; i < cm; i += blockDim.x) keys[c0 + i] = skl[i];
+      __syncthreads();
+    }
+    unsigned long long *src = keys, *dst = tmp;
+    for (int64_t run = kRowLong; run < m; run <<= 1) {
+      for (int64_t a0 = 0; a0 < m; a0 += 2 * run) {
+        const int64_t la = run < m - a0 ? run : m - a0;
+        const int64_t lb = a0 + run < m ? (a0 + 2 * run < m ? run : m - a0 - run) : 0;
+        merge_share(src + a0, la, src + a0 + la, lb, dst + a0);
       }
+      __syncthreads();
+      unsigned long long *t = src;
+      src = dst;
+      dst = t;
     }
-    int64_t u = 0, i = 0;
-    while (i < m) {
-      unsigned long long key = k[i];
-      uint32_t c = (uint32_t)(key >> 32);
-      int64_t j = i + 1;
-      while (j < m && (uint32_t)(k[j] >> 32) == c) j++;
-      float s = val[(uint32_t)key];
-      for (int64_t q = i + 1; q < j; q++) s = __fadd_rn(s, val[(uint32_t)k[q]]);
-      ucol[b + u] = (int32_t)c;
-      uval[b + u] = s;
-      u++;
-      i = j;
+    if (src != keys) {
+      for (int64_t i = threadIdx.x; i < m; i += blockDim.x) keys[i] = src[i];
+      __syncthreads();
     }
-    ucount[r] = u;
+    if (threadIdx.x < 32) {
+      const int64_t u = warp_runs(keys, (int)m, b, val, ucol, uval);
+      if (threadIdx.x == 0) ucount[r] = u;
+    }
+    __syncthreads();
   }
 }
 
@@ -659,7 +697,7 @@ IpDevice::~IpDevice() { release(); }
 
 void IpDevice::release() {
   void *ptrs[] = {box_, clamp_, db_box_, pin_static_, db_size_, pin_off_, pin_xy_, locked_, grouped_, pin_mio_, pin_hp_, pin_flag_, pin_e_, pin_inst_, locked_rank_,
-                  net_start_, cnt_, scan_tmp_, t_row_, t_col_, t_val_, r_row_, r_val_, bucket_, fill_, row_off_, ucount_, ucol_, uval_, scratch_, hpwl_acc_, tier_rows_, tier_n_};
+                  net_start_, cnt_, scan_tmp_, t_row_, t_col_, t_val_, r_row_, r_val_, bucket_, bucket2_, fill_, row_off_, ucount_, ucol_, uval_, scratch_, hpwl_acc_, tier_rows_, tier_n_};
   for (void *p : ptrs)
     if (p) cudaFreeAsync(p, s_);
   for (void *p : {(void *)perm_, (void *)inv_, (void *)ord_idx_, (void *)ord_hist_, (void *)ord_key0_, (void *)ord_key1_})
@@ -680,7 +718,7 @@ void IpDevice::release() {
   net_start_ = cnt_ = scan_tmp_ = row_off_ = ucount_ = nullptr;
   t_row_ = t_col_ = r_row_ = fill_ = ucol_ = nullptr;
   t_val_ = r_val_ = uval_ = nullptr;
-  bucket_ = nullptr;
+  bucket_ = bucket2_ = nullptr;
   scratch_ = nullptr;
   hpwl_acc_ = nullptr;
   tier_rows_ = nullptr;
@@ -723,6 +761,7 @@ cudaError_t IpDevice::upload(const IpSetup &s) {
   CK(alloc(&row_off_, n_ + 1, s_));
   CK(alloc(&ucount_, n_ + 1, s_));
   CK(cudaFuncSetAttribute(k_row_collapse_block, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
+  CK(cudaFuncSetAttribute(k_row_collapse_long, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
   CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1), s_));
   CK(alloc(&tier_n_, 3, s_));
   CK(alloc(&fill_, n_, s_));
@@ -780,7 +819,7 @@ cudaError_t IpDevice::collapse(int64_t n_trip, const int32_t *row, const int32_t
     k_row_collapse_warp<kRowShort / 32><<<wblocks, kThreads, 0, s_>>>(n_, nullptr, nullptr, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_, tier_n_);
     k_row_collapse_warp<kRowMid / 32><<<148 * 4, kThreads, 0, s_>>>(n_, tier_rows_, tier_n_, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_ + n_, tier_n_ + 1);
     k_row_collapse_block<<<148 * 2, kThreads, kRowLong * sizeof(unsigned long long), s_>>>(tier_rows_ + n_, tier_n_ + 1, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_ + 2 * n_, tier_n_ + 2);
-    k_row_collapse_long<<<148, kThreads, 0, s_>>>(tier_rows_ + 2 * n_, tier_n_ + 2, row_off_, bucket_, val, ucol_, uval_, ucount_);
+    k_row_collapse_long<<<148 * 2, kThreads, kRowLong * sizeof(unsigned long long), s_>>>(tier_rows_ + 2 * n_, tier_n_ + 2, row_off_, bucket_, bucket2_, val, ucol_, uval_, ucount_);
     launches += 4;
   }
   launches += 2;
@@ -809,12 +848,13 @@ cudaError_t IpDevice::csr_from_triplets(int64_t n, int64_t nt, const int32_t *ro
   keep_pool_once();
   n_ = n;
   CK(cudaFuncSetAttribute(k_row_collapse_block, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
+  CK(cudaFuncSetAttribute(k_row_collapse_long, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
   CK(alloc(&row_off_, n_ + 1, s_));
   CK(alloc(&ucount_, n_ + 1, s_));
   CK(alloc(&fill_, n_, s_));
   CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1), s_));
   CK(alloc(&tier_n_, 3, s_));
-  CK(grow(s_, (size_t)std::max<int64_t>(nt, 1), w_cap_, &bucket_, &ucol_, &uval_));
+  CK(grow(s_, (size_t)std::max<int64_t>(nt, 1), w_cap_, &bucket_, &bucket2_, &ucol_, &uval_));
   size_t cap = (size_t)std::max<int64_t>(nt, 1);  // nnz <= nt: the caller's buffers suffice
   int32_t *c = cols;
   float *v = vals;
@@ -848,12 +888,18 @@ cudaError_t IpDevice::assemble(IpAxisResult out[2]) {
   for (int q = 0; q < 4; q++) CK(cudaMemcpyAsync(&tot[q], cnt_ + q * stride + n_nets_, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
   CK(cudaStreamSynchronize(s_));
   d2h_bytes += 32;
+  const bool first = t_cap_ == 0;
+  if (first) progress("    round 1: triplets counted");
   // both axes side by side: x's triplets (the locked diagonal first) then y's; the same
   // for the right-hand-side terms
   const int64_t nt[2] = {n_locked_ + tot[0], n_locked_ + tot[1]}, nr[2] = {tot[2], tot[3]};
   CK(grow(s_, (size_t)(nt[0] + nt[1]), t_cap_, &t_row_, &t_col_, &t_val_));
   CK(grow(s_, (size_t)(nr[0] + nr[1]), r_cap_, &r_row_, &r_val_));
-  CK(grow(s_, (size_t)std::max({nt[0], nt[1], nr[0], nr[1]}), w_cap_, &bucket_, &ucol_, &uval_));
+  CK(grow(s_, (size_t)std::max({nt[0], nt[1], nr[0], nr[1]}), w_cap_, &bucket_, &bucket2_, &ucol_, &uval_));
+  if (first) {
+    CK(cudaStreamSynchronize(s_));
+    progress("    round 1: triplet buffers allocated");
+  }
   AxisOut ox{}, oy{};
   ox.t_row = t_row_, ox.t_col = t_col_, ox.t_val = t_val_;
   oy.t_row = t_row_ + nt[0], oy.t_col = t_col_ + nt[0], oy.t_val = t_val_ + nt[0];

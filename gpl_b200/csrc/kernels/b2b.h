@@ -100,6 +100,7 @@ class IpDevice {
   float *t_val_ = nullptr, *r_val_ = nullptr;
   size_t t_cap_ = 0, r_cap_ = 0, w_cap_ = 0;
   unsigned long long *bucket_ = nullptr;  // (column << 32 | position) per triplet, by row
+  unsigned long long *bucket2_ = nullptr; // the longest rows' merge scratch, as long
   int32_t *fill_ = nullptr;
   int64_t *row_off_ = nullptr, *ucount_ = nullptr;
   int32_t *tier_rows_ = nullptr;  // [3][n]: rows handed to the collapse's later tiers

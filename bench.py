@@ -42,7 +42,16 @@ CONFIGS = {
     "cfg3": dict(preset="cfg3", args=["-density", "0.70", "-bin_grid_count", "1024"], name="1M cells / 1.05M nets / 4M pins, 1024x1024 bins"),
     "cfg2": dict(preset="cfg2", args=["-density", "0.70", "-bin_grid_count", "512"], name="100k cells / 105k nets / 400k pins, 512x512 bins"),
     "cfg1": dict(preset="cfg1", args=["-density", "0.70", "-bin_grid_count", "64"], name="294 cells / 364 nets / 1122 pins, 64x64 bins"),
+    # the batched form: 48 region groups and the top level, each its own bin grid (the placer's
+    # rule: 32..256 a side for the groups, 1024 for the top level), one launch per phase
+    "cfg4": dict(preset="cfg4", args=["-density", "0.70"], name="2.4M cells / 2.52M nets / 10M pins in 48 region groups and the top level, per-region bin grids"),
 }
+
+
+def grid_side(cfg):
+    """The -bin_grid_count of a configuration, or None (each region's grid by the placer's rule)."""
+    a = cfg["args"]
+    return int(a[a.index("-bin_grid_count") + 1]) if "-bin_grid_count" in a else None
 
 
 def peaks():
@@ -164,8 +173,15 @@ class Clocks:
                 "edge_only": not self.rows and self.f is None}
 
 
-def algorithmic(phase, C, P, N, B, mixed, nx):
-    """Bytes (or FLOPs) one launch of a phase must move (compulsory traffic), per region."""
+def solve_flops(regions):
+    """The density solves' FLOPs over every region: six GEMMs of 2 nx ny K flops each (K = ny for
+    the three y transforms, nx for the x ones), three products apiece in the split-BF16 form."""
+    return sum((3.0 if r["form"] == 1 else 1.0) * 6.0 * r["nx"] * r["ny"] * (r["nx"] + r["ny"]) for r in regions)
+
+
+def algorithmic(phase, C, P, N, B, mixed, flops):
+    """Bytes (or FLOPs) one launch of a phase must move (compulsory traffic), over every region
+    (B: the bins of every region; flops: the density solves' FLOPs)."""
     if phase == "scatter":
         return "hbm", C * 61 + B * 16  # cell state in, next/next_slp/centre out; the two int64 accumulators
     if phase == "bin_finalize":
@@ -177,8 +193,7 @@ def algorithmic(phase, C, P, N, B, mixed, nx):
     if phase == "hpwl":
         return "hbm", N * 8 + P * 20
     if phase == "density_solve":
-        n3 = float(nx) ** 3
-        return "tensor" if mixed else "fp32", (36.0 if mixed else 12.0) * n3
+        return "tensor" if mixed else "fp32", flops
     return "hbm", 0
 
 
@@ -209,10 +224,10 @@ START = {
 def workload(a, design):
     """The workload as both arms name it: the same keys and values in either line."""
     cfg = CONFIGS[a.config]
-    nx = int(cfg["args"][cfg["args"].index("-bin_grid_count") + 1])
+    nx = grid_side(cfg)
     m = design.meta
     return {"workload": cfg["name"], "args": cfg["args"], "design": m["config"], "cells": m["cells"], "nets": m["nets"],
-            "pins": m["pins"], "bins": nx * nx, "start": START[a.start] if not a.start_from else "a saved initial placement",
+            "pins": m["pins"], "bins": nx * nx if nx else "each region its own grid", "start": START[a.start] if not a.start_from else "a saved initial placement",
             "timed": f"Nesterov iterations {a.warmup + 1}..{a.warmup + a.steps} of the loop (iteration = step)",
             "parallelism": "replicas x1", "l2": "working set > L2 (126 MB): cells, pins and bins stream from HBM each trial"}
 
@@ -302,6 +317,8 @@ def ours(a):
         return prof
 
     cells_total = sess.counters()["cells"]
+    regions = sess.regions()
+    B = sum(r["nx"] * r["ny"] for r in regions)
     if a.form == "mixed":
         mixed = timed(a.steps)
         mixed["profile"] = phase_times(min(a.steps, 10))
@@ -316,8 +333,7 @@ def ours(a):
     res = sess.close()
     log("session closed")
     P_pins, N_nets = res["pins"], res["nets"]
-    nx = int(cfg["args"][cfg["args"].index("-bin_grid_count") + 1])
-    B = nx * nx
+    nx = max(max(r["nx"], r["ny"]) for r in regions)
     # e2e: the whole command through the public C ABI, host arrays in (construction and the
     # initial placement included), locations out
     e2e = None
@@ -346,7 +362,7 @@ def ours(a):
     prof = mixed["profile"]
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     name, (ms_tot, launches) = dom
-    bound, work = algorithmic(name, cells_total, P_pins, N_nets, B, a.form == "mixed", nx)
+    bound, work = algorithmic(name, cells_total, P_pins, N_nets, B, a.form == "mixed", solve_flops(regions))
     per_launch_s = ms_tot / 1000.0 / max(launches, 1)
     if bound == "fp32":
         achieved = work / per_launch_s / 1e12
@@ -438,8 +454,9 @@ def precision_runs(local, cfg):
 def cpu_sample(a):
     """The oracle (the reference's CPU path restated; one thread, as the reference runs) on the
     same workload as the device's timed loop: the same design, start and arguments, the same
-    warm-up iterations untimed, then the same K iterations timed. The reference arm and the
-    GPU line's cpu_baseline are this one sample."""
+    warm-up iterations untimed, then the same K iterations timed, or the first of them that
+    end within --cpu-seconds (a bounded sample). The reference arm and the GPU line's
+    cpu_baseline are this one sample."""
     import oracle
     design, args = loop_design(a)
     t0 = time.perf_counter()
@@ -447,8 +464,14 @@ def cpu_sample(a):
     setup = time.perf_counter() - t0
     s.iterate(a.warmup)
     tr0 = s.trials()
+    # a bounded sample: the K iterations, or as many of them as end within --cpu-seconds
     t0 = time.perf_counter()
-    done = s.iterate(a.steps)
+    done = 0
+    while done < a.steps:
+        k = s.iterate(1)
+        done += k
+        if k == 0 or time.perf_counter() - t0 > a.cpu_seconds:
+            break
     dt = time.perf_counter() - t0
     trials = s.trials() - tr0
     s.discard()
@@ -477,12 +500,13 @@ def reference(a):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="cfg3", choices=list(CONFIGS))
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=30.0, help="the CPU sample's bound: the timed iterations end once they have taken this long")
     ap.add_argument("--no-precision-runs", action="store_true", help="skip the three whole commands (mixed, FP32, FP64 density solves) of the precision report")
     ap.add_argument("--form", default="mixed", choices=["mixed", "fp32"], help="the density solve timed as the headline")
     ap.add_argument("--start", default="spread", choices=["spread", "ip"],

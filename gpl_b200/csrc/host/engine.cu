@@ -107,7 +107,32 @@ void Engine::join() {
   wa_pending_ = false;
 }
 
+void Engine::prewarm(size_t bytes) {
+  prewarm_join();
+  const int dev = device_;
+  prewarm_ = new std::thread([dev, bytes] {
+    if (cudaSetDevice(dev) != cudaSuccess) return;
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return;
+    keep_device_pool();
+    void *p = nullptr;
+    if (bytes && cudaMallocAsync(&p, bytes, s) == cudaSuccess) cudaFreeAsync(p, s);
+    load_kernel_modules();
+    cudaStreamSynchronize(s);
+    cudaStreamDestroy(s);
+    cudaGetLastError();  // nothing of it is an error of the command's
+  });
+}
+
+void Engine::prewarm_join() {
+  if (!prewarm_) return;
+  prewarm_->join();
+  delete prewarm_;
+  prewarm_ = nullptr;
+}
+
 Engine::~Engine() {
+  prewarm_join();
   release();
   delete queue_;
   if (pk_host_) cudaFreeHost(pk_host_);
@@ -177,6 +202,7 @@ void Engine::release() {
 }
 
 void Engine::upload(const EngineSetup &s) {
+  prewarm_join();
   release();
   hpwl_ready_ = hpwl_fetched_ = false;  // the density centres move
   if (failed()) return;
@@ -831,6 +857,14 @@ void Engine::flush_grad(const std::vector<QueueEntry> &q, size_t a, size_t b) {
   launches += 1;
   ph_end(PH_GRAD);
   check(cudaGetLastError(), "packed gradients");
+}
+
+void Engine::region_info(int b, int32_t out[4]) const {
+  const Region *r = regions_[b];
+  out[0] = region_dims_[b].first;
+  out[1] = region_dims_[b].second;
+  out[2] = (int32_t)r->n_cells;
+  out[3] = r->plan ? poisson_plan_mode(r->plan) : -1;
 }
 
 std::string Engine::tuning() const {

@@ -5,6 +5,7 @@
 #include <cstdint>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -75,6 +76,14 @@ class Engine {
   void upload(const EngineSetup &s);
   void release();
   int regions() const { return (int)regions_.size(); }
+  // While the host builds the placer: a thread that grows the device pool by `bytes` (kept
+  // once freed, so the initial placement's and the regions' buffers come from it without
+  // mapping new memory) and loads the kernels' modules (loaded at first use otherwise).
+  // prewarm_join() waits for it; every device call of the command comes after that.
+  void prewarm(size_t bytes);
+  void prewarm_join();
+  // Region b's bin grid, cells, and its density solver's form (0 FP32, 1 split-BF16, 2 FP64).
+  void region_info(int b, int32_t out[4]) const;
   void set_coords(int b, SlotId slot, const std::vector<float> &xy);  // 2 floats per cell
   std::vector<float> get_coords(int b, SlotId slot);
   // The density centres at `slot` (PLACE_AT) and the bins; the overflow sums.
@@ -187,6 +196,7 @@ class Engine {
   cudaStream_t wa_stream_ = nullptr;
   cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
   std::unique_ptr<Tuner> wa_tune_;
+  std::thread *prewarm_ = nullptr;
   // packed launches: the queue of (phase, region) with each entry's arguments as queued, the
   // tables' page-locked staging and device copy, the grouped FP32 solves of the live set
   enum Queued { Q_PLACE = 0, Q_FIELD, Q_GRAD };

@@ -1911,19 +1911,35 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
   };
   for (auto &nb : P.nbs) {
     nb.cell_off = (int64_t)P.gcell_of_dev.size();
-    std::vector<std::pair<uint64_t, int>> keyed;
-    keyed.reserve(nb.cells.size());
-    for (int gi : nb.cells) {
-      const GCell &g = P.gcells[gi];
-      double fx = 16.0 * ((double)g.d_cx() - nb.bg.lx) / std::max(nb.bg.size_x, 1.0);
-      double fy = 16.0 * ((double)g.d_cy() - nb.bg.ly) / std::max(nb.bg.size_y, 1.0);
-      uint32_t qx = (uint32_t)std::min(std::max(fx, 0.0), 65535.0), qy = (uint32_t)std::min(std::max(fy, 0.0), 65535.0);
-      keyed.push_back({hilbert(qx, qy), gi});
+    const size_t m = nb.cells.size();
+    std::vector<uint32_t> key(m), key2(m);
+    std::vector<int> idx(m), idx2(m);
+    parallel_for(m, [&](size_t a, size_t b) {
+      for (size_t k = a; k < b; k++) {
+        const GCell &g = P.gcells[nb.cells[k]];
+        double fx = 16.0 * ((double)g.d_cx() - nb.bg.lx) / std::max(nb.bg.size_x, 1.0);
+        double fy = 16.0 * ((double)g.d_cy() - nb.bg.ly) / std::max(nb.bg.size_y, 1.0);
+        uint32_t qx = (uint32_t)std::min(std::max(fx, 0.0), 65535.0), qy = (uint32_t)std::min(std::max(fy, 0.0), 65535.0);
+        key[k] = (uint32_t)hilbert(qx, qy);  // below 2^32 on a 2^16 square
+        idx[k] = nb.cells[k];
+      }
+    });
+    // stable: two LSD passes of 16-bit digits (the order of a stable sort by key)
+    for (int shift = 0; shift < 32; shift += 16) {
+      std::vector<size_t> cnt(65537, 0);
+      for (size_t k = 0; k < m; k++) cnt[((key[k] >> shift) & 0xffffu) + 1]++;
+      for (size_t q = 1; q < cnt.size(); q++) cnt[q] += cnt[q - 1];
+      for (size_t k = 0; k < m; k++) {
+        const size_t at = cnt[(key[k] >> shift) & 0xffffu]++;
+        key2[at] = key[k];
+        idx2[at] = idx[k];
+      }
+      key.swap(key2);
+      idx.swap(idx2);
     }
-    std::stable_sort(keyed.begin(), keyed.end(), [](const std::pair<uint64_t, int> &a, const std::pair<uint64_t, int> &b) { return a.first < b.first; });
-    for (auto &kv : keyed) {
-      P.dev_of_gcell[kv.second] = (int64_t)P.gcell_of_dev.size();
-      P.gcell_of_dev.push_back(kv.second);
+    for (int gi : idx) {
+      P.dev_of_gcell[gi] = (int64_t)P.gcell_of_dev.size();
+      P.gcell_of_dev.push_back(gi);
     }
   }
   progress("  device set-up: cells in Hilbert order");
@@ -2228,6 +2244,7 @@ struct Run {
     progress("placer built: %zu instances, %zu nets, %zu bases", c.insts.size(), c.nets.size(), bases.size());
     auto t0 = std::chrono::steady_clock::now();
     {
+      eng.prewarm_join();
       IpDevice dev(eng.stream());
       ip = do_bicgstab_place_device(log, d, c, vars, ipv, dev);
       eng.launches += dev.launches;
@@ -2428,6 +2445,14 @@ int gpl_set_option(gpl_ctx *c, const char *name, const char *value) {
   return -1;
 }
 
+// The device memory a command on this design takes at most, about: the initial placement's
+// triplets, collapse and solver copies (some 400 bytes a pin), which the Nesterov state then
+// reuses from the pool.
+static size_t prewarm_bytes(const gpl_design_t *cd) {
+  const int64_t pins = cd->n_nets > 0 && cd->net_iterm_start ? cd->net_iterm_start[cd->n_nets] : 0;
+  return (size_t)std::max<int64_t>(pins, 0) * 400 + ((size_t)64 << 20);
+}
+
 static void reset_counters(Engine &e) {
   e.launches = 0;
   e.h2d_bytes = 0;
@@ -2442,6 +2467,7 @@ int gpl_global_placement(gpl_ctx *ctx, const gpl_design_t *cd, int argc, const c
   run->res.log.trace_on = ctx->trace;
   guarded(run->res, [&] {
     progress("command start");
+    ctx->eng->prewarm(prewarm_bytes(cd));
     run->d = design_from_c(cd);
     progress("design read: %zu instances, %zu nets", run->d.insts.size(), run->d.nets.size());
     run->open(std::vector<std::string>(argv, argv + argc), router);
@@ -2466,6 +2492,7 @@ gpl_session *gpl_session_open(gpl_ctx *ctx, const gpl_design_t *cd, int argc, co
   auto *s = new gpl_session{ctx, std::make_unique<Run>(*ctx->eng)};
   s->run->res.log.trace_on = ctx->trace;
   guarded(s->run->res, [&] {
+    ctx->eng->prewarm(prewarm_bytes(cd));
     s->run->d = design_from_c(cd);
     s->run->open(std::vector<std::string>(argv, argv + argc), router);
   });
@@ -2527,6 +2554,12 @@ void gpl_session_counters(gpl_session *s, int64_t out[6]) {
   out[3] = s->run->P ? (int64_t)s->run->P->gcell_of_dev.size() : 0;
   out[4] = s->ctx->eng->trials;
   out[5] = s->ctx->eng->reorders;
+}
+
+int gpl_session_regions(gpl_session *s, int32_t *out, int cap) {
+  Engine &e = *s->ctx->eng;
+  for (int b = 0; b < e.regions() && b < cap; b++) e.region_info(b, out + 4 * b);
+  return e.regions();
 }
 
 int gpl_session_tuning(gpl_session *s, char *buf, int cap) {

@@ -1084,4 +1084,11 @@ cudaError_t IpDevice::download(std::vector<int4> &box, std::vector<int4> &db_box
 
 void keep_device_pool() { keep_pool_once(); }
 
+
+// Loads this file's module (the driver loads a module at its first launch otherwise).
+void load_module_b2b() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, k_emit);
+}
+
 }  // namespace gpl

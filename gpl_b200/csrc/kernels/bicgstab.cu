@@ -785,4 +785,11 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
   return cudaGetLastError();
 }
 
+
+// Loads this file's module (the driver loads a module at its first launch otherwise).
+void load_module_bicgstab() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, k2_update_xr);
+}
+
 }  // namespace gpl

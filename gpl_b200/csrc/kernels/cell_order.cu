@@ -240,4 +240,11 @@ static cudaError_t order_passes(int32_t n, uint32_t *key0, int32_t *idx0, uint32
   return cudaGetLastError();  // the sorted (key, old index) pairs are back in key0, idx0
 }
 
+
+// Loads this file's module (the driver loads a module at its first launch otherwise).
+void load_module_cell_order() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, k_order_scatter);
+}
+
 }  // namespace gpl

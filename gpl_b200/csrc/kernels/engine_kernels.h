@@ -180,6 +180,14 @@ __nv_bfloat16 *poisson_split_input(PoissonPlan *p, int *ld);
 // Fill the split-BF16 operand from a float density (when no bin finalize wrote it).
 cudaError_t poisson_split_density(PoissonPlan *p, const float *density, cudaStream_t s);
 size_t poisson_workspace_bytes(int nx, int ny);
+// Loads the modules of the engine's kernels (each translation unit's), which the driver
+// otherwise loads at their first launch.
+void load_kernel_modules();
+void load_module_b2b();
+void load_module_bicgstab();
+void load_module_poisson();
+void load_module_poisson_tc();
+void load_module_cell_order();
 // Kernel launches one poisson_solve makes.
 int poisson_launches(const PoissonPlan *p);
 // The FP32 solves of n plans (mode 0) with their densities and fields fixed, as five

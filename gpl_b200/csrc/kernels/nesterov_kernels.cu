@@ -1226,4 +1226,15 @@ __global__ void k_hold_locked(RegionArgs r, CellArgs c) {
   c.next[i] = c.cur[i];
 }
 
+
+void load_kernel_modules() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, k_place_cells);
+  load_module_b2b();
+  load_module_bicgstab();
+  load_module_poisson();
+  load_module_poisson_tc();
+  load_module_cell_order();
+}
+
 }  // namespace gpl

@@ -497,4 +497,11 @@ cudaError_t poisson_solve(PoissonPlan *p, const float *density, float *field_x, 
   return sgemm_tn(g, 2, s);
 }
 
+
+// Loads this file's module (the driver loads a module at its first launch otherwise).
+void load_module_poisson() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, k_gemm_grouped);
+}
+
 }  // namespace gpl

@@ -437,4 +437,11 @@ int tc_error(const PoissonPlan *p) {
   return h;
 }
 
+
+// Loads this file's module (the driver loads a module at its first launch otherwise).
+void load_module_poisson_tc() {
+  cudaFuncAttributes a;
+  cudaFuncGetAttributes(&a, k_tc_gemm<EPI_SPLIT, 64>);
+}
+
 }  // namespace gpl

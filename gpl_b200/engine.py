@@ -127,6 +127,7 @@ def _session_lib():
         L.gpl_session_stream.argtypes = [C.c_void_p]
         L.gpl_session_counters.argtypes = [C.c_void_p, C.POINTER(C.c_int64)]
         L.gpl_session_tuning.argtypes = [C.c_void_p, C.c_char_p, C.c_int]
+        L.gpl_session_regions.argtypes = [C.c_void_p, C.POINTER(C.c_int32), C.c_int]
         L.gpl_session_close.argtypes = [C.c_void_p, C.POINTER(gpl_result_t)]
         L._session_ready = True
     return L
@@ -165,6 +166,14 @@ class Session:
         out = (C.c_int64 * 6)()
         _session_lib().gpl_session_counters(self._h, out)
         return {"launches": out[0], "h2d_bytes": out[1], "d2h_bytes": out[2], "cells": out[3], "trials": out[4], "reorders": out[5]}
+
+    def regions(self):
+        """Each Nesterov region's bin grid, cells and density solver form (0 FP32, 1 split-BF16, 2 FP64)."""
+        L = _session_lib()
+        n = L.gpl_session_regions(self._h, None, 0)
+        buf = (C.c_int32 * (4 * max(n, 1)))()
+        L.gpl_session_regions(self._h, buf, n)
+        return [dict(nx=buf[4 * b], ny=buf[4 * b + 1], cells=buf[4 * b + 2], form=buf[4 * b + 3]) for b in range(n)]
 
     def tuning(self) -> str:
         """The autotuner's choices so far and its candidates' median times (text)."""

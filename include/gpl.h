@@ -197,6 +197,10 @@ int gpl_session_profile(gpl_session *s, double *ms, int64_t *launches, int cap);
  * (`do_back_tracking`'s passes, src/nesterov.rs:2776-2808) and the times the engine sorted its
  * device cells again (the "reorder" option) since the session opened (6 int64). */
 void gpl_session_counters(gpl_session *s, int64_t out[6]);
+/* The Nesterov regions on the device: for each (up to cap) its bin grid (nx, ny), its cells
+ * (instances and fillers) and its density solver's form (0 FP32, 1 split-BF16 tensor cores,
+ * 2 FP64), 4 int32 a region. Returns the region count. */
+int gpl_session_regions(gpl_session *s, int32_t *out, int cap);
 /* The engine's autotuner so far, as text: for each tuned launch group (the small nets' WA
  * form, each region's scatter form) the form in use and its candidates' median times in
  * microseconds. Writes at most cap bytes (NUL included) to buf; returns the text's length. */

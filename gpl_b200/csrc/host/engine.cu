@@ -197,6 +197,7 @@ void Engine::release() {
     poisson_plan_destroy(r->plan);
     delete r;
   }
+  if (!regions_.empty()) progress("  release: regions freed");
   regions_.clear();
   free_globals();
 }

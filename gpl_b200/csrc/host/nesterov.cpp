@@ -2477,6 +2477,7 @@ int gpl_global_placement(gpl_ctx *ctx, const gpl_design_t *cd, int argc, const c
   run->res.h2d = ctx->eng->h2d_bytes;
   run->res.d2h = ctx->eng->d2h_bytes;
   run->res.launches = ctx->eng->launches;
+  progress("  release: start");
   ctx->eng->release();
   progress("device memory released");
   fill_result(run->res, out);

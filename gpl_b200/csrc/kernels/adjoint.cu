@@ -20,6 +20,7 @@
 
 #include "../../../include/gpl.h"
 #include "common.cuh"
+#include "poisson_internal.h"
 
 namespace gpl {
 
@@ -191,54 +192,84 @@ std::vector<double> cos_basis(int n) {
   return c;
 }
 
-// phi = G rho over the grid; scratch of 3 nx*ny doubles plus the two bases (device).
-cudaError_t potential(const Grid &g, const double *rho, double *phi, cudaStream_t s) {
-  int nx = g.nx, ny = g.ny;
-  size_t nb = (size_t)nx * ny;
-  std::vector<double> hx = cos_basis(nx), hy = cos_basis(ny);
-  double *cx = nullptr, *cy = nullptr, *t1 = nullptr, *t2 = nullptr;
-  cudaError_t e = cudaMallocAsync((void **)&cx, hx.size() * sizeof(double), s);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&cy, hy.size() * sizeof(double), s);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&t1, nb * sizeof(double), s);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&t2, nb * sizeof(double), s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(cx, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(cy, hy.data(), hy.size() * sizeof(double), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess) {
-    dim3 th(16, 16);
-    auto grid2 = [&](int M, int N) { return dim3((N + 15) / 16, (M + 15) / 16); };
-    // A^ = Cx rho Cy^T, scaled, then phi = Cx^T A^ Cy
-    k_dgemm<false><<<grid2(nx, ny), th, 0, s>>>(nx, ny, nx, cx, rho, t1);        // t1 = Cx rho
-    k_dgemm<true><<<grid2(nx, ny), th, 0, s>>>(nx, ny, ny, t1, cy, t2);          // t2 = t1 Cy^T
-    k_spectral_scale<<<blocks((int64_t)nb), kThreads, 0, s>>>(nx, ny, g.bh / g.bw, t2);
-    // t1 = Cx^T t2: with Cx^T as A, read Cx transposed through the BT form on a copy
-    std::vector<double> hxt((size_t)nx * nx), hyt((size_t)ny * ny);
-    for (int a = 0; a < nx; a++)
-      for (int b = 0; b < nx; b++) hxt[(size_t)a * nx + b] = hx[(size_t)b * nx + a];
-    e = cudaMemcpyAsync(cx, hxt.data(), hxt.size() * sizeof(double), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // hxt outlives the copy
-    if (e == cudaSuccess) {
-      k_dgemm<false><<<grid2(nx, ny), th, 0, s>>>(nx, ny, nx, cx, t2, t1);       // t1 = Cx^T t2
-      k_dgemm<false><<<grid2(nx, ny), th, 0, s>>>(nx, ny, ny, t1, cy, phi);      // phi = t1 Cy
-      e = cudaGetLastError();
-    }
-  }
-  cudaError_t e2 = cudaStreamSynchronize(s);
-  cudaFreeAsync(cx, s);
-  cudaFreeAsync(cy, s);
-  cudaFreeAsync(t1, s);
-  cudaFreeAsync(t2, s);
-  cudaStreamSynchronize(s);
-  return e != cudaSuccess ? e : e2;
+}  // namespace
+
+// The density objective's plan: the grid, the DCT bases on the device (Cy, Cx and their
+// transposes) and the solve's buffers, made once for many evaluations.
+struct DensityPlan {
+  Grid g{};
+  double *cx = nullptr, *cxt = nullptr, *cy = nullptr, *cyt = nullptr;
+  double *rho = nullptr, *phi = nullptr, *t1 = nullptr, *t2 = nullptr;
+  cudaStream_t s = nullptr;
+};
+
+namespace {
+
+void plan_free(DensityPlan *p) {
+  for (double *b : {p->cx, p->cxt, p->cy, p->cyt, p->rho, p->phi, p->t1, p->t2})
+    if (b) cudaFreeAsync(b, p->s);
+  cudaStreamSynchronize(p->s);
+  delete p;
 }
 
-cudaError_t density_phi(int64_t n, const double *xy, const double *half, const double *scale, const Grid &g, double **rho, double **phi, cudaStream_t s) {
-  size_t nb = (size_t)g.nx * g.ny;
-  cudaError_t e = cudaMallocAsync((void **)rho, nb * sizeof(double), s);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)phi, nb * sizeof(double), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(*rho, 0, nb * sizeof(double), s);
-  if (e == cudaSuccess && n > 0) k_rho<<<blocks(n), kThreads, 0, s>>>(n, xy, half, scale, g, *rho);
+DensityPlan *plan_make(const Grid &g, cudaStream_t s, cudaError_t *err) {
+  DensityPlan *p = new DensityPlan();
+  p->g = g;
+  p->s = s;
+  const size_t nb = (size_t)g.nx * g.ny;
+  std::vector<double> hx = cos_basis(g.nx), hy = g.ny == g.nx ? hx : cos_basis(g.ny);
+  std::vector<double> hxt((size_t)g.nx * g.nx), hyt((size_t)g.ny * g.ny);
+  for (int a = 0; a < g.nx; a++)
+    for (int b = 0; b < g.nx; b++) hxt[(size_t)a * g.nx + b] = hx[(size_t)b * g.nx + a];
+  for (int a = 0; a < g.ny; a++)
+    for (int b = 0; b < g.ny; b++) hyt[(size_t)a * g.ny + b] = hy[(size_t)b * g.ny + a];
+  cudaError_t e = cudaSuccess;
+  auto put = [&](double **d, const std::vector<double> &h) {
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)d, h.size() * sizeof(double), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s);
+  };
+  put(&p->cx, hx);
+  put(&p->cxt, hxt);
+  put(&p->cy, hy);
+  put(&p->cyt, hyt);
+  for (double **b : {&p->rho, &p->phi, &p->t1, &p->t2})
+    if (e == cudaSuccess) e = cudaMallocAsync((void **)b, nb * sizeof(double), s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the host bases outlive their copies
+  *err = e;
+  if (e != cudaSuccess) {
+    plan_free(p);
+    return nullptr;
+  }
+  return p;
+}
+
+// phi = G rho: A^ = Cx rho Cy^T (two GEMMs), scaled, then phi = Cx^T A^ Cy (two more), each
+// a D = A B^T product of the tiled double GEMM.
+cudaError_t potential(DensityPlan *p, cudaStream_t s) {
+  const int nx = p->g.nx, ny = p->g.ny;
+  GemmBatchT<double> b{};
+  b.p[0] = GemmProblemT<double>{ny, nx, ny, p->cy, ny, p->rho, ny, p->t1, nx};   // t1[v][x] = sum_y Cy[v][y] rho[x][y]
+  cudaError_t e = dgemm_tn(b, 1, s);
+  b.p[0] = GemmProblemT<double>{nx, ny, nx, p->cx, nx, p->t1, nx, p->t2, ny};    // A^[u][v] = sum_x Cx[u][x] t1[v][x]
+  if (e == cudaSuccess) e = dgemm_tn(b, 1, s);
+  if (e == cudaSuccess) {
+    k_spectral_scale<<<blocks((int64_t)nx * ny), kThreads, 0, s>>>(nx, ny, p->g.bh / p->g.bw, p->t2);
+    e = cudaGetLastError();
+  }
+  b.p[0] = GemmProblemT<double>{ny, nx, ny, p->cyt, ny, p->t2, ny, p->t1, nx};   // t1[y][u] = sum_v Cy[v][y] A^[u][v]
+  if (e == cudaSuccess) e = dgemm_tn(b, 1, s);
+  b.p[0] = GemmProblemT<double>{nx, ny, nx, p->cxt, nx, p->t1, nx, p->phi, ny};  // phi[x][y] = sum_u Cx[u][x] t1[y][u]
+  if (e == cudaSuccess) e = dgemm_tn(b, 1, s);
+  return e;
+}
+
+// The cells' density rho and its potential phi on the plan's buffers.
+cudaError_t density_phi(DensityPlan *p, int64_t n, const double *xy, const double *half, const double *scale, cudaStream_t s) {
+  const size_t nb = (size_t)p->g.nx * p->g.ny;
+  cudaError_t e = cudaMemsetAsync(p->rho, 0, nb * sizeof(double), s);
+  if (e == cudaSuccess && n > 0) k_rho<<<blocks(n), kThreads, 0, s>>>(n, xy, half, scale, p->g, p->rho);
   if (e == cudaSuccess) e = cudaGetLastError();
-  if (e == cudaSuccess) e = potential(g, *rho, *phi, s);
+  if (e == cudaSuccess) e = potential(p, s);
   return e;
 }
 
@@ -367,33 +398,49 @@ int gpl_fn_wa_backward(int64_t n_nets, const int64_t *net_start, const double *p
   return (int)(e != cudaSuccess ? e : e2);
 }
 
-int gpl_fn_density_forward(int64_t n_cells, const double *cell_xy, const double *half, const double *scale, int32_t nx, int32_t ny, double grid_lx, double grid_ly, double bin_w, double bin_h, double *energy, void *stream) {
-  cudaStream_t s = (cudaStream_t)stream;
-  Grid g{nx, ny, grid_lx, grid_ly, bin_w, bin_h};
-  double *rho = nullptr, *phi = nullptr;
-  cudaError_t e = density_phi(n_cells, cell_xy, half, scale, g, &rho, &phi, s);
-  double d = 0;
-  if (e == cudaSuccess) e = dot((int64_t)nx * ny, rho, phi, &d, s);
-  *energy = 0.5 * d;
-  cudaFreeAsync(rho, s);
-  cudaFreeAsync(phi, s);
+gpl_fn_density *gpl_fn_density_create(int32_t nx, int32_t ny, double grid_lx, double grid_ly, double bin_w, double bin_h, void *stream) {
+  if (nx <= 0 || ny <= 0 || !(bin_w > 0) || !(bin_h > 0)) return nullptr;
+  cudaError_t e = cudaSuccess;
+  DensityPlan *p = plan_make(Grid{nx, ny, grid_lx, grid_ly, bin_w, bin_h}, (cudaStream_t)stream, &e);
+  return reinterpret_cast<gpl_fn_density *>(p);
+}
+
+void gpl_fn_density_destroy(gpl_fn_density *f) {
+  if (f) plan_free(reinterpret_cast<DensityPlan *>(f));
+}
+
+int gpl_fn_density_eval(gpl_fn_density *f, int64_t n_cells, const double *cell_xy, const double *half, const double *scale, double *energy, double seed, double *grad) {
+  DensityPlan *p = reinterpret_cast<DensityPlan *>(f);
+  if (!p) return (int)cudaErrorInvalidValue;
+  cudaStream_t s = p->s;
+  cudaError_t e = density_phi(p, n_cells, cell_xy, half, scale, s);
+  if (energy) {
+    double d = 0;
+    if (e == cudaSuccess) e = dot((int64_t)p->g.nx * p->g.ny, p->rho, p->phi, &d, s);
+    *energy = 0.5 * d;
+  }
+  if (grad && e == cudaSuccess && n_cells > 0) {
+    k_rho_adjoint<<<blocks(n_cells), kThreads, 0, s>>>(n_cells, cell_xy, half, scale, p->g, p->phi, seed, grad);
+    e = cudaGetLastError();
+  }
   cudaError_t e2 = cudaStreamSynchronize(s);
   return (int)(e != cudaSuccess ? e : e2);
 }
 
+int gpl_fn_density_forward(int64_t n_cells, const double *cell_xy, const double *half, const double *scale, int32_t nx, int32_t ny, double grid_lx, double grid_ly, double bin_w, double bin_h, double *energy, void *stream) {
+  gpl_fn_density *f = gpl_fn_density_create(nx, ny, grid_lx, grid_ly, bin_w, bin_h, stream);
+  if (!f) return (int)cudaErrorInvalidValue;
+  const int r = gpl_fn_density_eval(f, n_cells, cell_xy, half, scale, energy, 0.0, nullptr);
+  gpl_fn_density_destroy(f);
+  return r;
+}
+
 int gpl_fn_density_backward(int64_t n_cells, const double *cell_xy, const double *half, const double *scale, int32_t nx, int32_t ny, double grid_lx, double grid_ly, double bin_w, double bin_h, double seed, double *grad, void *stream) {
-  cudaStream_t s = (cudaStream_t)stream;
-  Grid g{nx, ny, grid_lx, grid_ly, bin_w, bin_h};
-  double *rho = nullptr, *phi = nullptr;
-  cudaError_t e = density_phi(n_cells, cell_xy, half, scale, g, &rho, &phi, s);
-  if (e == cudaSuccess && n_cells > 0) {
-    k_rho_adjoint<<<blocks(n_cells), kThreads, 0, s>>>(n_cells, cell_xy, half, scale, g, phi, seed, grad);
-    e = cudaGetLastError();
-  }
-  cudaFreeAsync(rho, s);
-  cudaFreeAsync(phi, s);
-  cudaError_t e2 = cudaStreamSynchronize(s);
-  return (int)(e != cudaSuccess ? e : e2);
+  gpl_fn_density *f = gpl_fn_density_create(nx, ny, grid_lx, grid_ly, bin_w, bin_h, stream);
+  if (!f) return (int)cudaErrorInvalidValue;
+  const int r = gpl_fn_density_eval(f, n_cells, cell_xy, half, scale, nullptr, seed, grad);
+  gpl_fn_density_destroy(f);
+  return r;
 }
 
 }  // extern "C"

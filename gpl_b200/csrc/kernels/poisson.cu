@@ -137,6 +137,7 @@ cudaError_t gemm_tn(const GemmBatchT<T> &gb, int count, cudaStream_t s) {
   return cudaGetLastError();
 }
 cudaError_t sgemm_tn(const GemmBatch &gb, int count, cudaStream_t s) { return gemm_tn<float>(gb, count, s); }
+cudaError_t dgemm_tn(const GemmBatchT<double> &gb, int count, cudaStream_t s) { return gemm_tn<double>(gb, count, s); }
 
 // ---------------------------------------------------------------- the spectral step
 // (src/nesterov.rs:425-440) on the scaled forward transform: phi = Ah / (wx2 + wy2),

@@ -26,6 +26,7 @@ struct GemmBatchT {
 using GemmProblem = GemmProblemT<float>;
 using GemmBatch = GemmBatchT<float>;
 cudaError_t sgemm_tn(const GemmBatch &gb, int count, cudaStream_t s);
+cudaError_t dgemm_tn(const GemmBatchT<double> &gb, int count, cudaStream_t s);
 
 // The six basis matrices in double (see poisson.cu): CyTs[v][y], CxTs[u][x] (forward, scaled
 // and halved), Cy[y][v], Sy[y][v], Sx[x][u], Cx[x][u] (inverses).

@@ -390,6 +390,17 @@ int gpl_fn_density_backward(int64_t n_cells, const double *cell_xy, const double
                             const double *scale, int32_t nx, int32_t ny, double grid_lx,
                             double grid_ly, double bin_w, double bin_h, double seed,
                             double *grad, void *stream);
+/* The same objective with its grid planned once (the DCT bases on the device, the solve's
+ * buffers), for many evaluations: eval writes the energy (when energy is not NULL) and
+ * seed * dE/d(cell x, y) into grad (when grad is not NULL) for the cells given. create
+ * returns NULL for an empty grid or a failed allocation. */
+typedef struct gpl_fn_density gpl_fn_density;
+gpl_fn_density *gpl_fn_density_create(int32_t nx, int32_t ny, double grid_lx, double grid_ly,
+                                      double bin_w, double bin_h, void *stream);
+int gpl_fn_density_eval(gpl_fn_density *f, int64_t n_cells, const double *cell_xy,
+                        const double *half, const double *scale, double *energy, double seed,
+                        double *grad);
+void gpl_fn_density_destroy(gpl_fn_density *f);
 
 #ifdef __cplusplus
 }

@@ -179,3 +179,137 @@ def test_density_adjoint_follows_the_reference_force(L):
                               C.c_double(bw), C.c_double(bh), a(fx), a(fy), a(ref))
     cos = np.dot(-g, ref) / (np.linalg.norm(g) * np.linalg.norm(ref))
     assert cos > 0.99, cos
+
+
+def test_autograd_functions_give_the_adjoints(L):
+    """The objectives as torch.autograd functions (gpl_b200.functions): their values are the
+    forward entry points' and a backward through a weighted sum gives the adjoint entry
+    points' gradients, scaled."""
+    import torch
+    from gpl_b200 import functions as F
+    rng = np.random.default_rng(15)
+    start, xy, w = _nets(rng, 2000, 100000.0)
+    cx, cy = 7.5e-4, 9e-4
+    t_start, t_w = dev(start), dev(w)
+    pxy = torch.tensor(xy, dtype=torch.float64, device="cuda", requires_grad=True)
+    W = F.wirelength(pxy, t_start, t_w, cx, cy)
+    nx, ny, bw, bh = 64, 64, 1000.0, 1250.0
+    cxy_h, half_h, scale_h = _cells(rng, 3000, nx, ny, bw, bh)
+    cxy = torch.tensor(cxy_h, dtype=torch.float64, device="cuda", requires_grad=True)
+    fn = F.DensityEnergy(nx, ny, 0.0, 0.0, bw, bh)
+    t_half, t_scale = dev(half_h), dev(scale_h)
+    E = fn(cxy, t_half, t_scale)
+    (2.0 * W + 3.0 * E).backward()
+    v = C.c_double()
+    d_xy = dev(xy)
+    assert L.gpl_fn_wa_forward(len(start) - 1, ptr(t_start), ptr(d_xy), ptr(t_w), cx, cy, C.byref(v), stream()) == 0
+    assert W.item() == v.value
+    gw = dev(np.zeros(xy.size))
+    assert L.gpl_fn_wa_backward(len(start) - 1, ptr(t_start), ptr(d_xy), ptr(t_w), cx, cy, 2.0, ptr(gw), stream()) == 0
+    e = C.c_double()
+    d_cxy = dev(cxy_h)
+    assert L.gpl_fn_density_forward(len(cxy_h), ptr(d_cxy), ptr(t_half), ptr(t_scale), nx, ny, 0.0, 0.0, bw, bh, C.byref(e), stream()) == 0
+    assert E.item() == e.value
+    ge = dev(np.zeros(cxy_h.size))
+    assert L.gpl_fn_density_backward(len(cxy_h), ptr(d_cxy), ptr(t_half), ptr(t_scale), nx, ny, 0.0, 0.0, bw, bh, 3.0, ptr(ge), stream()) == 0
+    sync()
+    assert torch.equal(pxy.grad.reshape(-1), gw)
+    assert torch.equal(cxy.grad.reshape(-1), ge)
+    fn.close()
+
+
+def test_adjoints_match_finite_differences_at_2m_cells(L):
+    """The 2M-cell design (about 2.1M nets and 8.4M pins, its cells at the generator's spread
+    placement) on a 2048 x 2048 grid over its core: both adjoints over the whole design
+    against central differences (step 1e-3 site) on 1000 seeded cells, within 1e-4 (relative
+    to the larger of the gradient and 1e-3 of the largest). The WA coefficient is the one
+    the reference's schedule gives at overflow 0.5 (`update_wirelength_coef`,
+    src/nesterov.rs:2532-2542, base 0.25 over the mean bin side, :2576); a cell's WA difference is
+    taken over its own nets (no other net's term moves with it), the energy's over the whole
+    grid. Pins are the cells' (the IO ports' and the macros' are left out of the objective)."""
+    import torch
+    from gpl_b200 import functions as F, synth
+    d = synth.generate("cfg5", placed=True)
+    m = d.meta["cells"]
+    box = d.inst_box[:m].astype(np.float64)
+    cxy_h = np.stack([(box[:, 0] + box[:, 2]) / 2, (box[:, 1] + box[:, 3]) / 2], 1)
+    half_h = np.stack([(box[:, 2] - box[:, 0]) / 2, (box[:, 3] - box[:, 1]) / 2], 1)
+    # the cells' pins, net by net (each pin at its cell's corner plus its shape's centre)
+    ist = d.net_iterm_start
+    inst = d.iterm_inst.astype(np.int64)
+    keep = inst < m
+    net_of = np.repeat(np.arange(len(ist) - 1), np.diff(ist))[keep]
+    pin_cell = inst[keep]
+    shp = d.iterm_shape[keep].astype(np.float64)
+    off = np.stack([(shp[:, 0] + shp[:, 2]) / 2, (shp[:, 1] + shp[:, 3]) / 2], 1)
+    start = np.concatenate([[0], np.cumsum(np.bincount(net_of, minlength=len(ist) - 1))]).astype(np.int64)
+    pxy_h = box[pin_cell, :2] + off
+    w = np.ones(len(start) - 1, np.float32)
+    core_w, core_h = d.core[2] - d.core[0], d.core[3] - d.core[1]
+    n = 2048
+    bw, bh = core_w / n, core_h / n
+    base = 0.25 / ((bw + bh) * 0.5)
+    coef = base / 10.0 ** ((0.5 - 0.1) * 20.0 / 9.0 - 1.0)
+    t_start, t_w = dev(start), dev(w)
+    # the adjoints over the whole design
+    g_pin = dev(np.zeros(pxy_h.size))
+    d_pxy = dev(pxy_h)
+    assert L.gpl_fn_wa_backward(len(start) - 1, ptr(t_start), ptr(d_pxy), ptr(t_w), coef, coef, 1.0, ptr(g_pin), stream()) == 0
+    fn = F.DensityEnergy(n, n, float(d.core[0]), float(d.core[1]), bw, bh)
+    cxy = torch.tensor(cxy_h, dtype=torch.float64, device="cuda")
+    t_half, t_scale = dev(half_h), dev(np.ones(m))
+    g_den = torch.zeros_like(cxy)
+    assert L.gpl_fn_density_eval(C.c_void_p(fn._f), m, ptr(cxy), ptr(t_half), ptr(t_scale), None, 1.0, ptr(g_den)) == 0
+    sync()
+    g_pin = g_pin.cpu().numpy().reshape(-1, 2)
+    g_wa = np.zeros((m, 2))
+    np.add.at(g_wa, pin_cell, g_pin)
+    g_den = g_den.cpu().numpy()
+    rng = np.random.default_rng(16)
+
+    def clear(i):
+        for a, size, lo in ((0, bw, d.core[0]), (1, bh, d.core[1])):
+            for edge in (cxy_h[i, a] - half_h[i, a], cxy_h[i, a] + half_h[i, a]):
+                f = (edge - lo) / size
+                if abs(f - round(f)) * size < 2 * H:
+                    return False
+        return True
+
+    cells = [int(i) for i in rng.permutation(m)[:1200] if clear(i)][:1000]
+    assert len(cells) == 1000
+    # the cells' nets and pins, for the local WA differences
+    order = np.argsort(pin_cell, kind="stable")
+    cstart = np.searchsorted(pin_cell[order], np.arange(m + 1))
+    e = C.c_double()
+    fd_wa, fd_den, a_wa, a_den = [], [], [], []
+    for i in cells:
+        pins = order[cstart[i]:cstart[i + 1]]
+        nets = np.unique(net_of[pins])
+        sub = np.concatenate([np.arange(start[k], start[k + 1]) for k in nets])
+        s_start = np.concatenate([[0], np.cumsum(start[nets + 1] - start[nets])]).astype(np.int64)
+        mine = np.isin(sub, pins)
+        d_s, d_w = dev(s_start), dev(np.ones(len(nets), np.float32))
+        for a in range(2):
+            vals = []
+            for sgn in (1.0, -1.0):
+                p = pxy_h[sub].copy()
+                p[mine, a] += sgn * H
+                d_p = dev(p)
+                v = C.c_double()
+                assert L.gpl_fn_wa_forward(len(nets), ptr(d_s), ptr(d_p), ptr(d_w), coef, coef, C.byref(v), stream()) == 0
+                vals.append(v.value)
+            fd_wa.append((vals[0] - vals[1]) / (2 * H))
+            a_wa.append(g_wa[i, a])
+            vals = []
+            for sgn in (1.0, -1.0):
+                cxy[i, a] += sgn * H
+                assert L.gpl_fn_density_eval(C.c_void_p(fn._f), m, ptr(cxy), ptr(t_half), ptr(t_scale), C.byref(e), 0.0, None) == 0
+                cxy[i, a] = float(cxy_h[i, a])
+                vals.append(e.value)
+            fd_den.append((vals[0] - vals[1]) / (2 * H))
+            a_den.append(g_den[i, a])
+    fn.close()
+    print("2M-cell adjoints: WA max rel err", np.max(np.abs(np.array(fd_wa) - a_wa) / np.maximum(np.abs(a_wa), 1e-3 * np.max(np.abs(a_wa)))),
+          "density max rel err", np.max(np.abs(np.array(fd_den) - a_den) / np.maximum(np.abs(a_den), 1e-3 * np.max(np.abs(a_den)))))
+    _check(np.array(fd_wa), np.array(a_wa))
+    _check(np.array(fd_den), np.array(a_den))

@@ -184,7 +184,8 @@ def test_density_adjoint_follows_the_reference_force(L):
 def test_autograd_functions_give_the_adjoints(L):
     """The objectives as torch.autograd functions (gpl_b200.functions): their values are the
     forward entry points' and a backward through a weighted sum gives the adjoint entry
-    points' gradients, scaled."""
+    points' gradients, scaled (the WA's bit for bit; the energy's to the last bits its
+    double-precision bin sums leave to the order of their atomic adds)."""
     import torch
     from gpl_b200 import functions as F
     rng = np.random.default_rng(15)
@@ -209,12 +210,13 @@ def test_autograd_functions_give_the_adjoints(L):
     e = C.c_double()
     d_cxy = dev(cxy_h)
     assert L.gpl_fn_density_forward(len(cxy_h), ptr(d_cxy), ptr(t_half), ptr(t_scale), nx, ny, 0.0, 0.0, bw, bh, C.byref(e), stream()) == 0
-    assert E.item() == e.value
+    # the density's bins add in double with atomics, so its last bits vary from call to call
+    assert abs(E.item() - e.value) <= 1e-12 * abs(e.value)
     ge = dev(np.zeros(cxy_h.size))
     assert L.gpl_fn_density_backward(len(cxy_h), ptr(d_cxy), ptr(t_half), ptr(t_scale), nx, ny, 0.0, 0.0, bw, bh, 3.0, ptr(ge), stream()) == 0
     sync()
     assert torch.equal(pxy.grad.reshape(-1), gw)
-    assert torch.equal(cxy.grad.reshape(-1), ge)
+    assert torch.allclose(cxy.grad.reshape(-1), ge, rtol=1e-9, atol=1e-12 * float(ge.abs().max()))
     fn.close()
 
 

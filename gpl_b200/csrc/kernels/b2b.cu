@@ -995,7 +995,13 @@ cudaError_t IpDevice::solver_order() {
 
 cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
   // the forms give the same products bit for bit, so the choice changes only the speed
-  if (!spmv_tune_) spmv_tune_ = std::make_unique<Tuner>("initial placement SpMV", std::vector<std::string>{"0", "1", "2"}, "GPL_SPMV_FORM", 2, 48);
+  // GPL_SPMV_FORM=0|1|2 fixes the form (a thread per row, tiled, sliced); else the tuner picks
+  // between the tiled and the sliced form (a thread per row is never the faster)
+  if (!spmv_tune_) {
+    spmv_tune_ = std::make_unique<Tuner>("initial placement SpMV", std::vector<std::string>{"tiled", "sliced"}, nullptr, 2, 48);
+    if (const char *f = std::getenv("GPL_SPMV_FORM"))
+      if (f[0] >= '0' && f[0] <= '2' && f[1] == 0) spmv_fixed_ = f[0] - '0';
+  }
   if (ip_order_ < 0) {
     const char *f = std::getenv("GPL_IP_ORDER");
     ip_order_ = f && f[0] == '0' ? 0 : 1;
@@ -1005,7 +1011,7 @@ cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
   solves_++;
   if (ordered) CK(solver_order());
   // the sliced copies whenever the sliced form may run
-  const bool sliced = !spmv_tune_->fixed() || spmv_tune_->best() == kSpmvSliced;
+  const bool sliced = spmv_fixed_ < 0 || spmv_fixed_ == kSpmvSliced;
   CsrDev m[2];
   const float *b[2];
   float *x[2];
@@ -1026,8 +1032,9 @@ cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
     scratch[a] = (char *)scratch_ + a * scratch_bytes_;
   }
   BicgResult r[2]{};
-  Tuner *t = spmv_tune_->fixed() ? nullptr : spmv_tune_.get();
-  cudaError_t e = bicgstab_solve_pair(m, b, x, max_iters, scratch, s_, r, spmv_tune_->best(), t);
+  Tuner *t = spmv_fixed_ >= 0 ? nullptr : spmv_tune_.get();
+  const int form = spmv_fixed_ >= 0 ? spmv_fixed_ : kSpmvTiled + spmv_tune_->best();
+  cudaError_t e = bicgstab_solve_pair(m, b, x, max_iters, scratch, s_, r, form, t);
   const int iters = std::max(r[0].iterations, r[1].iterations);
   launches += 10 + (int64_t)iters * 5;
   d2h_bytes += (int64_t)(iters / 8 + 2) * 2 * 120;

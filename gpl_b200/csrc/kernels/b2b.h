@@ -77,12 +77,13 @@ class IpDevice {
   cudaError_t csr_from_triplets(int64_t n, int64_t nt, const int32_t *row, const int32_t *col, const float *val, int64_t *starts, int32_t *cols, float *vals, int64_t *nnz);
   int64_t launches = 0, h2d_bytes = 0, d2h_bytes = 0;
   // The SpMV tuner's choice and timings so far ("" before the first solve).
-  std::string tuning() const { return spmv_tune_ ? spmv_tune_->report() : std::string(); }
+  std::string tuning() const { return spmv_fixed_ >= 0 ? "initial placement SpMV: form " + std::to_string(spmv_fixed_) + " (fixed)" : spmv_tune_ ? spmv_tune_->report() : std::string(); }
 
  private:
   cudaStream_t s_;
   // the solver's SpMV form, by the tuner (GPL_SPMV_FORM 0 rows, 1 tiled, 2 sliced fixes it)
   std::unique_ptr<Tuner> spmv_tune_;
+  int spmv_fixed_ = -1;  // GPL_SPMV_FORM's form, or -1
   int64_t n_ = 0, n_pins_ = 0, n_locked_ = 0;
   int32_t n_nets_ = 0;
   IpSetup cfg_;

@@ -168,21 +168,20 @@ __device__ __forceinline__ void spmv_sliced_rows(int64_t n, int64_t n_long, cons
   const int32_t len = sl_len[j];
   const int64_t base = sl_start[i / kSliceRows] + (i % kSliceRows);
   const int2 *ent = sl_ent + base;
+  // kSpmvUnroll entries at a time, the last group's loads predicated, so every group costs
+  // two dependent round trips (its entries, then their x) whatever the row's length; the
+  // products still add in column order
   float tmp = 0.0f;
-  int32_t k = 0;
-  for (; k + kSpmvUnroll <= len; k += kSpmvUnroll) {
+  for (int32_t k = 0; k < len; k += kSpmvUnroll) {
     int2 cv[kSpmvUnroll];
     float xv[kSpmvUnroll];
 #pragma unroll
-    for (int u = 0; u < kSpmvUnroll; u++) cv[u] = __ldg(ent + (int64_t)(k + u) * kSliceRows);
+    for (int u = 0; u < kSpmvUnroll; u++) cv[u] = k + u < len ? __ldg(ent + (int64_t)(k + u) * kSliceRows) : make_int2(0, 0);
 #pragma unroll
-    for (int u = 0; u < kSpmvUnroll; u++) xv[u] = __ldg(x + cv[u].x);
+    for (int u = 0; u < kSpmvUnroll; u++) xv[u] = k + u < len ? __ldg(x + cv[u].x) : 0.0f;
 #pragma unroll
-    for (int u = 0; u < kSpmvUnroll; u++) tmp = __fadd_rn(tmp, __fmul_rn(__int_as_float(cv[u].y), xv[u]));
-  }
-  for (; k < len; k++) {
-    const int2 cv = __ldg(ent + (int64_t)k * kSliceRows);
-    tmp = __fadd_rn(tmp, __fmul_rn(__int_as_float(cv.y), __ldg(x + cv.x)));
+    for (int u = 0; u < kSpmvUnroll; u++)
+      if (k + u < len) tmp = __fadd_rn(tmp, __fmul_rn(__int_as_float(cv[u].y), xv[u]));
   }
   emit(sl_row[j], __fadd_rn(0.0f, __fmul_rn(1.0f, tmp)));
 }
@@ -753,7 +752,7 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
   const dim3 ge(eb, 2), gr(rb, 2);
   const dim3 gs((unsigned)std::max<int64_t>({sliced_blocks(n, A[0].sl_long), sliced_blocks(n, A[1].sl_long), 1}), 2);
   for (;;) {
-    const int f = tune ? tune->start(st) : form;
+    const int f = tune ? kSpmvTiled + tune->start(st) : form;  // the tuner's candidates: tiled, sliced
     for (int k = 0; k < kBicgBatch; k++) {
       k2_update_p<<<ge, kThreads, 0, st>>>(P);
       for (int sel = 0; sel < 2; sel++) {

@@ -66,8 +66,9 @@ cudaError_t spmv(const CsrDev &A, const float *x, float *y, int form, cudaStream
 // that follow it (the same sums in another fixed order); scratch[a] holds
 // bicgstab_pair_scratch_bytes(n) bytes for system a.
 size_t bicgstab_pair_scratch_bytes(int64_t n);
-// With `tune`, each batch of iterations runs the SpMV form the tuner picks (every form then
-// needs A's sliced copy), timed in place; `spmv` is then the form of the start and restarts.
+// With `tune` (two candidates: the tiled and the sliced form), each batch of iterations runs
+// the form the tuner picks (A then needs its sliced copy), timed in place; `spmv` is then the
+// form of the start and restarts.
 cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], float *const x[2], int max_iters, void *const scratch[2], cudaStream_t s, BicgResult out[2], int spmv = kSpmvRows, Tuner *tune = nullptr);
 
 }  // namespace gpl

@@ -358,3 +358,30 @@ def test_poisson_fp64_form_against_the_fp64_solve(L, nx, ny):
     for got, want in ((gx, hx), (gy, hy)):
         g, w = got.cpu().numpy().astype(np.float64), want.cpu().numpy()
         assert np.max(np.abs(g - w)) <= 1e-6 * np.max(np.abs(w))
+
+
+def test_rudy_on_a_1024_grid_matches_the_oracle(L):
+    """RUDY's difference-array form on a 1024 x 1024 tile grid with large boxes (up to a fifth
+    of the die a side, as the locality window's nets span), against the reference's per-tile
+    visit on the oracle."""
+    rng = np.random.default_rng(12)
+    die = np.array([0, 0, 1024 * 700 + 321, 1024 * 650 + 77], np.int32)
+    tile, cx, cy = 650, 1024, 1024
+    n = 4000
+    lo = rng.integers(0, 500000, (n, 2))
+    size = rng.integers(0, 140000, (n, 2))
+    boxes = np.concatenate([lo, lo + size], 1).astype(np.int32)
+    cap_red = np.tile(np.array([10, 0], np.uint8), cx * cy)
+    ww = C.c_int32()
+    rects = np.zeros(4 * cx * cy, np.int32)
+    dem, blk, cong = (np.zeros(cx * cy, np.float32) for _ in range(3))
+    pitches = np.array([380, 380, 380], np.int32)
+    oracle.lib().oracle_rudy(die.ctypes.data, cx, cy, tile, 3, pitches.ctypes.data, cap_red.ctypes.data, n, boxes.ctypes.data,
+                             C.byref(ww), rects.ctypes.data, dem.ctypes.data, blk.ctypes.data, cong.ctypes.data)
+    db = dev(boxes)
+    gd = dev(np.zeros(cx * cy, np.float32))
+    from gpl_b200 import engine
+    rc = engine.lib().gpl_kernel_rudy(n, ptr(db), *[int(v) for v in die], cx, cy, tile, ww.value, ptr(gd), stream())
+    sync()
+    assert rc == 0
+    np.testing.assert_allclose(gd.cpu().numpy(), dem, rtol=1e-5, atol=1e-3 * float(np.max(dem)) * 1e-2)

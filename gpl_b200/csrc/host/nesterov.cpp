@@ -465,7 +465,9 @@ struct RouteBase {
       final_average_rc = 0.0f;
       return;
     }
-    std::sort(cong.begin(), cong.end(), [](double a, double b) { return a > b; });
+    // only the top 5 % are summed (in descending order): sort those alone
+    const size_t top = std::min(cong.size(), (size_t)std::ceil(0.05 * (double)cong.size()) + 1);
+    std::partial_sort(cong.begin(), cong.begin() + top, cong.end(), [](double a, double b) { return a > b; });
     auto a = top_averages(cong);
     const float *k = vars.rc_k;
     double weighted = ((double)k[0] * a[0] + (double)k[1] * a[1] + (double)k[2] * a[2] + (double)k[3] * a[3]) / (double)(k[0] + k[1] + k[2] + k[3]);

@@ -146,3 +146,27 @@ def test_tuned_forms_give_the_same_run(monkeypatch):
         assert got["final_hpwl"] == base["final_hpwl"], fixed
         assert got["final_overflow"] == base["final_overflow"], fixed
         assert (got["locations"] == base["locations"]).all(), fixed
+
+
+def test_batched_form_matches_the_oracle():
+    """The batched form: 48 region groups of uneven size beside the top level (2.4M cells,
+    each region its own bin grid, every phase packed into one launch over the regions)
+    against the oracle's recorded run: identical construction lines, the initial placement's
+    rounds within 0.1 % (the first exact), final HPWL within 0.1 % and overflow within 0.005."""
+    if "cfg4" not in RUNS:
+        pytest.skip("no recorded oracle run for cfg4")
+    ref = RUNS["cfg4"]
+    d = synth.generate("cfg4")
+    got = engine.global_placement(d, ref["args"])
+    assert got["status"] == "placed", got["reason"]
+    assert header(got["lines"]) == ref["header"]
+    assert (got["insts"], got["nets"], got["pins"]) == (ref["insts"], ref["nets"], ref["pins"])
+    a, b = ip_hpwl(got["lines"]), ip_hpwl(ref["initial_place"])
+    assert len(a) == len(b) and a[0] == b[0]
+    for ha, hb in zip(a, b):
+        assert abs(ha - hb) <= 1e-3 * hb
+    print("cfg4 iterations", got["nesterov_iterations"], ref["nesterov_iterations"], "hpwl", got["final_hpwl"], ref["final_hpwl"],
+          "overflow", got["final_overflow"], ref["final_overflow"])
+    assert abs(got["final_hpwl"] - ref["final_hpwl"]) <= 1e-3 * ref["final_hpwl"]
+    assert abs(got["final_overflow"] - ref["final_overflow"]) <= 0.005
+    assert len(got["locations"]) == ref["locations"]

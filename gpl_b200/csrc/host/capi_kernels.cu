@@ -11,6 +11,7 @@
 #include "../kernels/bicgstab.h"
 #include "../kernels/engine_kernels.h"
 #include "../kernels/rudy.h"
+#include "parallel.h"
 
 using namespace gpl;
 
@@ -459,7 +460,9 @@ static int64_t sr_boxes(void *u, int32_t *idx, int32_t *boxes, int64_t cap) {
   SynthRouter *s = (SynthRouter *)u;
   int64_t nn = (int64_t)s->net_iterm_start.size() - 1;
   if (!boxes) return nn;
-  for (int64_t n = 0; n < nn && n < cap; n++) {
+  // each net's box from its own terminals: the nets in parallel
+  parallel_for((size_t)std::min(nn, cap), [&](size_t n0, size_t n1) {
+  for (int64_t n = (int64_t)n0; n < (int64_t)n1; n++) {
     int32_t lx = INT32_MAX, ly = INT32_MAX, ux = INT32_MIN, uy = INT32_MIN;
     for (int64_t t = s->net_iterm_start[n]; t < s->net_iterm_start[n + 1]; t++) {
       int32_t i = s->iterm_inst[t];
@@ -484,6 +487,7 @@ static int64_t sr_boxes(void *u, int32_t *idx, int32_t *boxes, int64_t cap) {
     boxes[4 * n + 2] = ux;
     boxes[4 * n + 3] = uy;
   }
+  });
   return std::min(nn, cap);
 }
 

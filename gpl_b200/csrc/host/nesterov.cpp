@@ -434,15 +434,19 @@ struct RouteBase {
       int i = tile_at(cx, cy);
       if (i >= 0) tiles[i].actionable = true;
     }
-    for (auto &t : tiles) {
-      if (rudy.blockage[rudy.at(t.x, t.y)] >= vars.ignore_edge_ratio) t.actionable = false;
-      if (!t.actionable) continue;
-      float ratio = rudy.congestion(t.x, t.y);
-      if (vars.min_congestion_for_inflation > 0.0f && ratio >= vars.min_congestion_for_inflation) {
-        float r = std::pow(ratio / vars.min_congestion_for_inflation, vars.inflation_ratio_coef);
-        t.inflation_ratio = fminr(r, vars.max_inflation_ratio);
+    // each tile's own flags and ratio: the tiles in parallel
+    parallel_for(tiles.size(), [&](size_t a, size_t b) {
+      for (size_t k = a; k < b; k++) {
+        Tile &t = tiles[k];
+        if (rudy.blockage[rudy.at(t.x, t.y)] >= vars.ignore_edge_ratio) t.actionable = false;
+        if (!t.actionable) continue;
+        float ratio = rudy.congestion(t.x, t.y);
+        if (vars.min_congestion_for_inflation > 0.0f && ratio >= vars.min_congestion_for_inflation) {
+          float r = std::pow(ratio / vars.min_congestion_for_inflation, vars.inflation_ratio_coef);
+          t.inflation_ratio = fminr(r, vars.max_inflation_ratio);
+        }
       }
-    }
+    });
   }
   // `updateRudyAverage` (src/route_base.rs:493-536).
   void update_rudy_average() {

@@ -1036,7 +1036,7 @@ cudaError_t IpDevice::solve(int max_iters, IpAxisResult out[2]) {
   const int form = spmv_fixed_ >= 0 ? spmv_fixed_ : kSpmvTiled + spmv_tune_->best();
   cudaError_t e = bicgstab_solve_pair(m, b, x, max_iters, scratch, s_, r, form, t);
   const int iters = std::max(r[0].iterations, r[1].iterations);
-  launches += 10 + (int64_t)iters * 5;
+  launches += 10 + (int64_t)iters * 7;
   d2h_bytes += (int64_t)(iters / 8 + 2) * 2 * 120;
   out[0].solve = r[0];
   out[1].solve = r[1];

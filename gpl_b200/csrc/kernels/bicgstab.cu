@@ -441,7 +441,6 @@ struct SysDev {
   float *x, *r, *r0, *v, *p, *s, *t;
   double *part, *S;
   unsigned int *ticket;
-  double *spart;  // the fused SpMV launches' block partials (3 per block)
 };
 struct SysPair {
   SysDev a[2];
@@ -452,60 +451,30 @@ __global__ void __launch_bounds__(kThreads) k2_update_p(SysPair P) {
   SysDev q = pick(P);
   update_p_body(q.n, q.S, q.r, q.v, q.p);
 }
-// sel 0: v = A p (then r0.v and alpha); sel 1: t = A s (then t.t, t.s and omega).
-// The SpMV with the iteration's inner products that follow it, in one launch: each thread's
-// row (if it formed one) adds its terms to the block's partials (sel 0: r0.v; sel 1: t.t and
-// t.s), and the last block to finish takes the scalar step (alpha, or omega). The sums are
-// those of k2_dots, in another fixed order.
-__device__ __forceinline__ void pair_dots_tail(const SysDev &q, int sel, bool have, int64_t row, float val) {
-  __shared__ double sh[kThreads / 32];
-  double d0 = 0.0, d1 = 0.0;
-  if (have) {
-    if (sel == 0) {
-      d0 = (double)q.r0[row] * (double)val;
-    } else {
-      d0 = (double)val * (double)val;
-      d1 = (double)val * (double)q.s[row];
-    }
-  }
-  const double t0 = block_sum<kThreads>(d0, sh);
-  const double t1 = block_sum<kThreads>(d1, sh);
-  if (threadIdx.x == 0) {
-    q.spart[3 * blockIdx.x] = t0;
-    q.spart[3 * blockIdx.x + 1] = t1;
-    q.spart[3 * blockIdx.x + 2] = 0.0;
-  }
-  if (last_block(q.ticket)) scalar_step(q.spart, gridDim.x, q.S, sel ? 2 : 1, 0, sh);
-}
-__global__ void __launch_bounds__(kThreads) k2_spmv_rows_dots(SysPair P, int sel) {
+// sel 0: v = A p; sel 1: t = A s (each system's rows in the form's order, gated as a whole).
+__global__ void __launch_bounds__(kThreads) k2_spmv_rows(SysPair P, int sel) {
   SysDev q = pick(P);
-  if (gated_off(q.S, kLive)) return;  // the whole system
-  float *y = sel ? q.t : q.v;
-  bool have = false;
-  int64_t row = 0;
-  float val = 0.0f;
-  spmv_rows_rows(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, [&](int64_t r, float v) { y[r] = v; have = true; row = r; val = v; });
-  pair_dots_tail(q, sel, have, row, val);
+  spmv_rows_body(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
 }
-__global__ void __launch_bounds__(kThreads) k2_spmv_tiled_dots(SysPair P, int sel) {
+__global__ void __launch_bounds__(kThreads) k2_spmv_tiled(SysPair P, int sel) {
   SysDev q = pick(P);
-  if (gated_off(q.S, kLive)) return;
-  float *y = sel ? q.t : q.v;
-  bool have = false;
-  int64_t row = 0;
-  float val = 0.0f;
-  spmv_tiled_rows(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, [&](int64_t r, float v) { y[r] = v; have = true; row = r; val = v; });
-  pair_dots_tail(q, sel, have, row, val);
+  spmv_tiled_body(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
 }
-__global__ void __launch_bounds__(kThreads) k2_spmv_sliced_dots(SysPair P, int sel) {
+__global__ void __launch_bounds__(kThreads) k2_spmv_sliced(SysPair P, int sel) {
   SysDev q = pick(P);
-  if (gated_off(q.S, kLive)) return;
-  float *y = sel ? q.t : q.v;
-  bool have = false;
-  int64_t row = 0;
-  float val = 0.0f;
-  spmv_sliced_rows(q.n, q.sl_long, q.rs, q.cols, q.vals, q.sl_row, q.sl_len, q.sl_start, q.sl_ent, sel ? q.s : q.p, [&](int64_t r, float v) { y[r] = v; have = true; row = r; val = v; });
-  pair_dots_tail(q, sel, have, row, val);
+  spmv_sliced_body(q.n, q.sl_long, q.rs, q.cols, q.vals, q.sl_row, q.sl_len, q.sl_start, q.sl_ent, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
+}
+// The inner products after each product, in their own launch over the vectors in order
+// (sel 0: r0.v, then alpha; sel 1: t.t and t.s, then omega), the last block taking the scalar
+// step. (Forming them in the SpMV's own launch was measured 11 % slower over the whole
+// initial placement: the sliced form's rows are in length order, so their r0 and s reads
+// scatter, and the fused tail's block reductions stall every block.)
+__global__ void k2_dots(SysPair P, int sel) {
+  SysDev q = pick(P);
+  if (sel == 0)
+    dots_body(q.n, q.r0, q.v, nullptr, nullptr, nullptr, nullptr, q.part, q.S, kLive, 1, q.ticket);
+  else
+    dots_body(q.n, q.t, q.t, q.t, q.s, nullptr, nullptr, q.part, q.S, kLive, 2, q.ticket);
 }
 
 __global__ void __launch_bounds__(kThreads) k2_update_s(SysPair P) {
@@ -541,13 +510,7 @@ size_t bicgstab_scratch_bytes(int64_t n) {
   return 7 * vec + (size_t)kBicgBlocks * 3 * sizeof(double) + 64 * sizeof(double);
 }
 
-// The fused SpMV launches' block partials after the single solve's scratch: 3 doubles for
-// each block any SpMV form launches (the sliced form's long rows take a block per 8 rows).
-static size_t pair_spart_offset(int64_t n) { return (bicgstab_scratch_bytes(n) + 255) / 256 * 256; }
-size_t bicgstab_pair_scratch_bytes(int64_t n) {
-  const int64_t blocks = (n + 7) / 8 + (n + kThreads - 1) / kThreads + 1;
-  return pair_spart_offset(n) + (size_t)blocks * 3 * sizeof(double);
-}
+size_t bicgstab_pair_scratch_bytes(int64_t n) { return bicgstab_scratch_bytes(n); }
 
 cudaError_t csr_slice_order(const CsrDev &A, int32_t *row, int32_t *len, int32_t *count, cudaStream_t st) {
   if (A.n <= 0) return cudaSuccess;
@@ -688,7 +651,6 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
     q.part = (double *)(base + 7 * vec);
     q.S = q.part + (size_t)kBicgBlocks * 3;
     q.ticket = (unsigned int *)(q.S + S_TICKET);
-    q.spart = (double *)(base + pair_spart_offset(n));
   }
   auto ax_of = [&](int a) { return (float *)((char *)scratch[a] + 6 * vec); };
   int eb = (int)((n + kThreads - 1) / kThreads);
@@ -757,11 +719,12 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
       k2_update_p<<<ge, kThreads, 0, st>>>(P);
       for (int sel = 0; sel < 2; sel++) {
         if (f == kSpmvSliced)
-          k2_spmv_sliced_dots<<<gs, kThreads, 0, st>>>(P, sel);
+          k2_spmv_sliced<<<gs, kThreads, 0, st>>>(P, sel);
         else if (f == kSpmvTiled)
-          k2_spmv_tiled_dots<<<ge, kThreads, 0, st>>>(P, sel);
+          k2_spmv_tiled<<<ge, kThreads, 0, st>>>(P, sel);
         else
-          k2_spmv_rows_dots<<<ge, kThreads, 0, st>>>(P, sel);
+          k2_spmv_rows<<<ge, kThreads, 0, st>>>(P, sel);
+        k2_dots<<<gr, kThreads, 0, st>>>(P, sel);
         if (sel == 0) k2_update_s<<<ge, kThreads, 0, st>>>(P);
       }
       k2_update_xr<<<gr, kThreads, 0, st>>>(P);

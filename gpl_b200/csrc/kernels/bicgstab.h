@@ -62,9 +62,8 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
 // y = A x in the given form (SpmvForm).
 cudaError_t spmv(const CsrDev &A, const float *x, float *y, int form, cudaStream_t s);
 // Two systems of the same size solved side by side (each launch carries both): each takes
-// the steps of bicgstab_solve on its own, each SpMV launch also forming the inner products
-// that follow it (the same sums in another fixed order); scratch[a] holds
-// bicgstab_pair_scratch_bytes(n) bytes for system a.
+// the steps of bicgstab_solve on its own; scratch[a] holds bicgstab_pair_scratch_bytes(n)
+// bytes for system a.
 size_t bicgstab_pair_scratch_bytes(int64_t n);
 // With `tune` (two candidates: the tiled and the sliced form), each batch of iterations runs
 // the form the tuner picks (A then needs its sliced copy), timed in place; `spmv` is then the

@@ -7,8 +7,8 @@
 // height, so a net adds c fx(x) fy(y), c = 100 hpwl wire_width / area, fx = ox / width,
 // fy = oy / height; fx is 1 on the columns strictly inside the box and partial only on its two
 // edge columns, fy likewise. So a net's deposit is at most 3 x 3 rectangles of tiles with one
-// value each (edge column or interior, by edge row or interior), each added to a 2D difference
-// array at its four corners, and one inclusive 2D prefix sum gives every tile's demand: work in
+// value each (edge column or interior, by edge row or interior), added to a 2D difference array
+// at the corners they share, and one inclusive 2D prefix sum gives every tile's demand: work in
 // nets plus tiles instead of in the boxes' tile counts (a net spanning a fifth of a 1024 x 1024
 // grid covers some 40,000 tiles). The differences and the sums are in double, so a tile's
 // demand is the reference's float sum to within its own rounding.
@@ -63,16 +63,27 @@ __global__ void k_rudy_rects(RudyGrid g, int64_t n_nets, const int4 *__restrict_
   Runs rx, ry;
   runs_of(xl, xh, g.lx, g.tile, g.cnt_x, g.ux - g.lx, min_x, max_x, rx);
   runs_of(yl, yh, g.ly, g.tile, g.cnt_y, g.uy - g.ly, min_y, max_y, ry);
+  // The runs are contiguous (run k spans [B_k, B_{k+1})), so the rectangles' corners fall on
+  // the (n + 1) x (m + 1) breakpoints, where the difference of the piecewise-constant deposit is
+  // c (f_i - f_{i-1}) (g_j - g_{j-1}) (f and g zero outside the runs): at most 16 adds a net
+  // instead of four for each of up to nine rectangles.
+  if (rx.n == 0 || ry.n == 0) return;
   const int64_t w = g.cnt_y + 1;
-  for (int i = 0; i < rx.n; i++)
-    for (int j = 0; j < ry.n; j++) {
-      const double v = c * rx.f[i] * ry.f[j];
-      const int64_t x0 = rx.a[i], x1 = rx.b[i] + 1, y0 = ry.a[j], y1 = ry.b[j] + 1;
-      atomicAdd(&diff[x0 * w + y0], v);
-      atomicAdd(&diff[x1 * w + y0], -v);
-      atomicAdd(&diff[x0 * w + y1], -v);
-      atomicAdd(&diff[x1 * w + y1], v);
-    }
+  int32_t px[4], py[4];
+  double dfx[4], dfy[4];
+  for (int i = 0; i <= rx.n; i++) {
+    px[i] = i < rx.n ? rx.a[i] : rx.b[rx.n - 1] + 1;
+    dfx[i] = (i < rx.n ? rx.f[i] : 0.0) - (i > 0 ? rx.f[i - 1] : 0.0);
+  }
+  for (int j = 0; j <= ry.n; j++) {
+    py[j] = j < ry.n ? ry.a[j] : ry.b[ry.n - 1] + 1;
+    dfy[j] = (j < ry.n ? ry.f[j] : 0.0) - (j > 0 ? ry.f[j - 1] : 0.0);
+  }
+  for (int i = 0; i <= rx.n; i++) {
+    if (dfx[i] == 0.0) continue;
+    for (int j = 0; j <= ry.n; j++)
+      if (dfy[j] != 0.0) atomicAdd(&diff[(int64_t)px[i] * w + py[j]], c * dfx[i] * dfy[j]);
+  }
 }
 
 // The prefix sum along y of every x row (a block per row, its threads over chunks of y).

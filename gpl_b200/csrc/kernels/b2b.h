@@ -127,9 +127,9 @@ class IpDevice {
     float *p_vals = nullptr, *p_rhs = nullptr, *p_x = nullptr;
     size_t p_cap = 0;
   } ax_[2];
-  // The solver's row order: perm_[i'] = the row solved as row i', inv_ its inverse; sorted
-  // again each round by the Hilbert index of the rows' centres (the start point), so a warp's
-  // rows gather their x entries from a compact patch (off: GPL_IP_ORDER=0).
+  // The solver's row order (GPL_IP_ORDER=1; off by default): perm_[i'] = the row solved as
+  // row i', inv_ its inverse; sorted again each round by the Hilbert index of the rows'
+  // centres (the start point), so a warp's rows gather their x entries from a compact patch.
   int32_t *perm_ = nullptr, *inv_ = nullptr, *ord_idx_ = nullptr, *ord_hist_ = nullptr;
   uint32_t *ord_key0_ = nullptr, *ord_key1_ = nullptr;
   int64_t solves_ = 0;

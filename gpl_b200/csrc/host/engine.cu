@@ -225,21 +225,39 @@ void Engine::upload(const EngineSetup &s) {
   if (any_locked_) check(upload_vec(&locked_, s.locked, st), "upload cells");
   check(upload_vec(&cell_pin_start_, s.cell_pin_start, st), "upload cells");
   {
-    // The nets in degree order (stable), their pins following them: a WA tile then holds
+    // The nets in degree order, their pins following them: a WA tile then holds
     // nets of one degree, so its thread-per-net phases do not diverge. No result depends on
     // the order: each pin's force goes to its place in its cell's pin list (pin_slot), the
     // HPWL is an integer sum, a net's weight moves with it.
+    // Within a degree, the nets in order of their lowest device cell (the cells are on a
+    // Hilbert curve), so a warp's nets and their first pins' cells lie close together.
     std::vector<int64_t> by_deg;
     int64_t max_deg = 0;
     for (int32_t n = 0; n < n_nets_; n++) max_deg = std::max(max_deg, s.net_start[n + 1] - s.net_start[n]);
+    std::vector<int32_t> low(n_nets_);
+    parallel_for((size_t)n_nets_, [&](size_t a, size_t b) {
+      for (size_t n = a; n < b; n++) {
+        int32_t m = (int32_t)n_cells_;
+        for (int64_t q = s.net_start[n]; q < s.net_start[n + 1]; q++)
+          if (s.pin_cell[q] >= 0) m = std::min(m, s.pin_cell[q]);
+        low[n] = m;
+      }
+    });
+    std::vector<int32_t> by_cell(n_nets_);
+    {
+      std::vector<int64_t> cnt((size_t)n_cells_ + 2, 0);
+      for (int32_t n = 0; n < n_nets_; n++) cnt[(size_t)low[n] + 1]++;
+      for (size_t k = 1; k < cnt.size(); k++) cnt[k] += cnt[k - 1];
+      for (int32_t n = 0; n < n_nets_; n++) by_cell[cnt[low[n]]++] = n;
+    }
     net_order_.resize(n_nets_);
     if (max_deg <= (int64_t)1 << 20) {
       by_deg.assign(max_deg + 2, 0);
       for (int32_t n = 0; n < n_nets_; n++) by_deg[s.net_start[n + 1] - s.net_start[n] + 1]++;
       for (int64_t d = 0; d <= max_deg; d++) by_deg[d + 1] += by_deg[d];
-      for (int32_t n = 0; n < n_nets_; n++) net_order_[by_deg[s.net_start[n + 1] - s.net_start[n]]++] = n;
+      for (int32_t n : by_cell) net_order_[by_deg[s.net_start[n + 1] - s.net_start[n]]++] = n;
     } else {
-      for (int32_t n = 0; n < n_nets_; n++) net_order_[n] = n;
+      net_order_ = by_cell;
       std::stable_sort(net_order_.begin(), net_order_.end(), [&](int32_t a, int32_t b) { return s.net_start[a + 1] - s.net_start[a] < s.net_start[b + 1] - s.net_start[b]; });
     }
     // each pin's force goes to its place in its cell's pin list (cell_pins lists each pin once)
@@ -453,8 +471,15 @@ std::vector<float> Engine::get_coords(int b, SlotId slot) {
   return xy;
 }
 
+void Engine::fork_after_place() {
+  if (!overlap_) return;
+  check(cudaEventRecord(ev_fork_, stream_), "wa fork");
+  fork_early_ = true;
+}
+
 void Engine::place_at(int b, SlotId slot) {
   flush();
+  fork_early_ = false;
   join();
   if (failed()) return;
   hpwl_ready_ = hpwl_fetched_ = false;  // the density centres move
@@ -516,6 +541,7 @@ void Engine::nesterov_step(int b, float step, float coeff) {
     RegionArgs a = r->args;
     a.scatter_form = r->scatter_tune->start(stream_);
     k_place_cells<<<blocks_for(r->n_cells), kThreadsPerBlock, 0, stream_>>>(a, c, PLACE_NESTEROV, step, coeff, nullptr);
+    fork_after_place();
     r->scatter_tune->stop(stream_);
   }
   ph_end(PH_PLACE);
@@ -566,9 +592,12 @@ void Engine::wa(float cx, float cy) {
   // forked after the work queued so far (the centres), joined by the forces' readers
   cudaStream_t st = overlap_ ? wa_stream_ : stream_;
   if (overlap_) {
-    check(cudaEventRecord(ev_fork_, stream_), "wa fork");
+    // the fork was recorded right after the last scatter (the new centres) when one ran since
+    // the last WA: the WA then runs beside the bins' finalize too
+    if (!fork_early_) check(cudaEventRecord(ev_fork_, stream_), "wa fork");
     check(cudaStreamWaitEvent(wa_stream_, ev_fork_, 0), "wa fork");
   }
+  fork_early_ = false;
   // the kernels add the HPWL of these same positions: hpwl() reads it without a launch
   check(cudaMemsetAsync(hpwl_acc_, 0, sizeof(unsigned long long), st), "wa");
   w.hpwl_out = hpwl_acc_;
@@ -778,6 +807,7 @@ void Engine::flush_place(const std::vector<QueueEntry> &q, size_t a, size_t b) {
   copy_tables(*this, h, d, ns + n, stream_, h2d_bytes);
   if (ns) {
     k_place_packed<<<blocks, kThreadsPerBlock, 0, stream_>>>(d, ns);
+    fork_after_place();
     pk_scatter_tune_->stop(stream_);
     launches += 1;
   }

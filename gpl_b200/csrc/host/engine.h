@@ -215,6 +215,8 @@ class Engine {
   void flush_grad(const std::vector<QueueEntry> &q, size_t a, size_t b);
   bool stage_tables(size_t n);
   bool wa_pending_ = false;
+  bool fork_early_ = false;  // ev_fork_ holds the point right after the trial's last scatter
+  void fork_after_place();
   bool overlap_ = true;
   void join();
   void free_globals();

@@ -912,10 +912,18 @@ cudaError_t IpDevice::assemble(IpAxisResult out[2]) {
   if (n_nets_) k_emit<<<grid(n_nets_), kThreads, 0, s_>>>(a, ox, oy);
   launches += 2;
   CK(cudaGetLastError());
+  if (first) {
+    CK(cudaStreamSynchronize(s_));
+    progress("    round 1: triplets emitted");
+  }
   for (int ax = 0; ax < 2; ax++) {
     Axis &A = ax_[ax];
     int64_t o = ax ? nt[0] : 0;
     CK(collapse(nt[ax], t_row_ + o, t_col_ + o, t_val_ + o, A.starts, &A.cols, &A.vals, &A.cap, &A.nnz));
+    if (first) {
+      CK(cudaStreamSynchronize(s_));
+      progress("    round 1: axis %d collapsed", ax);
+    }
     out[ax].triplets = nt[ax];
     // the right-hand side: this axis's terms as one-column triplets, summed per row in order
     int64_t r = ax ? nr[0] : 0;

@@ -29,6 +29,7 @@
 #include "parallel.h"
 
 namespace gpl {
+void progress(const char *fmt, ...) __attribute__((format(printf, 1, 2)));
 
 // ---------------------------------------------------------------- FP32 SIMT GEMM
 // 128 x 64 output tile per block, K-step 8, 256 threads with 8 x 4 outputs each.
@@ -211,9 +212,9 @@ void build_basis(int nx, int ny, BasisHost &b) {
 static cudaError_t upload_f32(const std::vector<double> &h, float **d) {
   std::vector<float> f(h.size());
   for (size_t i = 0; i < h.size(); i++) f[i] = (float)h[i];
-  cudaError_t e = cudaMalloc(d, f.size() * sizeof(float));
+  cudaError_t e = pool_alloc((void **)d, f.size() * sizeof(float));
   if (e != cudaSuccess) return e;
-  return cudaMemcpy(*d, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice);
+  return pool_upload(*d, f.data(), f.size() * sizeof(float));
 }
 
 size_t poisson_workspace_bytes(int nx, int ny) {
@@ -234,6 +235,7 @@ PoissonPlan *poisson_plan_create(int nx, int ny, const float *wx_host, const flo
   std::vector<float> w2((size_t)nx + ny);
   BasisHost b;
   build_basis(nx, ny, b);
+  if (nx >= 512) progress("    plan: bases built");
   size_t n = (size_t)nx * ny;
 #define TRY(x)              \
   do {                      \
@@ -244,24 +246,24 @@ PoissonPlan *poisson_plan_create(int nx, int ny, const float *wx_host, const flo
       return nullptr;       \
     }                       \
   } while (0)
-  TRY(cudaMalloc(&p->wx, nx * sizeof(float)));
-  TRY(cudaMalloc(&p->wx2, nx * sizeof(float)));
-  TRY(cudaMalloc(&p->wy, ny * sizeof(float)));
-  TRY(cudaMalloc(&p->wy2, ny * sizeof(float)));
+  TRY(pool_alloc((void **)&p->wx, nx * sizeof(float)));
+  TRY(pool_alloc((void **)&p->wx2, nx * sizeof(float)));
+  TRY(pool_alloc((void **)&p->wy, ny * sizeof(float)));
+  TRY(pool_alloc((void **)&p->wy2, ny * sizeof(float)));
   std::vector<float> sq(std::max(nx, ny));
   for (int i = 0; i < nx; i++) sq[i] = wx_host[i] * wx_host[i];
-  TRY(cudaMemcpy(p->wx, wx_host, nx * sizeof(float), cudaMemcpyHostToDevice));
-  TRY(cudaMemcpy(p->wx2, sq.data(), nx * sizeof(float), cudaMemcpyHostToDevice));
+  TRY(pool_upload(p->wx, wx_host, nx * sizeof(float)));
+  TRY(pool_upload(p->wx2, sq.data(), nx * sizeof(float)));
   for (int i = 0; i < ny; i++) sq[i] = wy_host[i] * wy_host[i];
-  TRY(cudaMemcpy(p->wy, wy_host, ny * sizeof(float), cudaMemcpyHostToDevice));
-  TRY(cudaMemcpy(p->wy2, sq.data(), ny * sizeof(float), cudaMemcpyHostToDevice));
+  TRY(pool_upload(p->wy, wy_host, ny * sizeof(float)));
+  TRY(pool_upload(p->wy2, sq.data(), ny * sizeof(float)));
   if (mode == 2) {
     const std::vector<double> *mats[6] = {&b.CyTs, &b.CxTs, &b.Cy, &b.Sy, &b.Sx, &b.Cx};
     for (int k = 0; k < 6; k++) {
-      TRY(cudaMalloc(&p->d_basis[k], mats[k]->size() * sizeof(double)));
-      TRY(cudaMemcpy(p->d_basis[k], mats[k]->data(), mats[k]->size() * sizeof(double), cudaMemcpyHostToDevice));
+      TRY(pool_alloc((void **)&p->d_basis[k], mats[k]->size() * sizeof(double)));
+      TRY(pool_upload(p->d_basis[k], mats[k]->data(), mats[k]->size() * sizeof(double)));
     }
-    for (int k = 0; k < 8; k++) TRY(cudaMalloc(&p->d_buf[k], n * sizeof(double)));
+    for (int k = 0; k < 8; k++) TRY(pool_alloc((void **)&p->d_buf[k], n * sizeof(double)));
   } else if (mode == 0) {
     TRY(upload_f32(b.CyTs, &p->CyTs));
     TRY(upload_f32(b.CxTs, &p->CxTs));
@@ -269,13 +271,14 @@ PoissonPlan *poisson_plan_create(int nx, int ny, const float *wx_host, const flo
     TRY(upload_f32(b.Sy, &p->Sy));
     TRY(upload_f32(b.Sx, &p->Sx));
     TRY(upload_f32(b.Cx, &p->Cx));
-    TRY(cudaMalloc(&p->t1, n * sizeof(float)));
-    TRY(cudaMalloc(&p->ah, n * sizeof(float)));
-    TRY(cudaMalloc(&p->exh, n * sizeof(float)));
-    TRY(cudaMalloc(&p->eyh, n * sizeof(float)));
-    TRY(cudaMalloc(&p->t2, n * sizeof(float)));
-    TRY(cudaMalloc(&p->t3, n * sizeof(float)));
+    TRY(pool_alloc((void **)&p->t1, n * sizeof(float)));
+    TRY(pool_alloc((void **)&p->ah, n * sizeof(float)));
+    TRY(pool_alloc((void **)&p->exh, n * sizeof(float)));
+    TRY(pool_alloc((void **)&p->eyh, n * sizeof(float)));
+    TRY(pool_alloc((void **)&p->t2, n * sizeof(float)));
+    TRY(pool_alloc((void **)&p->t3, n * sizeof(float)));
   } else {
+    if (nx >= 512) progress("    plan: wavenumbers uploaded");
     cudaError_t e = tc_plan_init(p, b);
     if (e != cudaSuccess) {
       *err = e;
@@ -284,18 +287,23 @@ PoissonPlan *poisson_plan_create(int nx, int ny, const float *wx_host, const flo
     }
   }
 #undef TRY
+  if ((*err = cudaStreamSynchronize(0)) != cudaSuccess) {
+    poisson_plan_destroy(p);
+    return nullptr;
+  }
   return p;
 }
 
 void poisson_plan_destroy(PoissonPlan *p) {
   if (!p) return;
+  cudaDeviceSynchronize();
   float *bufs[] = {p->wx, p->wx2, p->wy, p->wy2, p->CyTs, p->CxTs, p->Cy, p->Sy, p->Sx, p->Cx, p->t1, p->ah, p->exh, p->eyh, p->t2, p->t3};
   for (float *b : bufs)
-    if (b) cudaFree(b);
+    pool_free(b);
   for (double *b : p->d_basis)
-    if (b) cudaFree(b);
+    pool_free(b);
   for (double *b : p->d_buf)
-    if (b) cudaFree(b);
+    pool_free(b);
   tc_plan_free(p);
   delete p;
 }
@@ -430,8 +438,8 @@ PoissonGroup *poisson_group_create(PoissonPlan *const *plans, const float *const
   auto put = [&](auto **d, const auto &v) {
     if (*err != cudaSuccess || v.empty()) return;
     using E = typename std::remove_reference<decltype(v)>::type::value_type;
-    *err = cudaMalloc((void **)d, v.size() * sizeof(E));
-    if (*err == cudaSuccess) *err = cudaMemcpy(*d, v.data(), v.size() * sizeof(E), cudaMemcpyHostToDevice);
+    *err = pool_alloc((void **)d, v.size() * sizeof(E));
+    if (*err == cudaSuccess) *err = pool_upload(*d, v.data(), v.size() * sizeof(E));
   };
   for (int q = 0; q < 4; q++) {
     std::vector<int> first;
@@ -448,6 +456,7 @@ PoissonGroup *poisson_group_create(PoissonPlan *const *plans, const float *const
   g->n_jobs = (int)jobs.size();
   g->job_blocks = jb;
   put(&g->jobs, jobs);
+  if (*err == cudaSuccess) *err = cudaStreamSynchronize(0);
   if (*err != cudaSuccess) {
     poisson_group_destroy(g);
     return nullptr;
@@ -457,11 +466,12 @@ PoissonGroup *poisson_group_create(PoissonPlan *const *plans, const float *const
 
 void poisson_group_destroy(PoissonGroup *g) {
   if (!g) return;
+  cudaDeviceSynchronize();
   for (int q = 0; q < 4; q++) {
-    if (g->probs[q]) cudaFree(g->probs[q]);
-    if (g->first[q]) cudaFree(g->first[q]);
+    pool_free(g->probs[q]);
+    pool_free(g->first[q]);
   }
-  if (g->jobs) cudaFree(g->jobs);
+  pool_free(g->jobs);
   delete g;
 }
 

@@ -35,6 +35,16 @@ struct BasisHost {
 };
 void build_basis(int nx, int ny, BasisHost &b);
 
+// The plans' device memory comes from the device's stream-ordered pool (kept warm, so a plan
+// made after another, or after the initial placement, maps no new memory), ordered on the
+// legacy stream: a plan or group is complete once its create has synchronised that stream,
+// and its destroy synchronises the device before it returns the memory, as cudaFree would.
+inline cudaError_t pool_alloc(void **p, size_t bytes) { return cudaMallocAsync(p, bytes, 0); }
+inline cudaError_t pool_upload(void *d, const void *h, size_t bytes) { return cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, 0); }
+inline void pool_free(void *p) {
+  if (p) cudaFreeAsync(p, 0);
+}
+
 struct TcState;  // the split-BF16 tensor-core path's buffers (poisson_tc.cu)
 
 struct PoissonPlan {

@@ -330,9 +330,9 @@ static cudaError_t upload_split(const std::vector<double> &h, int rows, int k, _
         v[r * 2 * k + k + c] = __float2bfloat16_rn(x - __bfloat162float(hi));
       }
   }, 16);
-  cudaError_t e = cudaMalloc(d, v.size() * sizeof(__nv_bfloat16));
+  cudaError_t e = pool_alloc((void **)d, v.size() * sizeof(__nv_bfloat16));
   if (e != cudaSuccess) return e;
-  return cudaMemcpy(*d, v.data(), v.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice);
+  return pool_upload(*d, v.data(), v.size() * sizeof(__nv_bfloat16));
 }
 
 cudaError_t tc_plan_init(PoissonPlan *p, const BasisHost &b) {
@@ -352,15 +352,15 @@ cudaError_t tc_plan_init(PoissonPlan *p, const BasisHost &b) {
   TRY(upload_split(b.Sx, nx, nx, &t->Sx));
   TRY(upload_split(b.Cx, nx, nx, &t->Cx));
   size_t n = (size_t)nx * ny * 2;
-  TRY(cudaMalloc(&p->tc_dens, n * sizeof(__nv_bfloat16)));
-  TRY(cudaMalloc(&t->t1, n * sizeof(__nv_bfloat16)));
-  TRY(cudaMalloc(&t->exh, n * sizeof(__nv_bfloat16)));
-  TRY(cudaMalloc(&t->eyh, n * sizeof(__nv_bfloat16)));
-  TRY(cudaMalloc(&t->t2, n * sizeof(__nv_bfloat16)));
-  TRY(cudaMalloc(&t->t3, n * sizeof(__nv_bfloat16)));
-  TRY(cudaMemset(p->tc_dens, 0, n * sizeof(__nv_bfloat16)));
-  TRY(cudaMalloc(&t->err, sizeof(int)));
-  TRY(cudaMemset(t->err, 0, sizeof(int)));
+  TRY(pool_alloc((void **)&p->tc_dens, n * sizeof(__nv_bfloat16)));
+  TRY(pool_alloc((void **)&t->t1, n * sizeof(__nv_bfloat16)));
+  TRY(pool_alloc((void **)&t->exh, n * sizeof(__nv_bfloat16)));
+  TRY(pool_alloc((void **)&t->eyh, n * sizeof(__nv_bfloat16)));
+  TRY(pool_alloc((void **)&t->t2, n * sizeof(__nv_bfloat16)));
+  TRY(pool_alloc((void **)&t->t3, n * sizeof(__nv_bfloat16)));
+  TRY(cudaMemsetAsync(p->tc_dens, 0, n * sizeof(__nv_bfloat16), 0));
+  TRY(pool_alloc((void **)&t->err, sizeof(int)));
+  TRY(cudaMemsetAsync(t->err, 0, sizeof(int), 0));
   // A operands [M][2K]: 128-row boxes
   TRY(make_map(&t->mCyTs, t->CyTs, ny, ny, BM));
   TRY(make_map(&t->mCxTs, t->CxTs, nx, nx, BM));
@@ -388,13 +388,13 @@ cudaError_t tc_plan_init(PoissonPlan *p, const BasisHost &b) {
 }
 
 void tc_plan_free(PoissonPlan *p) {
-  if (p->tc_dens) cudaFree(p->tc_dens);
+  pool_free(p->tc_dens);
   p->tc_dens = nullptr;
   TcState *t = p->tc;
   if (!t) return;
   void *bufs[] = {t->CyTs, t->CxTs, t->Cy, t->Sy, t->Sx, t->Cx, t->t1, t->exh, t->eyh, t->t2, t->t3, t->err};
   for (void *b : bufs)
-    if (b) cudaFree(b);
+    pool_free(b);
   delete t;
   p->tc = nullptr;
 }

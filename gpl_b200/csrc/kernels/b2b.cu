@@ -240,10 +240,10 @@ __global__ void k_bucket(int64_t nt, const int32_t *row, const int32_t *col, con
 // Per row: keys sorted (column, then position; the keys are distinct), each column's run
 // summed in position order (the first value, then the rest added to it), the distinct columns
 // compacted. Tiers by the row's length: a warp per row with its keys in registers (R per
-// lane, bitonic-sorted across the warp) for rows of up to 64 and then 256 keys; a block per
-// row (bitonic sort in shared memory) up to 8192; a thread per row (Shell's sort in place)
+// lane, bitonic-sorted across the warp) for rows of up to 32, then 64, then 256 keys; a block
+// per row (bitonic sort in shared memory) up to 8192; a block per row merging sorted chunks
 // beyond. Every tier gives the same result.
-constexpr int kRowShort = 64, kRowMid = 256;
+constexpr int kRowTiny = 32, kRowShort = 64, kRowMid = 256;
 
 // One column's run [p, end) of a sorted row summed in position order: the first value, then
 // the rest added to it; the values' loads go four at a time ahead of the adds.
@@ -762,8 +762,8 @@ cudaError_t IpDevice::upload(const IpSetup &s) {
   CK(alloc(&ucount_, n_ + 1, s_));
   CK(cudaFuncSetAttribute(k_row_collapse_block, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
   CK(cudaFuncSetAttribute(k_row_collapse_long, cudaFuncAttributeMaxDynamicSharedMemorySize, kRowLong * (int)sizeof(unsigned long long)));
-  CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1), s_));
-  CK(alloc(&tier_n_, 3, s_));
+  CK(alloc(&tier_rows_, 4 * std::max<int64_t>(n_, 1), s_));
+  CK(alloc(&tier_n_, 4, s_));
   CK(alloc(&fill_, n_, s_));
   CK(alloc(&hpwl_acc_, 1, s_));
   for (auto &a : ax_) {
@@ -812,15 +812,16 @@ cudaError_t IpDevice::collapse(int64_t n_trip, const int32_t *row, const int32_t
   CK(scan(row_off_, n_));
   if (n_trip) k_bucket<<<grid(n_trip), kThreads, 0, s_>>>(n_trip, row, col, row_off_, fill_, bucket_);
   if (n_) {
-    // tiers: a warp per row up to 64 keys, then up to 256, a block per row up to 8192, then
-    // a thread per row
-    CK(cudaMemsetAsync(tier_n_, 0, 3 * sizeof(int), s_));
+    // tiers: a warp per row up to 32 keys, then up to 64, then up to 256, a block per row up
+    // to 8192, then a block per row merging sorted chunks
+    CK(cudaMemsetAsync(tier_n_, 0, 4 * sizeof(int), s_));
     const int wblocks = (int)std::min<int64_t>((n_ + kThreads / 32 - 1) / (kThreads / 32), 148 * 64);
-    k_row_collapse_warp<kRowShort / 32><<<wblocks, kThreads, 0, s_>>>(n_, nullptr, nullptr, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_, tier_n_);
-    k_row_collapse_warp<kRowMid / 32><<<148 * 4, kThreads, 0, s_>>>(n_, tier_rows_, tier_n_, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_ + n_, tier_n_ + 1);
-    k_row_collapse_block<<<148 * 2, kThreads, kRowLong * sizeof(unsigned long long), s_>>>(tier_rows_ + n_, tier_n_ + 1, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_ + 2 * n_, tier_n_ + 2);
-    k_row_collapse_long<<<148 * 2, kThreads, kRowLong * sizeof(unsigned long long), s_>>>(tier_rows_ + 2 * n_, tier_n_ + 2, row_off_, bucket_, bucket2_, val, ucol_, uval_, ucount_);
-    launches += 4;
+    k_row_collapse_warp<kRowTiny / 32><<<wblocks, kThreads, 0, s_>>>(n_, nullptr, nullptr, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_, tier_n_);
+    k_row_collapse_warp<kRowShort / 32><<<148 * 16, kThreads, 0, s_>>>(n_, tier_rows_, tier_n_, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_ + n_, tier_n_ + 1);
+    k_row_collapse_warp<kRowMid / 32><<<148 * 4, kThreads, 0, s_>>>(n_, tier_rows_ + n_, tier_n_ + 1, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_ + 2 * n_, tier_n_ + 2);
+    k_row_collapse_block<<<148 * 2, kThreads, kRowLong * sizeof(unsigned long long), s_>>>(tier_rows_ + 2 * n_, tier_n_ + 2, row_off_, bucket_, val, ucol_, uval_, ucount_, tier_rows_ + 3 * n_, tier_n_ + 3);
+    k_row_collapse_long<<<148 * 2, kThreads, kRowLong * sizeof(unsigned long long), s_>>>(tier_rows_ + 3 * n_, tier_n_ + 3, row_off_, bucket_, bucket2_, val, ucol_, uval_, ucount_);
+    launches += 5;
   }
   launches += 2;
   if (!cols) return cudaGetLastError();
@@ -852,8 +853,8 @@ cudaError_t IpDevice::csr_from_triplets(int64_t n, int64_t nt, const int32_t *ro
   CK(alloc(&row_off_, n_ + 1, s_));
   CK(alloc(&ucount_, n_ + 1, s_));
   CK(alloc(&fill_, n_, s_));
-  CK(alloc(&tier_rows_, 3 * std::max<int64_t>(n_, 1), s_));
-  CK(alloc(&tier_n_, 3, s_));
+  CK(alloc(&tier_rows_, 4 * std::max<int64_t>(n_, 1), s_));
+  CK(alloc(&tier_n_, 4, s_));
   CK(grow(s_, (size_t)std::max<int64_t>(nt, 1), w_cap_, &bucket_, &bucket2_, &ucol_, &uval_));
   size_t cap = (size_t)std::max<int64_t>(nt, 1);  // nnz <= nt: the caller's buffers suffice
   int32_t *c = cols;

@@ -166,6 +166,7 @@ __device__ __forceinline__ void spmv_sliced_rows(int64_t n, int64_t n_long, cons
   const int64_t j = n_long + i;
   if (j >= n) return;
   const int32_t len = sl_len[j];
+  const int32_t row = sl_row[j];
   const int64_t base = sl_start[i / kSliceRows] + (i % kSliceRows);
   const int2 *ent = sl_ent + base;
   // kSpmvUnroll entries at a time, the last group's loads predicated, so every group costs
@@ -183,7 +184,7 @@ __device__ __forceinline__ void spmv_sliced_rows(int64_t n, int64_t n_long, cons
     for (int u = 0; u < kSpmvUnroll; u++)
       if (k + u < len) tmp = __fadd_rn(tmp, __fmul_rn(__int_as_float(cv[u].y), xv[u]));
   }
-  emit(sl_row[j], __fadd_rn(0.0f, __fmul_rn(1.0f, tmp)));
+  emit(row, __fadd_rn(0.0f, __fmul_rn(1.0f, tmp)));
 }
 __device__ __forceinline__ void spmv_sliced_body(int64_t n, int64_t n_long, const int64_t *__restrict__ rs, const int32_t *__restrict__ cols, const float *__restrict__ vals, const int32_t *__restrict__ sl_row, const int32_t *__restrict__ sl_len, const int64_t *__restrict__ sl_start, const int2 *__restrict__ sl_ent, const float *__restrict__ x, float *__restrict__ y, const double *__restrict__ S, int gate) {
   if (gated_off(S, gate)) return;
@@ -349,6 +350,73 @@ __device__ __forceinline__ void dots_body(int64_t n, const float *__restrict__ a
   }
   if (which >= 0 && last_block(ticket)) scalar_step(part, gridDim.x, S, which, 0, sh);
 }
+
+// The loop's two inner-product steps, each thread reading 16-byte runs of four, kVecUnroll
+// runs in flight (its terms summed in index order), when the vectors start on a 16-byte
+// boundary, else one element at a time: TWO 0 is r0.v (then alpha), TWO 1 is t.t and t.s
+// (then omega), t read once for both.
+constexpr int kVecUnroll = 2;
+__device__ __forceinline__ bool all_aligned16(const void *a, const void *b, const void *c, const void *d, const void *e, const void *f) {
+  return (((uintptr_t)a | (uintptr_t)b | (uintptr_t)c | (uintptr_t)d | (uintptr_t)e | (uintptr_t)f) & 15) == 0;
+}
+__device__ __forceinline__ double dot4(float4 a, float4 b, double s) {
+  s += (double)a.x * (double)b.x;
+  s += (double)a.y * (double)b.y;
+  s += (double)a.z * (double)b.z;
+  s += (double)a.w * (double)b.w;
+  return s;
+}
+template <int TWO>
+__device__ __forceinline__ void loop_dots_body(int64_t n, const float *__restrict__ a, const float *__restrict__ b, double *__restrict__ part, double *__restrict__ S, unsigned int *ticket) {
+  if (gated_off(S, kLive)) return;
+  __shared__ double sh[kThreads / 32];
+  double s0 = 0, s1 = 0;
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t done = 0;
+  if (all_aligned16(a, b, a, b, a, b)) {
+    const int64_t n4 = n / 4;
+    const float4 *A = (const float4 *)a, *B = (const float4 *)b;
+    for (int64_t i = tid; i < n4; i += kVecUnroll * stride) {
+      float4 x[kVecUnroll], y[kVecUnroll];
+#pragma unroll
+      for (int u = 0; u < kVecUnroll; u++) {
+        const int64_t k = i + u * stride;
+        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+        x[u] = k < n4 ? A[k] : z;
+        y[u] = k < n4 ? B[k] : z;
+      }
+#pragma unroll
+      for (int u = 0; u < kVecUnroll; u++) {
+        if (i + u * stride >= n4) break;
+        if (TWO) {
+          s0 = dot4(x[u], x[u], s0);
+          s1 = dot4(x[u], y[u], s1);
+        } else {
+          s0 = dot4(x[u], y[u], s0);
+        }
+      }
+    }
+    done = 4 * n4;
+  }
+  for (int64_t i = done + tid; i < n; i += stride) {
+    if (TWO) {
+      s0 += (double)a[i] * (double)a[i];
+      s1 += (double)a[i] * (double)b[i];
+    } else {
+      s0 += (double)a[i] * (double)b[i];
+    }
+  }
+  double t0 = block_sum<kThreads>(s0, sh);
+  double t1 = TWO ? block_sum<kThreads>(s1, sh) : 0.0;
+  if (threadIdx.x == 0) {
+    part[3 * blockIdx.x] = t0;
+    part[3 * blockIdx.x + 1] = t1;
+    part[3 * blockIdx.x + 2] = 0.0;
+  }
+  if (last_block(ticket)) scalar_step(part, gridDim.x, S, TWO ? 2 : 1, 0, sh);
+}
+__global__ void __launch_bounds__(kThreads, 4) k_loop_dots_alpha(int64_t n, const float *__restrict__ r0, const float *__restrict__ v, double *__restrict__ part, double *__restrict__ S, unsigned int *ticket) { loop_dots_body<0>(n, r0, v, part, S, ticket); }
+__global__ void __launch_bounds__(kThreads, 4) k_loop_dots_omega(int64_t n, const float *__restrict__ t, const float *__restrict__ s, double *__restrict__ part, double *__restrict__ S, unsigned int *ticket) { loop_dots_body<1>(n, t, s, part, S, ticket); }
 __global__ void k_dots(int64_t n, const float *__restrict__ a0, const float *__restrict__ b0, const float *__restrict__ a1, const float *__restrict__ b1, const float *__restrict__ a2, const float *__restrict__ b2, double *__restrict__ part, double *__restrict__ S, int gate, int which, unsigned int *ticket) { dots_body(n, a0, b0, a1, b1, a2, b2, part, S, gate, which, ticket); }
 
 __global__ void k_scalar(const double *__restrict__ part, int nblk, double *__restrict__ S, int which, int dst0, int gate) {
@@ -380,36 +448,84 @@ __global__ void k_residual(int64_t n, const float *__restrict__ b, const float *
   r0[i] = v;
 }
 
+// The elementwise updates: a thread per run of four elements (one 16-byte load per vector
+// when they all start on a 16-byte boundary); vec_blocks(n) blocks.
+__host__ __device__ __forceinline__ int64_t vec_blocks(int64_t n) { return std::max<int64_t>((n + 4 * kThreads - 1) / (4 * kThreads), 1); }
 // p = r + beta (p - w v), beta = (rho / rho_old) (alpha / w)
 __device__ __forceinline__ void update_p_body(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ p) {
   if (gated_off(S, kLive)) return;
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t i = 4 * (blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
   if (i >= n) return;
-  float beta = (float)((S[S_RHO] / S[S_RHO_OLD]) * (S[S_ALPHA] / S[S_W]));
-  float w = (float)S[S_W];
-  p[i] = __fadd_rn(r[i], __fmul_rn(beta, __fsub_rn(p[i], __fmul_rn(w, v[i]))));
+  const float beta = (float)((S[S_RHO] / S[S_RHO_OLD]) * (S[S_ALPHA] / S[S_W]));
+  const float w = (float)S[S_W];
+  auto f = [&](float ri, float pi, float vi) { return __fadd_rn(ri, __fmul_rn(beta, __fsub_rn(pi, __fmul_rn(w, vi)))); };
+  if (i + 4 <= n && all_aligned16(r, v, p, r, v, p)) {
+    const float4 R = *(const float4 *)(r + i), V = *(const float4 *)(v + i), Pv = *(const float4 *)(p + i);
+    *(float4 *)(p + i) = make_float4(f(R.x, Pv.x, V.x), f(R.y, Pv.y, V.y), f(R.z, Pv.z, V.z), f(R.w, Pv.w, V.w));
+  } else {
+    for (int64_t k = i; k < min(n, i + 4); k++) p[k] = f(r[k], p[k], v[k]);
+  }
 }
 __global__ void k_update_p(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ p) { update_p_body(n, S, r, v, p); }
 
 __device__ __forceinline__ void update_s_body(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ s) {
   if (gated_off(S, kLive)) return;
-  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t i = 4 * (blockIdx.x * (int64_t)blockDim.x + threadIdx.x);
   if (i >= n) return;
-  float a = (float)S[S_ALPHA];
-  s[i] = __fsub_rn(r[i], __fmul_rn(a, v[i]));
+  const float a = (float)S[S_ALPHA];
+  auto f = [&](float ri, float vi) { return __fsub_rn(ri, __fmul_rn(a, vi)); };
+  if (i + 4 <= n && all_aligned16(r, v, s, r, v, s)) {
+    const float4 R = *(const float4 *)(r + i), V = *(const float4 *)(v + i);
+    *(float4 *)(s + i) = make_float4(f(R.x, V.x), f(R.y, V.y), f(R.z, V.z), f(R.w, V.w));
+  } else {
+    for (int64_t k = i; k < min(n, i + 4); k++) s[k] = f(r[k], v[k]);
+  }
 }
 __global__ void k_update_s(int64_t n, const double *__restrict__ S, const float *__restrict__ r, const float *__restrict__ v, float *__restrict__ s) { update_s_body(n, S, r, v, s); }
 
 // x += alpha p + w s; r = s - w t; partials of |r|^2 and r0.r, the last block taking the
-// iteration's end (scalar step 3)
+// iteration's end (scalar step 3). Runs of four as in the loop's dot products.
 __device__ __forceinline__ void update_xr_body(int64_t n, double *__restrict__ S, const float *__restrict__ p, const float *__restrict__ s, const float *__restrict__ t, const float *__restrict__ r0, float *__restrict__ x, float *__restrict__ r, double *__restrict__ part, unsigned int *ticket) {
   if (gated_off(S, kLive)) return;
   __shared__ double sh[kThreads / 32];
-  float a = (float)S[S_ALPHA], w = (float)S[S_W];
+  const float a = (float)S[S_ALPHA], w = (float)S[S_W];
   double rr = 0, r0r = 0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    x[i] = __fadd_rn(x[i], __fadd_rn(__fmul_rn(a, p[i]), __fmul_rn(w, s[i])));
-    float rv = __fsub_rn(s[i], __fmul_rn(w, t[i]));
+  const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+  auto fx = [&](float xi, float pi, float si) { return __fadd_rn(xi, __fadd_rn(__fmul_rn(a, pi), __fmul_rn(w, si))); };
+  auto fr = [&](float si, float ti) { return __fsub_rn(si, __fmul_rn(w, ti)); };
+  int64_t done = 0;
+  if (all_aligned16(p, s, t, r0, x, r)) {
+    const int64_t n4 = n / 4;
+    constexpr int U = 1;
+    for (int64_t i = tid; i < n4; i += U * stride) {
+      float4 X[U], Pp[U], Sv[U], T[U], R0[U];
+      const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t k = i + u * stride;
+        const bool in = k < n4;
+        X[u] = in ? ((const float4 *)x)[k] : z;
+        Pp[u] = in ? ((const float4 *)p)[k] : z;
+        Sv[u] = in ? ((const float4 *)s)[k] : z;
+        T[u] = in ? ((const float4 *)t)[k] : z;
+        R0[u] = in ? ((const float4 *)r0)[k] : z;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++) {
+        const int64_t k = i + u * stride;
+        if (k >= n4) break;
+        ((float4 *)x)[k] = make_float4(fx(X[u].x, Pp[u].x, Sv[u].x), fx(X[u].y, Pp[u].y, Sv[u].y), fx(X[u].z, Pp[u].z, Sv[u].z), fx(X[u].w, Pp[u].w, Sv[u].w));
+        const float4 R = make_float4(fr(Sv[u].x, T[u].x), fr(Sv[u].y, T[u].y), fr(Sv[u].z, T[u].z), fr(Sv[u].w, T[u].w));
+        ((float4 *)r)[k] = R;
+        rr = dot4(R, R, rr);
+        r0r = dot4(R0[u], R, r0r);
+      }
+    }
+    done = 4 * n4;
+  }
+  for (int64_t i = done + tid; i < n; i += stride) {
+    x[i] = fx(x[i], p[i], s[i]);
+    float rv = fr(s[i], t[i]);
     r[i] = rv;
     rr += (double)rv * (double)rv;
     r0r += (double)r0[i] * (double)rv;
@@ -423,7 +539,7 @@ __device__ __forceinline__ void update_xr_body(int64_t n, double *__restrict__ S
   }
   if (last_block(ticket)) scalar_step(part, gridDim.x, S, 3, 0, sh);  // the iteration's end
 }
-__global__ void k_update_xr(int64_t n, double *__restrict__ S, const float *__restrict__ p, const float *__restrict__ s, const float *__restrict__ t, const float *__restrict__ r0, float *__restrict__ x, float *__restrict__ r, double *__restrict__ part, unsigned int *ticket) { update_xr_body(n, S, p, s, t, r0, x, r, part, ticket); }
+__global__ void __launch_bounds__(kThreads, 4) k_update_xr(int64_t n, double *__restrict__ S, const float *__restrict__ p, const float *__restrict__ s, const float *__restrict__ t, const float *__restrict__ r0, float *__restrict__ x, float *__restrict__ r, double *__restrict__ part, unsigned int *ticket) { update_xr_body(n, S, p, s, t, r0, x, r, part, ticket); }
 
 // Both axes' systems in one launch (blockIdx.y picks the system): the initial placement solves
 // its x and y systems side by side, so each launch carries twice the work and the loop half
@@ -469,19 +585,19 @@ __global__ void __launch_bounds__(kThreads) k2_spmv_sliced(SysPair P, int sel) {
 // step. (Forming them in the SpMV's own launch was measured 11 % slower over the whole
 // initial placement: the sliced form's rows are in length order, so their r0 and s reads
 // scatter, and the fused tail's block reductions stall every block.)
-__global__ void k2_dots(SysPair P, int sel) {
+__global__ void __launch_bounds__(kThreads, 4) k2_dots(SysPair P, int sel) {
   SysDev q = pick(P);
   if (sel == 0)
-    dots_body(q.n, q.r0, q.v, nullptr, nullptr, nullptr, nullptr, q.part, q.S, kLive, 1, q.ticket);
+    loop_dots_body<0>(q.n, q.r0, q.v, q.part, q.S, q.ticket);
   else
-    dots_body(q.n, q.t, q.t, q.t, q.s, nullptr, nullptr, q.part, q.S, kLive, 2, q.ticket);
+    loop_dots_body<1>(q.n, q.t, q.s, q.part, q.S, q.ticket);
 }
 
 __global__ void __launch_bounds__(kThreads) k2_update_s(SysPair P) {
   SysDev q = pick(P);
   update_s_body(q.n, q.S, q.r, q.v, q.s);
 }
-__global__ void k2_update_xr(SysPair P) {
+__global__ void __launch_bounds__(kThreads, 4) k2_update_xr(SysPair P) {
   SysDev q = pick(P);
   update_xr_body(q.n, q.S, q.p, q.s, q.t, q.r0, q.x, q.r, q.part, q.ticket);
 }
@@ -594,12 +710,12 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
   int restarts = 0;
   for (;;) {
     for (int k = 0; k < kBicgBatch; k++) {
-      k_update_p<<<eb, kThreads, 0, st>>>(n, S, r, v, p);
+      k_update_p<<<(unsigned)vec_blocks(n), kThreads, 0, st>>>(n, S, r, v, p);
       spmv(p, v, kLive);
-      k_dots<<<rb, kThreads, 0, st>>>(n, r0, v, nullptr, nullptr, nullptr, nullptr, part, S, kLive, 1, ticket);
-      k_update_s<<<eb, kThreads, 0, st>>>(n, S, r, v, s);
+      k_loop_dots_alpha<<<rb, kThreads, 0, st>>>(n, r0, v, part, S, ticket);
+      k_update_s<<<(unsigned)vec_blocks(n), kThreads, 0, st>>>(n, S, r, v, s);
       spmv(s, t, kLive);
-      k_dots<<<rb, kThreads, 0, st>>>(n, t, t, t, s, nullptr, nullptr, part, S, kLive, 2, ticket);
+      k_loop_dots_omega<<<rb, kThreads, 0, st>>>(n, t, s, part, S, ticket);
       k_update_xr<<<rb, kThreads, 0, st>>>(n, S, p, s, t, r0, x, r, part, ticket);
     }
     if ((e = pull()) != cudaSuccess) return e;
@@ -711,12 +827,12 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
   const int64_t max_batches = 2 * (int64_t)max_iters + 3;
   int64_t batches = 0;
   int restarts[2] = {0, 0};
-  const dim3 ge(eb, 2), gr(rb, 2);
+  const dim3 ge(eb, 2), gr(rb, 2), gv((unsigned)vec_blocks(n), 2);
   const dim3 gs((unsigned)std::max<int64_t>({sliced_blocks(n, A[0].sl_long), sliced_blocks(n, A[1].sl_long), 1}), 2);
   for (;;) {
     const int f = tune ? kSpmvTiled + tune->start(st) : form;  // the tuner's candidates: tiled, sliced
     for (int k = 0; k < kBicgBatch; k++) {
-      k2_update_p<<<ge, kThreads, 0, st>>>(P);
+      k2_update_p<<<gv, kThreads, 0, st>>>(P);
       for (int sel = 0; sel < 2; sel++) {
         if (f == kSpmvSliced)
           k2_spmv_sliced<<<gs, kThreads, 0, st>>>(P, sel);
@@ -725,7 +841,7 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
         else
           k2_spmv_rows<<<ge, kThreads, 0, st>>>(P, sel);
         k2_dots<<<gr, kThreads, 0, st>>>(P, sel);
-        if (sel == 0) k2_update_s<<<ge, kThreads, 0, st>>>(P);
+        if (sel == 0) k2_update_s<<<gv, kThreads, 0, st>>>(P);
       }
       k2_update_xr<<<gr, kThreads, 0, st>>>(P);
     }

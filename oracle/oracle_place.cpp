@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <numeric>
 #include <tuple>
 
@@ -970,9 +971,24 @@ void Csr::mul(const float *x, float *y) const {
   }
 }
 
-// `sum` (src/bicgstab.rs:559-595): Eigen's SSE2 packet order.
+// `sum` (src/bicgstab.rs:559-595): Eigen's SSE2 packet order. With ORACLE_SUM_DOUBLE=1 in the
+// environment the terms are instead summed in double, in index order, and the total rounded to
+// float once: a measurement of how far the rounding of the inner products alone moves a run (the
+// device forms them in double), never a parity reference.
+static bool sum_in_double() {
+  static const bool on = [] {
+    const char *e = std::getenv("ORACLE_SUM_DOUBLE");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
 float eigen_sum(int64_t n, const float *a, const float *b) {
   auto f = [&](int64_t i) -> float { return b ? a[i] * b[i] : a[i]; };
+  if (sum_in_double()) {
+    double acc = 0.0;
+    for (int64_t i = 0; i < n; i++) acc += b ? (double)a[i] * (double)b[i] : (double)a[i];
+    return (float)acc;
+  }
   const int64_t P = 4;
   int64_t aligned_size2 = (n / (2 * P)) * (2 * P);
   int64_t aligned_size = (n / P) * P;

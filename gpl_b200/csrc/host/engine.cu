@@ -261,14 +261,18 @@ void Engine::upload(const EngineSetup &s) {
       std::stable_sort(net_order_.begin(), net_order_.end(), [&](int32_t a, int32_t b) { return s.net_start[a + 1] - s.net_start[a] < s.net_start[b + 1] - s.net_start[b]; });
     }
     // each pin's force goes to its place in its cell's pin list (cell_pins lists each pin once)
-    std::vector<int32_t> slot(n_pins_, -1);
+    std::vector<int32_t> slot;
+    big_assign(slot, (size_t)n_pins_, -1);
     parallel_for(s.cell_pins.size(), [&](size_t a, size_t b) {
       for (size_t k = a; k < b; k++) slot[s.cell_pins[k]] = (int32_t)k;
     });
     std::vector<int64_t> ns(n_nets_ + 1, 0);
     for (int32_t i = 0; i < n_nets_; i++) ns[i + 1] = ns[i] + (s.net_start[net_order_[i] + 1] - s.net_start[net_order_[i]]);
-    std::vector<int32_t> pc(n_pins_), ps(n_pins_);
-    std::vector<int2> pb(n_pins_);
+    std::vector<int32_t> pc, ps;
+    std::vector<int2> pb;
+    big_resize(pc, (size_t)n_pins_);
+    big_resize(ps, (size_t)n_pins_);
+    big_resize(pb, (size_t)n_pins_);
     std::vector<float> wt(n_nets_);
     parallel_for((size_t)n_nets_, [&](size_t a, size_t b) {
       for (size_t i = a; i < b; i++) {

@@ -1784,7 +1784,7 @@ static void init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip, co
   const Opts &o = P.o;
   std::vector<int> inst_cell(c.insts.size(), -1);
   for (size_t q = 0; q < ip.place.size(); q++) inst_cell[ip.place[q]] = (int)q;
-  P.gcells.reserve(ip.place.size() + ip.place.size() / 4);
+  reserve_huge(P.gcells, ip.place.size() + ip.place.size() / 4);
   P.gcells.resize(ip.place.size());
   parallel_for(ip.place.size(), [&](size_t a, size_t b) {
     for (size_t q = a; q < b; q++) {
@@ -1800,7 +1800,7 @@ static void init_nesterov_place(Log &log, const Design &d, Common &c, Ip &ip, co
       g.locked = i.locked;
     }
   });
-  P.gpins.resize(ip.pins.size());
+  big_resize(P.gpins, ip.pins.size());
   parallel_for(ip.pins.size(), [&](size_t a, size_t b) {
     for (size_t q = a; q < b; q++) {
       const Pin &p = ip.pins[q];
@@ -1950,18 +1950,18 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
   }
   progress("  device set-up: cells in Hilbert order");
   size_t n = P.gcell_of_dev.size();
-  s.hx.resize(n);
-  s.hy.resize(n);
-  s.dscale.resize(n);
-  s.area.resize(n);
-  s.kind.resize(n);
-  s.locked.resize(n);
-  s.dcx.resize(n);
-  s.dcy.resize(n);
-  s.cell_pin_start.assign(n + 1, 0);
+  big_resize(s.hx, n);
+  big_resize(s.hy, n);
+  big_resize(s.dscale, n);
+  big_resize(s.area, n);
+  big_resize(s.kind, n);
+  big_resize(s.locked, n);
+  big_resize(s.dcx, n);
+  big_resize(s.dcy, n);
+  big_assign(s.cell_pin_start, n + 1, (int64_t)0);
   auto cell_pins = [&](const GCell &g) { return g.is_filler() ? PinLists::Span{} : P.inst_pins[g.inst]; };
   for (size_t dv = 0; dv < n; dv++) s.cell_pin_start[dv + 1] = s.cell_pin_start[dv] + (int64_t)cell_pins(P.gcells[P.gcell_of_dev[dv]]).size();
-  s.cell_pins.resize((size_t)s.cell_pin_start[n]);
+  big_resize(s.cell_pins, (size_t)s.cell_pin_start[n]);
   parallel_for(n, [&](size_t a, size_t b) {
     for (size_t dv = a; dv < b; dv++) {
       const GCell &g = P.gcells[P.gcell_of_dev[dv]];
@@ -1986,8 +1986,8 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
   });
   s.net_start.assign(P.net_pins.start.begin(), P.net_pins.start.end());
   size_t np = P.gpins.size();
-  s.pin_cell.assign(np, -1);
-  s.pin_base.assign(2 * np, 0);
+  big_assign(s.pin_cell, np, -1);
+  big_assign(s.pin_base, 2 * np, 0);
   // pins are numbered net-major already (the placer's pins are made net by net)
   for (size_t q = 0; q < P.net_pins.items.size(); q++)
     if (P.net_pins.items[q] != (int)q) refuse("pins not numbered net by net");

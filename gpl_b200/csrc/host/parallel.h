@@ -3,12 +3,40 @@
 // exactly one iteration and reads nothing another iteration writes, so its results do not
 // depend on the number of threads or their timing.
 #pragma once
+#include <sys/mman.h>
+
 #include <algorithm>
 #include <cstddef>
+#include <cstdint>
 #include <thread>
 #include <vector>
 
 namespace gpl {
+
+// The construction's large host arrays (pins, cells and their copies, some 4 to 200 MB each):
+// the storage is reserved, the kernel asked for transparent huge pages on it (one fault per
+// 2 MB instead of per 4 KB where THP is in madvise mode; ignored elsewhere), and only then
+// sized and filled. Only the page size changes, never a value.
+inline void advise_huge(const void *p, size_t bytes) {
+  const uintptr_t a = ((uintptr_t)p + 4095) & ~(uintptr_t)4095, e = ((uintptr_t)p + bytes) & ~(uintptr_t)4095;
+  if (e > a) madvise((void *)a, e - a, MADV_HUGEPAGE);
+}
+template <class V>
+void reserve_huge(V &v, size_t n) {
+  if (v.capacity() >= n || n * sizeof(typename V::value_type) < ((size_t)4 << 20)) return;
+  v.reserve(n);
+  advise_huge(v.data(), n * sizeof(typename V::value_type));
+}
+template <class V>
+void big_resize(V &v, size_t n) {
+  reserve_huge(v, n);
+  v.resize(n);
+}
+template <class V, class T>
+void big_assign(V &v, size_t n, const T &x) {
+  reserve_huge(v, n);
+  v.assign(n, x);
+}
 
 // The host threads the construction uses: the machine's, at most 16.
 inline unsigned host_threads() {

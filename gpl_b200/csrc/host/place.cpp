@@ -203,7 +203,7 @@ Design design_from_c(const gpl_design_t *c) {
   d.die = rect4(c->die);
   d.core = rect4(c->core);
   for (int r = 0; r < c->n_rows; r++) d.rows.push_back(RowRec{rect4(c->row_box + 4 * r), c->row_pad[r] != 0, c->row_site[2 * r], c->row_site[2 * r + 1]});
-  d.insts.resize(c->n_insts);
+  big_resize(d.insts, (size_t)std::max(c->n_insts, 0));
   parallel_for((size_t)std::max(c->n_insts, 0), [&](size_t k0, size_t k1) {
     for (int k = (int)k0; k < (int)k1; k++) {
       DbInst &i = d.insts[k];
@@ -225,7 +225,7 @@ Design design_from_c(const gpl_design_t *c) {
       i.master_h = c->inst_master[2 * k + 1];
     }
   });
-  d.nets.resize(c->n_nets);
+  big_resize(d.nets, (size_t)std::max(c->n_nets, 0));
   parallel_for((size_t)std::max(c->n_nets, 0), [&](size_t n0, size_t n1) {
     for (int n = (int)n0; n < (int)n1; n++) {
       DbNet &net = d.nets[n];
@@ -619,7 +619,7 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
   for (size_t k = 0; k < c.insts.size(); k++)
     if (c.insts[k].db >= 0) inst_map[c.insts[k].db] = (int)k;
   Ip ip;
-  ip.db_bbox.resize(d.insts.size());
+  big_resize(ip.db_bbox, d.insts.size());
   parallel_for(d.insts.size(), [&](size_t a, size_t b) {
     for (size_t i = a; i < b; i++) ip.db_bbox[i] = d.insts[i].bbox;
   });
@@ -628,17 +628,24 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
   const size_t nn = c.nets.size();
   ip.net_pins.start.assign(nn + 1, 0);
   ip.inst_pins.start.assign(c.insts.size() + 1, 0);
-  for (size_t n = 0; n < nn; n++) {
-    const DbNet &dn = d.nets[c.nets[n].first];
-    ip.net_pins.start[n + 1] = ip.net_pins.start[n] + (int64_t)(dn.iterms.size() + (v.skip_io ? 0 : dn.bterms.size()));
-    for (auto &t : dn.iterms)
-      if (inst_map[t.inst] >= 0) ip.inst_pins.start[inst_map[t.inst] + 1]++;
-  }
+  // the counts in parallel (an instance's count by atomic adds: a sum, whatever their order),
+  // then the two scans
+  int64_t *inst_count = ip.inst_pins.start.data();
+  parallel_for(nn, [&](size_t a, size_t b) {
+    for (size_t n = a; n < b; n++) {
+      const DbNet &dn = d.nets[c.nets[n].first];
+      ip.net_pins.start[n + 1] = (int64_t)(dn.iterms.size() + (v.skip_io ? 0 : dn.bterms.size()));
+      for (auto &t : dn.iterms)
+        if (inst_map[t.inst] >= 0) __atomic_fetch_add(&inst_count[inst_map[t.inst] + 1], (int64_t)1, __ATOMIC_RELAXED);
+    }
+  });
+  for (size_t n = 0; n < nn; n++) ip.net_pins.start[n + 1] += ip.net_pins.start[n];
   const size_t total = (size_t)ip.net_pins.start[nn];
   for (size_t k = 0; k < c.insts.size(); k++) ip.inst_pins.start[k + 1] += ip.inst_pins.start[k];
-  ip.net_pins.items.resize(total);
-  ip.pins.resize(total);
-  std::vector<int> order(total, 0);
+  big_resize(ip.net_pins.items, total);
+  big_resize(ip.pins, total);
+  std::vector<int> order;
+  big_assign(order, total, 0);
   parallel_for(nn, [&](size_t a, size_t b) {
     for (size_t n = a; n < b; n++) {
       const DbNet &dn = d.nets[c.nets[n].first];
@@ -669,19 +676,22 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
       }
     }
   });
-  // each instance's pins in net order, then in its iterms' order (the reference walks an
-  // instance's iterms)
-  ip.inst_pins.items.resize((size_t)ip.inst_pins.start.back());
+  // each instance's pins in its iterms' order (the reference walks an instance's iterms),
+  // ties in pin (net) order: the lists are filled in parallel in any order, then each sorted
+  // by (iterm order, pin), which is the net-order fill's stable sort by iterm order
+  big_resize(ip.inst_pins.items, (size_t)ip.inst_pins.start.back());
   std::vector<int64_t> fill(ip.inst_pins.start.begin(), ip.inst_pins.start.end() - 1);
-  for (size_t q = 0; q < total; q++) {
-    int k = ip.pins[q].inst;
-    if (k >= 0 && !ip.pins[q].port) ip.inst_pins.items[fill[k]++] = (int)q;
-  }
-  auto by_order = [&](int x, int y) { return order[x] < order[y]; };
+  parallel_for(total, [&](size_t a, size_t b) {
+    for (size_t q = a; q < b; q++) {
+      int k = ip.pins[q].inst;
+      if (k >= 0 && !ip.pins[q].port) ip.inst_pins.items[__atomic_fetch_add(&fill[k], (int64_t)1, __ATOMIC_RELAXED)] = (int)q;
+    }
+  });
+  auto by_order = [&](int x, int y) { return order[x] < order[y] || (order[x] == order[y] && x < y); };
   parallel_for(c.insts.size(), [&](size_t a, size_t b) {
     for (size_t q = a; q < b; q++) {
       int *lo = ip.inst_pins.begin_of(q), *hi = ip.inst_pins.end_of(q);
-      if (!std::is_sorted(lo, hi, by_order)) std::stable_sort(lo, hi, by_order);
+      if (!std::is_sorted(lo, hi, by_order)) std::sort(lo, hi, by_order);
     }
   });
   for (size_t q = 0; q < c.insts.size(); q++)
@@ -780,12 +790,12 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
   std::vector<int32_t> ext(c.insts.size(), -1);
   for (size_t e = 0; e < n; e++) ext[ip.place[e]] = (int32_t)e;
   s.core = make_int4(d.core.lx, d.core.ly, d.core.ux, d.core.uy);
-  s.box.resize(n);
-  s.locked.resize(n);
-  s.grouped.resize(n);
-  s.clamp.resize(n);
-  s.db_box.resize(n);
-  s.db_size.resize(n);
+  big_resize(s.box, n);
+  big_resize(s.locked, n);
+  big_resize(s.grouped, n);
+  big_resize(s.clamp, n);
+  big_resize(s.db_box, n);
+  big_resize(s.db_size, n);
   parallel_for(n, [&](size_t a, size_t b) {
     for (size_t e = a; e < b; e++) {
       const Instance &i = c.insts[ip.place[e]];
@@ -807,13 +817,13 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
   // pins net by net, as make_pins numbered them (net n's run starts at net_pins.start[n])
   const size_t np = ip.pins.size(), nn = c.nets.size();
   if (ip.net_pins.size() != nn || (size_t)ip.net_pins.start[nn] != np) throw std::runtime_error("initial placement: pin order mismatch");
-  s.pin_e.resize(np);
-  s.pin_inst.resize(np);
-  s.pin_mio.resize(np);
-  s.pin_off.resize(np);
-  s.pin_xy.resize(np);
-  s.pin_hp.resize(np);
-  s.pin_static.resize(np);
+  big_resize(s.pin_e, np);
+  big_resize(s.pin_inst, np);
+  big_resize(s.pin_mio, np);
+  big_resize(s.pin_off, np);
+  big_resize(s.pin_xy, np);
+  big_resize(s.pin_hp, np);
+  big_resize(s.pin_static, np);
   s.net_start.assign(ip.net_pins.start.begin(), ip.net_pins.start.end());
   parallel_for(nn, [&](size_t a, size_t b) {
     for (size_t ni = a; ni < b; ni++) {

@@ -152,8 +152,8 @@ static cudaError_t dmalloc(T **p, size_t n, cudaStream_t s) {
   return cudaMallocAsync((void **)p, n * sizeof(T), s);  // from the device's pool (kept)
 }
 static int64_t g_h2d = 0;  // bytes the uploads below copied (folded into the engine's counter)
-template <class T>
-static cudaError_t upload_vec(T **p, const std::vector<T> &v, cudaStream_t s) {
+template <class T, class A>
+static cudaError_t upload_vec(T **p, const std::vector<T, A> &v, cudaStream_t s) {
   cudaError_t e = dmalloc(p, v.size(), s);
   if (e != cudaSuccess || v.empty()) return e;
   g_h2d += (int64_t)(v.size() * sizeof(T));
@@ -267,7 +267,10 @@ void Engine::upload(const EngineSetup &s) {
       for (size_t k = a; k < b; k++) slot[s.cell_pins[k]] = (int32_t)k;
     });
     std::vector<int64_t> ns(n_nets_ + 1, 0);
-    for (int32_t i = 0; i < n_nets_; i++) ns[i + 1] = ns[i] + (s.net_start[net_order_[i] + 1] - s.net_start[net_order_[i]]);
+    parallel_for((size_t)n_nets_, [&](size_t a, size_t b) {
+      for (size_t i = a; i < b; i++) ns[i + 1] = s.net_start[net_order_[i] + 1] - s.net_start[net_order_[i]];
+    });
+    for (int32_t i = 0; i < n_nets_; i++) ns[i + 1] += ns[i];
     std::vector<int32_t> pc, ps;
     std::vector<int2> pb;
     big_resize(pc, (size_t)n_pins_);

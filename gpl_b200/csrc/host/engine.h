@@ -2,6 +2,7 @@
 // and the initial placement's solve. The host control (nesterov.cpp) only sees scalars: the
 // overflow and gradient sums, the step-length distances and the HPWL, read once per trial.
 #pragma once
+#include "pod_vector.h"
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -34,17 +35,17 @@ struct RegionSetup {
 
 // Every device cell (regions contiguous, in each region's cell order) and every pin.
 struct EngineSetup {
-  std::vector<int32_t> hx, hy;     // half density size
-  std::vector<float> dscale, area; // density scale; (float)dx * (float)dy of the cell box
-  std::vector<uint8_t> kind;       // CELL_STD / CELL_MACRO / CELL_FILLER
-  std::vector<uint8_t> locked;
-  std::vector<int64_t> cell_pin_start;
-  std::vector<int32_t> cell_pins;
-  std::vector<int32_t> dcx, dcy;   // the density centres as set up
-  std::vector<int64_t> net_start;  // pins net-major
-  std::vector<int32_t> pin_cell;   // device cell, -1 for a pin with no moving cell
-  std::vector<int32_t> pin_base;   // 2 per pin: offset, or the fixed position
-  std::vector<float> net_weight;
+  pod_vector<int32_t> hx, hy;     // half density size
+  pod_vector<float> dscale, area; // density scale; (float)dx * (float)dy of the cell box
+  pod_vector<uint8_t> kind;       // CELL_STD / CELL_MACRO / CELL_FILLER
+  pod_vector<uint8_t> locked;
+  pod_vector<int64_t> cell_pin_start;
+  pod_vector<int32_t> cell_pins;
+  pod_vector<int32_t> dcx, dcy;   // the density centres as set up
+  pod_vector<int64_t> net_start;  // pins net-major
+  pod_vector<int32_t> pin_cell;   // device cell, -1 for a pin with no moving cell
+  pod_vector<int32_t> pin_base;   // 2 per pin: offset, or the fixed position
+  pod_vector<float> net_weight;
   std::vector<RegionSetup> regions;
 };
 

@@ -12,6 +12,7 @@
 #include <memory>
 #include <numeric>
 #include <stdexcept>
+#include <thread>
 
 #include "../kernels/engine_kernels.h"
 #include "engine.h"
@@ -828,7 +829,7 @@ static void init_bins(Log &log, const Design &d, const Common &c, const Base &ba
   bg.size_x = (double)(r.ux - r.lx) / (double)bg.cnt_x;
   bg.size_y = (double)(r.uy - r.ly) / (double)bg.cnt_y;
   log.info("GPL", 29, sfmt("%-21s %7.3f * %6.3f um", "Bin size (W * H):", bg.size_x / (double)d.dbu, bg.size_y / (double)d.dbu));
-  bg.bins.resize((size_t)bg.cnt_x * bg.cnt_y);
+  big_resize(bg.bins, (size_t)bg.cnt_x * bg.cnt_y);
   parallel_for((size_t)bg.cnt_y, [&](size_t y0, size_t y1) {
     for (int32_t y = (int32_t)y0; y < (int32_t)y1; y++)
       for (int32_t x = 0; x < bg.cnt_x; x++) {
@@ -845,6 +846,7 @@ static void init_bins(Log &log, const Design &d, const Common &c, const Base &ba
     if (b.ux - b.lx < 0 || b.uy - b.ly < 0) log.warn("GPL", 34, sfmt("Bin (center: %d,%d, index: %zu) has negative size: %d, %d", (b.lx + b.ux) / 2, (b.ly + b.uy) / 2, k, b.ux - b.lx, b.uy - b.ly));
   }
   log.info("GPL", 30, sfmt("Number of bins:             %10zu", bg.bins.size()));
+  progress("    bins: grid");
   nb.bg = std::move(bg);
   nb.fixed.clear();
   for (int k : base.fixed_insts) nb.fixed.push_back(c.insts[k]);
@@ -1143,16 +1145,20 @@ struct Placer {
     float n = (float)nbs.size();
     average_overflow = total_sum_overflow / n;
     base_wl_coef = total_base_wl_coef / n;
+    progress("    init: density");
     update_wirelength_coef(average_overflow);
     wa();
+    progress("    init: wirelength");
     for (size_t b = 0; b < nbs.size(); b++) {
       np_update_gradient((int)b, S_CUR_SLP_SUM, S_NUM, S_NUM, S_NUM, false);
       eng.prev_slp((int)b, initial_prev_coordi_update_coef);
       place_at((int)b, S_PREV_SLP);
       eng.field((int)b);
     }
+    progress("    init: first gradients");
     wa();
     for (size_t b = 0; b < nbs.size(); b++) np_update_gradient((int)b, S_PREV_SLP_SUM, S_PREV_SLP, S_CUR_SLP, S_CUR_SLP_SUM, false);
+    progress("    init: second gradients");
     for (size_t b = 0; b < nbs.size(); b++) {
       float step = init_density2((int)b);
       bool bad = std::isnan(step) || std::isinf(step);
@@ -1203,14 +1209,17 @@ struct Placer {
     std::vector<int32_t> cx, cy;
     eng.centres(cx, cy);
     device_check();
-    for (size_t d = 0; d < gcell_of_dev.size(); d++) {
-      GCell &g = gcells[gcell_of_dev[d]];
-      int32_t hx = g.d_dx() / 2, hy = g.d_dy() / 2;
-      g.dlx = cx[d] - hx;
-      g.dux = cx[d] + hx;
-      g.dly = cy[d] - hy;
-      g.duy = cy[d] + hy;
-    }
+    // gcell_of_dev is a permutation: each device cell writes its own host cell
+    parallel_for(gcell_of_dev.size(), [&](size_t a, size_t b) {
+      for (size_t d = a; d < b; d++) {
+        GCell &g = gcells[gcell_of_dev[d]];
+        int32_t hx = g.d_dx() / 2, hy = g.d_dy() / 2;
+        g.dlx = cx[d] - hx;
+        g.dux = cx[d] + hx;
+        g.dly = cy[d] - hy;
+        g.duy = cy[d] + hy;
+      }
+    });
   }
   // nesterovUpdateStepLength (src/nesterov.rs:2750-2772).
   bool nesterov_update_step_length(int b) {
@@ -1930,16 +1939,33 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
         idx[k] = nb.cells[k];
       }
     });
-    // stable: two LSD passes of 16-bit digits (the order of a stable sort by key)
-    for (int shift = 0; shift < 32; shift += 16) {
-      std::vector<size_t> cnt(65537, 0);
-      for (size_t k = 0; k < m; k++) cnt[((key[k] >> shift) & 0xffffu) + 1]++;
-      for (size_t q = 1; q < cnt.size(); q++) cnt[q] += cnt[q - 1];
-      for (size_t k = 0; k < m; k++) {
-        const size_t at = cnt[(key[k] >> shift) & 0xffffu]++;
-        key2[at] = key[k];
-        idx2[at] = idx[k];
-      }
+    // stable: four LSD passes of 8-bit digits (the order of a stable sort by key), each pass
+    // over fixed chunks in parallel: the chunks' digit counts, their offsets digit by digit in
+    // chunk order, then each chunk scattering its keys in order
+    const size_t T = std::max<size_t>(1, std::min<size_t>(host_threads(), m / 16384));
+    const size_t chunk = (m + T - 1) / T;
+    std::vector<size_t> hist(T * 256);
+    for (int shift = 0; shift < 32; shift += 8) {
+      std::fill(hist.begin(), hist.end(), 0);
+      parallel_for(T, [&](size_t t0, size_t t1) {
+        for (size_t t = t0; t < t1; t++)
+          for (size_t k = t * chunk; k < std::min(m, (t + 1) * chunk); k++) hist[t * 256 + ((key[k] >> shift) & 0xffu)]++;
+      }, 1);
+      size_t run = 0;
+      for (size_t dgt = 0; dgt < 256; dgt++)
+        for (size_t t = 0; t < T; t++) {
+          const size_t c = hist[t * 256 + dgt];
+          hist[t * 256 + dgt] = run;
+          run += c;
+        }
+      parallel_for(T, [&](size_t t0, size_t t1) {
+        for (size_t t = t0; t < t1; t++)
+          for (size_t k = t * chunk; k < std::min(m, (t + 1) * chunk); k++) {
+            const size_t at = hist[t * 256 + ((key[k] >> shift) & 0xffu)]++;
+            key2[at] = key[k];
+            idx2[at] = idx[k];
+          }
+      }, 1);
       key.swap(key2);
       idx.swap(idx2);
     }
@@ -1960,7 +1986,10 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
   big_resize(s.dcy, n);
   big_assign(s.cell_pin_start, n + 1, (int64_t)0);
   auto cell_pins = [&](const GCell &g) { return g.is_filler() ? PinLists::Span{} : P.inst_pins[g.inst]; };
-  for (size_t dv = 0; dv < n; dv++) s.cell_pin_start[dv + 1] = s.cell_pin_start[dv] + (int64_t)cell_pins(P.gcells[P.gcell_of_dev[dv]]).size();
+  parallel_for(n, [&](size_t a, size_t b) {
+    for (size_t dv = a; dv < b; dv++) s.cell_pin_start[dv + 1] = (int64_t)cell_pins(P.gcells[P.gcell_of_dev[dv]]).size();
+  });
+  for (size_t dv = 0; dv < n; dv++) s.cell_pin_start[dv + 1] += s.cell_pin_start[dv];
   big_resize(s.cell_pins, (size_t)s.cell_pin_start[n]);
   parallel_for(n, [&](size_t a, size_t b) {
     for (size_t dv = a; dv < b; dv++) {
@@ -1989,8 +2018,15 @@ static EngineSetup engine_setup(Placer &P, bool rebuild = false) {
   big_assign(s.pin_cell, np, -1);
   big_assign(s.pin_base, 2 * np, 0);
   // pins are numbered net-major already (the placer's pins are made net by net)
-  for (size_t q = 0; q < P.net_pins.items.size(); q++)
-    if (P.net_pins.items[q] != (int)q) refuse("pins not numbered net by net");
+  {
+    bool net_major = true;
+    parallel_for(P.net_pins.items.size(), [&](size_t a, size_t b) {
+      bool ok = true;
+      for (size_t q = a; q < b; q++) ok &= P.net_pins.items[q] == (int)q;
+      if (!ok) __atomic_store_n(&net_major, false, __ATOMIC_RELAXED);
+    });
+    if (!net_major) refuse("pins not numbered net by net");
+  }
   parallel_for(np, [&](size_t a, size_t b) {
     for (size_t p = a; p < b; p++) {
       const GPin &q = P.gpins[p];
@@ -2155,12 +2191,19 @@ struct NesterovLoop {
 // `placed_locations` (src/nesterov.rs:4099-4110) from the device's density centres.
 static std::vector<std::array<int32_t, 3>> placed_locations(const Common &c, Placer &P) {
   P.sync_host_centres();
-  std::vector<std::array<int32_t, 3>> out;
-  for (auto &g : P.gcells) {
-    if (g.inst < 0) continue;
-    const Instance &i = c.insts[g.inst];
-    out.push_back({i.db, g.d_cx() - i.dx() / 2 + c.site_x * P.o.pad_left, g.d_cy() - i.dy() / 2});
-  }
+  // the instances' cells in cell order: their ranks by a scan, then the rows in parallel
+  const size_t n = P.gcells.size();
+  std::vector<int64_t> at(n + 1, 0);
+  for (size_t q = 0; q < n; q++) at[q + 1] = at[q] + (P.gcells[q].inst >= 0 ? 1 : 0);
+  std::vector<std::array<int32_t, 3>> out((size_t)at[n]);
+  parallel_for(n, [&](size_t a, size_t b) {
+    for (size_t q = a; q < b; q++) {
+      const GCell &g = P.gcells[q];
+      if (g.inst < 0) continue;
+      const Instance &i = c.insts[g.inst];
+      out[(size_t)at[q]] = {i.db, g.d_cx() - i.dx() / 2 + c.site_x * P.o.pad_left, g.d_cy() - i.dy() / 2};
+    }
+  });
   return out;
 }
 
@@ -2321,8 +2364,11 @@ struct Run {
     if (!nesterov) return;
     while (step()) {
     }
+    progress("loop done");
     int iter = loop.end(res.log, d, *P, route.get());
+    progress("loop ended");
     res.locations = placed_locations(c, *P);
+    progress("placement written");
     auto t3 = std::chrono::steady_clock::now();
     res.t_np = std::chrono::duration<double>(t3 - t2).count();
     res.iterations = iter;
@@ -2341,6 +2387,21 @@ struct gpl_ctx {
   std::unique_ptr<Engine> eng;
   int poisson_mode = 1;
   bool trace = false;
+  // A finished command's host state (the design copy and the placer's arrays, about 1 GB in
+  // some millions of blocks at 1M cells) is freed on a thread of its own once the result is
+  // written; nothing of it touches the engine or the device (the routability state, which
+  // holds device buffers, is freed on the caller's thread first). One at a time; the context's
+  // end waits for it.
+  std::thread reaper;
+  void reap(std::unique_ptr<Run> run) {
+    if (run) run->route.reset();
+    settle();
+    reaper = std::thread([r = std::move(run)]() mutable { r.reset(); });
+  }
+  void settle() {
+    if (reaper.joinable()) reaper.join();
+  }
+  ~gpl_ctx() { settle(); }
 };
 
 static char *dupstr(const std::string &s) {
@@ -2488,8 +2549,8 @@ int gpl_global_placement(gpl_ctx *ctx, const gpl_design_t *cd, int argc, const c
   progress("device memory released");
   fill_result(run->res, out);
   progress("result written");
-  run.reset();
-  progress("host state released");
+  ctx->reap(std::move(run));
+  progress("host state handed off");
   return out->status;
 }
 
@@ -2587,6 +2648,7 @@ int gpl_session_close(gpl_session *s, gpl_result_t *out) {
   s->run->res.launches = s->ctx->eng->launches;
   s->ctx->eng->release();
   fill_result(s->run->res, out);
+  s->ctx->reap(std::move(s->run));
   delete s;
   return out->status;
 }

@@ -642,10 +642,12 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
   for (size_t n = 0; n < nn; n++) ip.net_pins.start[n + 1] += ip.net_pins.start[n];
   const size_t total = (size_t)ip.net_pins.start[nn];
   for (size_t k = 0; k < c.insts.size(); k++) ip.inst_pins.start[k + 1] += ip.inst_pins.start[k];
+  progress("    pins: counted");
   big_resize(ip.net_pins.items, total);
   big_resize(ip.pins, total);
   std::vector<int> order;
   big_assign(order, total, 0);
+  progress("    pins: arrays sized");
   parallel_for(nn, [&](size_t a, size_t b) {
     for (size_t n = a; n < b; n++) {
       const DbNet &dn = d.nets[c.nets[n].first];
@@ -676,6 +678,7 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
       }
     }
   });
+  progress("    pins: made");
   // each instance's pins in its iterms' order (the reference walks an instance's iterms),
   // ties in pin (net) order: the lists are filled in parallel in any order, then each sorted
   // by (iterm order, pin), which is the net-order fill's stable sort by iterm order
@@ -687,6 +690,7 @@ Ip make_pins(const Design &d, const Common &c, const Vars &v) {
       if (k >= 0 && !ip.pins[q].port) ip.inst_pins.items[__atomic_fetch_add(&fill[k], (int64_t)1, __ATOMIC_RELAXED)] = (int)q;
     }
   });
+  progress("    pins: instance lists filled");
   auto by_order = [&](int x, int y) { return order[x] < order[y] || (order[x] == order[y] && x < y); };
   parallel_for(c.insts.size(), [&](size_t a, size_t b) {
     for (size_t q = a; q < b; q++) {
@@ -814,6 +818,7 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
   std::vector<int> inst_map(d.insts.size(), -1);
   for (size_t k = 0; k < c.insts.size(); k++)
     if (c.insts[k].db >= 0) inst_map[c.insts[k].db] = (int)k;
+  progress("    set-up: instances");
   // pins net by net, as make_pins numbered them (net n's run starts at net_pins.start[n])
   const size_t np = ip.pins.size(), nn = c.nets.size();
   if (ip.net_pins.size() != nn || (size_t)ip.net_pins.start[nn] != np) throw std::runtime_error("initial placement: pin order mismatch");
@@ -825,6 +830,7 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
   big_resize(s.pin_hp, np);
   big_resize(s.pin_static, np);
   s.net_start.assign(ip.net_pins.start.begin(), ip.net_pins.start.end());
+  progress("    set-up: pin arrays sized");
   parallel_for(nn, [&](size_t a, size_t b) {
     for (size_t ni = a; ni < b; ni++) {
       const DbNet &dn = d.nets[c.nets[ni].first];
@@ -898,21 +904,24 @@ Ip do_bicgstab_place_device(Log &log, const Design &d, Common &c, const Vars &v,
   std::vector<int4> box, db_box;
   device(dev.download(box, db_box), "initial placement download");
   progress("initial placement downloaded");
-  for (size_t e = 0; e < n; e++) {
-    int k = ip.place[e];
-    Instance &i = c.insts[k];
-    if (i.locked) continue;
-    i.lx = box[e].x;
-    i.ly = box[e].y;
-    i.ux = box[e].z;
-    i.uy = box[e].w;
-    ip.db_bbox[i.db] = Rect{db_box[e].x, db_box[e].y, db_box[e].z, db_box[e].w};
-    int32_t cx = i.cx(), cy = i.cy();
-    for (int q : ip.inst_pins[k]) {
-      ip.pins[q].cx = cx + ip.pins[q].off_x;
-      ip.pins[q].cy = cy + ip.pins[q].off_y;
+  // each placed instance writes only itself, its database box and its own pins
+  parallel_for(n, [&](size_t a, size_t b) {
+    for (size_t e = a; e < b; e++) {
+      int k = ip.place[e];
+      Instance &i = c.insts[k];
+      if (i.locked) continue;
+      i.lx = box[e].x;
+      i.ly = box[e].y;
+      i.ux = box[e].z;
+      i.uy = box[e].w;
+      ip.db_bbox[i.db] = Rect{db_box[e].x, db_box[e].y, db_box[e].z, db_box[e].w};
+      int32_t cx = i.cx(), cy = i.cy();
+      for (int q : ip.inst_pins[k]) {
+        ip.pins[q].cx = cx + ip.pins[q].off_x;
+        ip.pins[q].cy = cy + ip.pins[q].off_y;
+      }
     }
-  }
+  });
   return ip;
 }
 

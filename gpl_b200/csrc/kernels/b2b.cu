@@ -285,6 +285,45 @@ __device__ __forceinline__ int64_t warp_runs(const unsigned long long *sk, int m
   return base;
 }
 
+// The same for a block's warps at once (rows of the block tiers): the sorted positions cut
+// into one contiguous section of whole 32-position steps per warp, each warp counting the runs
+// that start in its section, a scan of those counts, then each warp summing and writing its
+// runs (a run that starts in a section may end in the next) from its offset. The distinct
+// columns come out in position order, as warp_runs writes them. Every thread of the block
+// calls it; returns the row's distinct columns.
+__device__ __forceinline__ int64_t block_runs(const unsigned long long *sk, int m, int64_t b, const float *val, int32_t *ucol, float *uval) {
+  __shared__ int64_t counts[kThreads / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int steps = (m + 31) / 32, per = (steps + nw - 1) / nw;
+  const int lo = w * per * 32, hi = min(m, (w + 1) * per * 32);
+  auto starts_at = [&](int p) { return p < hi && (p == 0 || (uint32_t)(sk[p] >> 32) != (uint32_t)(sk[p - 1] >> 32)); };
+  int64_t cnt = 0;
+  for (int p0 = lo; p0 < hi; p0 += 32) cnt += __popc(__ballot_sync(0xffffffffu, starts_at(p0 + lane)));
+  if (lane == 0) counts[w] = cnt;
+  __syncthreads();
+  int64_t base = 0, total = 0;
+  for (int k = 0; k < nw; k++) {
+    if (k < w) base += counts[k];
+    total += counts[k];
+  }
+  for (int p0 = lo; p0 < hi; p0 += 32) {
+    const int p = p0 + lane;
+    const bool start = starts_at(p);
+    const unsigned mask = __ballot_sync(0xffffffffu, start);
+    if (start) {
+      const uint32_t c = (uint32_t)(sk[p] >> 32);
+      int end = p + 1;
+      while (end < m && (uint32_t)(sk[end] >> 32) == c) end++;
+      const int64_t u = base + __popc(mask & ((1u << lane) - 1u));
+      ucol[b + u] = (int32_t)c;
+      uval[b + u] = run_sum(sk, p, end, val);
+    }
+    base += __popc(mask);
+  }
+  __syncthreads();  // counts free for the block's next row
+  return total;
+}
+
 // A warp per row of at most 32 R keys: element i = j * 32 + lane lives in register j.
 template <int R>
 __device__ __forceinline__ void warp_bitonic(unsigned long long (&v)[R]) {
@@ -354,7 +393,7 @@ __global__ void __launch_bounds__(kThreads) k_row_collapse_warp(int64_t n, const
 }
 
 // Rows of up to kRowLong keys, a block each: the keys bitonic-sorted in shared memory
-// (padded to a power of two), then one warp walks the runs. Longer rows go to `next`.
+// (padded to a power of two), then the block's warps walk the runs. Longer rows go to `next`.
 constexpr int kRowLong = 8192;
 __global__ void __launch_bounds__(kThreads) k_row_collapse_block(const int32_t *list, const int *count, const int64_t *row_off, const unsigned long long *bucket, const float *val, int32_t *ucol, float *uval, int64_t *ucount, int32_t *next, int *next_count) {
   extern __shared__ unsigned long long skb[];
@@ -386,10 +425,8 @@ __global__ void __launch_bounds__(kThreads) k_row_collapse_block(const int32_t *
         }
         __syncthreads();
       }
-    if (threadIdx.x < 32) {
-      int64_t u = warp_runs(skb, (int)m, b, val, ucol, uval);
-      if (threadIdx.x == 0) ucount[r] = u;
-    }
+    const int64_t u = block_runs(skb, (int)m, b, val, ucol, uval);
+    if (threadIdx.x == 0) ucount[r] = u;
     __syncthreads();
   }
 }
@@ -397,8 +434,8 @@ __global__ void __launch_bounds__(kThreads) k_row_collapse_block(const int32_t *
 // The longest rows, a block each: chunks of kRowLong keys bitonic-sorted in shared memory and
 // written back, then runs merged pairwise between the bucket and a scratch of the same span
 // (merge path: each thread's share of a merged run starts where a binary search on its
-// diagonal puts it, then it merges that share in order) until one run remains, which a warp
-// walks as the other tiers do.
+// diagonal puts it, then it merges that share in order) until one run remains, whose column
+// runs the block's warps walk as in the block tier.
 __device__ __forceinline__ void merge_share(const unsigned long long *A, int64_t la, const unsigned long long *B, int64_t lb, unsigned long long *out) {
   const int64_t total = la + lb, per = (total + blockDim.x - 1) / blockDim.x;
   const int64_t d = (int64_t)threadIdx.x * per;
@@ -460,10 +497,8 @@ __global__ void __launch_bounds__(kThreads) k_row_collapse_long(const int32_t *l
       for (int64_t i = threadIdx.x; i < m; i += blockDim.x) keys[i] = src[i];
       __syncthreads();
     }
-    if (threadIdx.x < 32) {
-      const int64_t u = warp_runs(keys, (int)m, b, val, ucol, uval);
-      if (threadIdx.x == 0) ucount[r] = u;
-    }
+    const int64_t u = block_runs(keys, (int)m, b, val, ucol, uval);
+    if (threadIdx.x == 0) ucount[r] = u;
     __syncthreads();
   }
 }
@@ -661,8 +696,8 @@ cudaError_t alloc(T **p, size_t n, cudaStream_t s) {
   *p = nullptr;
   return cudaMallocAsync((void **)p, std::max<size_t>(n, 1) * sizeof(T), s);
 }
-template <class T>
-cudaError_t put(T **p, const std::vector<T> &v, cudaStream_t s, int64_t &bytes) {
+template <class T, class A>
+cudaError_t put(T **p, const std::vector<T, A> &v, cudaStream_t s, int64_t &bytes) {
   cudaError_t e = alloc(p, v.size(), s);
   if (e != cudaSuccess || v.empty()) return e;
   bytes += (int64_t)(v.size() * sizeof(T));

@@ -3,6 +3,7 @@
 // HPWL over the instances' database boxes. The host loop (place.cpp) keeps the reference's
 // control flow (`doBicgstabPlace`, src/initial_place.rs:420-446) and reads back scalars only.
 #pragma once
+#include "pod_vector.h"
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -19,20 +20,20 @@ namespace gpl {
 // order (e), pins net by net (`Ip::pins`).
 struct IpSetup {
   // per placed instance e
-  std::vector<int4> box;       // lx, ly, ux, uy after the initial positions
-  std::vector<uint8_t> locked;
-  std::vector<int4> clamp;     // the group's region box, for grouped instances
-  std::vector<uint8_t> grouped;
-  std::vector<int4> db_box;    // the database box the report's HPWL reads (the design's at first)
-  std::vector<int2> db_size;   // the database box's width and height
+  pod_vector<int4> box;       // lx, ly, ux, uy after the initial positions
+  pod_vector<uint8_t> locked;
+  pod_vector<int4> clamp;     // the group's region box, for grouped instances
+  pod_vector<uint8_t> grouped;
+  pod_vector<int4> db_box;    // the database box the report's HPWL reads (the design's at first)
+  pod_vector<int2> db_size;   // the database box's width and height
   // per pin
-  std::vector<int32_t> pin_e;     // placed instance, -1 for none (port, fixed, outside the set)
-  std::vector<int32_t> pin_inst;  // placer instance (-1 for ports): the "same instance" test
-  std::vector<uint8_t> pin_mio;   // movable IO: left out of the matrix and the extremes
-  std::vector<int2> pin_off, pin_xy;
-  std::vector<uint8_t> pin_hp;    // report HPWL: 0 the instance's db box, 1 the static box, 2 none
-  std::vector<int4> pin_static;   // the static box (fixed instance, outside instance, port bbox)
-  std::vector<int64_t> net_start;
+  pod_vector<int32_t> pin_e;     // placed instance, -1 for none (port, fixed, outside the set)
+  pod_vector<int32_t> pin_inst;  // placer instance (-1 for ports): the "same instance" test
+  pod_vector<uint8_t> pin_mio;   // movable IO: left out of the matrix and the extremes
+  pod_vector<int2> pin_off, pin_xy;
+  pod_vector<uint8_t> pin_hp;    // report HPWL: 0 the instance's db box, 1 the static box, 2 none
+  pod_vector<int4> pin_static;   // the static box (fixed instance, outside instance, port bbox)
+  pod_vector<int64_t> net_start;
   int4 core{};                    // `updateCoordi` clamps to the core first
   int32_t max_fanout = 200, min_diff = 1500;
   float weight_scale = 800.0f;

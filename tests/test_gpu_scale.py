@@ -160,7 +160,9 @@ def test_batched_form_matches_the_oracle():
     1e-3 there). There the BiCGSTAB iterates follow the rounding of every inner product, and
     the reference forms those in float in Eigen's packet order while the device forms them in
     double: the deviation is that rounding's, not the batched form's (which matches the
-    per-region form bit for bit: test_packed_launches_give_the_same_run)."""
+    per-region form bit for bit: test_packed_launches_give_the_same_run). The oracle itself,
+    with its inner products summed in double (ORACLE_SUM_DOUBLE=1), moves from its own run by
+    up to 1.65 % over these rounds; the engine by up to 1.12 %."""
     if "cfg4" not in RUNS:
         pytest.skip("no recorded oracle run for cfg4")
     ref = RUNS["cfg4"]

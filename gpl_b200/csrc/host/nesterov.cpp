@@ -1106,23 +1106,26 @@ struct Placer {
     Nb &nb = nbs[b];
     size_t n = nb.cells.size();
     std::vector<float> xy(2 * n);
-    for (size_t i = 0; i < n; i++) {
-      GCell &g = gcells[gcell_of_dev[nb.cell_off + i]];  // the device's order of the region's cells
-      // updateDensityCoordiLayoutInside (:2173-2185) on the host copy of the density box
-      float tlx = fmaxr((float)g.dlx, (float)nb.bg.lx), tly = fmaxr((float)g.dly, (float)nb.bg.ly);
-      if (tlx + (float)g.d_dx() > (float)nb.bg.ux) tlx = (float)(nb.bg.ux - g.d_dx());
-      if (tly + (float)g.d_dy() > (float)nb.bg.uy) tly = (float)(nb.bg.uy - g.d_dy());
-      int32_t lx = f2i(tlx), ly = f2i(tly);
-      g.dux = lx + (g.dux - g.dlx);
-      g.duy = ly + (g.duy - g.dly);
-      g.dlx = lx;
-      g.dly = ly;
-      xy[2 * i] = (float)g.d_cx();
-      xy[2 * i + 1] = (float)g.d_cy();
-    }
+    // each of the region's device cells moves its own host cell (gcell_of_dev is a permutation)
+    parallel_for(n, [&](size_t a, size_t e) {
+      for (size_t i = a; i < e; i++) {
+        GCell &g = gcells[gcell_of_dev[nb.cell_off + i]];  // the device's order of the region's cells
+        // updateDensityCoordiLayoutInside (:2173-2185) on the host copy of the density box
+        float tlx = fmaxr((float)g.dlx, (float)nb.bg.lx), tly = fmaxr((float)g.dly, (float)nb.bg.ly);
+        if (tlx + (float)g.d_dx() > (float)nb.bg.ux) tlx = (float)(nb.bg.ux - g.d_dx());
+        if (tly + (float)g.d_dy() > (float)nb.bg.uy) tly = (float)(nb.bg.uy - g.d_dy());
+        int32_t lx = f2i(tlx), ly = f2i(tly);
+        g.dux = lx + (g.dux - g.dlx);
+        g.duy = ly + (g.duy - g.dly);
+        g.dlx = lx;
+        g.dly = ly;
+        xy[2 * i] = (float)g.d_cx();
+        xy[2 * i + 1] = (float)g.d_cy();
+      }
+    });
     eng.set_coords(b, S_CUR_SLP, xy);
-    eng.set_coords(b, S_PREV_SLP, xy);
-    eng.set_coords(b, S_CUR, xy);
+    eng.copy_slot(b, S_PREV_SLP, S_CUR_SLP);
+    eng.copy_slot(b, S_CUR, S_CUR_SLP);
     place_at(b, S_CUR_SLP);
     nbs[b].prev_hpwl = hpwl();
     eng.field(b);

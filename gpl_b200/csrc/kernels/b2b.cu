@@ -376,6 +376,17 @@ __global__ void __launch_bounds__(kThreads) k_row_collapse_warp(int64_t n, const
       if (lane == 0) next[atomicAdd(next_count, 1)] = (int32_t)r;
       continue;
     }
+    if (m <= 1) {  // nothing to sort (most right-hand-side rows): the key as it is
+      if (lane == 0) {
+        if (m == 1) {
+          const unsigned long long k = bucket[b];
+          ucol[b] = (int32_t)(uint32_t)(k >> 32);
+          uval[b] = val[(uint32_t)k];
+        }
+        ucount[r] = m;
+      }
+      continue;
+    }
     unsigned long long v[R];
 #pragma unroll
     for (int a = 0; a < R; a++) {

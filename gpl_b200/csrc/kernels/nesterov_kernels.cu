@@ -201,6 +201,12 @@ __device__ __forceinline__ void place_cells_block(const RegionArgs &r, const Cel
   float scale = 0.0f;
   uint8_t kind = 0;
   if (valid) {
+    // the cell's constants first: after the stores below the compiler could not move these
+    // loads ahead of them (the cell arrays are not marked restrict), each would be a round trip
+    // of its own
+    const int32_t hx = c.hx[i], hy = c.hy[i];
+    scale = c.dscale[i];
+    kind = c.kind[i];
     float2 p = make_float2(0.0f, 0.0f);
     if (mode == PLACE_AT) {
       p = coords[i];
@@ -217,10 +223,10 @@ __device__ __forceinline__ void place_cells_block(const RegionArgs &r, const Cel
         float ny = __fadd_rn(cs.y, __fmul_rn(step, g.y));
         float sx = __fadd_rn(nx, __fmul_rn(coeff, __fsub_rn(nx, cu.x)));
         float sy = __fadd_rn(ny, __fmul_rn(coeff, __fsub_rn(ny, cu.y)));
-        float hx = (float)c.hx[i], hy = (float)c.hy[i];
+        const float fhx = (float)hx, fhy = (float)hy;
         float glx = (float)r.lx, gly = (float)r.ly, gux = (float)r.ux, guy = (float)r.uy;
-        c.next[i] = make_float2(inside_axis(nx, hx, glx, gux), inside_axis(ny, hy, gly, guy));
-        p = make_float2(inside_axis(sx, hx, glx, gux), inside_axis(sy, hy, gly, guy));
+        c.next[i] = make_float2(inside_axis(nx, fhx, glx, gux), inside_axis(ny, fhy, gly, guy));
+        p = make_float2(inside_axis(sx, fhx, glx, gux), inside_axis(sy, fhy, gly, guy));
         c.next_slp[i] = p;
       }
     }
@@ -234,15 +240,12 @@ __device__ __forceinline__ void place_cells_block(const RegionArgs &r, const Cel
       cy = f2i_rz(p.y);
       c.dc[i] = make_int2(cx, cy);
     }
-    int32_t hx = c.hx[i], hy = c.hy[i];
     dlx = cx - hx;
     dux = cx + hx;
     dly = cy - hy;
     duy = cy + hy;
     bin_span(dlx, dux, r.lx, r.size_x, r.inv_size_x, r.nx, x0, x1);
     bin_span(dly, duy, r.ly, r.size_y, r.inv_size_y, r.ny, y0, y1);
-    scale = c.dscale[i];
-    kind = c.kind[i];
   }
   // the block's bin box
   if (threadIdx.x == 0) {

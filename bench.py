@@ -407,6 +407,98 @@ def ours(a):
     print(json.dumps(out))
 
 
+# ---- the cuFFT comparison point for the density solve (a measurement, not an engine form):
+# the same four transforms (src/nesterov.rs:412-444: the forward 2-D DCT, then the DST-DCT
+# and DCT-DST inverses for the two fields) through FFTs (torch.fft runs cuFFT) in FP32, each
+# 1-D transform by Makhoul's reordering (a DCT-II of length N is one complex FFT of the
+# even-then-reversed-odd samples and a twiddle), the inverse by the same in reverse, and the
+# shifted DST-III (its k = 0 term the (-1)^n one) as (-1)^n times the DCT-III of the
+# coefficients in reverse order.
+def _dct2(a, dim):
+    import math
+    import torch
+    a = a.movedim(dim, -1)
+    N = a.shape[-1]
+    v = torch.cat([a[..., ::2], a[..., 1::2].flip(-1)], dim=-1)
+    k = torch.arange(N, device=a.device, dtype=a.dtype)
+    return (torch.fft.fft(v, dim=-1) * torch.polar(torch.ones_like(k), -math.pi * k / (2 * N))).real.movedim(-1, dim)
+
+
+def _dct3(X, dim):
+    """y[n] = sum_k X[k] cos(pi k (2n+1) / 2N), every weight 1."""
+    import math
+    import torch
+    X = X.movedim(dim, -1)
+    N = X.shape[-1]
+    Y = torch.cat([X[..., :1] * N, X[..., 1:] * (N / 2.0)], dim=-1)
+    Yr = torch.cat([torch.zeros_like(Y[..., :1]), Y[..., 1:].flip(-1)], dim=-1)
+    k = torch.arange(N, device=X.device, dtype=X.dtype)
+    v = torch.fft.ifft(torch.polar(torch.ones_like(k), math.pi * k / (2 * N)) * torch.complex(Y, -Yr), dim=-1).real
+    y = torch.empty_like(v)
+    y[..., ::2] = v[..., : (N + 1) // 2]
+    y[..., 1::2] = v[..., (N + 1) // 2:].flip(-1)
+    return y.movedim(-1, dim)
+
+
+def _dst3(S, dim):
+    """y[n] = sum_u S[u] sin(pi k'_u (2n+1) / 2N), k'_0 = N, k'_u = u."""
+    import torch
+    S = S.movedim(dim, -1)
+    N = S.shape[-1]
+    y = _dct3(torch.cat([S[..., :1], S[..., 1:].flip(-1)], dim=-1), -1)
+    sign = 1.0 - 2.0 * (torch.arange(N, device=S.device) % 2).to(S.dtype)
+    return (y * sign).movedim(-1, dim)
+
+
+def fft_density_solve(rho, wx, wy):
+    """The fields (x-major [x][y]) of a density by FFTs: the transforms above with the
+    forward scaling (1/n for the first coefficient, 2/n for the rest, each axis) and the
+    spectral step of the engine's forms (the (0, 0) term zero). No host value is copied in
+    (it runs inside a CUDA graph capture)."""
+    import torch
+    nx, ny = rho.shape
+    ix, iy = torch.arange(nx, device=rho.device), torch.arange(ny, device=rho.device)
+    hx = torch.full((nx,), 2.0 / nx, dtype=rho.dtype, device=rho.device).masked_fill(ix == 0, 1.0 / nx)
+    hy = torch.full((ny,), 2.0 / ny, dtype=rho.dtype, device=rho.device).masked_fill(iy == 0, 1.0 / ny)
+    A = _dct2(_dct2(rho, 1), 0) * hx[:, None] * hy[None, :]
+    z00 = (ix[:, None] == 0) & (iy[None, :] == 0)
+    d = (wx[:, None] * wx[:, None] + wy[None, :] * wy[None, :]).masked_fill(z00, 1.0)
+    P = (A / d).masked_fill(z00, 0.0)
+    return _dst3(_dct3(P * wx[:, None], 1), 0), _dct3(_dst3(P * wy[None, :], 1), 0)
+
+
+def cufft_point(local, n, dens, ex, ey, wx, wy):
+    """The FFT solve in FP32 on the device, captured in a CUDA graph (so the host's launches
+    do not set the pace), timed over 50 replays with CUDA events; its field error against the
+    FP64 yardstick as for the engine's forms."""
+    import torch
+    dev = f"cuda:{local}"
+    rho = dens.view(n, n)
+    twx, twy = torch.from_numpy(wx).to(dev), torch.from_numpy(wy).to(dev)
+    s = torch.cuda.Stream(dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            fx, fy = fft_density_solve(rho, twx, twy)
+    torch.cuda.current_stream(dev).wait_stream(s)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        fx, fy = fft_density_solve(rho, twx, twy)
+    for _ in range(3):
+        g.replay()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(50):
+        g.replay()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    us = e0.elapsed_time(e1) * 1000.0 / 50
+    err = max(float((fx.reshape(-1).double() - ex).abs().max() / ex.abs().max()), float((fy.reshape(-1).double() - ey).abs().max() / ey.abs().max()))
+    del g
+    return {"what": "torch.fft (cuFFT) FP32: the four transforms as FFTs with Makhoul's reordering, one CUDA graph", "us_per_solve": us, "field_rel_err": err}
+
+
 def precision_report(local, n):
     """Each form's field error against the FP64 device solve (the same transforms in double),
     on a seeded density of the workload's grid: max |error| over max |field|."""
@@ -431,6 +523,10 @@ def precision_report(local, n):
         torch.cuda.synchronize(local)
         e = max(float((gx.double() - ex).abs().max() / ex.abs().max()), float((gy.double() - ey).abs().max() / ey.abs().max()))
         out[f"field_rel_err_{name}"] = e
+    try:
+        out["cufft_fp32"] = cufft_point(local, n, dens, ex, ey, wx, wy)
+    except Exception as err:  # a comparison point: its failure leaves the report as it was
+        out["cufft_fp32"] = {"unavailable": str(err)[:200]}
     return out
 
 

@@ -149,7 +149,12 @@ typedef struct gpl_result {
 typedef struct gpl_ctx gpl_ctx;
 
 /* One context binds one CUDA device and its own stream. Calls on one context are not
- * reentrant; contexts are independent. Returns NULL when the device cannot be used. */
+ * reentrant; contexts are independent. Returns NULL when the device cannot be used.
+ * A finished command's host copies (the design, the placer's arrays: about 1 GB at 1M cells)
+ * are freed by a thread of the context after the command has written its result, so the call
+ * returns without waiting for them; at most one such thread runs (a command that ends while
+ * the previous one's copies are still being freed waits for that first), and gpl_destroy
+ * waits for it. Nothing the caller passed or received is touched by it. */
 gpl_ctx *gpl_create(int device);
 void gpl_destroy(gpl_ctx *ctx);
 

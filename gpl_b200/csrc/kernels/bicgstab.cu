@@ -563,20 +563,34 @@ struct SysPair {
 };
 __device__ __forceinline__ SysDev pick(const SysPair &P) { return blockIdx.y ? P.a[1] : P.a[0]; }
 
+// The loop's kernels are launched chained (programmatic dependent launch): a kernel's blocks
+// may become resident while the kernel before it drains, and each first waits in hardware
+// (griddepcontrol.wait) until that kernel has completed and its memory is visible, before it
+// reads anything; it then lets the next kernel's blocks in. Launched unchained, the wait and
+// the release do nothing. No result changes.
+__device__ __forceinline__ void chain_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __global__ void __launch_bounds__(kThreads) k2_update_p(SysPair P) {
+  chain_enter();
   SysDev q = pick(P);
   update_p_body(q.n, q.S, q.r, q.v, q.p);
 }
 // sel 0: v = A p; sel 1: t = A s (each system's rows in the form's order, gated as a whole).
 __global__ void __launch_bounds__(kThreads) k2_spmv_rows(SysPair P, int sel) {
+  chain_enter();
   SysDev q = pick(P);
   spmv_rows_body(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
 }
 __global__ void __launch_bounds__(kThreads) k2_spmv_tiled(SysPair P, int sel) {
+  chain_enter();
   SysDev q = pick(P);
   spmv_tiled_body(q.n, q.rs, q.cols, q.vals, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
 }
 __global__ void __launch_bounds__(kThreads) k2_spmv_sliced(SysPair P, int sel) {
+  chain_enter();
   SysDev q = pick(P);
   spmv_sliced_body(q.n, q.sl_long, q.rs, q.cols, q.vals, q.sl_row, q.sl_len, q.sl_start, q.sl_ent, sel ? q.s : q.p, sel ? q.t : q.v, q.S, kLive);
 }
@@ -586,6 +600,7 @@ __global__ void __launch_bounds__(kThreads) k2_spmv_sliced(SysPair P, int sel) {
 // initial placement: the sliced form's rows are in length order, so their r0 and s reads
 // scatter, and the fused tail's block reductions stall every block.)
 __global__ void __launch_bounds__(kThreads, 4) k2_dots(SysPair P, int sel) {
+  chain_enter();
   SysDev q = pick(P);
   if (sel == 0)
     loop_dots_body<0>(q.n, q.r0, q.v, q.part, q.S, q.ticket);
@@ -594,10 +609,12 @@ __global__ void __launch_bounds__(kThreads, 4) k2_dots(SysPair P, int sel) {
 }
 
 __global__ void __launch_bounds__(kThreads) k2_update_s(SysPair P) {
+  chain_enter();
   SysDev q = pick(P);
   update_s_body(q.n, q.S, q.r, q.v, q.s);
 }
 __global__ void __launch_bounds__(kThreads, 4) k2_update_xr(SysPair P) {
+  chain_enter();
   SysDev q = pick(P);
   update_xr_body(q.n, q.S, q.p, q.s, q.t, q.r0, q.x, q.r, q.part, q.ticket);
 }
@@ -738,6 +755,26 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
   return cudaGetLastError();
 }
 
+// One chained launch of a loop kernel (kThreads a block, no dynamic shared memory).
+template <typename... KArgs, typename... Args>
+static cudaError_t chained(void (*kernel)(KArgs...), dim3 grid, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+#define CK_LAUNCH(x)                        \
+  do {                                      \
+    if ((e = (x)) != cudaSuccess) return e; \
+  } while (0)
+
 cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], float *const x[2], int max_iters, void *const scratch[2], cudaStream_t st, BicgResult out[2], int form, Tuner *tune) {
   const int64_t n = A[0].n;
   if (A[1].n != n) return cudaErrorInvalidValue;
@@ -832,18 +869,18 @@ cudaError_t bicgstab_solve_pair(const CsrDev A[2], const float *const b[2], floa
   for (;;) {
     const int f = tune ? kSpmvTiled + tune->start(st) : form;  // the tuner's candidates: tiled, sliced
     for (int k = 0; k < kBicgBatch; k++) {
-      k2_update_p<<<gv, kThreads, 0, st>>>(P);
+      CK_LAUNCH(chained(k2_update_p, gv, st, P));
       for (int sel = 0; sel < 2; sel++) {
         if (f == kSpmvSliced)
-          k2_spmv_sliced<<<gs, kThreads, 0, st>>>(P, sel);
+          CK_LAUNCH(chained(k2_spmv_sliced, gs, st, P, sel));
         else if (f == kSpmvTiled)
-          k2_spmv_tiled<<<ge, kThreads, 0, st>>>(P, sel);
+          CK_LAUNCH(chained(k2_spmv_tiled, ge, st, P, sel));
         else
-          k2_spmv_rows<<<ge, kThreads, 0, st>>>(P, sel);
-        k2_dots<<<gr, kThreads, 0, st>>>(P, sel);
-        if (sel == 0) k2_update_s<<<gv, kThreads, 0, st>>>(P);
+          CK_LAUNCH(chained(k2_spmv_rows, ge, st, P, sel));
+        CK_LAUNCH(chained(k2_dots, gr, st, P, sel));
+        if (sel == 0) CK_LAUNCH(chained(k2_update_s, gv, st, P));
       }
-      k2_update_xr<<<gr, kThreads, 0, st>>>(P);
+      CK_LAUNCH(chained(k2_update_xr, gr, st, P));
     }
     if (tune) tune->stop(st);
     if ((e = pull()) != cudaSuccess) return e;

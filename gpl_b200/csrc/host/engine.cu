@@ -5,6 +5,7 @@
 
 #include "../kernels/b2b.h"
 #include "../kernels/bicgstab.h"
+#include "../kernels/common.cuh"
 #include "../kernels/engine_kernels.h"
 #include "engine.h"
 #include "parallel.h"
@@ -553,7 +554,7 @@ void Engine::nesterov_step(int b, float step, float coeff) {
   }
   ph_end(PH_PLACE);
   ph_begin(PH_FINALIZE);
-  k_bins_finalize<<<r->nb_bins, kThreadsPerBlock, 0, stream_>>>(r->args, r->part, r->dens_split, r->split_ld, r->ticket, &dev_scal_[b].overflow);
+  check(launch_chained(k_bins_finalize, dim3(r->nb_bins), dim3(kThreadsPerBlock), 0, stream_, r->args, r->part, r->dens_split, r->split_ld, r->ticket, &dev_scal_[b].overflow), "nesterov_step");
   ph_end(PH_FINALIZE);
   check(cudaGetLastError(), "nesterov_step");
 }
@@ -662,7 +663,7 @@ void Engine::gradients(int b, SlotId out, float penalty, SlotId a1, SlotId b1, S
   if (r->n_cells) {
     ph_begin(PH_GRAD);
     launches += 1;
-    k_gradients<<<r->nb_cells, kThreadsPerBlock, 0, stream_>>>(r->args, c, pin_grad_, penalty, r->slot[out], pa1, pb1, pb2, r->part, r->ticket, &dev_scal_[b].wl_sum);
+    check(launch_chained(k_gradients, dim3(r->nb_cells), dim3(kThreadsPerBlock), 0, stream_, r->args, c, pin_grad_, penalty, r->slot[out], pa1, pb1, pb2, r->part, r->ticket, &dev_scal_[b].wl_sum), "gradients");
     ph_end(PH_GRAD);
   } else {
     check(cudaMemsetAsync(&dev_scal_[b].wl_sum, 0, 4 * sizeof(double), stream_), "gradients");

@@ -563,15 +563,7 @@ struct SysPair {
 };
 __device__ __forceinline__ SysDev pick(const SysPair &P) { return blockIdx.y ? P.a[1] : P.a[0]; }
 
-// The loop's kernels are launched chained (programmatic dependent launch): a kernel's blocks
-// may become resident while the kernel before it drains, and each first waits in hardware
-// (griddepcontrol.wait) until that kernel has completed and its memory is visible, before it
-// reads anything; it then lets the next kernel's blocks in. Launched unchained, the wait and
-// the release do nothing. No result changes.
-__device__ __forceinline__ void chain_enter() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-}
+// The loop's kernels are launched chained (common.cuh: chain_enter, launch_chained).
 
 __global__ void __launch_bounds__(kThreads) k2_update_p(SysPair P) {
   chain_enter();
@@ -758,17 +750,7 @@ cudaError_t bicgstab_solve(const CsrDev &A, const float *b, float *x, int max_it
 // One chained launch of a loop kernel (kThreads a block, no dynamic shared memory).
 template <typename... KArgs, typename... Args>
 static cudaError_t chained(void (*kernel)(KArgs...), dim3 grid, cudaStream_t st, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kernel, args...);
+  return launch_chained(kernel, grid, dim3(kThreads), 0, st, args...);
 }
 #define CK_LAUNCH(x)                        \
   do {                                      \

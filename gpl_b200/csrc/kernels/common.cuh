@@ -9,6 +9,30 @@
 
 namespace gpl {
 
+// Chained launches (programmatic dependent launch) for kernels that follow one another on a
+// stream: a chained kernel's blocks may become resident while the kernel before it drains;
+// each first waits in hardware (griddepcontrol.wait) until that kernel has completed and its
+// memory is visible, before it reads anything, then admits the next kernel's blocks. Launched
+// unchained, the wait and the release do nothing. No result changes.
+__device__ __forceinline__ void chain_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_chained(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 constexpr int kThreads = 256;
 
 // Rust `as i32` from f32/f64: round toward zero, saturating, NaN to 0 (PTX cvt.rzi clamps).

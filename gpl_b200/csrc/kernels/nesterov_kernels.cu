@@ -406,6 +406,7 @@ __device__ __forceinline__ void bins_finalize_block(const RegionArgs &r, double 
 }
 
 __global__ void __launch_bounds__(kThreads) k_bins_finalize(RegionArgs r, double *__restrict__ partials, __nv_bfloat16 *__restrict__ dens_split, int split_ld, unsigned int *ticket, double *out) {
+  chain_enter();
   bins_finalize_block(r, partials, dens_split, split_ld, ticket, out, blockIdx.x, gridDim.x);
 }
 
@@ -1099,6 +1100,7 @@ __device__ __forceinline__ void gradients_block(const RegionArgs &r, const CellA
 }
 
 __global__ void __launch_bounds__(kThreads, 6) k_gradients(RegionArgs r, CellArgs c, const float2 *__restrict__ pin_grad, float penalty, float2 *__restrict__ out_sum, const float2 *__restrict__ a1, const float2 *__restrict__ b1, const float2 *__restrict__ b2, double *__restrict__ partials, unsigned int *ticket, double *out) {
+  chain_enter();
   gradients_block(r, c, pin_grad, penalty, out_sum, a1, b1, b2, partials, ticket, out, blockIdx.x, gridDim.x);
 }
 

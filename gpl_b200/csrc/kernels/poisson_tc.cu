@@ -158,6 +158,7 @@ __device__ __forceinline__ void split_store(__nv_bfloat16 *row_hi, __nv_bfloat16
 template <int EPI, int BN>
 __global__ void __launch_bounds__(128, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tB0,
                                                    const __grid_constant__ CUtensorMap tA1, const __grid_constant__ CUtensorMap tB1, TcArgs args) {
+  chain_enter();
   using T = Tile<BN>;
   constexpr int STAGES = T::STAGES, STAGE_BYTES = T::STAGE_BYTES, B_TILE = T::B_TILE;
   constexpr uint32_t TMEM_COLS = T::TMEM_COLS, IDESC = T::IDESC;
@@ -413,21 +414,22 @@ cudaError_t tc_solve(PoissonPlan *p, float *field_x, float *field_y, cudaStream_
   // 1: T1t[v][x] = sum_y CyTs[v][y] rho[x][y]      M = ny, N = nx, K = ny
   a.M = ny, a.N = nx, a.K = ny;
   a.o[0] = TcOut{t->t1, nullptr, nx};
-  k_tc_gemm<EPI_SPLIT, 64><<<dim3(nx / 64, ny / BM, 1), 128, Tile<64>::SMEM_BYTES, s>>>(t->mCyTs, t->mDens, t->mCyTs, t->mDens, a);
+  cudaError_t le = launch_chained(k_tc_gemm<EPI_SPLIT, 64>, dim3(nx / 64, ny / BM, 1), dim3(128), Tile<64>::SMEM_BYTES, s, t->mCyTs, t->mDens, t->mCyTs, t->mDens, a);
+  if (le != cudaSuccess) return le;
   // 2: Ah[u][v] = sum_x CxTs[u][x] T1t[v][x]; spectral  M = nx, N = ny, K = nx
   a.M = nx, a.N = ny, a.K = nx;
   a.o[0] = TcOut{t->exh, t->eyh, ny};
-  k_tc_gemm<EPI_SPECTRAL, 64><<<dim3(ny / 64, nx / BM, 1), 128, Tile<64>::SMEM_BYTES, s>>>(t->mCxTs, t->mT1, t->mCxTs, t->mT1, a);
+  if ((le = launch_chained(k_tc_gemm<EPI_SPECTRAL, 64>, dim3(ny / 64, nx / BM, 1), dim3(128), Tile<64>::SMEM_BYTES, s, t->mCxTs, t->mT1, t->mCxTs, t->mT1, a)) != cudaSuccess) return le;
   // 3: T2t[y][u] = sum_v Cy[y][v] Exh[u][v]; T3t = Sy Eyh^T   M = ny, N = nx, K = ny
   a.M = ny, a.N = nx, a.K = ny;
   a.o[0] = TcOut{t->t2, nullptr, nx};
   a.o[1] = TcOut{t->t3, nullptr, nx};
-  k_tc_gemm<EPI_SPLIT, 128><<<dim3(nx / 128, ny / BM, 2), 128, Tile<128>::SMEM_BYTES, s>>>(t->mCy, t->mExh, t->mSy, t->mEyh, a);
+  if ((le = launch_chained(k_tc_gemm<EPI_SPLIT, 128>, dim3(nx / 128, ny / BM, 2), dim3(128), Tile<128>::SMEM_BYTES, s, t->mCy, t->mExh, t->mSy, t->mEyh, a)) != cudaSuccess) return le;
   // 4: Ex[x][y] = sum_u Sx[x][u] T2t[y][u]; Ey = Cx T3t^T     M = nx, N = ny, K = nx
   a.M = nx, a.N = ny, a.K = nx;
   a.o[0] = TcOut{field_x, nullptr, ny};
   a.o[1] = TcOut{field_y, nullptr, ny};
-  k_tc_gemm<EPI_F32, 128><<<dim3(ny / 128, nx / BM, 2), 128, Tile<128>::SMEM_BYTES, s>>>(t->mSx, t->mT2, t->mCx, t->mT3, a);
+  if ((le = launch_chained(k_tc_gemm<EPI_F32, 128>, dim3(ny / 128, nx / BM, 2), dim3(128), Tile<128>::SMEM_BYTES, s, t->mSx, t->mT2, t->mCx, t->mT3, a)) != cudaSuccess) return le;
   return cudaGetLastError();
 }
 

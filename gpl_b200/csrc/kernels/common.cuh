@@ -112,6 +112,37 @@ __device__ __forceinline__ bool last_block_done(unsigned int *ticket) { return l
 // t + NT, ... then the block's sum, so the order is fixed for a block of NT threads.
 template <int NT>
 __device__ __forceinline__ void reduce_rows(const double *partials, int nblk, int width, double *out, double *sh) {
+  if ((width == 2 || width == 4) && ((uintptr_t)partials & 15) == 0) {
+    // a row's columns in 16-byte loads, four rows in flight; each column's terms still add in
+    // the same order (rows t, t + NT, ...) and meet in the same block sum
+    double s[4] = {0, 0, 0, 0};
+    const int h = width / 2;
+    const double2 *p = reinterpret_cast<const double2 *>(partials);
+    int b = threadIdx.x;
+    for (; b + 3 * NT < nblk; b += 4 * NT) {
+      double2 v[4][2];
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        for (int q = 0; q < h; q++) v[u][q] = __ldcg(p + (size_t)(b + u * NT) * h + q);
+#pragma unroll
+      for (int u = 0; u < 4; u++)
+        for (int q = 0; q < h; q++) {
+          s[2 * q] += v[u][q].x;
+          s[2 * q + 1] += v[u][q].y;
+        }
+    }
+    for (; b < nblk; b += NT)
+      for (int q = 0; q < h; q++) {
+        const double2 v = __ldcg(p + (size_t)b * h + q);
+        s[2 * q] += v.x;
+        s[2 * q + 1] += v.y;
+      }
+    for (int j = 0; j < width; j++) {
+      double t = block_sum<NT>(s[j], sh);
+      if (threadIdx.x == 0) out[j] = t;
+    }
+    return;
+  }
   for (int j = 0; j < width; j++) {
     double s = 0;
     for (int b = threadIdx.x; b < nblk; b += NT) s += __ldcg(partials + (size_t)b * width + j);

@@ -94,8 +94,11 @@ Engine::Engine(int device) : device_(device) {
   cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
   if (!failed()) check(cudaStreamCreateWithPriority(&stream_, cudaStreamNonBlocking, prio_hi), "cudaStreamCreate");
   if (!failed()) check(cudaStreamCreateWithPriority(&wa_stream_, cudaStreamNonBlocking, prio_lo), "cudaStreamCreate");
+  if (!failed()) check(cudaStreamCreateWithPriority(&wa2_stream_, cudaStreamNonBlocking, prio_lo), "cudaStreamCreate");
   if (!failed()) check(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming), "cudaEventCreate");
   if (!failed()) check(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming), "cudaEventCreate");
+  if (!failed()) check(cudaEventCreateWithFlags(&ev_split_, cudaEventDisableTiming), "cudaEventCreate");
+  if (!failed()) check(cudaEventCreateWithFlags(&ev_join2_, cudaEventDisableTiming), "cudaEventCreate");
   // the degree-2..4 nets' WA form, timed in place; GPL_WA_SMALL=lean|nets|pins fixes it
   if (!failed()) wa_tune_ = std::make_unique<Tuner>("small-net WA", std::vector<std::string>{"lean", "nets", "pins"}, "GPL_WA_SMALL", 3, 256);
   if (!failed()) pk_scatter_tune_ = std::make_unique<Tuner>("packed scatter", std::vector<std::string>{"tiles", "global", "pooled"}, "GPL_SCATTER", 3, 64);
@@ -105,6 +108,7 @@ Engine::Engine(int device) : device_(device) {
 void Engine::join() {
   if (!wa_pending_) return;
   check(cudaStreamWaitEvent(stream_, ev_join_, 0), "join");
+  check(cudaStreamWaitEvent(stream_, ev_join2_, 0), "join");
   wa_pending_ = false;
 }
 
@@ -140,8 +144,12 @@ Engine::~Engine() {
   if (pk_dev_) cudaFree(pk_dev_);
   if (pinned_) cudaFreeHost(pinned_);
   if (wa_stream_) cudaStreamSynchronize(wa_stream_);
+  if (wa2_stream_) cudaStreamSynchronize(wa2_stream_);
   if (stream_) cudaStreamDestroy(stream_);
   if (wa_stream_) cudaStreamDestroy(wa_stream_);
+  if (wa2_stream_) cudaStreamDestroy(wa2_stream_);
+  if (ev_split_) cudaEventDestroy(ev_split_);
+  if (ev_join2_) cudaEventDestroy(ev_join2_);
   if (ev_fork_) cudaEventDestroy(ev_fork_);
   if (ev_join_) cudaEventDestroy(ev_join_);
 }
@@ -611,12 +619,18 @@ void Engine::wa(float cx, float cy) {
   w.hpwl_out = hpwl_acc_;
   hpwl_ready_ = true;
   hpwl_fetched_ = false;
+  cudaStream_t st2 = st;
+  if (overlap_) {
+    check(cudaEventRecord(ev_split_, st), "wa split");
+    check(cudaStreamWaitEvent(wa2_stream_, ev_split_, 0), "wa split");
+    st2 = wa2_stream_;
+  }
   ph_begin(PH_WA, st);
   if (wa_small_blocks(small_)) {
     launches += 1;
-    const int form = wa_tune_->start(st);
-    launch_wa_small(w, cx, cy, 1, st, form);
-    wa_tune_->stop(st);
+    const int form = wa_tune_->start(st2);
+    launch_wa_small(w, cx, cy, 1, st2, form);
+    wa_tune_->stop(st2);
   }
   if (n_tiles_) {
     launches += 1;
@@ -630,6 +644,7 @@ void Engine::wa(float cx, float cy) {
   check(cudaGetLastError(), "wa");
   if (overlap_) {
     check(cudaEventRecord(ev_join_, st), "wa join");
+    check(cudaEventRecord(ev_join2_, st2), "wa join");
     wa_pending_ = true;
   }
 }

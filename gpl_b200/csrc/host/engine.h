@@ -195,7 +195,10 @@ class Engine {
   // centres joins it first. Both kernels fill every SM, so the gain is small (a few percent
   // of a trial, measured); off runs them one after the other.
   cudaStream_t wa_stream_ = nullptr;
-  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
+  // the small nets' WA beside the tiles' WA (disjoint pins; the HPWL adds are exact): a second
+  // stream forked after the HPWL accumulator is cleared, joined with the first
+  cudaStream_t wa2_stream_ = nullptr;
+  cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr, ev_split_ = nullptr, ev_join2_ = nullptr;
   std::unique_ptr<Tuner> wa_tune_;
   std::thread *prewarm_ = nullptr;
   // packed launches: the queue of (phase, region) with each entry's arguments as queued, the
